@@ -1,0 +1,443 @@
+#!/usr/bin/env python
+"""Benchmark of the LJ hot path: pair-interactions per second on the 1,048,576-molecule FCC box
+(rho 0.75, T 0.9, rc 3.0, dt 0.002, truncated-shifted LJ), FP32 pair arithmetic with FP64
+accumulation on one B200 (one independent box per GPU when run on several).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision mixed|fp64]
+
+One step = Leapfrog kick+drift, periodic wrap + linked-cell binning, the pair traversal (forces,
+Upot, virial) and the closing kick with sum m v^2, i.e. Simulation::simulateStep's hot path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "LJ pair-interactions/s, 1M atoms, 1 B200: FP32/FP64-acc vs FP64 at ≤1e-5 err"
+UNIT = "pair-interactions/s"
+FLOPS_PER_PAIR = 31  # algorithmic flops per interacting pair (FMA = 2): see DESIGN.md
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--no-compare", action="store_true", help="skip the FP64 drop-in comparison leg")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=25.0, help="bound of the CPU baseline sample")
+    return ap.parse_args()
+
+
+def workload_config(system, precision):
+    return {"workload": "lj_fcc_1m_rho0.75_T0.9_rc3.0", "n_molecules": int(system.n), "density": 0.75,
+            "temperature": 0.9, "cutoff": float(system.cutoff), "dt": float(system.dt),
+            "potential": "LJ 12-6 truncated-shifted, single species", "ensemble": "NVE",
+            "pair_arithmetic": "fp32, fp64 accumulation" if precision == "mixed" else "fp64",
+            "l2": "flushed (256 MiB write) before every timed step"}
+
+
+# ---------------------------------------------------------------------------- distributed plumbing
+
+class Dist:
+    def __init__(self, want):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.barrier()
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (read-only queries)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------- our arm
+
+def make_system(rank: int):
+    from madpac_b200 import workloads as W
+
+    return W.config_c2(seed=2 + rank)
+
+
+def time_device_resident(M, lc, system, steps, warmup, flush, stream):
+    """Device-resident steps: inputs in HBM, L2 flushed before every step, CUDA events on the
+    library's stream around each step. Returns (seconds, pairs, records, launches)."""
+    import torch
+
+    dt = system.dt
+    for _ in range(warmup):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        lc.runAsync(1, dt)
+    lc.readSteps(warmup)
+    launches0 = lc.profileRead()[1][3]
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            ev[k][0].record(stream)
+        lc.runAsync(1, dt)
+        ev[k][1].record(stream)
+    rec = lc.readSteps(steps)
+    torch.cuda.synchronize()
+    launches = int(lc.profileRead()[1][3] - launches0)
+    seconds = sum(a.elapsed_time(b) for a, b in ev) * 1e-3
+    return seconds, float(rec[:, 3].sum()), rec, launches
+
+
+def time_kernels(lc, system, steps, flush, stream):
+    """Per-kernel-group device time (CUDA events on the library's stream) over `steps` steps."""
+    import torch
+
+    lc.profileRead(reset=True)
+    lc.profileEnable(True)
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        lc.runAsync(1, system.dt)
+    rec = lc.readSteps(steps)
+    t, cnt = lc.profileRead(reset=True)
+    lc.profileEnable(False)
+    return t, cnt, rec
+
+
+def time_e2e(M, lc, system, steps, stream):
+    """The same steps through the C ABI with host buffers: per step the caller uploads r, v from
+    pinned host memory, runs mdgpu_step and downloads r, v, F and the step's scalars."""
+    import torch
+
+    n = system.n
+    pin = lambda: torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
+    r, v, F = pin(), pin(), pin()
+    st = lc.getParticles()
+    r[:], v[:] = st["r"], st["v"]
+    pairs = 0.0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        lc.setState(r=r, v=v)
+        out = lc.step(system.dt, 1.0)
+        pairs += out[3]
+        st = lc.lib.mdgpu_get_particles(lc.h, n, None, None, r.ctypes.data, v.ctypes.data, F.ctypes.data)
+        if st != 0:
+            raise M.MdgpuError(st, lc.lib.mdgpu_last_error(lc.h).decode())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    seconds = e0.elapsed_time(e1) * 1e-3
+    return seconds, pairs, 48 * n, 72 * n + 32
+
+
+def count_pairs_host(system) -> float:
+    from scipy.spatial import cKDTree
+
+    tree = cKDTree(np.mod(system.r, system.length), boxsize=system.length)
+    return (tree.count_neighbors(tree, system.cutoff) - system.n) / 2.0
+
+
+def cpu_baseline(system, seconds_bound: float, pairs=None):
+    """The reference's own CPU path on a bounded sample of the same workload: the reference
+    harness (oracle/_ref/ref_driver, the unmodified MarDyn sources) when it was built, else the
+    oracle's C restatement; single-threaded like the reference's sequential build."""
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    if pairs is None:
+        pairs = count_pairs_host(system)
+    if os.path.exists(ref):
+        from madpac_b200 import workloads as W
+
+        tmp = tempfile.mkdtemp(prefix="mdref_")
+        W.write_inp(system, os.path.join(tmp, "sys.inp"))
+        W.write_cfg(system, os.path.join(tmp, "sys.cfg"), "sys.inp")
+        nsteps = 3
+        out = subprocess.run([ref, "--time", "sys.cfg", str(nsteps)], cwd=tmp, capture_output=True, text=True,
+                             timeout=max(120.0, 8 * seconds_bound))
+        sec = json.loads(out.stdout.strip().splitlines()[-1])["seconds_per_step"]
+        kind, sample = "reference", f"{nsteps} steps of the full {system.n}-molecule box (after prepare_start)"
+    else:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        o = O.Oracle(system)
+        o.init()
+        o.prepare_start()
+        nsteps = 2
+        t0 = time.perf_counter()
+        for _ in range(nsteps):
+            o.step()
+        sec = (time.perf_counter() - t0) / nsteps
+        kind, sample = "port", f"{nsteps} steps of the full {system.n}-molecule box on the oracle"
+    return {"value": pairs / sec, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample,
+            "seconds_per_step": sec, "pairs_per_step": pairs}
+
+
+def run_ours(args, dist: Dist):
+    import torch
+
+    from madpac_b200 import mdgpu as M
+
+    torch.cuda.set_device(dist.local)
+    precision = M.MIXED if args.precision == "mixed" else M.FP64
+    system = make_system(dist.rank)
+    lc = M.LinkedCells.from_system(system, precision, device=dist.local)
+    lc.update()
+    lc.traversePairs()
+    stream = torch.cuda.ExternalStream(lc.stream())
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{dist.local}")
+
+    dist.barrier()
+    clocks = ClockSampler(dist.local)
+    clocks.start()
+    seconds, pairs, rec, launches = time_device_resident(M, lc, system, args.steps, args.warmup, flush, stream)
+    clk = clocks.stop()
+    dist.barrier()
+    t_max = dist.max(seconds)
+    pairs_all = dist.sum(pairs)
+    value = pairs_all / t_max
+
+    # kernel-level timing for the roofline (separate, profiled pass)
+    tk, cnt, rec2 = time_kernels(lc, system, args.steps, flush, stream)
+    pair_ms = tk[1] / max(cnt[1], 1)
+    pairs_per_launch = float(rec2[:, 3].mean())
+    fp32_peak, fp64_peak = M.device_peaks(dist.local)
+    peak = fp32_peak if precision == M.MIXED else fp64_peak
+    achieved = pairs_per_launch * FLOPS_PER_PAIR / (pair_ms * 1e-3) / 1e12
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "pair_kernel_traffic.json")
+    if os.path.exists(tf):
+        d = json.load(open(tf)).get(args.precision)
+        if d:
+            traffic = d["dram_bytes_per_pair"] * pairs_per_launch
+    n = system.n
+    bin_bytes = n * 184.0
+    int_bytes = n * (124.0 + 76.0)
+    hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs") if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+
+    # end to end through the C ABI with host buffers
+    e2e_s, e2e_pairs, h2d, d2h = time_e2e(M, lc, system, max(3, args.steps // 2), stream)
+    e2e_s = dist.max(e2e_s)
+    e2e_value = dist.sum(e2e_pairs) / e2e_s
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 pair arithmetic, f64 accumulation" if precision == M.MIXED else "f64",
+        "data": "synthetic (seeded FCC lattice, Maxwell-Boltzmann velocities)",
+        "config": workload_config(system, args.precision),
+        "steps_per_s": args.steps / t_max,
+        "pairs_per_step": pairs / args.steps,
+        "roofline": {"bound": "fp32" if precision == M.MIXED else "fp64", "kernel": "pair traversal",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": "measured FMA microbenchmark (mdgpu_device_peaks)",
+                     "flops_per_pair": FLOPS_PER_PAIR, "launch_ms": pair_ms},
+        "kernels_ms_per_step": {"binning": tk[0] / args.steps, "pairs": tk[1] / args.steps,
+                                "integration": tk[2] / args.steps},
+        "hbm_kernels": {"binning_gbs": bin_bytes / (tk[0] / args.steps * 1e-3) / 1e9,
+                        "integration_gbs": int_bytes / (tk[2] / args.steps * 1e-3) / 1e9,
+                        "peak_gbs": hbm, "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if not args.no_compare and dist.world == 1:
+        other = M.FP64 if precision == M.MIXED else M.MIXED
+        lc2 = M.LinkedCells.from_system(system, other, device=dist.local)
+        lc2.update()
+        lc2.traversePairs()
+        ref_lc = lc2 if other == M.FP64 else None
+        s2, p2, _, _ = time_device_resident(M, lc2, system, args.steps, args.warmup, flush,
+                                            torch.cuda.ExternalStream(lc2.stream()))
+        out["fp64_dropin" if other == M.FP64 else "mixed"] = {"value": p2 / s2, "ms_per_step": s2 / args.steps * 1e3}
+        # accuracy of the mixed form at the first force evaluation, against the FP64 drop-in
+        a = M.LinkedCells.from_system(system, M.MIXED, device=dist.local)
+        b = M.LinkedCells.from_system(system, M.FP64, device=dist.local)
+        a.update()
+        b.update()
+        ua, wa, _ = a.traversePairs()
+        ub, wb, _ = b.traversePairs()
+        Fa, Fb = a.getParticles()["F"], b.getParticles()["F"]
+        rms = float(np.sqrt(np.mean(np.sum(Fb * Fb, axis=1))))
+        out["accuracy_vs_fp64"] = {
+            "force_err_rms": float(np.sqrt(np.mean(np.sum((Fa - Fb) ** 2, axis=1)))) / rms,
+            "force_err_max": float(np.max(np.linalg.norm(Fa - Fb, axis=1))) / rms,
+            "upot_rel": abs(ua - ub) / abs(ub), "virial_rel": abs(wa - wb) / abs(wb)}
+        for x in (lc2, a, b):
+            x.close()
+        del ref_lc
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        try:
+            out["cpu_baseline"] = cpu_baseline(system, args.cpu_seconds, pairs=float(rec[0, 3]))
+        except Exception as e:  # the baseline is reported, never required
+            out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    lc.close()
+    return out
+
+
+# ---------------------------------------------------------------------------- reference arm
+
+def run_reference(args, dist: Dist):
+    """The reference's own CPU implementation (unmodified MarDyn sources, sequential build) on the
+    same workload; rank 0 only."""
+    system = make_system(0)
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    pairs = count_pairs_host(system)
+    if os.path.exists(ref):
+        from madpac_b200 import workloads as W
+
+        tmp = tempfile.mkdtemp(prefix="mdref_")
+        W.write_inp(system, os.path.join(tmp, "sys.inp"))
+        W.write_cfg(system, os.path.join(tmp, "sys.cfg"), "sys.inp")
+        # bounded: at most ~150 s of stepping
+        probe = subprocess.run([ref, "--time", "sys.cfg", "1"], cwd=tmp, capture_output=True, text=True)
+        t1 = json.loads(probe.stdout.strip().splitlines()[-1])["seconds_per_step"]
+        nsteps = max(1, min(args.steps, int(150.0 / max(t1, 1e-3))))
+        out = subprocess.run([ref, "--time", "sys.cfg", str(nsteps)], cwd=tmp, capture_output=True, text=True)
+        sec = json.loads(out.stdout.strip().splitlines()[-1])["seconds_per_step"]
+        kind, sample = "reference", (f"{nsteps} timed steps (of {args.steps} asked; bounded to ~150 s) of the full "
+                                     f"{system.n}-molecule box, after prepare_start and one untimed probe step")
+    else:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        o = O.Oracle(system)
+        o.init()
+        o.prepare_start()
+        for _ in range(min(args.warmup, 1)):
+            o.step()
+        nsteps = max(1, min(args.steps, 10))
+        t0 = time.perf_counter()
+        for _ in range(nsteps):
+            o.step()
+        sec = (time.perf_counter() - t0) / nsteps
+        kind, sample = "port", f"{nsteps} steps of the full {system.n}-molecule box on the C restatement"
+    value = pairs / sec
+    return {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": dist.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(system, "fp64"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+class _Solo:
+    """Rank bookkeeping without a process group (the reference arm runs on rank 0 only)."""
+
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        solo = _Solo()
+        if solo.rank == 0:
+            print(json.dumps(run_reference(args, solo)), flush=True)
+        return
+    dist = Dist(args.gpus)
+    out = run_ours(args, dist)
+    if dist.rank == 0:
+        print(json.dumps(out), flush=True)
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,145 @@
+/*
+ * mdgpu.h -- C ABI of the B200 (sm_100a) short-range Lennard-Jones hot path that stands in for
+ * MarDyn's LinkedCells container, its LJ pair handler and its Leapfrog integrator.
+ *
+ * All entry points take plain host pointers and sizes (no CUDA or torch types), return an int
+ * status (MDGPU_OK = 0) and leave a message for mdgpu_last_error(). Particle arrays are given and
+ * returned in the caller's order (the order of the last mdgpu_set_particles call); positions,
+ * velocities and forces are (n, 3) row-major doubles. Component ids are 0-based.
+ *
+ * Reference interfaces (paths relative to madpac/mardyn/) each entry point replaces are named
+ * beside it. The shim in madpac_b200/shim/ binds them to MarDyn's ParticleContainer and
+ * Integrator classes.
+ */
+#ifndef MDGPU_H
+#define MDGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference's exit() paths become status codes) ---------------------- */
+#define MDGPU_OK 0
+#define MDGPU_ERR_ARG 1              /* bad argument or unsupported configuration */
+#define MDGPU_ERR_CUDA 2             /* a CUDA runtime call failed */
+#define MDGPU_ERR_STATE 3            /* cells invalid: call mdgpu_update first (LinkedCells.cpp:294-297 exit(1)) */
+#define MDGPU_ERR_BOX_TOO_SMALL 5    /* fewer than 2 cells per dimension (LinkedCells.cpp:81-88 exit(5)) */
+#define MDGPU_ERR_OUTSIDE_HALO 6     /* a molecule left the halo box in one step (LinkedCells.cpp:539-541) */
+#define MDGPU_ERR_SAME_POSITION 7    /* two molecules at the same position (Molecule.cpp:455-456 exit(1)) */
+#define MDGPU_ERR_NONFINITE 8        /* a force, energy or velocity became NaN/Inf */
+#define MDGPU_ERR_TIMEOUT 9          /* a bounded device-side wait gave up */
+#define MDGPU_ERR_CAPACITY 10        /* a workload exceeds a fixed device buffer */
+
+/* ---- precision modes ---------------------------------------------------------------------- */
+#define MDGPU_FP64 0   /* every pair in double precision, same operation order as PotForceLJ */
+#define MDGPU_MIXED 1  /* pair arithmetic in FP32, forces/energy/virial accumulated in FP64 */
+
+/* One single-site LJ component: one LJ centre at the molecule origin.
+ * Mirrors Component::addLJcenter (molecules/Component.cpp:44-72) with do_shift the
+ * TRUNCATED_SHIFTED flag read by InputOldstyle (io/InputOldstyle.cpp:162-166). */
+typedef struct mdgpu_component {
+	double eps;
+	double sigma;
+	double mass;
+	int do_shift;
+} mdgpu_component;
+
+typedef struct mdgpu_ctx mdgpu_ctx;
+
+/* Build a container for a periodic box [0, length) on CUDA device `device`.
+ * Replaces the LinkedCells constructor (particleContainer/LinkedCells.cpp:41-94), its
+ * initializeCells/calculateNeighbourIndices (:457-533), Comp2Param::initialize
+ * (molecules/Comp2Param.cpp:28-115) and Domain::initParameterStreams (Domain.cpp:570-572).
+ * cutoff is cutoffRadius (cells and pair search), lj_cutoff is LJCutoffRadius (0 = cutoff);
+ * cells_in_cutoff must be 1. mix holds (xi, eta) for each component pair i<j in the order of
+ * InputOldstyle.cpp:206-215 (may be NULL for one component). */
+int mdgpu_create(mdgpu_ctx** out, const double length[3], double cutoff, double lj_cutoff,
+                 double cells_in_cutoff, int ncomp, const mdgpu_component* comps, const double* mix,
+                 int precision, int device);
+/* Frees every device buffer of the context. */
+int mdgpu_destroy(mdgpu_ctx* ctx);
+/* Message of the last failed call on this context ("" if none). */
+const char* mdgpu_last_error(const mdgpu_ctx* ctx);
+/* Switch between MDGPU_FP64 and MDGPU_MIXED. */
+int mdgpu_set_precision(mdgpu_ctx* ctx, int precision);
+
+/* Load n molecules (replaces the InputOldstyle::readPhaseSpace -> LinkedCells::addParticle loop,
+ * io/InputOldstyle.cpp:324-378, LinkedCells.cpp:182-204). F may be NULL (zero forces). */
+int mdgpu_set_particles(mdgpu_ctx* ctx, int64_t n, const uint64_t* id, const int32_t* cid,
+                        const double* r, const double* v, const double* F);
+/* Overwrite positions and velocities of the loaded molecules (caller order). */
+int mdgpu_set_state(mdgpu_ctx* ctx, int64_t n, const double* r, const double* v);
+/* Read molecules back in caller order (replaces iteration with ParticleContainer::begin/next,
+ * ParticleContainer.h:100-113). Any output pointer may be NULL. */
+int mdgpu_get_particles(mdgpu_ctx* ctx, int64_t n, uint64_t* id, int32_t* cid, double* r, double* v,
+                        double* F);
+/* Number of molecules held (replaces LinkedCells::getNumberOfParticles, LinkedCells.cpp:301-303). */
+int mdgpu_num_particles(const mdgpu_ctx* ctx, int64_t* n);
+/* Cell geometry: box_cells[3] = boxWidthInNumCells, cell_length[3], halo_min[3]
+ * (LinkedCells.cpp:54-66). */
+int mdgpu_get_geometry(const mdgpu_ctx* ctx, int32_t box_cells[3], double cell_length[3],
+                       double halo_min[3]);
+
+/* Periodic wrap and linked-cell binning by counting sort (replaces LinkedCells::update,
+ * LinkedCells.cpp:165-180, together with the wrap that DomainDecompDummy::exchangeMolecules +
+ * LinkedCells::deleteOuterParticles perform, parallel/DomainDecompDummy.cpp:22-116,
+ * LinkedCells.cpp:339-371). */
+int mdgpu_update(mdgpu_ctx* ctx);
+/* Cell index of each molecule in caller order, in the reference's halo-inclusive numbering
+ * (LinkedCells::getCellIndexOfMolecule, LinkedCells.cpp:535-551). */
+int mdgpu_get_cell_index(mdgpu_ctx* ctx, int64_t n, int64_t* cell);
+/* Forces on all molecules plus the local potential energy and virial (replaces
+ * LinkedCells::traversePairs -> BlockTraverse::traversePairs, BlockTraverse.cpp:89-350, with
+ * ParticlePairs2PotForceAdapter::init/processPair/finish, adapter/ParticlePairs2PotForceAdapter.h:52-115,
+ * and PotForce/PotForceLJ, molecules/potforce.h:41-53, 319-363). upot and virial receive what
+ * finish() stores with Domain::setLocalUpot/setLocalVirial (Domain.cpp:102-108); npairs (may be
+ * NULL) receives the number of unordered pairs with r < cutoff. */
+int mdgpu_traverse_pairs(mdgpu_ctx* ctx, double* upot, double* virial, double* npairs);
+/* Leapfrog first half: v = vcorr*v + dt/(2m)*F; r += dt*v for every molecule (replaces
+ * Leapfrog::transition1to2, integrators/Leapfrog.cpp:37-51, Molecule::upd_preF, Molecule.cpp:128-135). */
+int mdgpu_leapfrog_pre(mdgpu_ctx* ctx, double dt, double vcorr);
+/* Leapfrog second half: v += dt_half/m*F and sum m v^2 (replaces Leapfrog::transition2to3,
+ * Leapfrog.cpp:53-99, Molecule::upd_postF, Molecule.cpp:193-216). */
+int mdgpu_leapfrog_post(mdgpu_ctx* ctx, double dt_half, double* summv2);
+/* v *= beta for every molecule (the velocity scaling of Simulation::thermostatEtc,
+ * Simulation.cpp:1172-1176). */
+int mdgpu_scale_velocities(mdgpu_ctx* ctx, double beta);
+/* Far-field LJ corrections UpotCorr and VirialCorr for unshifted pairs (replaces
+ * Domain::initFarFieldCorr, Domain.cpp:574-677, single-centre LJ part). */
+int mdgpu_far_field_correction(mdgpu_ctx* ctx, double* upot_corr, double* virial_corr);
+/* One NVE/thermostatted time step as Simulation::simulateStep runs it (Simulation.cpp:1218-1229):
+ * leapfrog_pre(dt, vcorr), update, traverse_pairs, leapfrog_post(dt/2). out[0..3] = local Upot,
+ * local virial, sum m v^2, pair count. */
+int mdgpu_step(mdgpu_ctx* ctx, double dt, double vcorr, double* out4);
+/* nsteps NVE steps without host round trips; per_step (may be NULL) receives nsteps rows of the
+ * four values of mdgpu_step. */
+int mdgpu_run(mdgpu_ctx* ctx, int32_t nsteps, double dt, double* per_step);
+
+/* Enqueue nsteps NVE steps on the context's stream and return without waiting; each step's four
+ * values (see mdgpu_step) are appended to a device-side record kept until mdgpu_read_steps. */
+int mdgpu_run_async(mdgpu_ctx* ctx, int32_t nsteps, double dt);
+/* Wait for the enqueued steps, copy the first nsteps records (nsteps x 4), clear the record and
+ * report status. */
+int mdgpu_read_steps(mdgpu_ctx* ctx, int32_t nsteps, double* per_step);
+
+/* Device-side timing of the kernels this context launches, for benchmarking: when enabled, CUDA
+ * events on the context's stream bracket the binning, pair and integration kernels. times_ms[0..2]
+ * = total binning, pair, integration milliseconds since the last reset; counts[0..3] = launches of
+ * each group and of all kernels. */
+int mdgpu_profile_enable(mdgpu_ctx* ctx, int enable);
+int mdgpu_profile_read(mdgpu_ctx* ctx, double times_ms[3], int64_t counts[4], int reset);
+/* The cudaStream_t the context launches on, as an opaque pointer. */
+int mdgpu_get_stream(const mdgpu_ctx* ctx, void** stream);
+/* Block until the context's stream is idle and report any pending device status. */
+int mdgpu_synchronize(mdgpu_ctx* ctx);
+/* Measured peak FMA throughput of CUDA device `device` (dependent FMA chains in registers, all
+ * SMs busy), in TFLOP/s counting an FMA as 2 flops; used as the roofline of the pair kernels. */
+int mdgpu_device_peaks(int device, double* fp32_tflops, double* fp64_tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MDGPU_H */

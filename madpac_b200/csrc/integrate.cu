@@ -1,0 +1,127 @@
+// Leapfrog (velocity Verlet) update, velocity scaling and the per-step record of mdgpu_run.
+//
+// The translational updates follow Molecule::upd_preF (molecules/Molecule.cpp:128-135) and
+// Molecule::upd_postF (Molecule.cpp:193-205) operation by operation, with explicit
+// round-to-nearest intrinsics so that no multiply-add contraction changes a bit:
+//   pre:  v = vcorr*v + dtInv2m*F;  r += dt*v           (dtInv2m = (0.5*dt)/m)
+//   post: v += dtInv2m*F;  sum m*(v0^2+v1^2+v2^2)       (dtInv2m = dt_half/m)
+// For single-site LJ molecules the quaternion and angular-momentum parts of those functions
+// leave r and v untouched (no torque, zero inertia), so they are not evaluated.
+#include <cuda_runtime.h>
+
+#include "md_internal.h"
+#include "reduce.cuh"
+
+namespace mdgpu {
+namespace {
+
+struct SpeciesScale {
+	double dtInv2m[kMaxSpecies];
+	double mass[kMaxSpecies];
+};
+
+__global__ void __launch_bounds__(kReduceBlock) k_leapfrog_pre(int64_t n, Particles p, SpeciesScale s, double dt,
+                                                              double vcorr) {
+	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const double a = s.dtInv2m[p.cid[i]];
+	double v;
+	v = __dadd_rn(__dmul_rn(vcorr, p.vx[i]), __dmul_rn(a, p.fx[i]));
+	p.vx[i] = v;
+	p.rx[i] = __dadd_rn(p.rx[i], __dmul_rn(dt, v));
+	v = __dadd_rn(__dmul_rn(vcorr, p.vy[i]), __dmul_rn(a, p.fy[i]));
+	p.vy[i] = v;
+	p.ry[i] = __dadd_rn(p.ry[i], __dmul_rn(dt, v));
+	v = __dadd_rn(__dmul_rn(vcorr, p.vz[i]), __dmul_rn(a, p.fz[i]));
+	p.vz[i] = v;
+	p.rz[i] = __dadd_rn(p.rz[i], __dmul_rn(dt, v));
+}
+
+__global__ void __launch_bounds__(kReduceBlock) k_leapfrog_post(int64_t n, Particles p, SpeciesScale s,
+                                                               double* partials, int* status) {
+	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	double mv2 = 0.0;
+	if (i < n) {
+		const int t = p.cid[i];
+		const double a = s.dtInv2m[t];
+		const double vx = __dadd_rn(p.vx[i], __dmul_rn(a, p.fx[i]));
+		const double vy = __dadd_rn(p.vy[i], __dmul_rn(a, p.fy[i]));
+		const double vz = __dadd_rn(p.vz[i], __dmul_rn(a, p.fz[i]));
+		p.vx[i] = vx;
+		p.vy[i] = vy;
+		p.vz[i] = vz;
+		const double v2 = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
+		mv2 = __dmul_rn(s.mass[t], v2);
+		if (!(v2 == v2) || isinf(v2)) atomicOr(status, kStatusNonFinite);
+	}
+	block_sum3(mv2, 0.0, 0.0, partials);
+}
+
+__global__ void k_scale(int64_t n, Particles p, double beta) {
+	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	p.vx[i] = __dmul_rn(p.vx[i], beta);
+	p.vy[i] = __dmul_rn(p.vy[i], beta);
+	p.vz[i] = __dmul_rn(p.vz[i], beta);
+}
+
+// dst[0..3] = local Upot, local virial, sum m v^2, pair count of the step just finished.
+__global__ void k_record(const double* __restrict__ scalars, double* dst) {
+	if (threadIdx.x == 0) {
+		dst[0] = scalars[0] * 0.5 / 6.;
+		dst[1] = scalars[1] * 0.5;
+		dst[2] = scalars[3];
+		dst[3] = scalars[2] * 0.5;
+	}
+}
+
+SpeciesScale make_scale(const Context* c, double dt_half) {
+	SpeciesScale s{};
+	for (int k = 0; k < c->sp.n; k++) {
+		s.dtInv2m[k] = dt_half / c->sp.mass[k];
+		s.mass[k] = c->sp.mass[k];
+	}
+	return s;
+}
+
+inline unsigned blocks_for(int64_t n) { return (unsigned) ((n + kReduceBlock - 1) / kReduceBlock); }
+
+}  // namespace
+
+cudaError_t launch_leapfrog_pre(Context* c, double dt, double vcorr) {
+	if (c->n == 0) return cudaSuccess;
+	prof_begin(c, 2);
+	// dt_halve = .5 * dt, dtInv2m = dt_halve / m  (Molecule.cpp:130-131)
+	k_leapfrog_pre<<<blocks_for(c->n), kReduceBlock, 0, c->stream>>>(c->n, c->p, make_scale(c, .5 * dt), dt, vcorr);
+	cudaError_t e = cudaGetLastError();
+	prof_end(c, 2, 1);
+	return e;
+}
+
+cudaError_t launch_leapfrog_post(Context* c, double dt_half) {
+	prof_begin(c, 2);
+	int64_t nb = c->n > 0 ? blocks_for(c->n) : 1;
+	k_leapfrog_post<<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(c->n, c->p, make_scale(c, dt_half), c->partials,
+	                                                               c->status);
+	cudaError_t e = cudaGetLastError();
+	prof_end(c, 2, 1);
+	if (e != cudaSuccess) return e;
+	return launch_reduce(c, nb, c->scalars + 3, 1);
+}
+
+cudaError_t launch_scale(Context* c, double beta) {
+	if (c->n == 0) return cudaSuccess;
+	prof_begin(c, 2);
+	k_scale<<<blocks_for(c->n), kReduceBlock, 0, c->stream>>>(c->n, c->p, beta);
+	cudaError_t e = cudaGetLastError();
+	prof_end(c, 2, 1);
+	return e;
+}
+
+cudaError_t launch_step_record(Context* c, double* dst) {
+	k_record<<<1, 32, 0, c->stream>>>(c->scalars, dst);
+	count_launches(c, 1);
+	return cudaGetLastError();
+}
+
+}  // namespace mdgpu

@@ -1,0 +1,124 @@
+// Internal state of an mdgpu context and the launch helpers shared by the .cu files.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "mdgpu.h"
+
+namespace mdgpu {
+
+constexpr int kMaxSpecies = 8;
+constexpr int kReduceBlock = 256;   // block size of every kernel that writes reduction partials
+
+// Device status bits (OR-ed by kernels, mapped to MDGPU_ERR_* by the host).
+enum : int {
+	kStatusOutsideHalo = 1,
+	kStatusSamePosition = 2,
+	kStatusNonFinite = 4,
+	kStatusTimeout = 8,
+	kStatusCapacity = 16,
+};
+
+// Comp2Param stream entries per ordered component pair, as doubles and floats.
+struct Species {
+	int n;
+	double eps24[kMaxSpecies * kMaxSpecies];
+	double sig2[kMaxSpecies * kMaxSpecies];
+	double shift6[kMaxSpecies * kMaxSpecies];
+	double mass[kMaxSpecies];
+};
+
+// What the pair kernels read: cutoffs and the Comp2Param table (uploaded once per context).
+struct PairParams {
+	int ns;
+	double rc2, rclj2;
+	double eps24[kMaxSpecies * kMaxSpecies];
+	double sig2[kMaxSpecies * kMaxSpecies];
+	double shift6[kMaxSpecies * kMaxSpecies];
+};
+
+// LinkedCells geometry. The device keeps only the box's own cells (nc per dimension, no halo
+// layer); the reference's halo-inclusive numbering is recovered as inner index + 1 per dimension.
+struct Grid {
+	int nc[3];
+	double L[3];
+	double cell_length[3];
+	double halo_min[3];
+	int64_t ncells;
+};
+
+// Particle arrays in cell-sorted order (structure of arrays).
+struct Particles {
+	double *rx, *ry, *rz;
+	double *vx, *vy, *vz;
+	double *fx, *fy, *fz;
+	uint64_t* id;
+	int32_t* cid;
+	int32_t* uidx;   // index in the caller's order
+};
+
+struct Context {
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	int precision = MDGPU_FP64;
+	double rc = 0, rc_lj = 0;
+	Grid g{};
+	Species sp{};
+	double eps[kMaxSpecies], sigma[kMaxSpecies];
+	int do_shift[kMaxSpecies];
+	int64_t n = 0;
+	int64_t cap = 0;
+	bool cells_valid = false;
+	std::string err;
+
+	Particles p{};      // current (sorted) arrays
+	Particles q{};      // permutation target
+	int32_t* cell = nullptr;        // inner cell of each particle (sorted order after update)
+	int32_t* rank = nullptr;        // arrival rank within the cell (unordered)
+	int32_t* perm = nullptr;        // sorted slot -> previous slot, before the per-cell id sort
+	int32_t* cell_count = nullptr;  // ncells
+	int32_t* cell_start = nullptr;  // ncells + 1
+	int32_t* scan_tmp = nullptr;    // block sums of the scan
+	int64_t scan_blocks = 0;
+	double* partials = nullptr;     // per-block reduction partials (4 doubles per block)
+	int64_t partial_cap = 0;
+	double* scalars = nullptr;      // device results of the last reductions
+	double* steps_out = nullptr;    // per-step results of mdgpu_run / mdgpu_run_async
+	int64_t steps_cap = 0;
+	int64_t steps_written = 0;      // records appended since the last mdgpu_read_steps
+	int* status = nullptr;          // device status word
+	PairParams* d_pp = nullptr;     // device copy of the pair parameters
+	double* h_scalars = nullptr;    // pinned host mirror
+	int* h_status = nullptr;
+
+	// kernel timing
+	bool profiling = false;
+	cudaEvent_t ev_a[3] = {nullptr, nullptr, nullptr};
+	cudaEvent_t ev_b[3] = {nullptr, nullptr, nullptr};
+	double prof_ms[3] = {0, 0, 0};
+	int64_t prof_count[4] = {0, 0, 0, 0};
+};
+
+// ---- launch helpers implemented in the .cu files -------------------------------------------
+// Each returns cudaSuccess or the launch error; kernels report data errors in ctx->status.
+cudaError_t launch_bin(Context* c, bool permute_forces);
+cudaError_t launch_pairs(Context* c);                 // partials -> scalars[0..2] (U6sum, W, npairs)
+cudaError_t launch_leapfrog_pre(Context* c, double dt, double vcorr);
+cudaError_t launch_leapfrog_post(Context* c, double dt_half);   // scalars[3] = sum m v^2
+cudaError_t launch_scale(Context* c, double beta);
+cudaError_t launch_reduce(Context* c, int64_t nblocks, double* out, int nval);
+cudaError_t launch_step_record(Context* c, double* dst);        // dst[0..3] <- step scalars
+
+// Timing brackets around a group of launches (0 = binning, 1 = pairs, 2 = integration).
+void prof_begin(Context* c, int group);
+void prof_end(Context* c, int group, int launches);
+void count_launches(Context* c, int launches);
+
+}  // namespace mdgpu
+
+struct mdgpu_ctx {
+	mdgpu::Context c;
+};

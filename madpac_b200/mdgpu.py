@@ -1,0 +1,397 @@
+"""Python host side of the B200 LJ hot path, over the C ABI of libmdgpu.so (include/mdgpu.h).
+
+The classes mirror the reference's interfaces for this path so that code written against MarDyn's
+sequential LJ loop reads the same (paths relative to madpac/mardyn/):
+
+* ``LinkedCells``  -- ParticleContainer/LinkedCells (particleContainer/LinkedCells.h:60-312): ``update``,
+  ``traversePairs`` (with the ParticlePairs2PotForceAdapter folded in), ``deleteOuterParticles``,
+  ``getNumberOfParticles``, ``getCellIndexOfMolecule``.
+* ``Leapfrog``     -- the three-state integrator (integrators/Leapfrog.cpp:14-108):
+  ``eventNewTimestep`` / ``eventForcesCalculated``.
+* ``Domain``       -- the Upot/virial/temperature/thermostat part of Domain (Domain.cpp:102-376).
+* ``Simulation``   -- ``prepare_start`` and ``simulateStep`` in the order of Simulation.cpp:907-1229.
+
+Errors raise ``MdgpuError`` carrying the status code (the reference calls ``exit(code)``).
+The compute path is the CUDA library only: if libmdgpu.so cannot be loaded, every constructor
+raises; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmdgpu.so")
+
+FP64 = 0
+MIXED = 1
+
+STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_STATE", 5: "ERR_BOX_TOO_SMALL",
+                6: "ERR_OUTSIDE_HALO", 7: "ERR_SAME_POSITION", 8: "ERR_NONFINITE", 9: "ERR_TIMEOUT",
+                10: "ERR_CAPACITY"}
+
+# Every entry point of include/mdgpu.h: name -> (restype, argtypes)
+_VP = ctypes.c_void_p
+_D = ctypes.c_double
+_I = ctypes.c_int
+_I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
+SIGNATURES = {
+    "mdgpu_create": (_I, [ctypes.POINTER(_VP), _VP, _D, _D, _D, _I, _VP, _VP, _I, _I]),
+    "mdgpu_destroy": (_I, [_VP]),
+    "mdgpu_last_error": (ctypes.c_char_p, [_VP]),
+    "mdgpu_set_precision": (_I, [_VP, _I]),
+    "mdgpu_set_particles": (_I, [_VP, _I64, _VP, _VP, _VP, _VP, _VP]),
+    "mdgpu_set_state": (_I, [_VP, _I64, _VP, _VP]),
+    "mdgpu_get_particles": (_I, [_VP, _I64, _VP, _VP, _VP, _VP, _VP]),
+    "mdgpu_num_particles": (_I, [_VP, _VP]),
+    "mdgpu_get_geometry": (_I, [_VP, _VP, _VP, _VP]),
+    "mdgpu_update": (_I, [_VP]),
+    "mdgpu_get_cell_index": (_I, [_VP, _I64, _VP]),
+    "mdgpu_traverse_pairs": (_I, [_VP, _VP, _VP, _VP]),
+    "mdgpu_leapfrog_pre": (_I, [_VP, _D, _D]),
+    "mdgpu_leapfrog_post": (_I, [_VP, _D, _VP]),
+    "mdgpu_scale_velocities": (_I, [_VP, _D]),
+    "mdgpu_far_field_correction": (_I, [_VP, _VP, _VP]),
+    "mdgpu_step": (_I, [_VP, _D, _D, _VP]),
+    "mdgpu_run": (_I, [_VP, _I32, _D, _VP]),
+    "mdgpu_run_async": (_I, [_VP, _I32, _D]),
+    "mdgpu_read_steps": (_I, [_VP, _I32, _VP]),
+    "mdgpu_device_peaks": (_I, [_I, _VP, _VP]),
+    "mdgpu_profile_enable": (_I, [_VP, _I]),
+    "mdgpu_profile_read": (_I, [_VP, _VP, _VP, _I]),
+    "mdgpu_get_stream": (_I, [_VP, _VP]),
+    "mdgpu_synchronize": (_I, [_VP]),
+}
+
+_lib = None
+
+
+class MdgpuError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"mdgpu status {code} ({STATUS_NAMES.get(code, '?')}): {message}")
+        self.code = code
+
+
+class _MdComponent(ctypes.Structure):
+    _fields_ = [("eps", ctypes.c_double), ("sigma", ctypes.c_double), ("mass", ctypes.c_double),
+                ("do_shift", ctypes.c_int)]
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libmdgpu.so (built by madpac_b200.build) and declare every entry point."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise OSError(f"{path} is missing: build it with `python -m madpac_b200.build`")
+        lib = ctypes.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _c64(a, dtype=np.float64, shape=None) -> np.ndarray:
+    out = np.ascontiguousarray(a, dtype=dtype)
+    if shape is not None:
+        out = out.reshape(shape)
+    return out
+
+
+def device_peaks(device: int = 0):
+    """(FP32, FP64) peak FMA throughput of the device in TFLOP/s, measured by a short kernel."""
+    lib = load_library()
+    a, b = ctypes.c_double(), ctypes.c_double()
+    st = lib.mdgpu_device_peaks(int(device), ctypes.byref(a), ctypes.byref(b))
+    if st != 0:
+        raise MdgpuError(st, "device peak measurement failed")
+    return a.value, b.value
+
+
+class LinkedCells:
+    """The GPU container: the molecules of one periodic box [0, L) binned into cells of edge >= rc."""
+
+    def __init__(self, length: Sequence[float], cutoffRadius: float, components, mixcoeff=None,
+                 LJCutoffRadius: float = 0.0, cellsInCutoffRadius: float = 1.0, precision: int = FP64,
+                 device: int = 0):
+        self.lib = load_library()
+        comps = (_MdComponent * len(components))()
+        for k, c in enumerate(components):
+            comps[k].eps, comps[k].sigma, comps[k].mass = float(c.eps), float(c.sigma), float(c.mass)
+            comps[k].do_shift = 1 if c.do_shift else 0
+        self._length = _c64(length)
+        mix = None if mixcoeff is None else _c64(mixcoeff).reshape(-1)
+        if mix is not None and mix.size == 0:
+            mix = None
+        self._mix = mix
+        h = ctypes.c_void_p()
+        st = self.lib.mdgpu_create(ctypes.byref(h), _ptr(self._length), float(cutoffRadius), float(LJCutoffRadius),
+                                   float(cellsInCutoffRadius), len(components), ctypes.cast(comps, ctypes.c_void_p),
+                                   _ptr(mix), int(precision), int(device))
+        self.h = h.value
+        if st != 0:
+            msg = self.lib.mdgpu_last_error(self.h).decode() if self.h else ""
+            if self.h:
+                self.lib.mdgpu_destroy(self.h)
+            self.h = None
+            raise MdgpuError(st, msg)
+        self.n = 0
+        self.components = components
+
+    @classmethod
+    def from_system(cls, system, precision: int = FP64, device: int = 0) -> "LinkedCells":
+        lc = cls(system.length, system.cutoff, system.components, system.mix, system.lj_cutoff, 1.0, precision,
+                 device)
+        lc.addParticles(system.ids, system.cid, system.r, system.v)
+        return lc
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.mdgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int) -> None:
+        if st != 0:
+            raise MdgpuError(st, self.lib.mdgpu_last_error(self.h).decode())
+
+    # -- ParticleContainer-like surface ---------------------------------------------------------
+    def addParticles(self, ids, cid, r, v, F=None) -> None:
+        ids = _c64(ids, np.uint64)
+        n = ids.shape[0]
+        self._check(self.lib.mdgpu_set_particles(self.h, n, _ptr(ids), _ptr(_c64(cid, np.int32)),
+                                                 _ptr(_c64(r, shape=(n, 3))), _ptr(_c64(v, shape=(n, 3))),
+                                                 _ptr(None if F is None else _c64(F, shape=(n, 3)))))
+        self.n = n
+
+    def setState(self, r=None, v=None) -> None:
+        self._check(self.lib.mdgpu_set_state(self.h, self.n, _ptr(None if r is None else _c64(r, shape=(self.n, 3))),
+                                             _ptr(None if v is None else _c64(v, shape=(self.n, 3)))))
+
+    def getNumberOfParticles(self) -> int:
+        n = ctypes.c_int64()
+        self._check(self.lib.mdgpu_num_particles(self.h, ctypes.byref(n)))
+        return n.value
+
+    def update(self) -> None:
+        self._check(self.lib.mdgpu_update(self.h))
+
+    def deleteOuterParticles(self) -> None:
+        """No-op: the periodic wrap happens inside update()."""
+
+    def traversePairs(self):
+        """Forces on all molecules; returns (local Upot, local virial, unordered pairs within rc)."""
+        u, w, p = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.mdgpu_traverse_pairs(self.h, ctypes.byref(u), ctypes.byref(w), ctypes.byref(p)))
+        return u.value, w.value, p.value
+
+    def getCellIndexOfMolecule(self) -> np.ndarray:
+        out = np.zeros(self.n, dtype=np.int64)
+        self._check(self.lib.mdgpu_get_cell_index(self.h, self.n, _ptr(out)))
+        return out
+
+    def getParticles(self) -> Dict[str, np.ndarray]:
+        n = self.n
+        ids = np.zeros(n, dtype=np.uint64)
+        cid = np.zeros(n, dtype=np.int32)
+        r, v, F = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros((n, 3))
+        self._check(self.lib.mdgpu_get_particles(self.h, n, _ptr(ids), _ptr(cid), _ptr(r), _ptr(v), _ptr(F)))
+        return dict(id=ids, cid=cid, r=r, v=v, F=F)
+
+    def geometry(self) -> Dict[str, np.ndarray]:
+        nc = np.zeros(3, dtype=np.int32)
+        cl, hm = np.zeros(3), np.zeros(3)
+        self._check(self.lib.mdgpu_get_geometry(self.h, _ptr(nc), _ptr(cl), _ptr(hm)))
+        return dict(box_cells=nc, cell_length=cl, halo_min=hm)
+
+    def setPrecision(self, precision: int) -> None:
+        self._check(self.lib.mdgpu_set_precision(self.h, int(precision)))
+
+    # -- integrator primitives -------------------------------------------------------------------
+    def leapfrogPre(self, dt: float, vcorr: float) -> None:
+        self._check(self.lib.mdgpu_leapfrog_pre(self.h, float(dt), float(vcorr)))
+
+    def leapfrogPost(self, dt_half: float) -> float:
+        s = ctypes.c_double()
+        self._check(self.lib.mdgpu_leapfrog_post(self.h, float(dt_half), ctypes.byref(s)))
+        return s.value
+
+    def scaleVelocities(self, beta: float) -> None:
+        self._check(self.lib.mdgpu_scale_velocities(self.h, float(beta)))
+
+    def farFieldCorrection(self):
+        u, w = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.mdgpu_far_field_correction(self.h, ctypes.byref(u), ctypes.byref(w)))
+        return u.value, w.value
+
+    def step(self, dt: float, vcorr: float = 1.0) -> np.ndarray:
+        out = np.zeros(4)
+        self._check(self.lib.mdgpu_step(self.h, float(dt), float(vcorr), _ptr(out)))
+        return out
+
+    def run(self, nsteps: int, dt: float, record: bool = True) -> Optional[np.ndarray]:
+        out = np.zeros((nsteps, 4)) if record else None
+        self._check(self.lib.mdgpu_run(self.h, int(nsteps), float(dt), _ptr(out)))
+        return out
+
+    def runAsync(self, nsteps: int, dt: float) -> None:
+        self._check(self.lib.mdgpu_run_async(self.h, int(nsteps), float(dt)))
+
+    def readSteps(self, nsteps: int) -> np.ndarray:
+        out = np.zeros((nsteps, 4))
+        self._check(self.lib.mdgpu_read_steps(self.h, int(nsteps), _ptr(out)))
+        return out
+
+    def profileEnable(self, on: bool = True) -> None:
+        self._check(self.lib.mdgpu_profile_enable(self.h, 1 if on else 0))
+
+    def profileRead(self, reset: bool = False):
+        t = np.zeros(3)
+        cnt = np.zeros(4, dtype=np.int64)
+        self._check(self.lib.mdgpu_profile_read(self.h, _ptr(t), _ptr(cnt), 1 if reset else 0))
+        return t, cnt
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.lib.mdgpu_get_stream(self.h, ctypes.byref(s)))
+        return s.value or 0
+
+    def synchronize(self) -> None:
+        self._check(self.lib.mdgpu_synchronize(self.h))
+
+
+MIN_BETA = 0.9  # Domain.h:33
+
+
+class Domain:
+    """Upot, virial, temperature and the thermostat factor (Domain.cpp:102-263, one thermostat)."""
+
+    def __init__(self, target_temperature: float = 1.0, nve: bool = True):
+        self.target_temperature = float(target_temperature)
+        self.nve = nve
+        self.local_upot = 0.0
+        self.local_virial = 0.0
+        self.summv2 = 0.0
+        self.upot_corr = 0.0
+        self.virial_corr = 0.0
+        self.global_upot = 0.0
+        self.global_virial = 0.0
+        self.temperature = target_temperature
+        self.beta_trans = 1.0
+        self.n = 0
+
+    def setLocalUpot(self, u: float) -> None:
+        self.local_upot = u
+
+    def setLocalVirial(self, w: float) -> None:
+        self.local_virial = w
+
+    def getGlobalBetaTrans(self) -> float:
+        return self.beta_trans
+
+    def calculateGlobalValues(self, tfactor: float = 1.0) -> None:
+        """Domain::calculateGlobalValues (Domain.cpp:158-263) for one process and one thermostat."""
+        self.global_upot = self.local_upot + self.upot_corr
+        self.global_virial = self.local_virial + self.virial_corr
+        n = self.n
+        self.temperature = (self.summv2 + 0.0) / float(3 * n + 0) if n > 0 else self.target_temperature
+        ti = tfactor * self.target_temperature
+        if ti > 0.0 and not self.nve:
+            self.beta_trans = math.pow(3.0 * n * ti / self.summv2, 0.4)
+        else:
+            self.beta_trans = 1.0
+        if self.beta_trans < MIN_BETA:
+            raise MdgpuError(8, "explosion: beta_trans below MIN_BETA (the selective thermostat is not provided)")
+
+
+class Leapfrog:
+    """MarDyn's three-state Leapfrog (integrators/Leapfrog.cpp:14-108) driving the GPU kernels."""
+
+    def __init__(self, timestepLength: float):
+        self._state = 3
+        self._dt = float(timestepLength)
+
+    def getTimestepLength(self) -> float:
+        return self._dt
+
+    def eventNewTimestep(self, cont: LinkedCells, domain: Domain) -> None:
+        if self._state == 3:
+            self._state = 1
+            vcorr = 2. - 1. / domain.getGlobalBetaTrans()
+            cont.leapfrogPre(self._dt, vcorr)
+            self._state = 2
+
+    def eventForcesCalculated(self, cont: LinkedCells, domain: Domain) -> None:
+        if self._state == 2:
+            domain.summv2 = cont.leapfrogPost(0.5 * self._dt)
+            domain.n = cont.getNumberOfParticles()
+            self._state = 3
+
+
+class Simulation:
+    """The reference's step sequence (Simulation.cpp:907-1229) on the GPU container."""
+
+    def __init__(self, system, precision: int = FP64, device: int = 0):
+        self.system = system
+        self.container = LinkedCells.from_system(system, precision, device)
+        self.domain = Domain(system.temperature, system.nve)
+        self.domain.n = system.n
+        self.domain.upot_corr, self.domain.virial_corr = self.container.farFieldCorrection()
+        self.integrator = Leapfrog(system.dt)
+        self.npairs = 0.0
+        self.simstep = 0
+
+    def _forces(self) -> None:
+        u, w, p = self.container.traversePairs()
+        self.domain.setLocalUpot(u)
+        self.domain.setLocalVirial(w)
+        self.npairs = p
+
+    def prepare_start(self) -> None:
+        self.container.update()
+        self._forces()
+        self.domain.summv2 = self._summv2()
+        self.domain.calculateGlobalValues(1.0)
+
+    def _summv2(self) -> float:
+        st = self.container.getParticles()
+        m = self.system.mass()[st["cid"]]
+        return float(np.sum(m * np.sum(st["v"] * st["v"], axis=1)))
+
+    def simulateStep(self, tfactor: float = 1.0) -> None:
+        self.integrator.eventNewTimestep(self.container, self.domain)
+        self.container.update()
+        self._forces()
+        self.container.deleteOuterParticles()
+        self.integrator.eventForcesCalculated(self.container, self.domain)
+        self.domain.calculateGlobalValues(tfactor)
+        if not self.domain.nve:
+            self.container.scaleVelocities(self.domain.getGlobalBetaTrans())
+        self.simstep += 1
+
+    def scalars(self) -> Dict[str, float]:
+        d = self.domain
+        return dict(upot=d.local_upot, virial=d.local_virial, summv2=d.summv2, global_upot=d.global_upot,
+                    global_virial=d.global_virial, T=d.temperature, beta_trans=d.beta_trans, npairs=self.npairs)
+
+    def state(self) -> Dict[str, np.ndarray]:
+        st = self.container.getParticles()
+        o = np.argsort(st["id"], kind="stable")
+        st = {k: a[o] for k, a in st.items()}
+        st["cell"] = self.container.getCellIndexOfMolecule()[o]
+        return st

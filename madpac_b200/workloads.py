@@ -1,0 +1,317 @@
+"""Seeded synthetic LJ systems and MarDyn's old-style phase-space format.
+
+The workloads are the five single-site Lennard-Jones systems the benchmark and the parity tests
+run (FCC lattices with Maxwell-Boltzmann velocities drawn from ``numpy.random.default_rng(seed)``,
+zero net momentum, rescaled to the exact target temperature). No public dataset is involved.
+
+``write_inp``/``read_inp`` implement the subset of MarDyn's old-style phase-space format used by
+single-site LJ components: the header of ``InputOldstyle::readPhaseSpaceHeader``
+(mardyn/io/InputOldstyle.cpp:35-261: ``Length``, ``Temperature``, ``NumberOfComponents`` with one
+LJ centre line ``x y z m eps sigma tcutoff do_shift`` per component (:162-166), the inertia line,
+the mixing coefficients ``xi eta`` for i<j (:206-215) and epsilon_RF) and the molecule section of
+``InputOldstyle::readPhaseSpace`` (:263-392) in the ``ICRV`` or ``ICRVQD`` layouts.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class Component:
+    """One single-site LJ component (one LJ centre at the molecule origin)."""
+
+    eps: float = 1.0
+    sigma: float = 1.0
+    mass: float = 1.0
+    do_shift: bool = False
+
+
+@dataclasses.dataclass
+class System:
+    """A periodic box of single-site LJ molecules (all arrays in molecule order)."""
+
+    length: np.ndarray                 # (3,) box edge lengths; the box is [0, L)
+    components: List[Component]
+    mix: np.ndarray                    # (ncomp*(ncomp-1)/2, 2) xi, eta for i<j
+    ids: np.ndarray                    # (N,) uint64 molecule ids
+    cid: np.ndarray                    # (N,) int32 0-based component ids
+    r: np.ndarray                      # (N, 3) float64 positions
+    v: np.ndarray                      # (N, 3) float64 velocities
+    temperature: float = 1.0           # target temperature written to the header
+    cutoff: float = 2.5                # cutoffRadius (cells and pair search)
+    lj_cutoff: float = 2.5             # LJCutoffRadius
+    dt: float = 0.002                  # timestepLength
+    nve: bool = True
+    name: str = "system"
+
+    @property
+    def n(self) -> int:
+        return int(self.ids.shape[0])
+
+    def eps(self) -> np.ndarray:
+        return np.array([c.eps for c in self.components], dtype=np.float64)
+
+    def sigma(self) -> np.ndarray:
+        return np.array([c.sigma for c in self.components], dtype=np.float64)
+
+    def mass(self) -> np.ndarray:
+        return np.array([c.mass for c in self.components], dtype=np.float64)
+
+    def do_shift(self) -> np.ndarray:
+        return np.array([1 if c.do_shift else 0 for c in self.components], dtype=np.int32)
+
+
+# ----------------------------------------------------------------------------- generators
+
+def fcc_sites(ncell: Sequence[int], a: Sequence[float], offset: Sequence[float]) -> np.ndarray:
+    """FCC lattice sites of ncell[0] x ncell[1] x ncell[2] cubic unit cells of edge a."""
+    basis = np.array([[0.0, 0.0, 0.0], [0.5, 0.5, 0.0], [0.5, 0.0, 0.5], [0.0, 0.5, 0.5]])
+    ix, iy, iz = np.meshgrid(np.arange(ncell[0]), np.arange(ncell[1]), np.arange(ncell[2]),
+                             indexing="ij")
+    cells = np.stack([ix.ravel(), iy.ravel(), iz.ravel()], axis=1).astype(np.float64)
+    pts = (cells[:, None, :] + basis[None, :, :]).reshape(-1, 3)
+    return pts * np.asarray(a, dtype=np.float64) + np.asarray(offset, dtype=np.float64)
+
+
+def maxwell_boltzmann(rng: np.random.Generator, mass: np.ndarray, temperature: float) -> np.ndarray:
+    """Velocities with zero net momentum, scaled so that sum m v^2 / (3N) equals temperature
+    (the reference's temperature with no rotational degrees of freedom, Domain.cpp:244-246)."""
+    n = mass.shape[0]
+    v = rng.standard_normal((n, 3)) * np.sqrt(temperature / mass)[:, None]
+    p = (mass[:, None] * v).sum(axis=0) / mass.sum()
+    v -= p[None, :]
+    summv2 = float((mass[:, None] * v * v).sum())
+    v *= math.sqrt(3.0 * n * temperature / summv2)
+    return v
+
+
+def _wrap(r: np.ndarray, length: np.ndarray) -> np.ndarray:
+    r = np.mod(r, length[None, :])
+    r[r >= length[None, :]] = 0.0
+    return r
+
+
+def lj_fcc_box(n_cells: int, density: float, temperature: float, seed: int, cutoff: float,
+               components: Optional[List[Component]] = None, fractions: Optional[Sequence[float]] = None,
+               mix: Optional[np.ndarray] = None, dt: float = 0.002, nve: bool = True,
+               n_atoms: Optional[int] = None, name: str = "fcc") -> System:
+    """A cubic periodic FCC box of 4*n_cells^3 sites at the given number density.
+
+    If n_atoms is given (fewer than the sites), a seeded random subset of the sites is kept and
+    the box edge follows from n_atoms/density. The lattice is offset by a/4 so that no molecule
+    sits on a cell face.
+    """
+    rng = np.random.default_rng(seed)
+    nsites = 4 * n_cells ** 3
+    n = nsites if n_atoms is None else int(n_atoms)
+    if n > nsites:
+        raise ValueError("n_atoms exceeds the lattice sites")
+    L = (n / density) ** (1.0 / 3.0)
+    a = L / n_cells
+    r = fcc_sites([n_cells] * 3, [a] * 3, [a / 4.0] * 3)
+    if n < nsites:
+        keep = np.sort(rng.choice(nsites, size=n, replace=False))
+        r = r[keep]
+    components = components or [Component(1.0, 1.0, 1.0, False)]
+    nc = len(components)
+    if nc == 1:
+        cid = np.zeros(n, dtype=np.int32)
+    else:
+        fr = np.asarray(fractions if fractions is not None else [1.0 / nc] * nc, dtype=np.float64)
+        counts = np.floor(fr / fr.sum() * n).astype(np.int64)
+        counts[0] += n - counts.sum()
+        cid = np.repeat(np.arange(nc, dtype=np.int32), counts)
+        cid = cid[rng.permutation(n)]
+    if mix is None:
+        mix = np.ones((nc * (nc - 1) // 2, 2), dtype=np.float64)
+    length = np.array([L, L, L], dtype=np.float64)
+    mass = np.array([components[c].mass for c in range(nc)])[cid]
+    v = maxwell_boltzmann(rng, mass, temperature)
+    return System(length=length, components=components, mix=np.asarray(mix, dtype=np.float64),
+                  ids=np.arange(1, n + 1, dtype=np.uint64), cid=cid, r=_wrap(r, length), v=v,
+                  temperature=temperature, cutoff=cutoff, lj_cutoff=cutoff, dt=dt, nve=nve, name=name)
+
+
+def two_species() -> List[Component]:
+    """Species A/B: sigma_A=1.0, sigma_B=0.9, eps_A=1.0, eps_B=0.8, m=1, truncated-shifted."""
+    return [Component(1.0, 1.0, 1.0, True), Component(0.8, 0.9, 1.0, True)]
+
+
+def config_c1(seed: int = 1) -> System:
+    """32,000-atom single-species FCC box, rho=0.8, T=1.0, rc=2.5, dt=0.002, plain truncated LJ."""
+    return lj_fcc_box(20, 0.8, 1.0, seed, 2.5, [Component(1.0, 1.0, 1.0, False)], name="c1_32k")
+
+
+def config_c2(seed: int = 2) -> System:
+    """1,048,576-atom single-species FCC box, rho=0.75, T=0.9, rc=3.0, truncated-shifted LJ."""
+    return lj_fcc_box(64, 0.75, 0.9, seed, 3.0, [Component(1.0, 1.0, 1.0, True)], name="c2_1m")
+
+
+def config_c3(seed: int = 3, n_total: int = 4194304) -> System:
+    """Two-species slab: Lx=Ly, Lz=3Lx; FCC liquid (rho~0.70) in the middle third and a sparse
+    vapour (rho~0.02) elsewhere; A/B 50/50 with Lorentz-Berthelot mixing (xi=eta=1); T=0.85;
+    rc=2.5 (sigma_A units)."""
+    rng = np.random.default_rng(seed)
+    Lx = (n_total / (0.70 + 0.02 * 2.0)) ** (1.0 / 3.0)
+    n_cells = int(round((0.70 * Lx ** 3 / 4.0) ** (1.0 / 3.0)))
+    a = Lx / n_cells
+    liquid = fcc_sites([n_cells] * 3, [a] * 3, [a / 4.0, a / 4.0, Lx + a / 4.0])
+    n_vap = n_total - liquid.shape[0]
+    # vapour on a simple-cubic grid filling z in [0, Lx) and [2Lx, 3Lx); a seeded subset is kept
+    m = int(math.ceil((n_vap / 2.0) ** (1.0 / 3.0))) + 1
+    av = Lx / m
+    g = (np.stack(np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij"), -1)
+         .reshape(-1, 3).astype(np.float64) + 0.5) * av
+    sites = np.concatenate([g, g + np.array([0.0, 0.0, 2.0 * Lx])])
+    keep = np.sort(rng.choice(sites.shape[0], size=n_vap, replace=False))
+    r = np.concatenate([liquid, sites[keep]])
+    n = r.shape[0]
+    comps = two_species()
+    cid = np.repeat(np.arange(2, dtype=np.int32), [n - n // 2, n // 2])[rng.permutation(n)]
+    length = np.array([Lx, Lx, 3.0 * Lx])
+    mass = np.ones(n)
+    v = maxwell_boltzmann(rng, mass, 0.85)
+    return System(length=length, components=comps, mix=np.ones((1, 2)), ids=np.arange(1, n + 1, dtype=np.uint64),
+                  cid=cid, r=_wrap(r, length), v=v, temperature=0.85, cutoff=2.5, lj_cutoff=2.5,
+                  dt=0.002, nve=True, name="c3_slab_4m")
+
+
+def config_c4(seed: int = 4, n_boxes: int = 512) -> List[System]:
+    """Independent cubic boxes: N log-uniform in [256, 8192], rho U[0.6, 0.9], T U[0.7, 1.5],
+    rc=2.5, truncated-shifted single-species LJ."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for b in range(n_boxes):
+        n = int(round(math.exp(rng.uniform(math.log(256), math.log(8192)))))
+        rho = float(rng.uniform(0.6, 0.9))
+        T = float(rng.uniform(0.7, 1.5))
+        ncell = int(math.ceil((n / 4.0) ** (1.0 / 3.0)))
+        out.append(lj_fcc_box(ncell, rho, T, int(rng.integers(1 << 31)), 2.5,
+                              [Component(1.0, 1.0, 1.0, True)], n_atoms=n, name=f"c4_box{b}"))
+    return out
+
+
+def config_c5(seed: int = 5) -> System:
+    """16,384-atom two-species FCC box (A/B 50/50 of the slab species), rho=0.8, T=1.0, rc=2.5."""
+    return lj_fcc_box(16, 0.8, 1.0, seed, 2.5, two_species(), [0.5, 0.5], np.ones((1, 2)), name="c5_16k")
+
+
+# ----------------------------------------------------------------------------- file format
+
+def write_inp(sys_: System, path: str, fmt: str = "ICRV") -> None:
+    """Write the old-style phase-space file (header + molecules, component ids 1-based)."""
+    nc = len(sys_.components)
+    lines = ["mardyn trunk 20090721", "currentTime 0.0",
+             f"Temperature {float(sys_.temperature)!r}",
+             "Length {!r} {!r} {!r}".format(*[float(x) for x in sys_.length]),
+             f"NumberOfComponents {nc}"]
+    for c in sys_.components:
+        lines.append("1 0 0 0 0")
+        lines.append(f"0.0 0.0 0.0 {float(c.mass)!r} {float(c.eps)!r} {float(c.sigma)!r} {float(sys_.lj_cutoff)!r} {1 if c.do_shift else 0}")
+        lines.append("0.0 0.0 0.0")
+    k = 0
+    for i in range(nc):
+        for j in range(i + 1, nc):
+            lines.append(f"{float(sys_.mix[k, 0])!r} {float(sys_.mix[k, 1])!r}")
+            k += 1
+    lines.append("1.0e+10")
+    lines.append(f"NumberOfMolecules {sys_.n}")
+    lines.append(f"MoleculeFormat {fmt}")
+    head = "\n".join(lines) + "\n"
+    cols = [sys_.ids.astype(np.float64), (sys_.cid + 1).astype(np.float64), sys_.r[:, 0], sys_.r[:, 1],
+            sys_.r[:, 2], sys_.v[:, 0], sys_.v[:, 1], sys_.v[:, 2]]
+    with open(path, "w") as f:
+        f.write(head)
+        if fmt == "ICRV":
+            body = np.column_stack(cols)
+            np.savetxt(f, body, fmt=["%d", "%d"] + ["%.17g"] * 6)
+        elif fmt == "ICRVQD":
+            n = sys_.n
+            extra = np.column_stack([np.ones(n), np.zeros(n), np.zeros(n), np.zeros(n),
+                                     np.zeros(n), np.zeros(n), np.zeros(n)])
+            body = np.column_stack(cols + [extra])
+            np.savetxt(f, body, fmt=["%d", "%d"] + ["%.17g"] * 13)
+        else:
+            raise ValueError(f"unsupported molecule format {fmt}")
+
+
+def read_inp(path: str) -> System:
+    """Read an old-style phase-space file with single-site LJ components (ICRV/ICRVQD/IRV)."""
+    with open(path) as f:
+        text = "\n".join(ln for ln in f.read().splitlines() if not ln.lstrip().startswith("#"))
+    toks = text.split()
+    pos = 0
+
+    def nxt() -> str:
+        nonlocal pos
+        t = toks[pos]
+        pos += 1
+        return t
+
+    magic = nxt()
+    if magic not in ("mardyn", "MOLDY", "ls1r1", "mrdyn", "MDProject", "Mardyn", "MARDYN"):
+        raise ValueError(f"{path}: not a valid OldStyle input file")
+    if nxt() != "trunk":
+        raise ValueError(f"{path}: wrong input file specifier")
+    nxt()
+    temperature, length, comps, mix = 1.0, None, [], []
+    while True:
+        t = nxt()
+        if t in ("currentTime", "t"):
+            nxt()
+        elif t in ("Temperature", "T"):
+            temperature = float(nxt())
+        elif t in ("Length", "L"):
+            length = np.array([float(nxt()), float(nxt()), float(nxt())])
+        elif t in ("NumberOfComponents", "C"):
+            nc = int(nxt())
+            for _ in range(nc):
+                nlj, nq, nd, nqq, nt = (int(nxt()) for _ in range(5))
+                if nlj != 1 or nq or nd or nqq or nt:
+                    raise ValueError("only single-site LJ components are supported")
+                x, y, z, m, eps, sig, tcut, shift = (float(nxt()) for _ in range(8))
+                if x or y or z:
+                    raise ValueError("the LJ centre must sit at the molecule origin")
+                comps.append(Component(eps, sig, m, shift != 0))
+                nxt(); nxt(); nxt()
+            for i in range(nc):
+                for j in range(i + 1, nc):
+                    mix.append((float(nxt()), float(nxt())))
+            nxt()  # epsilon_RF
+            break
+        else:
+            raise ValueError(f"unsupported header token {t}")
+    t = nxt()
+    if t not in ("NumberOfMolecules", "N"):
+        raise ValueError("expected NumberOfMolecules")
+    n = int(nxt())
+    fmt = "ICRVQD"
+    if toks[pos] in ("MoleculeFormat", "M"):
+        pos += 1
+        fmt = nxt()
+    ncol = {"ICRVQD": 15, "ICRV": 8, "IRV": 7, "ICRVFQDM": 21}[fmt]
+    body = np.array(toks[pos:pos + n * ncol], dtype=np.float64).reshape(n, ncol)
+    if fmt == "IRV":
+        ids, cid, r, v = body[:, 0], np.ones(n), body[:, 1:4], body[:, 4:7]
+    else:
+        ids, cid, r, v = body[:, 0], body[:, 1], body[:, 2:5], body[:, 5:8]
+    nc = len(comps)
+    return System(length=length, components=comps,
+                  mix=np.array(mix, dtype=np.float64).reshape(nc * (nc - 1) // 2, 2),
+                  ids=ids.astype(np.uint64), cid=(cid.astype(np.int32) - 1), r=r.copy(), v=v.copy(),
+                  temperature=temperature, name=path)
+
+
+def write_cfg(sys_: System, cfg_path: str, inp_name: str) -> None:
+    """Old-style MarDyn config for the system (tokens of Simulation::initConfigOldstyle)."""
+    lines = ["mardynconfig", f"timestepLength {float(sys_.dt)!r}", f"cutoffRadius {float(sys_.cutoff)!r}",
+             f"LJCutoffRadius {float(sys_.lj_cutoff)!r}", f"phaseSpaceFile OldStyle {inp_name}",
+             "datastructure LinkedCells 1"]
+    if sys_.nve:
+        lines.append("NVE")
+    with open(cfg_path, "w") as f:
+        f.write("\n".join(lines) + "\n")

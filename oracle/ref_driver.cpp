@@ -1,0 +1,159 @@
+// Test harness around the reference MarDyn sources (compiled unmodified by oracle/Makefile).
+//
+// It runs exactly the reference's own step sequence -- Simulation::prepare_start
+// (mardyn/Simulation.cpp:907-993) followed by Simulation::simulateStep
+// (mardyn/Simulation.cpp:1218-1229) -- on an old-style .cfg/.inp pair and records, per step:
+//   * the local potential energy and virial that ParticlePairs2PotForceAdapter::finish
+//     stored in Domain (mardyn/particleContainer/adapter/ParticlePairs2PotForceAdapter.h:64-67),
+//   * sum m v^2 over the molecules,
+// and, for the steps named on the command line, every molecule's id, component, r, v, F and
+// LinkedCells cell index (LinkedCells::getCellIndexOfMolecule, LinkedCells.cpp:535-547).
+//
+// The reference never prints per-molecule forces, so this harness exists only to pin the
+// oracle and the GPU path against the reference itself. It is test infrastructure.
+//
+// usage: ref_driver <cfg> <nsteps> <outdir> <dumpsteps: comma list, 0 = after prepare_start>
+//        ref_driver --time <cfg> <nsteps>      (timing only: prints seconds per step as JSON)
+#include <sys/time.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <set>
+#include <sstream>
+#include <string>
+#include <vector>
+
+// getCellIndexOfMolecule is private in LinkedCells; the harness reads it directly.
+#define private public
+#include "particleContainer/LinkedCells.h"
+#undef private
+
+#include "Domain.h"
+#include "Simulation.h"
+#include "molecules/Molecule.h"
+#include "particleContainer/ParticleContainer.h"
+#include "utils/Logger.h"
+
+using Log::global_log;
+
+namespace {
+
+double now_s() {
+	struct timeval tv;
+	gettimeofday(&tv, nullptr);
+	return tv.tv_sec + 1e-6 * tv.tv_usec;
+}
+
+struct Rec {
+	unsigned long id;
+	long cid;
+	double r[3], v[3], F[3];
+	long cell;
+};
+
+}  // namespace
+
+class RefDriver : public Simulation {
+public:
+	double summv2() {
+		double s = 0.0;
+		for (Molecule* m = _moleculeContainer->begin(); m != _moleculeContainer->end(); m = _moleculeContainer->next()) {
+			double v2 = m->v(0) * m->v(0) + m->v(1) * m->v(1) + m->v(2) * m->v(2);
+			s += m->getMass() * v2;
+		}
+		return s;
+	}
+
+	void writeScalars(FILE* f, long step) {
+		fprintf(f, "%ld %.17g %.17g %.17g %lu\n", step, _domain->getLocalUpot(), _domain->getLocalVirial(), summv2(),
+		        _moleculeContainer->getNumberOfParticles());
+	}
+
+	void writeArrays(const std::string& outdir, long step) {
+		LinkedCells* lc = dynamic_cast<LinkedCells*>(_moleculeContainer);
+		std::vector<Rec> recs;
+		for (Molecule* m = _moleculeContainer->begin(); m != _moleculeContainer->end(); m = _moleculeContainer->next()) {
+			Rec r;
+			r.id = m->id();
+			r.cid = m->componentid();
+			for (int d = 0; d < 3; d++) {
+				r.r[d] = m->r(d);
+				r.v[d] = m->v(d);
+				r.F[d] = m->F(d);
+			}
+			r.cell = lc ? (long) lc->getCellIndexOfMolecule(m) : -1;
+			recs.push_back(r);
+		}
+		std::sort(recs.begin(), recs.end(), [](const Rec& a, const Rec& b) { return a.id < b.id; });
+		char name[512];
+		snprintf(name, sizeof(name), "%s/step%06ld.bin", outdir.c_str(), step);
+		FILE* f = fopen(name, "wb");
+		if (!f) {
+			fprintf(stderr, "cannot open %s\n", name);
+			std::exit(2);
+		}
+		long n = (long) recs.size();
+		fwrite(&n, sizeof(long), 1, f);
+		for (const Rec& r : recs) fwrite(&r.id, sizeof(unsigned long), 1, f);
+		for (const Rec& r : recs) fwrite(&r.cid, sizeof(long), 1, f);
+		for (const Rec& r : recs) fwrite(r.r, sizeof(double), 3, f);
+		for (const Rec& r : recs) fwrite(r.v, sizeof(double), 3, f);
+		for (const Rec& r : recs) fwrite(r.F, sizeof(double), 3, f);
+		for (const Rec& r : recs) fwrite(&r.cell, sizeof(long), 1, f);
+		fclose(f);
+	}
+
+	void run(unsigned long nsteps, const std::string& outdir, const std::set<long>& dumps) {
+		std::string sname = outdir + "/scalars.txt";
+		FILE* sf = fopen(sname.c_str(), "w");
+		prepare_start();
+		writeScalars(sf, 0);
+		if (dumps.count(0)) writeArrays(outdir, 0);
+		// Simulation::simulate runs _simstep = _initSimulation .. _numberOfTimesteps inclusive.
+		_numberOfTimesteps = _initSimulation + nsteps - 1;
+		simulateStart();
+		long k = 1;
+		for (_simstep = _initSimulation; _simstep <= _numberOfTimesteps; k++) {
+			simulateStep();
+			writeScalars(sf, k);
+			if (dumps.count(k)) writeArrays(outdir, k);
+		}
+		fclose(sf);
+	}
+
+	double timeSteps(unsigned long nsteps) {
+		prepare_start();
+		_numberOfTimesteps = _initSimulation + nsteps - 1;
+		simulateStart();
+		double t0 = now_s();
+		for (_simstep = _initSimulation; _simstep <= _numberOfTimesteps;) simulateStep();
+		return (now_s() - t0) / nsteps;
+	}
+};
+
+int main(int argc, char** argv) {
+	global_log = new Log::Logger(Log::MARDYN_Error);
+	if (argc >= 4 && std::string(argv[1]) == "--time") {
+		RefDriver sim;
+		sim.readConfigFile(argv[2]);
+		unsigned long n = strtoul(argv[3], nullptr, 10);
+		double s = sim.timeSteps(n);
+		printf("{\"seconds_per_step\": %.9g, \"steps\": %lu}\n", s, n);
+		return 0;
+	}
+	if (argc < 5) {
+		fprintf(stderr, "usage: ref_driver <cfg> <nsteps> <outdir> <dumpsteps>\n");
+		return 1;
+	}
+	std::set<long> dumps;
+	std::stringstream ss(argv[4]);
+	std::string tok;
+	while (std::getline(ss, tok, ','))
+		if (!tok.empty()) dumps.insert(strtol(tok.c_str(), nullptr, 10));
+	RefDriver sim;
+	sim.readConfigFile(argv[1]);
+	sim.run(strtoul(argv[2], nullptr, 10), argv[3], dumps);
+	return 0;
+}
