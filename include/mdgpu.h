@@ -66,6 +66,10 @@ const char* mdgpu_last_error(const mdgpu_ctx* ctx);
 /* Switch between MDGPU_FP64 and MDGPU_MIXED. */
 int mdgpu_set_precision(mdgpu_ctx* ctx, int precision);
 
+/* Select the pair kernel: 0 = shared-memory brick kernel (default), 1 = simple per-molecule
+ * gather kernel (same arithmetic, kept as an independent second implementation). */
+int mdgpu_set_pair_kernel(mdgpu_ctx* ctx, int kind);
+
 /* Load n molecules (replaces the InputOldstyle::readPhaseSpace -> LinkedCells::addParticle loop,
  * io/InputOldstyle.cpp:324-378, LinkedCells.cpp:182-204). F may be NULL (zero forces). */
 int mdgpu_set_particles(mdgpu_ctx* ctx, int64_t n, const uint64_t* id, const int32_t* cid,

@@ -9,8 +9,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmdgpu.so")
-SOURCES = ["api.cu", "binning.cu", "pairs.cu", "integrate.cu", "peaks.cu"]
-HEADERS = ["md_internal.h", "reduce.cuh"]
+SOURCES = ["api.cu", "binning.cu", "pairs.cu", "pairs_brick.cu", "integrate.cu", "peaks.cu"]
+HEADERS = ["md_internal.h", "reduce.cuh", "pair_common.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -363,6 +363,14 @@ int mdgpu_set_precision(mdgpu_ctx* ctx, int precision) {
 	return MDGPU_OK;
 }
 
+int mdgpu_set_pair_kernel(mdgpu_ctx* ctx, int kind) {
+	if (!ctx) return MDGPU_ERR_ARG;
+	Context* c = &ctx->c;
+	if (kind != 0 && kind != 1) return fail(c, MDGPU_ERR_ARG, "pair kernel must be 0 (brick) or 1 (gather)");
+	c->pair_kernel = kind;
+	return MDGPU_OK;
+}
+
 int mdgpu_set_particles(mdgpu_ctx* ctx, int64_t n, const uint64_t* id, const int32_t* cid, const double* r,
                         const double* v, const double* F) {
 	if (!ctx) return MDGPU_ERR_ARG;
@@ -391,7 +399,10 @@ int mdgpu_set_particles(mdgpu_ctx* ctx, int64_t n, const uint64_t* id, const int
 		MD_CUDA(cudaMalloc(&c->cell, sizeof(int32_t) * n));
 		MD_CUDA(cudaMalloc(&c->rank, sizeof(int32_t) * n));
 		MD_CUDA(cudaMalloc(&c->perm, sizeof(int32_t) * n));
-		c->partial_cap = (n + kReduceBlock - 1) / kReduceBlock + 1024;
+		// per-block partials of the widest reduction: per-molecule blocks or one per 2x2x2 brick
+		const int64_t bricks = (int64_t) ((c->g.nc[0] + 1) / 2) * ((c->g.nc[1] + 1) / 2) * ((c->g.nc[2] + 1) / 2);
+		const int64_t blocks = (n + kReduceBlock - 1) / kReduceBlock;
+		c->partial_cap = (blocks > bricks ? blocks : bricks) + 1024;
 		MD_CUDA(cudaMalloc(&c->partials, sizeof(double) * 4 * c->partial_cap));
 		c->cap = n;
 	}

@@ -64,6 +64,7 @@ struct Context {
 	int device = 0;
 	cudaStream_t stream = nullptr;
 	int precision = MDGPU_FP64;
+	int pair_kernel = 0;            // 0 = shared-memory brick kernel, 1 = simple gather kernel
 	double rc = 0, rc_lj = 0;
 	Grid g{};
 	Species sp{};
@@ -84,7 +85,7 @@ struct Context {
 	int32_t* scan_tmp = nullptr;    // block sums of the scan
 	int64_t scan_blocks = 0;
 	double* partials = nullptr;     // per-block reduction partials (4 doubles per block)
-	int64_t partial_cap = 0;
+	int64_t partial_cap = 0;        // in blocks (4 doubles each)
 	double* scalars = nullptr;      // device results of the last reductions
 	double* steps_out = nullptr;    // per-step results of mdgpu_run / mdgpu_run_async
 	int64_t steps_cap = 0;

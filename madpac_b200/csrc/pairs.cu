@@ -1,4 +1,7 @@
-// Lennard-Jones 12-6 pair forces, potential energy and virial over the linked cells.
+// Lennard-Jones 12-6 pair forces, potential energy and virial over the linked cells: the simple
+// gather kernel (one thread per molecule, operands straight from global memory) and the final
+// fixed-order reduction. The default pair kernel is the shared-memory brick kernel of
+// pairs_brick.cu; this one is kept as an independent second implementation for the tests.
 //
 // Every molecule i gathers from all molecules j of the 27 cells around its own (periodic images
 // are the neighbour cell's molecules shifted by +-L, computed as the reference computes a halo
@@ -17,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include "md_internal.h"
+#include "pair_common.cuh"
 #include "reduce.cuh"
 
 namespace mdgpu {
@@ -28,105 +32,35 @@ __global__ void __launch_bounds__(kReduceBlock) k_pairs_gather(int64_t n, const 
                                                                const double* __restrict__ ry,
                                                                const double* __restrict__ rz,
                                                                const int32_t* __restrict__ cid,
-                                                               const int32_t* __restrict__ cell,
                                                                const int32_t* __restrict__ start, Grid g,
                                                                const PairParams* __restrict__ pp,
                                                                double* __restrict__ fx, double* __restrict__ fy,
                                                                double* __restrict__ fz, double* partials,
                                                                int* status) {
-	__shared__ double s_eps24[kMaxSpecies * kMaxSpecies], s_sig2[kMaxSpecies * kMaxSpecies],
-	    s_shift6[kMaxSpecies * kMaxSpecies];
-	int ns = pp->ns;
+	constexpr int KK = kMaxSpecies * kMaxSpecies;
+	__shared__ double s_par[3 * KK];
+	const int ns = pp->ns;
 	for (int k = threadIdx.x; k < ns * ns; k += blockDim.x) {
-		s_eps24[k] = pp->eps24[k];
-		s_sig2[k] = pp->sig2[k];
-		s_shift6[k] = pp->shift6[k];
+		s_par[k] = pp->eps24[k];
+		s_par[KK + k] = pp->sig2[k];
+		s_par[2 * KK + k] = pp->shift6[k];
 	}
 	__syncthreads();
-	const double rc2 = pp->rc2, rclj2 = pp->rclj2;
-	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	double U = 0.0, W = 0.0, np = 0.0;
 	bool same = false;
 	if (i < n) {
-		const double xi = rx[i], yi = ry[i], zi = rz[i];
-		const int ti = cid[i];
-		const int c = cell[i];
-		const int cx = c % g.nc[0], cy = (c / g.nc[0]) % g.nc[1], cz = c / (g.nc[0] * g.nc[1]);
-		double Fx = 0.0, Fy = 0.0, Fz = 0.0;
-		for (int dz = -1; dz <= 1; dz++) {
-			int z = cz + dz;
-			double sz = 0.0;
-			if (z < 0) { z += g.nc[2]; sz = -g.L[2]; }
-			else if (z >= g.nc[2]) { z -= g.nc[2]; sz = g.L[2]; }
-			for (int dy = -1; dy <= 1; dy++) {
-				int y = cy + dy;
-				double sy = 0.0;
-				if (y < 0) { y += g.nc[1]; sy = -g.L[1]; }
-				else if (y >= g.nc[1]) { y -= g.nc[1]; sy = g.L[1]; }
-				for (int dx = -1; dx <= 1; dx++) {
-					int x = cx + dx;
-					double sx = 0.0;
-					if (x < 0) { x += g.nc[0]; sx = -g.L[0]; }
-					else if (x >= g.nc[0]) { x -= g.nc[0]; sx = g.L[0]; }
-					const int nb = (z * g.nc[1] + y) * g.nc[0] + x;
-					const bool shifted = (sx != 0.0) || (sy != 0.0) || (sz != 0.0);
-					const int j0 = start[nb], j1 = start[nb + 1];
-					for (int j = j0; j < j1; j++) {
-						if (j == i && !shifted) continue;
-						double xj = rx[j], yj = ry[j], zj = rz[j];
-						if (shifted) {
-							xj = __dadd_rn(xj, sx);
-							yj = __dadd_rn(yj, sy);
-							zj = __dadd_rn(zj, sz);
-						}
-						const double d0 = __dsub_rn(xi, xj), d1 = __dsub_rn(yi, yj), d2 = __dsub_rn(zi, zj);
-						const double dd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
-						if (!(dd < rc2)) continue;
-						np += 1.0;
-						if (dd == 0.0) same = true;
-						if (!(dd < rclj2)) continue;
-						const int pk = ti * ns + cid[j];
-						if (!kMixed) {
-							const double eps24 = s_eps24[pk], sig2 = s_sig2[pk];
-							const double invdr2 = __ddiv_rn(1.0, dd);
-							double lj6 = __dmul_rn(sig2, invdr2);
-							lj6 = __dmul_rn(__dmul_rn(lj6, lj6), lj6);
-							const double lj12 = __dmul_rn(lj6, lj6);
-							const double lj12m6 = __dsub_rn(lj12, lj6);
-							const double u = __dadd_rn(__dmul_rn(eps24, lj12m6), s_shift6[pk]);
-							const double fac = __dmul_rn(__dmul_rn(eps24, __dadd_rn(lj12, lj12m6)), invdr2);
-							const double f0 = __dmul_rn(fac, d0), f1 = __dmul_rn(fac, d1), f2 = __dmul_rn(fac, d2);
-							Fx += f0;
-							Fy += f1;
-							Fz += f2;
-							U += u;
-							W = __dadd_rn(W, __dadd_rn(__dadd_rn(__dmul_rn(d0, f0), __dmul_rn(d1, f1)), __dmul_rn(d2, f2)));
-						} else {
-							const float e0 = (float) d0, e1 = (float) d1, e2 = (float) d2;
-							const float ddf = e0 * e0 + e1 * e1 + e2 * e2;
-							const float eps24 = (float) s_eps24[pk], sig2 = (float) s_sig2[pk];
-							const float invdr2 = 1.0f / ddf;
-							float lj6 = sig2 * invdr2;
-							lj6 = lj6 * lj6 * lj6;
-							const float lj12 = lj6 * lj6;
-							const float lj12m6 = lj12 - lj6;
-							const float u = eps24 * lj12m6;
-							const float fac = eps24 * (lj12 + lj12m6) * invdr2;
-							const float f0 = fac * e0, f1 = fac * e1, f2 = fac * e2;
-							Fx += (double) f0;
-							Fy += (double) f1;
-							Fz += (double) f2;
-							U += (double) u + s_shift6[pk];
-							W += (double) (e0 * f0 + e1 * f1 + e2 * f2);
-						}
-					}
-				}
-			}
-		}
-		fx[i] = Fx;
-		fy[i] = Fy;
-		fz[i] = Fz;
-		if (!(Fx == Fx && Fy == Fy && Fz == Fz) || isinf(Fx) || isinf(Fy) || isinf(Fz)) atomicOr(status, kStatusNonFinite);
+		const PairSums s = gather_pairs<kMixed>(i, rx, ry, rz, cid, start, g, s_par, ns, pp->rc2, pp->rclj2);
+		fx[i] = s.F[0];
+		fy[i] = s.F[1];
+		fz[i] = s.F[2];
+		U = s.U;
+		W = s.W;
+		np = s.np;
+		same = s.same;
+		if (!(s.F[0] == s.F[0] && s.F[1] == s.F[1] && s.F[2] == s.F[2]) || isinf(s.F[0]) || isinf(s.F[1]) ||
+		    isinf(s.F[2]))
+			atomicOr(status, kStatusNonFinite);
 	}
 	if (same) atomicOr(status, kStatusSamePosition);
 	block_sum3(U, W, np, partials);
@@ -161,18 +95,21 @@ cudaError_t launch_reduce(Context* c, int64_t nblocks, double* out, int nval) {
 	return cudaGetLastError();
 }
 
+cudaError_t launch_pairs_brick(Context* c);
+
 cudaError_t launch_pairs(Context* c) {
+	if (c->pair_kernel == 0 && c->n < (int64_t(1) << 28)) return launch_pairs_brick(c);
 	prof_begin(c, 1);
 	int64_t nb = (c->n + kReduceBlock - 1) / kReduceBlock;
 	if (nb == 0) nb = 1;
 	if (c->precision == MDGPU_MIXED)
 		k_pairs_gather<true><<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(
-		    c->n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->cell, c->cell_start, c->g, c->d_pp, c->p.fx, c->p.fy,
-		    c->p.fz, c->partials, c->status);
+		    c->n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->cell_start, c->g, c->d_pp, c->p.fx, c->p.fy, c->p.fz,
+		    c->partials, c->status);
 	else
 		k_pairs_gather<false><<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(
-		    c->n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->cell, c->cell_start, c->g, c->d_pp, c->p.fx, c->p.fy,
-		    c->p.fz, c->partials, c->status);
+		    c->n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->cell_start, c->g, c->d_pp, c->p.fx, c->p.fy, c->p.fz,
+		    c->partials, c->status);
 	cudaError_t e = cudaGetLastError();
 	prof_end(c, 1, 1);
 	if (e != cudaSuccess) return e;

@@ -45,6 +45,7 @@ SIGNATURES = {
     "mdgpu_destroy": (_I, [_VP]),
     "mdgpu_last_error": (ctypes.c_char_p, [_VP]),
     "mdgpu_set_precision": (_I, [_VP, _I]),
+    "mdgpu_set_pair_kernel": (_I, [_VP, _I]),
     "mdgpu_set_particles": (_I, [_VP, _I64, _VP, _VP, _VP, _VP, _VP]),
     "mdgpu_set_state": (_I, [_VP, _I64, _VP, _VP]),
     "mdgpu_get_particles": (_I, [_VP, _I64, _VP, _VP, _VP, _VP, _VP]),
@@ -218,6 +219,10 @@ class LinkedCells:
         cl, hm = np.zeros(3), np.zeros(3)
         self._check(self.lib.mdgpu_get_geometry(self.h, _ptr(nc), _ptr(cl), _ptr(hm)))
         return dict(box_cells=nc, cell_length=cl, halo_min=hm)
+
+    def setPairKernel(self, kind: int) -> None:
+        """0 = shared-memory brick kernel (default), 1 = simple gather kernel."""
+        self._check(self.lib.mdgpu_set_pair_kernel(self.h, int(kind)))
 
     def setPrecision(self, precision: int) -> None:
         self._check(self.lib.mdgpu_set_precision(self.h, int(precision)))

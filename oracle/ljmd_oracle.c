@@ -56,6 +56,7 @@ struct orc_sys {
 	double global_upot, global_virial, T, beta_trans, T_target;
 	int nve;
 	double npairs;
+	double u6_hi, u6_lo, w_hi, w_lo; /* compensated sums of the same pair terms */
 	/* RDF */
 	int rdf_on, rdf_bins;
 	double rdf_interval, rdf_max2;
@@ -402,6 +403,16 @@ int orc_exchange(orc_sys* s) {
 	return ORC_OK;
 }
 
+/* Compensated (double-double) accumulation, used only for the exactly-summed energy and virial
+ * the tests compare against; the reference's own sums are kept separately. */
+static void dd_add(double* hi, double* lo, double x) {
+	double s = *hi + x;
+	double bp = s - *hi;
+	double err = (*hi - (s - bp)) + (x - bp);
+	*hi = s;
+	*lo += err;
+}
+
 /* Molecule::isLessThan, Molecule.cpp:439-461 */
 static int is_less_than(const orc_mol* a, const orc_mol* b, int* err) {
 	if (a->r[2] < b->r[2]) return 1;
@@ -450,6 +461,10 @@ static void process_pair(orc_sys* s, orc_mol* m1, orc_mol* m2, const double drm[
 	for (int d = 0; d < 3; ++d) m2->F[d] -= f[d];
 	*upot6 += u;
 	for (int d = 0; d < 3; ++d) *virial += drm[d] * f[d];
+	if (mol_mol) {
+		dd_add(&s->u6_hi, &s->u6_lo, u);
+		dd_add(&s->w_hi, &s->w_lo, drm[0] * f[0] + drm[1] * f[1] + drm[2] * f[2]);
+	}
 }
 
 /* BlockTraverse::traversePairs, BlockTraverse.cpp:89-350 (LJ part; Tersoff passes are no-ops for
@@ -463,6 +478,7 @@ int orc_traverse(orc_sys* s) {
 	double rc2 = s->rc * s->rc, rcLJ2 = s->rcLJ * s->rcLJ;
 	int err = 0;
 	s->npairs = 0;
+	s->u6_hi = s->u6_lo = s->w_hi = s->w_lo = 0.0;
 	for (long k = s->head; k < s->tail; k++) {
 		orc_mol* m = &s->pool[s->order_buf[k]];
 		m->F[0] = m->F[1] = m->F[2] = 0.0;
@@ -736,6 +752,8 @@ void orc_scalars(const orc_sys* s, double* out) {
 	out[8] = s->virial_corr;
 	out[9] = s->npairs;
 	out[10] = s->summv2_end;
+	out[11] = (s->u6_hi + s->u6_lo) / 6.;
+	out[12] = s->w_hi + s->w_lo;
 }
 
 void orc_geometry(const orc_sys* s, int* oi, double* od) {

@@ -55,9 +55,11 @@ int orc_step(orc_sys* s, double dt, double tfactor);
 long orc_count(const orc_sys* s);
 /* Molecules in container order; any pointer may be NULL. cell[] is getCellIndexOfMolecule. */
 void orc_get(const orc_sys* s, unsigned long* id, int* cid, double* r, double* v, double* F, long* cell);
-/* out[0..10] = local Upot, local virial, summv2 (of Leapfrog::transition2to3), global Upot,
+/* out[0..12] = local Upot, local virial, summv2 (of Leapfrog::transition2to3), global Upot,
  *              global virial, T, beta_trans, UpotCorr, VirialCorr, number of processPair calls of
- *              the last traversal, sum m v^2 of the molecules at the end of the step */
+ *              the last traversal, sum m v^2 of the molecules at the end of the step, and the
+ *              local Upot and virial of the same pair terms summed with compensation (accurate to
+ *              ~1e-16 relative, unlike the reference's sequential sums) */
 void orc_scalars(const orc_sys* s, double* out);
 /* LinkedCells geometry: out_i[0..8] = boxWidthInNumCells[3], haloWidthInNumCells[3], cellsPerDim[3];
  * out_d[0..8] = cellLength[3], haloBoundingBoxMin[3], haloBoundingBoxMax[3] */

@@ -164,10 +164,10 @@ class Oracle:
         return out
 
     def scalars(self) -> Dict[str, float]:
-        out = np.zeros(11)
+        out = np.zeros(13)
         lib().orc_scalars(self.h, _p(out))
         keys = ["upot", "virial", "summv2", "global_upot", "global_virial", "T", "beta_trans",
-                "upot_corr", "virial_corr", "npairs", "summv2_end"]
+                "upot_corr", "virial_corr", "npairs", "summv2_end", "upot_exact", "virial_exact"]
         return dict(zip(keys, out.tolist()))
 
     def geometry(self):

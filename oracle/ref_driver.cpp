@@ -111,9 +111,10 @@ public:
 		prepare_start();
 		writeScalars(sf, 0);
 		if (dumps.count(0)) writeArrays(outdir, 0);
-		// Simulation::simulate runs _simstep = _initSimulation .. _numberOfTimesteps inclusive.
-		_numberOfTimesteps = _initSimulation + nsteps - 1;
+		// Simulation::simulate runs _simstep = _initSimulation .. _numberOfTimesteps inclusive;
+		// simulateStart sets _initSimulation (Simulation.cpp:1011), so it comes first.
 		simulateStart();
+		_numberOfTimesteps = _initSimulation + nsteps - 1;
 		long k = 1;
 		for (_simstep = _initSimulation; _simstep <= _numberOfTimesteps; k++) {
 			simulateStep();
@@ -125,8 +126,8 @@ public:
 
 	double timeSteps(unsigned long nsteps) {
 		prepare_start();
-		_numberOfTimesteps = _initSimulation + nsteps - 1;
 		simulateStart();
+		_numberOfTimesteps = _initSimulation + nsteps - 1;
 		double t0 = now_s();
 		for (_simstep = _initSimulation; _simstep <= _numberOfTimesteps;) simulateStep();
 		return (now_s() - t0) / nsteps;

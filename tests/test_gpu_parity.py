@@ -1,10 +1,13 @@
 """GPU parity through the C ABI against the reference (golden fixtures made by the compiled
 reference) and the oracle. Tolerances:
   * cell assignment and periodic wrap: bit-exact;
-  * MDGPU_FP64 forces: max_i |F_i - F_i^ref| / rms(F^ref) <= 1e-12 at step 0; Upot, virial and
-    sum m v^2 relative error <= 1e-12 at step 0 and <= 1e-9 along a trajectory (the GPU sums the
-    same pair terms in another order, and molecular dynamics amplifies the last-bit differences);
-  * MDGPU_MIXED forces: rms_i |F_i - F_i^ref| / rms(F^ref) <= 1e-5.
+  * MDGPU_FP64 forces: max_i |F_i - F_i^ref| / max(rms(F^ref), 1) <= 1e-12 at step 0 (the floor of
+    1 epsilon/sigma keeps the perfect-lattice starts, whose net forces are rounding noise, well
+    posed); Upot and virial within 1e-12 (relative) of the same pair terms summed exactly (the
+    oracle's compensated sums: the reference's own sequential sum carries ~1e-12 of rounding on a
+    lattice), and within 1e-9 of the reference along a trajectory (the GPU sums the same pair terms
+    in another order, and molecular dynamics amplifies the last-bit differences);
+  * MDGPU_MIXED forces on a thermalised configuration: rms_i |F_i - F_i^ref| / rms(F^ref) <= 1e-5.
 """
 import numpy as np
 import pytest
@@ -18,7 +21,7 @@ pytestmark = pytest.mark.gpu
 
 
 def force_err_max(F, Fref):
-    rms = np.sqrt(np.mean(np.sum(Fref * Fref, axis=1)))
+    rms = max(np.sqrt(np.mean(np.sum(Fref * Fref, axis=1))), 1.0)
     return float(np.max(np.linalg.norm(F - Fref, axis=1)) / rms)
 
 
@@ -42,8 +45,14 @@ def test_step0_fp64_matches_reference(name):
     np.testing.assert_array_equal(st["r"], g["s0_r"])
     assert force_err_max(st["F"], g["s0_F"]) <= 1e-12
     sc = sim.scalars()
-    assert rel(sc["upot"], g["upot"][0]) <= 1e-12
-    assert rel(sc["virial"], g["virial"][0]) <= 1e-12
+    o = O.Oracle(system)
+    o.init()
+    o.prepare_start()
+    so = o.scalars()
+    assert so["upot"] == g["upot"][0] and so["virial"] == g["virial"][0]
+    assert rel(sc["upot"], so["upot_exact"]) <= 1e-12
+    assert rel(sc["virial"], so["virial_exact"]) <= 1e-12
+    assert rel(sc["upot"], g["upot"][0]) <= 1e-10
 
 
 @pytest.mark.parametrize("name", GOLDEN_NAMES)
@@ -124,15 +133,23 @@ def test_pair_count_known_answer_lattice(precision):
     assert rel(u, o.scalars()["upot"]) <= (1e-12 if precision == M.FP64 else 1e-6)
 
 
-@pytest.mark.parametrize("name", ["fcc864_unshifted", "two_species_2048", "slab_8000"])
+@pytest.mark.parametrize("name", GOLDEN_NAMES)
 def test_mixed_precision_force_error(name):
+    # the last dumped step of each fixture: molecules have left their lattice sites
     system, g, meta = system_from_golden(name)
-    sim = M.Simulation(system, M.MIXED)
-    sim.prepare_start()
-    st = sim.state()
-    assert force_err_rms(st["F"], g["s0_F"]) <= 1e-5
-    assert rel(sim.scalars()["upot"], g["upot"][0]) <= 1e-5
-    assert rel(sim.scalars()["virial"], g["virial"][0]) <= 1e-5
+    k = max(meta["dumps"])
+    o = np.argsort(system.ids)
+    lc = M.LinkedCells.from_system(system, M.MIXED)
+    r = np.empty_like(system.r)
+    r[o] = g[f"s{k}_r"]
+    lc.setState(r=r)
+    lc.update()
+    u, w, _ = lc.traversePairs()
+    st = lc.getParticles()
+    F = st["F"][np.argsort(st["id"])]
+    assert force_err_rms(F, g[f"s{k}_F"]) <= 1e-5
+    assert rel(u, g["upot"][k]) <= 1e-5
+    assert rel(w, g["virial"][k]) <= 1e-5
 
 
 def test_fp64_is_deterministic():
@@ -173,7 +190,8 @@ def test_c1_100_steps_against_oracle():
     o.prepare_start()
     sim = M.Simulation(system, M.FP64)
     sim.prepare_start()
-    assert rel(sim.scalars()["upot"], o.scalars()["upot"]) <= 1e-12
+    assert rel(sim.scalars()["upot"], o.scalars()["upot_exact"]) <= 1e-12
+    assert rel(sim.scalars()["virial"], o.scalars()["virial_exact"]) <= 1e-12
     for k in range(100):
         o.step()
         sim.simulateStep()
