@@ -41,11 +41,15 @@ def parse():
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 drop-in comparison leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=25.0, help="bound of the CPU baseline sample")
+    ap.add_argument("--fcc-cells", type=int, default=64,
+                    help="FCC unit cells per box edge (64 -> 1,048,576 molecules; smaller for profiling)")
+    ap.add_argument("--pair-kernel", choices=["brick", "gather"], default="brick")
+    ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
 
 def workload_config(system, precision):
-    return {"workload": "lj_fcc_1m_rho0.75_T0.9_rc3.0", "n_molecules": int(system.n), "density": 0.75,
+    return {"workload": f"lj_fcc_{system.n}_rho0.75_T0.9_rc3.0", "n_molecules": int(system.n), "density": 0.75,
             "temperature": 0.9, "cutoff": float(system.cutoff), "dt": float(system.dt),
             "potential": "LJ 12-6 truncated-shifted, single species", "ensemble": "NVE",
             "pair_arithmetic": "fp32, fp64 accumulation" if precision == "mixed" else "fp64",
@@ -149,10 +153,12 @@ class ClockSampler:
 
 # ---------------------------------------------------------------------------- our arm
 
-def make_system(rank: int):
+def make_system(rank: int, fcc_cells: int = 64):
     from madpac_b200 import workloads as W
 
-    return W.config_c2(seed=2 + rank)
+    if fcc_cells == 64:
+        return W.config_c2(seed=2 + rank)
+    return W.lj_fcc_box(fcc_cells, 0.75, 0.9, 2 + rank, 3.0, [W.Component(1.0, 1.0, 1.0, True)])
 
 
 def time_device_resident(M, lc, system, steps, warmup, flush, stream):
@@ -274,8 +280,10 @@ def run_ours(args, dist: Dist):
 
     torch.cuda.set_device(dist.local)
     precision = M.MIXED if args.precision == "mixed" else M.FP64
-    system = make_system(dist.rank)
+    system = make_system(dist.rank, args.fcc_cells)
     lc = M.LinkedCells.from_system(system, precision, device=dist.local)
+    kernel = 0 if args.pair_kernel == "brick" else 1
+    lc.setPairKernel(kernel)
     lc.update()
     lc.traversePairs()
     stream = torch.cuda.ExternalStream(lc.stream())
@@ -311,9 +319,12 @@ def run_ours(args, dist: Dist):
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
 
     # end to end through the C ABI with host buffers
-    e2e_s, e2e_pairs, h2d, d2h = time_e2e(M, lc, system, max(3, args.steps // 2), stream)
-    e2e_s = dist.max(e2e_s)
-    e2e_value = dist.sum(e2e_pairs) / e2e_s
+    if args.no_e2e:
+        e2e_value, h2d, d2h = None, 0, 0
+    else:
+        e2e_s, e2e_pairs, h2d, d2h = time_e2e(M, lc, system, max(3, args.steps // 2), stream)
+        e2e_s = dist.max(e2e_s)
+        e2e_value = dist.sum(e2e_pairs) / e2e_s
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
@@ -340,6 +351,7 @@ def run_ours(args, dist: Dist):
     if not args.no_compare and dist.world == 1:
         other = M.FP64 if precision == M.MIXED else M.MIXED
         lc2 = M.LinkedCells.from_system(system, other, device=dist.local)
+        lc2.setPairKernel(kernel)
         lc2.update()
         lc2.traversePairs()
         ref_lc = lc2 if other == M.FP64 else None
@@ -380,7 +392,7 @@ def run_ours(args, dist: Dist):
 def run_reference(args, dist: Dist):
     """The reference's own CPU implementation (unmodified MarDyn sources, sequential build) on the
     same workload; rank 0 only."""
-    system = make_system(0)
+    system = make_system(0, args.fcc_cells)
     ref = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
     pairs = count_pairs_host(system)
     if os.path.exists(ref):
