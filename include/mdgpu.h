@@ -143,6 +143,24 @@ int mdgpu_synchronize(mdgpu_ctx* ctx);
  * SMs busy), in TFLOP/s counting an FMA as 2 flops; used as the roofline of the pair kernels. */
 int mdgpu_device_peaks(int device, double* fp32_tflops, double* fp64_tflops);
 
+/* Forces, local potential energy and virial of one periodic box without any device allocation.
+ * No counterpart in the reference: this is for callers that cannot call cudaMalloc while they
+ * run (hosts that own all device memory through their own pool, code inside a stream capture,
+ * latency-bound loops that must not block on the driver's allocator). Inputs and outputs are the
+ * caller's device buffers: d_r (n, 3) positions and d_cid (n) 0-based component ids in, d_F
+ * (n, 3) forces out; upot and virial (host, may be NULL) receive what mdgpu_traverse_pairs
+ * returns. All intermediate buffers live in one static device array of about 7.5 MB that every
+ * GPU loading the library holds until exit, so n <= 32768 and the cell grid <= 32768 cells
+ * (larger inputs return MDGPU_ERR_CAPACITY). Calls share that array and keep its last contents
+ * (each call clears what must start at zero); calls that overlap on the GPU race and must be
+ * serialised. The first call on a device looks up the array's address with that device current;
+ * make it before any stream capture. stream may be NULL (default stream); the call waits for it.
+ * errbuf (may be NULL) receives a message of at most errlen bytes. */
+int mdgpu_forces_noalloc(int device, void* stream, int64_t n, const double* d_r, const int32_t* d_cid,
+                         const double length[3], double cutoff, double lj_cutoff, int ncomp,
+                         const mdgpu_component* comps, const double* mix, int precision, double* d_F,
+                         double* upot, double* virial, char* errbuf, int errlen);
+
 #ifdef __cplusplus
 }
 #endif

@@ -67,6 +67,8 @@ SIGNATURES = {
     "mdgpu_profile_read": (_I, [_VP, _VP, _VP, _I]),
     "mdgpu_get_stream": (_I, [_VP, _VP]),
     "mdgpu_synchronize": (_I, [_VP]),
+    "mdgpu_forces_noalloc": (_I, [_I, _VP, _I64, _VP, _VP, _VP, _D, _D, _I, _VP, _VP, _I, _VP, _VP, _VP,
+                                  ctypes.c_char_p, _I]),
 }
 
 _lib = None
@@ -117,6 +119,35 @@ def device_peaks(device: int = 0):
     if st != 0:
         raise MdgpuError(st, "device peak measurement failed")
     return a.value, b.value
+
+
+def forces_noalloc(d_r: int, d_cid: int, d_F: int, n: int, length, cutoff: float, components, mixcoeff=None,
+                   LJCutoffRadius: float = 0.0, precision: int = FP64, device: int = 0, stream: int = 0):
+    """Forces, local Upot and virial of one box with no device allocation inside the call.
+
+    For callers that cannot allocate device memory while they run (a host owning all memory
+    through its own pool, a stream being captured, a latency-bound loop): d_r, d_cid and d_F are
+    device addresses of buffers the caller owns ((n, 3) float64, (n,) int32, (n, 3) float64).
+    At most 32768 molecules and 32768 cells (the size of the library's static scratch array).
+    Returns (upot, virial).
+    """
+    lib = load_library()
+    comps = (_MdComponent * len(components))()
+    for k, c in enumerate(components):
+        comps[k].eps, comps[k].sigma, comps[k].mass = float(c.eps), float(c.sigma), float(c.mass)
+        comps[k].do_shift = 1 if c.do_shift else 0
+    length = _c64(length)
+    mix = None if mixcoeff is None else _c64(mixcoeff).reshape(-1)
+    if mix is not None and mix.size == 0:
+        mix = None
+    u, w = ctypes.c_double(), ctypes.c_double()
+    err = ctypes.create_string_buffer(256)
+    st = lib.mdgpu_forces_noalloc(int(device), stream or None, int(n), d_r, d_cid, _ptr(length), float(cutoff),
+                                  float(LJCutoffRadius), len(components), ctypes.cast(comps, ctypes.c_void_p),
+                                  _ptr(mix), int(precision), d_F, ctypes.byref(u), ctypes.byref(w), err, 256)
+    if st != 0:
+        raise MdgpuError(st, err.value.decode())
+    return u.value, w.value
 
 
 class LinkedCells:
