@@ -129,6 +129,15 @@ int mdgpu_run_async(mdgpu_ctx* ctx, int32_t nsteps, double dt);
  * report status. */
 int mdgpu_read_steps(mdgpu_ctx* ctx, int32_t nsteps, double* per_step);
 
+/* Adjoint of the forces and potential energy at the current positions (call after mdgpu_update;
+ * no counterpart in the reference, which has no gradients). Given the cotangents gF = dL/dF
+ * ((n, 3), caller order) and gU = dL/dUpot of a loss L, returns dL/dr ((n, 3), caller order) and,
+ * for every component pair (a, b), dL/d(eps_ab) and dL/d(sigma_ab) in ncomp x ncomp symmetric
+ * arrays (may be NULL), where eps_ab = eps24/24 and sigma_ab = sqrt(sig2) of the Comp2Param stream
+ * (molecules/Comp2Param.cpp:28-115) and truncated-shifted pairs include the shift's dependence.
+ * Double precision. */
+int mdgpu_adjoint(mdgpu_ctx* ctx, const double* gF, double gU, double* dL_dr, double* dL_deps, double* dL_dsigma);
+
 /* Device-side timing of the kernels this context launches, for benchmarking: when enabled, CUDA
  * events on the context's stream bracket the binning, pair and integration kernels. times_ms[0..2]
  * = total binning, pair, integration milliseconds since the last reset; counts[0..3] = launches of

@@ -1,0 +1,160 @@
+// Adjoint (vector-Jacobian product) of the LJ forces and potential energy.
+//
+// For a loss L whose cotangents are gF_i = dL/dF_i and gU = dL/dUpot, this kernel returns
+// dL/dr_k and dL/d(eps_ab), dL/d(sigma_ab) for every component pair, where the pair parameters are
+// eps_ab = eps24/24 and sigma_ab = sqrt(sig2) of the Comp2Param stream (Comp2Param.cpp:28-115;
+// paths relative to madpac/mardyn/). The reference has no gradients; the forward quantities are
+// those of PotForceLJ (molecules/potforce.h:41-53) with Upot = sum (u6 + shift6)/6
+// (ParticlePairs2PotForceAdapter.h:65).
+//
+// Per pair, d = r_i - r_j, q = d.d, s6 = (sig2/q)^3, s12 = s6^2:
+//   f = fac d,  fac = eps24 (2 s12 - s6)/q,  dfac/dq = eps24 (4 s6 - 14 s12)/q^2
+//   J = df/dd = fac I + 2 dfac/dq d d^T   (symmetric),   dU_pair/dd = -f
+//   dL/dr_i += J (gF_i - gF_j) - gU f
+//   df/deps24 = f/eps24;  df/dsig2 = eps24 (12 s12 - 3 s6)/(q sig2) d
+//   dU_pair/deps24 = (s12 - s6 + c6)/6,  dU_pair/dsig2 = eps24 (6 s12 - 3 s6 + c6')/(6 sig2)
+// with c6 = sr6 - sr6^2, c6' = 3 sr6 - 6 sr6^2 (sr6 = (sig2/rcLJ^2)^3) for truncated-shifted pair
+// types (shift6 != 0) and 0 otherwise. Every molecule gathers over its 27 neighbour cells (each
+// pair is seen from both sides, so parameter terms carry a factor 1/2). FP64 throughout.
+#include <cuda_runtime.h>
+
+#include "md_internal.h"
+#include "reduce.cuh"
+
+namespace mdgpu {
+namespace {
+
+constexpr int KK = kMaxSpecies * kMaxSpecies;
+
+__global__ void __launch_bounds__(kReduceBlock) k_adjoint(int64_t n, Particles p, const int32_t* __restrict__ start,
+                                                         Grid g, const PairParams* __restrict__ pp, double rclj,
+                                                         const double* __restrict__ gfx, const double* __restrict__ gfy,
+                                                         const double* __restrict__ gfz, double gU,
+                                                         double* __restrict__ ox, double* __restrict__ oy,
+                                                         double* __restrict__ oz, double* __restrict__ pgrad) {
+	__shared__ double s_e24[KK], s_s2[KK], s_sh[KK];
+	__shared__ double s_acc[2 * KK];
+	const int ns = pp->ns;
+	for (int k = threadIdx.x; k < KK; k += blockDim.x) {
+		s_e24[k] = k < ns * ns ? pp->eps24[k] : 0.0;
+		s_s2[k] = k < ns * ns ? pp->sig2[k] : 0.0;
+		s_sh[k] = k < ns * ns ? pp->shift6[k] : 0.0;
+		s_acc[k] = 0.0;
+		s_acc[KK + k] = 0.0;
+	}
+	__syncthreads();
+	const double rc2 = pp->rc2, rclj2 = pp->rclj2, rclj6 = rclj2 * rclj2 * rclj2;
+	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	double acc_e[KK], acc_s[KK];
+	for (int k = 0; k < ns * ns; k++) acc_e[k] = acc_s[k] = 0.0;
+	if (i < n) {
+		const double xi = p.rx[i], yi = p.ry[i], zi = p.rz[i];
+		const double wix = gfx[i], wiy = gfy[i], wiz = gfz[i];
+		const int ti = p.cid[i];
+		int cc[3];
+		const double r[3] = {xi, yi, zi};
+		for (int d = 0; d < 3; d++) {
+			int c = (int) floor(__ddiv_rn(__dsub_rn(r[d], g.halo_min[d]), g.cell_length[d])) - 1;
+			cc[d] = c < 0 ? 0 : (c >= g.nc[d] ? g.nc[d] - 1 : c);
+		}
+		double ax = 0.0, ay = 0.0, az = 0.0;
+		for (int dz = -1; dz <= 1; dz++) {
+			int z = cc[2] + dz;
+			double sz = 0.0;
+			if (z < 0) {
+				z += g.nc[2];
+				sz = -g.L[2];
+			} else if (z >= g.nc[2]) {
+				z -= g.nc[2];
+				sz = g.L[2];
+			}
+			for (int dy = -1; dy <= 1; dy++) {
+				int y = cc[1] + dy;
+				double sy = 0.0;
+				if (y < 0) {
+					y += g.nc[1];
+					sy = -g.L[1];
+				} else if (y >= g.nc[1]) {
+					y -= g.nc[1];
+					sy = g.L[1];
+				}
+				for (int dx = -1; dx <= 1; dx++) {
+					int x = cc[0] + dx;
+					double sx = 0.0;
+					if (x < 0) {
+						x += g.nc[0];
+						sx = -g.L[0];
+					} else if (x >= g.nc[0]) {
+						x -= g.nc[0];
+						sx = g.L[0];
+					}
+					const int nb = (z * g.nc[1] + y) * g.nc[0] + x;
+					const bool shifted = (sx != 0.0) || (sy != 0.0) || (sz != 0.0);
+					for (int j = start[nb]; j < start[nb + 1]; j++) {
+						if (j == i && !shifted) continue;
+						const double d0 = xi - (p.rx[j] + sx), d1 = yi - (p.ry[j] + sy), d2 = zi - (p.rz[j] + sz);
+						const double q = d0 * d0 + d1 * d1 + d2 * d2;
+						if (!(q < rc2) || !(q < rclj2)) continue;
+						const int pk = ti * ns + p.cid[j];
+						const double e24 = s_e24[pk], sg2 = s_s2[pk];
+						const double iq = 1.0 / q;
+						double s6 = sg2 * iq;
+						s6 = s6 * s6 * s6;
+						const double s12 = s6 * s6;
+						const double fac = e24 * (2.0 * s12 - s6) * iq;
+						const double dfac = e24 * (4.0 * s6 - 14.0 * s12) * iq * iq;
+						const double w0 = wix - gfx[j], w1 = wiy - gfy[j], w2 = wiz - gfz[j];
+						const double dw = d0 * w0 + d1 * w1 + d2 * w2;
+						// J w - gU f
+						ax += fac * w0 + 2.0 * dfac * dw * d0 - gU * fac * d0;
+						ay += fac * w1 + 2.0 * dfac * dw * d1 - gU * fac * d1;
+						az += fac * w2 + 2.0 * dfac * dw * d2 - gU * fac * d2;
+						// parameter terms (half: the pair is seen from both sides)
+						const bool shf = s_sh[pk] != 0.0;
+						double sr6 = sg2 * sg2 * sg2 / rclj6;
+						const double c6 = shf ? sr6 - sr6 * sr6 : 0.0;
+						const double c6s = shf ? 3.0 * sr6 - 6.0 * sr6 * sr6 : 0.0;
+						acc_e[pk] += 0.5 * (fac * dw / e24 + gU * (s12 - s6 + c6) / 6.0);
+						acc_s[pk] += 0.5 * (e24 * (12.0 * s12 - 3.0 * s6) * iq / sg2 * dw +
+						                    gU * e24 * (6.0 * s12 - 3.0 * s6 + c6s) / (6.0 * sg2));
+					}
+				}
+			}
+		}
+		ox[i] = ax;
+		oy[i] = ay;
+		oz[i] = az;
+	}
+	// block sum of the per-type parameter terms, then one partial row per block
+	for (int k = 0; k < ns * ns; k++) {
+		const double ve = warp_sum(acc_e[k]), vs = warp_sum(acc_s[k]);
+		if ((threadIdx.x & 31) == 0) {
+			atomicAdd(&s_acc[k], ve);
+			atomicAdd(&s_acc[KK + k], vs);
+		}
+	}
+	__syncthreads();
+	for (int k = threadIdx.x; k < 2 * KK; k += blockDim.x) pgrad[(int64_t) blockIdx.x * 2 * KK + k] = s_acc[k];
+}
+
+__global__ void k_adjoint_params(int64_t nblocks, const double* __restrict__ pgrad, double* __restrict__ out) {
+	const int k = threadIdx.x;
+	if (k >= 2 * KK) return;
+	double s = 0.0;
+	for (int64_t b = 0; b < nblocks; b++) s += pgrad[b * 2 * KK + k];
+	out[k] = s;
+}
+
+}  // namespace
+
+cudaError_t launch_adjoint(Context* c, const double* gfx, const double* gfy, const double* gfz, double gU, double* ox,
+                           double* oy, double* oz, double* pgrad, double* pout) {
+	const int64_t nb = (c->n + kReduceBlock - 1) / kReduceBlock;
+	k_adjoint<<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(c->n, c->p, c->cell_start, c->g, c->d_pp, c->rc_lj, gfx,
+	                                                          gfy, gfz, gU, ox, oy, oz, pgrad);
+	k_adjoint_params<<<1, 2 * KK, 0, c->stream>>>(nb, pgrad, pout);
+	count_launches(c, 2);
+	return cudaGetLastError();
+}
+
+}  // namespace mdgpu

@@ -340,6 +340,7 @@ int mdgpu_destroy(mdgpu_ctx* ctx) {
 	cudaFree(c->steps_out);
 	cudaFree(c->status);
 	cudaFree(c->d_pp);
+	cudaFree(c->adj);
 	cudaFree(full->x.stage.ptr);
 	if (c->h_scalars) cudaFreeHost(c->h_scalars);
 	if (c->h_status) cudaFreeHost(c->h_status);
@@ -677,6 +678,52 @@ int mdgpu_read_steps(mdgpu_ctx* ctx, int32_t nsteps, double* per_step) {
 	c->steps_written = 0;
 	if (st) c->cells_valid = false;
 	return st;
+}
+
+int mdgpu_adjoint(mdgpu_ctx* ctx, const double* gF, double gU, double* dL_dr, double* dL_deps, double* dL_dsigma) {
+	if (!ctx) return MDGPU_ERR_ARG;
+	Context* c = &ctx->c;
+	if (!gF || !dL_dr) return fail(c, MDGPU_ERR_ARG, "gF and dL_dr are required");
+	if (!c->cells_valid) return fail(c, MDGPU_ERR_STATE, "cell structure invalid, call mdgpu_update first");
+	MD_CUDA(cudaSetDevice(c->device));
+	constexpr int KK = kMaxSpecies * kMaxSpecies;
+	const int64_t n = c->n;
+	const int64_t nb = (n + kReduceBlock - 1) / kReduceBlock;
+	const int64_t need = 6 * n + nb * 2 * KK + 2 * KK;
+	if (need > c->adj_cap) {
+		cudaFree(c->adj);
+		c->adj = nullptr;
+		MD_CUDA(cudaMalloc(&c->adj, sizeof(double) * need));
+		c->adj_cap = need;
+	}
+	double *gx = c->adj, *gy = gx + n, *gz = gy + n, *ox = gz + n, *oy = ox + n, *oz = oy + n;
+	double* pgrad = oz + n;
+	double* pout = pgrad + nb * 2 * KK;
+	void* st;
+	MD_CUDA(staging(c, extra(c)->stage, sizeof(double) * 3 * n, &st));
+	double* aos = (double*) st;
+	MD_CUDA(cudaMemcpyAsync(aos, gF, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+	k_load_aos<<<blocks_for(n), kThreads, 0, c->stream>>>(n, aos, c->p.uidx, gx, gy, gz);
+	count_launches(c, 1);
+	MD_CUDA(launch_adjoint(c, gx, gy, gz, gU, ox, oy, oz, pgrad, pout));
+	k_store_aos<<<blocks_for(n), kThreads, 0, c->stream>>>(n, ox, oy, oz, c->p.uidx, aos);
+	count_launches(c, 1);
+	MD_CUDA(cudaMemcpyAsync(dL_dr, aos, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream));
+	double par[2 * KK];
+	MD_CUDA(cudaMemcpyAsync(par, pout, sizeof(par), cudaMemcpyDeviceToHost, c->stream));
+	int sts = check_status(c);
+	if (sts) return sts;
+	// one parameter per unordered component pair: both orientations of the table contribute
+	const int ns = c->sp.n;
+	for (int a = 0; a < ns; a++)
+		for (int b = 0; b < ns; b++) {
+			const int ab = a * ns + b, ba = b * ns + a;
+			const double ge = a == b ? par[ab] : par[ab] + par[ba];
+			const double gs = a == b ? par[KK + ab] : par[KK + ab] + par[KK + ba];
+			if (dL_deps) dL_deps[ab] = 24.0 * ge;                            // eps24 = 24 eps_ab
+			if (dL_dsigma) dL_dsigma[ab] = 2.0 * std::sqrt(c->sp.sig2[ab]) * gs;  // sig2 = sigma_ab^2
+		}
+	return MDGPU_OK;
 }
 
 int mdgpu_profile_enable(mdgpu_ctx* ctx, int enable) {

@@ -92,6 +92,8 @@ struct Context {
 	int64_t steps_written = 0;      // records appended since the last mdgpu_read_steps
 	int* status = nullptr;          // device status word
 	PairParams* d_pp = nullptr;     // device copy of the pair parameters
+	double* adj = nullptr;          // adjoint buffers: cotangents, outputs, parameter partials
+	int64_t adj_cap = 0;
 	double* h_scalars = nullptr;    // pinned host mirror
 	int* h_status = nullptr;
 
@@ -111,6 +113,8 @@ cudaError_t launch_leapfrog_pre(Context* c, double dt, double vcorr);
 cudaError_t launch_leapfrog_post(Context* c, double dt_half);   // scalars[3] = sum m v^2
 cudaError_t launch_scale(Context* c, double beta);
 cudaError_t launch_reduce(Context* c, int64_t nblocks, double* out, int nval);
+cudaError_t launch_adjoint(Context* c, const double* gfx, const double* gfy, const double* gfz, double gU, double* ox,
+                           double* oy, double* oz, double* pgrad, double* pout);
 cudaError_t launch_step_record(Context* c, double* dst);        // dst[0..3] <- step scalars
 
 // Timing brackets around a group of launches (0 = binning, 1 = pairs, 2 = integration).

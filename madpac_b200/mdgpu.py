@@ -63,6 +63,7 @@ SIGNATURES = {
     "mdgpu_run_async": (_I, [_VP, _I32, _D]),
     "mdgpu_read_steps": (_I, [_VP, _I32, _VP]),
     "mdgpu_device_peaks": (_I, [_I, _VP, _VP]),
+    "mdgpu_adjoint": (_I, [_VP, _VP, _D, _VP, _VP, _VP]),
     "mdgpu_profile_enable": (_I, [_VP, _I]),
     "mdgpu_profile_read": (_I, [_VP, _VP, _VP, _I]),
     "mdgpu_get_stream": (_I, [_VP, _VP]),
@@ -274,6 +275,17 @@ class LinkedCells:
         u, w = ctypes.c_double(), ctypes.c_double()
         self._check(self.lib.mdgpu_far_field_correction(self.h, ctypes.byref(u), ctypes.byref(w)))
         return u.value, w.value
+
+    def adjoint(self, gF, gU: float):
+        """(dL/dr (n, 3), dL/d eps_ab, dL/d sigma_ab) for cotangents gF = dL/dF, gU = dL/dUpot at the
+        current positions (after update)."""
+        ns = len(self.components)
+        gr = np.zeros((self.n, 3))
+        ge = np.zeros((ns, ns))
+        gs = np.zeros((ns, ns))
+        self._check(self.lib.mdgpu_adjoint(self.h, _ptr(_c64(gF, shape=(self.n, 3))), float(gU), _ptr(gr), _ptr(ge),
+                                           _ptr(gs)))
+        return gr, ge, gs
 
     def step(self, dt: float, vcorr: float = 1.0) -> np.ndarray:
         out = np.zeros(4)
