@@ -45,6 +45,11 @@ def parse():
                     help="FCC unit cells per box edge (64 -> 1,048,576 molecules; smaller for profiling)")
     ap.add_argument("--pair-kernel", choices=["brick", "gather"], default="brick")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", choices=["c2", "batched"], default="c2",
+                    help="c2: the 1M-molecule box (headline); batched: the 512-box ensemble")
+    ap.add_argument("--boxes", type=int, default=512, help="boxes of the batched ensemble")
+    ap.add_argument("--loop-steps", type=int, default=20,
+                    help="steps of the loop-over-single-box comparison of the batched workload")
     return ap.parse_args()
 
 
@@ -387,6 +392,144 @@ def run_ours(args, dist: Dist):
     return out
 
 
+# ---------------------------------------------------------------------------- batched ensemble
+
+BATCH_METRIC = "LJ pair-interactions/s, 512-box ensemble (N 256-8192), 1 B200"
+
+
+def _ref_box_time(args_):
+    """Seconds per step of the reference harness on one box (runs in a worker process)."""
+    ref, system, nsteps = args_
+    from madpac_b200 import workloads as W
+
+    tmp = tempfile.mkdtemp(prefix="mdref_")
+    W.write_inp(system, os.path.join(tmp, "sys.inp"))
+    W.write_cfg(system, os.path.join(tmp, "sys.cfg"), "sys.inp")
+    out = subprocess.run([ref, "--time", "sys.cfg", str(nsteps)], cwd=tmp, capture_output=True, text=True, timeout=600)
+    return json.loads(out.stdout.strip().splitlines()[-1])["seconds_per_step"]
+
+
+def batched_cpu_baseline(systems, pairs_per_box, cores=8, sample_boxes=32, nsteps=20):
+    """The reference harness on a sample of the boxes (every k-th by size), `cores` processes at a
+    time, as 512 separate reference runs would go; throughput = sampled pairs*steps / wall time."""
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    if not os.path.exists(ref):
+        return {"value": None, "error": "oracle/_ref/ref_driver was not built"}
+    import multiprocessing as mp
+
+    order = np.argsort([s.n for s in systems])
+    pick = order[:: max(1, len(systems) // sample_boxes)][:sample_boxes]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        secs = pool.map(_ref_box_time, [(ref, systems[k], nsteps) for k in pick])
+    wall = time.perf_counter() - t0
+    # wall includes process start and input writing; the per-box step times give the stepping rate
+    step_rate = sum(pairs_per_box[k] for k in pick) / sum(secs) * cores
+    return {"value": step_rate, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{len(pick)} of {len(systems)} boxes (every {max(1, len(systems) // sample_boxes)}-th by size), "
+                      f"{nsteps} steps each, {cores} concurrent single-threaded reference processes; "
+                      f"rate = sum(pairs per step) / sum(seconds per step) x {cores}",
+            "wall_seconds": wall}
+
+
+def run_batched(args, dist: Dist):
+    import torch
+
+    from madpac_b200 import mdgpu as M
+    from madpac_b200 import workloads as W
+
+    torch.cuda.set_device(dist.local)
+    precision = M.MIXED if args.precision == "mixed" else M.FP64
+    systems = W.config_c4(seed=4 + dist.rank, n_boxes=args.boxes)
+    dt = systems[0].dt
+    b = M.Batch.from_systems(systems, precision, device=dist.local)
+    prep = b.prepare()
+    best, cand_ms = b.autotune(dt, trial_steps=5)
+    b.run(args.warmup, dt, record=False)
+    dist.barrier()
+    clocks = ClockSampler(dist.local)
+    clocks.start()
+    recs = b.run(args.steps, dt)
+    clk = clocks.stop()
+    seconds = dist.max(b.lastRunMs() * 1e-3)
+    pairs = float(recs[:, :, 3].sum())
+    value = dist.sum(pairs) / seconds
+    ntot = sum(s.n for s in systems)
+
+    # end to end: host arrays in, records and the final state out, through the batch C ABI
+    e2e = None
+    if not args.no_e2e:
+        st = b.getParticles()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.setParticles(st["id"], st["cid"], st["r"], st["v"])
+        b.prepare()
+        r2 = b.run(args.steps, dt)
+        b.getParticles()
+        e2e_s = dist.max(time.perf_counter() - t0)
+        e2e = {"value": dist.sum(float(r2[:, :, 3].sum())) / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": (60 * ntot) / args.steps, "d2h_bytes_per_step": 32 * len(systems) + 84 * ntot / args.steps,
+               "note": "one upload of id, cid, r, v and one download of the final state per run of `steps` steps"}
+
+    # the comparison: one single-box context per box, stepped in a host loop (own stream each)
+    loop = None
+    if args.loop_steps > 0:
+        ctxs = []
+        for s in systems:
+            lc = M.LinkedCells.from_system(s, precision, device=dist.local)
+            lc.update()
+            lc.traversePairs()
+            ctxs.append(lc)
+        for lc in ctxs:
+            lc.runAsync(2, dt)
+        for lc in ctxs:
+            lc.readSteps(2)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.loop_steps):
+            for lc in ctxs:
+                lc.runAsync(1, dt)
+        lpairs = 0.0
+        for lc in ctxs:
+            lpairs += float(lc.readSteps(args.loop_steps)[:, 3].sum())
+        torch.cuda.synchronize()
+        lsec = time.perf_counter() - t0
+        launches = sum(lc.profileRead()[1][3] for lc in ctxs)
+        for lc in ctxs:
+            lc.close()
+        loop = {"value": lpairs / lsec, "ms_per_step": lsec / args.loop_steps * 1e3, "steps": args.loop_steps,
+                "timing": "host wall clock around the loop, synchronised at both ends",
+                "launches_per_step": launches / (args.loop_steps + 2)}
+    out = {
+        "metric": BATCH_METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": seconds / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 pair arithmetic, f64 accumulation" if precision == M.MIXED else "f64",
+        "data": "synthetic (seeded FCC subsets, Maxwell-Boltzmann velocities)",
+        "config": {"workload": f"c4_{len(systems)}_boxes", "n_boxes": len(systems), "n_molecules": ntot,
+                   "n_min": min(s.n for s in systems), "n_max": max(s.n for s in systems), "cutoff": 2.5,
+                   "dt": dt, "ensemble": "NVE", "tiles": {"list_cap": best[0], "ctas_per_sm": best[1],
+                                                         "brick_queue": best[2]},
+                   "autotune_ms_per_step": {f"cap{c}_ctas{t}_q{q}": v for (c, t, q), v in cand_ms.items()},
+                   "l2": f"working set larger than L2 ({ntot * 200 / 1e6:.0f} MB of molecule arrays)"},
+        "steps_per_s": args.steps / seconds, "box_steps_per_s": len(systems) * args.steps / seconds,
+        "pairs_per_step": pairs / args.steps,
+        "timing": "CUDA events around the graph launch of all timed steps",
+        "gpu_launches": args.steps,
+        "e2e": e2e, "loop_single_box": loop,
+        "speedup_vs_loop": (value / loop["value"]) if loop else None,
+        "clocks": clk,
+    }
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        try:
+            out["cpu_baseline"] = batched_cpu_baseline(systems, prep[:, 3])
+        except Exception as e:
+            out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    b.close()
+    return out
+
+
 # ---------------------------------------------------------------------------- reference arm
 
 def run_reference(args, dist: Dist):
@@ -449,7 +592,7 @@ def main():
             print(json.dumps(run_reference(args, solo)), flush=True)
         return
     dist = Dist(args.gpus)
-    out = run_ours(args, dist)
+    out = run_batched(args, dist) if args.workload == "batched" else run_ours(args, dist)
     if dist.rank == 0:
         print(json.dumps(out), flush=True)
     dist.close()

@@ -170,6 +170,46 @@ int mdgpu_forces_noalloc(int device, void* stream, int64_t n, const double* d_r,
                          const mdgpu_component* comps, const double* mix, int precision, double* d_F,
                          double* upot, double* virial, char* errbuf, int errlen);
 
+/* ---- batched ensemble of independent boxes ------------------------------------------------
+ * No reference counterpart: in MarDyn every box is its own Simulation with its own LinkedCells
+ * (Simulation.cpp:907-1308), run one after the other. A batch holds nboxes independent periodic
+ * boxes [0, L_b) of n_b molecules that share the cutoffs, the components and the precision mode,
+ * and advances all of them with one persistent (cooperative) kernel launch per step, replayed from
+ * a captured CUDA graph. Per box and step the kernel does what mdgpu_step does for one box
+ * (Leapfrog pre, wrap and binning, pair forces, Leapfrog post), with the same arithmetic.
+ * Molecule arrays are box-major: box 0's n_0 molecules, then box 1's, and so on. Per-box records
+ * are 4 doubles {Upot, virial, sum m v^2, pairs}, as the out4 of mdgpu_step. */
+typedef struct mdgpu_batch mdgpu_batch;
+
+/* lengths: nboxes x 3; counts: molecules per box. Boxes whose cell sort does not fit in shared
+ * memory (about 17,000 molecules) are rejected with MDGPU_ERR_CAPACITY. */
+int mdgpu_batch_create(mdgpu_batch** out, int32_t nboxes, const double* lengths, const int64_t* counts,
+                       double cutoff, double lj_cutoff, double cells_in_cutoff, int ncomp,
+                       const mdgpu_component* comps, const double* mix, int precision, int device);
+int mdgpu_batch_destroy(mdgpu_batch* b);
+const char* mdgpu_batch_last_error(const mdgpu_batch* b);
+int mdgpu_batch_set_particles(mdgpu_batch* b, int64_t ntotal, const uint64_t* id, const int32_t* cid,
+                              const double* r, const double* v);
+int mdgpu_batch_get_particles(mdgpu_batch* b, int64_t ntotal, uint64_t* id, int32_t* cid, double* r,
+                              double* v, double* F);
+/* Initial binning and force evaluation of every box (as Simulation::prepare_start); out: nboxes x 4
+ * (may be NULL). */
+int mdgpu_batch_prepare(mdgpu_batch* b, double* out);
+/* nsteps NVE steps of every box; per_step: nsteps x nboxes x 4 (may be NULL). */
+int mdgpu_batch_run(mdgpu_batch* b, int32_t nsteps, double dt, double* per_step);
+/* Tile shape of the persistent kernel: per-lane candidate list depth (32 or 64), CTAs per SM
+ * (1 or 2; sets the shared-memory staging capacity), brick distribution (0 static, 1 queue). */
+int mdgpu_batch_set_tiles(mdgpu_batch* b, int32_t list_cap, int32_t ctas_per_sm, int32_t dynamic);
+int mdgpu_batch_get_tiles(const mdgpu_batch* b, int32_t tiles[3]);
+/* Times every tile shape for trial_steps steps from the current state (restored afterwards), keeps
+ * the fastest; best: its 3 values, ms: device ms per step of each of the 8 candidates (may be NULL). */
+int mdgpu_batch_autotune(mdgpu_batch* b, double dt, int32_t trial_steps, int32_t best[3], double* ms);
+/* Device time of the last mdgpu_batch_run (CUDA events around the graph launch). */
+int mdgpu_batch_last_run_ms(const mdgpu_batch* b, double* ms);
+/* Limit of each grid-barrier wait in nanoseconds (default 2e9); a wait that runs out sets
+ * MDGPU_ERR_TIMEOUT and the kernel returns. */
+int mdgpu_batch_set_barrier_timeout(mdgpu_batch* b, int64_t ns);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,8 +9,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmdgpu.so")
-SOURCES = ["api.cu", "binning.cu", "pairs.cu", "pairs_brick.cu", "integrate.cu", "peaks.cu", "noalloc.cu", "adjoint.cu"]
-HEADERS = ["md_internal.h", "reduce.cuh", "pair_common.cuh"]
+SOURCES = ["api.cu", "binning.cu", "pairs.cu", "pairs_brick.cu", "integrate.cu", "peaks.cu", "noalloc.cu", "adjoint.cu", "batch.cu"]
+HEADERS = ["md_internal.h", "reduce.cuh", "pair_common.cuh", "brick.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

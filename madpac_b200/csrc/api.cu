@@ -208,63 +208,51 @@ Extra* extra(Context* c) { return &reinterpret_cast<mdgpu_ctx_full*>(reinterpret
 }  // namespace
 }  // namespace mdgpu
 
-using namespace mdgpu;
+namespace mdgpu {
 
-extern "C" {
-
-int mdgpu_create(mdgpu_ctx** out, const double length[3], double cutoff, double lj_cutoff, double cells_in_cutoff,
-                 int ncomp, const mdgpu_component* comps, const double* mix, int precision, int device) {
-	if (!out || !length || !comps) return MDGPU_ERR_ARG;
-	*out = nullptr;
-	mdgpu_ctx_full* full = new (std::nothrow) mdgpu_ctx_full();
-	if (!full) return MDGPU_ERR_ARG;
-	Context* c = &full->pub.c;
-	*out = &full->pub;
-	if (ncomp < 1 || ncomp > kMaxSpecies) return fail(c, MDGPU_ERR_ARG, "ncomp must be in 1..8");
-	if (!(cutoff > 0)) return fail(c, MDGPU_ERR_ARG, "cutoff must be positive");
-	if (cells_in_cutoff != 1.0) return fail(c, MDGPU_ERR_ARG, "only cellsInCutoffRadius = 1 is supported");
-	if (precision != MDGPU_FP64 && precision != MDGPU_MIXED) return fail(c, MDGPU_ERR_ARG, "unknown precision mode");
-	if (ncomp > 1 && !mix) return fail(c, MDGPU_ERR_ARG, "mixing coefficients are required for ncomp > 1");
-	int ndev = 0;
-	cudaError_t e = cudaGetDeviceCount(&ndev);
-	if (e != cudaSuccess || ndev == 0) return fail(c, MDGPU_ERR_CUDA, "no CUDA device is available");
-	if (device < 0 || device >= ndev) return fail(c, MDGPU_ERR_ARG, "device index out of range");
-	c->device = device;
-	c->precision = precision;
-	c->rc = cutoff;
-	c->rc_lj = lj_cutoff == 0.0 ? cutoff : lj_cutoff;
-	MD_CUDA(cudaSetDevice(device));
+int setup_grid(const double length[3], double cutoff, double cells_in_cutoff, Grid& g, std::string& err) {
 	// LinkedCells geometry for the bounding box [0, L) (LinkedCells.cpp:54-71)
 	int64_t ncells = 1;
 	for (int d = 0; d < 3; d++) {
-		if (!(length[d] > 0)) return fail(c, MDGPU_ERR_ARG, "box lengths must be positive");
+		if (!(length[d] > 0)) {
+			err = "box lengths must be positive";
+			return MDGPU_ERR_ARG;
+		}
 		double bbmin = 0.0, bbmax = length[d];
 		int w = (int) std::floor((bbmax - bbmin) / cutoff * cells_in_cutoff);
 		if (w == 0) w = 1;
-		if (w < 2)
-			return fail(c, MDGPU_ERR_BOX_TOO_SMALL,
-			            "the box must hold at least 2 cells of edge >= cutoff in every dimension");
-		c->g.nc[d] = w;
-		c->g.L[d] = length[d];
-		c->g.cell_length[d] = (bbmax - bbmin) / w;
-		double halo_len = 1 * c->g.cell_length[d];
-		c->g.halo_min[d] = bbmin - halo_len;
+		if (w < 2) {
+			err = "the box must hold at least 2 cells of edge >= cutoff in every dimension";
+			return MDGPU_ERR_BOX_TOO_SMALL;
+		}
+		g.nc[d] = w;
+		g.L[d] = length[d];
+		g.cell_length[d] = (bbmax - bbmin) / w;
+		double halo_len = 1 * g.cell_length[d];
+		g.halo_min[d] = bbmin - halo_len;
 		ncells *= w;
 	}
-	if (ncells > (int64_t) 0x7fffffff) return fail(c, MDGPU_ERR_CAPACITY, "too many cells");
-	c->g.ncells = ncells;
+	if (ncells > (int64_t) 0x7fffffff) {
+		err = "too many cells";
+		return MDGPU_ERR_CAPACITY;
+	}
+	g.ncells = ncells;
+	return MDGPU_OK;
+}
+
+int setup_species(int ncomp, const mdgpu_component* comps, const double* mix, double rcLJ, Species& sp,
+                  std::string& err) {
 	// Comp2Param stream entries (Comp2Param.cpp:28-115; shift6 of Component::addLJcenter,
 	// Component.cpp:47-55), one LJ centre per component
-	Species& sp = c->sp;
+	sp = Species{};
 	sp.n = ncomp;
-	double rcLJ = c->rc_lj;
 	int mixpos = 0;
 	for (int i = 0; i < ncomp; i++) {
 		const mdgpu_component& a = comps[i];
-		if (!(a.mass > 0)) return fail(c, MDGPU_ERR_ARG, "component masses must be positive");
-		c->eps[i] = a.eps;
-		c->sigma[i] = a.sigma;
-		c->do_shift[i] = a.do_shift;
+		if (!(a.mass > 0)) {
+			err = "component masses must be positive";
+			return MDGPU_ERR_ARG;
+		}
 		sp.mass[i] = a.mass;
 		double shift6i = 0.0;
 		if (a.do_shift) {
@@ -295,6 +283,62 @@ int mdgpu_create(mdgpu_ctx** out, const double length[3], double cutoff, double 
 			}
 		}
 	}
+	return MDGPU_OK;
+}
+
+PairParams pair_params(const Species& sp, double rc, double rc_lj) {
+	PairParams hp{};
+	hp.ns = sp.n;
+	hp.rc2 = rc * rc;
+	hp.rclj2 = rc_lj * rc_lj;
+	for (int k = 0; k < kMaxSpecies * kMaxSpecies; k++) {
+		hp.eps24[k] = sp.eps24[k];
+		hp.sig2[k] = sp.sig2[k];
+		hp.shift6[k] = sp.shift6[k];
+	}
+	return hp;
+}
+
+}  // namespace mdgpu
+
+using namespace mdgpu;
+
+extern "C" {
+
+int mdgpu_create(mdgpu_ctx** out, const double length[3], double cutoff, double lj_cutoff, double cells_in_cutoff,
+                 int ncomp, const mdgpu_component* comps, const double* mix, int precision, int device) {
+	if (!out || !length || !comps) return MDGPU_ERR_ARG;
+	*out = nullptr;
+	mdgpu_ctx_full* full = new (std::nothrow) mdgpu_ctx_full();
+	if (!full) return MDGPU_ERR_ARG;
+	Context* c = &full->pub.c;
+	*out = &full->pub;
+	if (ncomp < 1 || ncomp > kMaxSpecies) return fail(c, MDGPU_ERR_ARG, "ncomp must be in 1..8");
+	if (!(cutoff > 0)) return fail(c, MDGPU_ERR_ARG, "cutoff must be positive");
+	if (cells_in_cutoff != 1.0) return fail(c, MDGPU_ERR_ARG, "only cellsInCutoffRadius = 1 is supported");
+	if (precision != MDGPU_FP64 && precision != MDGPU_MIXED) return fail(c, MDGPU_ERR_ARG, "unknown precision mode");
+	if (ncomp > 1 && !mix) return fail(c, MDGPU_ERR_ARG, "mixing coefficients are required for ncomp > 1");
+	int ndev = 0;
+	cudaError_t e = cudaGetDeviceCount(&ndev);
+	if (e != cudaSuccess || ndev == 0) return fail(c, MDGPU_ERR_CUDA, "no CUDA device is available");
+	if (device < 0 || device >= ndev) return fail(c, MDGPU_ERR_ARG, "device index out of range");
+	c->device = device;
+	c->precision = precision;
+	c->rc = cutoff;
+	c->rc_lj = lj_cutoff == 0.0 ? cutoff : lj_cutoff;
+	MD_CUDA(cudaSetDevice(device));
+	{
+		int st = setup_grid(length, cutoff, cells_in_cutoff, c->g, c->err);
+		if (st) return st;
+		st = setup_species(ncomp, comps, mix, c->rc_lj, c->sp, c->err);
+		if (st) return st;
+	}
+	const int64_t ncells = c->g.ncells;
+	for (int i = 0; i < ncomp; i++) {
+		c->eps[i] = comps[i].eps;
+		c->sigma[i] = comps[i].sigma;
+		c->do_shift[i] = comps[i].do_shift;
+	}
 	MD_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
 	MD_CUDA(cudaMalloc(&c->cell_count, sizeof(int32_t) * ncells));
 	MD_CUDA(cudaMalloc(&c->cell_start, sizeof(int32_t) * (ncells + 1)));
@@ -306,15 +350,7 @@ int mdgpu_create(mdgpu_ctx** out, const double length[3], double cutoff, double 
 	MD_CUDA(cudaMemset(c->status, 0, sizeof(int)));
 	MD_CUDA(cudaMallocHost(&c->h_scalars, sizeof(double) * 64));
 	MD_CUDA(cudaMallocHost(&c->h_status, sizeof(int)));
-	PairParams hp{};
-	hp.ns = ncomp;
-	hp.rc2 = c->rc * c->rc;
-	hp.rclj2 = c->rc_lj * c->rc_lj;
-	for (int k = 0; k < kMaxSpecies * kMaxSpecies; k++) {
-		hp.eps24[k] = sp.eps24[k];
-		hp.sig2[k] = sp.sig2[k];
-		hp.shift6[k] = sp.shift6[k];
-	}
+	PairParams hp = pair_params(c->sp, c->rc, c->rc_lj);
 	MD_CUDA(cudaMalloc(&c->d_pp, sizeof(PairParams)));
 	MD_CUDA(cudaMemcpy(c->d_pp, &hp, sizeof(PairParams), cudaMemcpyHostToDevice));
 	c->err.clear();

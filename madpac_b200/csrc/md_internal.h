@@ -117,6 +117,13 @@ cudaError_t launch_adjoint(Context* c, const double* gfx, const double* gfy, con
                            double* oy, double* oz, double* pgrad, double* pout);
 cudaError_t launch_step_record(Context* c, double* dst);        // dst[0..3] <- step scalars
 
+// Set-up shared by the single-box and the batched contexts (api.cu): LinkedCells geometry of the
+// box [0, L), the Comp2Param table, and its device form. Return an MDGPU_* code, message in err.
+int setup_grid(const double length[3], double cutoff, double cells_in_cutoff, Grid& g, std::string& err);
+int setup_species(int ncomp, const mdgpu_component* comps, const double* mix, double rc_lj, Species& sp,
+                  std::string& err);
+PairParams pair_params(const Species& sp, double rc, double rc_lj);
+
 // Timing brackets around a group of launches (0 = binning, 1 = pairs, 2 = integration).
 void prof_begin(Context* c, int group);
 void prof_end(Context* c, int group, int launches);

@@ -42,7 +42,7 @@ template <bool kMixed>
 __device__ PairSums gather_pairs(int64_t i, const double* __restrict__ rx, const double* __restrict__ ry,
                                  const double* __restrict__ rz, const int32_t* __restrict__ cid,
                                  const int32_t* __restrict__ start, const Grid& g, const double* params, int ns,
-                                 double rc2, double rclj2) {
+                                 double rc2, double rclj2, int32_t coff = 0) {
 	constexpr int KK = kMaxSpecies * kMaxSpecies;
 	PairSums s{{0.0, 0.0, 0.0}, 0.0, 0.0, 0.0, false};
 	const double xi = rx[i], yi = ry[i], zi = rz[i];
@@ -84,7 +84,7 @@ __device__ PairSums gather_pairs(int64_t i, const double* __restrict__ rx, const
 					x -= g.nc[0];
 					sx = g.L[0];
 				}
-				const int nb = (z * g.nc[1] + y) * g.nc[0] + x;
+				const int nb = coff + (z * g.nc[1] + y) * g.nc[0] + x;
 				const bool shifted = (sx != 0.0) || (sy != 0.0) || (sz != 0.0);
 				const int j0 = start[nb], j1 = start[nb + 1];
 				for (int j = j0; j < j1; j++) {

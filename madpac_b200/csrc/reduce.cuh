@@ -10,8 +10,8 @@ __device__ __forceinline__ double warp_sum(double v) {
 	return v;
 }
 
-// Block-wide sum of three doubles into partials[blockIdx.x*4 + k] (blockDim.x <= kReduceBlock).
-__device__ __forceinline__ void block_sum3(double a, double b, double c, double* partials) {
+// Block-wide sum of three doubles into partials[slot*4 + k] (blockDim.x <= kReduceBlock).
+__device__ __forceinline__ void block_sum3_at(double a, double b, double c, double* partials, int64_t slot) {
 	__shared__ double sh[3][kReduceBlock / 32];
 	a = warp_sum(a);
 	b = warp_sum(b);
@@ -30,11 +30,15 @@ __device__ __forceinline__ void block_sum3(double a, double b, double c, double*
 			s1 += sh[1][w];
 			s2 += sh[2][w];
 		}
-		partials[blockIdx.x * 4 + 0] = s0;
-		partials[blockIdx.x * 4 + 1] = s1;
-		partials[blockIdx.x * 4 + 2] = s2;
-		partials[blockIdx.x * 4 + 3] = 0.0;
+		partials[slot * 4 + 0] = s0;
+		partials[slot * 4 + 1] = s1;
+		partials[slot * 4 + 2] = s2;
+		partials[slot * 4 + 3] = 0.0;
 	}
+}
+
+__device__ __forceinline__ void block_sum3(double a, double b, double c, double* partials) {
+	block_sum3_at(a, b, c, partials, blockIdx.x);
 }
 
 }  // namespace mdgpu

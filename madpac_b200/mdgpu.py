@@ -70,6 +70,18 @@ SIGNATURES = {
     "mdgpu_synchronize": (_I, [_VP]),
     "mdgpu_forces_noalloc": (_I, [_I, _VP, _I64, _VP, _VP, _VP, _D, _D, _I, _VP, _VP, _I, _VP, _VP, _VP,
                                   ctypes.c_char_p, _I]),
+    "mdgpu_batch_create": (_I, [ctypes.POINTER(_VP), _I32, _VP, _VP, _D, _D, _D, _I, _VP, _VP, _I, _I]),
+    "mdgpu_batch_destroy": (_I, [_VP]),
+    "mdgpu_batch_last_error": (ctypes.c_char_p, [_VP]),
+    "mdgpu_batch_set_particles": (_I, [_VP, _I64, _VP, _VP, _VP, _VP]),
+    "mdgpu_batch_get_particles": (_I, [_VP, _I64, _VP, _VP, _VP, _VP, _VP]),
+    "mdgpu_batch_prepare": (_I, [_VP, _VP]),
+    "mdgpu_batch_run": (_I, [_VP, _I32, _D, _VP]),
+    "mdgpu_batch_set_tiles": (_I, [_VP, _I32, _I32, _I32]),
+    "mdgpu_batch_get_tiles": (_I, [_VP, _VP]),
+    "mdgpu_batch_autotune": (_I, [_VP, _D, _I32, _VP, _VP]),
+    "mdgpu_batch_last_run_ms": (_I, [_VP, _VP]),
+    "mdgpu_batch_set_barrier_timeout": (_I, [_VP, _I64]),
 }
 
 _lib = None
@@ -149,6 +161,127 @@ def forces_noalloc(d_r: int, d_cid: int, d_F: int, n: int, length, cutoff: float
     if st != 0:
         raise MdgpuError(st, err.value.decode())
     return u.value, w.value
+
+
+def _components(components):
+    comps = (_MdComponent * len(components))()
+    for k, c in enumerate(components):
+        comps[k].eps, comps[k].sigma, comps[k].mass = float(c.eps), float(c.sigma), float(c.mass)
+        comps[k].do_shift = 1 if c.do_shift else 0
+    return comps
+
+
+class Batch:
+    """An ensemble of independent periodic boxes (no reference counterpart: the reference runs one
+    Simulation per box). All boxes share cutoffs, components and precision; every step of every box
+    is one persistent kernel launch, replayed from a captured CUDA graph. Molecule arrays are
+    box-major (box 0's molecules, then box 1's, ...)."""
+
+    TILE_CANDIDATES = [(cap, ctas, dyn) for cap in (32, 64) for ctas in (1, 2) for dyn in (0, 1)]
+
+    def __init__(self, lengths, counts, cutoffRadius: float, components, mixcoeff=None,
+                 LJCutoffRadius: float = 0.0, precision: int = FP64, device: int = 0):
+        self.lib = load_library()
+        self._lengths = _c64(lengths).reshape(-1, 3)
+        self.counts = _c64(counts, np.int64).reshape(-1)
+        if self._lengths.shape[0] != self.counts.shape[0]:
+            raise ValueError("one length triple per box")
+        self.nboxes = int(self.counts.shape[0])
+        self.ntotal = int(self.counts.sum())
+        self.offsets = np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int64)
+        comps = _components(components)
+        mix = None if mixcoeff is None else _c64(mixcoeff).reshape(-1)
+        if mix is not None and mix.size == 0:
+            mix = None
+        h = ctypes.c_void_p()
+        st = self.lib.mdgpu_batch_create(ctypes.byref(h), self.nboxes, _ptr(self._lengths), _ptr(self.counts),
+                                         float(cutoffRadius), float(LJCutoffRadius), 1.0, len(components),
+                                         ctypes.cast(comps, ctypes.c_void_p), _ptr(mix), int(precision), int(device))
+        self.h = h.value
+        if st != 0:
+            msg = self.lib.mdgpu_batch_last_error(self.h).decode() if self.h else ""
+            if self.h:
+                self.lib.mdgpu_batch_destroy(self.h)
+            self.h = None
+            raise MdgpuError(st, msg)
+
+    @classmethod
+    def from_systems(cls, systems, precision: int = FP64, device: int = 0) -> "Batch":
+        s0 = systems[0]
+        b = cls([s.length for s in systems], [s.n for s in systems], s0.cutoff, s0.components, s0.mix, s0.lj_cutoff,
+                precision, device)
+        b.setParticles(np.concatenate([s.ids for s in systems]), np.concatenate([s.cid for s in systems]),
+                       np.concatenate([s.r for s in systems]), np.concatenate([s.v for s in systems]))
+        return b
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.mdgpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int) -> None:
+        if st != 0:
+            raise MdgpuError(st, self.lib.mdgpu_batch_last_error(self.h).decode())
+
+    def setParticles(self, ids, cid, r, v) -> None:
+        n = self.ntotal
+        self._check(self.lib.mdgpu_batch_set_particles(self.h, n, _ptr(_c64(ids, np.uint64)), _ptr(_c64(cid, np.int32)),
+                                                       _ptr(_c64(r, shape=(n, 3))), _ptr(_c64(v, shape=(n, 3)))))
+
+    def getParticles(self) -> Dict[str, np.ndarray]:
+        n = self.ntotal
+        ids = np.zeros(n, dtype=np.uint64)
+        cid = np.zeros(n, dtype=np.int32)
+        r, v, F = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros((n, 3))
+        self._check(self.lib.mdgpu_batch_get_particles(self.h, n, _ptr(ids), _ptr(cid), _ptr(r), _ptr(v), _ptr(F)))
+        return dict(id=ids, cid=cid, r=r, v=v, F=F)
+
+    def box(self, state: Dict[str, np.ndarray], k: int) -> Dict[str, np.ndarray]:
+        """The slice of a getParticles() result that belongs to box k."""
+        a, b = self.offsets[k], self.offsets[k + 1]
+        return {key: val[a:b] for key, val in state.items()}
+
+    def prepare(self) -> np.ndarray:
+        """Initial binning and forces of every box; returns (nboxes, 4) {Upot, virial, sum m v^2, pairs}."""
+        out = np.zeros((self.nboxes, 4))
+        self._check(self.lib.mdgpu_batch_prepare(self.h, _ptr(out)))
+        return out
+
+    def run(self, nsteps: int, dt: float, record: bool = True) -> Optional[np.ndarray]:
+        """nsteps NVE steps of every box; returns (nsteps, nboxes, 4) step records."""
+        out = np.zeros((nsteps, self.nboxes, 4)) if record else None
+        self._check(self.lib.mdgpu_batch_run(self.h, int(nsteps), float(dt), _ptr(out)))
+        return out
+
+    def setTiles(self, list_cap: int, ctas_per_sm: int, dynamic: int) -> None:
+        self._check(self.lib.mdgpu_batch_set_tiles(self.h, int(list_cap), int(ctas_per_sm), int(dynamic)))
+
+    def tiles(self):
+        t = np.zeros(3, dtype=np.int32)
+        self._check(self.lib.mdgpu_batch_get_tiles(self.h, _ptr(t)))
+        return tuple(int(x) for x in t)
+
+    def autotune(self, dt: float, trial_steps: int = 5):
+        """Times every tile shape from the current state (restored afterwards) and keeps the fastest.
+        Returns (best (list_cap, ctas_per_sm, dynamic), {candidate: ms per step})."""
+        best = np.zeros(3, dtype=np.int32)
+        ms = np.zeros(len(self.TILE_CANDIDATES))
+        self._check(self.lib.mdgpu_batch_autotune(self.h, float(dt), int(trial_steps), _ptr(best), _ptr(ms)))
+        return tuple(int(x) for x in best), dict(zip(self.TILE_CANDIDATES, ms.tolist()))
+
+    def lastRunMs(self) -> float:
+        ms = ctypes.c_double()
+        self._check(self.lib.mdgpu_batch_last_run_ms(self.h, ctypes.byref(ms)))
+        return ms.value
+
+    def setBarrierTimeout(self, ns: int) -> None:
+        self._check(self.lib.mdgpu_batch_set_barrier_timeout(self.h, int(ns)))
 
 
 class LinkedCells:
