@@ -45,6 +45,8 @@ def parse():
                     help="FCC unit cells per box edge (64 -> 1,048,576 molecules; smaller for profiling)")
     ap.add_argument("--pair-kernel", choices=["brick", "gather"], default="brick")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--skin", type=float, default=0.0,
+                    help="Verlet skin of the step (0: cells and candidates rebuilt every step)")
     ap.add_argument("--workload", choices=["c2", "batched"], default="c2",
                     help="c2: the 1M-molecule box (headline); batched: the 512-box ensemble")
     ap.add_argument("--boxes", type=int, default=512, help="boxes of the batched ensemble")
@@ -291,6 +293,7 @@ def run_ours(args, dist: Dist):
     lc.setPairKernel(kernel)
     lc.update()
     lc.traversePairs()
+    lc.setSkin(args.skin)
     stream = torch.cuda.ExternalStream(lc.stream())
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{dist.local}")
 
@@ -359,6 +362,7 @@ def run_ours(args, dist: Dist):
         lc2.setPairKernel(kernel)
         lc2.update()
         lc2.traversePairs()
+        lc2.setSkin(args.skin)
         ref_lc = lc2 if other == M.FP64 else None
         s2, p2, _, _ = time_device_resident(M, lc2, system, args.steps, args.warmup, flush,
                                             torch.cuda.ExternalStream(lc2.stream()))

@@ -170,6 +170,19 @@ int mdgpu_forces_noalloc(int device, void* stream, int64_t n, const double* d_r,
                          const mdgpu_component* comps, const double* mix, int precision, double* d_F,
                          double* upot, double* virial, char* errbuf, int errlen);
 
+/* Verlet-skin mode of mdgpu_step / mdgpu_run / mdgpu_run_async (skin > 0; 0 = off, the default).
+ * No reference counterpart: the reference rebuilds its cells every step (LinkedCells::update).
+ * With a skin, the binning (on cells of edge >= cutoff + skin) and the candidate search run only
+ * in steps where some molecule has moved more than skin/2 since the last build, decided on the
+ * device; the other steps evaluate each molecule's recorded candidates. Every pair within the
+ * cutoff is still evaluated with the exact test (r^2 < rc^2), so forces, Upot and virial are those
+ * of the per-step traversal up to summation order. Positions are wrapped into [0, L) at each build
+ * and on output (mdgpu_get_particles). After such steps the cell structure is not the reference's:
+ * call mdgpu_update before mdgpu_traverse_pairs, mdgpu_get_cell_index or mdgpu_adjoint. */
+int mdgpu_set_skin(mdgpu_ctx* ctx, double skin);
+/* Number of list builds of the Verlet-skin mode so far (synchronises the context's stream). */
+int mdgpu_skin_builds(mdgpu_ctx* ctx, int64_t* builds);
+
 /* ---- batched ensemble of independent boxes ------------------------------------------------
  * No reference counterpart: in MarDyn every box is its own Simulation with its own LinkedCells
  * (Simulation.cpp:907-1308), run one after the other. A batch holds nboxes independent periodic

@@ -42,6 +42,24 @@ __global__ void k_store_aos(int64_t n, const double* __restrict__ x, const doubl
 	aos[3 * u + 2] = z[s];
 }
 
+// positions -> caller order with the periodic wrap r<0 -> r+L, r>=L -> r-L
+__global__ void k_store_pos(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                            const double* __restrict__ z, const int32_t* __restrict__ uidx, Grid g,
+                            double* __restrict__ aos) {
+	int64_t s = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= n) return;
+	int64_t u = uidx[s];
+	const double r[3] = {x[s], y[s], z[s]};
+	for (int d = 0; d < 3; d++) {
+		double w = r[d];
+		if (w < 0.0)
+			w = __dadd_rn(w, g.L[d]);
+		else if (w >= g.L[d])
+			w = __dsub_rn(w, g.L[d]);
+		aos[3 * u + d] = w;
+	}
+}
+
 template <typename T>
 __global__ void k_store_scalar(int64_t n, const T* __restrict__ x, const int32_t* __restrict__ uidx, T* __restrict__ out) {
 	int64_t s = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
@@ -377,6 +395,11 @@ int mdgpu_destroy(mdgpu_ctx* ctx) {
 	cudaFree(c->status);
 	cudaFree(c->d_pp);
 	cudaFree(c->adj);
+	cudaFree(c->nbr);
+	cudaFree(c->nbr_count);
+	cudaFree(c->r_ref);
+	cudaFree(c->rebuild);
+	cudaFree(c->builds);
 	cudaFree(full->x.stage.ptr);
 	if (c->h_scalars) cudaFreeHost(c->h_scalars);
 	if (c->h_status) cudaFreeHost(c->h_status);
@@ -419,6 +442,27 @@ int mdgpu_set_particles(mdgpu_ctx* ctx, int64_t n, const uint64_t* id, const int
 	for (int64_t i = 0; i < n; i++) {
 		if (cid[i] < 0 || cid[i] >= c->sp.n) return fail(c, MDGPU_ERR_ARG, "component id out of range");
 		x->species_count[cid[i]]++;
+	}
+	// largest cell occupancy (the reference's cell formula after the periodic wrap): sizes the
+	// neighbour lists of the Verlet-skin mode
+	{
+		std::vector<int32_t> occ((size_t) c->g.ncells, 0);
+		int mx = 0;
+		for (int64_t i = 0; i < n; i++) {
+			int64_t cell = 0;
+			for (int d = 2; d >= 0; d--) {
+				double x = r[3 * i + d];
+				if (x < 0.0)
+					x += c->g.L[d];
+				else if (x >= c->g.L[d])
+					x -= c->g.L[d];
+				int cc = (int) std::floor((x - c->g.halo_min[d]) / c->g.cell_length[d]) - 1;
+				cc = cc < 0 ? 0 : (cc >= c->g.nc[d] ? c->g.nc[d] - 1 : cc);
+				cell = cell * c->g.nc[d] + cc;
+			}
+			mx = std::max(mx, ++occ[(size_t) cell]);
+		}
+		c->max_occ = mx;
 	}
 	MD_CUDA(cudaSetDevice(c->device));
 	MD_CUDA(cudaStreamSynchronize(c->stream));
@@ -465,6 +509,7 @@ int mdgpu_set_particles(mdgpu_ctx* ctx, int64_t n, const uint64_t* id, const int
 	MD_CUDA(cudaGetLastError());
 	MD_CUDA(cudaStreamSynchronize(c->stream));
 	c->cells_valid = false;
+	c->lists_valid = false;
 	return MDGPU_OK;
 }
 
@@ -504,7 +549,10 @@ int mdgpu_get_particles(mdgpu_ctx* ctx, int64_t n, uint64_t* id, int32_t* cid, d
 	} sets[3] = {{r, c->p.rx, c->p.ry, c->p.rz}, {v, c->p.vx, c->p.vy, c->p.vz}, {F, c->p.fx, c->p.fy, c->p.fz}};
 	for (auto& s : sets) {
 		if (!s.out) continue;
-		k_store_aos<<<blocks_for(n), kThreads, 0, c->stream>>>(n, s.x, s.y, s.z, c->p.uidx, aos);
+		if (s.out == r)   // positions in [0, L) as after LinkedCells::update (the skin mode defers the wrap)
+			k_store_pos<<<blocks_for(n), kThreads, 0, c->stream>>>(n, s.x, s.y, s.z, c->p.uidx, c->g, aos);
+		else
+			k_store_aos<<<blocks_for(n), kThreads, 0, c->stream>>>(n, s.x, s.y, s.z, c->p.uidx, aos);
 		MD_CUDA(cudaMemcpyAsync(s.out, aos, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream));
 		MD_CUDA(cudaStreamSynchronize(c->stream));
 	}
@@ -544,6 +592,7 @@ int mdgpu_update(mdgpu_ctx* ctx) {
 	if (c->n == 0) return fail(c, MDGPU_ERR_STATE, "no molecules loaded");
 	MD_CUDA(cudaSetDevice(c->device));
 	MD_CUDA(launch_bin(c, true));
+	c->lists_valid = false;
 	int st = check_status(c);
 	c->cells_valid = (st == MDGPU_OK);
 	return st;
@@ -638,19 +687,107 @@ int mdgpu_far_field_correction(mdgpu_ctx* ctx, double* upot_corr, double* virial
 	return MDGPU_OK;
 }
 
+namespace {
+// Verlet-skin buffers sized for the loaded molecules; the first step after a change of the sort
+// order builds the lists.
+int skin_prepare(Context* c) {
+	const int64_t n = c->n;
+	const double rl = c->rc + c->skin;
+	const double cell_vol = c->g.cell_length[0] * c->g.cell_length[1] * c->g.cell_length[2];
+	const double rho_max = (c->max_occ > 0 ? c->max_occ : 1) / cell_vol;
+	int cap = (int) std::ceil(1.25 * 4.18879020478639 * rl * rl * rl * rho_max) + 32;
+	cap = (cap + 31) & ~31;
+	cap = std::min(cap, 65504);
+	if (c->list_n != n || c->list_cap < cap) {
+		cudaFree(c->nbr);
+		cudaFree(c->nbr_count);
+		cudaFree(c->r_ref);
+		c->nbr = nullptr;
+		c->nbr_count = nullptr;
+		c->r_ref = nullptr;
+		c->list_n = 0;
+		MD_CUDA(cudaMalloc(&c->nbr, sizeof(unsigned short) * (size_t) cap * n));
+		MD_CUDA(cudaMalloc(&c->nbr_count, sizeof(unsigned short) * n));
+		MD_CUDA(cudaMalloc(&c->r_ref, sizeof(double) * 3 * n));
+		c->list_n = n;
+		c->list_cap = cap;
+		c->lists_valid = false;
+	}
+	if (!c->rebuild) {
+		MD_CUDA(cudaMalloc(&c->rebuild, sizeof(int)));
+		MD_CUDA(cudaMalloc(&c->builds, sizeof(unsigned long long)));
+		MD_CUDA(cudaMemsetAsync(c->builds, 0, sizeof(unsigned long long), c->stream));
+	}
+	if (!c->lists_valid) {
+		MD_CUDA(cudaMemsetAsync(c->rebuild, 0xff, sizeof(int), c->stream));
+		c->lists_valid = true;
+	}
+	return MDGPU_OK;
+}
+
+// One Simulation::simulateStep hot path, its record written to dst (device).
+int enqueue_one(Context* c, double dt, double vcorr, double* dst) {
+	if (c->skin > 0.0) {
+		int st = skin_prepare(c);
+		if (st) return st;
+		MD_CUDA(launch_leapfrog_pre(c, dt, vcorr, true));
+		MD_CUDA(launch_bin(c, false, c->rebuild, &c->gs));
+		MD_CUDA(launch_pairs_skin(c));
+		MD_CUDA(launch_leapfrog_post(c, 0.5 * dt, true));
+	} else {
+		MD_CUDA(launch_leapfrog_pre(c, dt, vcorr));
+		MD_CUDA(launch_bin(c, false));
+		c->lists_valid = false;
+		MD_CUDA(launch_pairs(c));
+		MD_CUDA(launch_leapfrog_post(c, 0.5 * dt));
+	}
+	MD_CUDA(launch_step_record(c, dst));
+	return MDGPU_OK;
+}
+}  // namespace
+
+int mdgpu_set_skin(mdgpu_ctx* ctx, double skin) {
+	if (!ctx) return MDGPU_ERR_ARG;
+	Context* c = &ctx->c;
+	if (!(skin >= 0.0) || !(skin < c->rc)) return fail(c, MDGPU_ERR_ARG, "skin must be in [0, cutoff)");
+	if (skin > 0.0) {
+		// the lists are built over cells of edge >= cutoff + skin (their own grid), so that every
+		// molecule that can come within the cutoff before the next build is in the 27 cells around
+		Grid gs{};
+		std::string err;
+		const double length[3] = {c->g.L[0], c->g.L[1], c->g.L[2]};
+		int st = setup_grid(length, c->rc + skin, 1.0, gs, err);
+		if (st) return fail(c, st, "cutoff + skin: " + err);
+		c->gs = gs;
+	}
+	c->skin = skin;
+	c->lists_valid = false;
+	return MDGPU_OK;
+}
+
+int mdgpu_skin_builds(mdgpu_ctx* ctx, int64_t* builds) {
+	if (!ctx || !builds) return MDGPU_ERR_ARG;
+	Context* c = &ctx->c;
+	*builds = 0;
+	if (!c->builds) return MDGPU_OK;
+	unsigned long long v = 0;
+	MD_CUDA(cudaSetDevice(c->device));
+	MD_CUDA(cudaMemcpyAsync(&v, c->builds, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
+	MD_CUDA(cudaStreamSynchronize(c->stream));
+	*builds = (int64_t) v;
+	return MDGPU_OK;
+}
+
 int mdgpu_step(mdgpu_ctx* ctx, double dt, double vcorr, double* out4) {
 	if (!ctx) return MDGPU_ERR_ARG;
 	Context* c = &ctx->c;
 	if (c->n == 0) return fail(c, MDGPU_ERR_STATE, "no molecules loaded");
 	MD_CUDA(cudaSetDevice(c->device));
-	MD_CUDA(launch_leapfrog_pre(c, dt, vcorr));
-	MD_CUDA(launch_bin(c, false));
-	MD_CUDA(launch_pairs(c));
-	MD_CUDA(launch_leapfrog_post(c, 0.5 * dt));
-	MD_CUDA(launch_step_record(c, c->scalars + 8));
+	int st = enqueue_one(c, dt, vcorr, c->scalars + 8);
+	if (st) return st;
 	MD_CUDA(cudaMemcpyAsync(c->h_scalars + 8, c->scalars + 8, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->stream));
-	int st = check_status(c);
-	c->cells_valid = (st == MDGPU_OK);
+	st = check_status(c);
+	c->cells_valid = (st == MDGPU_OK) && c->skin == 0.0;
 	if (st) return st;
 	if (out4)
 		for (int k = 0; k < 4; k++) out4[k] = c->h_scalars[8 + k];
@@ -676,11 +813,8 @@ int enqueue_steps(Context* c, int32_t nsteps, double dt) {
 		c->steps_cap = cap;
 	}
 	for (int k = 0; k < nsteps; k++) {
-		MD_CUDA(launch_leapfrog_pre(c, dt, 1.0));
-		MD_CUDA(launch_bin(c, false));
-		MD_CUDA(launch_pairs(c));
-		MD_CUDA(launch_leapfrog_post(c, 0.5 * dt));
-		MD_CUDA(launch_step_record(c, c->steps_out + 4 * c->steps_written));
+		int st = enqueue_one(c, dt, 1.0, c->steps_out + 4 * c->steps_written);
+		if (st) return st;
 		c->steps_written++;
 	}
 	return MDGPU_OK;
@@ -699,7 +833,7 @@ int mdgpu_run_async(mdgpu_ctx* ctx, int32_t nsteps, double dt) {
 	if (!ctx) return MDGPU_ERR_ARG;
 	Context* c = &ctx->c;
 	int st = enqueue_steps(c, nsteps, dt);
-	c->cells_valid = (st == MDGPU_OK);
+	c->cells_valid = (st == MDGPU_OK) && c->skin == 0.0;
 	return st;
 }
 

@@ -23,7 +23,8 @@ constexpr int kScanBlock = 1024;   // elements per scan block (256 threads x 4)
 
 __global__ void k_bin_cells(int64_t n, double* __restrict__ rx, double* __restrict__ ry,
                             double* __restrict__ rz, Grid g, int32_t* __restrict__ cell,
-                            int32_t* __restrict__ rank, int32_t* __restrict__ count, int* status) {
+                            int32_t* __restrict__ rank, int32_t* __restrict__ count, int* status, const int* gate) {
+	if (gate && *gate == 0) return;
 	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	double r[3] = {rx[i], ry[i], rz[i]};
@@ -57,7 +58,8 @@ __global__ void k_bin_cells(int64_t n, double* __restrict__ rx, double* __restri
 
 // Block-local exclusive scan of kScanBlock counts; block totals go to sums.
 __global__ void k_scan_local(int64_t n, const int32_t* __restrict__ in, int32_t* __restrict__ out,
-                             int32_t* __restrict__ sums) {
+                             int32_t* __restrict__ sums, const int* gate) {
+	if (gate && *gate == 0) return;
 	__shared__ int32_t warp_tot[8];
 	int64_t base = (int64_t) blockIdx.x * kScanBlock + threadIdx.x * 4;
 	int32_t v[4];
@@ -92,7 +94,8 @@ __global__ void k_scan_local(int64_t n, const int32_t* __restrict__ in, int32_t*
 }
 
 // Single block: exclusive scan of the block totals, total appended at sums[nb].
-__global__ void k_scan_sums(int64_t nb, int32_t* sums) {
+__global__ void k_scan_sums(int64_t nb, int32_t* sums, const int* gate) {
+	if (gate && *gate == 0) return;
 	__shared__ int32_t carry;
 	if (threadIdx.x == 0) carry = 0;
 	__syncthreads();
@@ -127,14 +130,17 @@ __global__ void k_scan_sums(int64_t nb, int32_t* sums) {
 	if (threadIdx.x == 0) sums[nb] = carry;
 }
 
-__global__ void k_scan_add(int64_t n, int32_t* __restrict__ out, const int32_t* __restrict__ sums, int64_t nb) {
+__global__ void k_scan_add(int64_t n, int32_t* __restrict__ out, const int32_t* __restrict__ sums, int64_t nb,
+                           const int* gate) {
+	if (gate && *gate == 0) return;
 	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n) out[i] += sums[i / kScanBlock];
 	if (i == 0) out[n] = sums[nb];
 }
 
 __global__ void k_scatter(int64_t n, const int32_t* __restrict__ cell, const int32_t* __restrict__ rank,
-                          const int32_t* __restrict__ start, int32_t* __restrict__ perm) {
+                          const int32_t* __restrict__ start, int32_t* __restrict__ perm, const int* gate) {
+	if (gate && *gate == 0) return;
 	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n) perm[start[cell[i]] + rank[i]] = (int32_t) i;
 }
@@ -145,7 +151,9 @@ __device__ __forceinline__ bool key_less(uint64_t ka, int32_t sa, uint64_t kb, i
 
 // One warp per cell: order the cell's molecules by (id, previous slot) and gather all fields.
 __global__ void k_cell_sort(int64_t ncells, const int32_t* __restrict__ start, const int32_t* __restrict__ perm,
-                            Particles src, Particles dst, int32_t* __restrict__ cell_out, bool with_forces) {
+                            Particles src, Particles dst, int32_t* __restrict__ cell_out, bool with_forces,
+                            const int* gate) {
+	if (gate && *gate == 0) return;
 	int64_t c = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	int lane = threadIdx.x & 31;
 	if (c >= ncells) return;
@@ -192,36 +200,61 @@ __global__ void k_cell_sort(int64_t ncells, const int32_t* __restrict__ start, c
 	}
 }
 
+// Gated mode: the sorted arrays (and their cells) back into the current buffer.
+__global__ void k_copy_back(int64_t n, Particles src, Particles dst, const int32_t* __restrict__ cell_src,
+                            int32_t* __restrict__ cell_dst, const int* gate) {
+	if (*gate == 0) return;
+	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	dst.rx[i] = src.rx[i];
+	dst.ry[i] = src.ry[i];
+	dst.rz[i] = src.rz[i];
+	dst.vx[i] = src.vx[i];
+	dst.vy[i] = src.vy[i];
+	dst.vz[i] = src.vz[i];
+	dst.id[i] = src.id[i];
+	dst.cid[i] = src.cid[i];
+	dst.uidx[i] = src.uidx[i];
+	cell_dst[i] = cell_src[i];
+}
+
 inline unsigned blocks_for(int64_t n, int t) { return (unsigned) ((n + t - 1) / t); }
 
 }  // namespace
 
-cudaError_t launch_bin(Context* c, bool permute_forces) {
-	const int64_t n = c->n, nc = c->g.ncells;
+cudaError_t launch_bin(Context* c, bool permute_forces, const int* gate, const Grid* grid) {
+	const Grid& g = grid ? *grid : c->g;
+	const int64_t n = c->n, nc = g.ncells;
 	cudaStream_t s = c->stream;
 	prof_begin(c, 0);
 	cudaMemsetAsync(c->cell_count, 0, sizeof(int32_t) * nc, s);
-	if (n > 0) k_bin_cells<<<blocks_for(n, 256), 256, 0, s>>>(n, c->p.rx, c->p.ry, c->p.rz, c->g, c->cell, c->rank,
-	                                                          c->cell_count, c->status);
+	if (n > 0) k_bin_cells<<<blocks_for(n, 256), 256, 0, s>>>(n, c->p.rx, c->p.ry, c->p.rz, g, c->cell, c->rank,
+	                                                          c->cell_count, c->status, gate);
 	int64_t nb = (nc + kScanBlock - 1) / kScanBlock;
-	k_scan_local<<<(unsigned) nb, 256, 0, s>>>(nc, c->cell_count, c->cell_start, c->scan_tmp);
-	k_scan_sums<<<1, 1024, 0, s>>>(nb, c->scan_tmp);
-	k_scan_add<<<blocks_for(nc, 256), 256, 0, s>>>(nc, c->cell_start, c->scan_tmp, nb);
+	k_scan_local<<<(unsigned) nb, 256, 0, s>>>(nc, c->cell_count, c->cell_start, c->scan_tmp, gate);
+	k_scan_sums<<<1, 1024, 0, s>>>(nb, c->scan_tmp, gate);
+	k_scan_add<<<blocks_for(nc, 256), 256, 0, s>>>(nc, c->cell_start, c->scan_tmp, nb, gate);
 	int launches = 4;
 	if (n > 0) {
-		k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(n, c->cell, c->rank, c->cell_start, c->perm);
+		k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(n, c->cell, c->rank, c->cell_start, c->perm, gate);
 		k_cell_sort<<<blocks_for(nc * 32, 256), 256, 0, s>>>(nc, c->cell_start, c->perm, c->p, c->q, c->rank,
-		                                                     permute_forces);
+		                                                     permute_forces, gate);
 		launches += 2;
+		if (gate) {
+			k_copy_back<<<blocks_for(n, 256), 256, 0, s>>>(n, c->q, c->p, c->rank, c->cell, gate);
+			launches += 1;
+		}
 	}
 	cudaError_t e = cudaGetLastError();
-	// the sorted cell of each particle was written into `rank`; swap buffers
-	Particles t = c->p;
-	c->p = c->q;
-	c->q = t;
-	int32_t* tc = c->cell;
-	c->cell = c->rank;
-	c->rank = tc;
+	if (!gate) {
+		// the sorted cell of each particle was written into `rank`; swap buffers
+		Particles t = c->p;
+		c->p = c->q;
+		c->q = t;
+		int32_t* tc = c->cell;
+		c->cell = c->rank;
+		c->rank = tc;
+	}
 	prof_end(c, 0, launches);
 	return e;
 }

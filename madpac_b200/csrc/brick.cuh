@@ -10,9 +10,11 @@
 //           so the 3 cells of each neighbour row of a cell form one contiguous slot range.
 //           Positions are stored in a local frame
 //           X = x + shift - c_brick + C, C = 1.5 * 2^k with all X of the region in [2^k, 2^(k+1)]:
-//           differences of their float "hi" parts are exact (Sterbenz), and a float "lo" part holds
-//           X - hi, so (hi_i - hi_j) + (lo_i - lo_j) is X_i - X_j to float rounding. The FP64 mode
-//           also stages the double image position x + shift.
+//           differences of their float "hi" parts are exact (Sterbenz), and the "lo" part X - hi
+//           is kept as 9-bit fixed point (steps of 1/512 ulp of the binade) in the 4th word of the
+//           same float4, with the component id: (hi_i - hi_j) + (lo_i - lo_j) is X_i - X_j to
+//           about 2e-9 absolute, one 16-byte shared load per candidate. The FP64 mode also stages
+//           the double image position x + shift.
 //  filter   Each lane holds one molecule i; every pair of consecutive staged molecules j of the 9
 //           neighbour rows is broadcast to all lanes, which test r^2 in packed half precision
 //           against rc^2 plus a margin covering the rounding, and append hits to their own list.
@@ -63,6 +65,9 @@ struct Box {
 	int32_t coff;
 	float frame_c[3];     // C per dimension
 	float rc2_h;          // rc^2 + margin covering half-precision rounding (packed filter)
+	float lo_step[3];     // fixed-point step of the lo parts: 2^(k-32) for the binade [2^k, 2^(k+1))
+	float lo_inv[3];      // 1 / lo_step
+	float lo_c[3];        // -(2^23 + 256) * lo_step (decoding constant)
 };
 
 struct SmemLayout {
@@ -77,17 +82,18 @@ struct __align__(16) HalfPair {
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
-__host__ __device__ inline SmemLayout layout(int s_cap, bool fp64, int list_cap) {
+// list_cap: per-lane candidate list depth of the filter (0 for the list kernel, which reads its
+// lists from global memory); half: whether the packed half-precision copy is staged.
+__host__ __device__ inline SmemLayout layout(int s_cap, bool fp64, int list_cap, bool half = true) {
 	SmemLayout L;
 	size_t o = 0;
 	L.hi = o;
 	o = align16(o + sizeof(float4) * s_cap);
 	L.lo = o;
-	if (!fp64) o = align16(o + sizeof(float4) * s_cap);
 	L.img = o;
 	if (fp64) o = align16(o + sizeof(double) * 3 * s_cap);
 	L.h16 = o;
-	o = align16(o + sizeof(HalfPair) * (s_cap / 2 + 20));  // 32-slot blocks may read past the end
+	if (half) o = align16(o + sizeof(HalfPair) * (s_cap / 2 + 20));  // 32-slot blocks may read past the end
 	L.cstart = o;
 	o = align16(o + sizeof(int) * 65);
 	L.lists = o;
@@ -107,27 +113,33 @@ __host__ __device__ inline SmemLayout layout(int s_cap, bool fp64, int list_cap)
 }
 
 // Largest staged capacity (a multiple of 64) whose layout fits in `budget` bytes.
-inline int capacity_for(size_t budget, bool fp64, int list_cap) {
+inline int capacity_for(size_t budget, bool fp64, int list_cap, bool half = true) {
 	int s_cap = 256;
-	while (layout(s_cap + 64, fp64, list_cap).total <= budget) s_cap += 64;
+	while (layout(s_cap + 64, fp64, list_cap, half).total <= budget) s_cap += 64;
 	return s_cap > 65535 ? 65535 : s_cap;
 }
 
 // Frame constants of one box (host side).
-inline void init_box(Box& b, const Grid& g, double rc, int32_t coff) {
+// drift: how far a molecule may be outside its cell when staged (half the skin in the Verlet-skin
+// mode, 0 otherwise).
+inline void init_box(Box& b, const Grid& g, double rc, int32_t coff, double drift = 0.0) {
 	b.g = g;
 	b.coff = coff;
 	for (int d = 0; d < 3; d++) {
 		b.nb[d] = (g.nc[d] + 1) / 2;
 		const double cl = g.cell_length[d];
-		// smallest 2^k with the staged region X in [C - 2cl, C + 2cl] inside [2^k, 2^(k+1)]
+		// smallest 2^k with the staged region X in [C - 2cl - drift, C + 2cl + drift] inside
+		// [2^k, 2^(k+1)]
 		double pk = 1.0;
-		while (pk < 4.0 * cl) pk *= 2.0;
+		while (pk < 4.0 * cl + 2.0 * drift) pk *= 2.0;
 		b.frame_c[d] = (float) (1.5 * pk);
+		b.lo_step[d] = (float) std::ldexp(pk, -32);
+		b.lo_inv[d] = (float) std::ldexp(1.0 / pk, 32);
+		b.lo_c[d] = -8388864.0f * b.lo_step[d];
 	}
 	// half-precision filter: coordinates within +-2 cells of the brick centre; each rounding is at
 	// most half an ulp of the largest coordinate, plus the rounding of the packed r^2 itself
-	const double cmax = 2.0 * std::max(g.cell_length[0], std::max(g.cell_length[1], g.cell_length[2]));
+	const double cmax = 2.0 * std::max(g.cell_length[0], std::max(g.cell_length[1], g.cell_length[2])) + drift;
 	const double uc = std::ldexp(1.0, std::ilogb(cmax) - 10);   // half ulp at cmax (10-bit mantissa)
 	const double du = 2.0 * uc * 1.7320508;                     // |error of the difference vector|
 	const double r2max = (rc + du) * (rc + du);
@@ -168,37 +180,81 @@ __device__ __forceinline__ void load_params(unsigned char* smem, const SmemLayou
 	}
 }
 
-// Forces on the molecules of brick `brick` (index within its box) of box `bx`; U, W and the pair
-// count go to partials[slot]. The pair table must already be in shared memory (load_params).
-// Ends with a CTA-wide barrier after which no thread reads the staged data.
-template <bool kFP64, bool kSingle, bool kLjIsRc, int kCap>
-__device__ __forceinline__ void pairs(const Const& p, const Box& bx, int brick, int64_t slot, unsigned char* smem,
-                                      const double* rx, const double* ry, const double* rz, const int32_t* cid,
-                                      const int32_t* cstart, double* fx, double* fy, double* fz, double* partials,
-                                      int* status) {
-	const SmemLayout L = layout(p.s_cap, kFP64, kCap);
-	float4* s_hi = reinterpret_cast<float4*>(smem + L.hi);
-	float4* s_lo = reinterpret_cast<float4*>(smem + L.lo);
-	double* s_img = reinterpret_cast<double*>(smem + L.img);
-	HalfPair* s_h16 = reinterpret_cast<HalfPair*>(smem + L.h16);
-	__half* s_h = reinterpret_cast<__half*>(s_h16);
-	int* s_cs = reinterpret_cast<int*>(smem + L.cstart);        // staged slot of each staged cell (65)
-	unsigned short* s_list = reinterpret_cast<unsigned short*>(smem + L.lists);
-	int* s_cnt = reinterpret_cast<int*>(smem + L.ccount);
-	int* s_gst = reinterpret_cast<int*>(smem + L.gstart);
-	double* s_ck = reinterpret_cast<double*>(smem + L.cell_k);
-	double* s_csh = reinterpret_cast<double*>(smem + L.cell_shift);
-	double* s_pd = reinterpret_cast<double*>(smem + L.params);  // eps24, sig2, shift6 (double)
-	float* s_pf = reinterpret_cast<float*>(s_pd + 3 * KK);
-	const Grid& g = bx.g;
+// Views of the shared-memory layout.
+struct Smem {
+	float4* hi;
+	double* img;
+	HalfPair* h16;
+	__half* h;
+	int* cs;              // staged slot of each staged cell (65)
+	unsigned short* list;
+	int* cnt;
+	int* gst;
+	double* ck;
+	double* csh;
+	double* pd;           // eps24, sig2, shift6 (double)
+	float* pf;            // the same as float
+};
 
-	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-	const int ns = p.ns;
+__device__ __forceinline__ Smem views(unsigned char* smem, const SmemLayout& L) {
+	Smem S;
+	S.hi = reinterpret_cast<float4*>(smem + L.hi);
+	S.img = reinterpret_cast<double*>(smem + L.img);
+	S.h16 = reinterpret_cast<HalfPair*>(smem + L.h16);
+	S.h = reinterpret_cast<__half*>(S.h16);
+	S.cs = reinterpret_cast<int*>(smem + L.cstart);
+	S.list = reinterpret_cast<unsigned short*>(smem + L.lists);
+	S.cnt = reinterpret_cast<int*>(smem + L.ccount);
+	S.gst = reinterpret_cast<int*>(smem + L.gstart);
+	S.ck = reinterpret_cast<double*>(smem + L.cell_k);
+	S.csh = reinterpret_cast<double*>(smem + L.cell_shift);
+	S.pd = reinterpret_cast<double*>(smem + L.params);
+	S.pf = reinterpret_cast<float*>(S.pd + 3 * KK);
+	return S;
+}
+
+// Warp w's brick cell: local (1 + (w&1), 1 + ((w>>1)&1), 1 + (w>>2)) in the 4x4x4 staged region;
+// false when it lies beyond the grid (odd cell counts: the last brick of a dimension is partial).
+__device__ __forceinline__ bool own_cell(const Box& bx, int brick, int w, int& icell) {
 	const int bxi = brick % bx.nb[0];
 	const int byi = (brick / bx.nb[0]) % bx.nb[1];
 	const int bzi = brick / (bx.nb[0] * bx.nb[1]);
-	const int bc[3] = {bxi, byi, bzi};
+	const int il[3] = {1 + (w & 1), 1 + ((w >> 1) & 1), 1 + (w >> 2)};
+	icell = il[0] + 4 * il[1] + 16 * il[2];
+	return 2 * bxi + il[0] - 1 < bx.g.nc[0] && 2 * byi + il[1] - 1 < bx.g.nc[1] && 2 * bzi + il[2] - 1 < bx.g.nc[2];
+}
 
+// The packed 4th word of a staged molecule: lo parts as 9-bit fields (value + 256, bits 0-8, 9-17,
+// 18-26) in steps of Box::lo_step, component id in bits 27-29.
+__device__ __forceinline__ unsigned pack_lo(float lx, float ly, float lz, int cid, const Box& bx) {
+	const float l[3] = {lx, ly, lz};
+	unsigned w = (unsigned) cid << 27;
+	for (int d = 0; d < 3; d++) {
+		int q = __float2int_rn(l[d] * bx.lo_inv[d]);   // power-of-two step: exact product
+		q = max(-255, min(255, q));
+		w |= (unsigned) (q + 256) << (9 * d);
+	}
+	return w;
+}
+
+// lo = fma(2^23 + field, step, -(2^23 + 256) * step): exact in one FMA (power-of-two step).
+__device__ __forceinline__ float3 unpack_lo(unsigned w, const Box& bx) {
+	return make_float3(fmaf(__uint_as_float(0x4B000000u | (w & 511u)), bx.lo_step[0], bx.lo_c[0]),
+	                   fmaf(__uint_as_float(0x4B000000u | ((w >> 9) & 511u)), bx.lo_step[1], bx.lo_c[1]),
+	                   fmaf(__uint_as_float(0x4B000000u | ((w >> 18) & 511u)), bx.lo_step[2], bx.lo_c[2]));
+}
+
+__device__ __forceinline__ int unpack_cid(unsigned w) { return (int) ((w >> 27) & 7u); }
+
+// Stages the 4x4x4 cells around brick `brick` (positions in the local frame; double images in the
+// FP64 mode). Returns false when the region exceeds the staged capacity (nothing staged then; the
+// cell ranges s_gst/s_cnt are set either way). Ends with a CTA barrier.
+template <bool kFP64, bool kHalf = true>
+__device__ __forceinline__ bool stage(const Const& p, const Box& bx, int brick, const Smem& S, const double* rx,
+                                      const double* ry, const double* rz, const int32_t* cid, const int32_t* cstart) {
+	const Grid& g = bx.g;
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	const int bc[3] = {brick % bx.nb[0], (brick / bx.nb[0]) % bx.nb[1], brick / (bx.nb[0] * bx.nb[1])};
 	// staged cells k = lx + 4 ly + 16 lz, local l in 0..3, global 2b - 1 + l with periodic wrap
 	if (tid < 64) {
 		const int l[3] = {tid & 3, (tid >> 2) & 3, tid >> 4};
@@ -214,71 +270,183 @@ __device__ __forceinline__ void pairs(const Const& p, const Box& bx, int brick, 
 				sh = g.L[d];
 			}
 			gc[d] = gcd;
-			s_csh[3 * tid + d] = sh;
+			S.csh[3 * tid + d] = sh;
 			// frame: X = x + K, K = shift - c_brick + C
 			const double cbr = (2 * bc[d] + 1) * g.cell_length[d];
-			s_ck[3 * tid + d] = (sh - cbr) + (double) bx.frame_c[d];
+			S.ck[3 * tid + d] = (sh - cbr) + (double) bx.frame_c[d];
 		}
 		const int gcell = bx.coff + (gc[2] * g.nc[1] + gc[1]) * g.nc[0] + gc[0];
 		const int st = cstart[gcell];
-		s_gst[tid] = st;
-		s_cnt[tid] = max(0, cstart[gcell + 1] - st);
+		S.gst[tid] = st;
+		S.cnt[tid] = max(0, cstart[gcell + 1] - st);
 	}
 	__syncthreads();
 	// exclusive scan of the 64 staged-cell counts (warp 0, two per lane)
 	if (warp == 0) {
-		const int a = s_cnt[2 * lane], b = s_cnt[2 * lane + 1];
+		const int a = S.cnt[2 * lane], b = S.cnt[2 * lane + 1];
 		int inc = a + b;
 		for (int o = 1; o < 32; o <<= 1) {
 			const int y = __shfl_up_sync(kFull, inc, o);
 			if (lane >= o) inc += y;
 		}
 		const int excl = inc - (a + b);
-		s_cs[2 * lane] = excl;
-		s_cs[2 * lane + 1] = excl + a;
-		if (lane == 31) s_cs[64] = inc;
+		S.cs[2 * lane] = excl;
+		S.cs[2 * lane + 1] = excl + a;
+		if (lane == 31) S.cs[64] = inc;
 	}
 	__syncthreads();
-	const int total = s_cs[64];
-	const bool staged = total <= p.s_cap;
-
-	// ---- staging: cell-major, each staged cell's molecules in their (id) order ---------------
+	const bool staged = S.cs[64] <= p.s_cap;
+	// cell-major, each staged cell's molecules in their (id) order
 	if (staged) {
 		for (int c = warp; c < 64; c += kWarps) {
-			const int st = s_gst[c], cnt = s_cnt[c], base = s_cs[c];
-			const double kx = s_ck[3 * c], ky = s_ck[3 * c + 1], kz = s_ck[3 * c + 2];
-			const double shx = s_csh[3 * c], shy = s_csh[3 * c + 1], shz = s_csh[3 * c + 2];
+			const int st = S.gst[c], cnt = S.cnt[c], base = S.cs[c];
+			const double kx = S.ck[3 * c], ky = S.ck[3 * c + 1], kz = S.ck[3 * c + 2];
+			const double shx = S.csh[3 * c], shy = S.csh[3 * c + 1], shz = S.csh[3 * c + 2];
 			for (int e = lane; e < cnt; e += 32) {
 				const int gi = st + e;
 				const double x = rx[gi], y = ry[gi], z = rz[gi];
 				const double Xd = __dadd_rn(x, kx), Yd = __dadd_rn(y, ky), Zd = __dadd_rn(z, kz);
 				const float X = __double2float_rn(Xd), Y = __double2float_rn(Yd), Z = __double2float_rn(Zd);
 				const int slot_s = base + e;
-				s_hi[slot_s] = make_float4(X, Y, Z, __int_as_float((gi << 3) | cid[gi]));
-				// half-precision copy relative to the brick centre (slot pairs share one HalfPair)
-				__half* hp = s_h + 8 * (slot_s >> 1) + (slot_s & 1);
-				hp[0] = __float2half_rn(X - bx.frame_c[0]);
-				hp[2] = __float2half_rn(Y - bx.frame_c[1]);
-				hp[4] = __float2half_rn(Z - bx.frame_c[2]);
+				const unsigned w = pack_lo(__double2float_rn(Xd - (double) X), __double2float_rn(Yd - (double) Y),
+				                           __double2float_rn(Zd - (double) Z), cid[gi], bx);
+				S.hi[slot_s] = make_float4(X, Y, Z, __uint_as_float(w));
+				if (kHalf) {
+					// half-precision copy relative to the brick centre (slot pairs share one HalfPair)
+					__half* hp = S.h + 8 * (slot_s >> 1) + (slot_s & 1);
+					hp[0] = __float2half_rn(X - bx.frame_c[0]);
+					hp[2] = __float2half_rn(Y - bx.frame_c[1]);
+					hp[4] = __float2half_rn(Z - bx.frame_c[2]);
+				}
 				if (kFP64) {
-					s_img[slot_s] = __dadd_rn(x, shx);
-					s_img[p.s_cap + slot_s] = __dadd_rn(y, shy);
-					s_img[2 * p.s_cap + slot_s] = __dadd_rn(z, shz);
-				} else {
-					s_lo[slot_s] = make_float4(__double2float_rn(Xd - (double) X), __double2float_rn(Yd - (double) Y),
-					                           __double2float_rn(Zd - (double) Z), 0.f);
+					S.img[slot_s] = __dadd_rn(x, shx);
+					S.img[p.s_cap + slot_s] = __dadd_rn(y, shy);
+					S.img[2 * p.s_cap + slot_s] = __dadd_rn(z, shz);
 				}
 			}
 		}
 	}
 	__syncthreads();
+	return staged;
+}
+
+// One list entry j of molecule i in FP32 with FP64-ready accumulators (branch-free: an invalid
+// entry, v = false, or a pair outside the cutoff contributes zeros; the rare pairs within a few ulp
+// of rc are decided in double from the same hi/lo parts).
+template <bool kSingle, bool kLjIsRc>
+__device__ __forceinline__ void lj32(const Const& p, bool v, const float4& hi_i, const float3& lo_i, int ti, int ns,
+                                     const float4 hj, const Box& bx, const float* pf, float eps24_1, float sig2_1,
+                                     float shift6_1, float& ax, float& ay, float& az, float& au, float& aw, int& anp,
+                                     bool& same) {
+	const float3 lj = unpack_lo(__float_as_uint(hj.w), bx);
+	const float h0 = hi_i.x - hj.x, h1 = hi_i.y - hj.y, h2 = hi_i.z - hj.z;  // exact
+	const float e0 = h0 + (lo_i.x - lj.x), e1 = h1 + (lo_i.y - lj.y), e2 = h2 + (lo_i.z - lj.z);
+	const float d2f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2));
+	bool in = v && d2f < p.rc2f;
+	const bool amb = v && fabsf(d2f - p.rc2f) <= p.band;
+	if (__any_sync(kFull, amb)) {
+		if (amb) {
+			const double a0 = (double) h0 + ((double) lo_i.x - (double) lj.x);
+			const double a1 = (double) h1 + ((double) lo_i.y - (double) lj.y);
+			const double a2 = (double) h2 + ((double) lo_i.z - (double) lj.z);
+			in = a0 * a0 + a1 * a1 + a2 * a2 < p.rc2;
+		}
+	}
+	anp += in ? 1 : 0;
+	same |= in && d2f == 0.f;
+	const bool lj_in = kLjIsRc ? in : (in && d2f < p.rclj2f);
+	float eps24, sig2, shift6;
+	if (kSingle) {
+		eps24 = eps24_1;
+		sig2 = sig2_1;
+		shift6 = shift6_1;
+	} else {
+		const int pk = ti * ns + unpack_cid(__float_as_uint(hj.w));
+		eps24 = pf[pk];
+		sig2 = pf[KK + pk];
+		shift6 = pf[2 * KK + pk];
+	}
+	const float inv = rcp_approx(lj_in ? d2f : 1.0f);
+	const float s2 = sig2 * inv;
+	const float s6 = s2 * s2 * s2;
+	const float s12 = s6 * s6;
+	const float m = s12 - s6;
+	const float fac = lj_in ? eps24 * (s12 + m) * inv : 0.f;
+	ax = fmaf(fac, e0, ax);
+	ay = fmaf(fac, e1, ay);
+	az = fmaf(fac, e2, az);
+	au += lj_in ? fmaf(eps24, m, shift6) : 0.f;
+	aw = fmaf(fac, d2f, aw);
+}
+
+// One list entry j (staged slot) of molecule i at the double image position (xi, yi, zi), in FP64
+// with the reference's operation order.
+template <bool kSingle>
+__device__ __forceinline__ void lj64(const Const& p, double xi, double yi, double zi, int ti, int ns, int j,
+                                     const Smem& S, double& ax, double& ay, double& az, double& au, double& aw,
+                                     int& anp, bool& same) {
+	const double d0 = __dsub_rn(xi, S.img[j]);
+	const double d1 = __dsub_rn(yi, S.img[p.s_cap + j]);
+	const double d2 = __dsub_rn(zi, S.img[2 * p.s_cap + j]);
+	const double dd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+	if (!(dd < p.rc2)) return;
+	anp++;
+	if (dd == 0.0) same = true;
+	if (!(dd < p.rclj2)) return;
+	int pk = 0;
+	if (!kSingle) pk = ti * ns + unpack_cid(__float_as_uint(S.hi[j].w));
+	double f0, f1, f2, u, w;
+	lj_pair_fp64(d0, d1, d2, dd, S.pd[pk], S.pd[KK + pk], S.pd[2 * KK + pk], f0, f1, f2, u, w);
+	ax += f0;
+	ay += f1;
+	az += f2;
+	au += u;
+	aw = __dadd_rn(aw, w);
+}
+
+// Neighbour lists of the Verlet-skin mode: entry k of molecule i (sorted slot) is a staged slot of
+// i's brick region, stored at ((k/8)*n + i)*8 + k%8, so that one 16-byte load gives a lane 8 entries
+// and a warp's loads are contiguous; count[i] entries, kListOverflow when more than cap were found.
+struct Lists {
+	unsigned short* nbr;
+	unsigned short* count;
+	double *rx_ref, *ry_ref, *rz_ref;   // positions at the build
+	int64_t n;
+	int cap;
+	unsigned long long* builds;        // incremented once per build
+};
+constexpr unsigned short kListOverflow = 0xffff;
+
+// Forces on the molecules of brick `brick` (index within its box) of box `bx`; U, W and the pair
+// count go to partials[slot]. The pair table must already be in shared memory (load_params).
+// Ends with a CTA-wide barrier after which no thread reads the staged data.
+template <bool kFP64, bool kSingle, bool kLjIsRc, int kCap>
+__device__ __forceinline__ void pairs(const Const& p, const Box& bx, int brick, int64_t slot, unsigned char* smem,
+                                      const double* rx, const double* ry, const double* rz, const int32_t* cid,
+                                      const int32_t* cstart, double* fx, double* fy, double* fz, double* partials,
+                                      int* status) {
+	const SmemLayout L = layout(p.s_cap, kFP64, kCap);
+	const Smem S = views(smem, L);
+	float4* s_hi = S.hi;
+	double* s_img = S.img;
+	HalfPair* s_h16 = S.h16;
+	int* s_cs = S.cs;
+	unsigned short* s_list = S.list;
+	int* s_cnt = S.cnt;
+	int* s_gst = S.gst;
+	double* s_pd = S.pd;
+	float* s_pf = S.pf;
+	const Grid& g = bx.g;
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	const int ns = p.ns;
+	const bool staged = stage<kFP64>(p, bx, brick, S, rx, ry, rz, cid, cstart);
 
 	// ---- pairs: warp w owns brick cell (1 + (w&1), 1 + ((w>>1)&1), 1 + (w>>2)) -----------------
 	double U = 0.0, W = 0.0, NP = 0.0;
 	bool same = false;
 	const int il[3] = {1 + (warp & 1), 1 + ((warp >> 1) & 1), 1 + (warp >> 2)};
-	const bool cell_ok = 2 * bxi + il[0] - 1 < g.nc[0] && 2 * byi + il[1] - 1 < g.nc[1] && 2 * bzi + il[2] - 1 < g.nc[2];
-	const int icell = il[0] + 4 * il[1] + 16 * il[2];
+	int icell;
+	const bool cell_ok = own_cell(bx, brick, warp, icell);
 	if (cell_ok && !staged) {
 		// over capacity: gather from global memory
 		const int st = s_gst[icell], cnt = s_cnt[icell];
@@ -299,17 +467,15 @@ __device__ __forceinline__ void pairs(const Const& p, const Box& bx, int brick, 
 			const bool act = b0 + lane < ni;
 			const int slot_i = i0 + (act ? b0 + lane : 0);
 			const float4 hi_i = s_hi[slot_i];
-			float4 lo_i = make_float4(0.f, 0.f, 0.f, 0.f);
+			const float3 lo_i = unpack_lo(__float_as_uint(hi_i.w), bx);
 			double xi = 0, yi = 0, zi = 0;
 			if (kFP64) {
 				xi = s_img[slot_i];
 				yi = s_img[p.s_cap + slot_i];
 				zi = s_img[2 * p.s_cap + slot_i];
-			} else {
-				lo_i = s_lo[slot_i];
 			}
-			const int ti = __float_as_int(hi_i.w) & 7;
-			const int gi = __float_as_int(hi_i.w) >> 3;
+			const int ti = unpack_cid(__float_as_uint(hi_i.w));
+			const int gi = s_gst[icell] + (slot_i - i0);
 			int cnt = 0;
 			double Fx = 0.0, Fy = 0.0, Fz = 0.0;
 			const float eps24_1 = s_pf[0], sig2_1 = s_pf[KK], shift6_1 = s_pf[2 * KK];
@@ -319,67 +485,12 @@ __device__ __forceinline__ void pairs(const Const& p, const Box& bx, int brick, 
 			auto pair_fp32 = [&](int tt, float& ax, float& ay, float& az, float& au, float& aw, int& anp) {
 				const bool v = tt < cnt;
 				const int j = v ? (int) mylist[tt * 32] : slot_i;
-				const float4 hj = s_hi[j];
-				const float4 lj = s_lo[j];
-				const float h0 = hi_i.x - hj.x, h1 = hi_i.y - hj.y, h2 = hi_i.z - hj.z;  // exact
-				const float e0 = h0 + (lo_i.x - lj.x), e1 = h1 + (lo_i.y - lj.y), e2 = h2 + (lo_i.z - lj.z);
-				const float d2f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2));
-				bool in = v && d2f < p.rc2f;
-				const bool amb = v && fabsf(d2f - p.rc2f) <= p.band;
-				if (__any_sync(kFull, amb)) {
-					if (amb) {
-						const double a0 = (double) h0 + ((double) lo_i.x - (double) lj.x);
-						const double a1 = (double) h1 + ((double) lo_i.y - (double) lj.y);
-						const double a2 = (double) h2 + ((double) lo_i.z - (double) lj.z);
-						in = a0 * a0 + a1 * a1 + a2 * a2 < p.rc2;
-					}
-				}
-				anp += in ? 1 : 0;
-				same |= in && d2f == 0.f;
-				const bool lj_in = kLjIsRc ? in : (in && d2f < p.rclj2f);
-				float eps24, sig2, shift6;
-				if (kSingle) {
-					eps24 = eps24_1;
-					sig2 = sig2_1;
-					shift6 = shift6_1;
-				} else {
-					const int pk = ti * ns + (__float_as_int(hj.w) & 7);
-					eps24 = s_pf[pk];
-					sig2 = s_pf[KK + pk];
-					shift6 = s_pf[2 * KK + pk];
-				}
-				const float inv = rcp_approx(lj_in ? d2f : 1.0f);
-				const float s2 = sig2 * inv;
-				const float s6 = s2 * s2 * s2;
-				const float s12 = s6 * s6;
-				const float m = s12 - s6;
-				const float fac = lj_in ? eps24 * (s12 + m) * inv : 0.f;
-				ax = fmaf(fac, e0, ax);
-				ay = fmaf(fac, e1, ay);
-				az = fmaf(fac, e2, az);
-				au += lj_in ? fmaf(eps24, m, shift6) : 0.f;
-				aw = fmaf(fac, d2f, aw);
+				lj32<kSingle, kLjIsRc>(p, v, hi_i, lo_i, ti, ns, s_hi[j], bx, s_pf, eps24_1, sig2_1, shift6_1, ax, ay, az,
+				                       au, aw, anp, same);
 			};
 			auto pair_fp64 = [&](int tt, double& ax, double& ay, double& az, double& au, double& aw, int& anp) {
 				if (tt >= cnt) return;
-				const int j = mylist[tt * 32];
-				const double d0 = __dsub_rn(xi, s_img[j]);
-				const double d1 = __dsub_rn(yi, s_img[p.s_cap + j]);
-				const double d2 = __dsub_rn(zi, s_img[2 * p.s_cap + j]);
-				const double dd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
-				if (!(dd < p.rc2)) return;
-				anp++;
-				if (dd == 0.0) same = true;
-				if (!(dd < p.rclj2)) return;
-				int pk = 0;
-				if (!kSingle) pk = ti * ns + (__float_as_int(s_hi[j].w) & 7);
-				double f0, f1, f2, u, w;
-				lj_pair_fp64(d0, d1, d2, dd, s_pd[pk], s_pd[KK + pk], s_pd[2 * KK + pk], f0, f1, f2, u, w);
-				ax += f0;
-				ay += f1;
-				az += f2;
-				au += u;
-				aw = __dadd_rn(aw, w);
+				lj64<kSingle>(p, xi, yi, zi, ti, ns, mylist[tt * 32], S, ax, ay, az, au, aw, anp, same);
 			};
 			auto flush = [&]() {
 				const int mx = __reduce_max_sync(kFull, cnt);
@@ -457,6 +568,298 @@ __device__ __forceinline__ void pairs(const Const& p, const Box& bx, int brick, 
 			}
 			flush();
 			if (act) {
+				fx[gi] = Fx;
+				fy[gi] = Fy;
+				fz[gi] = Fz;
+				if (!(Fx == Fx && Fy == Fy && Fz == Fz) || isinf(Fx) || isinf(Fy) || isinf(Fz))
+					atomicOr(status, kStatusNonFinite);
+			}
+		}
+	}
+	if (same) atomicOr(status, kStatusSamePosition);
+	block_sum3_at(U, W, NP, partials, slot);
+}
+
+// Shared-memory bytes of build_lists for a staged capacity s_cap.
+__host__ __device__ inline size_t build_bytes(int s_cap) {
+	return align16(sizeof(HalfPair) * (s_cap / 2 + 20)) + align16(sizeof(int) * 65) + 2 * align16(sizeof(int) * 64) +
+	       sizeof(double) * 3 * 64;
+}
+
+// Verlet-skin build for brick `brick`: stages the half-precision copy of the 4x4x4 cells around it
+// (the same slots as stage() gives them) and writes to each own molecule's list every candidate
+// that the packed filter finds within the list radius (bx.rc2_h holds rc + skin plus the rounding
+// margin), with the positions of the build. No forces: list_pairs evaluates the lists.
+__device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap, unsigned char* smem,
+                                            const double* rx, const double* ry, const double* rz,
+                                            const int32_t* cstart, Lists lists) {
+	HalfPair* s_h16 = reinterpret_cast<HalfPair*>(smem);
+	__half* s_h = reinterpret_cast<__half*>(smem);
+	size_t o = align16(sizeof(HalfPair) * (s_cap / 2 + 20));
+	int* s_cs = reinterpret_cast<int*>(smem + o);
+	o += align16(sizeof(int) * 65);
+	int* s_cnt = reinterpret_cast<int*>(smem + o);
+	o += align16(sizeof(int) * 64);
+	int* s_gst = reinterpret_cast<int*>(smem + o);
+	o += align16(sizeof(int) * 64);
+	double* s_ck = reinterpret_cast<double*>(smem + o);
+	const Grid& g = bx.g;
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	const int bc[3] = {brick % bx.nb[0], (brick / bx.nb[0]) % bx.nb[1], brick / (bx.nb[0] * bx.nb[1])};
+	if (tid < 64) {
+		const int l[3] = {tid & 3, (tid >> 2) & 3, tid >> 4};
+		int gc[3];
+		for (int d = 0; d < 3; d++) {
+			int gcd = 2 * bc[d] - 1 + l[d];
+			double sh = 0.0;
+			if (gcd < 0) {
+				gcd += g.nc[d];
+				sh = -g.L[d];
+			} else if (gcd >= g.nc[d]) {
+				gcd -= g.nc[d];
+				sh = g.L[d];
+			}
+			gc[d] = gcd;
+			const double cbr = (2 * bc[d] + 1) * g.cell_length[d];
+			s_ck[3 * tid + d] = (sh - cbr) + (double) bx.frame_c[d];
+		}
+		const int gcell = bx.coff + (gc[2] * g.nc[1] + gc[1]) * g.nc[0] + gc[0];
+		const int st = cstart[gcell];
+		s_gst[tid] = st;
+		s_cnt[tid] = max(0, cstart[gcell + 1] - st);
+	}
+	__syncthreads();
+	if (warp == 0) {
+		const int a = s_cnt[2 * lane], b = s_cnt[2 * lane + 1];
+		int inc = a + b;
+		for (int of = 1; of < 32; of <<= 1) {
+			const int y = __shfl_up_sync(kFull, inc, of);
+			if (lane >= of) inc += y;
+		}
+		const int excl = inc - (a + b);
+		s_cs[2 * lane] = excl;
+		s_cs[2 * lane + 1] = excl + a;
+		if (lane == 31) s_cs[64] = inc;
+	}
+	__syncthreads();
+	const bool staged = s_cs[64] <= s_cap;
+	if (staged) {
+		for (int c = warp; c < 64; c += kWarps) {
+			const int st = s_gst[c], cnt = s_cnt[c], base = s_cs[c];
+			const double kx = s_ck[3 * c], ky = s_ck[3 * c + 1], kz = s_ck[3 * c + 2];
+			for (int e = lane; e < cnt; e += 32) {
+				const int gi = st + e;
+				const float X = __double2float_rn(__dadd_rn(rx[gi], kx));
+				const float Y = __double2float_rn(__dadd_rn(ry[gi], ky));
+				const float Z = __double2float_rn(__dadd_rn(rz[gi], kz));
+				const int slot_s = base + e;
+				__half* hp = s_h + 8 * (slot_s >> 1) + (slot_s & 1);
+				hp[0] = __float2half_rn(X - bx.frame_c[0]);
+				hp[2] = __float2half_rn(Y - bx.frame_c[1]);
+				hp[4] = __float2half_rn(Z - bx.frame_c[2]);
+			}
+		}
+	}
+	__syncthreads();
+	int icell;
+	if (own_cell(bx, brick, warp, icell)) {
+		const int st = s_gst[icell], ncell = s_cnt[icell], i0 = s_cs[icell];
+		const int il[3] = {1 + (warp & 1), 1 + ((warp >> 1) & 1), 1 + (warp >> 2)};
+		if (!staged) {
+			for (int e = lane; e < ncell; e += 32) {
+				lists.count[st + e] = kListOverflow;
+				lists.rx_ref[st + e] = rx[st + e];
+				lists.ry_ref[st + e] = ry[st + e];
+				lists.rz_ref[st + e] = rz[st + e];
+			}
+		} else {
+			const __half2 rc2h = __float2half2_rn(bx.rc2_h);
+			for (int b0 = 0; b0 < ncell; b0 += 32) {
+				const bool act = b0 + lane < ncell;
+				const int slot_i = i0 + (act ? b0 + lane : 0);
+				const int gi = st + (slot_i - i0);
+				const __half* hi = s_h + 8 * (slot_i >> 1) + (slot_i & 1);
+				const __half2 xi2 = act ? __half2half2(hi[0]) : __float2half2_rn(60000.f);
+				const __half2 yi2 = __half2half2(hi[2]);
+				const __half2 zi2 = __half2half2(hi[4]);
+				int cntg = 0;
+				for (int r = 0; r < 9; r++) {
+					const int ky = il[1] + (r % 3) - 1, kz = il[2] + (r / 3) - 1;
+					const int k0 = (il[0] - 1) + 4 * ky + 16 * kz;
+					const int a = s_cs[k0], b = s_cs[k0 + 3];
+					for (int base = a & ~1; base < b; base += 32) {
+						unsigned mask = 0u;
+#pragma unroll
+						for (int k = 0; k < 16; k++) {
+							const HalfPair H = s_h16[(base >> 1) + k];
+							const __half2 dx = __hsub2(xi2, H.x), dy = __hsub2(yi2, H.y), dz = __hsub2(zi2, H.z);
+							const __half2 d2 = __hfma2(dx, dx, __hfma2(dy, dy, __hmul2(dz, dz)));
+							const unsigned hm = __hlt2_mask(d2, rc2h);
+							mask |= ((hm & 1u) | ((hm >> 15) & 2u)) << (2 * k);
+						}
+						const int lo = a - base, hi_b = b - base;
+						unsigned valid = hi_b >= 32 ? 0xffffffffu : ((1u << hi_b) - 1u);
+						if (lo > 0) valid &= ~((1u << lo) - 1u);
+						const int self = slot_i - base;
+						if (self >= 0 && self < 32) valid &= ~(1u << self);
+						mask &= valid;
+						if (!act) mask = 0u;
+						while (mask) {
+							const int bit = __ffs(mask) - 1;
+							mask &= mask - 1u;
+							if (cntg < lists.cap)
+								lists.nbr[(((int64_t) (cntg >> 3) * lists.n + gi) << 3) + (cntg & 7)] =
+								    (unsigned short) (base + bit);
+							cntg++;
+						}
+					}
+				}
+				if (act) {
+					lists.count[gi] = cntg <= lists.cap ? (unsigned short) cntg : kListOverflow;
+					lists.rx_ref[gi] = rx[gi];
+					lists.ry_ref[gi] = ry[gi];
+					lists.rz_ref[gi] = rz[gi];
+				}
+			}
+		}
+	}
+	if (brick == 0 && tid == 0) atomicAdd(lists.builds, 1ull);
+}
+
+// Forces of brick `brick` from the neighbour lists that build_lists made on the same cell
+// structure, at the current positions: staging as in pairs, then the molecules of the brick's
+// own cells, 32 per warp regardless of their cell, each evaluate their list with the exact cutoff.
+// Chunks of 64 entries are summed in FP32 and added to FP64 accumulators.
+// Shared memory: layout(s_cap, kFP64, 0, false) (no filter lists, no half-precision copy).
+template <bool kFP64, bool kSingle, bool kLjIsRc>
+__device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int brick, int64_t slot,
+                                           unsigned char* smem, const double* rx, const double* ry, const double* rz,
+                                           const int32_t* cid, const int32_t* cstart, double* fx, double* fy,
+                                           double* fz, double* partials, int* status, const Lists lists) {
+	const SmemLayout L = layout(p.s_cap, kFP64, 0, false);
+	const Smem S = views(smem, L);
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	const int ns = p.ns;
+	const bool staged = stage<kFP64, false>(p, bx, brick, S, rx, ry, rz, cid, cstart);
+	__shared__ int s_own[9], s_ocell[8];
+	if (tid == 0) {
+		int acc = 0;
+		for (int w = 0; w < 8; w++) {
+			int ic;
+			const bool ok = own_cell(bx, brick, w, ic);
+			s_own[w] = acc;
+			s_ocell[w] = ic;
+			acc += ok ? S.cnt[ic] : 0;
+		}
+		s_own[8] = acc;
+	}
+	__syncthreads();
+	const int n_own = s_own[8];
+	double U = 0.0, W = 0.0, NP = 0.0;
+	bool same = false;
+	if (!staged) {
+		// over capacity: gather from global memory
+		for (int t = tid; t < n_own; t += kThreads) {
+			int w = 0;
+			while (w < 7 && s_own[w + 1] <= t) w++;
+			const int gi = S.gst[s_ocell[w]] + (t - s_own[w]);
+			PairSums s = gather_pairs<!kFP64>(gi, rx, ry, rz, cid, cstart, bx.g, S.pd, ns, p.rc2, p.rclj2, bx.coff);
+			fx[gi] = s.F[0];
+			fy[gi] = s.F[1];
+			fz[gi] = s.F[2];
+			U += s.U;
+			W += s.W;
+			NP += s.np;
+			same |= s.same;
+		}
+	} else {
+		const float eps24_1 = S.pf[0], sig2_1 = S.pf[KK], shift6_1 = S.pf[2 * KK];
+		for (int t0 = warp * 32; t0 < n_own; t0 += kThreads) {
+			const int t = t0 + lane;
+			const bool act = t < n_own;
+			int w = 0;
+			if (act)
+				while (w < 7 && s_own[w + 1] <= t) w++;
+			const int slot_i = act ? S.cs[s_ocell[w]] + (t - s_own[w]) : 0;
+			const float4 hi_i = S.hi[slot_i];
+			const float3 lo_i = unpack_lo(__float_as_uint(hi_i.w), bx);
+			double xi = 0, yi = 0, zi = 0;
+			if (kFP64) {
+				xi = S.img[slot_i];
+				yi = S.img[p.s_cap + slot_i];
+				zi = S.img[2 * p.s_cap + slot_i];
+			}
+			const int ti = unpack_cid(__float_as_uint(hi_i.w));
+			const int gi = act ? S.gst[s_ocell[w]] + (t - s_own[w]) : S.gst[s_ocell[0]];
+			int cnt = act ? (int) lists.count[gi] : 0;
+			const bool ovf = cnt == kListOverflow;
+			if (ovf) {
+				// the list overflowed at the build: gather this molecule from global memory
+				PairSums s = gather_pairs<!kFP64>(gi, rx, ry, rz, cid, cstart, bx.g, S.pd, ns, p.rc2, p.rclj2, bx.coff);
+				fx[gi] = s.F[0];
+				fy[gi] = s.F[1];
+				fz[gi] = s.F[2];
+				U += s.U;
+				W += s.W;
+				NP += s.np;
+				same |= s.same;
+				cnt = 0;
+			}
+			const int mx = __reduce_max_sync(kFull, cnt);
+			// blocks of 8 entries, one 16-byte load each, the next block loaded while this one is used
+			const uint4* my8 = reinterpret_cast<const uint4*>(lists.nbr) + gi;
+			const int nb8 = (mx + 7) >> 3;
+			double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+			int anp = 0;
+			uint4 nxt = nb8 > 0 ? my8[0] : make_uint4(0u, 0u, 0u, 0u);
+			if (kFP64) {
+				double ax[2] = {0, 0}, ay[2] = {0, 0}, az[2] = {0, 0}, au[2] = {0, 0}, aw[2] = {0, 0};
+				for (int b = 0; b < nb8; b++) {
+					const uint4 cur = nxt;
+					if (b + 1 < nb8) nxt = my8[(int64_t) (b + 1) * lists.n];
+					const unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
+#pragma unroll
+					for (int u = 0; u < 8; u++) {
+						const int kk = 8 * b + u;
+						const int j = min((int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu), p.s_cap - 1);
+						if (kk < cnt) lj64<kSingle>(p, xi, yi, zi, ti, ns, j, S, ax[u & 1], ay[u & 1], az[u & 1], au[u & 1],
+						                            aw[u & 1], anp, same);
+					}
+				}
+				Fx += ax[0] + ax[1];
+				Fy += ay[0] + ay[1];
+				Fz += az[0] + az[1];
+				U += au[0] + au[1];
+				W = __dadd_rn(W, __dadd_rn(aw[0], aw[1]));
+			} else {
+				float ax[4] = {0.f, 0.f, 0.f, 0.f}, ay[4] = {0.f, 0.f, 0.f, 0.f}, az[4] = {0.f, 0.f, 0.f, 0.f};
+				float au[4] = {0.f, 0.f, 0.f, 0.f}, aw[4] = {0.f, 0.f, 0.f, 0.f};
+				for (int b = 0; b < nb8; b++) {
+					const uint4 cur = nxt;
+					if (b + 1 < nb8) nxt = my8[(int64_t) (b + 1) * lists.n];
+					const unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
+#pragma unroll
+					for (int u = 0; u < 8; u++) {
+						const int kk = 8 * b + u;
+						const bool v = kk < cnt;
+						const int j = v ? min((int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu), p.s_cap - 1) : slot_i;
+						lj32<kSingle, kLjIsRc>(p, v, hi_i, lo_i, ti, ns, S.hi[j], bx, S.pf, eps24_1, sig2_1, shift6_1,
+						                       ax[u & 3], ay[u & 3], az[u & 3], au[u & 3], aw[u & 3], anp, same);
+					}
+					if ((b & 7) == 7 || b + 1 == nb8) {
+						// fold the FP32 partial sums of up to 64 entries into the FP64 accumulators
+						Fx += ((double) ax[0] + (double) ax[1]) + ((double) ax[2] + (double) ax[3]);
+						Fy += ((double) ay[0] + (double) ay[1]) + ((double) ay[2] + (double) ay[3]);
+						Fz += ((double) az[0] + (double) az[1]) + ((double) az[2] + (double) az[3]);
+						U += ((double) au[0] + (double) au[1]) + ((double) au[2] + (double) au[3]);
+						W += ((double) aw[0] + (double) aw[1]) + ((double) aw[2] + (double) aw[3]);
+#pragma unroll
+						for (int u = 0; u < 4; u++) ax[u] = ay[u] = az[u] = au[u] = aw[u] = 0.f;
+					}
+				}
+			}
+			NP += (double) anp;
+			if (act && !ovf) {
 				fx[gi] = Fx;
 				fy[gi] = Fy;
 				fz[gi] = Fz;

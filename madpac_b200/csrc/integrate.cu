@@ -20,26 +20,41 @@ struct SpeciesScale {
 	double mass[kMaxSpecies];
 };
 
+// Verlet-skin check of the pre-kick: the positions at the last build and the squared half skin.
+struct SkinCheck {
+	const double *rx, *ry, *rz;
+	double half2;
+	int* flag;
+};
+
 __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_pre(int64_t n, Particles p, SpeciesScale s, double dt,
-                                                              double vcorr) {
+                                                              double vcorr, SkinCheck sk) {
 	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	const double a = s.dtInv2m[p.cid[i]];
 	double v;
 	v = __dadd_rn(__dmul_rn(vcorr, p.vx[i]), __dmul_rn(a, p.fx[i]));
 	p.vx[i] = v;
-	p.rx[i] = __dadd_rn(p.rx[i], __dmul_rn(dt, v));
+	const double x = __dadd_rn(p.rx[i], __dmul_rn(dt, v));
+	p.rx[i] = x;
 	v = __dadd_rn(__dmul_rn(vcorr, p.vy[i]), __dmul_rn(a, p.fy[i]));
 	p.vy[i] = v;
-	p.ry[i] = __dadd_rn(p.ry[i], __dmul_rn(dt, v));
+	const double y = __dadd_rn(p.ry[i], __dmul_rn(dt, v));
+	p.ry[i] = y;
 	v = __dadd_rn(__dmul_rn(vcorr, p.vz[i]), __dmul_rn(a, p.fz[i]));
 	p.vz[i] = v;
-	p.rz[i] = __dadd_rn(p.rz[i], __dmul_rn(dt, v));
+	const double z = __dadd_rn(p.rz[i], __dmul_rn(dt, v));
+	p.rz[i] = z;
+	if (sk.flag) {
+		const double dx = x - sk.rx[i], dy = y - sk.ry[i], dz = z - sk.rz[i];
+		if (!(dx * dx + dy * dy + dz * dz <= sk.half2)) *sk.flag = 1;
+	}
 }
 
 __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_post(int64_t n, Particles p, SpeciesScale s,
-                                                               double* partials, int* status) {
+                                                               double* partials, int* status, int* clear_flag) {
 	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (clear_flag && i == 0) *clear_flag = 0;   // every pair kernel of this step has read it
 	double mv2 = 0.0;
 	if (i < n) {
 		const int t = p.cid[i];
@@ -88,21 +103,29 @@ inline unsigned blocks_for(int64_t n) { return (unsigned) ((n + kReduceBlock - 1
 
 }  // namespace
 
-cudaError_t launch_leapfrog_pre(Context* c, double dt, double vcorr) {
+cudaError_t launch_leapfrog_pre(Context* c, double dt, double vcorr, bool skin_check) {
 	if (c->n == 0) return cudaSuccess;
 	prof_begin(c, 2);
+	SkinCheck sk{};
+	if (skin_check) {
+		sk.rx = c->r_ref;
+		sk.ry = c->r_ref + c->n;
+		sk.rz = c->r_ref + 2 * c->n;
+		sk.half2 = 0.25 * c->skin * c->skin;
+		sk.flag = c->rebuild;
+	}
 	// dt_halve = .5 * dt, dtInv2m = dt_halve / m  (Molecule.cpp:130-131)
-	k_leapfrog_pre<<<blocks_for(c->n), kReduceBlock, 0, c->stream>>>(c->n, c->p, make_scale(c, .5 * dt), dt, vcorr);
+	k_leapfrog_pre<<<blocks_for(c->n), kReduceBlock, 0, c->stream>>>(c->n, c->p, make_scale(c, .5 * dt), dt, vcorr, sk);
 	cudaError_t e = cudaGetLastError();
 	prof_end(c, 2, 1);
 	return e;
 }
 
-cudaError_t launch_leapfrog_post(Context* c, double dt_half) {
+cudaError_t launch_leapfrog_post(Context* c, double dt_half, bool clear_flag) {
 	prof_begin(c, 2);
 	int64_t nb = c->n > 0 ? blocks_for(c->n) : 1;
 	k_leapfrog_post<<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(c->n, c->p, make_scale(c, dt_half), c->partials,
-	                                                               c->status);
+	                                                               c->status, clear_flag ? c->rebuild : nullptr);
 	cudaError_t e = cudaGetLastError();
 	prof_end(c, 2, 1);
 	if (e != cudaSuccess) return e;

@@ -92,6 +92,20 @@ struct Context {
 	int64_t steps_written = 0;      // records appended since the last mdgpu_read_steps
 	int* status = nullptr;          // device status word
 	PairParams* d_pp = nullptr;     // device copy of the pair parameters
+	// Verlet-skin mode of mdgpu_step / mdgpu_run (skin > 0): per-molecule candidate lists of radius
+	// rc + skin on a frozen cell structure, rebuilt (with the binning) by device-side gating when a
+	// molecule has moved more than skin/2 since the last build
+	double skin = 0.0;
+	Grid gs{};                      // cells of edge >= cutoff + skin on which the lists are built
+	int max_occ = 0;                // largest cell occupancy of the loaded positions (sizes the lists)
+	int list_cap = 0;               // list entries per molecule
+	int64_t list_n = 0;             // molecules the list buffers hold
+	unsigned short* nbr = nullptr;  // list_cap x n staged-slot indices
+	unsigned short* nbr_count = nullptr;
+	double* r_ref = nullptr;        // 3 x n positions at the last build
+	int* rebuild = nullptr;         // device flag: nonzero = build this step
+	unsigned long long* builds = nullptr;   // builds so far (device counter)
+	bool lists_valid = false;       // the sort order has not changed since the lists were built
 	double* adj = nullptr;          // adjoint buffers: cotangents, outputs, parameter partials
 	int64_t adj_cap = 0;
 	double* h_scalars = nullptr;    // pinned host mirror
@@ -107,10 +121,15 @@ struct Context {
 
 // ---- launch helpers implemented in the .cu files -------------------------------------------
 // Each returns cudaSuccess or the launch error; kernels report data errors in ctx->status.
-cudaError_t launch_bin(Context* c, bool permute_forces);
+// With a gate (Verlet-skin mode) every kernel returns at once unless *gate != 0, and the sorted
+// arrays are copied back into c->p so that the host-side buffer roles do not depend on the flag.
+cudaError_t launch_bin(Context* c, bool permute_forces, const int* gate = nullptr, const Grid* grid = nullptr);
 cudaError_t launch_pairs(Context* c);                 // partials -> scalars[0..2] (U6sum, W, npairs)
-cudaError_t launch_leapfrog_pre(Context* c, double dt, double vcorr);
-cudaError_t launch_leapfrog_post(Context* c, double dt_half);   // scalars[3] = sum m v^2
+cudaError_t launch_pairs_skin(Context* c);            // the same in the Verlet-skin mode
+// With skin_check the pre-kick also raises c->rebuild when a molecule is more than skin/2 from its
+// position at the last build; the post-kick with clear_flag resets c->rebuild for the next step.
+cudaError_t launch_leapfrog_pre(Context* c, double dt, double vcorr, bool skin_check = false);
+cudaError_t launch_leapfrog_post(Context* c, double dt_half, bool clear_flag = false);   // scalars[3] = sum m v^2
 cudaError_t launch_scale(Context* c, double beta);
 cudaError_t launch_reduce(Context* c, int64_t nblocks, double* out, int nval);
 cudaError_t launch_adjoint(Context* c, const double* gfx, const double* gfy, const double* gfz, double gU, double* ox,

@@ -1,5 +1,12 @@
-// Single-box pair kernel: one CTA per brick of 2x2x2 linked cells (the per-brick work is
-// brick::pairs in brick.cuh, which also documents the staging, filter and compute passes).
+// Single-box pair kernels: one CTA per brick of 2x2x2 linked cells (the per-brick work is in
+// brick.cuh, which also documents the staging, filter and compute passes).
+//
+//   k_pairs_brick  filter + exact evaluation every call (the drop-in traversal)
+//   k_build_lists  Verlet-skin mode, build step: each molecule's candidates within rc + skin
+//   k_pairs_list   Verlet-skin mode, every step: exact evaluation of the lists at the current
+//                  positions
+// In the Verlet-skin mode the build is launched every step and returns at once unless a device flag
+// (set by the Leapfrog pre-kick when a molecule moved more than skin/2 since the build) is set.
 #include <cuda_runtime.h>
 
 #include "brick.cuh"
@@ -16,7 +23,8 @@ __global__ void __launch_bounds__(brick::kThreads, 2)
                   const double* __restrict__ rz, const int32_t* __restrict__ cid,
                   const int32_t* __restrict__ cstart, const PairParams* __restrict__ pp,
                   double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
-                  double* __restrict__ partials, int* __restrict__ status) {
+                  double* __restrict__ partials, int* __restrict__ status, const int* __restrict__ gate,
+                  brick::Lists lists) {
 	extern __shared__ __align__(16) unsigned char smem[];
 	brick::load_params(smem, brick::layout(p.s_cap, kFP64, kListCap), pp, p.ns);
 	__syncthreads();
@@ -24,43 +32,133 @@ __global__ void __launch_bounds__(brick::kThreads, 2)
 	                                                fy, fz, partials, status);
 }
 
-}  // namespace
+// Verlet-skin build step (runs only when *gate != 0): the lists, no forces.
+__global__ void __launch_bounds__(brick::kThreads, 3)
+    k_build_lists(brick::Box bx, int s_cap, const double* __restrict__ rx, const double* __restrict__ ry,
+                  const double* __restrict__ rz, const int32_t* __restrict__ cstart, const int* __restrict__ gate,
+                  brick::Lists lists) {
+	if (*gate == 0) return;
+	extern __shared__ __align__(16) unsigned char smem[];
+	brick::build_lists(bx, blockIdx.x, s_cap, smem, rx, ry, rz, cstart, lists);
+}
 
-cudaError_t launch_pairs_brick(Context* c) {
+template <bool kFP64, bool kSingle, bool kLjIsRc>
+__global__ void __launch_bounds__(brick::kThreads, 2)
+    k_pairs_list(brick::Const p, brick::Box bx, const double* __restrict__ rx, const double* __restrict__ ry,
+                 const double* __restrict__ rz, const int32_t* __restrict__ cid,
+                 const int32_t* __restrict__ cstart, const PairParams* __restrict__ pp,
+                 double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
+                 double* __restrict__ partials, int* __restrict__ status, const int* __restrict__ gate,
+                 brick::Lists lists) {
+	extern __shared__ __align__(16) unsigned char smem[];
+	brick::load_params(smem, brick::layout(p.s_cap, kFP64, 0, false), pp, p.ns);
+	__syncthreads();
+	brick::list_pairs<kFP64, kSingle, kLjIsRc>(p, bx, blockIdx.x, blockIdx.x, smem, rx, ry, rz, cid, cstart, fx,
+	                                           fy, fz, partials, status, lists);
+}
+
+struct Plan {
+	brick::Const p;
+	brick::Box bx;
+	size_t bytes;
+	int nbricks;
+};
+
+// kind 0: plain traversal, 2: list evaluation of the skin mode (two CTAs per SM).
+Plan plan(Context* c, const Grid& g, double filter_radius, int kind) {
 	const bool fp64 = c->precision == MDGPU_FP64;
-	brick::Box bx{};
-	brick::init_box(bx, c->g, c->rc, 0);
-	// shared-memory capacity: two CTAs per SM
+	Plan P;
+	brick::init_box(P.bx, g, filter_radius, 0, kind == 0 ? 0.0 : 0.5 * c->skin);
 	static int max_optin = -1;
 	if (max_optin < 0) cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
 	size_t budget = 110 * 1024;
 	if (budget > (size_t) max_optin) budget = (size_t) max_optin;
-	const int s_cap = brick::capacity_for(budget, fp64, kListCap);
-	const brick::Const p = brick::make_const(c->sp.n, s_cap, c->rc, c->rc_lj);
-	const size_t bytes = brick::layout(s_cap, fp64, kListCap).total;
-	const int nbricks = bx.nb[0] * bx.nb[1] * bx.nb[2];
+	const int lcap = kind == 2 ? 0 : kListCap;
+	const bool half = kind != 2;
+	const int s_cap = brick::capacity_for(budget, fp64, lcap, half);
+	P.p = brick::make_const(c->sp.n, s_cap, c->rc, c->rc_lj);
+	P.bytes = brick::layout(s_cap, fp64, lcap, half).total;
+	P.nbricks = P.bx.nb[0] * P.bx.nb[1] * P.bx.nb[2];
+	return P;
+}
+
+template <typename K>
+cudaError_t go(Context* c, const Plan& P, K kern, const int* gate, const brick::Lists& lists) {
+	cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) P.bytes);
+	if (r == cudaSuccess)
+		kern<<<P.nbricks, brick::kThreads, P.bytes, c->stream>>>(P.p, P.bx, c->p.rx, c->p.ry, c->p.rz, c->p.cid,
+		                                                         c->cell_start, c->d_pp, c->p.fx, c->p.fy, c->p.fz,
+		                                                         c->partials, c->status, gate, lists);
+	return r;
+}
+
+// kind 0: plain traversal, 2: list evaluation of the skin mode
+template <int kKind>
+cudaError_t dispatch(Context* c, const Plan& P, const int* gate, const brick::Lists& lists) {
+	const bool fp64 = c->precision == MDGPU_FP64;
+	const bool single = c->sp.n == 1, ljrc = c->rc_lj == c->rc;
+	if (kKind == 2) {
+		if (fp64) return single ? go(c, P, k_pairs_list<true, true, false>, gate, lists)
+		                        : go(c, P, k_pairs_list<true, false, false>, gate, lists);
+		if (ljrc) return single ? go(c, P, k_pairs_list<false, true, true>, gate, lists)
+		                        : go(c, P, k_pairs_list<false, false, true>, gate, lists);
+		return single ? go(c, P, k_pairs_list<false, true, false>, gate, lists)
+		              : go(c, P, k_pairs_list<false, false, false>, gate, lists);
+	}
+	if (fp64) return single ? go(c, P, k_pairs_brick<true, true, false>, gate, lists)
+	                        : go(c, P, k_pairs_brick<true, false, false>, gate, lists);
+	if (ljrc) return single ? go(c, P, k_pairs_brick<false, true, true>, gate, lists)
+	                        : go(c, P, k_pairs_brick<false, false, true>, gate, lists);
+	return single ? go(c, P, k_pairs_brick<false, true, false>, gate, lists)
+	              : go(c, P, k_pairs_brick<false, false, false>, gate, lists);
+}
+
+brick::Lists lists_of(Context* c) {
+	brick::Lists l{};
+	l.nbr = c->nbr;
+	l.count = c->nbr_count;
+	l.rx_ref = c->r_ref;
+	l.ry_ref = c->r_ref + c->n;
+	l.rz_ref = c->r_ref + 2 * c->n;
+	l.n = c->n;
+	l.cap = c->list_cap;
+	l.builds = c->builds;
+	return l;
+}
+
+}  // namespace
+
+cudaError_t launch_pairs_brick(Context* c) {
+	const Plan P = plan(c, c->g, c->rc, 0);
 	prof_begin(c, 1);
-	cudaError_t e;
-	const bool single = c->sp.n == 1;
-	auto go = [&](auto kern) {
-		cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bytes);
-		if (r == cudaSuccess)
-			kern<<<nbricks, brick::kThreads, bytes, c->stream>>>(p, bx, c->p.rx, c->p.ry, c->p.rz, c->p.cid,
-			                                                     c->cell_start, c->d_pp, c->p.fx, c->p.fy, c->p.fz,
-			                                                     c->partials, c->status);
-		return r;
-	};
-	const bool ljrc = c->rc_lj == c->rc;
-	if (fp64)
-		e = single ? go(k_pairs_brick<true, true, false>) : go(k_pairs_brick<true, false, false>);
-	else if (ljrc)
-		e = single ? go(k_pairs_brick<false, true, true>) : go(k_pairs_brick<false, false, true>);
-	else
-		e = single ? go(k_pairs_brick<false, true, false>) : go(k_pairs_brick<false, false, false>);
+	cudaError_t e = dispatch<0>(c, P, nullptr, brick::Lists{});
 	if (e == cudaSuccess) e = cudaGetLastError();
 	prof_end(c, 1, 1);
 	if (e != cudaSuccess) return e;
-	return launch_reduce(c, nbricks, c->scalars, 3);
+	return launch_reduce(c, P.nbricks, c->scalars, 3);
+}
+
+cudaError_t launch_pairs_skin(Context* c) {
+	const brick::Lists l = lists_of(c);
+	prof_begin(c, 1);
+	// build (gated): half-precision staging only, three CTAs per SM
+	brick::Box bb{};
+	brick::init_box(bb, c->gs, c->rc + c->skin, 0, 0.5 * c->skin);
+	int s_cap = 256;
+	while (brick::build_bytes(s_cap + 64) <= 64 * 1024) s_cap += 64;
+	const size_t bbytes = brick::build_bytes(s_cap);
+	const int nbricks = bb.nb[0] * bb.nb[1] * bb.nb[2];
+	cudaError_t e = cudaFuncSetAttribute(k_build_lists, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bbytes);
+	if (e == cudaSuccess)
+		k_build_lists<<<nbricks, brick::kThreads, bbytes, c->stream>>>(bb, s_cap, c->p.rx, c->p.ry, c->p.rz,
+		                                                              c->cell_start, c->rebuild, l);
+	// evaluation, every step
+	const Plan P = plan(c, c->gs, c->rc, 2);
+	if (e == cudaSuccess) e = dispatch<2>(c, P, nullptr, l);
+	if (e == cudaSuccess) e = cudaGetLastError();
+	prof_end(c, 1, 2);
+	if (e != cudaSuccess) return e;
+	return launch_reduce(c, P.nbricks, c->scalars, 3);
 }
 
 }  // namespace mdgpu

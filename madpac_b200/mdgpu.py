@@ -70,6 +70,8 @@ SIGNATURES = {
     "mdgpu_synchronize": (_I, [_VP]),
     "mdgpu_forces_noalloc": (_I, [_I, _VP, _I64, _VP, _VP, _VP, _D, _D, _I, _VP, _VP, _I, _VP, _VP, _VP,
                                   ctypes.c_char_p, _I]),
+    "mdgpu_set_skin": (_I, [_VP, _D]),
+    "mdgpu_skin_builds": (_I, [_VP, _VP]),
     "mdgpu_batch_create": (_I, [ctypes.POINTER(_VP), _I32, _VP, _VP, _D, _D, _D, _I, _VP, _VP, _I, _I]),
     "mdgpu_batch_destroy": (_I, [_VP]),
     "mdgpu_batch_last_error": (ctypes.c_char_p, [_VP]),
@@ -391,6 +393,17 @@ class LinkedCells:
 
     def setPrecision(self, precision: int) -> None:
         self._check(self.lib.mdgpu_set_precision(self.h, int(precision)))
+
+    def setSkin(self, skin: float) -> None:
+        """Verlet-skin mode of step/run (0 = off): candidate lists of radius rc + skin rebuilt on the
+        device when a molecule moved more than skin/2; exact cutoff test on every pair."""
+        self._check(self.lib.mdgpu_set_skin(self.h, float(skin)))
+
+    def skinBuilds(self) -> int:
+        """List builds of the Verlet-skin mode so far."""
+        b = ctypes.c_int64()
+        self._check(self.lib.mdgpu_skin_builds(self.h, ctypes.byref(b)))
+        return b.value
 
     # -- integrator primitives -------------------------------------------------------------------
     def leapfrogPre(self, dt: float, vcorr: float) -> None:
