@@ -88,7 +88,7 @@ __host__ __device__ inline SmemLayout layout(int s_cap, bool fp64, int list_cap,
 	SmemLayout L;
 	size_t o = 0;
 	L.hi = o;
-	o = align16(o + sizeof(float4) * s_cap);
+	o = align16(o + sizeof(float4) * (s_cap + 1));   // + the far-away sentinel slot of the list kernel
 	L.lo = o;
 	L.img = o;
 	if (fp64) o = align16(o + sizeof(double) * 3 * s_cap);
@@ -330,6 +330,28 @@ __device__ __forceinline__ bool stage(const Const& p, const Box& bx, int brick, 
 	return staged;
 }
 
+// Cutoff decision for a pair within a few ulp of rc (rare): recomputed from the FP64 positions in
+// global memory with the FP64 path's operations (xi - (x_j + shift), sum of squares), so that the
+// mixed mode evaluates exactly the pairs the FP64 mode evaluates. j is a staged slot; its cell is
+// found by bisection of the staged-cell starts.
+static __device__ __noinline__ bool exact_cut(const Smem& S, double rc2, int j, int gi, const double* rx, const double* ry,
+                                       const double* rz) {
+	int lo = 0, hi = 63;
+	while (lo < hi) {
+		const int mid = (lo + hi + 1) >> 1;
+		if (S.cs[mid] <= j)
+			lo = mid;
+		else
+			hi = mid - 1;
+	}
+	const int gj = S.gst[lo] + (j - S.cs[lo]);
+	const double d0 = __dsub_rn(rx[gi], __dadd_rn(rx[gj], S.csh[3 * lo]));
+	const double d1 = __dsub_rn(ry[gi], __dadd_rn(ry[gj], S.csh[3 * lo + 1]));
+	const double d2 = __dsub_rn(rz[gi], __dadd_rn(rz[gj], S.csh[3 * lo + 2]));
+	const double dd = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+	return dd < rc2;
+}
+
 // One list entry j of molecule i in FP32 with FP64-ready accumulators (branch-free: an invalid
 // entry, v = false, or a pair outside the cutoff contributes zeros; the rare pairs within a few ulp
 // of rc are decided in double from the same hi/lo parts).
@@ -337,21 +359,15 @@ template <bool kSingle, bool kLjIsRc>
 __device__ __forceinline__ void lj32(const Const& p, bool v, const float4& hi_i, const float3& lo_i, int ti, int ns,
                                      const float4 hj, const Box& bx, const float* pf, float eps24_1, float sig2_1,
                                      float shift6_1, float& ax, float& ay, float& az, float& au, float& aw, int& anp,
-                                     bool& same) {
+                                     bool& same, const Smem& S, int j, int gi, const double* rx, const double* ry,
+                                     const double* rz) {
 	const float3 lj = unpack_lo(__float_as_uint(hj.w), bx);
 	const float h0 = hi_i.x - hj.x, h1 = hi_i.y - hj.y, h2 = hi_i.z - hj.z;  // exact
 	const float e0 = h0 + (lo_i.x - lj.x), e1 = h1 + (lo_i.y - lj.y), e2 = h2 + (lo_i.z - lj.z);
 	const float d2f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2));
 	bool in = v && d2f < p.rc2f;
 	const bool amb = v && fabsf(d2f - p.rc2f) <= p.band;
-	if (__any_sync(kFull, amb)) {
-		if (amb) {
-			const double a0 = (double) h0 + ((double) lo_i.x - (double) lj.x);
-			const double a1 = (double) h1 + ((double) lo_i.y - (double) lj.y);
-			const double a2 = (double) h2 + ((double) lo_i.z - (double) lj.z);
-			in = a0 * a0 + a1 * a1 + a2 * a2 < p.rc2;
-		}
-	}
+	if (amb) in = exact_cut(S, p.rc2, j, gi, rx, ry, rz);
 	anp += in ? 1 : 0;
 	same |= in && d2f == 0.f;
 	const bool lj_in = kLjIsRc ? in : (in && d2f < p.rclj2f);
@@ -414,6 +430,7 @@ struct Lists {
 	int64_t n;
 	int cap;
 	unsigned long long* builds;        // incremented once per build
+	int sentinel;                      // staged slot of the list kernel's far-away sentinel
 };
 constexpr unsigned short kListOverflow = 0xffff;
 
@@ -486,7 +503,7 @@ __device__ __forceinline__ void pairs(const Const& p, const Box& bx, int brick, 
 				const bool v = tt < cnt;
 				const int j = v ? (int) mylist[tt * 32] : slot_i;
 				lj32<kSingle, kLjIsRc>(p, v, hi_i, lo_i, ti, ns, s_hi[j], bx, s_pf, eps24_1, sig2_1, shift6_1, ax, ay, az,
-				                       au, aw, anp, same);
+				                       au, aw, anp, same, S, j, gi, rx, ry, rz);
 			};
 			auto pair_fp64 = [&](int tt, double& ax, double& ay, double& az, double& au, double& aw, int& anp) {
 				if (tt >= cnt) return;
@@ -715,6 +732,9 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 					}
 				}
 				if (act) {
+					// pad the last block of 8 with the list kernel's sentinel slot
+					for (int k = cntg; k < ((cntg + 7) & ~7) && k < lists.cap; k++)
+						lists.nbr[(((int64_t) (k >> 3) * lists.n + gi) << 3) + (k & 7)] = (unsigned short) lists.sentinel;
 					lists.count[gi] = cntg <= lists.cap ? (unsigned short) cntg : kListOverflow;
 					lists.rx_ref[gi] = rx[gi];
 					lists.ry_ref[gi] = ry[gi];
@@ -743,6 +763,8 @@ __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int br
 	const bool staged = stage<kFP64, false>(p, bx, brick, S, rx, ry, rz, cid, cstart);
 	__shared__ int s_own[9], s_ocell[8];
 	if (tid == 0) {
+		// sentinel slot: far from every molecule (entries past a list's end point to it)
+		S.hi[p.s_cap] = make_float4(1e15f, 1e15f, 1e15f, __uint_as_float((256u << 18) | (256u << 9) | 256u));
 		int acc = 0;
 		for (int w = 0; w < 8; w++) {
 			int ic;
@@ -832,29 +854,135 @@ __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int br
 				U += au[0] + au[1];
 				W = __dadd_rn(W, __dadd_rn(aw[0], aw[1]));
 			} else {
+				// FP32, branch-free. Per coordinate e = fma(m_i - m_j, step, hi_i - hi_j) with m = 2^23 +
+				// the 9-bit lo field (exact integer difference, one rounding). Single-species runs sum
+				// fac/eps24, s6 (s6 - 1) and s6 (2 s6 - 1) and apply eps24 and shift6 per molecule.
+				const unsigned wi = __float_as_uint(hi_i.w);
+				const float mix = __uint_as_float(0x4B000000u | (wi & 511u));
+				const float miy = __uint_as_float(0x4B000000u | ((wi >> 9) & 511u));
+				const float miz = __uint_as_float(0x4B000000u | ((wi >> 18) & 511u));
+				const int nblk = (cnt + 7) >> 3;
+				const unsigned sent2 = (unsigned) p.s_cap | ((unsigned) p.s_cap << 16);
 				float ax[4] = {0.f, 0.f, 0.f, 0.f}, ay[4] = {0.f, 0.f, 0.f, 0.f}, az[4] = {0.f, 0.f, 0.f, 0.f};
 				float au[4] = {0.f, 0.f, 0.f, 0.f}, aw[4] = {0.f, 0.f, 0.f, 0.f};
+				int nlj = 0;   // pairs inside the LJ cutoff (shift6 terms)
+				// one pair in FP32 with the given cutoff decision; sign +1 adds it, -1 removes it
+				auto pair32 = [&](int j, bool in, float sign) {
+					const float4 hj = S.hi[j];
+					const unsigned wj = __float_as_uint(hj.w);
+					const float e0 = fmaf(mix - __uint_as_float(0x4B000000u | (wj & 511u)), bx.lo_step[0], hi_i.x - hj.x);
+					const float e1 = fmaf(miy - __uint_as_float(0x4B000000u | ((wj >> 9) & 511u)), bx.lo_step[1], hi_i.y - hj.y);
+					const float e2 = fmaf(miz - __uint_as_float(0x4B000000u | ((wj >> 18) & 511u)), bx.lo_step[2], hi_i.z - hj.z);
+					const float d2f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2));
+					const bool lj_in = kLjIsRc ? in : (in && d2f < p.rclj2f);
+					anp += in ? (int) sign : 0;
+					if (!kLjIsRc) nlj += lj_in ? (int) sign : 0;
+					const float inv = lj_in ? rcp_approx(d2f) : 0.f;
+					float eps24 = 1.f, sig2 = sig2_1, shift6 = 0.f;
+					if (!kSingle) {
+						const int pk = ti * ns + unpack_cid(wj);
+						eps24 = S.pf[pk];
+						sig2 = S.pf[KK + pk];
+						shift6 = S.pf[2 * KK + pk];
+					}
+					const float s2 = sig2 * inv;
+					const float s6 = s2 * s2 * s2;
+					const float r = eps24 * (s6 * fmaf(2.f, s6, -1.f));
+					const float fac = sign * r * inv;
+					ax[0] = fmaf(fac, e0, ax[0]);
+					ay[0] = fmaf(fac, e1, ay[0]);
+					az[0] = fmaf(fac, e2, az[0]);
+					au[0] += sign * (fmaf(eps24 * s6, s6 - 1.f, 0.f) + (lj_in ? shift6 : 0.f));
+					aw[0] += sign * r;
+				};
 				for (int b = 0; b < nb8; b++) {
-					const uint4 cur = nxt;
+					uint4 cur = nxt;
 					if (b + 1 < nb8) nxt = my8[(int64_t) (b + 1) * lists.n];
+					if (b >= nblk) cur = make_uint4(sent2, sent2, sent2, sent2);
 					const unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
+					unsigned ambm = 0u;
 #pragma unroll
 					for (int u = 0; u < 8; u++) {
-						const int kk = 8 * b + u;
-						const bool v = kk < cnt;
-						const int j = v ? min((int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu), p.s_cap - 1) : slot_i;
-						lj32<kSingle, kLjIsRc>(p, v, hi_i, lo_i, ti, ns, S.hi[j], bx, S.pf, eps24_1, sig2_1, shift6_1,
-						                       ax[u & 3], ay[u & 3], az[u & 3], au[u & 3], aw[u & 3], anp, same);
+						const int j = (int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu);
+						const float4 hj = S.hi[j];
+						const unsigned wj = __float_as_uint(hj.w);
+						const float h0 = hi_i.x - hj.x, h1 = hi_i.y - hj.y, h2 = hi_i.z - hj.z;  // exact
+						const float g0 = mix - __uint_as_float(0x4B000000u | (wj & 511u));
+						const float g1 = miy - __uint_as_float(0x4B000000u | ((wj >> 9) & 511u));
+						const float g2 = miz - __uint_as_float(0x4B000000u | ((wj >> 18) & 511u));
+						const float e0 = fmaf(g0, bx.lo_step[0], h0);
+						const float e1 = fmaf(g1, bx.lo_step[1], h1);
+						const float e2 = fmaf(g2, bx.lo_step[2], h2);
+						const float d2f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2));
+						const bool in = d2f < p.rc2f;
+						// within a few ulp of rc: decided after the block as the FP64 computation does
+						ambm |= fabsf(d2f - p.rc2f) <= p.band ? (1u << u) : 0u;
+						anp += in ? 1 : 0;
+						const bool lj_in = kLjIsRc ? in : (in && d2f < p.rclj2f);
+						if (!kLjIsRc) nlj += lj_in ? 1 : 0;
+						const float inv = lj_in ? rcp_approx(d2f) : 0.f;
+						if (kSingle) {
+							const float s2 = sig2_1 * inv;
+							const float s6 = s2 * s2 * s2;
+							const float r = s6 * fmaf(2.f, s6, -1.f);
+							const float facp = r * inv;
+							ax[u & 3] = fmaf(facp, e0, ax[u & 3]);
+							ay[u & 3] = fmaf(facp, e1, ay[u & 3]);
+							az[u & 3] = fmaf(facp, e2, az[u & 3]);
+							au[u & 3] = fmaf(s6, s6 - 1.f, au[u & 3]);
+							aw[u & 3] += r;
+						} else {
+							const int pk = ti * ns + unpack_cid(wj);
+							const float eps24 = S.pf[pk], sig2 = S.pf[KK + pk], shift6 = S.pf[2 * KK + pk];
+							const float s2 = sig2 * inv;
+							const float s6 = s2 * s2 * s2;
+							const float r = eps24 * (s6 * fmaf(2.f, s6, -1.f));
+							const float fac = r * inv;
+							ax[u & 3] = fmaf(fac, e0, ax[u & 3]);
+							ay[u & 3] = fmaf(fac, e1, ay[u & 3]);
+							az[u & 3] = fmaf(fac, e2, az[u & 3]);
+							au[u & 3] = fmaf(eps24 * s6, s6 - 1.f, au[u & 3]) + (lj_in ? shift6 : 0.f);
+							aw[u & 3] += r;
+						}
+					}
+					if (__any_sync(kFull, ambm != 0u)) {
+						// rare: pairs within a few ulp of rc whose FP64 decision differs from the FP32 one
+						while (ambm) {
+							const int u = __ffs(ambm) - 1;
+							ambm &= ambm - 1u;
+							const int j = (int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu);
+							const float4 hj = S.hi[j];
+							const unsigned wj = __float_as_uint(hj.w);
+							const float e0 = fmaf(mix - __uint_as_float(0x4B000000u | (wj & 511u)), bx.lo_step[0], hi_i.x - hj.x);
+							const float e1 = fmaf(miy - __uint_as_float(0x4B000000u | ((wj >> 9) & 511u)), bx.lo_step[1], hi_i.y - hj.y);
+							const float e2 = fmaf(miz - __uint_as_float(0x4B000000u | ((wj >> 18) & 511u)), bx.lo_step[2], hi_i.z - hj.z);
+							const bool in_f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2)) < p.rc2f;
+							const bool in_d = exact_cut(S, p.rc2, j, gi, rx, ry, rz);
+							if (in_f != in_d) pair32(j, true, in_d ? 1.f : -1.f);
+						}
 					}
 					if ((b & 7) == 7 || b + 1 == nb8) {
 						// fold the FP32 partial sums of up to 64 entries into the FP64 accumulators
-						Fx += ((double) ax[0] + (double) ax[1]) + ((double) ax[2] + (double) ax[3]);
-						Fy += ((double) ay[0] + (double) ay[1]) + ((double) ay[2] + (double) ay[3]);
-						Fz += ((double) az[0] + (double) az[1]) + ((double) az[2] + (double) az[3]);
-						U += ((double) au[0] + (double) au[1]) + ((double) au[2] + (double) au[3]);
-						W += ((double) aw[0] + (double) aw[1]) + ((double) aw[2] + (double) aw[3]);
+						const double sc = kSingle ? (double) eps24_1 : 1.0;
+						Fx += sc * (((double) ax[0] + (double) ax[1]) + ((double) ax[2] + (double) ax[3]));
+						Fy += sc * (((double) ay[0] + (double) ay[1]) + ((double) ay[2] + (double) ay[3]));
+						Fz += sc * (((double) az[0] + (double) az[1]) + ((double) az[2] + (double) az[3]));
+						U += sc * (((double) au[0] + (double) au[1]) + ((double) au[2] + (double) au[3]));
+						W += sc * (((double) aw[0] + (double) aw[1]) + ((double) aw[2] + (double) aw[3]));
 #pragma unroll
 						for (int u = 0; u < 4; u++) ax[u] = ay[u] = az[u] = au[u] = aw[u] = 0.f;
+					}
+				}
+				if (kSingle) U += (double) shift6_1 * (double) (kLjIsRc ? anp : nlj);
+				if (!(Fx == Fx && Fy == Fy && Fz == Fz) && act && !ovf) {
+					// a zero distance gives 0 * inf: report it as the reference does (same position)
+					for (int k = 0; k < cnt; k++) {
+						const int j = lists.nbr[(((int64_t) (k >> 3) * lists.n + gi) << 3) + (k & 7)];
+						const float4 hj = S.hi[min(j, p.s_cap)];
+						const unsigned pos_bits = (1u << 27) - 1u;   // the lo fields, not the component id
+						if (hj.x == hi_i.x && hj.y == hi_i.y && hj.z == hi_i.z &&
+						    ((__float_as_uint(hj.w) ^ wi) & pos_bits) == 0u && j != slot_i)
+							same = true;
 					}
 				}
 			}

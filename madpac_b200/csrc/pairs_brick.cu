@@ -139,7 +139,9 @@ cudaError_t launch_pairs_brick(Context* c) {
 }
 
 cudaError_t launch_pairs_skin(Context* c) {
-	const brick::Lists l = lists_of(c);
+	brick::Lists l = lists_of(c);
+	const Plan P = plan(c, c->gs, c->rc, 2);
+	l.sentinel = P.p.s_cap;
 	prof_begin(c, 1);
 	// build (gated): half-precision staging only, three CTAs per SM
 	brick::Box bb{};
@@ -153,7 +155,6 @@ cudaError_t launch_pairs_skin(Context* c) {
 		k_build_lists<<<nbricks, brick::kThreads, bbytes, c->stream>>>(bb, s_cap, c->p.rx, c->p.ry, c->p.rz,
 		                                                              c->cell_start, c->rebuild, l);
 	// evaluation, every step
-	const Plan P = plan(c, c->gs, c->rc, 2);
 	if (e == cudaSuccess) e = dispatch<2>(c, P, nullptr, l);
 	if (e == cudaSuccess) e = cudaGetLastError();
 	prof_end(c, 1, 2);
