@@ -27,7 +27,7 @@ import numpy as np  # noqa: E402
 
 METRIC = "LJ pair-interactions/s, 1M atoms, 1 B200: FP32/FP64-acc vs FP64 at ≤1e-5 err"
 UNIT = "pair-interactions/s"
-FLOPS_PER_PAIR = 31  # algorithmic flops per interacting pair (FMA = 2): see DESIGN.md
+FLOPS_PER_PAIR = 31  # algorithmic flops per unordered pair within rc (FMA = 2): dr 3, r^2 5, 1/r^2 1, s^2 1, s^6 2, s^12 1, s^12-s^6 1, u 2, fac 3, f 3, virial 5, U 1
 L2_FLUSH_BYTES = 256 << 20
 
 

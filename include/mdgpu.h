@@ -8,8 +8,8 @@
  * velocities and forces are (n, 3) row-major doubles. Component ids are 0-based.
  *
  * Reference interfaces (paths relative to madpac/mardyn/) each entry point replaces are named
- * beside it. The shim in madpac_b200/shim/ binds them to MarDyn's ParticleContainer and
- * Integrator classes.
+ * beside it. A thin C++ shim (a ParticleContainer and an Integrator subclass on the MarDyn side)
+ * binds them to MarDyn's simulation loop.
  */
 #ifndef MDGPU_H
 #define MDGPU_H
