@@ -28,7 +28,6 @@ import numpy as np  # noqa: E402
 METRIC = "LJ pair-interactions/s, 1M atoms, 1 B200: FP32/FP64-acc vs FP64 at ≤1e-5 err"
 UNIT = "pair-interactions/s"
 FLOPS_PER_PAIR = 31  # algorithmic flops per unordered pair within rc (FMA = 2): dr 3, r^2 5, 1/r^2 1, s^2 1, s^6 2, s^12 1, s^12-s^6 1, u 2, fac 3, f 3, virial 5, U 1
-L2_FLUSH_BYTES = 256 << 20
 
 
 def parse():
@@ -72,7 +71,8 @@ def workload_config(system, precision, skin=0.0):
             "pair_search": (f"candidate lists of radius rc + {skin} rebuilt (with the binning) when a molecule moved "
                             f"more than {skin / 2:g} since the last build; exact r^2 < rc^2 test on every pair")
             if skin > 0 else "cells rebuilt and candidates searched every step",
-            "l2": "flushed (256 MiB write) before every timed step"}
+            "l2": "not flushed: each step reads the whole state (molecule arrays and candidate lists, "
+                  "several times the 126 MB L2); the timed steps run as one mdgpu_run_async"}
 
 
 # ---------------------------------------------------------------------------- distributed plumbing
@@ -182,43 +182,34 @@ def make_system(rank: int, fcc_cells: int = 64, workload: str = "c2"):
     return W.lj_fcc_box(fcc_cells, 0.75, 0.9, 2 + rank, 3.0, [W.Component(1.0, 1.0, 1.0, True)])
 
 
-def time_device_resident(M, lc, system, steps, warmup, flush, stream):
-    """Device-resident steps: inputs in HBM, L2 flushed before every step, CUDA events on the
-    library's stream around each step. Returns (seconds, pairs, records, launches)."""
+def time_device_resident(M, lc, system, steps, warmup, stream):
+    """Device-resident steps: inputs in HBM, all `steps` steps enqueued as one mdgpu_run_async
+    (consecutive steps share the kick between them), CUDA events on the library's stream around
+    them. No L2 flush: every step reads the whole state (molecule arrays and candidate lists,
+    several times the 126 MB L2). Returns (seconds, pairs, records, launches)."""
     import torch
 
     dt = system.dt
-    for _ in range(warmup):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        lc.runAsync(1, dt)
+    lc.runAsync(warmup, dt)
     lc.readSteps(warmup)
     launches0 = lc.profileRead()[1][3]
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
-    for k in range(steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-            ev[k][0].record(stream)
-        lc.runAsync(1, dt)
-        ev[k][1].record(stream)
+    e0.record(stream)
+    lc.runAsync(steps, dt)
+    e1.record(stream)
     rec = lc.readSteps(steps)
     torch.cuda.synchronize()
     launches = int(lc.profileRead()[1][3] - launches0)
-    seconds = sum(a.elapsed_time(b) for a, b in ev) * 1e-3
+    seconds = e0.elapsed_time(e1) * 1e-3
     return seconds, float(rec[:, 3].sum()), rec, launches
 
 
-def time_kernels(lc, system, steps, flush, stream):
+def time_kernels(lc, system, steps):
     """Per-kernel-group device time (CUDA events on the library's stream) over `steps` steps."""
-    import torch
-
     lc.profileRead(reset=True)
     lc.profileEnable(True)
-    for _ in range(steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        lc.runAsync(1, system.dt)
+    lc.runAsync(steps, system.dt)
     rec = lc.readSteps(steps)
     t, cnt = lc.profileRead(reset=True)
     lc.profileEnable(False)
@@ -309,12 +300,11 @@ def run_ours(args, dist: Dist):
     lc.traversePairs()
     lc.setSkin(args.skin)
     stream = torch.cuda.ExternalStream(lc.stream())
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{dist.local}")
 
     dist.barrier()
     clocks = ClockSampler(dist.local)
     clocks.start()
-    seconds, pairs, rec, launches = time_device_resident(M, lc, system, args.steps, args.warmup, flush, stream)
+    seconds, pairs, rec, launches = time_device_resident(M, lc, system, args.steps, args.warmup, stream)
     clk = clocks.stop()
     dist.barrier()
     t_max = dist.max(seconds)
@@ -322,7 +312,7 @@ def run_ours(args, dist: Dist):
     value = pairs_all / t_max
 
     # kernel-level timing for the roofline (separate, profiled pass)
-    tk, cnt, rec2 = time_kernels(lc, system, args.steps, flush, stream)
+    tk, cnt, rec2 = time_kernels(lc, system, args.steps)
     pair_ms = tk[1] / args.steps   # all pair launches of a step (the build is gated off in most steps)
     pairs_per_launch = float(rec2[:, 3].mean())
     fp32_peak, fp64_peak = M.device_peaks(dist.local)
@@ -384,7 +374,7 @@ def run_ours(args, dist: Dist):
             x.update()
             x.traversePairs()
             x.setSkin(skin)
-            s2, p2, _, _ = time_device_resident(M, x, system, csteps, args.warmup, flush,
+            s2, p2, _, _ = time_device_resident(M, x, system, csteps, args.warmup,
                                                 torch.cuda.ExternalStream(x.stream()))
             x.close()
             return {"value": p2 / s2, "ms_per_step": s2 / csteps * 1e3, "steps": csteps, "verlet_skin": skin}

@@ -77,6 +77,8 @@ __global__ void k_store_refcell(int64_t n, const int32_t* __restrict__ cell, con
 	out[uidx[s]] = ((int64_t) (iz + 1) * cy + (iy + 1)) * cx + (ix + 1);
 }
 
+__global__ void k_set_int(int* p, int v) { *p = v; }
+
 __global__ void k_iota(int64_t n, int32_t* __restrict__ a) {
 	int64_t s = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (s < n) a[s] = (int32_t) s;
@@ -109,7 +111,12 @@ int check_status(Context* c) {
 		return fail(c, MDGPU_ERR_OUTSIDE_HALO, "a molecule is outside the halo box (moved more than one cell in a step)");
 	if (st & kStatusSamePosition) return fail(c, MDGPU_ERR_SAME_POSITION, "two molecules have the same position");
 	if (st & kStatusNonFinite) return fail(c, MDGPU_ERR_NONFINITE, "non-finite force or velocity");
-	if (st & kStatusTimeout) return fail(c, MDGPU_ERR_TIMEOUT, "a bounded device wait gave up");
+	if (st & kStatusTimeout) {
+		// the cooperative rebuild's barrier words may be left mid-count: start them again
+		if (c->bar) MD_CUDA(cudaMemsetAsync(c->bar, 0, sizeof(unsigned) * 4, c->stream));
+		c->lists_valid = false;
+		return fail(c, MDGPU_ERR_TIMEOUT, "a bounded device wait gave up");
+	}
 	if (st & kStatusCapacity) return fail(c, MDGPU_ERR_CAPACITY, "a device buffer is too small for the workload");
 	return fail(c, MDGPU_ERR_CUDA, "unknown device status");
 }
@@ -400,6 +407,8 @@ int mdgpu_destroy(mdgpu_ctx* ctx) {
 	cudaFree(c->r_ref);
 	cudaFree(c->rebuild);
 	cudaFree(c->builds);
+	cudaFree(c->bar);
+	cudaFree(c->chunk);
 	cudaFree(full->x.stage.ptr);
 	if (c->h_scalars) cudaFreeHost(c->h_scalars);
 	if (c->h_status) cudaFreeHost(c->h_status);
@@ -713,13 +722,34 @@ int skin_prepare(Context* c) {
 		c->list_cap = cap;
 		c->lists_valid = false;
 	}
+	const int64_t parts = skin_partials_needed(c);
+	if (c->partial_cap < parts) {
+		MD_CUDA(cudaStreamSynchronize(c->stream));
+		cudaFree(c->partials);
+		c->partials = nullptr;
+		MD_CUDA(cudaMalloc(&c->partials, sizeof(double) * 4 * (parts + 1024)));
+		c->partial_cap = parts + 1024;
+	}
 	if (!c->rebuild) {
 		MD_CUDA(cudaMalloc(&c->rebuild, sizeof(int)));
+		MD_CUDA(cudaMemsetAsync(c->rebuild, 0xff, sizeof(int), c->stream));
 		MD_CUDA(cudaMalloc(&c->builds, sizeof(unsigned long long)));
 		MD_CUDA(cudaMemsetAsync(c->builds, 0, sizeof(unsigned long long), c->stream));
+		MD_CUDA(cudaMalloc(&c->bar, sizeof(unsigned) * 4));
+		MD_CUDA(cudaMemsetAsync(c->bar, 0, sizeof(unsigned) * 4, c->stream));
+		c->chunk_cap = 8192;
+		MD_CUDA(cudaMalloc(&c->chunk, sizeof(int32_t) * c->chunk_cap));
 	}
+	return MDGPU_OK;
+}
+
+// Opens skin-mode step `c->step_id`: asks for a build when the lists do not fit the sort order.
+int skin_open_step(Context* c) {
+	c->step_id++;
 	if (!c->lists_valid) {
-		MD_CUDA(cudaMemsetAsync(c->rebuild, 0xff, sizeof(int), c->stream));
+		k_set_int<<<1, 1, 0, c->stream>>>(c->rebuild, c->step_id);
+		count_launches(c, 1);
+		MD_CUDA(cudaGetLastError());
 		c->lists_valid = true;
 	}
 	return MDGPU_OK;
@@ -729,11 +759,12 @@ int skin_prepare(Context* c) {
 int enqueue_one(Context* c, double dt, double vcorr, double* dst) {
 	if (c->skin > 0.0) {
 		int st = skin_prepare(c);
+		if (!st) st = skin_open_step(c);
 		if (st) return st;
 		MD_CUDA(launch_leapfrog_pre(c, dt, vcorr, true));
-		MD_CUDA(launch_bin(c, false, c->rebuild, &c->gs));
+		MD_CUDA(launch_rebuild(c, c->gs));
 		MD_CUDA(launch_pairs_skin(c));
-		MD_CUDA(launch_leapfrog_post(c, 0.5 * dt, true));
+		MD_CUDA(launch_leapfrog_post(c, 0.5 * dt));
 	} else {
 		MD_CUDA(launch_leapfrog_pre(c, dt, vcorr));
 		MD_CUDA(launch_bin(c, false));
@@ -812,11 +843,38 @@ int enqueue_steps(Context* c, int32_t nsteps, double dt) {
 		c->steps_out = buf;
 		c->steps_cap = cap;
 	}
-	for (int k = 0; k < nsteps; k++) {
-		int st = enqueue_one(c, dt, 1.0, c->steps_out + 4 * c->steps_written);
+	if (nsteps == 0) return MDGPU_OK;
+	// the closing kick of step k and the opening kick of step k+1 run as one pass; the record of
+	// step k is written after it (its sum m v^2 comes from that pass)
+	const bool skin = c->skin > 0.0;
+	if (skin) {
+		int st = skin_prepare(c);
 		if (st) return st;
-		c->steps_written++;
 	}
+	for (int k = 0; k < nsteps; k++) {
+		if (skin) {
+			int st = skin_open_step(c);
+			if (st) return st;
+		}
+		if (k == 0) {
+			MD_CUDA(launch_leapfrog_pre(c, dt, 1.0, skin));
+		} else {
+			MD_CUDA(launch_leapfrog_post_pre(c, dt, skin));
+			MD_CUDA(launch_step_record(c, c->steps_out + 4 * c->steps_written));
+			c->steps_written++;
+		}
+		if (skin) {
+			MD_CUDA(launch_rebuild(c, c->gs));
+			MD_CUDA(launch_pairs_skin(c));
+		} else {
+			MD_CUDA(launch_bin(c, false));
+			c->lists_valid = false;
+			MD_CUDA(launch_pairs(c));
+		}
+	}
+	MD_CUDA(launch_leapfrog_post(c, 0.5 * dt));
+	MD_CUDA(launch_step_record(c, c->steps_out + 4 * c->steps_written));
+	c->steps_written++;
 	return MDGPU_OK;
 }
 }  // namespace

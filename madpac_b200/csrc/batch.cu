@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "brick.cuh"
+#include "grid_sync.cuh"
 #include "md_internal.h"
 #include "reduce.cuh"
 
@@ -72,47 +73,6 @@ struct StepArgs {
 	int integrate;              // 0: wrap, bin and forces only (initial force evaluation)
 	int dynamic;                // 0: bricks by static stride, 1: by atomic queue
 };
-
-__device__ __forceinline__ uint64_t global_ns() {
-	uint64_t t;
-	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-	return t;
-}
-
-__device__ __forceinline__ unsigned load_acquire(const unsigned* p) {
-	unsigned v;
-	asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-	return v;
-}
-
-// Grid-wide barrier with a bounded wait. Returns false (and sets the timeout status) when the wait
-// ran out; the caller then skips the rest of the launch.
-__device__ bool grid_barrier(unsigned* bar, int* status, int64_t timeout_ns, int* s_flag) {
-	__syncthreads();
-	if (threadIdx.x == 0) {
-		const unsigned gen = load_acquire(bar + 1);
-		__threadfence();
-		const unsigned arrived = atomicAdd(bar, 1u);
-		if (arrived == gridDim.x - 1) {
-			atomicExch(bar, 0u);
-			__threadfence();
-			atomicAdd(bar + 1, 1u);
-		} else {
-			const uint64_t t0 = global_ns();
-			while (load_acquire(bar + 1) == gen) {
-				__nanosleep(100);
-				if ((int64_t) (global_ns() - t0) > timeout_ns) {
-					atomicOr(status, kStatusTimeout);
-					*s_flag = 1;
-					break;
-				}
-			}
-		}
-		__threadfence();
-	}
-	__syncthreads();
-	return *s_flag == 0;
-}
 
 // Shared-memory bytes of phase A for a box of n molecules and m cells.
 __host__ __device__ inline size_t bin_bytes(int64_t n, int64_t m) {

@@ -2,18 +2,22 @@
 //
 // Per update (LinkedCells::update, particleContainer/LinkedCells.cpp:165-180, paths relative to
 // madpac/mardyn/):
-//   1. bin_cells:  periodic wrap of each coordinate (r<0 -> r+L, r>=L -> r-L: the position of the
+//   1. bin:        periodic wrap of each coordinate (r<0 -> r+L, r>=L -> r-L: the position of the
 //                  halo image that survives DomainDecompDummy::exchangeMolecules +
 //                  LinkedCells::deleteOuterParticles, parallel/DomainDecompDummy.cpp:64-70, 93-99,
 //                  LinkedCells.cpp:356-369), the cell coordinate floor((r - haloMin)/cellLength)
 //                  in IEEE double with no contraction (LinkedCells.cpp:543), and an atomic
 //                  arrival rank per cell.
-//   2. scan:       exclusive prefix sum of the cell counts (two-level).
+//   2. scan:       exclusive prefix sum of the cell counts.
 //   3. scatter:    slot = cell_start + rank (arrival order, not deterministic).
-//   4. cell_sort:  one warp per cell orders its molecules by id and gathers every field into
+//   4. cell sort:  one warp per cell orders its molecules by id and gathers every field into
 //                  the other buffer, so the final order (cell, id) does not depend on timing.
+// launch_bin runs these as separate kernels (the drop-in update). launch_rebuild runs them as one
+// cooperative kernel with bounded grid barriers that returns at once unless the Verlet-skin mode
+// asked for a build in this step.
 #include <cuda_runtime.h>
 
+#include "grid_sync.cuh"
 #include "md_internal.h"
 
 namespace mdgpu {
@@ -21,15 +25,10 @@ namespace {
 
 constexpr int kScanBlock = 1024;   // elements per scan block (256 threads x 4)
 
-__global__ void k_bin_cells(int64_t n, double* __restrict__ rx, double* __restrict__ ry,
-                            double* __restrict__ rz, Grid g, int32_t* __restrict__ cell,
-                            int32_t* __restrict__ rank, int32_t* __restrict__ count, int* status, const int* gate) {
-	if (gate && *gate == 0) return;
-	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n) return;
+// Wrap molecule i, return its inner cell and flag positions outside the halo box.
+__device__ __forceinline__ int32_t bin_one(int64_t i, double* rx, double* ry, double* rz, const Grid& g, bool& bad) {
 	double r[3] = {rx[i], ry[i], rz[i]};
 	int ci[3];
-	bool bad = false;
 	for (int d = 0; d < 3; d++) {
 		double x = r[d];
 		double xw = x;
@@ -47,116 +46,20 @@ __global__ void k_bin_cells(int64_t n, double* __restrict__ rx, double* __restri
 		ci[d] = c - 1;
 		if (!(x == x)) bad = true;
 	}
-	if (bad) atomicOr(status, kStatusOutsideHalo);
 	if (r[0] != rx[i]) rx[i] = r[0];
 	if (r[1] != ry[i]) ry[i] = r[1];
 	if (r[2] != rz[i]) rz[i] = r[2];
-	int32_t c = (int32_t) (((int64_t) ci[2] * g.nc[1] + ci[1]) * g.nc[0] + ci[0]);
-	cell[i] = c;
-	rank[i] = atomicAdd(&count[c], 1);
-}
-
-// Block-local exclusive scan of kScanBlock counts; block totals go to sums.
-__global__ void k_scan_local(int64_t n, const int32_t* __restrict__ in, int32_t* __restrict__ out,
-                             int32_t* __restrict__ sums, const int* gate) {
-	if (gate && *gate == 0) return;
-	__shared__ int32_t warp_tot[8];
-	int64_t base = (int64_t) blockIdx.x * kScanBlock + threadIdx.x * 4;
-	int32_t v[4];
-	int32_t t = 0;
-	for (int k = 0; k < 4; k++) {
-		v[k] = (base + k < n) ? in[base + k] : 0;
-		t += v[k];
-	}
-	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	int32_t inc = t;
-	for (int o = 1; o < 32; o <<= 1) {
-		int32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-		if (lane >= o) inc += y;
-	}
-	if (lane == 31) warp_tot[warp] = inc;
-	__syncthreads();
-	if (warp == 0) {
-		int32_t w = lane < 8 ? warp_tot[lane] : 0;
-		for (int o = 1; o < 8; o <<= 1) {
-			int32_t y = __shfl_up_sync(0xffffffffu, w, o);
-			if (lane >= o) w += y;
-		}
-		if (lane < 8) warp_tot[lane] = w;
-	}
-	__syncthreads();
-	int32_t excl = inc - t + (warp > 0 ? warp_tot[warp - 1] : 0);
-	for (int k = 0; k < 4; k++) {
-		if (base + k < n) out[base + k] = excl;
-		excl += v[k];
-	}
-	if (threadIdx.x == blockDim.x - 1) sums[blockIdx.x] = excl;
-}
-
-// Single block: exclusive scan of the block totals, total appended at sums[nb].
-__global__ void k_scan_sums(int64_t nb, int32_t* sums, const int* gate) {
-	if (gate && *gate == 0) return;
-	__shared__ int32_t carry;
-	if (threadIdx.x == 0) carry = 0;
-	__syncthreads();
-	for (int64_t base = 0; base < nb; base += blockDim.x) {
-		int64_t i = base + threadIdx.x;
-		int32_t v = i < nb ? sums[i] : 0;
-		int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-		__shared__ int32_t wt[32];
-		int32_t inc = v;
-		for (int o = 1; o < 32; o <<= 1) {
-			int32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-			if (lane >= o) inc += y;
-		}
-		if (lane == 31) wt[warp] = inc;
-		__syncthreads();
-		if (warp == 0) {
-			int nw = blockDim.x >> 5;
-			int32_t w = lane < nw ? wt[lane] : 0;
-			for (int o = 1; o < 32; o <<= 1) {
-				int32_t y = __shfl_up_sync(0xffffffffu, w, o);
-				if (lane >= o) w += y;
-			}
-			wt[lane] = w;
-		}
-		__syncthreads();
-		int32_t excl = carry + inc - v + (warp > 0 ? wt[warp - 1] : 0);
-		if (i < nb) sums[i] = excl;
-		__syncthreads();
-		if (threadIdx.x == blockDim.x - 1) carry = excl + v;
-		__syncthreads();
-	}
-	if (threadIdx.x == 0) sums[nb] = carry;
-}
-
-__global__ void k_scan_add(int64_t n, int32_t* __restrict__ out, const int32_t* __restrict__ sums, int64_t nb,
-                           const int* gate) {
-	if (gate && *gate == 0) return;
-	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
-	if (i < n) out[i] += sums[i / kScanBlock];
-	if (i == 0) out[n] = sums[nb];
-}
-
-__global__ void k_scatter(int64_t n, const int32_t* __restrict__ cell, const int32_t* __restrict__ rank,
-                          const int32_t* __restrict__ start, int32_t* __restrict__ perm, const int* gate) {
-	if (gate && *gate == 0) return;
-	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
-	if (i < n) perm[start[cell[i]] + rank[i]] = (int32_t) i;
+	return (int32_t) (((int64_t) ci[2] * g.nc[1] + ci[1]) * g.nc[0] + ci[0]);
 }
 
 __device__ __forceinline__ bool key_less(uint64_t ka, int32_t sa, uint64_t kb, int32_t sb) {
 	return ka < kb || (ka == kb && sa < sb);
 }
 
-// One warp per cell: order the cell's molecules by (id, previous slot) and gather all fields.
-__global__ void k_cell_sort(int64_t ncells, const int32_t* __restrict__ start, const int32_t* __restrict__ perm,
-                            Particles src, Particles dst, int32_t* __restrict__ cell_out, bool with_forces,
-                            const int* gate) {
-	if (gate && *gate == 0) return;
-	int64_t c = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	int lane = threadIdx.x & 31;
-	if (c >= ncells) return;
+// One warp per cell c: order the cell's molecules by (id, previous slot) and gather all fields.
+__device__ __forceinline__ void sort_cell(int64_t c, int lane, const int32_t* start, const int32_t* perm,
+                                          const Particles& src, const Particles& dst, int32_t* cell_out,
+                                          bool with_forces) {
 	int32_t s = start[c], m = start[c + 1] - s;
 	for (int32_t e0 = 0; e0 < m; e0 += 32) {
 		int32_t e = e0 + lane;
@@ -200,62 +103,279 @@ __global__ void k_cell_sort(int64_t ncells, const int32_t* __restrict__ start, c
 	}
 }
 
-// Gated mode: the sorted arrays (and their cells) back into the current buffer.
-__global__ void k_copy_back(int64_t n, Particles src, Particles dst, const int32_t* __restrict__ cell_src,
-                            int32_t* __restrict__ cell_dst, const int* gate) {
-	if (*gate == 0) return;
+__global__ void k_bin_cells(int64_t n, double* __restrict__ rx, double* __restrict__ ry, double* __restrict__ rz,
+                            Grid g, int32_t* __restrict__ cell, int32_t* __restrict__ rank,
+                            int32_t* __restrict__ count, int* status) {
 	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
-	dst.rx[i] = src.rx[i];
-	dst.ry[i] = src.ry[i];
-	dst.rz[i] = src.rz[i];
-	dst.vx[i] = src.vx[i];
-	dst.vy[i] = src.vy[i];
-	dst.vz[i] = src.vz[i];
-	dst.id[i] = src.id[i];
-	dst.cid[i] = src.cid[i];
-	dst.uidx[i] = src.uidx[i];
-	cell_dst[i] = cell_src[i];
+	bool bad = false;
+	const int32_t c = bin_one(i, rx, ry, rz, g, bad);
+	if (bad) atomicOr(status, kStatusOutsideHalo);
+	cell[i] = c;
+	rank[i] = atomicAdd(&count[c], 1);
+}
+
+// Block-local exclusive scan of kScanBlock counts; block totals go to sums.
+__global__ void k_scan_local(int64_t n, const int32_t* __restrict__ in, int32_t* __restrict__ out,
+                             int32_t* __restrict__ sums) {
+	__shared__ int32_t warp_tot[8];
+	int64_t base = (int64_t) blockIdx.x * kScanBlock + threadIdx.x * 4;
+	int32_t v[4];
+	int32_t t = 0;
+	for (int k = 0; k < 4; k++) {
+		v[k] = (base + k < n) ? in[base + k] : 0;
+		t += v[k];
+	}
+	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	int32_t inc = t;
+	for (int o = 1; o < 32; o <<= 1) {
+		int32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+		if (lane >= o) inc += y;
+	}
+	if (lane == 31) warp_tot[warp] = inc;
+	__syncthreads();
+	if (warp == 0) {
+		int32_t w = lane < 8 ? warp_tot[lane] : 0;
+		for (int o = 1; o < 8; o <<= 1) {
+			int32_t y = __shfl_up_sync(0xffffffffu, w, o);
+			if (lane >= o) w += y;
+		}
+		if (lane < 8) warp_tot[lane] = w;
+	}
+	__syncthreads();
+	int32_t excl = inc - t + (warp > 0 ? warp_tot[warp - 1] : 0);
+	for (int k = 0; k < 4; k++) {
+		if (base + k < n) out[base + k] = excl;
+		excl += v[k];
+	}
+	if (threadIdx.x == blockDim.x - 1) sums[blockIdx.x] = excl;
+}
+
+// Exclusive block scan of one value per thread (blockDim.x a multiple of 32, <= 1024): the
+// thread's exclusive prefix, the block total in *total. Every thread of the block must call it.
+__device__ __forceinline__ int32_t block_excl_scan(int32_t v, int32_t* total) {
+	__shared__ int32_t wt[32];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (int) (blockDim.x >> 5);
+	int32_t inc = v;
+	for (int o = 1; o < 32; o <<= 1) {
+		int32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+		if (lane >= o) inc += y;
+	}
+	if (lane == 31) wt[warp] = inc;
+	__syncthreads();
+	if (warp == 0) {
+		int32_t w = lane < nw ? wt[lane] : 0;
+		for (int o = 1; o < 32; o <<= 1) {
+			int32_t y = __shfl_up_sync(0xffffffffu, w, o);
+			if (lane >= o) w += y;
+		}
+		wt[lane] = w;
+	}
+	__syncthreads();
+	const int32_t excl = inc - v + (warp > 0 ? wt[warp - 1] : 0);
+	*total = wt[nw - 1];
+	__syncthreads();
+	return excl;
+}
+
+// Single block: exclusive scan of the block totals, total appended at sums[nb].
+__global__ void k_scan_sums(int64_t nb, int32_t* sums) {
+	int32_t carry = 0;
+	for (int64_t base = 0; base < nb; base += blockDim.x) {
+		int64_t i = base + threadIdx.x;
+		int32_t v = i < nb ? sums[i] : 0;
+		int32_t tot;
+		const int32_t excl = block_excl_scan(v, &tot);
+		if (i < nb) sums[i] = carry + excl;
+		carry += tot;
+	}
+	if (threadIdx.x == 0) sums[nb] = carry;
+}
+
+__global__ void k_scan_add(int64_t n, int32_t* __restrict__ out, const int32_t* __restrict__ sums, int64_t nb) {
+	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) out[i] += sums[i / kScanBlock];
+	if (i == 0) out[n] = sums[nb];
+}
+
+__global__ void k_scatter(int64_t n, const int32_t* __restrict__ cell, const int32_t* __restrict__ rank,
+                          const int32_t* __restrict__ start, int32_t* __restrict__ perm) {
+	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) perm[start[cell[i]] + rank[i]] = (int32_t) i;
+}
+
+__global__ void k_cell_sort(int64_t ncells, const int32_t* __restrict__ start, const int32_t* __restrict__ perm,
+                            Particles src, Particles dst, int32_t* __restrict__ cell_out, bool with_forces) {
+	int64_t c = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	if (c >= ncells) return;
+	sort_cell(c, threadIdx.x & 31, start, perm, src, dst, cell_out, with_forces);
+}
+
+// ---- the whole rebuild in one cooperative launch ----------------------------------------------
+
+struct RebuildArgs {
+	int64_t n;
+	Grid g;
+	Particles p, q;
+	int32_t *cell, *rank, *perm, *count, *start, *chunk;
+	int* status;
+	const int* flag;
+	int step;
+	unsigned* bar;
+	int64_t timeout_ns;
+};
+
+constexpr int kRebuildThreads = 256;
+
+__global__ void __launch_bounds__(kRebuildThreads) k_rebuild(RebuildArgs a) {
+	__shared__ int s_flag;
+	if (threadIdx.x == 0) s_flag = (*a.flag == a.step && !(*((volatile int*) a.status) & kStatusTimeout)) ? 0 : 1;
+	__syncthreads();
+	if (s_flag) return;   // no build requested for this step
+	const int64_t nthreads = (int64_t) gridDim.x * blockDim.x;
+	const int64_t tid = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	const int64_t nc = a.g.ncells;
+	for (int64_t c = tid; c < nc; c += nthreads) a.count[c] = 0;
+	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
+	bool bad = false;
+	for (int64_t i = tid; i < a.n; i += nthreads) {
+		const int32_t c = bin_one(i, a.p.rx, a.p.ry, a.p.rz, a.g, bad);
+		a.cell[i] = c;
+		a.rank[i] = atomicAdd(&a.count[c], 1);
+	}
+	if (bad) atomicOr(a.status, kStatusOutsideHalo);
+	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
+	// scan: one contiguous chunk of cells per CTA, the chunk sums by CTA 0, then each chunk again
+	const int64_t per = (nc + gridDim.x - 1) / gridDim.x;
+	const int64_t c0 = min((int64_t) blockIdx.x * per, nc), c1 = min(c0 + per, nc);
+	{
+		int32_t local = 0;
+		for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) local += a.count[c];
+		int32_t tot;
+		block_excl_scan(local, &tot);
+		if (threadIdx.x == 0) a.chunk[blockIdx.x] = tot;
+	}
+	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
+	if (blockIdx.x == 0) {
+		int32_t carry = 0;
+		for (int64_t b0 = 0; b0 < gridDim.x; b0 += blockDim.x) {
+			const int64_t b = b0 + threadIdx.x;
+			const int32_t v = b < gridDim.x ? a.chunk[b] : 0;
+			int32_t tot;
+			const int32_t excl = block_excl_scan(v, &tot);
+			if (b < gridDim.x) a.chunk[b] = carry + excl;
+			carry += tot;
+		}
+		if (threadIdx.x == 0) a.start[nc] = carry;
+	}
+	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
+	{
+		int32_t carry = a.chunk[blockIdx.x];
+		for (int64_t base = c0; base < c1; base += blockDim.x) {
+			const int64_t c = base + threadIdx.x;
+			const int32_t v = c < c1 ? a.count[c] : 0;
+			int32_t tot;
+			const int32_t excl = block_excl_scan(v, &tot);
+			if (c < c1) a.start[c] = carry + excl;
+			carry += tot;
+		}
+	}
+	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
+	for (int64_t i = tid; i < a.n; i += nthreads) a.perm[a.start[a.cell[i]] + a.rank[i]] = (int32_t) i;
+	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
+	const int lane = threadIdx.x & 31;
+	for (int64_t c = tid >> 5; c < nc; c += nthreads >> 5) sort_cell(c, lane, a.start, a.perm, a.p, a.q, a.rank, false);
+	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
+	// the sorted arrays back into the current buffer (the host's buffer roles stay fixed)
+	for (int64_t i = tid; i < a.n; i += nthreads) {
+		a.p.rx[i] = a.q.rx[i];
+		a.p.ry[i] = a.q.ry[i];
+		a.p.rz[i] = a.q.rz[i];
+		a.p.vx[i] = a.q.vx[i];
+		a.p.vy[i] = a.q.vy[i];
+		a.p.vz[i] = a.q.vz[i];
+		a.p.id[i] = a.q.id[i];
+		a.p.cid[i] = a.q.cid[i];
+		a.p.uidx[i] = a.q.uidx[i];
+		a.cell[i] = a.rank[i];
+	}
 }
 
 inline unsigned blocks_for(int64_t n, int t) { return (unsigned) ((n + t - 1) / t); }
 
 }  // namespace
 
-cudaError_t launch_bin(Context* c, bool permute_forces, const int* gate, const Grid* grid) {
-	const Grid& g = grid ? *grid : c->g;
-	const int64_t n = c->n, nc = g.ncells;
+cudaError_t launch_bin(Context* c, bool permute_forces) {
+	const int64_t n = c->n, nc = c->g.ncells;
 	cudaStream_t s = c->stream;
 	prof_begin(c, 0);
 	cudaMemsetAsync(c->cell_count, 0, sizeof(int32_t) * nc, s);
-	if (n > 0) k_bin_cells<<<blocks_for(n, 256), 256, 0, s>>>(n, c->p.rx, c->p.ry, c->p.rz, g, c->cell, c->rank,
-	                                                          c->cell_count, c->status, gate);
+	if (n > 0) k_bin_cells<<<blocks_for(n, 256), 256, 0, s>>>(n, c->p.rx, c->p.ry, c->p.rz, c->g, c->cell, c->rank,
+	                                                          c->cell_count, c->status);
 	int64_t nb = (nc + kScanBlock - 1) / kScanBlock;
-	k_scan_local<<<(unsigned) nb, 256, 0, s>>>(nc, c->cell_count, c->cell_start, c->scan_tmp, gate);
-	k_scan_sums<<<1, 1024, 0, s>>>(nb, c->scan_tmp, gate);
-	k_scan_add<<<blocks_for(nc, 256), 256, 0, s>>>(nc, c->cell_start, c->scan_tmp, nb, gate);
+	k_scan_local<<<(unsigned) nb, 256, 0, s>>>(nc, c->cell_count, c->cell_start, c->scan_tmp);
+	k_scan_sums<<<1, 1024, 0, s>>>(nb, c->scan_tmp);
+	k_scan_add<<<blocks_for(nc, 256), 256, 0, s>>>(nc, c->cell_start, c->scan_tmp, nb);
 	int launches = 4;
 	if (n > 0) {
-		k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(n, c->cell, c->rank, c->cell_start, c->perm, gate);
+		k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(n, c->cell, c->rank, c->cell_start, c->perm);
 		k_cell_sort<<<blocks_for(nc * 32, 256), 256, 0, s>>>(nc, c->cell_start, c->perm, c->p, c->q, c->rank,
-		                                                     permute_forces, gate);
+		                                                     permute_forces);
 		launches += 2;
-		if (gate) {
-			k_copy_back<<<blocks_for(n, 256), 256, 0, s>>>(n, c->q, c->p, c->rank, c->cell, gate);
-			launches += 1;
-		}
 	}
 	cudaError_t e = cudaGetLastError();
-	if (!gate) {
-		// the sorted cell of each particle was written into `rank`; swap buffers
-		Particles t = c->p;
-		c->p = c->q;
-		c->q = t;
-		int32_t* tc = c->cell;
-		c->cell = c->rank;
-		c->rank = tc;
-	}
+	// the sorted cell of each particle was written into `rank`; swap buffers
+	Particles t = c->p;
+	c->p = c->q;
+	c->q = t;
+	int32_t* tc = c->cell;
+	c->cell = c->rank;
+	c->rank = tc;
 	prof_end(c, 0, launches);
+	return e;
+}
+
+cudaError_t launch_rebuild(Context* c, const Grid& g) {
+	static int max_ctas = -1;
+	if (max_ctas < 0) {
+		int per_sm = 0, sms = 0;
+		cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rebuild, kRebuildThreads, 0);
+		if (e != cudaSuccess) return e;
+		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+		max_ctas = per_sm * sms;
+	}
+	prof_begin(c, 0);
+	RebuildArgs a{};
+	a.n = c->n;
+	a.g = g;
+	a.p = c->p;
+	a.q = c->q;
+	a.cell = c->cell;
+	a.rank = c->rank;
+	a.perm = c->perm;
+	a.count = c->cell_count;
+	a.start = c->cell_start;
+	a.chunk = c->chunk;
+	a.status = c->status;
+	a.flag = c->rebuild;
+	a.step = c->step_id;
+	a.bar = c->bar;
+	a.timeout_ns = 2000000000LL;
+	// one chunk sum per CTA
+	int grid = max_ctas;
+	if (grid > c->chunk_cap) grid = c->chunk_cap;
+	if (grid < 1) grid = 1;
+	cudaLaunchConfig_t cfg{};
+	cfg.gridDim = dim3((unsigned) grid);
+	cfg.blockDim = dim3(kRebuildThreads);
+	cfg.stream = c->stream;
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeCooperative;
+	attr[0].val.cooperative = 1;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+	cudaError_t e = cudaLaunchKernelEx(&cfg, k_rebuild, a);
+	prof_end(c, 0, 1);
 	return e;
 }
 

@@ -746,6 +746,217 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 	if (brick == 0 && tid == 0) atomicAdd(lists.builds, 1ull);
 }
 
+// One chunk of 32 of the brick's own molecules (t0 .. t0 + 31 in the order of the own cells
+// own[0..8] / ocell[0..7]) evaluating their lists, one molecule per lane: forces written, U, W,
+// pair count and the same-position flag accumulated into the caller's sums.
+template <bool kFP64, bool kSingle, bool kLjIsRc>
+__device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const Smem& S, const int* s_own,
+                                           const int* s_ocell, int t0, int n_own, const double* rx, const double* ry,
+                                           const double* rz, const int32_t* cid, const int32_t* cstart, double* fx,
+                                           double* fy, double* fz, int* status, const Lists& lists, double& U,
+                                           double& W, double& NP, bool& same) {
+	const int lane = threadIdx.x & 31;
+	const int ns = p.ns;
+	const float eps24_1 = S.pf[0], sig2_1 = S.pf[KK], shift6_1 = S.pf[2 * KK];
+	const int t = t0 + lane;
+	const bool act = t < n_own;
+	int w = 0;
+	if (act)
+		while (w < 7 && s_own[w + 1] <= t) w++;
+	const int slot_i = act ? S.cs[s_ocell[w]] + (t - s_own[w]) : 0;
+	const float4 hi_i = S.hi[slot_i];
+	const float3 lo_i = unpack_lo(__float_as_uint(hi_i.w), bx);
+	double xi = 0, yi = 0, zi = 0;
+	if (kFP64) {
+		xi = S.img[slot_i];
+		yi = S.img[p.s_cap + slot_i];
+		zi = S.img[2 * p.s_cap + slot_i];
+	}
+	const int ti = unpack_cid(__float_as_uint(hi_i.w));
+	const int gi = act ? S.gst[s_ocell[w]] + (t - s_own[w]) : S.gst[s_ocell[0]];
+	int cnt = act ? (int) lists.count[gi] : 0;
+	const bool ovf = cnt == kListOverflow;
+	if (ovf) {
+		// the list overflowed at the build: gather this molecule from global memory
+		PairSums s = gather_pairs<!kFP64>(gi, rx, ry, rz, cid, cstart, bx.g, S.pd, ns, p.rc2, p.rclj2, bx.coff);
+		fx[gi] = s.F[0];
+		fy[gi] = s.F[1];
+		fz[gi] = s.F[2];
+		U += s.U;
+		W += s.W;
+		NP += s.np;
+		same |= s.same;
+		cnt = 0;
+	}
+	const int mx = __reduce_max_sync(kFull, cnt);
+	// blocks of 8 entries, one 16-byte load each, the next block loaded while this one is used
+	const uint4* my8 = reinterpret_cast<const uint4*>(lists.nbr) + gi;
+	const int nb8 = (mx + 7) >> 3;
+	double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+	int anp = 0;
+	uint4 nxt = nb8 > 0 ? my8[0] : make_uint4(0u, 0u, 0u, 0u);
+	if (kFP64) {
+		double ax[2] = {0, 0}, ay[2] = {0, 0}, az[2] = {0, 0}, au[2] = {0, 0}, aw[2] = {0, 0};
+		for (int b = 0; b < nb8; b++) {
+			const uint4 cur = nxt;
+			if (b + 1 < nb8) nxt = my8[(int64_t) (b + 1) * lists.n];
+			const unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
+#pragma unroll
+			for (int u = 0; u < 8; u++) {
+				const int kk = 8 * b + u;
+				const int j = min((int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu), p.s_cap - 1);
+				if (kk < cnt) lj64<kSingle>(p, xi, yi, zi, ti, ns, j, S, ax[u & 1], ay[u & 1], az[u & 1], au[u & 1],
+				                            aw[u & 1], anp, same);
+			}
+		}
+		Fx += ax[0] + ax[1];
+		Fy += ay[0] + ay[1];
+		Fz += az[0] + az[1];
+		U += au[0] + au[1];
+		W = __dadd_rn(W, __dadd_rn(aw[0], aw[1]));
+	} else {
+		// FP32, branch-free. Per coordinate e = fma(m_i - m_j, step, hi_i - hi_j) with m = 2^23 +
+		// the 9-bit lo field (exact integer difference, one rounding). Single-species runs sum
+		// fac/eps24, s6 (s6 - 1) and s6 (2 s6 - 1) and apply eps24 and shift6 per molecule.
+		const unsigned wi = __float_as_uint(hi_i.w);
+		const float mix = __uint_as_float(0x4B000000u | (wi & 511u));
+		const float miy = __uint_as_float(0x4B000000u | ((wi >> 9) & 511u));
+		const float miz = __uint_as_float(0x4B000000u | ((wi >> 18) & 511u));
+		const int nblk = (cnt + 7) >> 3;
+		const unsigned sent2 = (unsigned) p.s_cap | ((unsigned) p.s_cap << 16);
+		float ax[4] = {0.f, 0.f, 0.f, 0.f}, ay[4] = {0.f, 0.f, 0.f, 0.f}, az[4] = {0.f, 0.f, 0.f, 0.f};
+		float au[4] = {0.f, 0.f, 0.f, 0.f}, aw[4] = {0.f, 0.f, 0.f, 0.f};
+		int nlj = 0;   // pairs inside the LJ cutoff (shift6 terms)
+		// one pair in FP32 with the given cutoff decision; sign +1 adds it, -1 removes it
+		auto pair32 = [&](int j, bool in, float sign) {
+			const float4 hj = S.hi[j];
+			const unsigned wj = __float_as_uint(hj.w);
+			const float e0 = fmaf(mix - __uint_as_float(0x4B000000u | (wj & 511u)), bx.lo_step[0], hi_i.x - hj.x);
+			const float e1 = fmaf(miy - __uint_as_float(0x4B000000u | ((wj >> 9) & 511u)), bx.lo_step[1], hi_i.y - hj.y);
+			const float e2 = fmaf(miz - __uint_as_float(0x4B000000u | ((wj >> 18) & 511u)), bx.lo_step[2], hi_i.z - hj.z);
+			const float d2f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2));
+			const bool lj_in = kLjIsRc ? in : (in && d2f < p.rclj2f);
+			anp += in ? (int) sign : 0;
+			if (!kLjIsRc) nlj += lj_in ? (int) sign : 0;
+			const float inv = lj_in ? rcp_approx(d2f) : 0.f;
+			float eps24 = 1.f, sig2 = sig2_1, shift6 = 0.f;
+			if (!kSingle) {
+				const int pk = ti * ns + unpack_cid(wj);
+				eps24 = S.pf[pk];
+				sig2 = S.pf[KK + pk];
+				shift6 = S.pf[2 * KK + pk];
+			}
+			const float s2 = sig2 * inv;
+			const float s6 = s2 * s2 * s2;
+			const float r = eps24 * (s6 * fmaf(2.f, s6, -1.f));
+			const float fac = sign * r * inv;
+			ax[0] = fmaf(fac, e0, ax[0]);
+			ay[0] = fmaf(fac, e1, ay[0]);
+			az[0] = fmaf(fac, e2, az[0]);
+			au[0] += sign * (fmaf(eps24 * s6, s6 - 1.f, 0.f) + (lj_in ? shift6 : 0.f));
+			aw[0] += sign * r;
+		};
+		for (int b = 0; b < nb8; b++) {
+			uint4 cur = nxt;
+			if (b + 1 < nb8) nxt = my8[(int64_t) (b + 1) * lists.n];
+			if (b >= nblk) cur = make_uint4(sent2, sent2, sent2, sent2);
+			const unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
+			unsigned ambm = 0u;
+#pragma unroll
+			for (int u = 0; u < 8; u++) {
+				const int j = (int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu);
+				const float4 hj = S.hi[j];
+				const unsigned wj = __float_as_uint(hj.w);
+				const float h0 = hi_i.x - hj.x, h1 = hi_i.y - hj.y, h2 = hi_i.z - hj.z;  // exact
+				const float g0 = mix - __uint_as_float(0x4B000000u | (wj & 511u));
+				const float g1 = miy - __uint_as_float(0x4B000000u | ((wj >> 9) & 511u));
+				const float g2 = miz - __uint_as_float(0x4B000000u | ((wj >> 18) & 511u));
+				const float e0 = fmaf(g0, bx.lo_step[0], h0);
+				const float e1 = fmaf(g1, bx.lo_step[1], h1);
+				const float e2 = fmaf(g2, bx.lo_step[2], h2);
+				const float d2f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2));
+				const bool in = d2f < p.rc2f;
+				// within a few ulp of rc: decided after the block as the FP64 computation does
+				ambm |= fabsf(d2f - p.rc2f) <= p.band ? (1u << u) : 0u;
+				anp += in ? 1 : 0;
+				const bool lj_in = kLjIsRc ? in : (in && d2f < p.rclj2f);
+				if (!kLjIsRc) nlj += lj_in ? 1 : 0;
+				const float inv = lj_in ? rcp_approx(d2f) : 0.f;
+				if (kSingle) {
+					const float s2 = sig2_1 * inv;
+					const float s6 = s2 * s2 * s2;
+					const float r = s6 * fmaf(2.f, s6, -1.f);
+					const float facp = r * inv;
+					ax[u & 3] = fmaf(facp, e0, ax[u & 3]);
+					ay[u & 3] = fmaf(facp, e1, ay[u & 3]);
+					az[u & 3] = fmaf(facp, e2, az[u & 3]);
+					au[u & 3] = fmaf(s6, s6 - 1.f, au[u & 3]);
+					aw[u & 3] += r;
+				} else {
+					const int pk = ti * ns + unpack_cid(wj);
+					const float eps24 = S.pf[pk], sig2 = S.pf[KK + pk], shift6 = S.pf[2 * KK + pk];
+					const float s2 = sig2 * inv;
+					const float s6 = s2 * s2 * s2;
+					const float r = eps24 * (s6 * fmaf(2.f, s6, -1.f));
+					const float fac = r * inv;
+					ax[u & 3] = fmaf(fac, e0, ax[u & 3]);
+					ay[u & 3] = fmaf(fac, e1, ay[u & 3]);
+					az[u & 3] = fmaf(fac, e2, az[u & 3]);
+					au[u & 3] = fmaf(eps24 * s6, s6 - 1.f, au[u & 3]) + (lj_in ? shift6 : 0.f);
+					aw[u & 3] += r;
+				}
+			}
+			if (__any_sync(kFull, ambm != 0u)) {
+				// rare: pairs within a few ulp of rc whose FP64 decision differs from the FP32 one
+				while (ambm) {
+					const int u = __ffs(ambm) - 1;
+					ambm &= ambm - 1u;
+					const int j = (int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu);
+					const float4 hj = S.hi[j];
+					const unsigned wj = __float_as_uint(hj.w);
+					const float e0 = fmaf(mix - __uint_as_float(0x4B000000u | (wj & 511u)), bx.lo_step[0], hi_i.x - hj.x);
+					const float e1 = fmaf(miy - __uint_as_float(0x4B000000u | ((wj >> 9) & 511u)), bx.lo_step[1], hi_i.y - hj.y);
+					const float e2 = fmaf(miz - __uint_as_float(0x4B000000u | ((wj >> 18) & 511u)), bx.lo_step[2], hi_i.z - hj.z);
+					const bool in_f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2)) < p.rc2f;
+					const bool in_d = exact_cut(S, p.rc2, j, gi, rx, ry, rz);
+					if (in_f != in_d) pair32(j, true, in_d ? 1.f : -1.f);
+				}
+			}
+			if ((b & 7) == 7 || b + 1 == nb8) {
+				// fold the FP32 partial sums of up to 64 entries into the FP64 accumulators
+				const double sc = kSingle ? (double) eps24_1 : 1.0;
+				Fx += sc * (((double) ax[0] + (double) ax[1]) + ((double) ax[2] + (double) ax[3]));
+				Fy += sc * (((double) ay[0] + (double) ay[1]) + ((double) ay[2] + (double) ay[3]));
+				Fz += sc * (((double) az[0] + (double) az[1]) + ((double) az[2] + (double) az[3]));
+				U += sc * (((double) au[0] + (double) au[1]) + ((double) au[2] + (double) au[3]));
+				W += sc * (((double) aw[0] + (double) aw[1]) + ((double) aw[2] + (double) aw[3]));
+#pragma unroll
+				for (int u = 0; u < 4; u++) ax[u] = ay[u] = az[u] = au[u] = aw[u] = 0.f;
+			}
+		}
+		if (kSingle) U += (double) shift6_1 * (double) (kLjIsRc ? anp : nlj);
+		if (!(Fx == Fx && Fy == Fy && Fz == Fz) && act && !ovf) {
+			// a zero distance gives 0 * inf: report it as the reference does (same position)
+			for (int k = 0; k < cnt; k++) {
+				const int j = lists.nbr[(((int64_t) (k >> 3) * lists.n + gi) << 3) + (k & 7)];
+				const float4 hj = S.hi[min(j, p.s_cap)];
+				const unsigned pos_bits = (1u << 27) - 1u;   // the lo fields, not the component id
+				if (hj.x == hi_i.x && hj.y == hi_i.y && hj.z == hi_i.z &&
+				    ((__float_as_uint(hj.w) ^ wi) & pos_bits) == 0u && j != slot_i)
+					same = true;
+			}
+		}
+	}
+	NP += (double) anp;
+	if (act && !ovf) {
+		fx[gi] = Fx;
+		fy[gi] = Fy;
+		fz[gi] = Fz;
+		if (!(Fx == Fx && Fy == Fy && Fz == Fz) || isinf(Fx) || isinf(Fy) || isinf(Fz))
+			atomicOr(status, kStatusNonFinite);
+	}
+}
+
 // Forces of brick `brick` from the neighbour lists that build_lists made on the same cell
 // structure, at the current positions: staging as in pairs, then the molecules of the brick's
 // own cells, 32 per warp regardless of their cell, each evaluate their list with the exact cutoff.
@@ -758,7 +969,7 @@ __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int br
                                            double* fz, double* partials, int* status, const Lists lists) {
 	const SmemLayout L = layout(p.s_cap, kFP64, 0, false);
 	const Smem S = views(smem, L);
-	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	const int tid = threadIdx.x, warp = tid >> 5;
 	const int ns = p.ns;
 	const bool staged = stage<kFP64, false>(p, bx, brick, S, rx, ry, rz, cid, cstart);
 	__shared__ int s_own[9], s_ocell[8];
@@ -795,206 +1006,9 @@ __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int br
 			same |= s.same;
 		}
 	} else {
-		const float eps24_1 = S.pf[0], sig2_1 = S.pf[KK], shift6_1 = S.pf[2 * KK];
-		for (int t0 = warp * 32; t0 < n_own; t0 += kThreads) {
-			const int t = t0 + lane;
-			const bool act = t < n_own;
-			int w = 0;
-			if (act)
-				while (w < 7 && s_own[w + 1] <= t) w++;
-			const int slot_i = act ? S.cs[s_ocell[w]] + (t - s_own[w]) : 0;
-			const float4 hi_i = S.hi[slot_i];
-			const float3 lo_i = unpack_lo(__float_as_uint(hi_i.w), bx);
-			double xi = 0, yi = 0, zi = 0;
-			if (kFP64) {
-				xi = S.img[slot_i];
-				yi = S.img[p.s_cap + slot_i];
-				zi = S.img[2 * p.s_cap + slot_i];
-			}
-			const int ti = unpack_cid(__float_as_uint(hi_i.w));
-			const int gi = act ? S.gst[s_ocell[w]] + (t - s_own[w]) : S.gst[s_ocell[0]];
-			int cnt = act ? (int) lists.count[gi] : 0;
-			const bool ovf = cnt == kListOverflow;
-			if (ovf) {
-				// the list overflowed at the build: gather this molecule from global memory
-				PairSums s = gather_pairs<!kFP64>(gi, rx, ry, rz, cid, cstart, bx.g, S.pd, ns, p.rc2, p.rclj2, bx.coff);
-				fx[gi] = s.F[0];
-				fy[gi] = s.F[1];
-				fz[gi] = s.F[2];
-				U += s.U;
-				W += s.W;
-				NP += s.np;
-				same |= s.same;
-				cnt = 0;
-			}
-			const int mx = __reduce_max_sync(kFull, cnt);
-			// blocks of 8 entries, one 16-byte load each, the next block loaded while this one is used
-			const uint4* my8 = reinterpret_cast<const uint4*>(lists.nbr) + gi;
-			const int nb8 = (mx + 7) >> 3;
-			double Fx = 0.0, Fy = 0.0, Fz = 0.0;
-			int anp = 0;
-			uint4 nxt = nb8 > 0 ? my8[0] : make_uint4(0u, 0u, 0u, 0u);
-			if (kFP64) {
-				double ax[2] = {0, 0}, ay[2] = {0, 0}, az[2] = {0, 0}, au[2] = {0, 0}, aw[2] = {0, 0};
-				for (int b = 0; b < nb8; b++) {
-					const uint4 cur = nxt;
-					if (b + 1 < nb8) nxt = my8[(int64_t) (b + 1) * lists.n];
-					const unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
-#pragma unroll
-					for (int u = 0; u < 8; u++) {
-						const int kk = 8 * b + u;
-						const int j = min((int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu), p.s_cap - 1);
-						if (kk < cnt) lj64<kSingle>(p, xi, yi, zi, ti, ns, j, S, ax[u & 1], ay[u & 1], az[u & 1], au[u & 1],
-						                            aw[u & 1], anp, same);
-					}
-				}
-				Fx += ax[0] + ax[1];
-				Fy += ay[0] + ay[1];
-				Fz += az[0] + az[1];
-				U += au[0] + au[1];
-				W = __dadd_rn(W, __dadd_rn(aw[0], aw[1]));
-			} else {
-				// FP32, branch-free. Per coordinate e = fma(m_i - m_j, step, hi_i - hi_j) with m = 2^23 +
-				// the 9-bit lo field (exact integer difference, one rounding). Single-species runs sum
-				// fac/eps24, s6 (s6 - 1) and s6 (2 s6 - 1) and apply eps24 and shift6 per molecule.
-				const unsigned wi = __float_as_uint(hi_i.w);
-				const float mix = __uint_as_float(0x4B000000u | (wi & 511u));
-				const float miy = __uint_as_float(0x4B000000u | ((wi >> 9) & 511u));
-				const float miz = __uint_as_float(0x4B000000u | ((wi >> 18) & 511u));
-				const int nblk = (cnt + 7) >> 3;
-				const unsigned sent2 = (unsigned) p.s_cap | ((unsigned) p.s_cap << 16);
-				float ax[4] = {0.f, 0.f, 0.f, 0.f}, ay[4] = {0.f, 0.f, 0.f, 0.f}, az[4] = {0.f, 0.f, 0.f, 0.f};
-				float au[4] = {0.f, 0.f, 0.f, 0.f}, aw[4] = {0.f, 0.f, 0.f, 0.f};
-				int nlj = 0;   // pairs inside the LJ cutoff (shift6 terms)
-				// one pair in FP32 with the given cutoff decision; sign +1 adds it, -1 removes it
-				auto pair32 = [&](int j, bool in, float sign) {
-					const float4 hj = S.hi[j];
-					const unsigned wj = __float_as_uint(hj.w);
-					const float e0 = fmaf(mix - __uint_as_float(0x4B000000u | (wj & 511u)), bx.lo_step[0], hi_i.x - hj.x);
-					const float e1 = fmaf(miy - __uint_as_float(0x4B000000u | ((wj >> 9) & 511u)), bx.lo_step[1], hi_i.y - hj.y);
-					const float e2 = fmaf(miz - __uint_as_float(0x4B000000u | ((wj >> 18) & 511u)), bx.lo_step[2], hi_i.z - hj.z);
-					const float d2f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2));
-					const bool lj_in = kLjIsRc ? in : (in && d2f < p.rclj2f);
-					anp += in ? (int) sign : 0;
-					if (!kLjIsRc) nlj += lj_in ? (int) sign : 0;
-					const float inv = lj_in ? rcp_approx(d2f) : 0.f;
-					float eps24 = 1.f, sig2 = sig2_1, shift6 = 0.f;
-					if (!kSingle) {
-						const int pk = ti * ns + unpack_cid(wj);
-						eps24 = S.pf[pk];
-						sig2 = S.pf[KK + pk];
-						shift6 = S.pf[2 * KK + pk];
-					}
-					const float s2 = sig2 * inv;
-					const float s6 = s2 * s2 * s2;
-					const float r = eps24 * (s6 * fmaf(2.f, s6, -1.f));
-					const float fac = sign * r * inv;
-					ax[0] = fmaf(fac, e0, ax[0]);
-					ay[0] = fmaf(fac, e1, ay[0]);
-					az[0] = fmaf(fac, e2, az[0]);
-					au[0] += sign * (fmaf(eps24 * s6, s6 - 1.f, 0.f) + (lj_in ? shift6 : 0.f));
-					aw[0] += sign * r;
-				};
-				for (int b = 0; b < nb8; b++) {
-					uint4 cur = nxt;
-					if (b + 1 < nb8) nxt = my8[(int64_t) (b + 1) * lists.n];
-					if (b >= nblk) cur = make_uint4(sent2, sent2, sent2, sent2);
-					const unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
-					unsigned ambm = 0u;
-#pragma unroll
-					for (int u = 0; u < 8; u++) {
-						const int j = (int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu);
-						const float4 hj = S.hi[j];
-						const unsigned wj = __float_as_uint(hj.w);
-						const float h0 = hi_i.x - hj.x, h1 = hi_i.y - hj.y, h2 = hi_i.z - hj.z;  // exact
-						const float g0 = mix - __uint_as_float(0x4B000000u | (wj & 511u));
-						const float g1 = miy - __uint_as_float(0x4B000000u | ((wj >> 9) & 511u));
-						const float g2 = miz - __uint_as_float(0x4B000000u | ((wj >> 18) & 511u));
-						const float e0 = fmaf(g0, bx.lo_step[0], h0);
-						const float e1 = fmaf(g1, bx.lo_step[1], h1);
-						const float e2 = fmaf(g2, bx.lo_step[2], h2);
-						const float d2f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2));
-						const bool in = d2f < p.rc2f;
-						// within a few ulp of rc: decided after the block as the FP64 computation does
-						ambm |= fabsf(d2f - p.rc2f) <= p.band ? (1u << u) : 0u;
-						anp += in ? 1 : 0;
-						const bool lj_in = kLjIsRc ? in : (in && d2f < p.rclj2f);
-						if (!kLjIsRc) nlj += lj_in ? 1 : 0;
-						const float inv = lj_in ? rcp_approx(d2f) : 0.f;
-						if (kSingle) {
-							const float s2 = sig2_1 * inv;
-							const float s6 = s2 * s2 * s2;
-							const float r = s6 * fmaf(2.f, s6, -1.f);
-							const float facp = r * inv;
-							ax[u & 3] = fmaf(facp, e0, ax[u & 3]);
-							ay[u & 3] = fmaf(facp, e1, ay[u & 3]);
-							az[u & 3] = fmaf(facp, e2, az[u & 3]);
-							au[u & 3] = fmaf(s6, s6 - 1.f, au[u & 3]);
-							aw[u & 3] += r;
-						} else {
-							const int pk = ti * ns + unpack_cid(wj);
-							const float eps24 = S.pf[pk], sig2 = S.pf[KK + pk], shift6 = S.pf[2 * KK + pk];
-							const float s2 = sig2 * inv;
-							const float s6 = s2 * s2 * s2;
-							const float r = eps24 * (s6 * fmaf(2.f, s6, -1.f));
-							const float fac = r * inv;
-							ax[u & 3] = fmaf(fac, e0, ax[u & 3]);
-							ay[u & 3] = fmaf(fac, e1, ay[u & 3]);
-							az[u & 3] = fmaf(fac, e2, az[u & 3]);
-							au[u & 3] = fmaf(eps24 * s6, s6 - 1.f, au[u & 3]) + (lj_in ? shift6 : 0.f);
-							aw[u & 3] += r;
-						}
-					}
-					if (__any_sync(kFull, ambm != 0u)) {
-						// rare: pairs within a few ulp of rc whose FP64 decision differs from the FP32 one
-						while (ambm) {
-							const int u = __ffs(ambm) - 1;
-							ambm &= ambm - 1u;
-							const int j = (int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu);
-							const float4 hj = S.hi[j];
-							const unsigned wj = __float_as_uint(hj.w);
-							const float e0 = fmaf(mix - __uint_as_float(0x4B000000u | (wj & 511u)), bx.lo_step[0], hi_i.x - hj.x);
-							const float e1 = fmaf(miy - __uint_as_float(0x4B000000u | ((wj >> 9) & 511u)), bx.lo_step[1], hi_i.y - hj.y);
-							const float e2 = fmaf(miz - __uint_as_float(0x4B000000u | ((wj >> 18) & 511u)), bx.lo_step[2], hi_i.z - hj.z);
-							const bool in_f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2)) < p.rc2f;
-							const bool in_d = exact_cut(S, p.rc2, j, gi, rx, ry, rz);
-							if (in_f != in_d) pair32(j, true, in_d ? 1.f : -1.f);
-						}
-					}
-					if ((b & 7) == 7 || b + 1 == nb8) {
-						// fold the FP32 partial sums of up to 64 entries into the FP64 accumulators
-						const double sc = kSingle ? (double) eps24_1 : 1.0;
-						Fx += sc * (((double) ax[0] + (double) ax[1]) + ((double) ax[2] + (double) ax[3]));
-						Fy += sc * (((double) ay[0] + (double) ay[1]) + ((double) ay[2] + (double) ay[3]));
-						Fz += sc * (((double) az[0] + (double) az[1]) + ((double) az[2] + (double) az[3]));
-						U += sc * (((double) au[0] + (double) au[1]) + ((double) au[2] + (double) au[3]));
-						W += sc * (((double) aw[0] + (double) aw[1]) + ((double) aw[2] + (double) aw[3]));
-#pragma unroll
-						for (int u = 0; u < 4; u++) ax[u] = ay[u] = az[u] = au[u] = aw[u] = 0.f;
-					}
-				}
-				if (kSingle) U += (double) shift6_1 * (double) (kLjIsRc ? anp : nlj);
-				if (!(Fx == Fx && Fy == Fy && Fz == Fz) && act && !ovf) {
-					// a zero distance gives 0 * inf: report it as the reference does (same position)
-					for (int k = 0; k < cnt; k++) {
-						const int j = lists.nbr[(((int64_t) (k >> 3) * lists.n + gi) << 3) + (k & 7)];
-						const float4 hj = S.hi[min(j, p.s_cap)];
-						const unsigned pos_bits = (1u << 27) - 1u;   // the lo fields, not the component id
-						if (hj.x == hi_i.x && hj.y == hi_i.y && hj.z == hi_i.z &&
-						    ((__float_as_uint(hj.w) ^ wi) & pos_bits) == 0u && j != slot_i)
-							same = true;
-					}
-				}
-			}
-			NP += (double) anp;
-			if (act && !ovf) {
-				fx[gi] = Fx;
-				fy[gi] = Fy;
-				fz[gi] = Fz;
-				if (!(Fx == Fx && Fy == Fy && Fz == Fz) || isinf(Fx) || isinf(Fy) || isinf(Fz))
-					atomicOr(status, kStatusNonFinite);
-			}
-		}
+		for (int t0 = warp * 32; t0 < n_own; t0 += kThreads)
+			list_chunk<kFP64, kSingle, kLjIsRc>(p, bx, S, s_own, s_ocell, t0, n_own, rx, ry, rz, cid, cstart, fx, fy, fz,
+			                                    status, lists, U, W, NP, same);
 	}
 	if (same) atomicOr(status, kStatusSamePosition);
 	block_sum3_at(U, W, NP, partials, slot);

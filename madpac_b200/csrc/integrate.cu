@@ -20,11 +20,13 @@ struct SpeciesScale {
 	double mass[kMaxSpecies];
 };
 
-// Verlet-skin check of the pre-kick: the positions at the last build and the squared half skin.
+// Verlet-skin check of the pre-kick: the positions at the last build, the squared half skin, and
+// the step id written to *flag when a molecule moved farther.
 struct SkinCheck {
 	const double *rx, *ry, *rz;
 	double half2;
 	int* flag;
+	int id;
 };
 
 __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_pre(int64_t n, Particles p, SpeciesScale s, double dt,
@@ -47,14 +49,51 @@ __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_pre(int64_t n, Partic
 	p.rz[i] = z;
 	if (sk.flag) {
 		const double dx = x - sk.rx[i], dy = y - sk.ry[i], dz = z - sk.rz[i];
-		if (!(dx * dx + dy * dy + dz * dz <= sk.half2)) *sk.flag = 1;
+		if (!(dx * dx + dy * dy + dz * dz <= sk.half2)) *sk.flag = sk.id;
 	}
 }
 
-__global__ void __launch_bounds__(kReduceBlock) k_leapfrog_post(int64_t n, Particles p, SpeciesScale s,
-                                                               double* partials, int* status, int* clear_flag) {
+// Closing kick (Molecule::upd_postF, sum m v^2) of one step, then the opening kick and drift
+// (Molecule::upd_preF with vcorr = 1) of the next, with the same roundings as the two kernels.
+__global__ void __launch_bounds__(kReduceBlock) k_leapfrog_post_pre(int64_t n, Particles p, SpeciesScale post,
+                                                                   SpeciesScale pre, double dt, double* partials,
+                                                                   int* status, SkinCheck sk) {
 	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
-	if (clear_flag && i == 0) *clear_flag = 0;   // every pair kernel of this step has read it
+	double mv2 = 0.0;
+	if (i < n) {
+		const int t = p.cid[i];
+		const double fx = p.fx[i], fy = p.fy[i], fz = p.fz[i];
+		const double a = post.dtInv2m[t];
+		const double vx = __dadd_rn(p.vx[i], __dmul_rn(a, fx));
+		const double vy = __dadd_rn(p.vy[i], __dmul_rn(a, fy));
+		const double vz = __dadd_rn(p.vz[i], __dmul_rn(a, fz));
+		const double v2 = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
+		mv2 = __dmul_rn(post.mass[t], v2);
+		if (!(v2 == v2) || isinf(v2)) atomicOr(status, kStatusNonFinite);
+		const double b = pre.dtInv2m[t];
+		const double wx = __dadd_rn(__dmul_rn(1.0, vx), __dmul_rn(b, fx));
+		const double wy = __dadd_rn(__dmul_rn(1.0, vy), __dmul_rn(b, fy));
+		const double wz = __dadd_rn(__dmul_rn(1.0, vz), __dmul_rn(b, fz));
+		p.vx[i] = wx;
+		p.vy[i] = wy;
+		p.vz[i] = wz;
+		const double x = __dadd_rn(p.rx[i], __dmul_rn(dt, wx));
+		const double y = __dadd_rn(p.ry[i], __dmul_rn(dt, wy));
+		const double z = __dadd_rn(p.rz[i], __dmul_rn(dt, wz));
+		p.rx[i] = x;
+		p.ry[i] = y;
+		p.rz[i] = z;
+		if (sk.flag) {
+			const double dx = x - sk.rx[i], dy = y - sk.ry[i], dz = z - sk.rz[i];
+			if (!(dx * dx + dy * dy + dz * dz <= sk.half2)) *sk.flag = sk.id;
+		}
+	}
+	block_sum3(mv2, 0.0, 0.0, partials);
+}
+
+__global__ void __launch_bounds__(kReduceBlock) k_leapfrog_post(int64_t n, Particles p, SpeciesScale s,
+                                                               double* partials, int* status) {
+	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	double mv2 = 0.0;
 	if (i < n) {
 		const int t = p.cid[i];
@@ -101,19 +140,25 @@ SpeciesScale make_scale(const Context* c, double dt_half) {
 
 inline unsigned blocks_for(int64_t n) { return (unsigned) ((n + kReduceBlock - 1) / kReduceBlock); }
 
-}  // namespace
-
-cudaError_t launch_leapfrog_pre(Context* c, double dt, double vcorr, bool skin_check) {
-	if (c->n == 0) return cudaSuccess;
-	prof_begin(c, 2);
+SkinCheck skin_check_of(const Context* c, bool on) {
 	SkinCheck sk{};
-	if (skin_check) {
+	if (on) {
 		sk.rx = c->r_ref;
 		sk.ry = c->r_ref + c->n;
 		sk.rz = c->r_ref + 2 * c->n;
 		sk.half2 = 0.25 * c->skin * c->skin;
 		sk.flag = c->rebuild;
+		sk.id = c->step_id;
 	}
+	return sk;
+}
+
+}  // namespace
+
+cudaError_t launch_leapfrog_pre(Context* c, double dt, double vcorr, bool skin_check) {
+	if (c->n == 0) return cudaSuccess;
+	prof_begin(c, 2);
+	const SkinCheck sk = skin_check_of(c, skin_check);
 	// dt_halve = .5 * dt, dtInv2m = dt_halve / m  (Molecule.cpp:130-131)
 	k_leapfrog_pre<<<blocks_for(c->n), kReduceBlock, 0, c->stream>>>(c->n, c->p, make_scale(c, .5 * dt), dt, vcorr, sk);
 	cudaError_t e = cudaGetLastError();
@@ -121,11 +166,23 @@ cudaError_t launch_leapfrog_pre(Context* c, double dt, double vcorr, bool skin_c
 	return e;
 }
 
-cudaError_t launch_leapfrog_post(Context* c, double dt_half, bool clear_flag) {
+cudaError_t launch_leapfrog_post_pre(Context* c, double dt, bool skin_check) {
+	prof_begin(c, 2);
+	int64_t nb = c->n > 0 ? blocks_for(c->n) : 1;
+	k_leapfrog_post_pre<<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(
+	    c->n, c->p, make_scale(c, 0.5 * dt), make_scale(c, .5 * dt), dt, c->partials, c->status,
+	    skin_check_of(c, skin_check));
+	cudaError_t e = cudaGetLastError();
+	prof_end(c, 2, 1);
+	if (e != cudaSuccess) return e;
+	return launch_reduce(c, nb, c->scalars + 3, 1);
+}
+
+cudaError_t launch_leapfrog_post(Context* c, double dt_half) {
 	prof_begin(c, 2);
 	int64_t nb = c->n > 0 ? blocks_for(c->n) : 1;
 	k_leapfrog_post<<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(c->n, c->p, make_scale(c, dt_half), c->partials,
-	                                                               c->status, clear_flag ? c->rebuild : nullptr);
+	                                                               c->status);
 	cudaError_t e = cudaGetLastError();
 	prof_end(c, 2, 1);
 	if (e != cudaSuccess) return e;

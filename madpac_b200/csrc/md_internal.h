@@ -103,7 +103,11 @@ struct Context {
 	unsigned short* nbr = nullptr;  // list_cap x n staged-slot indices
 	unsigned short* nbr_count = nullptr;
 	double* r_ref = nullptr;        // 3 x n positions at the last build
-	int* rebuild = nullptr;         // device flag: nonzero = build this step
+	int* rebuild = nullptr;         // device: the step id for which a build was asked
+	int step_id = 0;                // id of the step being enqueued (skin mode)
+	unsigned* bar = nullptr;        // grid-barrier words of the cooperative rebuild
+	int32_t* chunk = nullptr;       // per-CTA scan sums of the cooperative rebuild
+	int chunk_cap = 0;
 	unsigned long long* builds = nullptr;   // builds so far (device counter)
 	bool lists_valid = false;       // the sort order has not changed since the lists were built
 	double* adj = nullptr;          // adjoint buffers: cotangents, outputs, parameter partials
@@ -121,15 +125,20 @@ struct Context {
 
 // ---- launch helpers implemented in the .cu files -------------------------------------------
 // Each returns cudaSuccess or the launch error; kernels report data errors in ctx->status.
-// With a gate (Verlet-skin mode) every kernel returns at once unless *gate != 0, and the sorted
-// arrays are copied back into c->p so that the host-side buffer roles do not depend on the flag.
-cudaError_t launch_bin(Context* c, bool permute_forces, const int* gate = nullptr, const Grid* grid = nullptr);
+cudaError_t launch_bin(Context* c, bool permute_forces);
+// Verlet-skin mode: wrap, binning on grid g and sort in one cooperative launch that returns at
+// once unless *c->rebuild == c->step_id; the sorted arrays end in c->p (buffer roles unchanged).
+cudaError_t launch_rebuild(Context* c, const Grid& g);
 cudaError_t launch_pairs(Context* c);                 // partials -> scalars[0..2] (U6sum, W, npairs)
 cudaError_t launch_pairs_skin(Context* c);            // the same in the Verlet-skin mode
-// With skin_check the pre-kick also raises c->rebuild when a molecule is more than skin/2 from its
-// position at the last build; the post-kick with clear_flag resets c->rebuild for the next step.
+int64_t skin_partials_needed(const Context* c);       // reduction partials the skin-mode kernels write
+// With skin_check the pre-kick also sets *c->rebuild = c->step_id when a molecule is more than
+// skin/2 from its position at the last build.
 cudaError_t launch_leapfrog_pre(Context* c, double dt, double vcorr, bool skin_check = false);
-cudaError_t launch_leapfrog_post(Context* c, double dt_half, bool clear_flag = false);   // scalars[3] = sum m v^2
+cudaError_t launch_leapfrog_post(Context* c, double dt_half);   // scalars[3] = sum m v^2
+// The closing kick of one step and the opening kick of the next in one pass (mdgpu_run): the same
+// operations as launch_leapfrog_post(dt/2) followed by launch_leapfrog_pre(dt, 1).
+cudaError_t launch_leapfrog_post_pre(Context* c, double dt, bool skin_check);
 cudaError_t launch_scale(Context* c, double beta);
 cudaError_t launch_reduce(Context* c, int64_t nblocks, double* out, int nval);
 cudaError_t launch_adjoint(Context* c, const double* gfx, const double* gfy, const double* gfz, double gU, double* ox,

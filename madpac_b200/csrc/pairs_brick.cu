@@ -9,6 +9,8 @@
 // (set by the Leapfrog pre-kick when a molecule moved more than skin/2 since the build) is set.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "brick.cuh"
 #include "md_internal.h"
 
@@ -32,12 +34,12 @@ __global__ void __launch_bounds__(brick::kThreads, 2)
 	                                                fy, fz, partials, status);
 }
 
-// Verlet-skin build step (runs only when *gate != 0): the lists, no forces.
+// Verlet-skin build step (runs only when *gate is this step's id): the lists, no forces.
 __global__ void __launch_bounds__(brick::kThreads, 3)
     k_build_lists(brick::Box bx, int s_cap, const double* __restrict__ rx, const double* __restrict__ ry,
                   const double* __restrict__ rz, const int32_t* __restrict__ cstart, const int* __restrict__ gate,
-                  brick::Lists lists) {
-	if (*gate == 0) return;
+                  int step, brick::Lists lists) {
+	if (*gate != step) return;
 	extern __shared__ __align__(16) unsigned char smem[];
 	brick::build_lists(bx, blockIdx.x, s_cap, smem, rx, ry, rz, cstart, lists);
 }
@@ -56,6 +58,7 @@ __global__ void __launch_bounds__(brick::kThreads, 2)
 	brick::list_pairs<kFP64, kSingle, kLjIsRc>(p, bx, blockIdx.x, blockIdx.x, smem, rx, ry, rz, cid, cstart, fx,
 	                                           fy, fz, partials, status, lists);
 }
+
 
 struct Plan {
 	brick::Const p;
@@ -141,7 +144,7 @@ cudaError_t launch_pairs_brick(Context* c) {
 cudaError_t launch_pairs_skin(Context* c) {
 	brick::Lists l = lists_of(c);
 	const Plan P = plan(c, c->gs, c->rc, 2);
-	l.sentinel = P.p.s_cap;
+	l.sentinel = P.p.s_cap;   // the evaluation kernel's sentinel slot terminates every list
 	prof_begin(c, 1);
 	// build (gated): half-precision staging only, three CTAs per SM
 	brick::Box bb{};
@@ -153,13 +156,17 @@ cudaError_t launch_pairs_skin(Context* c) {
 	cudaError_t e = cudaFuncSetAttribute(k_build_lists, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bbytes);
 	if (e == cudaSuccess)
 		k_build_lists<<<nbricks, brick::kThreads, bbytes, c->stream>>>(bb, s_cap, c->p.rx, c->p.ry, c->p.rz,
-		                                                              c->cell_start, c->rebuild, l);
+		                                                              c->cell_start, c->rebuild, c->step_id, l);
 	// evaluation, every step
 	if (e == cudaSuccess) e = dispatch<2>(c, P, nullptr, l);
 	if (e == cudaSuccess) e = cudaGetLastError();
 	prof_end(c, 1, 2);
 	if (e != cudaSuccess) return e;
 	return launch_reduce(c, P.nbricks, c->scalars, 3);
+}
+
+int64_t skin_partials_needed(const Context* c) {
+	return (int64_t) ((c->gs.nc[0] + 1) / 2) * ((c->gs.nc[1] + 1) / 2) * ((c->gs.nc[2] + 1) / 2);
 }
 
 }  // namespace mdgpu
