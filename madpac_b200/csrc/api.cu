@@ -373,6 +373,8 @@ int mdgpu_create(mdgpu_ctx** out, const double length[3], double cutoff, double 
 	MD_CUDA(cudaMemset(c->scalars, 0, sizeof(double) * 64));
 	MD_CUDA(cudaMalloc(&c->status, sizeof(int)));
 	MD_CUDA(cudaMemset(c->status, 0, sizeof(int)));
+	MD_CUDA(cudaMalloc(&c->tickets, sizeof(unsigned) * 4));
+	MD_CUDA(cudaMemset(c->tickets, 0, sizeof(unsigned) * 4));
 	MD_CUDA(cudaMallocHost(&c->h_scalars, sizeof(double) * 64));
 	MD_CUDA(cudaMallocHost(&c->h_status, sizeof(int)));
 	PairParams hp = pair_params(c->sp, c->rc, c->rc_lj);
@@ -409,6 +411,7 @@ int mdgpu_destroy(mdgpu_ctx* ctx) {
 	cudaFree(c->builds);
 	cudaFree(c->bar);
 	cudaFree(c->chunk);
+	cudaFree(c->tickets);
 	cudaFree(full->x.stage.ptr);
 	if (c->h_scalars) cudaFreeHost(c->h_scalars);
 	if (c->h_status) cudaFreeHost(c->h_status);
@@ -859,8 +862,7 @@ int enqueue_steps(Context* c, int32_t nsteps, double dt) {
 		if (k == 0) {
 			MD_CUDA(launch_leapfrog_pre(c, dt, 1.0, skin));
 		} else {
-			MD_CUDA(launch_leapfrog_post_pre(c, dt, skin));
-			MD_CUDA(launch_step_record(c, c->steps_out + 4 * c->steps_written));
+			MD_CUDA(launch_leapfrog_post_pre(c, dt, skin, c->steps_out + 4 * c->steps_written));
 			c->steps_written++;
 		}
 		if (skin) {
@@ -872,8 +874,7 @@ int enqueue_steps(Context* c, int32_t nsteps, double dt) {
 			MD_CUDA(launch_pairs(c));
 		}
 	}
-	MD_CUDA(launch_leapfrog_post(c, 0.5 * dt));
-	MD_CUDA(launch_step_record(c, c->steps_out + 4 * c->steps_written));
+	MD_CUDA(launch_leapfrog_post(c, 0.5 * dt, c->steps_out + 4 * c->steps_written));
 	c->steps_written++;
 	return MDGPU_OK;
 }

@@ -33,19 +33,22 @@ __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_pre(int64_t n, Partic
                                                               double vcorr, SkinCheck sk) {
 	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
+	// every load first: the arrays may alias as far as the compiler knows
 	const double a = s.dtInv2m[p.cid[i]];
-	double v;
-	v = __dadd_rn(__dmul_rn(vcorr, p.vx[i]), __dmul_rn(a, p.fx[i]));
-	p.vx[i] = v;
-	const double x = __dadd_rn(p.rx[i], __dmul_rn(dt, v));
+	const double vx0 = p.vx[i], vy0 = p.vy[i], vz0 = p.vz[i];
+	const double fx = p.fx[i], fy = p.fy[i], fz = p.fz[i];
+	const double x0 = p.rx[i], y0 = p.ry[i], z0 = p.rz[i];
+	const double vx = __dadd_rn(__dmul_rn(vcorr, vx0), __dmul_rn(a, fx));
+	const double vy = __dadd_rn(__dmul_rn(vcorr, vy0), __dmul_rn(a, fy));
+	const double vz = __dadd_rn(__dmul_rn(vcorr, vz0), __dmul_rn(a, fz));
+	const double x = __dadd_rn(x0, __dmul_rn(dt, vx));
+	const double y = __dadd_rn(y0, __dmul_rn(dt, vy));
+	const double z = __dadd_rn(z0, __dmul_rn(dt, vz));
+	p.vx[i] = vx;
+	p.vy[i] = vy;
+	p.vz[i] = vz;
 	p.rx[i] = x;
-	v = __dadd_rn(__dmul_rn(vcorr, p.vy[i]), __dmul_rn(a, p.fy[i]));
-	p.vy[i] = v;
-	const double y = __dadd_rn(p.ry[i], __dmul_rn(dt, v));
 	p.ry[i] = y;
-	v = __dadd_rn(__dmul_rn(vcorr, p.vz[i]), __dmul_rn(a, p.fz[i]));
-	p.vz[i] = v;
-	const double z = __dadd_rn(p.rz[i], __dmul_rn(dt, v));
 	p.rz[i] = z;
 	if (sk.flag) {
 		const double dx = x - sk.rx[i], dy = y - sk.ry[i], dz = z - sk.rz[i];
@@ -55,18 +58,44 @@ __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_pre(int64_t n, Partic
 
 // Closing kick (Molecule::upd_postF, sum m v^2) of one step, then the opening kick and drift
 // (Molecule::upd_preF with vcorr = 1) of the next, with the same roundings as the two kernels.
+// Reduction of the block partials inside the kernel (last block) and the step record it completes.
+struct Fold {
+	unsigned* counter;
+	double* out;              // sum m v^2
+	const double* scalars;    // U6 sum, virial sum, pair count of the step (from the pair kernel)
+	double* record;           // {Upot, virial, sum m v^2, pairs} or null
+};
+
+__device__ __forceinline__ void fold(const Fold& f, const double* partials) {
+	if (last_block_sum(f.counter, partials, gridDim.x, 1, f.out) && threadIdx.x == 0 && f.record) {
+		f.record[0] = f.scalars[0] * 0.5 / 6.;
+		f.record[1] = f.scalars[1] * 0.5;
+		f.record[2] = f.out[0];
+		f.record[3] = f.scalars[2] * 0.5;
+	}
+}
+
 __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_post_pre(int64_t n, Particles p, SpeciesScale post,
                                                                    SpeciesScale pre, double dt, double* partials,
-                                                                   int* status, SkinCheck sk) {
+                                                                   int* status, SkinCheck sk, Fold f) {
 	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	double mv2 = 0.0;
 	if (i < n) {
+		// every load first: the arrays may alias as far as the compiler knows
 		const int t = p.cid[i];
 		const double fx = p.fx[i], fy = p.fy[i], fz = p.fz[i];
+		const double vx0 = p.vx[i], vy0 = p.vy[i], vz0 = p.vz[i];
+		const double x0 = p.rx[i], y0 = p.ry[i], z0 = p.rz[i];
+		double rx0 = 0, ry0 = 0, rz0 = 0;
+		if (sk.flag) {
+			rx0 = sk.rx[i];
+			ry0 = sk.ry[i];
+			rz0 = sk.rz[i];
+		}
 		const double a = post.dtInv2m[t];
-		const double vx = __dadd_rn(p.vx[i], __dmul_rn(a, fx));
-		const double vy = __dadd_rn(p.vy[i], __dmul_rn(a, fy));
-		const double vz = __dadd_rn(p.vz[i], __dmul_rn(a, fz));
+		const double vx = __dadd_rn(vx0, __dmul_rn(a, fx));
+		const double vy = __dadd_rn(vy0, __dmul_rn(a, fy));
+		const double vz = __dadd_rn(vz0, __dmul_rn(a, fz));
 		const double v2 = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
 		mv2 = __dmul_rn(post.mass[t], v2);
 		if (!(v2 == v2) || isinf(v2)) atomicOr(status, kStatusNonFinite);
@@ -74,33 +103,36 @@ __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_post_pre(int64_t n, P
 		const double wx = __dadd_rn(__dmul_rn(1.0, vx), __dmul_rn(b, fx));
 		const double wy = __dadd_rn(__dmul_rn(1.0, vy), __dmul_rn(b, fy));
 		const double wz = __dadd_rn(__dmul_rn(1.0, vz), __dmul_rn(b, fz));
+		const double x = __dadd_rn(x0, __dmul_rn(dt, wx));
+		const double y = __dadd_rn(y0, __dmul_rn(dt, wy));
+		const double z = __dadd_rn(z0, __dmul_rn(dt, wz));
 		p.vx[i] = wx;
 		p.vy[i] = wy;
 		p.vz[i] = wz;
-		const double x = __dadd_rn(p.rx[i], __dmul_rn(dt, wx));
-		const double y = __dadd_rn(p.ry[i], __dmul_rn(dt, wy));
-		const double z = __dadd_rn(p.rz[i], __dmul_rn(dt, wz));
 		p.rx[i] = x;
 		p.ry[i] = y;
 		p.rz[i] = z;
 		if (sk.flag) {
-			const double dx = x - sk.rx[i], dy = y - sk.ry[i], dz = z - sk.rz[i];
+			const double dx = x - rx0, dy = y - ry0, dz = z - rz0;
 			if (!(dx * dx + dy * dy + dz * dz <= sk.half2)) *sk.flag = sk.id;
 		}
 	}
 	block_sum3(mv2, 0.0, 0.0, partials);
+	fold(f, partials);
 }
 
 __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_post(int64_t n, Particles p, SpeciesScale s,
-                                                               double* partials, int* status) {
+                                                               double* partials, int* status, Fold f) {
 	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	double mv2 = 0.0;
 	if (i < n) {
 		const int t = p.cid[i];
 		const double a = s.dtInv2m[t];
-		const double vx = __dadd_rn(p.vx[i], __dmul_rn(a, p.fx[i]));
-		const double vy = __dadd_rn(p.vy[i], __dmul_rn(a, p.fy[i]));
-		const double vz = __dadd_rn(p.vz[i], __dmul_rn(a, p.fz[i]));
+		const double vx0 = p.vx[i], vy0 = p.vy[i], vz0 = p.vz[i];
+		const double fx = p.fx[i], fy = p.fy[i], fz = p.fz[i];
+		const double vx = __dadd_rn(vx0, __dmul_rn(a, fx));
+		const double vy = __dadd_rn(vy0, __dmul_rn(a, fy));
+		const double vz = __dadd_rn(vz0, __dmul_rn(a, fz));
 		p.vx[i] = vx;
 		p.vy[i] = vy;
 		p.vz[i] = vz;
@@ -109,6 +141,7 @@ __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_post(int64_t n, Parti
 		if (!(v2 == v2) || isinf(v2)) atomicOr(status, kStatusNonFinite);
 	}
 	block_sum3(mv2, 0.0, 0.0, partials);
+	fold(f, partials);
 }
 
 __global__ void k_scale(int64_t n, Particles p, double beta) {
@@ -166,27 +199,27 @@ cudaError_t launch_leapfrog_pre(Context* c, double dt, double vcorr, bool skin_c
 	return e;
 }
 
-cudaError_t launch_leapfrog_post_pre(Context* c, double dt, bool skin_check) {
+cudaError_t launch_leapfrog_post_pre(Context* c, double dt, bool skin_check, double* record) {
 	prof_begin(c, 2);
 	int64_t nb = c->n > 0 ? blocks_for(c->n) : 1;
+	const Fold f{c->tickets + 1, c->scalars + 3, c->scalars, record};
 	k_leapfrog_post_pre<<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(
 	    c->n, c->p, make_scale(c, 0.5 * dt), make_scale(c, .5 * dt), dt, c->partials, c->status,
-	    skin_check_of(c, skin_check));
+	    skin_check_of(c, skin_check), f);
 	cudaError_t e = cudaGetLastError();
 	prof_end(c, 2, 1);
-	if (e != cudaSuccess) return e;
-	return launch_reduce(c, nb, c->scalars + 3, 1);
+	return e;
 }
 
-cudaError_t launch_leapfrog_post(Context* c, double dt_half) {
+cudaError_t launch_leapfrog_post(Context* c, double dt_half, double* record) {
 	prof_begin(c, 2);
 	int64_t nb = c->n > 0 ? blocks_for(c->n) : 1;
+	const Fold f{c->tickets + 1, c->scalars + 3, c->scalars, record};
 	k_leapfrog_post<<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(c->n, c->p, make_scale(c, dt_half), c->partials,
-	                                                               c->status);
+	                                                               c->status, f);
 	cudaError_t e = cudaGetLastError();
 	prof_end(c, 2, 1);
-	if (e != cudaSuccess) return e;
-	return launch_reduce(c, nb, c->scalars + 3, 1);
+	return e;
 }
 
 cudaError_t launch_scale(Context* c, double beta) {

@@ -91,6 +91,7 @@ struct Context {
 	int64_t steps_cap = 0;
 	int64_t steps_written = 0;      // records appended since the last mdgpu_read_steps
 	int* status = nullptr;          // device status word
+	unsigned* tickets = nullptr;    // last-block counters of the in-kernel reductions (self-resetting)
 	PairParams* d_pp = nullptr;     // device copy of the pair parameters
 	// Verlet-skin mode of mdgpu_step / mdgpu_run (skin > 0): per-molecule candidate lists of radius
 	// rc + skin on a frozen cell structure, rebuilt (with the binning) by device-side gating when a
@@ -135,10 +136,12 @@ int64_t skin_partials_needed(const Context* c);       // reduction partials the 
 // With skin_check the pre-kick also sets *c->rebuild = c->step_id when a molecule is more than
 // skin/2 from its position at the last build.
 cudaError_t launch_leapfrog_pre(Context* c, double dt, double vcorr, bool skin_check = false);
-cudaError_t launch_leapfrog_post(Context* c, double dt_half);   // scalars[3] = sum m v^2
+// scalars[3] = sum m v^2 (reduced inside the kernel); with a record pointer the kernel also writes
+// the step's {Upot, virial, sum m v^2, pairs} there from scalars[0..2].
+cudaError_t launch_leapfrog_post(Context* c, double dt_half, double* record = nullptr);
 // The closing kick of one step and the opening kick of the next in one pass (mdgpu_run): the same
 // operations as launch_leapfrog_post(dt/2) followed by launch_leapfrog_pre(dt, 1).
-cudaError_t launch_leapfrog_post_pre(Context* c, double dt, bool skin_check);
+cudaError_t launch_leapfrog_post_pre(Context* c, double dt, bool skin_check, double* record);
 cudaError_t launch_scale(Context* c, double beta);
 cudaError_t launch_reduce(Context* c, int64_t nblocks, double* out, int nval);
 cudaError_t launch_adjoint(Context* c, const double* gfx, const double* gfy, const double* gfz, double gU, double* ox,

@@ -51,12 +51,14 @@ __global__ void __launch_bounds__(brick::kThreads, 2)
                  const int32_t* __restrict__ cstart, const PairParams* __restrict__ pp,
                  double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
                  double* __restrict__ partials, int* __restrict__ status, const int* __restrict__ gate,
-                 brick::Lists lists) {
+                 brick::Lists lists, unsigned* tickets, double* scalars) {
 	extern __shared__ __align__(16) unsigned char smem[];
 	brick::load_params(smem, brick::layout(p.s_cap, kFP64, 0, false), pp, p.ns);
 	__syncthreads();
 	brick::list_pairs<kFP64, kSingle, kLjIsRc>(p, bx, blockIdx.x, blockIdx.x, smem, rx, ry, rz, cid, cstart, fx,
 	                                           fy, fz, partials, status, lists);
+	// U6 sum, virial sum and pair count of the step, summed by the last brick to finish
+	last_block_sum(tickets, partials, gridDim.x, 3, scalars);
 }
 
 
@@ -85,13 +87,13 @@ Plan plan(Context* c, const Grid& g, double filter_radius, int kind) {
 	return P;
 }
 
-template <typename K>
-cudaError_t go(Context* c, const Plan& P, K kern, const int* gate, const brick::Lists& lists) {
+template <typename K, typename... Extra>
+cudaError_t go(Context* c, const Plan& P, K kern, const int* gate, const brick::Lists& lists, Extra... extra) {
 	cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) P.bytes);
 	if (r == cudaSuccess)
 		kern<<<P.nbricks, brick::kThreads, P.bytes, c->stream>>>(P.p, P.bx, c->p.rx, c->p.ry, c->p.rz, c->p.cid,
 		                                                         c->cell_start, c->d_pp, c->p.fx, c->p.fy, c->p.fz,
-		                                                         c->partials, c->status, gate, lists);
+		                                                         c->partials, c->status, gate, lists, extra...);
 	return r;
 }
 
@@ -101,12 +103,14 @@ cudaError_t dispatch(Context* c, const Plan& P, const int* gate, const brick::Li
 	const bool fp64 = c->precision == MDGPU_FP64;
 	const bool single = c->sp.n == 1, ljrc = c->rc_lj == c->rc;
 	if (kKind == 2) {
-		if (fp64) return single ? go(c, P, k_pairs_list<true, true, false>, gate, lists)
-		                        : go(c, P, k_pairs_list<true, false, false>, gate, lists);
-		if (ljrc) return single ? go(c, P, k_pairs_list<false, true, true>, gate, lists)
-		                        : go(c, P, k_pairs_list<false, false, true>, gate, lists);
-		return single ? go(c, P, k_pairs_list<false, true, false>, gate, lists)
-		              : go(c, P, k_pairs_list<false, false, false>, gate, lists);
+		unsigned* t = c->tickets;
+		double* out = c->scalars;
+		if (fp64) return single ? go(c, P, k_pairs_list<true, true, false>, gate, lists, t, out)
+		                        : go(c, P, k_pairs_list<true, false, false>, gate, lists, t, out);
+		if (ljrc) return single ? go(c, P, k_pairs_list<false, true, true>, gate, lists, t, out)
+		                        : go(c, P, k_pairs_list<false, false, true>, gate, lists, t, out);
+		return single ? go(c, P, k_pairs_list<false, true, false>, gate, lists, t, out)
+		              : go(c, P, k_pairs_list<false, false, false>, gate, lists, t, out);
 	}
 	if (fp64) return single ? go(c, P, k_pairs_brick<true, true, false>, gate, lists)
 	                        : go(c, P, k_pairs_brick<true, false, false>, gate, lists);
@@ -157,12 +161,11 @@ cudaError_t launch_pairs_skin(Context* c) {
 	if (e == cudaSuccess)
 		k_build_lists<<<nbricks, brick::kThreads, bbytes, c->stream>>>(bb, s_cap, c->p.rx, c->p.ry, c->p.rz,
 		                                                              c->cell_start, c->rebuild, c->step_id, l);
-	// evaluation, every step
+	// evaluation, every step (sums reduced inside the kernel)
 	if (e == cudaSuccess) e = dispatch<2>(c, P, nullptr, l);
 	if (e == cudaSuccess) e = cudaGetLastError();
 	prof_end(c, 1, 2);
-	if (e != cudaSuccess) return e;
-	return launch_reduce(c, P.nbricks, c->scalars, 3);
+	return e;
 }
 
 int64_t skin_partials_needed(const Context* c) {

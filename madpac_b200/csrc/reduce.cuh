@@ -41,4 +41,38 @@ __device__ __forceinline__ void block_sum3(double a, double b, double c, double*
 	block_sum3_at(a, b, c, partials, blockIdx.x);
 }
 
+// Run by every thread of every block after the block's partials (written by its thread 0) are in
+// place: the last block to arrive (ticket counter, reset here) sums the nparts partials in a fixed
+// order into out[0..nval) -- the same sums run to run, without a separate reduction launch.
+// Returns true in the block that did the sum (blockDim.x <= kReduceBlock).
+__device__ __forceinline__ bool last_block_sum(unsigned* counter, const double* partials, int64_t nparts, int nval,
+                                               double* out) {
+	__shared__ int s_last;
+	__shared__ double sh[4][kReduceBlock / 32];
+	__threadfence();
+	__syncthreads();
+	if (threadIdx.x == 0) s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+	__syncthreads();
+	if (!s_last) return false;
+	__threadfence();
+	double acc[4] = {0, 0, 0, 0};
+	for (int64_t b = threadIdx.x; b < nparts; b += blockDim.x)
+		for (int k = 0; k < nval; k++) acc[k] += __ldcg(partials + b * 4 + k);
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	for (int k = 0; k < nval; k++) {
+		const double v = warp_sum(acc[k]);
+		if (lane == 0) sh[k][warp] = v;
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		for (int k = 0; k < nval; k++) {
+			double t = 0;
+			for (int w = 0; w < (int) (blockDim.x >> 5); w++) t += sh[k][w];
+			out[k] = t;
+		}
+		*counter = 0u;
+	}
+	return true;
+}
+
 }  // namespace mdgpu
