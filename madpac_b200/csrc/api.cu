@@ -412,6 +412,7 @@ int mdgpu_destroy(mdgpu_ctx* ctx) {
 	cudaFree(c->bar);
 	cudaFree(c->chunk);
 	cudaFree(c->tickets);
+	cudaFree(c->brick_kind);
 	cudaFree(full->x.stage.ptr);
 	if (c->h_scalars) cudaFreeHost(c->h_scalars);
 	if (c->h_status) cudaFreeHost(c->h_status);
@@ -726,6 +727,12 @@ int skin_prepare(Context* c) {
 		c->lists_valid = false;
 	}
 	const int64_t parts = skin_partials_needed(c);
+	if (c->brick_kind == nullptr || c->list_n != n || c->lists_valid == false) {
+		cudaFree(c->brick_kind);
+		c->brick_kind = nullptr;
+		MD_CUDA(cudaMalloc(&c->brick_kind, parts));
+		MD_CUDA(cudaMemsetAsync(c->brick_kind, 0, parts, c->stream));
+	}
 	if (c->partial_cap < parts) {
 		MD_CUDA(cudaStreamSynchronize(c->stream));
 		cudaFree(c->partials);

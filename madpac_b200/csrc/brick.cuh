@@ -431,7 +431,11 @@ struct Lists {
 	int cap;
 	unsigned long long* builds;        // incremented once per build
 	int sentinel;                      // staged slot of the list kernel's far-away sentinel
+	unsigned char* kind;               // per brick: 1 = sparse (evaluated one warp per brick)
 };
+// A brick is sparse when its whole staged region holds at most kSparseCap molecules and its own
+// cells at most 32: one warp stages and evaluates it, without CTA-wide barriers.
+constexpr int kSparseCap = 128;
 constexpr unsigned short kListOverflow = 0xffff;
 
 // Forces on the molecules of brick `brick` (index within its box) of box `bx`; U, W and the pair
@@ -743,13 +747,21 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 			}
 		}
 	}
-	if (brick == 0 && tid == 0) atomicAdd(lists.builds, 1ull);
+	if (tid == 0) {
+		int n_own = 0;
+		for (int w = 0; w < kWarps; w++) {
+			int ic;
+			if (own_cell(bx, brick, w, ic)) n_own += s_cnt[ic];
+		}
+		lists.kind[brick] = (s_cs[64] <= kSparseCap && n_own <= 32) ? 1 : 0;
+		if (brick == 0) atomicAdd(lists.builds, 1ull);
+	}
 }
 
 // One chunk of 32 of the brick's own molecules (t0 .. t0 + 31 in the order of the own cells
 // own[0..8] / ocell[0..7]) evaluating their lists, one molecule per lane: forces written, U, W,
 // pair count and the same-position flag accumulated into the caller's sums.
-template <bool kFP64, bool kSingle, bool kLjIsRc>
+template <bool kFP64, bool kSingle, bool kLjIsRc, bool kClampJ = false>
 __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const Smem& S, const int* s_own,
                                            const int* s_ocell, int t0, int n_own, const double* rx, const double* ry,
                                            const double* rz, const int32_t* cid, const int32_t* cstart, double* fx,
@@ -864,7 +876,8 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 			unsigned ambm = 0u;
 #pragma unroll
 			for (int u = 0; u < 8; u++) {
-				const int j = (int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu);
+				int j = (int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu);
+				if (kClampJ) j = min(j, p.s_cap);   // a padding entry is the caller's sentinel slot
 				const float4 hj = S.hi[j];
 				const unsigned wj = __float_as_uint(hj.w);
 				const float h0 = hi_i.x - hj.x, h1 = hi_i.y - hj.y, h2 = hi_i.z - hj.z;  // exact
@@ -911,7 +924,8 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 				while (ambm) {
 					const int u = __ffs(ambm) - 1;
 					ambm &= ambm - 1u;
-					const int j = (int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu);
+					int j = (int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu);
+					if (kClampJ) j = min(j, p.s_cap);
 					const float4 hj = S.hi[j];
 					const unsigned wj = __float_as_uint(hj.w);
 					const float e0 = fmaf(mix - __uint_as_float(0x4B000000u | (wj & 511u)), bx.lo_step[0], hi_i.x - hj.x);
@@ -1012,6 +1026,135 @@ __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int br
 	}
 	if (same) atomicOr(status, kStatusSamePosition);
 	block_sum3_at(U, W, NP, partials, slot);
+}
+
+// A sparse brick (see kSparseCap) by one warp, in its own shared-memory area laid out as
+// layout(kSparseCap, kFP64, 0, false) plus 17 ints (own-cell prefix and cells): staging of the 4x4x4
+// region flattened over its molecules (cell found by bisection of the staged-cell starts), then
+// list_chunk; U, W, pair count to partials[brick]. Warp-level synchronisation only.
+__host__ __device__ inline size_t sparse_warp_bytes(bool fp64) {
+	return align16(layout(kSparseCap, fp64, 0, false).total + sizeof(int) * 17);
+}
+
+template <bool kFP64, bool kSingle, bool kLjIsRc>
+__device__ __forceinline__ void list_pairs_warp(const Const& p, const Box& bx, int brick, unsigned char* ws,
+                                                const double* rx, const double* ry, const double* rz,
+                                                const int32_t* cid, const int32_t* cstart, double* fx, double* fy,
+                                                double* fz, double* partials, int* status, const Lists& lists) {
+	const SmemLayout L = layout(kSparseCap, kFP64, 0, false);
+	const Smem S = views(ws, L);
+	int* own = reinterpret_cast<int*>(ws + L.total);
+	const int lane = threadIdx.x & 31;
+	const Grid& g = bx.g;
+	const int bc[3] = {brick % bx.nb[0], (brick / bx.nb[0]) % bx.nb[1], brick / (bx.nb[0] * bx.nb[1])};
+	for (int c = lane; c < 64; c += 32) {
+		const int l[3] = {c & 3, (c >> 2) & 3, c >> 4};
+		int gc[3];
+		for (int d = 0; d < 3; d++) {
+			int gcd = 2 * bc[d] - 1 + l[d];
+			double sh = 0.0;
+			if (gcd < 0) {
+				gcd += g.nc[d];
+				sh = -g.L[d];
+			} else if (gcd >= g.nc[d]) {
+				gcd -= g.nc[d];
+				sh = g.L[d];
+			}
+			gc[d] = gcd;
+			S.csh[3 * c + d] = sh;
+			const double cbr = (2 * bc[d] + 1) * g.cell_length[d];
+			S.ck[3 * c + d] = (sh - cbr) + (double) bx.frame_c[d];
+		}
+		const int gcell = bx.coff + (gc[2] * g.nc[1] + gc[1]) * g.nc[0] + gc[0];
+		const int st = cstart[gcell];
+		S.gst[c] = st;
+		S.cnt[c] = max(0, cstart[gcell + 1] - st);
+	}
+	__syncwarp();
+	{
+		const int a = S.cnt[2 * lane], b = S.cnt[2 * lane + 1];
+		int inc = a + b;
+		for (int o = 1; o < 32; o <<= 1) {
+			const int y = __shfl_up_sync(kFull, inc, o);
+			if (lane >= o) inc += y;
+		}
+		const int excl = inc - (a + b);
+		S.cs[2 * lane] = excl;
+		S.cs[2 * lane + 1] = excl + a;
+		if (lane == 31) S.cs[64] = inc;
+	}
+	__syncwarp();
+	const int total = S.cs[64];
+	const bool staged = total <= kSparseCap;
+	if (staged) {
+		for (int t = lane; t < total; t += 32) {
+			int lo = 0, hi = 63;
+			while (lo < hi) {
+				const int mid = (lo + hi + 1) >> 1;
+				if (S.cs[mid] <= t)
+					lo = mid;
+				else
+					hi = mid - 1;
+			}
+			const int gi = S.gst[lo] + (t - S.cs[lo]);
+			const double x = rx[gi], y = ry[gi], z = rz[gi];
+			const double Xd = __dadd_rn(x, S.ck[3 * lo]), Yd = __dadd_rn(y, S.ck[3 * lo + 1]);
+			const double Zd = __dadd_rn(z, S.ck[3 * lo + 2]);
+			const float X = __double2float_rn(Xd), Y = __double2float_rn(Yd), Z = __double2float_rn(Zd);
+			const unsigned w = pack_lo(__double2float_rn(Xd - (double) X), __double2float_rn(Yd - (double) Y),
+			                           __double2float_rn(Zd - (double) Z), cid[gi], bx);
+			S.hi[t] = make_float4(X, Y, Z, __uint_as_float(w));
+			if (kFP64) {
+				S.img[t] = __dadd_rn(x, S.csh[3 * lo]);
+				S.img[kSparseCap + t] = __dadd_rn(y, S.csh[3 * lo + 1]);
+				S.img[2 * kSparseCap + t] = __dadd_rn(z, S.csh[3 * lo + 2]);
+			}
+		}
+	}
+	if (lane == 0) {
+		int acc = 0;
+		for (int w = 0; w < 8; w++) {
+			int ic;
+			const bool ok = own_cell(bx, brick, w, ic);
+			own[w] = acc;
+			own[9 + w] = ic;
+			acc += ok ? S.cnt[ic] : 0;
+		}
+		own[8] = acc;
+	}
+	__syncwarp();
+	const int n_own = own[8];
+	double U = 0.0, W = 0.0, NP = 0.0;
+	bool same = false;
+	if (staged) {
+		for (int t0 = 0; t0 < n_own; t0 += 32)
+			list_chunk<kFP64, kSingle, kLjIsRc, true>(p, bx, S, own, own + 9, t0, n_own, rx, ry, rz, cid, cstart, fx,
+			                                          fy, fz, status, lists, U, W, NP, same);
+	} else {
+		for (int t = lane; t < n_own; t += 32) {
+			int w = 0;
+			while (w < 7 && own[w + 1] <= t) w++;
+			const int gi = S.gst[own[9 + w]] + (t - own[w]);
+			PairSums ps = gather_pairs<!kFP64>(gi, rx, ry, rz, cid, cstart, g, S.pd, p.ns, p.rc2, p.rclj2, bx.coff);
+			fx[gi] = ps.F[0];
+			fy[gi] = ps.F[1];
+			fz[gi] = ps.F[2];
+			U += ps.U;
+			W += ps.W;
+			NP += ps.np;
+			same |= ps.same;
+		}
+	}
+	if (same) atomicOr(status, kStatusSamePosition);
+	U = warp_sum(U);
+	W = warp_sum(W);
+	NP = warp_sum(NP);
+	if (lane == 0) {
+		partials[4 * (int64_t) brick + 0] = U;
+		partials[4 * (int64_t) brick + 1] = W;
+		partials[4 * (int64_t) brick + 2] = NP;
+		partials[4 * (int64_t) brick + 3] = 0.0;
+	}
 }
 
 }  // namespace brick

@@ -105,6 +105,7 @@ struct Context {
 	unsigned short* nbr_count = nullptr;
 	double* r_ref = nullptr;        // 3 x n positions at the last build
 	int* rebuild = nullptr;         // device: the step id for which a build was asked
+	unsigned char* brick_kind = nullptr;   // per skin-grid brick: 1 = sparse
 	int step_id = 0;                // id of the step being enqueued (skin mode)
 	unsigned* bar = nullptr;        // grid-barrier words of the cooperative rebuild
 	int32_t* chunk = nullptr;       // per-CTA scan sums of the cooperative rebuild

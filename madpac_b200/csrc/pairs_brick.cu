@@ -55,10 +55,45 @@ __global__ void __launch_bounds__(brick::kThreads, 2)
 	extern __shared__ __align__(16) unsigned char smem[];
 	brick::load_params(smem, brick::layout(p.s_cap, kFP64, 0, false), pp, p.ns);
 	__syncthreads();
-	brick::list_pairs<kFP64, kSingle, kLjIsRc>(p, bx, blockIdx.x, blockIdx.x, smem, rx, ry, rz, cid, cstart, fx,
-	                                           fy, fz, partials, status, lists);
+	// sparse bricks were evaluated by k_pairs_list_sparse (launched before)
+	if (!lists.kind[blockIdx.x])
+		brick::list_pairs<kFP64, kSingle, kLjIsRc>(p, bx, blockIdx.x, blockIdx.x, smem, rx, ry, rz, cid, cstart, fx,
+		                                           fy, fz, partials, status, lists);
 	// U6 sum, virial sum and pair count of the step, summed by the last brick to finish
 	last_block_sum(tickets, partials, gridDim.x, 3, scalars);
+}
+
+// Sparse bricks (few molecules, e.g. a vapour), one warp each, eight per CTA.
+template <bool kFP64, bool kSingle, bool kLjIsRc>
+__global__ void __launch_bounds__(brick::kThreads, 2)
+    k_pairs_list_sparse(brick::Const p, brick::Box bx, int nbricks, const double* __restrict__ rx,
+                        const double* __restrict__ ry, const double* __restrict__ rz,
+                        const int32_t* __restrict__ cid, const int32_t* __restrict__ cstart,
+                        const PairParams* __restrict__ pp, double* __restrict__ fx, double* __restrict__ fy,
+                        double* __restrict__ fz, double* __restrict__ partials, int* __restrict__ status,
+                        brick::Lists lists) {
+	extern __shared__ __align__(16) unsigned char smem[];
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int brick_id = blockIdx.x * brick::kWarps + warp;
+	if (brick_id >= nbricks || !lists.kind[brick_id]) return;
+	unsigned char* ws = smem + warp * brick::sparse_warp_bytes(kFP64);
+	const brick::SmemLayout L = brick::layout(brick::kSparseCap, kFP64, 0, false);
+	double* pd = reinterpret_cast<double*>(ws + L.params);
+	float* pf = reinterpret_cast<float*>(pd + 3 * brick::KK);
+	for (int k = lane; k < p.ns * p.ns; k += 32) {
+		pd[k] = pp->eps24[k];
+		pd[brick::KK + k] = pp->sig2[k];
+		pd[2 * brick::KK + k] = pp->shift6[k];
+		pf[k] = (float) pp->eps24[k];
+		pf[brick::KK + k] = (float) pp->sig2[k];
+		pf[2 * brick::KK + k] = (float) pp->shift6[k];
+	}
+	if (lane == 0)
+		reinterpret_cast<float4*>(ws + L.hi)[brick::kSparseCap] =
+		    make_float4(1e15f, 1e15f, 1e15f, __uint_as_float((256u << 18) | (256u << 9) | 256u));
+	__syncwarp();
+	brick::list_pairs_warp<kFP64, kSingle, kLjIsRc>(p, bx, brick_id, ws, rx, ry, rz, cid, cstart, fx, fy, fz,
+	                                                partials, status, lists);
 }
 
 
@@ -130,6 +165,7 @@ brick::Lists lists_of(Context* c) {
 	l.n = c->n;
 	l.cap = c->list_cap;
 	l.builds = c->builds;
+	l.kind = c->brick_kind;
 	return l;
 }
 
@@ -161,10 +197,26 @@ cudaError_t launch_pairs_skin(Context* c) {
 	if (e == cudaSuccess)
 		k_build_lists<<<nbricks, brick::kThreads, bbytes, c->stream>>>(bb, s_cap, c->p.rx, c->p.ry, c->p.rz,
 		                                                              c->cell_start, c->rebuild, c->step_id, l);
-	// evaluation, every step (sums reduced inside the kernel)
+	// evaluation, every step: sparse bricks one warp each, then the others (whose last CTA sums the
+	// partials of all bricks)
+	if (e == cudaSuccess) {
+		const bool fp64 = c->precision == MDGPU_FP64;
+		const bool single = c->sp.n == 1, ljrc = c->rc_lj == c->rc;
+		auto ks = fp64 ? (single ? k_pairs_list_sparse<true, true, false> : k_pairs_list_sparse<true, false, false>)
+		               : (single ? (ljrc ? k_pairs_list_sparse<false, true, true> : k_pairs_list_sparse<false, true, false>)
+		                         : (ljrc ? k_pairs_list_sparse<false, false, true>
+		                                 : k_pairs_list_sparse<false, false, false>));
+		const size_t sbytes = brick::kWarps * brick::sparse_warp_bytes(fp64);
+		const brick::Const ps = brick::make_const(c->sp.n, brick::kSparseCap, c->rc, c->rc_lj);
+		e = cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sbytes);
+		if (e == cudaSuccess)
+			ks<<<(P.nbricks + brick::kWarps - 1) / brick::kWarps, brick::kThreads, sbytes, c->stream>>>(
+			    ps, P.bx, P.nbricks, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->cell_start, c->d_pp, c->p.fx, c->p.fy,
+			    c->p.fz, c->partials, c->status, l);
+	}
 	if (e == cudaSuccess) e = dispatch<2>(c, P, nullptr, l);
 	if (e == cudaSuccess) e = cudaGetLastError();
-	prof_end(c, 1, 2);
+	prof_end(c, 1, 3);
 	return e;
 }
 
