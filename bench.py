@@ -123,8 +123,13 @@ class Dist:
 # ---------------------------------------------------------------------------- clocks
 
 class ClockSampler:
-    """nvidia-smi samples during the timed region (read-only queries)."""
+    """SM clock, power and clock-event reasons sampled during the timed region (read-only queries):
+    an NVML polling thread every 5 ms (timed regions of a few ms still get samples), else
+    nvidia-smi at 200 ms."""
 
+    # NVML clock-event reason bits (nvml.h: nvmlClocksEventReason*)
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40}
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -132,9 +137,44 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.path = None
+        self.thread = None
+        self.rows = []
+
+    def _nvml_loop(self, nv, h):
+        while not self.done:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                try:
+                    rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                except AttributeError:
+                    rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                self.rows.append((float(sm), float(mx), int(rs)))
+            except Exception:
+                pass
+            time.sleep(0.005)
 
     def start(self):
+        import threading
+
+        try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+            # NVML enumerates all GPUs; map the CUDA-visible index through the PCI bus id
+            import torch
+
+            pr = torch.cuda.get_device_properties(self.gpu)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            h = nv.nvmlDeviceGetHandleByPciBusId(bus.encode())
+            self.done = False
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.thread.start()
+            while not self.rows and self.thread.is_alive():
+                time.sleep(0.002)
+            return
+        except Exception:
+            self.thread = None
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
@@ -146,6 +186,15 @@ class ClockSampler:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.done = True
+            self.thread.join(timeout=2)
+            rows = self.rows[1:] if len(self.rows) > 1 else self.rows   # the first one precedes the region
+            if not rows:
+                return None
+            reasons = sorted({k for r in rows for k, bit in self.REASONS.items() if r[2] & bit})
+            return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                    "reasons": reasons, "samples": len(rows), "source": "NVML, 5 ms period"}
         if not self.proc:
             return None
         self.proc.terminate()
@@ -167,7 +216,7 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi, 200 ms period"}
 
 
 # ---------------------------------------------------------------------------- our arm
@@ -464,6 +513,7 @@ def run_batched(args, dist: Dist):
     systems = W.config_c4(seed=4 + dist.rank, n_boxes=args.boxes)
     dt = systems[0].dt
     b = M.Batch.from_systems(systems, precision, device=dist.local)
+    b.setSkin(args.skin)
     prep = b.prepare()
     best, cand_ms = b.autotune(dt, trial_steps=5)
     b.run(args.warmup, dt, record=False)
@@ -500,6 +550,7 @@ def run_batched(args, dist: Dist):
             lc = M.LinkedCells.from_system(s, precision, device=dist.local)
             lc.update()
             lc.traversePairs()
+            lc.setSkin(args.skin)
             ctxs.append(lc)
         for lc in ctxs:
             lc.runAsync(2, dt)
@@ -529,7 +580,8 @@ def run_batched(args, dist: Dist):
         "data": "synthetic (seeded FCC subsets, Maxwell-Boltzmann velocities)",
         "config": {"workload": f"c4_{len(systems)}_boxes", "n_boxes": len(systems), "n_molecules": ntot,
                    "n_min": min(s.n for s in systems), "n_max": max(s.n for s in systems), "cutoff": 2.5,
-                   "dt": dt, "ensemble": "NVE", "tiles": {"list_cap": best[0], "ctas_per_sm": best[1],
+                   "dt": dt, "ensemble": "NVE", "verlet_skin": args.skin,
+                   "skin_builds": b.skinBuilds() if args.skin > 0 else None, "tiles": {"list_cap": best[0], "ctas_per_sm": best[1],
                                                          "brick_queue": best[2]},
                    "autotune_ms_per_step": {f"cap{c}_ctas{t}_q{q}": v for (c, t, q), v in cand_ms.items()},
                    "l2": f"working set larger than L2 ({ntot * 200 / 1e6:.0f} MB of molecule arrays)"},

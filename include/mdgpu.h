@@ -222,6 +222,11 @@ int mdgpu_batch_last_run_ms(const mdgpu_batch* b, double* ms);
 /* Limit of each grid-barrier wait in nanoseconds (default 2e9); a wait that runs out sets
  * MDGPU_ERR_TIMEOUT and the kernel returns. */
 int mdgpu_batch_set_barrier_timeout(mdgpu_batch* b, int64_t ns);
+/* Verlet-skin mode of the batch (as mdgpu_set_skin, per box: a box is re-binned and its candidate
+ * lists rebuilt inside the step when one of its molecules moved more than skin/2). Takes effect at
+ * the next mdgpu_batch_prepare; 0 = off. mdgpu_batch_skin_builds: box list builds so far. */
+int mdgpu_batch_set_skin(mdgpu_batch* b, double skin);
+int mdgpu_batch_skin_builds(const mdgpu_batch* b, int64_t* builds);
 
 #ifdef __cplusplus
 }

@@ -72,6 +72,15 @@ struct StepArgs {
 	int64_t timeout_ns;
 	int integrate;              // 0: wrap, bin and forces only (initial force evaluation)
 	int dynamic;                // 0: bricks by static stride, 1: by atomic queue
+	// Verlet-skin mode: the state stays in src (dst is the sort scratch); a box is re-binned and its
+	// lists rebuilt when one of its molecules moved more than skin/2 since its last build
+	int skin;
+	double half_skin2;
+	brick::Lists lists;
+	int* box_flag;              // nboxes: 1 = built in this step
+	int* valid;                 // 0: every box builds (molecules just loaded)
+	int build_cap;              // staged capacity of the list build
+	brick::Const lc;            // constants of the list evaluation (its staged capacity)
 };
 
 // Shared-memory bytes of phase A for a box of n molecules and m cells.
@@ -222,20 +231,21 @@ __device__ void bin_box(const StepArgs& a, const BatchBox& B, unsigned char* sme
 __device__ void finish_box(const StepArgs& a, const BatchBox& B, int b) {
 	__shared__ double s_w[kThreads / 32];
 	const int tid = threadIdx.x;
+	const Particles& P = a.skin ? a.src : a.dst;
 	double mv2 = 0.0;
 	bool bad = false;
 	for (int t = tid; t < B.n; t += kThreads) {
 		const int64_t i = B.poff + t;
-		const int ty = a.dst.cid[i];
-		double vx = a.dst.vx[i], vy = a.dst.vy[i], vz = a.dst.vz[i];
+		const int ty = P.cid[i];
+		double vx = P.vx[i], vy = P.vy[i], vz = P.vz[i];
 		if (a.integrate) {
 			const double k = a.kick.post[ty];
-			vx = __dadd_rn(vx, __dmul_rn(k, a.dst.fx[i]));
-			vy = __dadd_rn(vy, __dmul_rn(k, a.dst.fy[i]));
-			vz = __dadd_rn(vz, __dmul_rn(k, a.dst.fz[i]));
-			a.dst.vx[i] = vx;
-			a.dst.vy[i] = vy;
-			a.dst.vz[i] = vz;
+			vx = __dadd_rn(vx, __dmul_rn(k, P.fx[i]));
+			vy = __dadd_rn(vy, __dmul_rn(k, P.fy[i]));
+			vz = __dadd_rn(vz, __dmul_rn(k, P.fz[i]));
+			P.vx[i] = vx;
+			P.vy[i] = vy;
+			P.vz[i] = vz;
 		}
 		const double v2 = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
 		mv2 += __dmul_rn(a.kick.mass[ty], v2);
@@ -265,6 +275,62 @@ __device__ void finish_box(const StepArgs& a, const BatchBox& B, int b) {
 	__syncthreads();
 }
 
+// Phase A of the Verlet-skin mode for box b: kick-drift in place (no wrap), displacement against
+// the positions of the box's last build; when one moved more than skin/2 (or the lists are not
+// valid) the box is wrapped, binned and sorted into the scratch buffer and copied back.
+__device__ void skin_box(const StepArgs& a, const BatchBox& B, int b, unsigned char* smem) {
+	__shared__ int s_any;
+	const int tid = threadIdx.x;
+	if (tid == 0) s_any = 0;
+	__syncthreads();
+	if (a.integrate) {
+		bool moved = false;
+		for (int t = tid; t < B.n; t += kThreads) {
+			const int64_t i = B.poff + t;
+			const double k = a.kick.pre[a.src.cid[i]];
+			const double vx0 = a.src.vx[i], vy0 = a.src.vy[i], vz0 = a.src.vz[i];
+			const double fx = a.src.fx[i], fy = a.src.fy[i], fz = a.src.fz[i];
+			const double x0 = a.src.rx[i], y0 = a.src.ry[i], z0 = a.src.rz[i];
+			const double vx = __dadd_rn(__dmul_rn(1.0, vx0), __dmul_rn(k, fx));
+			const double vy = __dadd_rn(__dmul_rn(1.0, vy0), __dmul_rn(k, fy));
+			const double vz = __dadd_rn(__dmul_rn(1.0, vz0), __dmul_rn(k, fz));
+			const double x = __dadd_rn(x0, __dmul_rn(a.dt, vx));
+			const double y = __dadd_rn(y0, __dmul_rn(a.dt, vy));
+			const double z = __dadd_rn(z0, __dmul_rn(a.dt, vz));
+			a.src.vx[i] = vx;
+			a.src.vy[i] = vy;
+			a.src.vz[i] = vz;
+			a.src.rx[i] = x;
+			a.src.ry[i] = y;
+			a.src.rz[i] = z;
+			const double dx = x - a.lists.rx_ref[i], dy = y - a.lists.ry_ref[i], dz = z - a.lists.rz_ref[i];
+			if (!(dx * dx + dy * dy + dz * dz <= a.half_skin2)) moved = true;
+		}
+		if (moved) s_any = 1;
+	}
+	__syncthreads();
+	const bool rebuild = s_any != 0 || *a.valid == 0;
+	if (rebuild) {
+		StepArgs a2 = a;
+		a2.integrate = 0;
+		bin_box(a2, B, smem);
+		for (int t = tid; t < B.n; t += kThreads) {
+			const int64_t i = B.poff + t;
+			a.src.rx[i] = a.dst.rx[i];
+			a.src.ry[i] = a.dst.ry[i];
+			a.src.rz[i] = a.dst.rz[i];
+			a.src.vx[i] = a.dst.vx[i];
+			a.src.vy[i] = a.dst.vy[i];
+			a.src.vz[i] = a.dst.vz[i];
+			a.src.id[i] = a.dst.id[i];
+			a.src.cid[i] = a.dst.cid[i];
+			a.src.uidx[i] = a.dst.uidx[i];
+		}
+	}
+	if (tid == 0) a.box_flag[b] = rebuild ? 1 : 0;
+	__syncthreads();
+}
+
 // Boxes of this CTA: j-th in the snake order over boxes sorted by decreasing size.
 template <typename F>
 __device__ __forceinline__ void for_my_boxes(const StepArgs& a, F&& f) {
@@ -276,7 +342,7 @@ __device__ __forceinline__ void for_my_boxes(const StepArgs& a, F&& f) {
 }
 
 template <bool kFP64, bool kSingle, bool kLjIsRc, int kCap>
-__global__ void __launch_bounds__(kThreads) k_batch_step(StepArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) k_batch_step(StepArgs a) {
 	extern __shared__ __align__(16) unsigned char smem[];
 	__shared__ int s_flag;
 	__shared__ int s_item;
@@ -285,15 +351,15 @@ __global__ void __launch_bounds__(kThreads) k_batch_step(StepArgs a) {
 	if (s_flag) return;   // an earlier launch gave up at a barrier: do nothing until the host resets
 
 	// ---- A: per box kick-drift, wrap, bin, sort ----------------------------------------------
-	for_my_boxes(a, [&](int b) { bin_box(a, a.boxes[b], smem); });
+	if (a.skin)
+		for_my_boxes(a, [&](int b) { skin_box(a, a.boxes[b], b, smem); });
+	else
+		for_my_boxes(a, [&](int b) { bin_box(a, a.boxes[b], smem); });
 	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
 
-	// ---- B: pair forces of every brick -------------------------------------------------------
-	const brick::SmemLayout L = brick::layout(a.pc.s_cap, kFP64, kCap);
-	brick::load_params(smem, L, a.pp, a.pc.ns);
-	__syncthreads();
-	auto do_brick = [&](int item) {
-		int lo = 0, hi = a.nboxes - 1;   // box with brick0[box] <= item < brick0[box + 1]
+	// brick of a global brick index: box with brick0[box] <= item < brick0[box + 1]
+	auto box_of = [&](int item) {
+		int lo = 0, hi = a.nboxes - 1;
 		while (lo < hi) {
 			const int mid = (lo + hi + 1) >> 1;
 			if (a.brick0[mid] <= item)
@@ -301,28 +367,70 @@ __global__ void __launch_bounds__(kThreads) k_batch_step(StepArgs a) {
 			else
 				hi = mid - 1;
 		}
-		const BatchBox& B = a.boxes[lo];
-		brick::pairs<kFP64, kSingle, kLjIsRc, kCap>(a.pc, B.bx, item - B.brick0, item, smem, a.dst.rx, a.dst.ry,
-		                                            a.dst.rz, a.dst.cid, a.cstart, a.dst.fx, a.dst.fy, a.dst.fz,
-		                                            a.partials, a.status);
-		__syncthreads();
+		return lo;
 	};
-	if (a.dynamic) {
-		for (;;) {
-			if (threadIdx.x == 0) s_item = (int) atomicAdd(a.bar + 2, 1u);
-			__syncthreads();
-			const int item = s_item;
-			__syncthreads();
-			if (item >= a.total_bricks) break;
-			do_brick(item);
+	// every brick once, by static stride or from the queue bar[q]
+	auto for_bricks = [&](int q, auto&& f) {
+		if (a.dynamic) {
+			for (;;) {
+				if (threadIdx.x == 0) s_item = (int) atomicAdd(a.bar + q, 1u);
+				__syncthreads();
+				const int item = s_item;
+				__syncthreads();
+				if (item >= a.total_bricks) break;
+				f(item);
+			}
+		} else {
+			for (int item = blockIdx.x; item < a.total_bricks; item += gridDim.x) f(item);
 		}
+	};
+
+	if (!a.skin) {
+		// ---- B: pair forces of every brick (filter and evaluation) ----------------------------
+		const brick::SmemLayout L = brick::layout(a.pc.s_cap, kFP64, kCap);
+		brick::load_params(smem, L, a.pp, a.pc.ns);
+		__syncthreads();
+		for_bricks(2, [&](int item) {
+			const BatchBox& B = a.boxes[box_of(item)];
+			brick::pairs<kFP64, kSingle, kLjIsRc, kCap>(a.pc, B.bx, item - B.brick0, item, smem, a.dst.rx, a.dst.ry,
+			                                            a.dst.rz, a.dst.cid, a.cstart, a.dst.fx, a.dst.fy, a.dst.fz,
+			                                            a.partials, a.status);
+			__syncthreads();
+		});
 	} else {
-		for (int item = blockIdx.x; item < a.total_bricks; item += gridDim.x) do_brick(item);
+		// ---- B1: candidate lists of the boxes that were re-binned -----------------------------
+		for_bricks(2, [&](int item) {
+			const int b = box_of(item);
+			if (!a.box_flag[b]) return;
+			const BatchBox& B = a.boxes[b];
+			brick::build_lists(B.bx, item - B.brick0, a.build_cap, smem, a.src.rx, a.src.ry, a.src.rz, a.cstart, a.lists,
+			                   item);
+			__syncthreads();
+		});
+		if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
+		// ---- B2: list evaluation of every brick -----------------------------------------------
+		const brick::SmemLayout L = brick::layout(a.lc.s_cap, kFP64, 0, false);
+		brick::load_params(smem, L, a.pp, a.lc.ns);
+		if (threadIdx.x == 0)
+			reinterpret_cast<float4*>(smem + L.hi)[a.lc.s_cap] =
+			    make_float4(1e15f, 1e15f, 1e15f, __uint_as_float((256u << 18) | (256u << 9) | 256u));
+		__syncthreads();
+		for_bricks(3, [&](int item) {
+			const BatchBox& B = a.boxes[box_of(item)];
+			brick::list_pairs<kFP64, kSingle, kLjIsRc>(a.lc, B.bx, item - B.brick0, item, smem, a.src.rx, a.src.ry,
+			                                           a.src.rz, a.src.cid, a.cstart, a.src.fx, a.src.fy, a.src.fz,
+			                                           a.partials, a.status, a.lists);
+			__syncthreads();
+		});
 	}
 	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
 
 	// ---- C: per box post-kick and records ----------------------------------------------------
-	if (blockIdx.x == 0 && threadIdx.x == 0) a.bar[2] = 0u;   // queue is idle until the next launch
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
+		a.bar[2] = 0u;   // queues are idle until the next launch
+		a.bar[3] = 0u;
+		if (a.skin) *a.valid = 1;
+	}
 	for_my_boxes(a, [&](int b) { finish_box(a, a.boxes[b], b); });
 }
 
@@ -351,6 +459,24 @@ __global__ void k_store3(int64_t n, const double* x, const double* y, const doub
 	aos[3 * u] = x[s];
 	aos[3 * u + 1] = y[s];
 	aos[3 * u + 2] = z[s];
+}
+
+// positions -> caller order, wrapped into [0, L) of their box (r<0 -> r+L, r>=L -> r-L)
+__global__ void k_store3_wrap(int64_t n, const double* x, const double* y, const double* z, const int32_t* uidx,
+                              const int32_t* bid, const double* len, double* __restrict__ aos) {
+	const int64_t s = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= n) return;
+	const int64_t u = uidx[s];
+	const double* L = len + 3 * bid[s];
+	const double r[3] = {x[s], y[s], z[s]};
+	for (int d = 0; d < 3; d++) {
+		double w = r[d];
+		if (w < 0.0)
+			w = __dadd_rn(w, L[d]);
+		else if (w >= L[d])
+			w = __dsub_rn(w, L[d]);
+		aos[3 * u + d] = w;
+	}
 }
 
 template <typename T>
@@ -390,6 +516,7 @@ struct Batch {
 	int64_t ntotal = 0;
 	int total_cells = 0, total_bricks = 0;
 	std::vector<BatchBox> h_boxes;
+	std::vector<int32_t> h_brick0;
 	std::vector<int32_t> h_order;
 	std::string err;
 	Particles buf[2]{};
@@ -418,6 +545,20 @@ struct Batch {
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 	double last_ms = 0.0;
 	int num_sms = 0, max_optin = 0;
+	// Verlet-skin mode
+	double skin = 0.0;
+	std::vector<double> h_len;    // nboxes x 3
+	std::vector<int64_t> h_count;
+	int list_cap = 0;
+	unsigned short* nbr = nullptr;
+	unsigned short* nbr_count = nullptr;
+	double* r_ref = nullptr;
+	int* box_flag = nullptr;
+	int* valid = nullptr;
+	unsigned char* kind = nullptr;
+	unsigned long long* builds = nullptr;
+	int32_t* d_bid = nullptr;     // box of each molecule slot
+	double* d_len = nullptr;      // nboxes x 3
 };
 
 namespace {
@@ -496,6 +637,8 @@ struct Launch {
 	int grid;
 	size_t smem;
 	brick::Const pc;
+	brick::Const lc;   // list evaluation (skin mode)
+	int build_cap;     // list build staging capacity (skin mode)
 };
 
 int plan(Batch* b, const Tiles& t, Launch& L) {
@@ -510,6 +653,14 @@ int plan(Batch* b, const Tiles& t, Launch& L) {
 	const int s_cap = brick::capacity_for(budget, fp64, t.cap);
 	L.pc = brick::make_const(b->sp.n, s_cap, b->rc, b->rc_lj);
 	L.smem = std::max(brick::layout(s_cap, fp64, t.cap).total, b->max_bin_bytes);
+	if (b->skin > 0.0) {
+		const int lcap = brick::capacity_for(budget, fp64, 0, false);
+		L.lc = brick::make_const(b->sp.n, lcap, b->rc, b->rc_lj);
+		int bcap = 256;
+		while (brick::build_bytes(bcap + 64) <= budget) bcap += 64;
+		L.build_cap = bcap;
+		L.smem = std::max({brick::layout(lcap, fp64, 0, false).total, brick::build_bytes(bcap), b->max_bin_bytes});
+	}
 	B_CUDA(cudaFuncSetAttribute(L.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) L.smem));
 	int per_sm = 0;
 	B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L.kern, kThreads, L.smem));
@@ -544,6 +695,24 @@ StepArgs args(Batch* b, const Launch& L, int src, int integrate, double dt, doub
 	a.timeout_ns = b->timeout_ns;
 	a.integrate = integrate;
 	a.dynamic = b->tiles.dynamic;
+	if (b->skin > 0.0) {
+		a.skin = 1;
+		a.half_skin2 = 0.25 * b->skin * b->skin;
+		a.lists.nbr = b->nbr;
+		a.lists.count = b->nbr_count;
+		a.lists.rx_ref = b->r_ref;
+		a.lists.ry_ref = b->r_ref + b->ntotal;
+		a.lists.rz_ref = b->r_ref + 2 * b->ntotal;
+		a.lists.n = b->ntotal;
+		a.lists.cap = b->list_cap;
+		a.lists.builds = b->builds;
+		a.lists.sentinel = L.lc.s_cap;
+		a.lists.kind = b->kind;
+		a.box_flag = b->box_flag;
+		a.valid = b->valid;
+		a.build_cap = L.build_cap;
+		a.lc = L.lc;
+	}
 	return a;
 }
 
@@ -592,7 +761,7 @@ int run_steps(Batch* b, int32_t nsteps, double dt) {
 		for (int k = 0; k < nsteps && e == cudaSuccess; k++) {
 			const StepArgs a = args(b, L, src, 1, dt, b->records + (int64_t) 4 * b->nboxes * k);
 			e = launch_step(b, L, a);
-			src = 1 - src;
+			if (b->skin == 0.0) src = 1 - src;   // the skin mode keeps the state in one buffer
 		}
 		cudaError_t e2 = cudaStreamEndCapture(b->stream, &graph);
 		if (e != cudaSuccess || e2 != cudaSuccess) {
@@ -613,7 +782,76 @@ int run_steps(Batch* b, int32_t nsteps, double dt) {
 	B_CUDA(cudaEventRecord(b->ev0, b->stream));
 	B_CUDA(cudaGraphLaunch(ge->exec, b->stream));
 	B_CUDA(cudaEventRecord(b->ev1, b->stream));
-	if (nsteps & 1) b->cur = 1 - b->cur;
+	if ((nsteps & 1) && b->skin == 0.0) b->cur = 1 - b->cur;
+	return MDGPU_OK;
+}
+
+// The per-box table (grids on cells of edge >= cutoff, or >= cutoff + skin in the skin mode) and the
+// offsets of every box's molecules, cells and bricks; host side only.
+int box_table(Batch* b) {
+	const int nboxes = b->nboxes;
+	const double grid_rc = b->rc + b->skin;
+	b->h_boxes.assign(nboxes, BatchBox{});
+	b->h_brick0.assign(nboxes + 1, 0);
+	b->max_bin_bytes = 0;
+	int64_t poff = 0, coff = 0, brick0 = 0;
+	for (int k = 0; k < nboxes; k++) {
+		if (b->h_count[k] < 1) return bfail(b, MDGPU_ERR_ARG, "every box needs at least one molecule");
+		Grid g{};
+		int st = setup_grid(b->h_len.data() + 3 * k, grid_rc, 1.0, g, b->err);
+		if (st) {
+			b->err = "box " + std::to_string(k) + ": " + b->err;
+			return st;
+		}
+		if (g.ncells > 65535) return bfail(b, MDGPU_ERR_CAPACITY, "box " + std::to_string(k) + " has more than 65535 cells");
+		if (b->h_count[k] > 65535)
+			return bfail(b, MDGPU_ERR_CAPACITY, "box " + std::to_string(k) + " has more than 65535 molecules");
+		BatchBox& B = b->h_boxes[k];
+		brick::init_box(B.bx, g, grid_rc, (int32_t) coff, 0.5 * b->skin);
+		B.poff = poff;
+		B.n = (int32_t) b->h_count[k];
+		B.brick0 = (int32_t) brick0;
+		b->h_brick0[k] = (int32_t) brick0;
+		b->max_bin_bytes = std::max(b->max_bin_bytes, bin_bytes(b->h_count[k], g.ncells));
+		poff += b->h_count[k];
+		coff += g.ncells;
+		brick0 += (int64_t) B.bx.nb[0] * B.bx.nb[1] * B.bx.nb[2];
+		if (poff >= (1LL << 28) || coff >= (1LL << 30) || brick0 >= (1LL << 30))
+			return bfail(b, MDGPU_ERR_CAPACITY, "the batch exceeds 2^28 molecules or 2^30 cells/bricks");
+	}
+	b->h_brick0[nboxes] = (int32_t) brick0;
+	b->ntotal = poff;
+	b->total_cells = (int) coff;
+	b->total_bricks = (int) brick0;
+	b->h_order.resize(nboxes);
+	for (int k = 0; k < nboxes; k++) b->h_order[k] = k;
+	std::stable_sort(b->h_order.begin(), b->h_order.end(),
+	                 [&](int x, int y) { return b->h_boxes[x].n > b->h_boxes[y].n; });
+	return MDGPU_OK;
+}
+
+// Device copies of the box table and the buffers sized by it (again after a change of the skin).
+int upload_table(Batch* b) {
+	void* old[] = {b->cstart, b->partials, b->d_boxes, b->d_brick0, b->d_order, b->kind};
+	for (void* x : old) cudaFree(x);
+	b->cstart = nullptr;
+	b->partials = nullptr;
+	b->d_boxes = nullptr;
+	b->d_brick0 = nullptr;
+	b->d_order = nullptr;
+	b->kind = nullptr;
+	for (auto& g : b->graphs) cudaGraphExecDestroy(g.exec);
+	b->graphs.clear();
+	const int nboxes = b->nboxes;
+	B_CUDA(cudaMalloc(&b->cstart, sizeof(int32_t) * (b->total_cells + 1)));
+	B_CUDA(cudaMalloc(&b->partials, sizeof(double) * 4 * b->total_bricks));
+	B_CUDA(cudaMalloc(&b->kind, b->total_bricks));
+	B_CUDA(cudaMalloc(&b->d_boxes, sizeof(BatchBox) * nboxes));
+	B_CUDA(cudaMemcpy(b->d_boxes, b->h_boxes.data(), sizeof(BatchBox) * nboxes, cudaMemcpyHostToDevice));
+	B_CUDA(cudaMalloc(&b->d_brick0, sizeof(int32_t) * (nboxes + 1)));
+	B_CUDA(cudaMemcpy(b->d_brick0, b->h_brick0.data(), sizeof(int32_t) * (nboxes + 1), cudaMemcpyHostToDevice));
+	B_CUDA(cudaMalloc(&b->d_order, sizeof(int32_t) * nboxes));
+	B_CUDA(cudaMemcpy(b->d_order, b->h_order.data(), sizeof(int32_t) * nboxes, cudaMemcpyHostToDevice));
 	return MDGPU_OK;
 }
 
@@ -653,40 +891,10 @@ int mdgpu_batch_create(mdgpu_batch** out, int32_t nboxes, const double* lengths,
 	b->nboxes = nboxes;
 	int st = setup_species(ncomp, comps, mix, b->rc_lj, b->sp, b->err);
 	if (st) return st;
-	b->h_boxes.resize(nboxes);
-	int64_t poff = 0, coff = 0, brick0 = 0;
-	std::vector<int32_t> h_brick0(nboxes + 1);
-	for (int k = 0; k < nboxes; k++) {
-		if (counts[k] < 1) return bfail(b, MDGPU_ERR_ARG, "every box needs at least one molecule");
-		Grid g{};
-		st = setup_grid(lengths + 3 * k, cutoff, cells_in_cutoff, g, b->err);
-		if (st) {
-			b->err = "box " + std::to_string(k) + ": " + b->err;
-			return st;
-		}
-		if (g.ncells > 65535) return bfail(b, MDGPU_ERR_CAPACITY, "box " + std::to_string(k) + " has more than 65535 cells");
-		if (counts[k] > 65535) return bfail(b, MDGPU_ERR_CAPACITY, "box " + std::to_string(k) + " has more than 65535 molecules");
-		BatchBox& B = b->h_boxes[k];
-		brick::init_box(B.bx, g, cutoff, (int32_t) coff);
-		B.poff = poff;
-		B.n = (int32_t) counts[k];
-		B.brick0 = (int32_t) brick0;
-		h_brick0[k] = (int32_t) brick0;
-		b->max_bin_bytes = std::max(b->max_bin_bytes, bin_bytes(counts[k], g.ncells));
-		poff += counts[k];
-		coff += g.ncells;
-		brick0 += (int64_t) B.bx.nb[0] * B.bx.nb[1] * B.bx.nb[2];
-		if (poff >= (1LL << 28) || coff >= (1LL << 30) || brick0 >= (1LL << 30))
-			return bfail(b, MDGPU_ERR_CAPACITY, "the batch exceeds 2^28 molecules or 2^30 cells/bricks");
-	}
-	h_brick0[nboxes] = (int32_t) brick0;
-	b->ntotal = poff;
-	b->total_cells = (int) coff;
-	b->total_bricks = (int) brick0;
-	b->h_order.resize(nboxes);
-	for (int k = 0; k < nboxes; k++) b->h_order[k] = k;
-	std::stable_sort(b->h_order.begin(), b->h_order.end(),
-	                 [&](int x, int y) { return b->h_boxes[x].n > b->h_boxes[y].n; });
+	b->h_len.assign(lengths, lengths + 3 * (size_t) nboxes);
+	b->h_count.assign(counts, counts + nboxes);
+	st = box_table(b);
+	if (st) return st;
 
 	B_CUDA(cudaSetDevice(device));
 	B_CUDA(cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device));
@@ -701,8 +909,8 @@ int mdgpu_batch_create(mdgpu_batch** out, int32_t nboxes, const double* lengths,
 	B_CUDA(cudaEventCreate(&b->ev0));
 	B_CUDA(cudaEventCreate(&b->ev1));
 	for (int k = 0; k < 2; k++) B_CUDA(alloc_particles(b->buf[k], b->ntotal));
-	B_CUDA(cudaMalloc(&b->cstart, sizeof(int32_t) * (b->total_cells + 1)));
-	B_CUDA(cudaMalloc(&b->partials, sizeof(double) * 4 * b->total_bricks));
+	st = upload_table(b);
+	if (st) return st;
 	B_CUDA(cudaMalloc(&b->prep, sizeof(double) * 4 * nboxes));
 	B_CUDA(cudaMalloc(&b->status, sizeof(int)));
 	B_CUDA(cudaMemset(b->status, 0, sizeof(int)));
@@ -712,12 +920,16 @@ int mdgpu_batch_create(mdgpu_batch** out, int32_t nboxes, const double* lengths,
 	PairParams hp = pair_params(b->sp, b->rc, b->rc_lj);
 	B_CUDA(cudaMalloc(&b->d_pp, sizeof(PairParams)));
 	B_CUDA(cudaMemcpy(b->d_pp, &hp, sizeof(PairParams), cudaMemcpyHostToDevice));
-	B_CUDA(cudaMalloc(&b->d_boxes, sizeof(BatchBox) * nboxes));
-	B_CUDA(cudaMemcpy(b->d_boxes, b->h_boxes.data(), sizeof(BatchBox) * nboxes, cudaMemcpyHostToDevice));
-	B_CUDA(cudaMalloc(&b->d_brick0, sizeof(int32_t) * (nboxes + 1)));
-	B_CUDA(cudaMemcpy(b->d_brick0, h_brick0.data(), sizeof(int32_t) * (nboxes + 1), cudaMemcpyHostToDevice));
-	B_CUDA(cudaMalloc(&b->d_order, sizeof(int32_t) * nboxes));
-	B_CUDA(cudaMemcpy(b->d_order, b->h_order.data(), sizeof(int32_t) * nboxes, cudaMemcpyHostToDevice));
+	// box of each molecule slot and the box lengths (positions are wrapped on output)
+	{
+		std::vector<int32_t> bid(b->ntotal);
+		for (int k = 0; k < nboxes; k++)
+			for (int64_t i = 0; i < b->h_count[k]; i++) bid[b->h_boxes[k].poff + i] = k;
+		B_CUDA(cudaMalloc(&b->d_bid, sizeof(int32_t) * b->ntotal));
+		B_CUDA(cudaMemcpy(b->d_bid, bid.data(), sizeof(int32_t) * b->ntotal, cudaMemcpyHostToDevice));
+		B_CUDA(cudaMalloc(&b->d_len, sizeof(double) * 3 * nboxes));
+		B_CUDA(cudaMemcpy(b->d_len, b->h_len.data(), sizeof(double) * 3 * nboxes, cudaMemcpyHostToDevice));
+	}
 	b->err.clear();
 	return MDGPU_OK;
 }
@@ -731,7 +943,8 @@ int mdgpu_batch_destroy(mdgpu_batch* h) {
 	for (int k = 0; k < 2; k++) free_particles(b->buf[k]);
 	if (b->backup_alloc) free_particles(b->backup);
 	void* bufs[] = {b->cstart, b->partials, b->records, b->prep, b->status, b->bar, b->d_pp, b->d_boxes,
-	                b->d_brick0, b->d_order, b->stage};
+	                b->d_brick0, b->d_order, b->stage, b->nbr, b->nbr_count, b->r_ref, b->box_flag,
+	                b->valid, b->kind, b->builds, b->d_bid, b->d_len};
 	for (void* x : bufs) cudaFree(x);
 	if (b->h_status) cudaFreeHost(b->h_status);
 	if (b->ev0) cudaEventDestroy(b->ev0);
@@ -772,6 +985,7 @@ int mdgpu_batch_set_particles(mdgpu_batch* h, int64_t ntotal, const uint64_t* id
 	B_CUDA(cudaMemcpyAsync(p.id, id, sizeof(uint64_t) * ntotal, cudaMemcpyHostToDevice, b->stream));
 	B_CUDA(cudaMemcpyAsync(p.cid, cid, sizeof(int32_t) * ntotal, cudaMemcpyHostToDevice, b->stream));
 	k_iota32<<<blocks(ntotal), kThreads, 0, b->stream>>>(ntotal, p.uidx);
+	if (b->valid) B_CUDA(cudaMemsetAsync(b->valid, 0, sizeof(int), b->stream));
 	B_CUDA(cudaGetLastError());
 	B_CUDA(cudaStreamSynchronize(b->stream));
 	b->loaded = true;
@@ -793,7 +1007,11 @@ int mdgpu_batch_get_particles(mdgpu_batch* h, int64_t ntotal, uint64_t* id, int3
 	} sets[3] = {{r, p.rx, p.ry, p.rz}, {v, p.vx, p.vy, p.vz}, {F, p.fx, p.fy, p.fz}};
 	for (auto& s : sets) {
 		if (!s.out) continue;
-		k_store3<<<blocks(ntotal), kThreads, 0, b->stream>>>(ntotal, s.x, s.y, s.z, p.uidx, b->stage);
+		if (s.out == r)
+			k_store3_wrap<<<blocks(ntotal), kThreads, 0, b->stream>>>(ntotal, s.x, s.y, s.z, p.uidx, b->d_bid, b->d_len,
+			                                                          b->stage);
+		else
+			k_store3<<<blocks(ntotal), kThreads, 0, b->stream>>>(ntotal, s.x, s.y, s.z, p.uidx, b->stage);
 		B_CUDA(cudaMemcpyAsync(s.out, b->stage, sizeof(double) * 3 * ntotal, cudaMemcpyDeviceToHost, b->stream));
 		B_CUDA(cudaStreamSynchronize(b->stream));
 	}
@@ -820,7 +1038,7 @@ int mdgpu_batch_prepare(mdgpu_batch* h, double* out) {
 	int st = plan(b, b->tiles, L);
 	if (st) return st;
 	B_CUDA(launch_step(b, L, args(b, L, b->cur, 0, 0.0, b->prep)));
-	b->cur = 1 - b->cur;
+	if (b->skin == 0.0) b->cur = 1 - b->cur;
 	st = check_status(b);
 	if (st) return st;
 	if (out) {
@@ -897,6 +1115,7 @@ int mdgpu_batch_autotune(mdgpu_batch* h, double dt, int32_t trial_steps, int32_t
 					double best_rep = 1e300;
 					for (int rep = 0; rep < 2 && st == MDGPU_OK; rep++) {
 						b->cur = cur0;
+						if (b->valid) B_CUDA(cudaMemsetAsync(b->valid, 0, sizeof(int), b->stream));
 						st = run_steps(b, trial_steps, dt);
 						if (st == MDGPU_OK) st = check_status(b);
 						if (st == MDGPU_OK) {
@@ -920,6 +1139,7 @@ int mdgpu_batch_autotune(mdgpu_batch* h, double dt, int32_t trial_steps, int32_t
 				if (ms) ms[k] = t;
 				k++;
 			}
+	if (b->valid) B_CUDA(cudaMemsetAsync(b->valid, 0, sizeof(int), b->stream));
 	B_CUDA(cudaStreamSynchronize(b->stream));
 	b->cur = cur0;
 	b->tiles = bestt;
@@ -934,6 +1154,62 @@ int mdgpu_batch_autotune(mdgpu_batch* h, double dt, int32_t trial_steps, int32_t
 int mdgpu_batch_last_run_ms(const mdgpu_batch* h, double* ms) {
 	if (!h || !ms) return MDGPU_ERR_ARG;
 	*ms = h->b.last_ms;
+	return MDGPU_OK;
+}
+
+int mdgpu_batch_set_skin(mdgpu_batch* h, double skin) {
+	if (!h) return MDGPU_ERR_ARG;
+	Batch* b = &h->b;
+	if (!(skin >= 0.0) || !(skin < b->rc)) return bfail(b, MDGPU_ERR_ARG, "skin must be in [0, cutoff)");
+	B_CUDA(cudaSetDevice(b->device));
+	B_CUDA(cudaStreamSynchronize(b->stream));
+	const double old = b->skin;
+	b->skin = skin;
+	int st = box_table(b);
+	if (!st) st = upload_table(b);
+	if (st) {
+		b->skin = old;
+		box_table(b);
+		upload_table(b);
+		return st;
+	}
+	if (b->max_bin_bytes > 110 * 1024) b->tiles.ctas = 1;
+	void* lists[] = {b->nbr, b->nbr_count, b->r_ref, b->box_flag, b->valid, b->builds};
+	for (void* x : lists) cudaFree(x);
+	b->nbr = b->nbr_count = nullptr;
+	b->r_ref = nullptr;
+	b->box_flag = b->valid = nullptr;
+	b->builds = nullptr;
+	if (skin > 0.0) {
+		// list capacity from the densest box (x 1.5 for local fluctuations)
+		double rho = 0.0;
+		for (int k = 0; k < b->nboxes; k++)
+			rho = std::max(rho, b->h_count[k] / (b->h_len[3 * k] * b->h_len[3 * k + 1] * b->h_len[3 * k + 2]));
+		const double rl = b->rc + skin;
+		int cap = (int) std::ceil(1.25 * 4.18879020478639 * rl * rl * rl * rho * 1.5) + 32;
+		cap = std::min((cap + 31) & ~31, 65504);
+		b->list_cap = cap;
+		B_CUDA(cudaMalloc(&b->nbr, sizeof(unsigned short) * (size_t) cap * b->ntotal));
+		B_CUDA(cudaMalloc(&b->nbr_count, sizeof(unsigned short) * b->ntotal));
+		B_CUDA(cudaMalloc(&b->r_ref, sizeof(double) * 3 * b->ntotal));
+		B_CUDA(cudaMalloc(&b->box_flag, sizeof(int) * b->nboxes));
+		B_CUDA(cudaMalloc(&b->valid, sizeof(int)));
+		B_CUDA(cudaMemset(b->valid, 0, sizeof(int)));
+		B_CUDA(cudaMalloc(&b->builds, sizeof(unsigned long long)));
+		B_CUDA(cudaMemset(b->builds, 0, sizeof(unsigned long long)));
+	}
+	b->prepared = false;
+	return MDGPU_OK;
+}
+
+int mdgpu_batch_skin_builds(const mdgpu_batch* h, int64_t* builds) {
+	if (!h || !builds) return MDGPU_ERR_ARG;
+	const Batch* b = &h->b;
+	*builds = 0;
+	if (!b->builds) return MDGPU_OK;
+	unsigned long long v = 0;
+	if (cudaMemcpy(&v, b->builds, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return MDGPU_ERR_CUDA;
+	*builds = (int64_t) v;
 	return MDGPU_OK;
 }
 

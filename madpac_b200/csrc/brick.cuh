@@ -613,7 +613,7 @@ __host__ __device__ inline size_t build_bytes(int s_cap) {
 // margin), with the positions of the build. No forces: list_pairs evaluates the lists.
 __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap, unsigned char* smem,
                                             const double* rx, const double* ry, const double* rz,
-                                            const int32_t* cstart, Lists lists) {
+                                            const int32_t* cstart, Lists lists, int64_t kind_slot) {
 	HalfPair* s_h16 = reinterpret_cast<HalfPair*>(smem);
 	__half* s_h = reinterpret_cast<__half*>(smem);
 	size_t o = align16(sizeof(HalfPair) * (s_cap / 2 + 20));
@@ -753,7 +753,7 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 			int ic;
 			if (own_cell(bx, brick, w, ic)) n_own += s_cnt[ic];
 		}
-		lists.kind[brick] = (s_cs[64] <= kSparseCap && n_own <= 32) ? 1 : 0;
+		lists.kind[kind_slot] = (s_cs[64] <= kSparseCap && n_own <= 32) ? 1 : 0;
 		if (brick == 0) atomicAdd(lists.builds, 1ull);
 	}
 }

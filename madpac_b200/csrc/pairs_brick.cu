@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(brick::kThreads, 3)
                   int step, brick::Lists lists) {
 	if (*gate != step) return;
 	extern __shared__ __align__(16) unsigned char smem[];
-	brick::build_lists(bx, blockIdx.x, s_cap, smem, rx, ry, rz, cstart, lists);
+	brick::build_lists(bx, blockIdx.x, s_cap, smem, rx, ry, rz, cstart, lists, blockIdx.x);
 }
 
 template <bool kFP64, bool kSingle, bool kLjIsRc>

@@ -84,6 +84,8 @@ SIGNATURES = {
     "mdgpu_batch_autotune": (_I, [_VP, _D, _I32, _VP, _VP]),
     "mdgpu_batch_last_run_ms": (_I, [_VP, _VP]),
     "mdgpu_batch_set_barrier_timeout": (_I, [_VP, _I64]),
+    "mdgpu_batch_set_skin": (_I, [_VP, _D]),
+    "mdgpu_batch_skin_builds": (_I, [_VP, _VP]),
 }
 
 _lib = None
@@ -284,6 +286,15 @@ class Batch:
 
     def setBarrierTimeout(self, ns: int) -> None:
         self._check(self.lib.mdgpu_batch_set_barrier_timeout(self.h, int(ns)))
+
+    def setSkin(self, skin: float) -> None:
+        """Verlet-skin mode per box (0 = off); takes effect at the next prepare()."""
+        self._check(self.lib.mdgpu_batch_set_skin(self.h, float(skin)))
+
+    def skinBuilds(self) -> int:
+        b = ctypes.c_int64()
+        self._check(self.lib.mdgpu_batch_skin_builds(self.h, ctypes.byref(b)))
+        return b.value
 
 
 class LinkedCells:

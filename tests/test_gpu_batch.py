@@ -4,7 +4,8 @@ step from a captured CUDA graph.
 * Against single-box contexts running the same steps: with the same tile shape (list depth 64) the
   per-brick arithmetic and the (cell, id) order are the same, so positions, velocities and forces are
   bit-identical; per-box Upot, virial and sum m v^2 agree to 1e-12 (the box sums run in another
-  order); pair counts are exact.
+  order); pair counts are exact. With a Verlet skin the two build their lists at different steps
+  (same pairs within rc, different entries near rc + skin), so the comparison is to rounding level.
 * Against the oracle (the reference's algorithm on the CPU): FP64 step records within 1e-9 along a
   short trajectory and forces within 1e-8, as for the single-box trajectory parity.
 * Every tile shape gives the same trajectory (FP64, 1e-12); the autotuner leaves the state as it
@@ -55,45 +56,65 @@ def rel(a, b):
     return np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
 
 
-def single_box_run(system, precision, nsteps):
+def single_box_run(system, precision, nsteps, skin=0.0):
     lc = M.LinkedCells.from_system(system, precision)
     lc.update()
     u, w, p = lc.traversePairs()
+    lc.setSkin(skin)
     recs = lc.run(nsteps, DT)
     st = lc.getParticles()
     lc.close()
     return np.array([u, w, p]), recs, st
 
 
+@pytest.mark.parametrize("skin", [0.0, 0.3])
 @pytest.mark.parametrize("precision", [M.FP64, M.MIXED])
 @pytest.mark.parametrize("make", [ensemble, two_species_ensemble])
-def test_batch_matches_single_box_bitwise(precision, make):
+def test_batch_matches_single_box_bitwise(precision, make, skin):
     systems = make()
-    nsteps = 12
+    nsteps = 12 if skin == 0.0 else 40
     b = M.Batch.from_systems(systems, precision)
     b.setTiles(64, 2, 1)
+    b.setSkin(skin)
     prep = b.prepare()
     recs = b.run(nsteps, DT)
     st = b.getParticles()
+    if skin > 0.0:
+        assert len(systems) <= b.skinBuilds() < len(systems) * (nsteps + 1)
     for k, s in enumerate(systems):
-        p0, r1, s1 = single_box_run(s, precision, nsteps)
+        p0, r1, s1 = single_box_run(s, precision, nsteps, skin)
         bk = b.box(st, k)
         np.testing.assert_array_equal(bk["id"], s1["id"])
-        np.testing.assert_array_equal(bk["r"], s1["r"])
-        np.testing.assert_array_equal(bk["v"], s1["v"])
-        np.testing.assert_array_equal(bk["F"], s1["F"])
-        assert np.all(rel(prep[k, :2], p0[:2]) <= 1e-12)
+        fp64 = precision == M.FP64
+        assert np.all(rel(prep[k, :2], p0[:2]) <= (1e-12 if skin == 0.0 or fp64 else 1e-6))
         assert prep[k, 3] == p0[2]
+        if skin == 0.0:
+            np.testing.assert_array_equal(bk["r"], s1["r"])
+            np.testing.assert_array_equal(bk["v"], s1["v"])
+            np.testing.assert_array_equal(bk["F"], s1["F"])
+            for step in range(nsteps):
+                assert np.all(rel(recs[step, k, :3], r1[step, :3]) <= 1e-12), (k, step, recs[step, k], r1[step])
+                assert recs[step, k, 3] == r1[step, 3]
+            continue
+        # Verlet skin: the batch builds its lists in prepare(), a single-box context at the first
+        # step of run(); the lists hold the same pairs within rc but differ near rc + skin, which
+        # moves entries between the partial accumulators (rounding-level differences only)
+        np.testing.assert_allclose(bk["r"], s1["r"], rtol=0, atol=1e-12 if fp64 else 1e-7)
+        np.testing.assert_allclose(bk["v"], s1["v"], rtol=0, atol=1e-12 if fp64 else 1e-6)
+        frms = np.sqrt(np.mean(np.sum(s1["F"] ** 2, axis=1)))
+        assert np.max(np.abs(bk["F"] - s1["F"])) / frms <= (1e-12 if fp64 else 1e-5)
         for step in range(nsteps):
-            assert np.all(rel(recs[step, k, :3], r1[step, :3]) <= 1e-12), (k, step, recs[step, k], r1[step])
-            assert recs[step, k, 3] == r1[step, 3]
+            assert np.all(rel(recs[step, k, :3], r1[step, :3]) <= (1e-12 if fp64 else 1e-6)), (k, step)
+            assert abs(recs[step, k, 3] - r1[step, 3]) <= (0 if fp64 else 2)
     b.close()
 
 
-def test_batch_fp64_matches_oracle():
+@pytest.mark.parametrize("skin", [0.0, 0.3])
+def test_batch_fp64_matches_oracle(skin):
     systems = ensemble(seed=21, sizes=(256, 900, 1700))
     nsteps = 8
     b = M.Batch.from_systems(systems, M.FP64)
+    b.setSkin(skin)
     prep = b.prepare()
     recs = b.run(nsteps, DT)
     st = b.getParticles()
