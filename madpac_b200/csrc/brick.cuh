@@ -758,6 +758,25 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 	}
 }
 
+#ifndef MDGPU_LIST_ACC
+#define MDGPU_LIST_ACC 1
+#endif
+// Independent FP32 partial sums per lane in list_chunk (entry u of a block of 8 goes to u % kListAcc).
+constexpr int kListAcc = MDGPU_LIST_ACC;
+static_assert(kListAcc == 1 || kListAcc == 2 || kListAcc == 4, "1, 2 or 4 partial sums");
+
+// Word k of a block of 8 list entries (register selection; k need not be a constant).
+__device__ __forceinline__ unsigned list_word(const uint4& v, int k) {
+	return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
+}
+
+// The partial sums in a fixed order, in FP64.
+__device__ __forceinline__ double acc_sum(const float* a) {
+	if (kListAcc == 4) return ((double) a[0] + (double) a[1]) + ((double) a[2] + (double) a[3]);
+	if (kListAcc == 2) return (double) a[0] + (double) a[1 % kListAcc];
+	return (double) a[0];
+}
+
 // One chunk of 32 of the brick's own molecules (t0 .. t0 + 31 in the order of the own cells
 // own[0..8] / ocell[0..7]) evaluating their lists, one molecule per lane: forces written, U, W,
 // pair count and the same-position flag accumulated into the caller's sums.
@@ -836,8 +855,9 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 		const float miz = __uint_as_float(0x4B000000u | ((wi >> 18) & 511u));
 		const int nblk = (cnt + 7) >> 3;
 		const unsigned sent2 = (unsigned) p.s_cap | ((unsigned) p.s_cap << 16);
-		float ax[4] = {0.f, 0.f, 0.f, 0.f}, ay[4] = {0.f, 0.f, 0.f, 0.f}, az[4] = {0.f, 0.f, 0.f, 0.f};
-		float au[4] = {0.f, 0.f, 0.f, 0.f}, aw[4] = {0.f, 0.f, 0.f, 0.f};
+		float ax[kListAcc], ay[kListAcc], az[kListAcc], au[kListAcc], aw[kListAcc];
+#pragma unroll
+		for (int a = 0; a < kListAcc; a++) ax[a] = ay[a] = az[a] = au[a] = aw[a] = 0.f;
 		int nlj = 0;   // pairs inside the LJ cutoff (shift6 terms)
 		// one pair in FP32 with the given cutoff decision; sign +1 adds it, -1 removes it
 		auto pair32 = [&](int j, bool in, float sign) {
@@ -872,11 +892,10 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 			uint4 cur = nxt;
 			if (b + 1 < nb8) nxt = my8[(int64_t) (b + 1) * lists.n];
 			if (b >= nblk) cur = make_uint4(sent2, sent2, sent2, sent2);
-			const unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
-			unsigned ambm = 0u;
+			bool amb = false;
 #pragma unroll
 			for (int u = 0; u < 8; u++) {
-				int j = (int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu);
+				int j = (int) ((list_word(cur, u >> 1) >> (16 * (u & 1))) & 0xffffu);
 				if (kClampJ) j = min(j, p.s_cap);   // a padding entry is the caller's sentinel slot
 				const float4 hj = S.hi[j];
 				const unsigned wj = __float_as_uint(hj.w);
@@ -890,21 +909,22 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 				const float d2f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2));
 				const bool in = d2f < p.rc2f;
 				// within a few ulp of rc: decided after the block as the FP64 computation does
-				ambm |= fabsf(d2f - p.rc2f) <= p.band ? (1u << u) : 0u;
+				amb |= fabsf(d2f - p.rc2f) <= p.band;
 				anp += in ? 1 : 0;
 				const bool lj_in = kLjIsRc ? in : (in && d2f < p.rclj2f);
 				if (!kLjIsRc) nlj += lj_in ? 1 : 0;
 				const float inv = lj_in ? rcp_approx(d2f) : 0.f;
+				const int a = u % kListAcc;
 				if (kSingle) {
 					const float s2 = sig2_1 * inv;
 					const float s6 = s2 * s2 * s2;
 					const float r = s6 * fmaf(2.f, s6, -1.f);
 					const float facp = r * inv;
-					ax[u & 3] = fmaf(facp, e0, ax[u & 3]);
-					ay[u & 3] = fmaf(facp, e1, ay[u & 3]);
-					az[u & 3] = fmaf(facp, e2, az[u & 3]);
-					au[u & 3] = fmaf(s6, s6 - 1.f, au[u & 3]);
-					aw[u & 3] += r;
+					ax[a] = fmaf(facp, e0, ax[a]);
+					ay[a] = fmaf(facp, e1, ay[a]);
+					az[a] = fmaf(facp, e2, az[a]);
+					au[a] = fmaf(s6, s6 - 1.f, au[a]);
+					aw[a] += r;
 				} else {
 					const int pk = ti * ns + unpack_cid(wj);
 					const float eps24 = S.pf[pk], sig2 = S.pf[KK + pk], shift6 = S.pf[2 * KK + pk];
@@ -912,40 +932,42 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 					const float s6 = s2 * s2 * s2;
 					const float r = eps24 * (s6 * fmaf(2.f, s6, -1.f));
 					const float fac = r * inv;
-					ax[u & 3] = fmaf(fac, e0, ax[u & 3]);
-					ay[u & 3] = fmaf(fac, e1, ay[u & 3]);
-					az[u & 3] = fmaf(fac, e2, az[u & 3]);
-					au[u & 3] = fmaf(eps24 * s6, s6 - 1.f, au[u & 3]) + (lj_in ? shift6 : 0.f);
-					aw[u & 3] += r;
+					ax[a] = fmaf(fac, e0, ax[a]);
+					ay[a] = fmaf(fac, e1, ay[a]);
+					az[a] = fmaf(fac, e2, az[a]);
+					au[a] = fmaf(eps24 * s6, s6 - 1.f, au[a]) + (lj_in ? shift6 : 0.f);
+					aw[a] += r;
 				}
 			}
-			if (__any_sync(kFull, ambm != 0u)) {
+			if (__any_sync(kFull, amb)) {
 				// rare: pairs within a few ulp of rc whose FP64 decision differs from the FP32 one
-				while (ambm) {
-					const int u = __ffs(ambm) - 1;
-					ambm &= ambm - 1u;
-					int j = (int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu);
+#pragma unroll 1
+				for (int u = 0; u < 8; u++) {
+					int j = (int) ((list_word(cur, u >> 1) >> (16 * (u & 1))) & 0xffffu);
 					if (kClampJ) j = min(j, p.s_cap);
 					const float4 hj = S.hi[j];
 					const unsigned wj = __float_as_uint(hj.w);
 					const float e0 = fmaf(mix - __uint_as_float(0x4B000000u | (wj & 511u)), bx.lo_step[0], hi_i.x - hj.x);
 					const float e1 = fmaf(miy - __uint_as_float(0x4B000000u | ((wj >> 9) & 511u)), bx.lo_step[1], hi_i.y - hj.y);
 					const float e2 = fmaf(miz - __uint_as_float(0x4B000000u | ((wj >> 18) & 511u)), bx.lo_step[2], hi_i.z - hj.z);
-					const bool in_f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2)) < p.rc2f;
-					const bool in_d = exact_cut(S, p.rc2, j, gi, rx, ry, rz);
-					if (in_f != in_d) pair32(j, true, in_d ? 1.f : -1.f);
+					const float d2f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2));
+					if (fabsf(d2f - p.rc2f) <= p.band) {
+						const bool in_f = d2f < p.rc2f;
+						const bool in_d = exact_cut(S, p.rc2, j, gi, rx, ry, rz);
+						if (in_f != in_d) pair32(j, true, in_d ? 1.f : -1.f);
+					}
 				}
 			}
 			if ((b & 7) == 7 || b + 1 == nb8) {
 				// fold the FP32 partial sums of up to 64 entries into the FP64 accumulators
 				const double sc = kSingle ? (double) eps24_1 : 1.0;
-				Fx += sc * (((double) ax[0] + (double) ax[1]) + ((double) ax[2] + (double) ax[3]));
-				Fy += sc * (((double) ay[0] + (double) ay[1]) + ((double) ay[2] + (double) ay[3]));
-				Fz += sc * (((double) az[0] + (double) az[1]) + ((double) az[2] + (double) az[3]));
-				U += sc * (((double) au[0] + (double) au[1]) + ((double) au[2] + (double) au[3]));
-				W += sc * (((double) aw[0] + (double) aw[1]) + ((double) aw[2] + (double) aw[3]));
+				Fx += sc * acc_sum(ax);
+				Fy += sc * acc_sum(ay);
+				Fz += sc * acc_sum(az);
+				U += sc * acc_sum(au);
+				W += sc * acc_sum(aw);
 #pragma unroll
-				for (int u = 0; u < 4; u++) ax[u] = ay[u] = az[u] = au[u] = aw[u] = 0.f;
+				for (int a = 0; a < kListAcc; a++) ax[a] = ay[a] = az[a] = au[a] = aw[a] = 0.f;
 			}
 		}
 		if (kSingle) U += (double) shift6_1 * (double) (kLjIsRc ? anp : nlj);

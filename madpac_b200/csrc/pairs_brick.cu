@@ -44,8 +44,14 @@ __global__ void __launch_bounds__(brick::kThreads, 3)
 	brick::build_lists(bx, blockIdx.x, s_cap, smem, rx, ry, rz, cstart, lists, blockIdx.x);
 }
 
+#ifndef MDGPU_LIST_MINB
+#define MDGPU_LIST_MINB 3
+#endif
+// Resident CTAs per SM of the FP32 list kernel (registers and shared memory are sized for it).
+constexpr int kListMinBlocks = MDGPU_LIST_MINB;
+
 template <bool kFP64, bool kSingle, bool kLjIsRc>
-__global__ void __launch_bounds__(brick::kThreads, 2)
+__global__ void __launch_bounds__(brick::kThreads, kFP64 ? 2 : kListMinBlocks)
     k_pairs_list(brick::Const p, brick::Box bx, const double* __restrict__ rx, const double* __restrict__ ry,
                  const double* __restrict__ rz, const int32_t* __restrict__ cid,
                  const int32_t* __restrict__ cstart, const PairParams* __restrict__ pp,
@@ -112,6 +118,7 @@ Plan plan(Context* c, const Grid& g, double filter_radius, int kind) {
 	static int max_optin = -1;
 	if (max_optin < 0) cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
 	size_t budget = 110 * 1024;
+	if (kind == 2 && !fp64) budget = std::min(budget, (size_t) (224 / kListMinBlocks - 2) * 1024);
 	if (budget > (size_t) max_optin) budget = (size_t) max_optin;
 	const int lcap = kind == 2 ? 0 : kListCap;
 	const bool half = kind != 2;
