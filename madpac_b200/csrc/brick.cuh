@@ -601,10 +601,20 @@ __device__ __forceinline__ void pairs(const Const& p, const Box& bx, int brick, 
 	block_sum3_at(U, W, NP, partials, slot);
 }
 
+// Entries of each lane's write-combining ring in build_lists: up to 7 unwritten entries plus the
+// 32 that one block of candidates can add; a power of two for the index wrap.
+constexpr int kBuildRing = 64;
+
 // Shared-memory bytes of build_lists for a staged capacity s_cap.
 __host__ __device__ inline size_t build_bytes(int s_cap) {
 	return align16(sizeof(HalfPair) * (s_cap / 2 + 20)) + align16(sizeof(int) * 65) + 2 * align16(sizeof(int) * 64) +
-	       sizeof(double) * 3 * 64;
+	       align16(sizeof(double) * 3 * 64) + sizeof(unsigned short) * kBuildRing * kThreads;
+}
+
+// Bits [lo, hi) of a 16-bit field (0 <= lo, hi <= 16).
+__device__ __forceinline__ unsigned range16(int lo, int hi) {
+	const unsigned up = hi >= 16 ? 0xffffu : ((1u << hi) - 1u);
+	return lo >= 16 ? 0u : up & ~((1u << lo) - 1u);
 }
 
 // Verlet-skin build for brick `brick`: stages the half-precision copy of the 4x4x4 cells around it
@@ -624,8 +634,10 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 	int* s_gst = reinterpret_cast<int*>(smem + o);
 	o += align16(sizeof(int) * 64);
 	double* s_ck = reinterpret_cast<double*>(smem + o);
+	o += align16(sizeof(double) * 3 * 64);
 	const Grid& g = bx.g;
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	unsigned short* ring = reinterpret_cast<unsigned short*>(smem + o) + kBuildRing * tid;
 	const int bc[3] = {brick % bx.nb[0], (brick / bx.nb[0]) % bx.nb[1], brick / (bx.nb[0] * bx.nb[1])};
 	if (tid < 64) {
 		const int l[3] = {tid & 3, (tid >> 2) & 3, tid >> 4};
@@ -695,6 +707,9 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 			}
 		} else {
 			const __half2 rc2h = __float2half2_rn(bx.rc2_h);
+			// each lane's entries go through its ring in shared memory and leave it in blocks of
+			// 8 (one 16-byte store each); the rotation by lane spreads the ring writes over banks
+			const int rot = 8 * (lane & 7);
 			for (int b0 = 0; b0 < ncell; b0 += 32) {
 				const bool act = b0 + lane < ncell;
 				const int slot_i = i0 + (act ? b0 + lane : 0);
@@ -703,43 +718,51 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 				const __half2 xi2 = act ? __half2half2(hi[0]) : __float2half2_rn(60000.f);
 				const __half2 yi2 = __half2half2(hi[2]);
 				const __half2 zi2 = __half2half2(hi[4]);
-				int cntg = 0;
+				uint4* dst = reinterpret_cast<uint4*>(lists.nbr) + gi;
+				int cnt = 0, done = 0;   // entries found; entries written (a multiple of 8)
 				for (int r = 0; r < 9; r++) {
 					const int ky = il[1] + (r % 3) - 1, kz = il[2] + (r / 3) - 1;
 					const int k0 = (il[0] - 1) + 4 * ky + 16 * kz;
 					const int a = s_cs[k0], b = s_cs[k0 + 3];
 					for (int base = a & ~1; base < b; base += 32) {
+						// bit k: slot base + 2k, bit 16 + k: slot base + 2k + 1
 						unsigned mask = 0u;
 #pragma unroll
 						for (int k = 0; k < 16; k++) {
 							const HalfPair H = s_h16[(base >> 1) + k];
 							const __half2 dx = __hsub2(xi2, H.x), dy = __hsub2(yi2, H.y), dz = __hsub2(zi2, H.z);
 							const __half2 d2 = __hfma2(dx, dx, __hfma2(dy, dy, __hmul2(dz, dz)));
-							const unsigned hm = __hlt2_mask(d2, rc2h);
-							mask |= ((hm & 1u) | ((hm >> 15) & 2u)) << (2 * k);
+							mask |= __hlt2_mask(d2, rc2h) & ((1u << k) | (1u << (16 + k)));
 						}
+						// keep slots in [a, b) and drop i itself
 						const int lo = a - base, hi_b = b - base;
-						unsigned valid = hi_b >= 32 ? 0xffffffffu : ((1u << hi_b) - 1u);
-						if (lo > 0) valid &= ~((1u << lo) - 1u);
+						mask &= range16(max(0, (lo + 1) >> 1), min(16, (hi_b + 1) >> 1)) |
+						        (range16(max(0, lo >> 1), min(16, hi_b >> 1)) << 16);
 						const int self = slot_i - base;
-						if (self >= 0 && self < 32) valid &= ~(1u << self);
-						mask &= valid;
+						if (self >= 0 && self < 32) mask &= ~(1u << ((self & 1) * 16 + (self >> 1)));
 						if (!act) mask = 0u;
 						while (mask) {
 							const int bit = __ffs(mask) - 1;
 							mask &= mask - 1u;
-							if (cntg < lists.cap)
-								lists.nbr[(((int64_t) (cntg >> 3) * lists.n + gi) << 3) + (cntg & 7)] =
-								    (unsigned short) (base + bit);
-							cntg++;
+							ring[(cnt + rot) & (kBuildRing - 1)] = (unsigned short) (base + 2 * (bit & 15) + (bit >> 4));
+							cnt++;
 						}
+						for (; done + 8 <= cnt; done += 8)
+							if (done < lists.cap)
+								dst[(int64_t) (done >> 3) * lists.n] =
+								    *reinterpret_cast<const uint4*>(ring + ((done + rot) & (kBuildRing - 1)));
 					}
 				}
 				if (act) {
-					// pad the last block of 8 with the list kernel's sentinel slot
-					for (int k = cntg; k < ((cntg + 7) & ~7) && k < lists.cap; k++)
-						lists.nbr[(((int64_t) (k >> 3) * lists.n + gi) << 3) + (k & 7)] = (unsigned short) lists.sentinel;
-					lists.count[gi] = cntg <= lists.cap ? (unsigned short) cntg : kListOverflow;
+					// the last block of 8, padded with the list kernel's sentinel slot
+					if (cnt > done) {
+						for (int k = cnt; k < done + 8; k++)
+							ring[(k + rot) & (kBuildRing - 1)] = (unsigned short) lists.sentinel;
+						if (done < lists.cap)
+							dst[(int64_t) (done >> 3) * lists.n] =
+							    *reinterpret_cast<const uint4*>(ring + ((done + rot) & (kBuildRing - 1)));
+					}
+					lists.count[gi] = cnt <= lists.cap ? (unsigned short) cnt : kListOverflow;
 					lists.rx_ref[gi] = rx[gi];
 					lists.ry_ref[gi] = ry[gi];
 					lists.rz_ref[gi] = rz[gi];

@@ -197,7 +197,7 @@ cudaError_t launch_pairs_skin(Context* c) {
 	brick::Box bb{};
 	brick::init_box(bb, c->gs, c->rc + c->skin, 0, 0.5 * c->skin);
 	int s_cap = 256;
-	while (brick::build_bytes(s_cap + 64) <= 64 * 1024) s_cap += 64;
+	while (brick::build_bytes(s_cap + 64) <= 72 * 1024) s_cap += 64;
 	const size_t bbytes = brick::build_bytes(s_cap);
 	const int nbricks = bb.nb[0] * bb.nb[1] * bb.nb[2];
 	cudaError_t e = cudaFuncSetAttribute(k_build_lists, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bbytes);
