@@ -265,6 +265,23 @@ int setup_grid(const double length[3], double cutoff, double cells_in_cutoff, Gr
 	return MDGPU_OK;
 }
 
+void even_grid(Grid& g) {
+	// 2x2x2-cell bricks tile an even number of cells exactly; with an odd count the last brick of
+	// a row owns one cell and leaves most of its CTA idle. Larger cells keep every pair within
+	// the radius inside the 27 cells around a molecule. Three cells stay three (two would make
+	// one brick of the whole box, staged eight times over).
+	int64_t ncells = 1;
+	for (int d = 0; d < 3; d++) {
+		if (g.nc[d] >= 5 && (g.nc[d] & 1)) {
+			g.nc[d] -= 1;
+			g.cell_length[d] = g.L[d] / g.nc[d];
+			g.halo_min[d] = -g.cell_length[d];
+		}
+		ncells *= g.nc[d];
+	}
+	g.ncells = ncells;
+}
+
 int setup_species(int ncomp, const mdgpu_component* comps, const double* mix, double rcLJ, Species& sp,
                   std::string& err) {
 	// Comp2Param stream entries (Comp2Param.cpp:28-115; shift6 of Component::addLJcenter,
@@ -799,6 +816,7 @@ int mdgpu_set_skin(mdgpu_ctx* ctx, double skin) {
 		const double length[3] = {c->g.L[0], c->g.L[1], c->g.L[2]};
 		int st = setup_grid(length, c->rc + skin, 1.0, gs, err);
 		if (st) return fail(c, st, "cutoff + skin: " + err);
+		even_grid(gs);
 		c->gs = gs;
 	}
 	c->skin = skin;

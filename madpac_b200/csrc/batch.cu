@@ -803,6 +803,7 @@ int box_table(Batch* b) {
 			b->err = "box " + std::to_string(k) + ": " + b->err;
 			return st;
 		}
+		if (b->skin > 0.0) even_grid(g);
 		if (g.ncells > 65535) return bfail(b, MDGPU_ERR_CAPACITY, "box " + std::to_string(k) + " has more than 65535 cells");
 		if (b->h_count[k] > 65535)
 			return bfail(b, MDGPU_ERR_CAPACITY, "box " + std::to_string(k) + " has more than 65535 molecules");

@@ -152,6 +152,8 @@ cudaError_t launch_step_record(Context* c, double* dst);        // dst[0..3] <- 
 // Set-up shared by the single-box and the batched contexts (api.cu): LinkedCells geometry of the
 // box [0, L), the Comp2Param table, and its device form. Return an MDGPU_* code, message in err.
 int setup_grid(const double length[3], double cutoff, double cells_in_cutoff, Grid& g, std::string& err);
+// The Verlet-skin grid: an odd cell count of 5 or more in a dimension is lowered by one (cells grow).
+void even_grid(Grid& g);
 int setup_species(int ncomp, const mdgpu_component* comps, const double* mix, double rc_lj, Species& sp,
                   std::string& err);
 PairParams pair_params(const Species& sp, double rc, double rc_lj);
