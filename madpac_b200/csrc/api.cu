@@ -369,6 +369,7 @@ int mdgpu_create(mdgpu_ctx** out, const double length[3], double cutoff, double 
 	c->rc = cutoff;
 	c->rc_lj = lj_cutoff == 0.0 ? cutoff : lj_cutoff;
 	MD_CUDA(cudaSetDevice(device));
+	MD_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
 	{
 		int st = setup_grid(length, cutoff, cells_in_cutoff, c->g, c->err);
 		if (st) return st;

@@ -9,6 +9,8 @@
 // leave r and v untouched (no torque, zero inertia), so they are not evaluated.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "md_internal.h"
 #include "reduce.cuh"
 
@@ -78,9 +80,8 @@ __device__ __forceinline__ void fold(const Fold& f, const double* partials) {
 __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_post_pre(int64_t n, Particles p, SpeciesScale post,
                                                                    SpeciesScale pre, double dt, double* partials,
                                                                    int* status, SkinCheck sk, Fold f) {
-	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	double mv2 = 0.0;
-	if (i < n) {
+	for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
 		// every load first: the arrays may alias as far as the compiler knows
 		const int t = p.cid[i];
 		const double fx = p.fx[i], fy = p.fy[i], fz = p.fz[i];
@@ -97,7 +98,7 @@ __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_post_pre(int64_t n, P
 		const double vy = __dadd_rn(vy0, __dmul_rn(a, fy));
 		const double vz = __dadd_rn(vz0, __dmul_rn(a, fz));
 		const double v2 = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
-		mv2 = __dmul_rn(post.mass[t], v2);
+		mv2 += __dmul_rn(post.mass[t], v2);
 		if (!(v2 == v2) || isinf(v2)) atomicOr(status, kStatusNonFinite);
 		const double b = pre.dtInv2m[t];
 		const double wx = __dadd_rn(__dmul_rn(1.0, vx), __dmul_rn(b, fx));
@@ -123,9 +124,8 @@ __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_post_pre(int64_t n, P
 
 __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_post(int64_t n, Particles p, SpeciesScale s,
                                                                double* partials, int* status, Fold f) {
-	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	double mv2 = 0.0;
-	if (i < n) {
+	for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
 		const int t = p.cid[i];
 		const double a = s.dtInv2m[t];
 		const double vx0 = p.vx[i], vy0 = p.vy[i], vz0 = p.vz[i];
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_post(int64_t n, Parti
 		p.vy[i] = vy;
 		p.vz[i] = vz;
 		const double v2 = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
-		mv2 = __dmul_rn(s.mass[t], v2);
+		mv2 += __dmul_rn(s.mass[t], v2);
 		if (!(v2 == v2) || isinf(v2)) atomicOr(status, kStatusNonFinite);
 	}
 	block_sum3(mv2, 0.0, 0.0, partials);
@@ -173,6 +173,17 @@ SpeciesScale make_scale(const Context* c, double dt_half) {
 
 inline unsigned blocks_for(int64_t n) { return (unsigned) ((n + kReduceBlock - 1) / kReduceBlock); }
 
+// Grid of the reducing kernels: the blocks that fit on the device at once (grid-stride loops), so
+// that each block's reduction and ticket are paid once per resident block, not per 256 molecules.
+template <typename K>
+unsigned resident_blocks(const Context* c, K kern, int64_t n) {
+	static int per_sm = 0;
+	if (per_sm == 0 && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kReduceBlock, 0) != cudaSuccess)
+		per_sm = 4;
+	const int64_t cap = (int64_t) std::max(per_sm, 1) * c->num_sms;
+	return (unsigned) std::max<int64_t>(1, std::min<int64_t>(blocks_for(n), cap));
+}
+
 SkinCheck skin_check_of(const Context* c, bool on) {
 	SkinCheck sk{};
 	if (on) {
@@ -201,9 +212,9 @@ cudaError_t launch_leapfrog_pre(Context* c, double dt, double vcorr, bool skin_c
 
 cudaError_t launch_leapfrog_post_pre(Context* c, double dt, bool skin_check, double* record) {
 	prof_begin(c, 2);
-	int64_t nb = c->n > 0 ? blocks_for(c->n) : 1;
+	const unsigned nb = resident_blocks(c, k_leapfrog_post_pre, c->n);
 	const Fold f{c->tickets + 1, c->scalars + 3, c->scalars, record};
-	k_leapfrog_post_pre<<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(
+	k_leapfrog_post_pre<<<nb, kReduceBlock, 0, c->stream>>>(
 	    c->n, c->p, make_scale(c, 0.5 * dt), make_scale(c, .5 * dt), dt, c->partials, c->status,
 	    skin_check_of(c, skin_check), f);
 	cudaError_t e = cudaGetLastError();
@@ -213,9 +224,9 @@ cudaError_t launch_leapfrog_post_pre(Context* c, double dt, bool skin_check, dou
 
 cudaError_t launch_leapfrog_post(Context* c, double dt_half, double* record) {
 	prof_begin(c, 2);
-	int64_t nb = c->n > 0 ? blocks_for(c->n) : 1;
+	const unsigned nb = resident_blocks(c, k_leapfrog_post, c->n);
 	const Fold f{c->tickets + 1, c->scalars + 3, c->scalars, record};
-	k_leapfrog_post<<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(c->n, c->p, make_scale(c, dt_half), c->partials,
+	k_leapfrog_post<<<nb, kReduceBlock, 0, c->stream>>>(c->n, c->p, make_scale(c, dt_half), c->partials,
 	                                                               c->status, f);
 	cudaError_t e = cudaGetLastError();
 	prof_end(c, 2, 1);

@@ -62,6 +62,7 @@ struct Particles {
 
 struct Context {
 	int device = 0;
+	int num_sms = 148;   // streaming multiprocessors of the device (set at creation)
 	cudaStream_t stream = nullptr;
 	int precision = MDGPU_FP64;
 	int pair_kernel = 0;            // 0 = shared-memory brick kernel, 1 = simple gather kernel

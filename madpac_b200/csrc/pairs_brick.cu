@@ -36,12 +36,16 @@ __global__ void __launch_bounds__(brick::kThreads, 2)
 
 // Verlet-skin build step (runs only when *gate is this step's id): the lists, no forces.
 __global__ void __launch_bounds__(brick::kThreads, 3)
-    k_build_lists(brick::Box bx, int s_cap, const double* __restrict__ rx, const double* __restrict__ ry,
-                  const double* __restrict__ rz, const int32_t* __restrict__ cstart, const int* __restrict__ gate,
-                  int step, brick::Lists lists) {
+    k_build_lists(brick::Box bx, int nbricks, int s_cap, const double* __restrict__ rx,
+                  const double* __restrict__ ry, const double* __restrict__ rz, const int32_t* __restrict__ cstart,
+                  const int* __restrict__ gate, int step, brick::Lists lists) {
 	if (*gate != step) return;
 	extern __shared__ __align__(16) unsigned char smem[];
-	brick::build_lists(bx, blockIdx.x, s_cap, smem, rx, ry, rz, cstart, lists, blockIdx.x);
+	// a resident grid walks the bricks: a step without a build costs one launch of that grid only
+	for (int b = blockIdx.x; b < nbricks; b += gridDim.x) {
+		brick::build_lists(bx, b, s_cap, smem, rx, ry, rz, cstart, lists, b);
+		__syncthreads();
+	}
 }
 
 #ifndef MDGPU_LIST_MINB
@@ -201,9 +205,10 @@ cudaError_t launch_pairs_skin(Context* c) {
 	const size_t bbytes = brick::build_bytes(s_cap);
 	const int nbricks = bb.nb[0] * bb.nb[1] * bb.nb[2];
 	cudaError_t e = cudaFuncSetAttribute(k_build_lists, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bbytes);
+	const int grid = std::min(nbricks, 3 * c->num_sms);   // three CTAs per SM (launch bounds, 72 KB each)
 	if (e == cudaSuccess)
-		k_build_lists<<<nbricks, brick::kThreads, bbytes, c->stream>>>(bb, s_cap, c->p.rx, c->p.ry, c->p.rz,
-		                                                              c->cell_start, c->rebuild, c->step_id, l);
+		k_build_lists<<<grid, brick::kThreads, bbytes, c->stream>>>(bb, nbricks, s_cap, c->p.rx, c->p.ry, c->p.rz,
+		                                                           c->cell_start, c->rebuild, c->step_id, l);
 	// evaluation, every step: sparse bricks one warp each, then the others (whose last CTA sums the
 	// partials of all bricks)
 	if (e == cudaSuccess) {
