@@ -2,6 +2,8 @@
 // the step sequence and device-side timing.
 #include <cuda_runtime.h>
 
+#include <utility>
+
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -791,8 +793,9 @@ int enqueue_one(Context* c, double dt, double vcorr, double* dst) {
 		if (st) return st;
 		MD_CUDA(launch_leapfrog_pre(c, dt, vcorr, true));
 		MD_CUDA(launch_rebuild(c, c->gs));
-		MD_CUDA(launch_pairs_skin(c));
-		MD_CUDA(launch_leapfrog_post(c, 0.5 * dt));
+		// the closing kick and the record come from the pair kernels
+		MD_CUDA(launch_pairs_skin(c, 2, dt, dst));
+		return MDGPU_OK;
 	} else {
 		MD_CUDA(launch_leapfrog_pre(c, dt, vcorr));
 		MD_CUDA(launch_bin(c, false));
@@ -873,32 +876,41 @@ int enqueue_steps(Context* c, int32_t nsteps, double dt) {
 		c->steps_cap = cap;
 	}
 	if (nsteps == 0) return MDGPU_OK;
-	// the closing kick of step k and the opening kick of step k+1 run as one pass; the record of
-	// step k is written after it (its sum m v^2 comes from that pass)
 	const bool skin = c->skin > 0.0;
 	if (skin) {
+		// the pair kernels apply the closing kick of step k and the opening kick and drift of step
+		// k+1 to the molecules whose forces they sum (new positions into the other buffer, whose
+		// role then swaps), and write each step's record
 		int st = skin_prepare(c);
 		if (st) return st;
-	}
-	for (int k = 0; k < nsteps; k++) {
-		if (skin) {
-			int st = skin_open_step(c);
+		for (int k = 0; k < nsteps; k++) {
+			st = skin_open_step(c);
 			if (st) return st;
+			if (k == 0) MD_CUDA(launch_leapfrog_pre(c, dt, 1.0, true));
+			MD_CUDA(launch_rebuild(c, c->gs));
+			const bool last = k + 1 == nsteps;
+			MD_CUDA(launch_pairs_skin(c, last ? 2 : 1, dt, c->steps_out + 4 * c->steps_written));
+			c->steps_written++;
+			if (!last) {
+				std::swap(c->p.rx, c->q.rx);
+				std::swap(c->p.ry, c->q.ry);
+				std::swap(c->p.rz, c->q.rz);
+			}
 		}
+		return MDGPU_OK;
+	}
+	// the closing kick of step k and the opening kick of step k+1 run as one pass; the record of
+	// step k is written after it (its sum m v^2 comes from that pass)
+	for (int k = 0; k < nsteps; k++) {
 		if (k == 0) {
-			MD_CUDA(launch_leapfrog_pre(c, dt, 1.0, skin));
+			MD_CUDA(launch_leapfrog_pre(c, dt, 1.0, false));
 		} else {
-			MD_CUDA(launch_leapfrog_post_pre(c, dt, skin, c->steps_out + 4 * c->steps_written));
+			MD_CUDA(launch_leapfrog_post_pre(c, dt, false, c->steps_out + 4 * c->steps_written));
 			c->steps_written++;
 		}
-		if (skin) {
-			MD_CUDA(launch_rebuild(c, c->gs));
-			MD_CUDA(launch_pairs_skin(c));
-		} else {
-			MD_CUDA(launch_bin(c, false));
-			c->lists_valid = false;
-			MD_CUDA(launch_pairs(c));
-		}
+		MD_CUDA(launch_bin(c, false));
+		c->lists_valid = false;
+		MD_CUDA(launch_pairs(c));
 	}
 	MD_CUDA(launch_leapfrog_post(c, 0.5 * dt, c->steps_out + 4 * c->steps_written));
 	c->steps_written++;

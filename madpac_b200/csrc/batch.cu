@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_step(StepArgs a) {
 			const BatchBox& B = a.boxes[box_of(item)];
 			brick::list_pairs<kFP64, kSingle, kLjIsRc>(a.lc, B.bx, item - B.brick0, item, smem, a.src.rx, a.src.ry,
 			                                           a.src.rz, a.src.cid, a.cstart, a.src.fx, a.src.fy, a.src.fz,
-			                                           a.partials, a.status, a.lists);
+			                                           a.partials, a.status, a.lists, brick::Kick{});
 			__syncthreads();
 		});
 	}

@@ -781,6 +781,68 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 	}
 }
 
+// What the list kernels do with a molecule's force once it is summed. Mode 0 stores it. Modes 1
+// and 2 apply the closing kick of the step, v += (dt/2m) F, and add m v^2 to the step's sum
+// (Molecule::upd_postF, molecules/Molecule.cpp:193-205); mode 2 (the last step of a run) stores F
+// and v, mode 1 goes on with the opening kick and drift of the next step, v = 1*v + (dt/2m) F,
+// r' = r + dt v (Molecule::upd_preF with vcorr = 1, Molecule.cpp:128-135), writes r' to the other
+// position buffer (other bricks still stage r) and flags a rebuild with `id` when r' is farther than
+// skin/2 from the position of the last build. Same operations and roundings as the Leapfrog kernels.
+struct Kick {
+	int mode;
+	int id;
+	double dt;
+	double half2;                 // (skin/2)^2
+	double post[kMaxSpecies];     // (0.5 dt) / m of the closing kick
+	double pre[kMaxSpecies];      // (0.5 dt) / m of the opening kick
+	double mass[kMaxSpecies];
+	double *vx, *vy, *vz;
+	double *ox, *oy, *oz;         // positions after the drift (mode 1)
+	int* flag;
+};
+
+__device__ __forceinline__ double finish(const Kick& k, int64_t gi, double Fx, double Fy, double Fz, const double* rx,
+                                         const double* ry, const double* rz, const int32_t* cid, const Lists& lists,
+                                         double* fx, double* fy, double* fz, int* status) {
+	if (!(Fx == Fx && Fy == Fy && Fz == Fz) || isinf(Fx) || isinf(Fy) || isinf(Fz)) atomicOr(status, kStatusNonFinite);
+	if (k.mode != 1) {
+		fx[gi] = Fx;
+		fy[gi] = Fy;
+		fz[gi] = Fz;
+	}
+	if (k.mode == 0) return 0.0;
+	const int t = cid[gi];
+	const double a = k.post[t];
+	const double vx = __dadd_rn(k.vx[gi], __dmul_rn(a, Fx));
+	const double vy = __dadd_rn(k.vy[gi], __dmul_rn(a, Fy));
+	const double vz = __dadd_rn(k.vz[gi], __dmul_rn(a, Fz));
+	const double v2 = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
+	if (!(v2 == v2) || isinf(v2)) atomicOr(status, kStatusNonFinite);
+	const double mv2 = __dmul_rn(k.mass[t], v2);
+	if (k.mode == 2) {
+		k.vx[gi] = vx;
+		k.vy[gi] = vy;
+		k.vz[gi] = vz;
+		return mv2;
+	}
+	const double b = k.pre[t];
+	const double wx = __dadd_rn(__dmul_rn(1.0, vx), __dmul_rn(b, Fx));
+	const double wy = __dadd_rn(__dmul_rn(1.0, vy), __dmul_rn(b, Fy));
+	const double wz = __dadd_rn(__dmul_rn(1.0, vz), __dmul_rn(b, Fz));
+	const double x = __dadd_rn(rx[gi], __dmul_rn(k.dt, wx));
+	const double y = __dadd_rn(ry[gi], __dmul_rn(k.dt, wy));
+	const double z = __dadd_rn(rz[gi], __dmul_rn(k.dt, wz));
+	k.vx[gi] = wx;
+	k.vy[gi] = wy;
+	k.vz[gi] = wz;
+	k.ox[gi] = x;
+	k.oy[gi] = y;
+	k.oz[gi] = z;
+	const double dx = x - lists.rx_ref[gi], dy = y - lists.ry_ref[gi], dz = z - lists.rz_ref[gi];
+	if (!(dx * dx + dy * dy + dz * dz <= k.half2)) *k.flag = k.id;
+	return mv2;
+}
+
 #ifndef MDGPU_LIST_ACC
 #define MDGPU_LIST_ACC 1
 #endif
@@ -807,8 +869,8 @@ template <bool kFP64, bool kSingle, bool kLjIsRc, bool kClampJ = false>
 __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const Smem& S, const int* s_own,
                                            const int* s_ocell, int t0, int n_own, const double* rx, const double* ry,
                                            const double* rz, const int32_t* cid, const int32_t* cstart, double* fx,
-                                           double* fy, double* fz, int* status, const Lists& lists, double& U,
-                                           double& W, double& NP, bool& same) {
+                                           double* fy, double* fz, int* status, const Lists& lists, const Kick& kick,
+                                           double& U, double& W, double& NP, double& MV, bool& same) {
 	const int lane = threadIdx.x & 31;
 	const int ns = p.ns;
 	const float eps24_1 = S.pf[0], sig2_1 = S.pf[KK], shift6_1 = S.pf[2 * KK];
@@ -833,9 +895,7 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 	if (ovf) {
 		// the list overflowed at the build: gather this molecule from global memory
 		PairSums s = gather_pairs<!kFP64>(gi, rx, ry, rz, cid, cstart, bx.g, S.pd, ns, p.rc2, p.rclj2, bx.coff);
-		fx[gi] = s.F[0];
-		fy[gi] = s.F[1];
-		fz[gi] = s.F[2];
+		MV += finish(kick, gi, s.F[0], s.F[1], s.F[2], rx, ry, rz, cid, lists, fx, fy, fz, status);
 		U += s.U;
 		W += s.W;
 		NP += s.np;
@@ -1007,13 +1067,7 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 		}
 	}
 	NP += (double) anp;
-	if (act && !ovf) {
-		fx[gi] = Fx;
-		fy[gi] = Fy;
-		fz[gi] = Fz;
-		if (!(Fx == Fx && Fy == Fy && Fz == Fz) || isinf(Fx) || isinf(Fy) || isinf(Fz))
-			atomicOr(status, kStatusNonFinite);
-	}
+	if (act && !ovf) MV += finish(kick, gi, Fx, Fy, Fz, rx, ry, rz, cid, lists, fx, fy, fz, status);
 }
 
 // Forces of brick `brick` from the neighbour lists that build_lists made on the same cell
@@ -1025,7 +1079,8 @@ template <bool kFP64, bool kSingle, bool kLjIsRc>
 __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int brick, int64_t slot,
                                            unsigned char* smem, const double* rx, const double* ry, const double* rz,
                                            const int32_t* cid, const int32_t* cstart, double* fx, double* fy,
-                                           double* fz, double* partials, int* status, const Lists lists) {
+                                           double* fz, double* partials, int* status, const Lists lists,
+                                           const Kick& kick) {
 	const SmemLayout L = layout(p.s_cap, kFP64, 0, false);
 	const Smem S = views(smem, L);
 	const int tid = threadIdx.x, warp = tid >> 5;
@@ -1047,7 +1102,7 @@ __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int br
 	}
 	__syncthreads();
 	const int n_own = s_own[8];
-	double U = 0.0, W = 0.0, NP = 0.0;
+	double U = 0.0, W = 0.0, NP = 0.0, MV = 0.0;
 	bool same = false;
 	if (!staged) {
 		// over capacity: gather from global memory
@@ -1056,9 +1111,7 @@ __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int br
 			while (w < 7 && s_own[w + 1] <= t) w++;
 			const int gi = S.gst[s_ocell[w]] + (t - s_own[w]);
 			PairSums s = gather_pairs<!kFP64>(gi, rx, ry, rz, cid, cstart, bx.g, S.pd, ns, p.rc2, p.rclj2, bx.coff);
-			fx[gi] = s.F[0];
-			fy[gi] = s.F[1];
-			fz[gi] = s.F[2];
+			MV += finish(kick, gi, s.F[0], s.F[1], s.F[2], rx, ry, rz, cid, lists, fx, fy, fz, status);
 			U += s.U;
 			W += s.W;
 			NP += s.np;
@@ -1067,10 +1120,10 @@ __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int br
 	} else {
 		for (int t0 = warp * 32; t0 < n_own; t0 += kThreads)
 			list_chunk<kFP64, kSingle, kLjIsRc>(p, bx, S, s_own, s_ocell, t0, n_own, rx, ry, rz, cid, cstart, fx, fy, fz,
-			                                    status, lists, U, W, NP, same);
+			                                    status, lists, kick, U, W, NP, MV, same);
 	}
 	if (same) atomicOr(status, kStatusSamePosition);
-	block_sum3_at(U, W, NP, partials, slot);
+	block_sum3_at(U, W, NP, partials, slot, MV);
 }
 
 // A sparse brick (see kSparseCap) by one warp, in its own shared-memory area laid out as
@@ -1085,7 +1138,8 @@ template <bool kFP64, bool kSingle, bool kLjIsRc>
 __device__ __forceinline__ void list_pairs_warp(const Const& p, const Box& bx, int brick, unsigned char* ws,
                                                 const double* rx, const double* ry, const double* rz,
                                                 const int32_t* cid, const int32_t* cstart, double* fx, double* fy,
-                                                double* fz, double* partials, int* status, const Lists& lists) {
+                                                double* fz, double* partials, int* status, const Lists& lists,
+                                                const Kick& kick) {
 	const SmemLayout L = layout(kSparseCap, kFP64, 0, false);
 	const Smem S = views(ws, L);
 	int* own = reinterpret_cast<int*>(ws + L.total);
@@ -1169,21 +1223,19 @@ __device__ __forceinline__ void list_pairs_warp(const Const& p, const Box& bx, i
 	}
 	__syncwarp();
 	const int n_own = own[8];
-	double U = 0.0, W = 0.0, NP = 0.0;
+	double U = 0.0, W = 0.0, NP = 0.0, MV = 0.0;
 	bool same = false;
 	if (staged) {
 		for (int t0 = 0; t0 < n_own; t0 += 32)
 			list_chunk<kFP64, kSingle, kLjIsRc, true>(p, bx, S, own, own + 9, t0, n_own, rx, ry, rz, cid, cstart, fx,
-			                                          fy, fz, status, lists, U, W, NP, same);
+			                                          fy, fz, status, lists, kick, U, W, NP, MV, same);
 	} else {
 		for (int t = lane; t < n_own; t += 32) {
 			int w = 0;
 			while (w < 7 && own[w + 1] <= t) w++;
 			const int gi = S.gst[own[9 + w]] + (t - own[w]);
 			PairSums ps = gather_pairs<!kFP64>(gi, rx, ry, rz, cid, cstart, g, S.pd, p.ns, p.rc2, p.rclj2, bx.coff);
-			fx[gi] = ps.F[0];
-			fy[gi] = ps.F[1];
-			fz[gi] = ps.F[2];
+			MV += finish(kick, gi, ps.F[0], ps.F[1], ps.F[2], rx, ry, rz, cid, lists, fx, fy, fz, status);
 			U += ps.U;
 			W += ps.W;
 			NP += ps.np;
@@ -1194,11 +1246,12 @@ __device__ __forceinline__ void list_pairs_warp(const Const& p, const Box& bx, i
 	U = warp_sum(U);
 	W = warp_sum(W);
 	NP = warp_sum(NP);
+	MV = warp_sum(MV);
 	if (lane == 0) {
 		partials[4 * (int64_t) brick + 0] = U;
 		partials[4 * (int64_t) brick + 1] = W;
 		partials[4 * (int64_t) brick + 2] = NP;
-		partials[4 * (int64_t) brick + 3] = 0.0;
+		partials[4 * (int64_t) brick + 3] = MV;
 	}
 }
 

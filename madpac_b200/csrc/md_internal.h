@@ -133,7 +133,11 @@ cudaError_t launch_bin(Context* c, bool permute_forces);
 // once unless *c->rebuild == c->step_id; the sorted arrays end in c->p (buffer roles unchanged).
 cudaError_t launch_rebuild(Context* c, const Grid& g);
 cudaError_t launch_pairs(Context* c);                 // partials -> scalars[0..2] (U6sum, W, npairs)
-cudaError_t launch_pairs_skin(Context* c);            // the same in the Verlet-skin mode
+// The same in the Verlet-skin mode; with kick_mode 1 or 2 the kernels also apply the closing kick
+// of the step (mode 2, the last step of a run: forces and velocities stored) or the closing kick,
+// the opening kick and drift of the next step into c->q's position arrays (mode 1: the caller swaps
+// the position buffers of c->p and c->q afterwards), and write the step record to `record`.
+cudaError_t launch_pairs_skin(Context* c, int kick_mode = 0, double dt = 0.0, double* record = nullptr);
 int64_t skin_partials_needed(const Context* c);       // reduction partials the skin-mode kernels write
 // With skin_check the pre-kick also sets *c->rebuild = c->step_id when a molecule is more than
 // skin/2 from its position at the last build.

@@ -61,16 +61,22 @@ __global__ void __launch_bounds__(brick::kThreads, kFP64 ? 2 : kListMinBlocks)
                  const int32_t* __restrict__ cstart, const PairParams* __restrict__ pp,
                  double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
                  double* __restrict__ partials, int* __restrict__ status, const int* __restrict__ gate,
-                 brick::Lists lists, unsigned* tickets, double* scalars) {
+                 brick::Lists lists, unsigned* tickets, double* scalars, brick::Kick kick, double* record) {
 	extern __shared__ __align__(16) unsigned char smem[];
 	brick::load_params(smem, brick::layout(p.s_cap, kFP64, 0, false), pp, p.ns);
 	__syncthreads();
 	// sparse bricks were evaluated by k_pairs_list_sparse (launched before)
 	if (!lists.kind[blockIdx.x])
 		brick::list_pairs<kFP64, kSingle, kLjIsRc>(p, bx, blockIdx.x, blockIdx.x, smem, rx, ry, rz, cid, cstart, fx,
-		                                           fy, fz, partials, status, lists);
-	// U6 sum, virial sum and pair count of the step, summed by the last brick to finish
-	last_block_sum(tickets, partials, gridDim.x, 3, scalars);
+		                                           fy, fz, partials, status, lists, kick);
+	// U6 sum, virial sum, pair count (and sum m v^2 of the closing kick) of the step, summed by the
+	// last brick to finish, which also writes the step record {Upot, virial, sum m v^2, pairs}
+	if (last_block_sum(tickets, partials, gridDim.x, kick.mode ? 4 : 3, scalars) && threadIdx.x == 0 && record) {
+		record[0] = scalars[0] * 0.5 / 6.;
+		record[1] = scalars[1] * 0.5;
+		record[2] = scalars[3];
+		record[3] = scalars[2] * 0.5;
+	}
 }
 
 // Sparse bricks (few molecules, e.g. a vapour), one warp each, eight per CTA.
@@ -81,7 +87,7 @@ __global__ void __launch_bounds__(brick::kThreads, 2)
                         const int32_t* __restrict__ cid, const int32_t* __restrict__ cstart,
                         const PairParams* __restrict__ pp, double* __restrict__ fx, double* __restrict__ fy,
                         double* __restrict__ fz, double* __restrict__ partials, int* __restrict__ status,
-                        brick::Lists lists) {
+                        brick::Lists lists, brick::Kick kick) {
 	extern __shared__ __align__(16) unsigned char smem[];
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const int brick_id = blockIdx.x * brick::kWarps + warp;
@@ -103,7 +109,7 @@ __global__ void __launch_bounds__(brick::kThreads, 2)
 		    make_float4(1e15f, 1e15f, 1e15f, __uint_as_float((256u << 18) | (256u << 9) | 256u));
 	__syncwarp();
 	brick::list_pairs_warp<kFP64, kSingle, kLjIsRc>(p, bx, brick_id, ws, rx, ry, rz, cid, cstart, fx, fy, fz,
-	                                                partials, status, lists);
+	                                                partials, status, lists, kick);
 }
 
 
@@ -145,18 +151,19 @@ cudaError_t go(Context* c, const Plan& P, K kern, const int* gate, const brick::
 
 // kind 0: plain traversal, 2: list evaluation of the skin mode
 template <int kKind>
-cudaError_t dispatch(Context* c, const Plan& P, const int* gate, const brick::Lists& lists) {
+cudaError_t dispatch(Context* c, const Plan& P, const int* gate, const brick::Lists& lists,
+                     const brick::Kick& kick = brick::Kick{}, double* record = nullptr) {
 	const bool fp64 = c->precision == MDGPU_FP64;
 	const bool single = c->sp.n == 1, ljrc = c->rc_lj == c->rc;
 	if (kKind == 2) {
 		unsigned* t = c->tickets;
 		double* out = c->scalars;
-		if (fp64) return single ? go(c, P, k_pairs_list<true, true, false>, gate, lists, t, out)
-		                        : go(c, P, k_pairs_list<true, false, false>, gate, lists, t, out);
-		if (ljrc) return single ? go(c, P, k_pairs_list<false, true, true>, gate, lists, t, out)
-		                        : go(c, P, k_pairs_list<false, false, true>, gate, lists, t, out);
-		return single ? go(c, P, k_pairs_list<false, true, false>, gate, lists, t, out)
-		              : go(c, P, k_pairs_list<false, false, false>, gate, lists, t, out);
+		if (fp64) return single ? go(c, P, k_pairs_list<true, true, false>, gate, lists, t, out, kick, record)
+		                        : go(c, P, k_pairs_list<true, false, false>, gate, lists, t, out, kick, record);
+		if (ljrc) return single ? go(c, P, k_pairs_list<false, true, true>, gate, lists, t, out, kick, record)
+		                        : go(c, P, k_pairs_list<false, false, true>, gate, lists, t, out, kick, record);
+		return single ? go(c, P, k_pairs_list<false, true, false>, gate, lists, t, out, kick, record)
+		              : go(c, P, k_pairs_list<false, false, false>, gate, lists, t, out, kick, record);
 	}
 	if (fp64) return single ? go(c, P, k_pairs_brick<true, true, false>, gate, lists)
 	                        : go(c, P, k_pairs_brick<true, false, false>, gate, lists);
@@ -192,8 +199,27 @@ cudaError_t launch_pairs_brick(Context* c) {
 	return launch_reduce(c, P.nbricks, c->scalars, 3);
 }
 
-cudaError_t launch_pairs_skin(Context* c) {
+cudaError_t launch_pairs_skin(Context* c, int kick_mode, double dt, double* record) {
 	brick::Lists l = lists_of(c);
+	brick::Kick kick{};
+	kick.mode = kick_mode;
+	if (kick_mode) {
+		kick.id = c->step_id + 1;   // the step whose rebuild a long drift asks for
+		kick.dt = dt;
+		kick.half2 = 0.25 * c->skin * c->skin;
+		for (int k = 0; k < c->sp.n; k++) {
+			kick.post[k] = (0.5 * dt) / c->sp.mass[k];
+			kick.pre[k] = (.5 * dt) / c->sp.mass[k];
+			kick.mass[k] = c->sp.mass[k];
+		}
+		kick.vx = c->p.vx;
+		kick.vy = c->p.vy;
+		kick.vz = c->p.vz;
+		kick.ox = c->q.rx;
+		kick.oy = c->q.ry;
+		kick.oz = c->q.rz;
+		kick.flag = c->rebuild;
+	}
 	const Plan P = plan(c, c->gs, c->rc, 2);
 	l.sentinel = P.p.s_cap;   // the evaluation kernel's sentinel slot terminates every list
 	prof_begin(c, 1);
@@ -224,9 +250,9 @@ cudaError_t launch_pairs_skin(Context* c) {
 		if (e == cudaSuccess)
 			ks<<<(P.nbricks + brick::kWarps - 1) / brick::kWarps, brick::kThreads, sbytes, c->stream>>>(
 			    ps, P.bx, P.nbricks, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->cell_start, c->d_pp, c->p.fx, c->p.fy,
-			    c->p.fz, c->partials, c->status, l);
+			    c->p.fz, c->partials, c->status, l, kick);
 	}
-	if (e == cudaSuccess) e = dispatch<2>(c, P, nullptr, l);
+	if (e == cudaSuccess) e = dispatch<2>(c, P, nullptr, l, kick, record);
 	if (e == cudaSuccess) e = cudaGetLastError();
 	prof_end(c, 1, 3);
 	return e;

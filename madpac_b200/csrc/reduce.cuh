@@ -10,30 +10,34 @@ __device__ __forceinline__ double warp_sum(double v) {
 	return v;
 }
 
-// Block-wide sum of three doubles into partials[slot*4 + k] (blockDim.x <= kReduceBlock).
-__device__ __forceinline__ void block_sum3_at(double a, double b, double c, double* partials, int64_t slot) {
-	__shared__ double sh[3][kReduceBlock / 32];
+// Block-wide sums of three (or four) doubles into partials[slot*4 + k] (blockDim.x <= kReduceBlock).
+__device__ __forceinline__ void block_sum3_at(double a, double b, double c, double* partials, int64_t slot,
+                                              double d = 0.0) {
+	__shared__ double sh[4][kReduceBlock / 32];
 	a = warp_sum(a);
 	b = warp_sum(b);
 	c = warp_sum(c);
+	d = warp_sum(d);
 	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	if (lane == 0) {
 		sh[0][warp] = a;
 		sh[1][warp] = b;
 		sh[2][warp] = c;
+		sh[3][warp] = d;
 	}
 	__syncthreads();
 	if (threadIdx.x == 0) {
-		double s0 = 0, s1 = 0, s2 = 0;
+		double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
 		for (int w = 0; w < (int) (blockDim.x >> 5); w++) {
 			s0 += sh[0][w];
 			s1 += sh[1][w];
 			s2 += sh[2][w];
+			s3 += sh[3][w];
 		}
 		partials[slot * 4 + 0] = s0;
 		partials[slot * 4 + 1] = s1;
 		partials[slot * 4 + 2] = s2;
-		partials[slot * 4 + 3] = 0.0;
+		partials[slot * 4 + 3] = s3;
 	}
 }
 
