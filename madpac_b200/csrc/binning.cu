@@ -56,50 +56,77 @@ __device__ __forceinline__ bool key_less(uint64_t ka, int32_t sa, uint64_t kb, i
 	return ka < kb || (ka == kb && sa < sb);
 }
 
+// Molecule `from` to slot `to` of the other buffer.
+__device__ __forceinline__ void move_one(int32_t from, int32_t to, uint64_t key, int64_t c, const Particles& src,
+                                         const Particles& dst, int32_t* cell_out, bool with_forces) {
+	dst.rx[to] = src.rx[from];
+	dst.ry[to] = src.ry[from];
+	dst.rz[to] = src.rz[from];
+	dst.vx[to] = src.vx[from];
+	dst.vy[to] = src.vy[from];
+	dst.vz[to] = src.vz[from];
+	if (with_forces) {
+		dst.fx[to] = src.fx[from];
+		dst.fy[to] = src.fy[from];
+		dst.fz[to] = src.fz[from];
+	}
+	dst.id[to] = key;
+	dst.cid[to] = src.cid[from];
+	dst.uidx[to] = src.uidx[from];
+	cell_out[to] = (int32_t) c;
+}
+
+// Cells of up to 32 x kSortRegs molecules are ranked from keys held in registers (warp shuffles);
+// larger ones read the keys from global memory.
+constexpr int kSortRegs = 4;
+
 // One warp per cell c: order the cell's molecules by (id, previous slot) and gather all fields.
+// Each molecule's slot is the number of the cell's molecules with a smaller key.
 __device__ __forceinline__ void sort_cell(int64_t c, int lane, const int32_t* start, const int32_t* perm,
                                           const Particles& src, const Particles& dst, int32_t* cell_out,
                                           bool with_forces) {
-	int32_t s = start[c], m = start[c + 1] - s;
+	const int32_t s = start[c], m = start[c + 1] - s;
+	if (m <= 32 * kSortRegs) {
+		uint64_t key[kSortRegs];
+		int32_t from[kSortRegs], pos[kSortRegs];
+#pragma unroll
+		for (int r = 0; r < kSortRegs; r++) {
+			const int32_t e = 32 * r + lane;
+			from[r] = 0x7fffffff;   // padding sorts after every molecule
+			key[r] = ~0ull;
+			pos[r] = 0;
+			if (e < m) {
+				from[r] = perm[s + e];
+				key[r] = src.id[from[r]];
+			}
+		}
+#pragma unroll
+		for (int r2 = 0; r2 < kSortRegs; r2++) {
+			if (32 * r2 >= m) break;
+			for (int k = 0; k < 32; k++) {
+				const uint64_t ok = __shfl_sync(0xffffffffu, key[r2], k);
+				const int32_t of = __shfl_sync(0xffffffffu, from[r2], k);
+#pragma unroll
+				for (int r = 0; r < kSortRegs; r++)
+					if (key_less(ok, of, key[r], from[r])) pos[r]++;
+			}
+		}
+#pragma unroll
+		for (int r = 0; r < kSortRegs; r++)
+			if (32 * r + lane < m) move_one(from[r], s + pos[r], key[r], c, src, dst, cell_out, with_forces);
+		return;
+	}
 	for (int32_t e0 = 0; e0 < m; e0 += 32) {
-		int32_t e = e0 + lane;
-		int32_t from = -1;
-		uint64_t key = 0;
+		const int32_t e = e0 + lane;
+		if (e >= m) continue;
+		const int32_t from = perm[s + e];
+		const uint64_t key = src.id[from];
 		int32_t pos = 0;
-		if (e < m) {
-			from = perm[s + e];
-			key = src.id[from];
+		for (int32_t k = 0; k < m; k++) {
+			const int32_t of = perm[s + k];
+			if (key_less(src.id[of], of, key, from)) pos++;
 		}
-		if (m <= 32) {
-			for (int k = 0; k < m; k++) {
-				uint64_t ok = __shfl_sync(0xffffffffu, key, k);
-				int32_t of = __shfl_sync(0xffffffffu, from, k);
-				if (key_less(ok, of, key, from)) pos++;
-			}
-		} else if (e < m) {
-			for (int32_t k = 0; k < m; k++) {
-				int32_t of = perm[s + k];
-				if (key_less(src.id[of], of, key, from)) pos++;
-			}
-		}
-		if (e < m) {
-			int32_t to = s + pos;
-			dst.rx[to] = src.rx[from];
-			dst.ry[to] = src.ry[from];
-			dst.rz[to] = src.rz[from];
-			dst.vx[to] = src.vx[from];
-			dst.vy[to] = src.vy[from];
-			dst.vz[to] = src.vz[from];
-			if (with_forces) {
-				dst.fx[to] = src.fx[from];
-				dst.fy[to] = src.fy[from];
-				dst.fz[to] = src.fz[from];
-			}
-			dst.id[to] = key;
-			dst.cid[to] = src.cid[from];
-			dst.uidx[to] = src.uidx[from];
-			cell_out[to] = (int32_t) c;
-		}
+		move_one(from, s + pos, key, c, src, dst, cell_out, with_forces);
 	}
 }
 
