@@ -430,6 +430,8 @@ int mdgpu_destroy(mdgpu_ctx* ctx) {
 	cudaFree(c->rebuild);
 	cudaFree(c->builds);
 	cudaFree(c->bar);
+	cudaFree(c->sparse_count);
+	if (c->h_sparse) cudaFreeHost(c->h_sparse);
 	cudaFree(c->chunk);
 	cudaFree(c->tickets);
 	cudaFree(c->brick_kind);
@@ -769,6 +771,10 @@ int skin_prepare(Context* c) {
 		MD_CUDA(cudaMemsetAsync(c->bar, 0, sizeof(unsigned) * 4, c->stream));
 		c->chunk_cap = 8192;
 		MD_CUDA(cudaMalloc(&c->chunk, sizeof(int32_t) * c->chunk_cap));
+		MD_CUDA(cudaMalloc(&c->sparse_count, sizeof(unsigned)));
+		MD_CUDA(cudaMemsetAsync(c->sparse_count, 0, sizeof(unsigned), c->stream));
+		MD_CUDA(cudaMallocHost(&c->h_sparse, sizeof(int)));
+		*c->h_sparse = 1;   // unknown until a build has run: launch the sparse-brick kernel
 	}
 	return MDGPU_OK;
 }
@@ -897,6 +903,9 @@ int enqueue_steps(Context* c, int32_t nsteps, double dt) {
 				std::swap(c->p.rz, c->q.rz);
 			}
 		}
+		// whether the last build found sparse bricks: decides, for later runs, whether the sparse-brick
+		// kernel is launched (the dense kernel evaluates every brick when it is not)
+		MD_CUDA(cudaMemcpyAsync(c->h_sparse, c->sparse_count, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
 		return MDGPU_OK;
 	}
 	// the closing kick of step k and the opening kick of step k+1 run as one pass; the record of

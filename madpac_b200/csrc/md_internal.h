@@ -112,6 +112,8 @@ struct Context {
 	int32_t* chunk = nullptr;       // per-CTA scan sums of the cooperative rebuild
 	int chunk_cap = 0;
 	unsigned long long* builds = nullptr;   // builds so far (device counter)
+	unsigned* sparse_count = nullptr;       // sparse bricks found by the last build (device)
+	int* h_sparse = nullptr;                // pinned host copy, read back at the end of each run
 	bool lists_valid = false;       // the sort order has not changed since the lists were built
 	double* adj = nullptr;          // adjoint buffers: cotangents, outputs, parameter partials
 	int64_t adj_cap = 0;

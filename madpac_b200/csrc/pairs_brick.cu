@@ -65,8 +65,8 @@ __global__ void __launch_bounds__(brick::kThreads, kFP64 ? 2 : kListMinBlocks)
 	extern __shared__ __align__(16) unsigned char smem[];
 	brick::load_params(smem, brick::layout(p.s_cap, kFP64, 0, false), pp, p.ns);
 	__syncthreads();
-	// sparse bricks were evaluated by k_pairs_list_sparse (launched before)
-	if (!lists.kind[blockIdx.x])
+	// sparse bricks were evaluated by k_pairs_list_sparse (launched before, when lists.kind is set)
+	if (!(lists.kind && lists.kind[blockIdx.x]))
 		brick::list_pairs<kFP64, kSingle, kLjIsRc>(p, bx, blockIdx.x, blockIdx.x, smem, rx, ry, rz, cid, cstart, fx,
 		                                           fy, fz, partials, status, lists, kick);
 	// U6 sum, virial sum, pair count (and sum m v^2 of the closing kick) of the step, summed by the
@@ -184,6 +184,7 @@ brick::Lists lists_of(Context* c) {
 	l.cap = c->list_cap;
 	l.builds = c->builds;
 	l.kind = c->brick_kind;
+	l.sparse_count = c->sparse_count;
 	return l;
 }
 
@@ -236,8 +237,12 @@ cudaError_t launch_pairs_skin(Context* c, int kick_mode, double dt, double* reco
 		k_build_lists<<<grid, brick::kThreads, bbytes, c->stream>>>(bb, nbricks, s_cap, c->p.rx, c->p.ry, c->p.rz,
 		                                                           c->cell_start, c->rebuild, c->step_id, l);
 	// evaluation, every step: sparse bricks one warp each, then the others (whose last CTA sums the
-	// partials of all bricks)
-	if (e == cudaSuccess) {
+	// partials of all bricks). When the last build of an earlier run found no sparse brick the
+	// dense kernel takes every brick (kind not consulted) and the sparse kernel is not launched.
+	const bool sparse = !c->h_sparse || *(volatile int*) c->h_sparse != 0;
+	brick::Lists ld = l;
+	if (!sparse) ld.kind = nullptr;
+	if (e == cudaSuccess && sparse) {
 		const bool fp64 = c->precision == MDGPU_FP64;
 		const bool single = c->sp.n == 1, ljrc = c->rc_lj == c->rc;
 		auto ks = fp64 ? (single ? k_pairs_list_sparse<true, true, false> : k_pairs_list_sparse<true, false, false>)
@@ -252,9 +257,9 @@ cudaError_t launch_pairs_skin(Context* c, int kick_mode, double dt, double* reco
 			    ps, P.bx, P.nbricks, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->cell_start, c->d_pp, c->p.fx, c->p.fy,
 			    c->p.fz, c->partials, c->status, l, kick);
 	}
-	if (e == cudaSuccess) e = dispatch<2>(c, P, nullptr, l, kick, record);
+	if (e == cudaSuccess) e = dispatch<2>(c, P, nullptr, ld, kick, record);
 	if (e == cudaSuccess) e = cudaGetLastError();
-	prof_end(c, 1, 3);
+	prof_end(c, 1, sparse ? 3 : 2);
 	return e;
 }
 
