@@ -430,7 +430,8 @@ int mdgpu_destroy(mdgpu_ctx* ctx) {
 	cudaFree(c->rebuild);
 	cudaFree(c->builds);
 	cudaFree(c->bar);
-	cudaFree(c->sparse_count);
+	cudaFree(c->brick_counts);
+	cudaFree(c->brick_list);
 	if (c->h_sparse) cudaFreeHost(c->h_sparse);
 	cudaFree(c->chunk);
 	cudaFree(c->tickets);
@@ -751,9 +752,12 @@ int skin_prepare(Context* c) {
 	const int64_t parts = skin_partials_needed(c);
 	if (c->brick_kind == nullptr || c->list_n != n || c->lists_valid == false) {
 		cudaFree(c->brick_kind);
+		cudaFree(c->brick_list);
 		c->brick_kind = nullptr;
+		c->brick_list = nullptr;
 		MD_CUDA(cudaMalloc(&c->brick_kind, parts));
 		MD_CUDA(cudaMemsetAsync(c->brick_kind, 0, parts, c->stream));
+		MD_CUDA(cudaMalloc(&c->brick_list, sizeof(int32_t) * 2 * parts));
 	}
 	if (c->partial_cap < parts) {
 		MD_CUDA(cudaStreamSynchronize(c->stream));
@@ -771,8 +775,8 @@ int skin_prepare(Context* c) {
 		MD_CUDA(cudaMemsetAsync(c->bar, 0, sizeof(unsigned) * 4, c->stream));
 		c->chunk_cap = 8192;
 		MD_CUDA(cudaMalloc(&c->chunk, sizeof(int32_t) * c->chunk_cap));
-		MD_CUDA(cudaMalloc(&c->sparse_count, sizeof(unsigned)));
-		MD_CUDA(cudaMemsetAsync(c->sparse_count, 0, sizeof(unsigned), c->stream));
+		MD_CUDA(cudaMalloc(&c->brick_counts, sizeof(unsigned) * 4));
+		MD_CUDA(cudaMemsetAsync(c->brick_counts, 0, sizeof(unsigned) * 4, c->stream));
 		MD_CUDA(cudaMallocHost(&c->h_sparse, sizeof(int)));
 		*c->h_sparse = 1;   // unknown until a build has run: launch the sparse-brick kernel
 	}
@@ -905,7 +909,7 @@ int enqueue_steps(Context* c, int32_t nsteps, double dt) {
 		}
 		// whether the last build found sparse bricks: decides, for later runs, whether the sparse-brick
 		// kernel is launched (the dense kernel evaluates every brick when it is not)
-		MD_CUDA(cudaMemcpyAsync(c->h_sparse, c->sparse_count, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+		MD_CUDA(cudaMemcpyAsync(c->h_sparse, c->brick_counts, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
 		return MDGPU_OK;
 	}
 	// the closing kick of step k and the opening kick of step k+1 run as one pass; the record of

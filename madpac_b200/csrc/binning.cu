@@ -250,7 +250,7 @@ struct RebuildArgs {
 	int step;
 	unsigned* bar;
 	int64_t timeout_ns;
-	unsigned* sparse_count;   // zeroed for the list build that follows
+	unsigned* brick_counts;   // sparse/dense brick counts, zeroed for the list build that follows
 };
 
 constexpr int kRebuildThreads = 256;
@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(kRebuildThreads) k_rebuild(RebuildArgs a) {
 	if (threadIdx.x == 0) s_flag = (*a.flag == a.step && !(*((volatile int*) a.status) & kStatusTimeout)) ? 0 : 1;
 	__syncthreads();
 	if (s_flag) return;   // no build requested for this step
-	if (blockIdx.x == 0 && threadIdx.x == 0 && a.sparse_count) *a.sparse_count = 0u;
+	if (blockIdx.x == 0 && threadIdx.x < 2 && a.brick_counts) a.brick_counts[threadIdx.x] = 0u;
 	const int64_t nthreads = (int64_t) gridDim.x * blockDim.x;
 	const int64_t tid = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	const int64_t nc = a.g.ncells;
@@ -390,7 +390,7 @@ cudaError_t launch_rebuild(Context* c, const Grid& g) {
 	a.step = c->step_id;
 	a.bar = c->bar;
 	a.timeout_ns = 2000000000LL;
-	a.sparse_count = c->sparse_count;
+	a.brick_counts = c->brick_counts;
 	// one chunk sum per CTA
 	int grid = max_ctas;
 	if (grid > c->chunk_cap) grid = c->chunk_cap;

@@ -432,7 +432,9 @@ struct Lists {
 	unsigned long long* builds;        // incremented once per build
 	int sentinel;                      // staged slot of the list kernel's far-away sentinel
 	unsigned char* kind;               // per brick: 1 = sparse (evaluated one warp per brick)
-	unsigned* sparse_count;            // sparse bricks of the build (or null)
+	unsigned* counts;                  // sparse [0] and dense [1] bricks of the build (or null)
+	int32_t* blist;                    // dense bricks at [0, nbricks), sparse ones from nbricks on
+	int nbricks;
 };
 // A brick is sparse when its whole staged region holds at most kSparseCap molecules and its own
 // cells at most 32: one warp stages and evaluates it, without CTA-wide barriers.
@@ -799,7 +801,10 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 		}
 		const bool sparse = s_cs[64] <= kSparseCap && n_own <= 32;
 		lists.kind[kind_slot] = sparse ? 1 : 0;
-		if (sparse && lists.sparse_count) atomicAdd(lists.sparse_count, 1u);
+		if (lists.counts) {
+			const unsigned at = atomicAdd(lists.counts + (sparse ? 0 : 1), 1u);
+			lists.blist[(sparse ? lists.nbricks : 0) + (int) at] = (int32_t) kind_slot;
+		}
 		if (brick == 0) atomicAdd(lists.builds, 1ull);
 	}
 }

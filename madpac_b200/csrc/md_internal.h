@@ -112,7 +112,11 @@ struct Context {
 	int32_t* chunk = nullptr;       // per-CTA scan sums of the cooperative rebuild
 	int chunk_cap = 0;
 	unsigned long long* builds = nullptr;   // builds so far (device counter)
-	unsigned* sparse_count = nullptr;       // sparse bricks found by the last build (device)
+	// device: bricks of the last build, sparse [0] and dense [1], and the work queues of the sparse [3]
+	// and dense [2] list kernels; brick_list: the dense bricks' indices, then (from nbricks on) the
+	// sparse ones, in the order the build found them
+	unsigned* brick_counts = nullptr;
+	int32_t* brick_list = nullptr;
 	int* h_sparse = nullptr;                // pinned host copy, read back at the end of each run
 	bool lists_valid = false;       // the sort order has not changed since the lists were built
 	double* adj = nullptr;          // adjoint buffers: cotangents, outputs, parameter partials

@@ -63,26 +63,48 @@ __global__ void __launch_bounds__(brick::kThreads, kFP64 ? 2 : kListMinBlocks)
                  double* __restrict__ partials, int* __restrict__ status, const int* __restrict__ gate,
                  brick::Lists lists, unsigned* tickets, double* scalars, brick::Kick kick, double* record) {
 	extern __shared__ __align__(16) unsigned char smem[];
+	__shared__ int s_item;
 	brick::load_params(smem, brick::layout(p.s_cap, kFP64, 0, false), pp, p.ns);
-	__syncthreads();
-	// sparse bricks were evaluated by k_pairs_list_sparse (launched before, when lists.kind is set)
-	if (!(lists.kind && lists.kind[blockIdx.x]))
+	if (lists.kind == nullptr) {
+		// every brick, one CTA each
+		__syncthreads();
 		brick::list_pairs<kFP64, kSingle, kLjIsRc>(p, bx, blockIdx.x, blockIdx.x, smem, rx, ry, rz, cid, cstart, fx,
 		                                           fy, fz, partials, status, lists, kick);
-	// U6 sum, virial sum, pair count (and sum m v^2 of the closing kick) of the step, summed by the
-	// last brick to finish, which also writes the step record {Upot, virial, sum m v^2, pairs}
-	if (last_block_sum(tickets, partials, gridDim.x, kick.mode ? 4 : 3, scalars) && threadIdx.x == 0 && record) {
-		record[0] = scalars[0] * 0.5 / 6.;
-		record[1] = scalars[1] * 0.5;
-		record[2] = scalars[3];
-		record[3] = scalars[2] * 0.5;
+	} else {
+		// the dense bricks of the last build (the sparse ones go to k_pairs_list_sparse): a resident
+		// grid takes them from a queue
+		const int nwork = (int) *(volatile unsigned*) (lists.counts + 1);
+		for (;;) {
+			__syncthreads();
+			if (threadIdx.x == 0) s_item = (int) atomicAdd(lists.counts + 2, 1u);
+			__syncthreads();
+			const int item = s_item;
+			if (item >= nwork) break;
+			const int b = lists.blist[item];
+			brick::list_pairs<kFP64, kSingle, kLjIsRc>(p, bx, b, b, smem, rx, ry, rz, cid, cstart, fx, fy, fz,
+			                                           partials, status, lists, kick);
+		}
+	}
+	// U6 sum, virial sum, pair count (and sum m v^2 of the closing kick) of the step over every
+	// brick's partials, summed by the last CTA to finish, which also writes the step record
+	// {Upot, virial, sum m v^2, pairs} and resets both work queues
+	if (last_block_sum(tickets, partials, lists.nbricks, kick.mode ? 4 : 3, scalars) && threadIdx.x == 0) {
+		lists.counts[2] = 0u;
+		lists.counts[3] = 0u;
+		if (record) {
+			record[0] = scalars[0] * 0.5 / 6.;
+			record[1] = scalars[1] * 0.5;
+			record[2] = scalars[3];
+			record[3] = scalars[2] * 0.5;
+		}
 	}
 }
 
-// Sparse bricks (few molecules, e.g. a vapour), one warp each, eight per CTA.
+// Sparse bricks (few molecules, e.g. a vapour), one warp each: every warp of a resident grid takes
+// the sparse bricks of the last build from a queue.
 template <bool kFP64, bool kSingle, bool kLjIsRc>
 __global__ void __launch_bounds__(brick::kThreads, 2)
-    k_pairs_list_sparse(brick::Const p, brick::Box bx, int nbricks, const double* __restrict__ rx,
+    k_pairs_list_sparse(brick::Const p, brick::Box bx, const double* __restrict__ rx,
                         const double* __restrict__ ry, const double* __restrict__ rz,
                         const int32_t* __restrict__ cid, const int32_t* __restrict__ cstart,
                         const PairParams* __restrict__ pp, double* __restrict__ fx, double* __restrict__ fy,
@@ -90,8 +112,6 @@ __global__ void __launch_bounds__(brick::kThreads, 2)
                         brick::Lists lists, brick::Kick kick) {
 	extern __shared__ __align__(16) unsigned char smem[];
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const int brick_id = blockIdx.x * brick::kWarps + warp;
-	if (brick_id >= nbricks || !lists.kind[brick_id]) return;
 	unsigned char* ws = smem + warp * brick::sparse_warp_bytes(kFP64);
 	const brick::SmemLayout L = brick::layout(brick::kSparseCap, kFP64, 0, false);
 	double* pd = reinterpret_cast<double*>(ws + L.params);
@@ -107,11 +127,27 @@ __global__ void __launch_bounds__(brick::kThreads, 2)
 	if (lane == 0)
 		reinterpret_cast<float4*>(ws + L.hi)[brick::kSparseCap] =
 		    make_float4(1e15f, 1e15f, 1e15f, __uint_as_float((256u << 18) | (256u << 9) | 256u));
-	__syncwarp();
-	brick::list_pairs_warp<kFP64, kSingle, kLjIsRc>(p, bx, brick_id, ws, rx, ry, rz, cid, cstart, fx, fy, fz,
-	                                                partials, status, lists, kick);
+	const int nwork = (int) *(volatile unsigned*) lists.counts;
+	for (;;) {
+		__syncwarp();
+		int item = 0;
+		if (lane == 0) item = (int) atomicAdd(lists.counts + 3, 1u);
+		item = __shfl_sync(brick::kFull, item, 0);
+		if (item >= nwork) break;
+		const int b = lists.blist[lists.nbricks + item];
+		brick::list_pairs_warp<kFP64, kSingle, kLjIsRc>(p, bx, b, ws, rx, ry, rz, cid, cstart, fx, fy, fz, partials,
+		                                                status, lists, kick);
+	}
 }
 
+// Resident grid of a kernel: the CTAs that fit on the device at once (at most `cap`).
+template <typename K>
+int resident_grid(const Context* c, K kern, size_t smem, int cap) {
+	int per_sm = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, brick::kThreads, smem) != cudaSuccess || per_sm < 1)
+		per_sm = 1;
+	return std::max(1, std::min(cap, per_sm * c->num_sms));
+}
 
 struct Plan {
 	brick::Const p;
@@ -142,8 +178,11 @@ Plan plan(Context* c, const Grid& g, double filter_radius, int kind) {
 template <typename K, typename... Extra>
 cudaError_t go(Context* c, const Plan& P, K kern, const int* gate, const brick::Lists& lists, Extra... extra) {
 	cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) P.bytes);
+	// the list kernel runs as a resident grid over a queue of the dense bricks when the sparse ones
+	// are evaluated apart (lists.kind set); otherwise one CTA per brick
+	const int grid = lists.kind && sizeof...(Extra) > 0 ? resident_grid(c, kern, P.bytes, P.nbricks) : P.nbricks;
 	if (r == cudaSuccess)
-		kern<<<P.nbricks, brick::kThreads, P.bytes, c->stream>>>(P.p, P.bx, c->p.rx, c->p.ry, c->p.rz, c->p.cid,
+		kern<<<grid, brick::kThreads, P.bytes, c->stream>>>(P.p, P.bx, c->p.rx, c->p.ry, c->p.rz, c->p.cid,
 		                                                         c->cell_start, c->d_pp, c->p.fx, c->p.fy, c->p.fz,
 		                                                         c->partials, c->status, gate, lists, extra...);
 	return r;
@@ -184,7 +223,9 @@ brick::Lists lists_of(Context* c) {
 	l.cap = c->list_cap;
 	l.builds = c->builds;
 	l.kind = c->brick_kind;
-	l.sparse_count = c->sparse_count;
+	l.counts = c->brick_counts;
+	l.blist = c->brick_list;
+	l.nbricks = (int) skin_partials_needed(c);
 	return l;
 }
 
@@ -252,10 +293,11 @@ cudaError_t launch_pairs_skin(Context* c, int kick_mode, double dt, double* reco
 		const size_t sbytes = brick::kWarps * brick::sparse_warp_bytes(fp64);
 		const brick::Const ps = brick::make_const(c->sp.n, brick::kSparseCap, c->rc, c->rc_lj);
 		e = cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sbytes);
+		const int sgrid = resident_grid(c, ks, sbytes, (P.nbricks + brick::kWarps - 1) / brick::kWarps);
 		if (e == cudaSuccess)
-			ks<<<(P.nbricks + brick::kWarps - 1) / brick::kWarps, brick::kThreads, sbytes, c->stream>>>(
-			    ps, P.bx, P.nbricks, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->cell_start, c->d_pp, c->p.fx, c->p.fy,
-			    c->p.fz, c->partials, c->status, l, kick);
+			ks<<<sgrid, brick::kThreads, sbytes, c->stream>>>(ps, P.bx, c->p.rx, c->p.ry, c->p.rz, c->p.cid,
+			                                                   c->cell_start, c->d_pp, c->p.fx, c->p.fy, c->p.fz,
+			                                                   c->partials, c->status, l, kick);
 	}
 	if (e == cudaSuccess) e = dispatch<2>(c, P, nullptr, ld, kick, record);
 	if (e == cudaSuccess) e = cudaGetLastError();
