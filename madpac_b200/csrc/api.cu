@@ -267,6 +267,22 @@ int setup_grid(const double length[3], double cutoff, double cells_in_cutoff, Gr
 	return MDGPU_OK;
 }
 
+// The Verlet-skin grid: cells of edge >= cutoff + skin, so that every molecule that can come within
+// the cutoff before the next build is in the 27 cells around; in a dilute liquid larger, so that a
+// cell holds about kSkinCellOcc molecules at the density around a typical molecule and a 2x2x2
+// brick fills the eight warps of its CTA; an even count per dimension where it is 5 or more.
+constexpr double kSkinCellOcc = 28.0;
+int skin_grid(const Context* c, double skin, Grid& gs, std::string& err) {
+	double edge = c->rc + skin;
+	if (c->rho_typ > 0.0) edge = std::max(edge, std::cbrt(kSkinCellOcc / c->rho_typ));
+	const double length[3] = {c->g.L[0], c->g.L[1], c->g.L[2]};
+	int st = setup_grid(length, edge, 1.0, gs, err);
+	if (st == MDGPU_ERR_BOX_TOO_SMALL && edge > c->rc + skin) st = setup_grid(length, c->rc + skin, 1.0, gs, err);
+	if (st) return st;
+	even_grid(gs);
+	return MDGPU_OK;
+}
+
 void even_grid(Grid& g) {
 	// 2x2x2-cell bricks tile an even number of cells exactly; with an odd count the last brick of
 	// a row owns one cell and leaves most of its CTA idle. Larger cells keep every pair within
@@ -499,6 +515,18 @@ int mdgpu_set_particles(mdgpu_ctx* ctx, int64_t n, const uint64_t* id, const int
 			mx = std::max(mx, ++occ[(size_t) cell]);
 		}
 		c->max_occ = mx;
+		// the density around a typical molecule: sum occ^2 / sum occ per cell volume
+		double s2 = 0.0;
+		for (int32_t o : occ) s2 += (double) o * o;
+		c->rho_typ = s2 / (double) n / (c->g.cell_length[0] * c->g.cell_length[1] * c->g.cell_length[2]);
+	}
+	if (c->skin > 0.0) {
+		// the skin grid follows the density of the new positions
+		Grid gs{};
+		std::string err;
+		int st = skin_grid(c, c->skin, gs, err);
+		if (st) return fail(c, st, "cutoff + skin: " + err);
+		c->gs = gs;
 	}
 	MD_CUDA(cudaSetDevice(c->device));
 	MD_CUDA(cudaStreamSynchronize(c->stream));
@@ -823,14 +851,10 @@ int mdgpu_set_skin(mdgpu_ctx* ctx, double skin) {
 	Context* c = &ctx->c;
 	if (!(skin >= 0.0) || !(skin < c->rc)) return fail(c, MDGPU_ERR_ARG, "skin must be in [0, cutoff)");
 	if (skin > 0.0) {
-		// the lists are built over cells of edge >= cutoff + skin (their own grid), so that every
-		// molecule that can come within the cutoff before the next build is in the 27 cells around
 		Grid gs{};
 		std::string err;
-		const double length[3] = {c->g.L[0], c->g.L[1], c->g.L[2]};
-		int st = setup_grid(length, c->rc + skin, 1.0, gs, err);
+		int st = skin_grid(c, skin, gs, err);
 		if (st) return fail(c, st, "cutoff + skin: " + err);
-		even_grid(gs);
 		c->gs = gs;
 	}
 	c->skin = skin;

@@ -100,6 +100,7 @@ struct Context {
 	double skin = 0.0;
 	Grid gs{};                      // cells of edge >= cutoff + skin on which the lists are built
 	int max_occ = 0;                // largest cell occupancy of the loaded positions (sizes the lists)
+	double rho_typ = 0.0;           // molecule-weighted mean cell density of the loaded positions
 	int list_cap = 0;               // list entries per molecule
 	int64_t list_n = 0;             // molecules the list buffers hold
 	unsigned short* nbr = nullptr;  // list_cap x n staged-slot indices
