@@ -14,6 +14,7 @@ import argparse
 import json
 import math
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -46,9 +47,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--skin", type=float, default=0.3,
                     help="Verlet skin of the step (0: cells and candidates rebuilt every step, as the reference)")
-    ap.add_argument("--workload", choices=["c2", "c3", "batched"], default="c2",
+    ap.add_argument("--workload", choices=["c2", "c3", "batched", "checkpoint"], default="c2",
                     help="c2: the 1M-molecule box (headline); c3: the 4M-molecule two-species slab; "
-                         "batched: the 512-box ensemble")
+                         "batched: the 512-box ensemble; checkpoint: phase-space file write and read of the "
+                         "1M-molecule box through the C ABI")
     ap.add_argument("--boxes", type=int, default=512, help="boxes of the batched ensemble")
     ap.add_argument("--loop-steps", type=int, default=20,
                     help="steps of the loop-over-single-box comparison of the batched workload")
@@ -609,6 +611,70 @@ def run_batched(args, dist: Dist):
     return out
 
 
+# ---------------------------------------------------------------------------- phase-space files
+
+def run_checkpoint(args, dist: Dist):
+    """Write (the reference's checkpoint layout, 6 digits, and 17 digits) and read back the
+    1,048,576-molecule box through mdgpu_write_checkpoint / mdgpu_read_phase_space: host wall clock
+    around each call, device transfers included; beside it the reference writing the same box's
+    checkpoint (Domain::writeCheckpoint via oracle/_ref/ref_driver --time-checkpoint)."""
+    import torch
+
+    from madpac_b200 import mdgpu as M
+    from madpac_b200 import workloads as W
+
+    torch.cuda.set_device(dist.local)
+    system = make_system(dist.rank, args.fcc_cells)
+    lc = M.LinkedCells.from_system(system, M.FP64, device=dist.local)
+    tmp = tempfile.mkdtemp(prefix="mdck_")
+    res = {}
+    for digits in (6, 17):
+        path = os.path.join(tmp, f"ck{digits}.txt")
+        lc.writeCheckpoint(path, 0.0, system.temperature, digits=digits if digits != 6 else 0)   # warm-up
+        times_w, times_r = [], []
+        for _ in range(max(1, args.steps)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            lc.writeCheckpoint(path, 0.0, system.temperature, digits=digits if digits != 6 else 0)
+            times_w.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            lc.readPhaseSpace(path)
+            torch.cuda.synchronize()
+            times_r.append(time.perf_counter() - t0)
+        size = os.path.getsize(path)
+        res[digits] = {"write_s": statistics.median(times_w), "read_s": statistics.median(times_r), "bytes": size}
+    n = system.n
+    w6 = res[6]["write_s"]
+    out = {
+        "metric": "phase-space checkpoint write, molecules/s (1M-molecule box, C ABI, reference layout)",
+        "value": n / w6, "unit": "molecules/s", "n_gpus": dist.world, "steps": args.steps, "warmup": 1,
+        "ms_per_step": w6 * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded FCC lattice, Maxwell-Boltzmann velocities)",
+        "config": {"workload": "checkpoint_1048576", "n_molecules": n, "format": "ICRVQD",
+                   "timing": "host wall clock per call (median of steps), device-to-host and host-to-device "
+                             "copies included; file on the host's local disk"},
+        "write_6_digits": {"seconds": w6, "molecules_per_s": n / w6, "bytes": res[6]["bytes"],
+                           "MB_per_s": res[6]["bytes"] / w6 / 1e6},
+        "read_6_digits": {"seconds": res[6]["read_s"], "molecules_per_s": n / res[6]["read_s"]},
+        "write_17_digits": {"seconds": res[17]["write_s"], "molecules_per_s": n / res[17]["write_s"],
+                            "bytes": res[17]["bytes"]},
+        "read_17_digits": {"seconds": res[17]["read_s"], "molecules_per_s": n / res[17]["read_s"]},
+        "threads": os.cpu_count(),
+    }
+    lc.close()
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    if dist.rank == 0 and not args.no_cpu_baseline and os.path.exists(ref):
+        W.write_inp(system, os.path.join(tmp, "sys.inp"))
+        W.write_cfg(system, os.path.join(tmp, "sys.cfg"), "sys.inp")
+        r = subprocess.run([ref, "--time-checkpoint", "sys.cfg", "ref_ck.txt"], cwd=tmp, capture_output=True, text=True,
+                           timeout=600)
+        secs = json.loads(r.stdout.strip().splitlines()[-1])["seconds"]
+        out["cpu_baseline"] = {"value": n / secs, "unit": "molecules/s", "cores": 1, "kind": "reference",
+                               "sample": "Domain::writeCheckpoint of the full box after prepare_start", "seconds": secs}
+    shutil.rmtree(tmp, ignore_errors=True)
+    return out
+
+
 # ---------------------------------------------------------------------------- reference arm
 
 def run_reference(args, dist: Dist):
@@ -671,7 +737,12 @@ def main():
             print(json.dumps(run_reference(args, solo)), flush=True)
         return
     dist = Dist(args.gpus)
-    out = run_batched(args, dist) if args.workload == "batched" else run_ours(args, dist)
+    if args.workload == "batched":
+        out = run_batched(args, dist)
+    elif args.workload == "checkpoint":
+        out = run_checkpoint(args, dist)
+    else:
+        out = run_ours(args, dist)
     if dist.rank == 0:
         print(json.dumps(out), flush=True)
     dist.close()

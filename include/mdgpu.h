@@ -80,6 +80,21 @@ int mdgpu_set_state(mdgpu_ctx* ctx, int64_t n, const double* r, const double* v)
  * ParticleContainer.h:100-113). Any output pointer may be NULL. */
 int mdgpu_get_particles(mdgpu_ctx* ctx, int64_t n, uint64_t* id, int32_t* cid, double* r, double* v,
                         double* F);
+/* Write the loaded molecules as an old-style phase-space file in the layout of the reference's
+ * checkpoint (replaces Domain::writeCheckpoint, Domain.cpp:462-568, with
+ * DomainDecompDummy::writeMoleculesToFile and Molecule::write, parallel/DomainDecompDummy.cpp:144-154,
+ * molecules/Molecule.cpp:263-270): header with currentTime, the box, the target temperature,
+ * the components, mixing coefficients and epsilonRF, then one ICRVQD line per molecule in caller
+ * order. digits: significant digits of the molecule lines, 0 = the reference's 6 (17 keeps the
+ * exact doubles). */
+int mdgpu_write_checkpoint(mdgpu_ctx* ctx, const char* path, double current_time, double temperature,
+                           double epsilon_rf, int digits);
+/* Load the molecules of an old-style phase-space file (replaces InputOldstyle::readPhaseSpaceHeader
+ * and readPhaseSpace, io/InputOldstyle.cpp:35-392, feeding LinkedCells::addParticle): formats
+ * ICRVQD, ICRVFQDM, ICRV and IRV; the file's box and single-site LJ components must match the
+ * context's (MDGPU_ERR_ARG otherwise). current_time and temperature (may be NULL) receive the
+ * header's values. */
+int mdgpu_read_phase_space(mdgpu_ctx* ctx, const char* path, double* current_time, double* temperature);
 /* Number of molecules held (replaces LinkedCells::getNumberOfParticles, LinkedCells.cpp:301-303). */
 int mdgpu_num_particles(const mdgpu_ctx* ctx, int64_t* n);
 /* Cell geometry: box_cells[3] = boxWidthInNumCells, cell_length[3], halo_min[3]

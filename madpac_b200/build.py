@@ -9,7 +9,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmdgpu.so")
-SOURCES = ["api.cu", "binning.cu", "pairs.cu", "pairs_brick.cu", "integrate.cu", "peaks.cu", "noalloc.cu", "adjoint.cu", "batch.cu"]
+SOURCES = ["api.cu", "binning.cu", "pairs.cu", "pairs_brick.cu", "integrate.cu", "peaks.cu", "noalloc.cu", "adjoint.cu",
+           "batch.cu", "phase_space.cu"]
 HEADERS = ["md_internal.h", "reduce.cuh", "pair_common.cuh", "brick.cuh"]
 
 NVCC_FLAGS = [

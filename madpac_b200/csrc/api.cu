@@ -400,6 +400,7 @@ int mdgpu_create(mdgpu_ctx** out, const double length[3], double cutoff, double 
 		c->sigma[i] = comps[i].sigma;
 		c->do_shift[i] = comps[i].do_shift;
 	}
+	for (int k = 0; k < ncomp * (ncomp - 1); k++) c->mix[k] = mix[k];
 	MD_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
 	MD_CUDA(cudaMalloc(&c->cell_count, sizeof(int32_t) * ncells));
 	MD_CUDA(cudaMalloc(&c->cell_start, sizeof(int32_t) * (ncells + 1)));

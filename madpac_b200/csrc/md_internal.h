@@ -71,6 +71,7 @@ struct Context {
 	Species sp{};
 	double eps[kMaxSpecies], sigma[kMaxSpecies];
 	int do_shift[kMaxSpecies];
+	double mix[kMaxSpecies * kMaxSpecies];   // xi, eta of each species pair i < j, row by row
 	int64_t n = 0;
 	int64_t cap = 0;
 	bool cells_valid = false;

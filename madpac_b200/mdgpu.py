@@ -71,6 +71,8 @@ SIGNATURES = {
     "mdgpu_forces_noalloc": (_I, [_I, _VP, _I64, _VP, _VP, _VP, _D, _D, _I, _VP, _VP, _I, _VP, _VP, _VP,
                                   ctypes.c_char_p, _I]),
     "mdgpu_set_skin": (_I, [_VP, _D]),
+    "mdgpu_write_checkpoint": (_I, [_VP, ctypes.c_char_p, _D, _D, _D, _I]),
+    "mdgpu_read_phase_space": (_I, [_VP, ctypes.c_char_p, _VP, _VP]),
     "mdgpu_skin_builds": (_I, [_VP, _VP]),
     "mdgpu_batch_create": (_I, [ctypes.POINTER(_VP), _I32, _VP, _VP, _D, _D, _D, _I, _VP, _VP, _I, _I]),
     "mdgpu_batch_destroy": (_I, [_VP]),
@@ -415,6 +417,22 @@ class LinkedCells:
         b = ctypes.c_int64()
         self._check(self.lib.mdgpu_skin_builds(self.h, ctypes.byref(b)))
         return b.value
+
+    # -- phase-space files ---------------------------------------------------------------------------
+    def writeCheckpoint(self, path: str, current_time: float = 0.0, temperature: float = 1.0,
+                        epsilon_rf: float = 1.0e10, digits: int = 0) -> None:
+        """The loaded molecules as an old-style phase-space file in the reference's checkpoint layout
+        (Domain::writeCheckpoint); digits 0 = the reference's 6 significant digits."""
+        self._check(self.lib.mdgpu_write_checkpoint(self.h, os.fsencode(path), float(current_time),
+                                                    float(temperature), float(epsilon_rf), int(digits)))
+
+    def readPhaseSpace(self, path: str):
+        """Load the molecules of an old-style phase-space file (InputOldstyle); returns the header's
+        (currentTime, Temperature)."""
+        t, T = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.mdgpu_read_phase_space(self.h, os.fsencode(path), ctypes.byref(t), ctypes.byref(T)))
+        self.n = self.getNumberOfParticles()
+        return t.value, T.value
 
     # -- integrator primitives -------------------------------------------------------------------
     def leapfrogPre(self, dt: float, vcorr: float) -> None:

@@ -14,6 +14,9 @@
 //
 // usage: ref_driver <cfg> <nsteps> <outdir> <dumpsteps: comma list, 0 = after prepare_start>
 //        ref_driver --time <cfg> <nsteps>      (timing only: prints seconds per step as JSON)
+//        ref_driver --checkpoint <cfg> <nsteps> <file> <outdir>   (the reference's checkpoint after
+//                   nsteps steps, and the exact state of that step)
+//        ref_driver --time-checkpoint <cfg> <file>   (seconds to write the initial state's checkpoint)
 #include <sys/time.h>
 
 #include <algorithm>
@@ -124,6 +127,25 @@ public:
 		fclose(sf);
 	}
 
+	// nsteps steps, then the reference's own checkpoint (Domain::writeCheckpoint, Domain.cpp:462-568)
+	// and the exact state of that step (writeArrays)
+	void checkpoint(unsigned long nsteps, const std::string& path, const std::string& outdir) {
+		prepare_start();
+		simulateStart();
+		_numberOfTimesteps = _initSimulation + nsteps - 1;
+		for (_simstep = _initSimulation; _simstep <= _numberOfTimesteps;) simulateStep();
+		_domain->writeCheckpoint(path, _moleculeContainer, _domainDecomposition);
+		writeArrays(outdir, (long) nsteps);
+	}
+
+	// seconds to write the checkpoint of the initial state (after prepare_start)
+	double timeCheckpoint(const std::string& path) {
+		prepare_start();
+		double t0 = now_s();
+		_domain->writeCheckpoint(path, _moleculeContainer, _domainDecomposition);
+		return now_s() - t0;
+	}
+
 	double timeSteps(unsigned long nsteps) {
 		prepare_start();
 		simulateStart();
@@ -142,6 +164,19 @@ int main(int argc, char** argv) {
 		unsigned long n = strtoul(argv[3], nullptr, 10);
 		double s = sim.timeSteps(n);
 		printf("{\"seconds_per_step\": %.9g, \"steps\": %lu}\n", s, n);
+		return 0;
+	}
+	if (argc >= 6 && std::string(argv[1]) == "--checkpoint") {
+		RefDriver sim;
+		sim.readConfigFile(argv[2]);
+		sim.checkpoint(strtoul(argv[3], nullptr, 10), argv[4], argv[5]);
+		return 0;
+	}
+	if (argc >= 4 && std::string(argv[1]) == "--time-checkpoint") {
+		RefDriver sim;
+		sim.readConfigFile(argv[2]);
+		double s = sim.timeCheckpoint(argv[3]);
+		printf("{\"seconds\": %.9g}\n", s);
 		return 0;
 	}
 	if (argc < 5) {
