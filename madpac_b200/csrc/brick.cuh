@@ -871,6 +871,13 @@ __device__ __forceinline__ double finish(const Kick& k, int64_t gi, double Fx, d
 	return mv2;
 }
 
+// Lanes per molecule for g molecules on one warp: the largest power of two with lpm * g <= 32.
+__device__ __forceinline__ int lanes_per_molecule(int g) {
+	int lpm = 1;
+	while (lpm * 2 * g <= 32) lpm *= 2;
+	return lpm;
+}
+
 #ifndef MDGPU_LIST_ACC
 #define MDGPU_LIST_ACC 1
 #endif
@@ -890,20 +897,24 @@ __device__ __forceinline__ double acc_sum(const float* a) {
 	return (double) a[0];
 }
 
-// One chunk of 32 of the brick's own molecules (t0 .. t0 + 31 in the order of the own cells
-// own[0..8] / ocell[0..7]) evaluating their lists, one molecule per lane: forces written, U, W,
-// pair count and the same-position flag accumulated into the caller's sums.
+// A warp evaluates the lists of the brick's own molecules t0 .. t1-1 (in the order of the own cells
+// own[0..8] / ocell[0..7]), lpm lanes per molecule (a power of two, (t1 - t0) * lpm <= 32): lane
+// sub = lane % lpm takes the blocks sub, sub + lpm, ... of its molecule's list, the lanes' forces
+// are summed by a fixed butterfly and the molecule is finished by its first lane; U, W, the pair
+// count and the same-position flag are accumulated into the caller's sums.
 template <bool kFP64, bool kSingle, bool kLjIsRc, bool kClampJ = false>
 __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const Smem& S, const int* s_own,
-                                           const int* s_ocell, int t0, int n_own, const double* rx, const double* ry,
+                                           const int* s_ocell, int t0, int t1, int lpm, const double* rx,
+                                           const double* ry,
                                            const double* rz, const int32_t* cid, const int32_t* cstart, double* fx,
                                            double* fy, double* fz, int* status, const Lists& lists, const Kick& kick,
                                            double& U, double& W, double& NP, double& MV, bool& same) {
 	const int lane = threadIdx.x & 31;
 	const int ns = p.ns;
 	const float eps24_1 = S.pf[0], sig2_1 = S.pf[KK], shift6_1 = S.pf[2 * KK];
-	const int t = t0 + lane;
-	const bool act = t < n_own;
+	const int sub = lane & (lpm - 1);
+	const int t = t0 + lane / lpm;
+	const bool act = t < t1;
 	int w = 0;
 	if (act)
 		while (w < 7 && s_own[w + 1] <= t) w++;
@@ -920,7 +931,7 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 	const int gi = act ? S.gst[s_ocell[w]] + (t - s_own[w]) : S.gst[s_ocell[0]];
 	int cnt = act ? (int) lists.count[gi] : 0;
 	const bool ovf = cnt == kListOverflow;
-	if (ovf) {
+	if (ovf && sub == 0) {
 		// the list overflowed at the build: gather this molecule from global memory
 		PairSums s = gather_pairs<!kFP64>(gi, rx, ry, rz, cid, cstart, bx.g, S.pd, ns, p.rc2, p.rclj2, bx.coff);
 		MV += finish(kick, gi, s.F[0], s.F[1], s.F[2], rx, ry, rz, cid, lists, fx, fy, fz, status);
@@ -928,20 +939,23 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 		W += s.W;
 		NP += s.np;
 		same |= s.same;
-		cnt = 0;
 	}
+	if (ovf) cnt = 0;
 	const int mx = __reduce_max_sync(kFull, cnt);
-	// blocks of 8 entries, one 16-byte load each, the next block loaded while this one is used
+	// blocks of 8 entries, one 16-byte load each, the next block loaded while this one is used;
+	// this lane's blocks are sub, sub + lpm, ... (nk of them at most, the same bound in every lane)
 	const uint4* my8 = reinterpret_cast<const uint4*>(lists.nbr) + gi;
 	const int nb8 = (mx + 7) >> 3;
+	const int nk = (nb8 + lpm - 1) / lpm;
 	double Fx = 0.0, Fy = 0.0, Fz = 0.0;
 	int anp = 0;
-	uint4 nxt = nb8 > 0 ? my8[0] : make_uint4(0u, 0u, 0u, 0u);
+	uint4 nxt = sub < nb8 ? my8[(int64_t) sub * lists.n] : make_uint4(0u, 0u, 0u, 0u);
 	if (kFP64) {
 		double ax[2] = {0, 0}, ay[2] = {0, 0}, az[2] = {0, 0}, au[2] = {0, 0}, aw[2] = {0, 0};
-		for (int b = 0; b < nb8; b++) {
+		for (int k = 0; k < nk; k++) {
+			const int b = sub + k * lpm;
 			const uint4 cur = nxt;
-			if (b + 1 < nb8) nxt = my8[(int64_t) (b + 1) * lists.n];
+			if (b + lpm < nb8) nxt = my8[(int64_t) (b + lpm) * lists.n];
 			const unsigned e[4] = {cur.x, cur.y, cur.z, cur.w};
 #pragma unroll
 			for (int u = 0; u < 8; u++) {
@@ -999,9 +1013,10 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 			au[0] += sign * (fmaf(eps24 * s6, s6 - 1.f, 0.f) + (lj_in ? shift6 : 0.f));
 			aw[0] += sign * r;
 		};
-		for (int b = 0; b < nb8; b++) {
+		for (int k = 0; k < nk; k++) {
+			const int b = sub + k * lpm;
 			uint4 cur = nxt;
-			if (b + 1 < nb8) nxt = my8[(int64_t) (b + 1) * lists.n];
+			if (b + lpm < nb8) nxt = my8[(int64_t) (b + lpm) * lists.n];
 			if (b >= nblk) cur = make_uint4(sent2, sent2, sent2, sent2);
 			bool amb = false;
 #pragma unroll
@@ -1069,7 +1084,7 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 					}
 				}
 			}
-			if ((b & 7) == 7 || b + 1 == nb8) {
+			if ((k & 7) == 7 || k + 1 == nk) {
 				// fold the FP32 partial sums of up to 64 entries into the FP64 accumulators
 				const double sc = kSingle ? (double) eps24_1 : 1.0;
 				Fx += sc * acc_sum(ax);
@@ -1095,7 +1110,13 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 		}
 	}
 	NP += (double) anp;
-	if (act && !ovf) MV += finish(kick, gi, Fx, Fy, Fz, rx, ry, rz, cid, lists, fx, fy, fz, status);
+	// the molecule's force: its lanes' partial sums in a fixed order
+	for (int o = 1; o < lpm; o <<= 1) {
+		Fx += __shfl_xor_sync(kFull, Fx, o);
+		Fy += __shfl_xor_sync(kFull, Fy, o);
+		Fz += __shfl_xor_sync(kFull, Fz, o);
+	}
+	if (act && !ovf && sub == 0) MV += finish(kick, gi, Fx, Fy, Fz, rx, ry, rz, cid, lists, fx, fy, fz, status);
 }
 
 // Forces of brick `brick` from the neighbour lists that build_lists made on the same cell
@@ -1146,9 +1167,18 @@ __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int br
 			same |= s.same;
 		}
 	} else {
-		for (int t0 = warp * 32; t0 < n_own; t0 += kThreads)
-			list_chunk<kFP64, kSingle, kLjIsRc>(p, bx, S, s_own, s_ocell, t0, n_own, rx, ry, rz, cid, cstart, fx, fy, fz,
-			                                    status, lists, kick, U, W, NP, MV, same);
+		// rounds of up to 256 molecules; in each, warp w takes g consecutive molecules with lpm lanes
+		// each (lpm * g <= 32), so a round's last molecules are spread over every warp and no warp
+		// is left alone with a few long lists
+		for (int base = 0; base < n_own; base += kThreads) {
+			const int m = min(kThreads, n_own - base);
+			const int g = (m + kWarps - 1) / kWarps;
+			const int lpm = lanes_per_molecule(g);
+			const int w0 = base + warp * g, w1 = min(w0 + g, base + m);
+			if (w0 < w1)
+				list_chunk<kFP64, kSingle, kLjIsRc>(p, bx, S, s_own, s_ocell, w0, w1, lpm, rx, ry, rz, cid, cstart, fx,
+				                                    fy, fz, status, lists, kick, U, W, NP, MV, same);
+		}
 	}
 	if (same) atomicOr(status, kStatusSamePosition);
 	block_sum3_at(U, W, NP, partials, slot, MV);
@@ -1254,9 +1284,12 @@ __device__ __forceinline__ void list_pairs_warp(const Const& p, const Box& bx, i
 	double U = 0.0, W = 0.0, NP = 0.0, MV = 0.0;
 	bool same = false;
 	if (staged) {
-		for (int t0 = 0; t0 < n_own; t0 += 32)
-			list_chunk<kFP64, kSingle, kLjIsRc, true>(p, bx, S, own, own + 9, t0, n_own, rx, ry, rz, cid, cstart, fx,
-			                                          fy, fz, status, lists, kick, U, W, NP, MV, same);
+		for (int t0 = 0; t0 < n_own; t0 += 32) {
+			const int g = min(32, n_own - t0);
+			list_chunk<kFP64, kSingle, kLjIsRc, true>(p, bx, S, own, own + 9, t0, t0 + g, lanes_per_molecule(g), rx, ry,
+			                                          rz, cid, cstart, fx, fy, fz, status, lists, kick, U, W, NP, MV,
+			                                          same);
+		}
 	} else {
 		for (int t = lane; t < n_own; t += 32) {
 			int w = 0;
