@@ -277,7 +277,10 @@ int skin_grid(const Context* c, double skin, Grid& gs, std::string& err) {
 	if (c->rho_typ > 0.0) edge = std::max(edge, std::cbrt(kSkinCellOcc / c->rho_typ));
 	const double length[3] = {c->g.L[0], c->g.L[1], c->g.L[2]};
 	int st = setup_grid(length, edge, 1.0, gs, err);
-	if (st == MDGPU_ERR_BOX_TOO_SMALL && edge > c->rc + skin) st = setup_grid(length, c->rc + skin, 1.0, gs, err);
+	// larger cells only where every dimension keeps 3 or more: with 2, one brick would hold the
+	// whole box and stage it eight times over
+	if (edge > c->rc + skin && (st || gs.nc[0] < 3 || gs.nc[1] < 3 || gs.nc[2] < 3))
+		st = setup_grid(length, c->rc + skin, 1.0, gs, err);
 	if (st) return st;
 	even_grid(gs);
 	return MDGPU_OK;

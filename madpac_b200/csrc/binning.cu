@@ -17,6 +17,8 @@
 // asked for a build in this step.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "grid_sync.cuh"
 #include "md_internal.h"
 
@@ -391,8 +393,10 @@ cudaError_t launch_rebuild(Context* c, const Grid& g) {
 	a.bar = c->bar;
 	a.timeout_ns = 2000000000LL;
 	a.brick_counts = c->brick_counts;
-	// one chunk sum per CTA
-	int grid = max_ctas;
+	// one chunk sum per CTA; no more CTAs than the molecules and cells need (a co-resident grid of
+	// the whole device would keep every other stream's kernels waiting, also in steps it is gated off)
+	const int64_t work = std::max<int64_t>(c->n, g.ncells);
+	int grid = (int) std::min<int64_t>(max_ctas, (work + kRebuildThreads - 1) / kRebuildThreads);
 	if (grid > c->chunk_cap) grid = c->chunk_cap;
 	if (grid < 1) grid = 1;
 	cudaLaunchConfig_t cfg{};

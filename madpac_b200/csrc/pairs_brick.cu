@@ -10,6 +10,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "brick.cuh"
 #include "md_internal.h"
@@ -140,12 +143,27 @@ __global__ void __launch_bounds__(brick::kThreads, 2)
 	}
 }
 
-// Resident grid of a kernel: the CTAs that fit on the device at once (at most `cap`).
+// Resident grid of a kernel: the CTAs that fit on the device at once (at most `cap`). The
+// occupancy query is a host call of several microseconds; its answer per (kernel, shared memory)
+// is kept, since small boxes stepped one launch at a time would otherwise pay it every step.
 template <typename K>
 int resident_grid(const Context* c, K kern, size_t smem, int cap) {
+	static std::mutex mu;
+	static std::map<std::pair<const void*, size_t>, int> known;
+	const auto key = std::make_pair(reinterpret_cast<const void*>(kern), smem);
 	int per_sm = 0;
-	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, brick::kThreads, smem) != cudaSuccess || per_sm < 1)
-		per_sm = 1;
+	{
+		std::lock_guard<std::mutex> lock(mu);
+		auto it = known.find(key);
+		if (it != known.end()) per_sm = it->second;
+	}
+	if (per_sm == 0) {
+		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, brick::kThreads, smem) != cudaSuccess ||
+		    per_sm < 1)
+			per_sm = 1;
+		std::lock_guard<std::mutex> lock(mu);
+		known[key] = per_sm;
+	}
 	return std::max(1, std::min(cap, per_sm * c->num_sms));
 }
 
