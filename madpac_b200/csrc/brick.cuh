@@ -1167,12 +1167,12 @@ __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int br
 			same |= s.same;
 		}
 	} else {
-		// rounds of up to 256 molecules; in each, warp w takes g consecutive molecules with lpm lanes
-		// each (lpm * g <= 32), so a round's last molecules are spread over every warp and no warp
-		// is left alone with a few long lists
+		// rounds of up to 256 molecules: the first as full warps of 32 (the fewest warp
+		// instructions), a later one spread over every warp, g consecutive molecules with lpm lanes
+		// each (lpm * g <= 32), so that no warp is left alone with a few long lists
 		for (int base = 0; base < n_own; base += kThreads) {
 			const int m = min(kThreads, n_own - base);
-			const int g = (m + kWarps - 1) / kWarps;
+			const int g = base == 0 ? 32 : (m + kWarps - 1) / kWarps;
 			const int lpm = lanes_per_molecule(g);
 			const int w0 = base + warp * g, w1 = min(w0 + g, base + m);
 			if (w0 < w1)
