@@ -604,17 +604,14 @@ __device__ __forceinline__ void pairs(const Const& p, const Box& bx, int brick, 
 	block_sum3_at(U, W, NP, partials, slot);
 }
 
-// build_lists keeps the hit masks of up to kBuildMasks 32-slot candidate blocks per lane in shared
-// memory and expands them in one loop (as long as the lane with the most hits, not the sum over the
-// blocks of each block's longest); the entries leave through an 8-entry ring per lane, 16 bytes at
-// a time.
-constexpr int kBuildMasks = 24;
+// Entries of each lane's write-combining ring in build_lists: up to 7 unwritten entries plus the
+// 32 that one block of candidates can add; a power of two for the index wrap.
+constexpr int kBuildRing = 64;
 
 // Shared-memory bytes of build_lists for a staged capacity s_cap.
 __host__ __device__ inline size_t build_bytes(int s_cap) {
 	return align16(sizeof(HalfPair) * (s_cap / 2 + 20)) + align16(sizeof(int) * 65) + 2 * align16(sizeof(int) * 64) +
-	       align16(sizeof(double) * 3 * 64) + sizeof(unsigned) * kBuildMasks * kThreads +
-	       sizeof(int) * kBuildMasks * kWarps + sizeof(unsigned short) * 8 * kThreads;
+	       align16(sizeof(double) * 3 * 64) + sizeof(unsigned short) * kBuildRing * kThreads;
 }
 
 // Bits [lo, hi) of a 16-bit field (0 <= lo, hi <= 16).
@@ -643,11 +640,7 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 	o += align16(sizeof(double) * 3 * 64);
 	const Grid& g = bx.g;
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-	unsigned* masks = reinterpret_cast<unsigned*>(smem + o) + tid;   // masks[k * kThreads]
-	o += sizeof(unsigned) * kBuildMasks * kThreads;
-	int* bases = reinterpret_cast<int*>(smem + o) + kBuildMasks * warp;
-	o += sizeof(int) * kBuildMasks * kWarps;
-	unsigned short* ring = reinterpret_cast<unsigned short*>(smem + o) + 8 * tid;
+	unsigned short* ring = reinterpret_cast<unsigned short*>(smem + o) + kBuildRing * tid;
 	const int bc[3] = {brick % bx.nb[0], (brick / bx.nb[0]) % bx.nb[1], brick / (bx.nb[0] * bx.nb[1])};
 	if (tid < 64) {
 		const int l[3] = {tid & 3, (tid >> 2) & 3, tid >> 4};
@@ -717,6 +710,9 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 			}
 		} else {
 			const __half2 rc2h = __float2half2_rn(bx.rc2_h);
+			// each lane's entries go through its ring in shared memory and leave it in blocks of
+			// 8 (one 16-byte store each); the rotation by lane spreads the ring writes over banks
+			const int rot = 8 * (lane & 7);
 			for (int b0 = 0; b0 < ncell; b0 += 32) {
 				const bool act = b0 + lane < ncell;
 				const int slot_i = i0 + (act ? b0 + lane : 0);
@@ -726,30 +722,7 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 				const __half2 yi2 = __half2half2(hi[2]);
 				const __half2 zi2 = __half2half2(hi[4]);
 				uint4* dst = reinterpret_cast<uint4*>(lists.nbr) + gi;
-				int cnt = 0;       // entries appended
-				int nm = 0;        // stored block masks (the same in every lane)
-				int pending = 0;   // hits in the stored masks
-				// append the hits of the stored masks in block order, 8 entries per 16-byte store
-				auto expand = [&]() {
-					__syncwarp();
-					const int iters = __reduce_max_sync(kFull, pending);
-					int k = 0;
-					unsigned m = nm > 0 ? masks[0] : 0u;
-					for (int it = 0; it < iters; it++) {
-						while (m == 0u && k + 1 < nm) m = masks[++k * kThreads];
-						if (m) {
-							const int bit = __ffs(m) - 1;
-							m &= m - 1u;
-							ring[cnt & 7] = (unsigned short) (bases[k] + 2 * (bit & 15) + (bit >> 4));
-							if ((cnt & 7) == 7 && cnt < lists.cap)
-								dst[(int64_t) (cnt >> 3) * lists.n] = *reinterpret_cast<const uint4*>(ring);
-							cnt++;
-						}
-					}
-					__syncwarp();
-					nm = 0;
-					pending = 0;
-				};
+				int cnt = 0, done = 0;   // entries found; entries written (a multiple of 8)
 				for (int r = 0; r < 9; r++) {
 					const int ky = il[1] + (r % 3) - 1, kz = il[2] + (r / 3) - 1;
 					const int k0 = (il[0] - 1) + 4 * ky + 16 * kz;
@@ -771,19 +744,26 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 						const int self = slot_i - base;
 						if (self >= 0 && self < 32) mask &= ~(1u << ((self & 1) * 16 + (self >> 1)));
 						if (!act) mask = 0u;
-						masks[nm * kThreads] = mask;
-						if (lane == 0) bases[nm] = base;
-						pending += __popc(mask);
-						if (++nm == kBuildMasks) expand();
+						while (mask) {
+							const int bit = __ffs(mask) - 1;
+							mask &= mask - 1u;
+							ring[(cnt + rot) & (kBuildRing - 1)] = (unsigned short) (base + 2 * (bit & 15) + (bit >> 4));
+							cnt++;
+						}
+						for (; done + 8 <= cnt; done += 8)
+							if (done < lists.cap)
+								dst[(int64_t) (done >> 3) * lists.n] =
+								    *reinterpret_cast<const uint4*>(ring + ((done + rot) & (kBuildRing - 1)));
 					}
 				}
-				expand();
 				if (act) {
 					// the last block of 8, padded with the list kernel's sentinel slot
-					if (cnt & 7) {
-						for (int k = cnt & 7; k < 8; k++) ring[k] = (unsigned short) lists.sentinel;
-						if (cnt < lists.cap)
-							dst[(int64_t) (cnt >> 3) * lists.n] = *reinterpret_cast<const uint4*>(ring);
+					if (cnt > done) {
+						for (int k = cnt; k < done + 8; k++)
+							ring[(k + rot) & (kBuildRing - 1)] = (unsigned short) lists.sentinel;
+						if (done < lists.cap)
+							dst[(int64_t) (done >> 3) * lists.n] =
+							    *reinterpret_cast<const uint4*>(ring + ((done + rot) & (kBuildRing - 1)));
 					}
 					lists.count[gi] = cnt <= lists.cap ? (unsigned short) cnt : kListOverflow;
 					lists.rx_ref[gi] = rx[gi];
