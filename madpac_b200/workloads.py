@@ -1,15 +1,17 @@
 """Seeded synthetic LJ systems and MarDyn's old-style phase-space format.
 
-The workloads are the five single-site Lennard-Jones systems the benchmark and the parity tests
-run (FCC lattices with Maxwell-Boltzmann velocities drawn from ``numpy.random.default_rng(seed)``,
-zero net momentum, rescaled to the exact target temperature). No public dataset is involved.
+The workloads are the single-site Lennard-Jones systems the benchmark and the parity tests run
+(FCC lattices with Maxwell-Boltzmann velocities drawn from ``numpy.random.default_rng(seed)``, zero
+net momentum, rescaled to the exact target temperature), and fluids of rigid multi-centre LJ
+molecules (the same lattices with seeded random orientations and angular momenta). No public
+dataset is involved.
 
 ``write_inp``/``read_inp`` implement the subset of MarDyn's old-style phase-space format used by
-single-site LJ components: the header of ``InputOldstyle::readPhaseSpaceHeader``
-(mardyn/io/InputOldstyle.cpp:35-261: ``Length``, ``Temperature``, ``NumberOfComponents`` with one
-LJ centre line ``x y z m eps sigma tcutoff do_shift`` per component (:162-166), the inertia line,
-the mixing coefficients ``xi eta`` for i<j (:206-215) and epsilon_RF) and the molecule section of
-``InputOldstyle::readPhaseSpace`` (:263-392) in the ``ICRV`` or ``ICRVQD`` layouts.
+LJ components: the header of ``InputOldstyle::readPhaseSpaceHeader``
+(mardyn/io/InputOldstyle.cpp:35-261: ``Length``, ``Temperature``, ``NumberOfComponents`` with the LJ
+centre lines ``x y z m eps sigma tcutoff do_shift`` of each component (:162-166), the inertia line
+(:188-195), the mixing coefficients ``xi eta`` for i<j (:206-215) and epsilon_RF) and the molecule
+section of ``InputOldstyle::readPhaseSpace`` (:263-392) in the ``ICRV`` or ``ICRVQD`` layouts.
 """
 from __future__ import annotations
 
@@ -21,13 +23,85 @@ import numpy as np
 
 
 @dataclasses.dataclass
+class Site:
+    """One LJ centre of a rigid molecule at (x, y, z) in the molecule's principal-axes frame (the
+    origin is the centre of mass, Component::addLJcenter, mardyn/molecules/Component.cpp:44-72)."""
+
+    x: float
+    y: float
+    z: float
+    mass: float
+    eps: float
+    sigma: float
+    do_shift: bool = False
+
+
+@dataclasses.dataclass
 class Component:
-    """One single-site LJ component (one LJ centre at the molecule origin)."""
+    """One LJ component: a single LJ centre at the molecule origin (eps, sigma, mass, do_shift) or,
+    with ``sites``, a rigid molecule of several LJ centres (``rigid_component``)."""
 
     eps: float = 1.0
     sigma: float = 1.0
     mass: float = 1.0
     do_shift: bool = False
+    sites: Optional[List[Site]] = None
+    inertia: Optional[Sequence[float]] = None   # the header's inertia line; values > 0 replace the moments
+
+    def lj_centres(self) -> List[Site]:
+        if self.sites is not None:
+            return list(self.sites)
+        return [Site(0.0, 0.0, 0.0, self.mass, self.eps, self.sigma, self.do_shift)]
+
+    def moments(self) -> np.ndarray:
+        """Principal moments I11, I22, I33: sum m (y^2+z^2), sum m (x^2+z^2), sum m (x^2+y^2) over the
+        centres, each replaced by the header's value where that is > 0 (InputOldstyle.cpp:188-195)."""
+        I = np.zeros(3)
+        for c in self.lj_centres():
+            I[0] += c.mass * (c.y * c.y + c.z * c.z)
+            I[1] += c.mass * (c.x * c.x + c.z * c.z)
+            I[2] += c.mass * (c.x * c.x + c.y * c.y)
+        if self.inertia is not None:
+            for d in range(3):
+                if self.inertia[d] > 0.0:
+                    I[d] = float(self.inertia[d])
+        return I
+
+    @property
+    def is_rigid(self) -> bool:
+        return self.sites is not None
+
+
+def rigid_component(sites: Sequence[Site], inertia: Optional[Sequence[float]] = None) -> Component:
+    """A rigid multi-centre component; its mass is the sum of the centres' masses."""
+    sites = list(sites)
+    return Component(sites[0].eps, sites[0].sigma, float(sum(c.mass for c in sites)), sites[0].do_shift,
+                     sites=sites, inertia=None if inertia is None else list(inertia))
+
+
+def two_centre(elongation: float = 0.5, eps: float = 1.0, sigma: float = 1.0, mass: float = 1.0,
+               do_shift: bool = True) -> Component:
+    """A two-centre LJ molecule (2CLJ): equal centres at z = +-elongation/2, half the mass each."""
+    h = 0.5 * elongation
+    return rigid_component([Site(0.0, 0.0, -h, 0.5 * mass, eps, sigma, do_shift),
+                            Site(0.0, 0.0, h, 0.5 * mass, eps, sigma, do_shift)])
+
+
+def three_centre_linear() -> Component:
+    """A linear three-centre molecule with a different middle centre (CO2-like proportions in LJ
+    units): middle (eps 0.6, sigma 0.9, m 0.4) at the origin, ends (eps 1.0, sigma 1.05, m 0.3) at
+    z = +-0.6; truncated-shifted."""
+    return rigid_component([Site(0.0, 0.0, 0.0, 0.4, 0.6, 0.9, True),
+                            Site(0.0, 0.0, -0.6, 0.3, 1.0, 1.05, True),
+                            Site(0.0, 0.0, 0.6, 0.3, 1.0, 1.05, True)])
+
+
+def bent_three_centre() -> Component:
+    """A bent three-centre molecule with three non-zero principal moments (centre of mass at the
+    origin, principal axes along x, y, z), plain truncated LJ."""
+    return rigid_component([Site(0.0, 0.0, 0.3, 0.5, 0.9, 1.0, False),
+                            Site(0.45, 0.0, -0.3, 0.25, 1.1, 0.95, False),
+                            Site(-0.45, 0.0, -0.3, 0.25, 1.1, 0.95, False)])
 
 
 @dataclasses.dataclass
@@ -47,10 +121,16 @@ class System:
     dt: float = 0.002                  # timestepLength
     nve: bool = True
     name: str = "system"
+    q: Optional[np.ndarray] = None     # (N, 4) orientation quaternions (w, x, y, z) of rigid molecules
+    D: Optional[np.ndarray] = None     # (N, 3) angular momenta (space frame) of rigid molecules
 
     @property
     def n(self) -> int:
         return int(self.ids.shape[0])
+
+    @property
+    def is_rigid(self) -> bool:
+        return any(c.is_rigid for c in self.components)
 
     def eps(self) -> np.ndarray:
         return np.array([c.eps for c in self.components], dtype=np.float64)
@@ -195,6 +275,53 @@ def config_c4(seed: int = 4, n_boxes: int = 512) -> List[System]:
     return out
 
 
+def rotate_inv(q: np.ndarray, d: np.ndarray) -> np.ndarray:
+    """Body frame -> space frame for unit quaternions q (N, 4) = (w, x, y, z) and vectors d (N, 3):
+    the matrix of Quaternion::rotateinv (mardyn/molecules/Quaternion.cpp:50-66), used here only to
+    draw space-frame angular momenta."""
+    w, x, y, z = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    ww, xx, yy, zz = w * w, x * x, y * y, z * z
+    xy, zw, xz, yw, yz, xw = x * y, z * w, x * z, y * w, y * z, x * w
+    out = np.empty_like(d)
+    out[:, 0] = (ww + xx - yy - zz) * d[:, 0] + 2.0 * (xy - zw) * d[:, 1] + 2.0 * (xz + yw) * d[:, 2]
+    out[:, 1] = 2.0 * (xy + zw) * d[:, 0] + (ww - xx + yy - zz) * d[:, 1] + 2.0 * (yz - xw) * d[:, 2]
+    out[:, 2] = 2.0 * (xz - yw) * d[:, 0] + 2.0 * (yz + xw) * d[:, 1] + (ww - xx - yy + zz) * d[:, 2]
+    return out
+
+
+def rigid_fcc_box(n_cells: int, density: float, temperature: float, seed: int, cutoff: float,
+                  components: List[Component], fractions: Optional[Sequence[float]] = None,
+                  mix: Optional[np.ndarray] = None, dt: float = 0.002, nve: bool = True,
+                  n_atoms: Optional[int] = None, name: str = "rigid") -> System:
+    """A fluid start of rigid multi-centre molecules: the molecule centres on the FCC lattice of
+    ``lj_fcc_box`` (density counts molecules), seeded uniformly random orientations, and angular
+    momenta whose body-frame angular velocities are Maxwell-Boltzmann about every axis with a
+    non-zero moment, scaled so that sum I w^2 equals rotDOF * T (the rotational part of the
+    reference's temperature, Domain.cpp:244-246)."""
+    s = lj_fcc_box(n_cells, density, temperature, seed, cutoff, components, fractions, mix, dt, nve, n_atoms, name)
+    rng = np.random.default_rng(seed + 7919)
+    n = s.n
+    q = rng.standard_normal((n, 4))
+    q /= np.linalg.norm(q, axis=1)[:, None]
+    I = np.stack([c.moments() for c in components])[s.cid]
+    has = I > 0.0
+    w = np.where(has, rng.standard_normal((n, 3)) * np.sqrt(temperature / np.where(has, I, 1.0)), 0.0)
+    sum_iw2 = float((I * w * w).sum())
+    rot_dof = int(has.sum())
+    if sum_iw2 > 0.0:
+        w *= math.sqrt(rot_dof * temperature / sum_iw2)
+    s.q = q
+    s.D = rotate_inv(q, I * w)
+    return s
+
+
+def config_2clj(seed: int = 6, n_cells: int = 40, density: float = 0.3, temperature: float = 2.0,
+                cutoff: float = 3.0) -> System:
+    """A two-centre LJ fluid (elongation 0.5, truncated-shifted, cutoff 3.0 on the molecule centres):
+    4 n_cells^3 molecules (256,000 at the default) at molecular density 0.3 and T = 2.0."""
+    return rigid_fcc_box(n_cells, density, temperature, seed, cutoff, [two_centre()], name=f"2clj_{4 * n_cells ** 3}")
+
+
 def config_c5(seed: int = 5) -> System:
     """16,384-atom two-species FCC box (A/B 50/50 of the slab species), rho=0.8, T=1.0, rc=2.5."""
     return lj_fcc_box(16, 0.8, 1.0, seed, 2.5, two_species(), [0.5, 0.5], np.ones((1, 2)), name="c5_16k")
@@ -202,17 +329,25 @@ def config_c5(seed: int = 5) -> System:
 
 # ----------------------------------------------------------------------------- file format
 
-def write_inp(sys_: System, path: str, fmt: str = "ICRV") -> None:
-    """Write the old-style phase-space file (header + molecules, component ids 1-based)."""
+def write_inp(sys_: System, path: str, fmt: Optional[str] = None) -> None:
+    """Write the old-style phase-space file (header + molecules, component ids 1-based). The molecule
+    layout defaults to ICRVQD for rigid molecules (orientations and angular momenta) and ICRV
+    otherwise."""
+    if fmt is None:
+        fmt = "ICRVQD" if sys_.is_rigid else "ICRV"
     nc = len(sys_.components)
     lines = ["mardyn trunk 20090721", "currentTime 0.0",
              f"Temperature {float(sys_.temperature)!r}",
              "Length {!r} {!r} {!r}".format(*[float(x) for x in sys_.length]),
              f"NumberOfComponents {nc}"]
     for c in sys_.components:
-        lines.append("1 0 0 0 0")
-        lines.append(f"0.0 0.0 0.0 {float(c.mass)!r} {float(c.eps)!r} {float(c.sigma)!r} {float(sys_.lj_cutoff)!r} {1 if c.do_shift else 0}")
-        lines.append("0.0 0.0 0.0")
+        centres = c.lj_centres()
+        lines.append(f"{len(centres)} 0 0 0 0")
+        for t in centres:
+            lines.append(f"{float(t.x)!r} {float(t.y)!r} {float(t.z)!r} {float(t.mass)!r} {float(t.eps)!r} "
+                         f"{float(t.sigma)!r} {float(sys_.lj_cutoff)!r} {1 if t.do_shift else 0}")
+        inertia = [0.0, 0.0, 0.0] if c.inertia is None else [float(x) for x in c.inertia]
+        lines.append("{!r} {!r} {!r}".format(*inertia))
     k = 0
     for i in range(nc):
         for j in range(i + 1, nc):
@@ -231,9 +366,9 @@ def write_inp(sys_: System, path: str, fmt: str = "ICRV") -> None:
             np.savetxt(f, body, fmt=["%d", "%d"] + ["%.17g"] * 6)
         elif fmt == "ICRVQD":
             n = sys_.n
-            extra = np.column_stack([np.ones(n), np.zeros(n), np.zeros(n), np.zeros(n),
-                                     np.zeros(n), np.zeros(n), np.zeros(n)])
-            body = np.column_stack(cols + [extra])
+            q = sys_.q if sys_.q is not None else np.tile([1.0, 0.0, 0.0, 0.0], (n, 1))
+            D = sys_.D if sys_.D is not None else np.zeros((n, 3))
+            body = np.column_stack(cols + [q, D])
             np.savetxt(f, body, fmt=["%d", "%d"] + ["%.17g"] * 13)
         else:
             raise ValueError(f"unsupported molecule format {fmt}")
@@ -271,13 +406,18 @@ def read_inp(path: str) -> System:
             nc = int(nxt())
             for _ in range(nc):
                 nlj, nq, nd, nqq, nt = (int(nxt()) for _ in range(5))
-                if nlj != 1 or nq or nd or nqq or nt:
-                    raise ValueError("only single-site LJ components are supported")
-                x, y, z, m, eps, sig, tcut, shift = (float(nxt()) for _ in range(8))
-                if x or y or z:
-                    raise ValueError("the LJ centre must sit at the molecule origin")
-                comps.append(Component(eps, sig, m, shift != 0))
-                nxt(); nxt(); nxt()
+                if nlj < 1 or nq or nd or nqq or nt:
+                    raise ValueError("only LJ components are supported")
+                centres = []
+                for _ in range(nlj):
+                    x, y, z, m, eps, sig, tcut, shift = (float(nxt()) for _ in range(8))
+                    centres.append(Site(x, y, z, m, eps, sig, shift != 0))
+                inertia = [float(nxt()) for _ in range(3)]
+                if nlj == 1 and not (centres[0].x or centres[0].y or centres[0].z) and not any(inertia):
+                    t = centres[0]
+                    comps.append(Component(t.eps, t.sigma, t.mass, t.do_shift))
+                else:
+                    comps.append(rigid_component(centres, inertia if any(inertia) else None))
             for i in range(nc):
                 for j in range(i + 1, nc):
                     mix.append((float(nxt()), float(nxt())))
@@ -299,11 +439,17 @@ def read_inp(path: str) -> System:
         ids, cid, r, v = body[:, 0], np.ones(n), body[:, 1:4], body[:, 4:7]
     else:
         ids, cid, r, v = body[:, 0], body[:, 1], body[:, 2:5], body[:, 5:8]
+    q = D = None
+    if fmt == "ICRVQD":
+        q, D = body[:, 8:12].copy(), body[:, 12:15].copy()
+    elif fmt == "ICRVFQDM":
+        q, D = body[:, 11:15].copy(), body[:, 15:18].copy()
     nc = len(comps)
+    rigid = any(c.is_rigid for c in comps)
     return System(length=length, components=comps,
                   mix=np.array(mix, dtype=np.float64).reshape(nc * (nc - 1) // 2, 2),
                   ids=ids.astype(np.uint64), cid=(cid.astype(np.int32) - 1), r=r.copy(), v=v.copy(),
-                  temperature=temperature, name=path)
+                  temperature=temperature, name=path, q=q if rigid else None, D=D if rigid else None)
 
 
 def write_cfg(sys_: System, cfg_path: str, inp_name: str) -> None:

@@ -214,7 +214,15 @@ def read_ref_dump(path: str) -> Dict[str, np.ndarray]:
         v = np.frombuffer(f.read(24 * n), dtype=np.float64).reshape(n, 3)
         F = np.frombuffer(f.read(24 * n), dtype=np.float64).reshape(n, 3)
         cell = np.frombuffer(f.read(8 * n), dtype=np.int64)
-    return dict(id=ids, cid=cid.astype(np.int32), r=r, v=v, F=F, cell=cell)
+    out = dict(id=ids, cid=cid.astype(np.int32), r=r, v=v, F=F, cell=cell)
+    rot = path[:-4] + ".rot.bin"
+    if os.path.exists(rot):
+        with open(rot, "rb") as f:
+            m = int(np.frombuffer(f.read(8), dtype=np.int64)[0])
+            out["q"] = np.frombuffer(f.read(32 * m), dtype=np.float64).reshape(m, 4)
+            out["D"] = np.frombuffer(f.read(24 * m), dtype=np.float64).reshape(m, 3)
+            out["M"] = np.frombuffer(f.read(24 * m), dtype=np.float64).reshape(m, 3)
+    return out
 
 
 def run_reference(system, nsteps: int, dump_steps=(), workdir: Optional[str] = None) -> Dict:
@@ -235,5 +243,8 @@ def run_reference(system, nsteps: int, dump_steps=(), workdir: Optional[str] = N
             p = line.split()
             scal.append(dict(step=int(p[0]), upot=float(p[1]), virial=float(p[2]), summv2=float(p[3]),
                              n=int(p[4])))
+    with open(os.path.join(tmp, "rot.txt")) as f:
+        for rec, line in zip(scal, f):
+            rec["sum_iw2"] = float(line.split()[1])
     dumps = {s: read_ref_dump(os.path.join(tmp, f"step{s:06d}.bin")) for s in dump_steps}
     return dict(scalars=scal, dumps=dumps, workdir=tmp)

@@ -7,7 +7,9 @@
 //     stored in Domain (mardyn/particleContainer/adapter/ParticlePairs2PotForceAdapter.h:64-67),
 //   * sum m v^2 over the molecules,
 // and, for the steps named on the command line, every molecule's id, component, r, v, F and
-// LinkedCells cell index (LinkedCells::getCellIndexOfMolecule, LinkedCells.cpp:535-547).
+// LinkedCells cell index (LinkedCells::getCellIndexOfMolecule, LinkedCells.cpp:535-547), and in a
+// second file its orientation q, angular momentum D and torque M (Molecule::q/D/M,
+// molecules/Molecule.h:85-89); rot.txt holds sum I w^2 per step (Molecule::calculate_mv2_Iw2).
 //
 // The reference never prints per-molecule forces, so this harness exists only to pin the
 // oracle and the GPU path against the reference itself. It is test infrastructure.
@@ -54,6 +56,7 @@ struct Rec {
 	long cid;
 	double r[3], v[3], F[3];
 	long cell;
+	double q[4], D[3], M[3];
 };
 
 }  // namespace
@@ -74,6 +77,13 @@ public:
 		        _moleculeContainer->getNumberOfParticles());
 	}
 
+	void writeRot(FILE* f, long step) {
+		double mv2 = 0.0, iw2 = 0.0;
+		for (Molecule* m = _moleculeContainer->begin(); m != _moleculeContainer->end(); m = _moleculeContainer->next())
+			m->calculate_mv2_Iw2(mv2, iw2);
+		fprintf(f, "%ld %.17g\n", step, iw2);
+	}
+
 	void writeArrays(const std::string& outdir, long step) {
 		LinkedCells* lc = dynamic_cast<LinkedCells*>(_moleculeContainer);
 		std::vector<Rec> recs;
@@ -87,6 +97,14 @@ public:
 				r.F[d] = m->F(d);
 			}
 			r.cell = lc ? (long) lc->getCellIndexOfMolecule(m) : -1;
+			r.q[0] = m->q().qw();
+			r.q[1] = m->q().qx();
+			r.q[2] = m->q().qy();
+			r.q[3] = m->q().qz();
+			for (int d = 0; d < 3; d++) {
+				r.D[d] = m->D(d);
+				r.M[d] = m->M(d);
+			}
 			recs.push_back(r);
 		}
 		std::sort(recs.begin(), recs.end(), [](const Rec& a, const Rec& b) { return a.id < b.id; });
@@ -106,13 +124,27 @@ public:
 		for (const Rec& r : recs) fwrite(r.F, sizeof(double), 3, f);
 		for (const Rec& r : recs) fwrite(&r.cell, sizeof(long), 1, f);
 		fclose(f);
+		snprintf(name, sizeof(name), "%s/step%06ld.rot.bin", outdir.c_str(), step);
+		f = fopen(name, "wb");
+		if (!f) {
+			fprintf(stderr, "cannot open %s\n", name);
+			std::exit(2);
+		}
+		fwrite(&n, sizeof(long), 1, f);
+		for (const Rec& r : recs) fwrite(r.q, sizeof(double), 4, f);
+		for (const Rec& r : recs) fwrite(r.D, sizeof(double), 3, f);
+		for (const Rec& r : recs) fwrite(r.M, sizeof(double), 3, f);
+		fclose(f);
 	}
 
 	void run(unsigned long nsteps, const std::string& outdir, const std::set<long>& dumps) {
 		std::string sname = outdir + "/scalars.txt";
 		FILE* sf = fopen(sname.c_str(), "w");
+		std::string rname = outdir + "/rot.txt";
+		FILE* rf = fopen(rname.c_str(), "w");
 		prepare_start();
 		writeScalars(sf, 0);
+		writeRot(rf, 0);
 		if (dumps.count(0)) writeArrays(outdir, 0);
 		// Simulation::simulate runs _simstep = _initSimulation .. _numberOfTimesteps inclusive;
 		// simulateStart sets _initSimulation (Simulation.cpp:1011), so it comes first.
@@ -122,9 +154,11 @@ public:
 		for (_simstep = _initSimulation; _simstep <= _numberOfTimesteps; k++) {
 			simulateStep();
 			writeScalars(sf, k);
+			writeRot(rf, k);
 			if (dumps.count(k)) writeArrays(outdir, k);
 		}
 		fclose(sf);
+		fclose(rf);
 	}
 
 	// nsteps steps, then the reference's own checkpoint (Domain::writeCheckpoint, Domain.cpp:462-568)

@@ -1,0 +1,63 @@
+"""Generate the rigid multi-centre fixtures in this folder with the reference MarDyn itself.
+
+oracle/_ref/ref_driver (the reference sources compiled unmodified, see oracle/Makefile, target
+`ref`) runs 10 steps of three seeded systems of rigid LJ molecules and dumps, after prepare_start
+and after step 10, every molecule's r, v, F and its orientation q, angular momentum D and torque M,
+with the potential energy, virial, sum m v^2 and sum I w^2 of every step. Kept here as
+rigid_<name>.npz (the start state is stored too, so the fixtures do not depend on the generator):
+
+* rigid_2clj_256:  two-centre LJ (elongation 0.5, truncated-shifted), rho 0.3, T 2.0, rc 3.0;
+* rigid_mix_256:   that molecule and a linear three-centre molecule with a different middle centre,
+                   50/50, xi 0.9, eta 1.05, rho 0.15, T 2.0, rc 3.0;
+* rigid_bent_256:  a bent three-centre molecule with three non-zero moments, plain LJ, rho 0.25,
+                   T 1.5, rc 2.5.
+
+Run from the repository root:
+
+    make -C oracle ref && python tests/golden/make_rigid_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from madpac_b200 import workloads as W  # noqa: E402
+import oracle as O  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+NSTEPS = 10
+
+
+def systems():
+    return [
+        W.rigid_fcc_box(4, 0.3, 2.0, 11, 3.0, [W.two_centre()], name="rigid_2clj_256"),
+        W.rigid_fcc_box(4, 0.15, 2.0, 12, 3.0, [W.two_centre(), W.three_centre_linear()], [0.5, 0.5],
+                        np.array([[0.9, 1.05]]), name="rigid_mix_256"),
+        W.rigid_fcc_box(4, 0.25, 1.5, 13, 2.5, [W.bent_three_centre()], name="rigid_bent_256"),
+    ]
+
+
+def main():
+    if not os.path.exists(O.REF_DRIVER):
+        raise SystemExit("build the reference harness first: make -C oracle ref")
+    for s in systems():
+        out = O.run_reference(s, NSTEPS, (0, NSTEPS))
+        d0, d1 = out["dumps"][0], out["dumps"][NSTEPS]
+        sc = out["scalars"]
+        np.savez_compressed(
+            os.path.join(OUT, f"{s.name}.npz"),
+            length=s.length, cutoff=s.cutoff, lj_cutoff=s.lj_cutoff, dt=s.dt, mix=s.mix,
+            ids=s.ids, cid=s.cid, r=s.r, v=s.v, q=s.q, D=s.D,
+            F0=d0["F"], M0=d0["M"],
+            r1=d1["r"], v1=d1["v"], q1=d1["q"], D1=d1["D"], F1=d1["F"], M1=d1["M"],
+            upot=np.array([x["upot"] for x in sc]), virial=np.array([x["virial"] for x in sc]),
+            summv2=np.array([x["summv2"] for x in sc]), sum_iw2=np.array([x["sum_iw2"] for x in sc]))
+        print("wrote", f"{s.name}.npz")
+
+
+if __name__ == "__main__":
+    main()
