@@ -243,6 +243,64 @@ int mdgpu_batch_set_barrier_timeout(mdgpu_batch* b, int64_t ns);
 int mdgpu_batch_set_skin(mdgpu_batch* b, double skin);
 int mdgpu_batch_skin_builds(const mdgpu_batch* b, int64_t* builds);
 
+/* ---- rigid multi-centre LJ molecules ------------------------------------------------------
+ * Molecules of several LJ centres with orientation q (quaternion w, x, y, z), angular momentum D
+ * (space frame) and torque M. Replaces, for such components, the same LinkedCells / pair handler /
+ * Leapfrog sequence as the single-centre context: PotForce's loop over centre pairs
+ * (molecules/potforce.h:319-363), Molecule::upd_cache and calcFM (molecules/Molecule.cpp:161-190,
+ * 386-411), and the rotational half of Molecule::upd_preF / upd_postF (Molecule.cpp:128-159,
+ * 193-216). Arrays in the caller's order: r, v, F, D, M are (n, 3), q is (n, 4). */
+#define MDGPU_MAX_SITES 6         /* LJ centres per component */
+#define MDGPU_MAX_SITE_TOTAL 16   /* LJ centres over all components */
+
+/* One LJ centre at r (principal-axes frame, the origin at the centre of mass), as read by
+ * InputOldstyle (io/InputOldstyle.cpp:162-166) and added by Component::addLJcenter
+ * (molecules/Component.cpp:44-72); the shift uses LJCutoffRadius as the centre's cutoff. */
+typedef struct mdgpu_site {
+	double r[3];
+	double mass;
+	double eps;
+	double sigma;
+	int do_shift;
+} mdgpu_site;
+
+typedef struct mdgpu_rigid mdgpu_rigid;
+
+/* nsites[c] centres for each component c, listed one component after another in `sites`;
+ * inertia: 3 per component or NULL, values > 0 replace the principal moments computed from the
+ * centres (the header's inertia line, InputOldstyle.cpp:188-195). Other arguments as mdgpu_create.
+ * On failure *out may still be set (read mdgpu_rigid_last_error, then destroy it). */
+int mdgpu_rigid_create(mdgpu_rigid** out, const double length[3], double cutoff, double lj_cutoff,
+                       double cells_in_cutoff, int ncomp, const int32_t* nsites, const mdgpu_site* sites,
+                       const double* inertia, const double* mix, int precision, int device);
+int mdgpu_rigid_destroy(mdgpu_rigid* h);
+const char* mdgpu_rigid_last_error(const mdgpu_rigid* h);
+int mdgpu_rigid_set_precision(mdgpu_rigid* h, int precision);
+/* Total mass and principal moments of component comp (Component::m, I11/I22/I33). */
+int mdgpu_rigid_get_inertia(const mdgpu_rigid* h, int32_t comp, double* mass, double I[3]);
+/* Loads the molecules (q and D required); forces and torques start at zero. */
+int mdgpu_rigid_set_particles(mdgpu_rigid* h, int64_t n, const uint64_t* id, const int32_t* cid, const double* r,
+                              const double* v, const double* q, const double* D);
+/* Any output pointer may be NULL. */
+int mdgpu_rigid_get_particles(mdgpu_rigid* h, int64_t n, uint64_t* id, int32_t* cid, double* r, double* v, double* F,
+                              double* q, double* D, double* M);
+/* LinkedCells::update of the molecule centres (with the periodic wrap). */
+int mdgpu_rigid_update(mdgpu_rigid* h);
+/* Molecule::upd_cache for all molecules, LinkedCells::traversePairs with the LJ centre loop, and
+ * Molecule::calcFM: F and M of every molecule, Upot = Upot6LJ/6, the virial sum drm.f and the
+ * number of molecule pairs within the cutoff. */
+int mdgpu_rigid_traverse_pairs(mdgpu_rigid* h, double* upot, double* virial, double* npairs);
+/* Molecule::upd_preF(dt, vcorr, Dcorr) for all molecules (Leapfrog::transition1to2). */
+int mdgpu_rigid_leapfrog_pre(mdgpu_rigid* h, double dt, double vcorr, double Dcorr);
+/* Molecule::upd_postF(dt_half) for all molecules (Leapfrog::transition2to3): sum m v^2, sum I w^2. */
+int mdgpu_rigid_leapfrog_post(mdgpu_rigid* h, double dt_half, double* summv2, double* sum_iw2);
+/* nsteps NVE steps of Simulation::simulateStep (after the forces of the start are in place);
+ * per_step (may be NULL): 5 doubles per step {Upot, virial, sum m v^2, sum I w^2, pairs}. */
+int mdgpu_rigid_run(mdgpu_rigid* h, int32_t nsteps, double dt, double* per_step);
+int mdgpu_rigid_get_stream(const mdgpu_rigid* h, void** stream);
+/* Kernel launches enqueued by the context so far. */
+int mdgpu_rigid_profile(mdgpu_rigid* h, int64_t* launches);
+
 #ifdef __cplusplus
 }
 #endif

@@ -191,6 +191,12 @@ Extra* extra(Context* c);
 
 void count_launches(Context* c, int launches) { c->prof_count[3] += launches; }
 
+int check_device_status(Context* c) { return check_status(c); }
+
+int set_error(Context* c, int code, const std::string& msg) { return fail(c, code, msg); }
+
+int set_cuda_error(Context* c, cudaError_t e, const char* where) { return cuda_fail(c, e, where); }
+
 void prof_begin(Context* c, int group) {
 	if (!c->profiling) return;
 	Extra* x = extra(c);

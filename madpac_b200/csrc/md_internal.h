@@ -171,6 +171,12 @@ int setup_species(int ncomp, const mdgpu_component* comps, const double* mix, do
                   std::string& err);
 PairParams pair_params(const Species& sp, double rc, double rc_lj);
 
+// Status helpers of api.cu for the other entry-point files: read and clear the device status word
+// (synchronises the stream) and map it to an MDGPU_* code; record an error message.
+int check_device_status(Context* c);
+int set_error(Context* c, int code, const std::string& msg);
+int set_cuda_error(Context* c, cudaError_t e, const char* where);
+
 // Timing brackets around a group of launches (0 = binning, 1 = pairs, 2 = integration).
 void prof_begin(Context* c, int group);
 void prof_end(Context* c, int group, int launches);

@@ -1,0 +1,859 @@
+// Rigid multi-centre LJ molecules: the container, pair handler and Leapfrog of MarDyn for molecules
+// of several LJ centres (paths relative to madpac/mardyn/).
+//
+// A rigid context wraps a single-box context for what does not depend on the molecules' shape: the
+// particle arrays, the LinkedCells binning and cell sort of the molecule centres (launch_bin, the
+// periodic wrap of DomainDecompDummy::exchangeMolecules), and the status word. What the centres add
+// lives here:
+//
+// * orientation q (4), angular momentum D (3, space frame) and torque M (3) of every molecule, kept
+//   in the caller's order (index uidx of the sorted arrays), so the cell sort never moves them;
+// * k_rigid_sites: Molecule::upd_cache (molecules/Molecule.cpp:161-190): each centre's offset
+//   d = q.rotateinv(site) (Quaternion.cpp:50-66) once per force evaluation, stored per sorted
+//   molecule, centre-major (d[(s*3 + k)*n + i]);
+// * k_rigid_pairs: the LJ block of PotForce (molecules/potforce.h:319-363) for every molecule pair
+//   whose centres are closer than rc (strict, particleContainer/BlockTraverse.cpp:155), every centre
+//   pair evaluated when dd < rcLJ^2: drs = (drm + d_i) - d_j (SiteSiteDistance, potforce.h:26-31),
+//   PotForceLJ (potforce.h:41-53), u += shift6, Upot6LJ += u, Virial += drm.f; the molecule's force
+//   is the sum of its centres' forces and its torque M = sum d x f (Molecule::calcFM,
+//   Molecule.cpp:386-411). One thread per molecule gathers over the 27 cells around it (each pair
+//   seen from both sides, halved at the end: no atomics, the same sums run to run), the site-pair
+//   parameters of Comp2Param::initialize (molecules/Comp2Param.cpp:28-115) in shared memory;
+// * k_rigid_pre / k_rigid_post: Molecule::upd_preF and upd_postF (Molecule.cpp:128-159, 193-216)
+//   with the quaternion algebra of Quaternion.cpp (rotate, differentiate, normalisation) and the
+//   sums m v^2 and I w^2 of Leapfrog::transition2to3 (integrators/Leapfrog.cpp:52-99).
+//
+// MDGPU_FP64 evaluates everything in double with the reference's operation order and no
+// contraction; MDGPU_MIXED evaluates each centre pair's LJ terms in float from the double site
+// distance and accumulates forces, torques, energy and virial in double.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "md_internal.h"
+#include "reduce.cuh"
+
+namespace mdgpu {
+
+constexpr int kMaxSites = MDGPU_MAX_SITES;            // LJ centres per component
+constexpr int kMaxSiteTotal = MDGPU_MAX_SITE_TOTAL;   // LJ centres over all components
+constexpr int kRigidThreads = kReduceBlock;
+
+// Site tables of a rigid context (device copy read by the kernels).
+struct RigidParams {
+	int nc, nsite_total, ns_max;
+	int nsites[kMaxSpecies];
+	int base[kMaxSpecies];                 // first centre of component c in the site tables
+	double site[kMaxSiteTotal][3];         // body-frame centre positions
+	double mass[kMaxSpecies];
+	double I[kMaxSpecies][3], invI[kMaxSpecies][3];
+	double rc2, rclj2;
+	// Comp2Param stream entries per ordered pair of centres (a, b), index a * kMaxSiteTotal + b
+	double eps24[kMaxSiteTotal * kMaxSiteTotal];
+	double sig2[kMaxSiteTotal * kMaxSiteTotal];
+	double shift6[kMaxSiteTotal * kMaxSiteTotal];
+};
+
+namespace {
+
+inline int64_t nblocks(int64_t n) { return (n + kRigidThreads - 1) / kRigidThreads; }
+
+// ---- quaternion algebra (Quaternion.cpp), in double without contraction -------------------------
+
+struct Quat {
+	double w, x, y, z;
+};
+
+// Quaternion::rotate: space frame -> body frame
+__device__ __forceinline__ void q_rotate(const Quat& q, const double d[3], double out[3]) {
+	const double ww = __dmul_rn(q.w, q.w), xx = __dmul_rn(q.x, q.x), yy = __dmul_rn(q.y, q.y),
+	             zz = __dmul_rn(q.z, q.z);
+	const double xy = __dmul_rn(q.x, q.y), zw = __dmul_rn(q.z, q.w), xz = __dmul_rn(q.x, q.z),
+	             yw = __dmul_rn(q.y, q.w);
+	out[0] = __dadd_rn(__dadd_rn(__dmul_rn(__dsub_rn(__dsub_rn(__dadd_rn(ww, xx), yy), zz), d[0]),
+	                             __dmul_rn(__dmul_rn(2., __dadd_rn(xy, zw)), d[1])),
+	                   __dmul_rn(__dmul_rn(2., __dsub_rn(xz, yw)), d[2]));
+	const double yz = __dmul_rn(q.y, q.z), xw = __dmul_rn(q.x, q.w);
+	out[1] = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(2., __dsub_rn(xy, zw)), d[0]),
+	                             __dmul_rn(__dsub_rn(__dadd_rn(__dsub_rn(ww, xx), yy), zz), d[1])),
+	                   __dmul_rn(__dmul_rn(2., __dadd_rn(yz, xw)), d[2]));
+	out[2] = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(2., __dadd_rn(xz, yw)), d[0]),
+	                             __dmul_rn(__dmul_rn(2., __dsub_rn(yz, xw)), d[1])),
+	                   __dmul_rn(__dadd_rn(__dsub_rn(__dsub_rn(ww, xx), yy), zz), d[2]));
+}
+
+// Quaternion::rotateinv: body frame -> space frame
+__device__ __forceinline__ void q_rotate_inv(const Quat& q, const double d[3], double out[3]) {
+	const double ww = __dmul_rn(q.w, q.w), xx = __dmul_rn(q.x, q.x), yy = __dmul_rn(q.y, q.y),
+	             zz = __dmul_rn(q.z, q.z);
+	const double xy = __dmul_rn(q.x, q.y), zw = __dmul_rn(q.z, q.w), xz = __dmul_rn(q.x, q.z),
+	             yw = __dmul_rn(q.y, q.w);
+	out[0] = __dadd_rn(__dadd_rn(__dmul_rn(__dsub_rn(__dsub_rn(__dadd_rn(ww, xx), yy), zz), d[0]),
+	                             __dmul_rn(__dmul_rn(2., __dsub_rn(xy, zw)), d[1])),
+	                   __dmul_rn(__dmul_rn(2., __dadd_rn(xz, yw)), d[2]));
+	const double yz = __dmul_rn(q.y, q.z), xw = __dmul_rn(q.x, q.w);
+	out[1] = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(2., __dadd_rn(xy, zw)), d[0]),
+	                             __dmul_rn(__dsub_rn(__dadd_rn(__dsub_rn(ww, xx), yy), zz), d[1])),
+	                   __dmul_rn(__dmul_rn(2., __dsub_rn(yz, xw)), d[2]));
+	out[2] = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(2., __dsub_rn(xz, yw)), d[0]),
+	                             __dmul_rn(__dmul_rn(2., __dadd_rn(yz, xw)), d[1])),
+	                   __dmul_rn(__dadd_rn(__dsub_rn(__dsub_rn(ww, xx), yy), zz), d[2]));
+}
+
+// Quaternion::differentiate: dq/dt for the body angular velocity w
+__device__ __forceinline__ Quat q_differentiate(const Quat& q, const double w[3]) {
+	Quat r;
+	r.w = __dmul_rn(.5, __dsub_rn(__dsub_rn(__dmul_rn(-q.x, w[0]), __dmul_rn(q.y, w[1])), __dmul_rn(q.z, w[2])));
+	r.x = __dmul_rn(.5, __dadd_rn(__dsub_rn(__dmul_rn(q.w, w[0]), __dmul_rn(q.z, w[1])), __dmul_rn(q.y, w[2])));
+	r.y = __dmul_rn(.5, __dsub_rn(__dadd_rn(__dmul_rn(q.z, w[0]), __dmul_rn(q.w, w[1])), __dmul_rn(q.x, w[2])));
+	r.z = __dmul_rn(.5, __dadd_rn(__dadd_rn(__dmul_rn(-q.y, w[0]), __dmul_rn(q.x, w[1])), __dmul_rn(q.w, w[2])));
+	return r;
+}
+
+__device__ __forceinline__ double q_magnitude2(const Quat& q) {
+	return __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(q.w, q.w), __dmul_rn(q.x, q.x)), __dmul_rn(q.y, q.y)),
+	                 __dmul_rn(q.z, q.z));
+}
+
+__device__ __forceinline__ Quat q_scale(Quat q, double s) {
+	q.w = __dmul_rn(q.w, s);
+	q.x = __dmul_rn(q.x, s);
+	q.y = __dmul_rn(q.y, s);
+	q.z = __dmul_rn(q.z, s);
+	return q;
+}
+
+__device__ __forceinline__ Quat q_add(Quat a, const Quat& b) {
+	a.w = __dadd_rn(a.w, b.w);
+	a.x = __dadd_rn(a.x, b.x);
+	a.y = __dadd_rn(a.y, b.y);
+	a.z = __dadd_rn(a.z, b.z);
+	return a;
+}
+
+__device__ __forceinline__ Quat load_q(const double* q, int64_t n, int64_t u) {
+	return Quat{q[u], q[n + u], q[2 * n + u], q[3 * n + u]};
+}
+
+__device__ __forceinline__ void store_q(double* q, int64_t n, int64_t u, const Quat& v) {
+	q[u] = v.w;
+	q[n + u] = v.x;
+	q[2 * n + u] = v.y;
+	q[3 * n + u] = v.z;
+}
+
+// ---- kernels ------------------------------------------------------------------------------------
+
+// Molecule::upd_cache: the centres' space-frame offsets of every (sorted) molecule
+__global__ void __launch_bounds__(kRigidThreads) k_rigid_sites(int64_t n, const int32_t* __restrict__ uidx,
+                                                               const int32_t* __restrict__ cid,
+                                                               const double* __restrict__ q,
+                                                               const RigidParams* __restrict__ P,
+                                                               double* __restrict__ ds) {
+	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const Quat qi = load_q(q, n, uidx[i]);
+	const int c = cid[i];
+	const int ns = P->nsites[c], b = P->base[c];
+	for (int s = 0; s < P->ns_max; s++) {
+		double d[3] = {0.0, 0.0, 0.0};
+		if (s < ns) {
+			const double body[3] = {P->site[b + s][0], P->site[b + s][1], P->site[b + s][2]};
+			q_rotate_inv(qi, body, d);
+		}
+		for (int k = 0; k < 3; k++) ds[(int64_t) (s * 3 + k) * n + i] = d[k];
+	}
+}
+
+struct RigidOut {
+	double* fx;
+	double* fy;
+	double* fz;
+	double* M;          // caller order, M[k*n + u]
+	double* partials;
+	unsigned* ticket;
+	double* scalars;    // [0..2] = sum u (both sides), sum drm.f (both sides), pairs (both sides)
+	int* status;
+};
+
+// One thread per sorted molecule i: force and torque from every molecule of the 27 cells around it.
+template <bool kMixed, int NS>
+__global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const double* __restrict__ rx,
+                                                               const double* __restrict__ ry,
+                                                               const double* __restrict__ rz,
+                                                               const int32_t* __restrict__ cid,
+                                                               const int32_t* __restrict__ uidx,
+                                                               const int32_t* __restrict__ start, Grid g,
+                                                               const RigidParams* __restrict__ P,
+                                                               const double* __restrict__ ds, RigidOut o) {
+	constexpr int TT = kMaxSiteTotal * kMaxSiteTotal;
+	__shared__ double s_e24[TT], s_sig2[TT], s_sh6[TT];
+	__shared__ int s_ns[kMaxSpecies], s_base[kMaxSpecies];
+	for (int k = threadIdx.x; k < TT; k += blockDim.x) {
+		s_e24[k] = P->eps24[k];
+		s_sig2[k] = P->sig2[k];
+		s_sh6[k] = P->shift6[k];
+	}
+	if (threadIdx.x < kMaxSpecies) {
+		s_ns[threadIdx.x] = P->nsites[threadIdx.x];
+		s_base[threadIdx.x] = P->base[threadIdx.x];
+	}
+	__syncthreads();
+	const double rc2 = P->rc2, rclj2 = P->rclj2;
+	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	double F[3] = {0.0, 0.0, 0.0}, Mt[3] = {0.0, 0.0, 0.0};
+	double U = 0.0, W = 0.0, np = 0.0;
+	bool same = false;
+	if (i < n) {
+		const double xi = rx[i], yi = ry[i], zi = rz[i];
+		const int ci = cid[i];
+		const int nsi = s_ns[ci], bi = s_base[ci];
+		double di[NS][3];
+#pragma unroll
+		for (int s = 0; s < NS; s++)
+#pragma unroll
+			for (int k = 0; k < 3; k++) di[s][k] = s < nsi ? ds[(int64_t) (s * 3 + k) * n + i] : 0.0;
+		int cc[3];
+		const double r[3] = {xi, yi, zi};
+		for (int d = 0; d < 3; d++) {
+			int c = (int) floor(__ddiv_rn(__dsub_rn(r[d], g.halo_min[d]), g.cell_length[d])) - 1;
+			cc[d] = c < 0 ? 0 : (c >= g.nc[d] ? g.nc[d] - 1 : c);
+		}
+		for (int dz = -1; dz <= 1; dz++) {
+			int z = cc[2] + dz;
+			double sz = 0.0;
+			if (z < 0) {
+				z += g.nc[2];
+				sz = -g.L[2];
+			} else if (z >= g.nc[2]) {
+				z -= g.nc[2];
+				sz = g.L[2];
+			}
+			for (int dy = -1; dy <= 1; dy++) {
+				int y = cc[1] + dy;
+				double sy = 0.0;
+				if (y < 0) {
+					y += g.nc[1];
+					sy = -g.L[1];
+				} else if (y >= g.nc[1]) {
+					y -= g.nc[1];
+					sy = g.L[1];
+				}
+				for (int dx = -1; dx <= 1; dx++) {
+					int x = cc[0] + dx;
+					double sx = 0.0;
+					if (x < 0) {
+						x += g.nc[0];
+						sx = -g.L[0];
+					} else if (x >= g.nc[0]) {
+						x -= g.nc[0];
+						sx = g.L[0];
+					}
+					const int nb = (z * g.nc[1] + y) * g.nc[0] + x;
+					const bool shifted = (sx != 0.0) || (sy != 0.0) || (sz != 0.0);
+					const int j0 = start[nb], j1 = start[nb + 1];
+					for (int j = j0; j < j1; j++) {
+						if (j == i && !shifted) continue;
+						double xj = rx[j], yj = ry[j], zj = rz[j];
+						if (shifted) {   // the halo image of j (DomainDecompDummy.cpp:64-70, 93-99)
+							xj = __dadd_rn(xj, sx);
+							yj = __dadd_rn(yj, sy);
+							zj = __dadd_rn(zj, sz);
+						}
+						const double m0 = __dsub_rn(xi, xj), m1 = __dsub_rn(yi, yj), m2 = __dsub_rn(zi, zj);
+						const double dd =
+						    __dadd_rn(__dadd_rn(__dmul_rn(m0, m0), __dmul_rn(m1, m1)), __dmul_rn(m2, m2));
+						if (!(dd < rc2)) continue;
+						np += 1.0;
+						if (dd == 0.0) same = true;
+						if (!(dd < rclj2)) continue;
+						const int cj = cid[j];
+						const int nsj = s_ns[cj], bj = s_base[cj];
+#pragma unroll
+						for (int sj = 0; sj < NS; sj++) {
+							if (sj >= nsj) break;
+							const double dj0 = ds[(int64_t) (sj * 3 + 0) * n + j];
+							const double dj1 = ds[(int64_t) (sj * 3 + 1) * n + j];
+							const double dj2 = ds[(int64_t) (sj * 3 + 2) * n + j];
+#pragma unroll
+							for (int si = 0; si < NS; si++) {
+								if (si >= nsi) break;
+								const int pk = (bi + si) * kMaxSiteTotal + bj + sj;
+								// SiteSiteDistance: drs = drm + d_i - d_j
+								const double s0 = __dsub_rn(__dadd_rn(m0, di[si][0]), dj0);
+								const double s1 = __dsub_rn(__dadd_rn(m1, di[si][1]), dj1);
+								const double s2 = __dsub_rn(__dadd_rn(m2, di[si][2]), dj2);
+								double f0, f1, f2;
+								if (!kMixed) {
+									const double dr2 = __dadd_rn(__dadd_rn(__dmul_rn(s0, s0), __dmul_rn(s1, s1)),
+									                             __dmul_rn(s2, s2));
+									const double eps24 = s_e24[pk];
+									const double invdr2 = __ddiv_rn(1.0, dr2);
+									double lj6 = __dmul_rn(s_sig2[pk], invdr2);
+									lj6 = __dmul_rn(__dmul_rn(lj6, lj6), lj6);
+									const double lj12 = __dmul_rn(lj6, lj6);
+									const double lj12m6 = __dsub_rn(lj12, lj6);
+									U = __dadd_rn(U, __dadd_rn(__dmul_rn(eps24, lj12m6), s_sh6[pk]));
+									const double fac = __dmul_rn(__dmul_rn(eps24, __dadd_rn(lj12, lj12m6)), invdr2);
+									f0 = __dmul_rn(fac, s0);
+									f1 = __dmul_rn(fac, s1);
+									f2 = __dmul_rn(fac, s2);
+								} else {
+									const float e0 = (float) s0, e1 = (float) s1, e2 = (float) s2;
+									const float dr2 = e0 * e0 + e1 * e1 + e2 * e2;
+									const float eps24 = (float) s_e24[pk];
+									const float inv = __fdividef(1.0f, dr2);
+									const float q2 = (float) s_sig2[pk] * inv;
+									const float q6 = q2 * q2 * q2;
+									const float q12 = q6 * q6;
+									const float qm = q12 - q6;
+									const float fac = eps24 * (q12 + qm) * inv;
+									U += (double) (eps24 * qm) + s_sh6[pk];
+									f0 = (double) (fac * e0);
+									f1 = (double) (fac * e1);
+									f2 = (double) (fac * e2);
+								}
+								F[0] = __dadd_rn(F[0], f0);
+								F[1] = __dadd_rn(F[1], f1);
+								F[2] = __dadd_rn(F[2], f2);
+								// M += d_i x f (Molecule::calcFM)
+								Mt[0] = __dadd_rn(Mt[0], __dsub_rn(__dmul_rn(di[si][1], f2), __dmul_rn(di[si][2], f1)));
+								Mt[1] = __dadd_rn(Mt[1], __dsub_rn(__dmul_rn(di[si][2], f0), __dmul_rn(di[si][0], f2)));
+								Mt[2] = __dadd_rn(Mt[2], __dsub_rn(__dmul_rn(di[si][0], f1), __dmul_rn(di[si][1], f0)));
+								// Virial += drm . f
+								W = __dadd_rn(W, __dadd_rn(__dadd_rn(__dmul_rn(m0, f0), __dmul_rn(m1, f1)),
+								                           __dmul_rn(m2, f2)));
+							}
+						}
+					}
+				}
+			}
+		}
+		o.fx[i] = F[0];
+		o.fy[i] = F[1];
+		o.fz[i] = F[2];
+		const int64_t u = uidx[i];
+		o.M[u] = Mt[0];
+		o.M[n + u] = Mt[1];
+		o.M[2 * n + u] = Mt[2];
+		const bool bad = !(isfinite(F[0]) && isfinite(F[1]) && isfinite(F[2]) && isfinite(Mt[0]) &&
+		                   isfinite(Mt[1]) && isfinite(Mt[2]));
+		if (bad) atomicOr(o.status, kStatusNonFinite);
+	}
+	if (same) atomicOr(o.status, kStatusSamePosition);
+	block_sum3(U, W, np, o.partials);
+	last_block_sum(o.ticket, o.partials, gridDim.x, 3, o.scalars);
+}
+
+struct RigidState {
+	double *rx, *ry, *rz, *vx, *vy, *vz;
+	const double *fx, *fy, *fz;
+	const int32_t* cid;
+	const int32_t* uidx;
+	double* q;
+	double* D;
+	const double* M;
+};
+
+// Molecule::upd_preF for every molecule
+__global__ void __launch_bounds__(kRigidThreads) k_rigid_pre(int64_t n, RigidState s, const RigidParams* __restrict__ P,
+                                                             double dt, double vcorr, double Dcorr) {
+	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const int c = s.cid[i];
+	const int64_t u = s.uidx[i];
+	const double dt_halve = __dmul_rn(.5, dt);
+	const double dtInv2m = __ddiv_rn(dt_halve, P->mass[c]);
+	double v0 = __dadd_rn(__dmul_rn(vcorr, s.vx[i]), __dmul_rn(dtInv2m, s.fx[i]));
+	double v1 = __dadd_rn(__dmul_rn(vcorr, s.vy[i]), __dmul_rn(dtInv2m, s.fy[i]));
+	double v2 = __dadd_rn(__dmul_rn(vcorr, s.vz[i]), __dmul_rn(dtInv2m, s.fz[i]));
+	s.vx[i] = v0;
+	s.vy[i] = v1;
+	s.vz[i] = v2;
+	s.rx[i] = __dadd_rn(s.rx[i], __dmul_rn(dt, v0));
+	s.ry[i] = __dadd_rn(s.ry[i], __dmul_rn(dt, v1));
+	s.rz[i] = __dadd_rn(s.rz[i], __dmul_rn(dt, v2));
+
+	const Quat q = load_q(s.q, n, u);
+	double D[3] = {s.D[u], s.D[n + u], s.D[2 * n + u]};
+	const double M[3] = {s.M[u], s.M[n + u], s.M[2 * n + u]};
+	double w[3];
+	q_rotate(q, D, w);
+	for (int d = 0; d < 3; d++) w[d] = __dmul_rn(w[d], P->invI[c][d]);
+	Quat qh = q_add(q_scale(q_differentiate(q, w), dt_halve), q);
+	qh = q_scale(qh, __ddiv_rn(1., __dsqrt_rn(q_magnitude2(qh))));
+	for (int d = 0; d < 3; d++) D[d] = __dadd_rn(__dmul_rn(Dcorr, D[d]), __dmul_rn(dt_halve, M[d]));
+	q_rotate(qh, D, w);
+	for (int d = 0; d < 3; d++) w[d] = __dmul_rn(w[d], P->invI[c][d]);
+	Quat qn = q_add(q, q_scale(q_differentiate(qh, w), dt));
+	qn = q_scale(qn, __ddiv_rn(1., __dsqrt_rn(q_magnitude2(qn))));
+	store_q(s.q, n, u, qn);
+	s.D[u] = D[0];
+	s.D[n + u] = D[1];
+	s.D[2 * n + u] = D[2];
+}
+
+// Molecule::upd_postF for every molecule; sums m v^2 and I w^2 into scalars[0..1]. With a record
+// pointer the last block also writes the step record {Upot, virial, sum m v^2, sum I w^2, pairs}
+// from the pair sums in pair_scalars.
+__global__ void __launch_bounds__(kRigidThreads) k_rigid_post(int64_t n, RigidState s, const RigidParams* __restrict__ P,
+                                                              double dt_half, double* partials, unsigned* ticket,
+                                                              double* scalars, const double* pair_scalars,
+                                                              double* record, int* status) {
+	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	double mv2 = 0.0, iw2 = 0.0;
+	if (i < n) {
+		const int c = s.cid[i];
+		const int64_t u = s.uidx[i];
+		const double m = P->mass[c];
+		const double dtInv2m = __ddiv_rn(dt_half, m);
+		const double v0 = __dadd_rn(s.vx[i], __dmul_rn(dtInv2m, s.fx[i]));
+		const double v1 = __dadd_rn(s.vy[i], __dmul_rn(dtInv2m, s.fy[i]));
+		const double v2 = __dadd_rn(s.vz[i], __dmul_rn(dtInv2m, s.fz[i]));
+		s.vx[i] = v0;
+		s.vy[i] = v1;
+		s.vz[i] = v2;
+		const double vv = __dadd_rn(__dadd_rn(__dmul_rn(v0, v0), __dmul_rn(v1, v1)), __dmul_rn(v2, v2));
+		mv2 = __dmul_rn(m, vv);
+		double D[3];
+		for (int d = 0; d < 3; d++) {
+			D[d] = __dadd_rn(s.D[d * n + u], __dmul_rn(dt_half, s.M[d * n + u]));
+			s.D[d * n + u] = D[d];
+		}
+		double w[3];
+		q_rotate(load_q(s.q, n, u), D, w);
+		for (int d = 0; d < 3; d++) {
+			w[d] = __dmul_rn(w[d], P->invI[c][d]);
+			iw2 = __dadd_rn(iw2, __dmul_rn(__dmul_rn(P->I[c][d], w[d]), w[d]));
+		}
+		if (!(isfinite(mv2) && isfinite(iw2))) atomicOr(status, kStatusNonFinite);
+	}
+	block_sum3(mv2, iw2, 0.0, partials);
+	if (last_block_sum(ticket, partials, gridDim.x, 2, scalars) && threadIdx.x == 0 && record) {
+		record[0] = pair_scalars[0] * 0.5 / 6.;
+		record[1] = pair_scalars[1] * 0.5;
+		record[2] = scalars[0];
+		record[3] = scalars[1];
+		record[4] = pair_scalars[2] * 0.5;
+	}
+}
+
+template <typename T>
+__global__ void k_gather_soa(int64_t n, int k, const T* __restrict__ src, T* __restrict__ dst) {
+	// (k, n) component-major -> (n, k) row-major
+	const int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= n * k) return;
+	const int64_t i = t / k, d = t % k;
+	dst[t] = src[d * n + i];
+}
+
+template <typename T>
+__global__ void k_scatter_soa(int64_t n, int k, const T* __restrict__ src, T* __restrict__ dst) {
+	// (n, k) row-major -> (k, n) component-major
+	const int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= n * k) return;
+	const int64_t i = t / k, d = t % k;
+	dst[d * n + i] = src[t];
+}
+
+}  // namespace
+}  // namespace mdgpu
+
+using namespace mdgpu;
+
+struct mdgpu_rigid {
+	mdgpu_ctx* inner = nullptr;
+	RigidParams hp{};
+	RigidParams* dp = nullptr;
+	double* q = nullptr;        // 4 x cap, caller order
+	double* D = nullptr;        // 3 x cap
+	double* M = nullptr;        // 3 x cap
+	double* ds = nullptr;       // 3 x ns_max x cap, sorted order
+	double* stage = nullptr;    // 4 x cap host <-> device staging
+	double* scal = nullptr;     // [0..2] pair sums, [3..4] kinetic sums
+	double* steps = nullptr;    // 5 doubles per step of mdgpu_rigid_run
+	int64_t steps_cap = 0;
+	unsigned* tickets = nullptr;
+	double* h_scal = nullptr;
+	int64_t cap = 0;
+};
+
+namespace {
+
+Context* ctx_of(mdgpu_rigid* h) { return &h->inner->c; }
+
+#define RG_CUDA(call)                                                       \
+	do {                                                                    \
+		cudaError_t e_ = (call);                                            \
+		if (e_ != cudaSuccess) return set_cuda_error(c, e_, #call);        \
+	} while (0)
+
+int launch_rigid_forces(mdgpu_rigid* h) {
+	Context* c = ctx_of(h);
+	const int64_t n = c->n;
+	const unsigned nb = (unsigned) nblocks(n);
+	k_rigid_sites<<<nb, kRigidThreads, 0, c->stream>>>(n, c->p.uidx, c->p.cid, h->q, h->dp, h->ds);
+	RigidOut o{c->p.fx, c->p.fy, c->p.fz, h->M, c->partials, h->tickets, h->scal, c->status};
+	const bool mixed = c->precision == MDGPU_MIXED;
+	const int ns = h->hp.ns_max;
+#define RG_PAIRS(MX, NSV)                                                                                   \
+	k_rigid_pairs<MX, NSV><<<nb, kRigidThreads, 0, c->stream>>>(n, c->p.rx, c->p.ry, c->p.rz, c->p.cid,     \
+	                                                            c->p.uidx, c->cell_start, c->g, h->dp, h->ds, o)
+	if (ns <= 1)
+		mixed ? RG_PAIRS(true, 1) : RG_PAIRS(false, 1);
+	else if (ns == 2)
+		mixed ? RG_PAIRS(true, 2) : RG_PAIRS(false, 2);
+	else if (ns == 3)
+		mixed ? RG_PAIRS(true, 3) : RG_PAIRS(false, 3);
+	else if (ns == 4)
+		mixed ? RG_PAIRS(true, 4) : RG_PAIRS(false, 4);
+	else
+		mixed ? RG_PAIRS(true, kMaxSites) : RG_PAIRS(false, kMaxSites);
+#undef RG_PAIRS
+	count_launches(c, 2);
+	RG_CUDA(cudaGetLastError());
+	return MDGPU_OK;
+}
+
+RigidState state_of(mdgpu_rigid* h) {
+	Context* c = ctx_of(h);
+	return RigidState{c->p.rx, c->p.ry, c->p.rz, c->p.vx, c->p.vy, c->p.vz, c->p.fx, c->p.fy, c->p.fz,
+	                  c->p.cid, c->p.uidx, h->q, h->D, h->M};
+}
+
+int launch_rigid_pre(mdgpu_rigid* h, double dt, double vcorr, double Dcorr) {
+	Context* c = ctx_of(h);
+	k_rigid_pre<<<(unsigned) nblocks(c->n), kRigidThreads, 0, c->stream>>>(c->n, state_of(h), h->dp, dt, vcorr, Dcorr);
+	count_launches(c, 1);
+	RG_CUDA(cudaGetLastError());
+	return MDGPU_OK;
+}
+
+int launch_rigid_post(mdgpu_rigid* h, double dt_half, double* record) {
+	Context* c = ctx_of(h);
+	k_rigid_post<<<(unsigned) nblocks(c->n), kRigidThreads, 0, c->stream>>>(
+	    c->n, state_of(h), h->dp, dt_half, c->partials, h->tickets + 1, h->scal + 3, h->scal, record, c->status);
+	count_launches(c, 1);
+	RG_CUDA(cudaGetLastError());
+	return MDGPU_OK;
+}
+
+// Site tables from the components (Comp2Param::initialize and Component::addLJcenter).
+int setup_rigid(Context* c, int ncomp, const int32_t* nsites, const mdgpu_site* sites, const double* inertia,
+                const double* mix, double rc, double rc_lj, RigidParams& P) {
+	P = RigidParams{};
+	P.nc = ncomp;
+	P.rc2 = rc * rc;
+	P.rclj2 = rc_lj * rc_lj;
+	int total = 0;
+	for (int k = 0; k < ncomp; k++) {
+		if (nsites[k] < 1 || nsites[k] > kMaxSites)
+			return set_error(c, MDGPU_ERR_ARG, "each component needs 1.." + std::to_string(kMaxSites) + " LJ centres");
+		P.nsites[k] = nsites[k];
+		P.base[k] = total;
+		total += nsites[k];
+		P.ns_max = std::max(P.ns_max, nsites[k]);
+	}
+	if (total > kMaxSiteTotal)
+		return set_error(c, MDGPU_ERR_ARG, "at most " + std::to_string(kMaxSiteTotal) + " LJ centres in all components");
+	P.nsite_total = total;
+	std::vector<double> shift(total, 0.0);
+	for (int k = 0; k < ncomp; k++) {
+		double m = 0.0, I[3] = {0.0, 0.0, 0.0};
+		for (int s = 0; s < nsites[k]; s++) {
+			const mdgpu_site& t = sites[P.base[k] + s];
+			if (!(t.mass > 0.0) || !(t.sigma > 0.0) || !(t.eps >= 0.0))
+				return set_error(c, MDGPU_ERR_ARG, "LJ centre with non-positive mass or sigma, or negative eps");
+			for (int d = 0; d < 3; d++) P.site[P.base[k] + s][d] = t.r[d];
+			m += t.mass;
+			const double x = t.r[0], y = t.r[1], z = t.r[2];
+			I[0] += t.mass * (y * y + z * z);
+			I[1] += t.mass * (x * x + z * z);
+			I[2] += t.mass * (x * x + y * y);
+			if (t.do_shift) {   // Component::addLJcenter, with the centre's cutoff = LJCutoffRadius
+				const double sigperrc2 = t.sigma * t.sigma / (rc_lj * rc_lj);
+				const double sigperrc6 = sigperrc2 * sigperrc2 * sigperrc2;
+				shift[P.base[k] + s] = 24.0 * t.eps * (sigperrc6 - sigperrc6 * sigperrc6);
+			}
+		}
+		P.mass[k] = m;
+		for (int d = 0; d < 3; d++) {
+			if (inertia && inertia[3 * k + d] > 0.0) I[d] = inertia[3 * k + d];   // InputOldstyle.cpp:188-195
+			P.I[k][d] = I[d];
+			P.invI[k][d] = I[d] != 0.0 ? 1.0 / I[d] : 0.0;                           // Molecule.cpp:342-350
+		}
+	}
+	int mixpos = 0;
+	for (int ci = 0; ci < ncomp; ci++) {
+		for (int a = 0; a < nsites[ci]; a++) {
+			const mdgpu_site& A = sites[P.base[ci] + a];
+			for (int b = 0; b < nsites[ci]; b++) {
+				const mdgpu_site& B = sites[P.base[ci] + b];
+				const int k = (P.base[ci] + a) * kMaxSiteTotal + P.base[ci] + b;
+				double sigma2 = .5 * (A.sigma + B.sigma);
+				sigma2 *= sigma2;
+				P.eps24[k] = 24. * std::sqrt(A.eps * B.eps);
+				P.sig2[k] = sigma2;
+				P.shift6[k] = shift[P.base[ci] + a];
+			}
+		}
+		for (int cj = ci + 1; cj < ncomp; cj++) {
+			const double xi = mix ? mix[2 * mixpos] : 1.0, eta = mix ? mix[2 * mixpos + 1] : 1.0;
+			mixpos++;
+			for (int a = 0; a < nsites[ci]; a++) {
+				const mdgpu_site& A = sites[P.base[ci] + a];
+				for (int b = 0; b < nsites[cj]; b++) {
+					const mdgpu_site& B = sites[P.base[cj] + b];
+					const double epsilon24 = 24. * xi * std::sqrt(A.eps * B.eps);
+					double sigma2 = eta * .5 * (A.sigma + B.sigma);
+					sigma2 *= sigma2;
+					const double sigperrc2 = sigma2 / (rc_lj * rc_lj);
+					const double sigperrc6 = sigperrc2 * sigperrc2 * sigperrc2;
+					const double shift6combined = epsilon24 * (sigperrc6 - sigperrc6 * sigperrc6);
+					const int kij = (P.base[ci] + a) * kMaxSiteTotal + P.base[cj] + b;
+					const int kji = (P.base[cj] + b) * kMaxSiteTotal + P.base[ci] + a;
+					P.eps24[kij] = P.eps24[kji] = epsilon24;
+					P.sig2[kij] = P.sig2[kji] = sigma2;
+					P.shift6[kij] = P.shift6[kji] = shift6combined;
+				}
+			}
+		}
+	}
+	return MDGPU_OK;
+}
+
+int ensure_capacity(mdgpu_rigid* h, int64_t n) {
+	Context* c = ctx_of(h);
+	if (n <= h->cap) return MDGPU_OK;
+	cudaFree(h->q);
+	cudaFree(h->D);
+	cudaFree(h->M);
+	cudaFree(h->ds);
+	cudaFree(h->stage);
+	h->q = h->D = h->M = h->ds = h->stage = nullptr;
+	h->cap = 0;
+	RG_CUDA(cudaMalloc(&h->q, sizeof(double) * 4 * n));
+	RG_CUDA(cudaMalloc(&h->D, sizeof(double) * 3 * n));
+	RG_CUDA(cudaMalloc(&h->M, sizeof(double) * 3 * n));
+	RG_CUDA(cudaMalloc(&h->ds, sizeof(double) * 3 * std::max(1, h->hp.ns_max) * n));
+	RG_CUDA(cudaMalloc(&h->stage, sizeof(double) * 4 * n));
+	h->cap = n;
+	return MDGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mdgpu_rigid_create(mdgpu_rigid** out, const double length[3], double cutoff, double lj_cutoff,
+                       double cells_in_cutoff, int ncomp, const int32_t* nsites, const mdgpu_site* sites,
+                       const double* inertia, const double* mix, int precision, int device) {
+	if (!out) return MDGPU_ERR_ARG;
+	*out = nullptr;
+	if (ncomp < 1 || ncomp > kMaxSpecies || !nsites || !sites) return MDGPU_ERR_ARG;
+	// the single-box context holds the molecule centres; its component table carries each component's
+	// total mass (the LJ table of the single-centre kernels is not used here)
+	std::vector<mdgpu_component> comps(ncomp);
+	int base = 0;
+	for (int k = 0; k < ncomp; k++) {
+		if (nsites[k] < 1 || nsites[k] > kMaxSites) return MDGPU_ERR_ARG;
+		double m = 0.0;
+		for (int s = 0; s < nsites[k]; s++) m += sites[base + s].mass;
+		comps[k] = mdgpu_component{sites[base].eps > 0 ? sites[base].eps : 1.0,
+		                           sites[base].sigma > 0 ? sites[base].sigma : 1.0, m > 0 ? m : 1.0, 0};
+		base += nsites[k];
+	}
+	mdgpu_ctx* inner = nullptr;
+	int st = mdgpu_create(&inner, length, cutoff, lj_cutoff, cells_in_cutoff, ncomp, comps.data(), mix, precision, device);
+	if (st) {
+		if (inner) mdgpu_destroy(inner);
+		return st;
+	}
+	mdgpu_rigid* h = new mdgpu_rigid();
+	h->inner = inner;
+	Context* c = ctx_of(h);
+	st = setup_rigid(c, ncomp, nsites, sites, inertia, mix, c->rc, c->rc_lj, h->hp);
+	if (st == MDGPU_OK) {
+		cudaError_t e = cudaMalloc(&h->dp, sizeof(RigidParams));
+		if (e == cudaSuccess) e = cudaMemcpy(h->dp, &h->hp, sizeof(RigidParams), cudaMemcpyHostToDevice);
+		if (e == cudaSuccess) e = cudaMalloc(&h->scal, sizeof(double) * 8);
+		if (e == cudaSuccess) e = cudaMemset(h->scal, 0, sizeof(double) * 8);
+		if (e == cudaSuccess) e = cudaMalloc(&h->tickets, sizeof(unsigned) * 2);
+		if (e == cudaSuccess) e = cudaMemset(h->tickets, 0, sizeof(unsigned) * 2);
+		if (e == cudaSuccess) e = cudaMallocHost(&h->h_scal, sizeof(double) * 8);
+		if (e != cudaSuccess) st = set_cuda_error(c, e, "mdgpu_rigid_create");
+	}
+	*out = h;   // returned even on failure so that mdgpu_rigid_last_error can be read
+	return st;
+}
+
+int mdgpu_rigid_destroy(mdgpu_rigid* h) {
+	if (!h) return MDGPU_ERR_ARG;
+	if (h->inner) cudaSetDevice(h->inner->c.device);
+	cudaFree(h->dp);
+	cudaFree(h->q);
+	cudaFree(h->D);
+	cudaFree(h->M);
+	cudaFree(h->ds);
+	cudaFree(h->stage);
+	cudaFree(h->scal);
+	cudaFree(h->steps);
+	cudaFree(h->tickets);
+	if (h->h_scal) cudaFreeHost(h->h_scal);
+	int st = h->inner ? mdgpu_destroy(h->inner) : MDGPU_OK;
+	delete h;
+	return st;
+}
+
+const char* mdgpu_rigid_last_error(const mdgpu_rigid* h) {
+	return h && h->inner ? h->inner->c.err.c_str() : "null context";
+}
+
+int mdgpu_rigid_set_precision(mdgpu_rigid* h, int precision) {
+	if (!h) return MDGPU_ERR_ARG;
+	return mdgpu_set_precision(h->inner, precision);
+}
+
+int mdgpu_rigid_get_inertia(const mdgpu_rigid* h, int32_t comp, double* mass, double I[3]) {
+	if (!h || comp < 0 || comp >= h->hp.nc) return MDGPU_ERR_ARG;
+	if (mass) *mass = h->hp.mass[comp];
+	if (I)
+		for (int d = 0; d < 3; d++) I[d] = h->hp.I[comp][d];
+	return MDGPU_OK;
+}
+
+int mdgpu_rigid_set_particles(mdgpu_rigid* h, int64_t n, const uint64_t* id, const int32_t* cid, const double* r,
+                              const double* v, const double* q, const double* D) {
+	if (!h) return MDGPU_ERR_ARG;
+	Context* c = ctx_of(h);
+	if (!q || !D) return set_error(c, MDGPU_ERR_ARG, "q and D are required");
+	int st = mdgpu_set_particles(h->inner, n, id, cid, r, v, nullptr);
+	if (st) return st;
+	st = ensure_capacity(h, n);
+	if (st) return st;
+	const unsigned nb4 = (unsigned) nblocks(4 * n), nb3 = (unsigned) nblocks(3 * n);
+	RG_CUDA(cudaMemcpyAsync(h->stage, q, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, c->stream));
+	k_scatter_soa<double><<<nb4, kRigidThreads, 0, c->stream>>>(n, 4, h->stage, h->q);
+	RG_CUDA(cudaStreamSynchronize(c->stream));
+	RG_CUDA(cudaMemcpyAsync(h->stage, D, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+	k_scatter_soa<double><<<nb3, kRigidThreads, 0, c->stream>>>(n, 3, h->stage, h->D);
+	RG_CUDA(cudaMemsetAsync(h->M, 0, sizeof(double) * 3 * n, c->stream));
+	RG_CUDA(cudaGetLastError());
+	RG_CUDA(cudaStreamSynchronize(c->stream));
+	return MDGPU_OK;
+}
+
+int mdgpu_rigid_get_particles(mdgpu_rigid* h, int64_t n, uint64_t* id, int32_t* cid, double* r, double* v, double* F,
+                              double* q, double* D, double* M) {
+	if (!h) return MDGPU_ERR_ARG;
+	Context* c = ctx_of(h);
+	int st = mdgpu_get_particles(h->inner, n, id, cid, r, v, F);
+	if (st) return st;
+	struct {
+		double* out;
+		const double* src;
+		int k;
+	} sets[3] = {{q, h->q, 4}, {D, h->D, 3}, {M, h->M, 3}};
+	for (auto& s : sets) {
+		if (!s.out) continue;
+		k_gather_soa<double><<<(unsigned) nblocks(s.k * n), kRigidThreads, 0, c->stream>>>(n, s.k, s.src, h->stage);
+		RG_CUDA(cudaMemcpyAsync(s.out, h->stage, sizeof(double) * s.k * n, cudaMemcpyDeviceToHost, c->stream));
+		RG_CUDA(cudaStreamSynchronize(c->stream));
+	}
+	RG_CUDA(cudaGetLastError());
+	return MDGPU_OK;
+}
+
+int mdgpu_rigid_update(mdgpu_rigid* h) {
+	if (!h) return MDGPU_ERR_ARG;
+	return mdgpu_update(h->inner);
+}
+
+int mdgpu_rigid_traverse_pairs(mdgpu_rigid* h, double* upot, double* virial, double* npairs) {
+	if (!h) return MDGPU_ERR_ARG;
+	Context* c = ctx_of(h);
+	if (!c->cells_valid)
+		return set_error(c, MDGPU_ERR_STATE, "cell structure in the container is invalid, call mdgpu_rigid_update first");
+	RG_CUDA(cudaSetDevice(c->device));
+	int st = launch_rigid_forces(h);
+	if (st) return st;
+	RG_CUDA(cudaMemcpyAsync(h->h_scal, h->scal, sizeof(double) * 3, cudaMemcpyDeviceToHost, c->stream));
+	st = check_device_status(c);
+	if (st) return st;
+	// ParticlePairs2PotForceAdapter::finish: Upot = Upot6LJ/6 (each pair was seen twice)
+	if (upot) *upot = h->h_scal[0] * 0.5 / 6.;
+	if (virial) *virial = h->h_scal[1] * 0.5;
+	if (npairs) *npairs = h->h_scal[2] * 0.5;
+	return MDGPU_OK;
+}
+
+int mdgpu_rigid_leapfrog_pre(mdgpu_rigid* h, double dt, double vcorr, double Dcorr) {
+	if (!h) return MDGPU_ERR_ARG;
+	Context* c = ctx_of(h);
+	if (c->n == 0) return set_error(c, MDGPU_ERR_STATE, "no molecules loaded");
+	RG_CUDA(cudaSetDevice(c->device));
+	int st = launch_rigid_pre(h, dt, vcorr, Dcorr);
+	c->cells_valid = false;
+	return st;
+}
+
+int mdgpu_rigid_leapfrog_post(mdgpu_rigid* h, double dt_half, double* summv2, double* sum_iw2) {
+	if (!h) return MDGPU_ERR_ARG;
+	Context* c = ctx_of(h);
+	if (c->n == 0) return set_error(c, MDGPU_ERR_STATE, "no molecules loaded");
+	RG_CUDA(cudaSetDevice(c->device));
+	int st = launch_rigid_post(h, dt_half, nullptr);
+	if (st) return st;
+	RG_CUDA(cudaMemcpyAsync(h->h_scal + 3, h->scal + 3, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->stream));
+	st = check_device_status(c);
+	if (st) return st;
+	if (summv2) *summv2 = h->h_scal[3];
+	if (sum_iw2) *sum_iw2 = h->h_scal[4];
+	return MDGPU_OK;
+}
+
+int mdgpu_rigid_run(mdgpu_rigid* h, int32_t nsteps, double dt, double* per_step) {
+	if (!h) return MDGPU_ERR_ARG;
+	Context* c = ctx_of(h);
+	if (nsteps < 0) return set_error(c, MDGPU_ERR_ARG, "nsteps must be >= 0");
+	if (c->n == 0) return set_error(c, MDGPU_ERR_STATE, "no molecules loaded");
+	RG_CUDA(cudaSetDevice(c->device));
+	if (nsteps > h->steps_cap) {
+		cudaFree(h->steps);
+		h->steps = nullptr;
+		h->steps_cap = 0;
+		RG_CUDA(cudaMalloc(&h->steps, sizeof(double) * 5 * nsteps));
+		h->steps_cap = nsteps;
+	}
+	for (int32_t k = 0; k < nsteps; k++) {
+		// Simulation::simulateStep: upd_preF, update (wrap, bin), upd_cache + traversePairs, upd_postF
+		int st = launch_rigid_pre(h, dt, 1.0, 1.0);
+		if (st) return st;
+		RG_CUDA(launch_bin(c, true));
+		st = launch_rigid_forces(h);
+		if (st) return st;
+		st = launch_rigid_post(h, 0.5 * dt, h->steps + 5 * (int64_t) k);
+		if (st) return st;
+	}
+	c->cells_valid = true;
+	c->lists_valid = false;
+	if (per_step && nsteps > 0)
+		RG_CUDA(cudaMemcpyAsync(per_step, h->steps, sizeof(double) * 5 * nsteps, cudaMemcpyDeviceToHost, c->stream));
+	return check_device_status(c);
+}
+
+int mdgpu_rigid_get_stream(const mdgpu_rigid* h, void** stream) {
+	if (!h || !stream) return MDGPU_ERR_ARG;
+	return mdgpu_get_stream(h->inner, stream);
+}
+
+int mdgpu_rigid_profile(mdgpu_rigid* h, int64_t* launches) {
+	if (!h || !launches) return MDGPU_ERR_ARG;
+	*launches = h->inner->c.prof_count[3];
+	return MDGPU_OK;
+}
+
+}  // extern "C"

@@ -88,6 +88,20 @@ SIGNATURES = {
     "mdgpu_batch_set_barrier_timeout": (_I, [_VP, _I64]),
     "mdgpu_batch_set_skin": (_I, [_VP, _D]),
     "mdgpu_batch_skin_builds": (_I, [_VP, _VP]),
+    "mdgpu_rigid_create": (_I, [ctypes.POINTER(_VP), _VP, _D, _D, _D, _I, _VP, _VP, _VP, _VP, _I, _I]),
+    "mdgpu_rigid_destroy": (_I, [_VP]),
+    "mdgpu_rigid_last_error": (ctypes.c_char_p, [_VP]),
+    "mdgpu_rigid_set_precision": (_I, [_VP, _I]),
+    "mdgpu_rigid_get_inertia": (_I, [_VP, _I32, _VP, _VP]),
+    "mdgpu_rigid_set_particles": (_I, [_VP, _I64, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "mdgpu_rigid_get_particles": (_I, [_VP, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "mdgpu_rigid_update": (_I, [_VP]),
+    "mdgpu_rigid_traverse_pairs": (_I, [_VP, _VP, _VP, _VP]),
+    "mdgpu_rigid_leapfrog_pre": (_I, [_VP, _D, _D, _D]),
+    "mdgpu_rigid_leapfrog_post": (_I, [_VP, _D, _VP, _VP]),
+    "mdgpu_rigid_run": (_I, [_VP, _I32, _D, _VP]),
+    "mdgpu_rigid_get_stream": (_I, [_VP, _VP]),
+    "mdgpu_rigid_profile": (_I, [_VP, _VP]),
 }
 
 _lib = None
@@ -102,6 +116,11 @@ class MdgpuError(RuntimeError):
 class _MdComponent(ctypes.Structure):
     _fields_ = [("eps", ctypes.c_double), ("sigma", ctypes.c_double), ("mass", ctypes.c_double),
                 ("do_shift", ctypes.c_int)]
+
+
+class _MdSite(ctypes.Structure):
+    _fields_ = [("r", ctypes.c_double * 3), ("mass", ctypes.c_double), ("eps", ctypes.c_double),
+                ("sigma", ctypes.c_double), ("do_shift", ctypes.c_int)]
 
 
 def load_library(path: str = LIB_PATH):
@@ -297,6 +316,139 @@ class Batch:
         b = ctypes.c_int64()
         self._check(self.lib.mdgpu_batch_skin_builds(self.h, ctypes.byref(b)))
         return b.value
+
+
+class RigidLinkedCells:
+    """The GPU container for rigid multi-centre LJ molecules (include/mdgpu.h, mdgpu_rigid_*): the
+    molecule centres binned into cells of edge >= rc as in ``LinkedCells``, every molecule with an
+    orientation q, angular momentum D and torque M. Mirrors the same reference sequence:
+    ``update`` (LinkedCells::update), ``traversePairs`` (Molecule::upd_cache, traversePairs with
+    PotForce's loop over LJ centre pairs, Molecule::calcFM), ``eventNewTimestep`` /
+    ``eventForcesCalculated`` (Molecule::upd_preF / upd_postF) and ``run`` (Simulation::simulateStep,
+    NVE). ``components`` are ``workloads.Component`` objects (single-centre ones count as one
+    centre at the origin)."""
+
+    def __init__(self, length: Sequence[float], cutoffRadius: float, components, mixcoeff=None,
+                 LJCutoffRadius: float = 0.0, cellsInCutoffRadius: float = 1.0, precision: int = FP64,
+                 device: int = 0):
+        self.lib = load_library()
+        centres = [c.lj_centres() for c in components]
+        nsites = np.array([len(cs) for cs in centres], dtype=np.int32)
+        sites = (_MdSite * int(nsites.sum()))()
+        k = 0
+        for cs in centres:
+            for t in cs:
+                sites[k].r[0], sites[k].r[1], sites[k].r[2] = float(t.x), float(t.y), float(t.z)
+                sites[k].mass, sites[k].eps, sites[k].sigma = float(t.mass), float(t.eps), float(t.sigma)
+                sites[k].do_shift = 1 if t.do_shift else 0
+                k += 1
+        inertia = np.zeros((len(components), 3))
+        for i, c in enumerate(components):
+            if getattr(c, "inertia", None) is not None:
+                inertia[i] = c.inertia
+        self._length = _c64(length)
+        mix = None if mixcoeff is None else _c64(mixcoeff).reshape(-1)
+        if mix is not None and mix.size == 0:
+            mix = None
+        h = ctypes.c_void_p()
+        st = self.lib.mdgpu_rigid_create(ctypes.byref(h), _ptr(self._length), float(cutoffRadius),
+                                         float(LJCutoffRadius), float(cellsInCutoffRadius), len(components),
+                                         _ptr(nsites), ctypes.cast(sites, ctypes.c_void_p), _ptr(inertia), _ptr(mix),
+                                         int(precision), int(device))
+        self.h = h.value
+        if st != 0:
+            msg = self.lib.mdgpu_rigid_last_error(self.h).decode() if self.h else ""
+            if self.h:
+                self.lib.mdgpu_rigid_destroy(self.h)
+            self.h = None
+            raise MdgpuError(st, msg)
+        self.n = 0
+        self.components = components
+
+    @classmethod
+    def from_system(cls, system, precision: int = FP64, device: int = 0) -> "RigidLinkedCells":
+        lc = cls(system.length, system.cutoff, system.components, system.mix, system.lj_cutoff, 1.0, precision, device)
+        n = system.n
+        q = system.q if system.q is not None else np.tile([1.0, 0.0, 0.0, 0.0], (n, 1))
+        D = system.D if system.D is not None else np.zeros((n, 3))
+        lc.addParticles(system.ids, system.cid, system.r, system.v, q, D)
+        return lc
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.mdgpu_rigid_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int) -> None:
+        if st != 0:
+            raise MdgpuError(st, self.lib.mdgpu_rigid_last_error(self.h).decode())
+
+    def setPrecision(self, precision: int) -> None:
+        self._check(self.lib.mdgpu_rigid_set_precision(self.h, int(precision)))
+
+    def inertia(self, comp: int):
+        """(mass, (I11, I22, I33)) of component comp."""
+        m = ctypes.c_double()
+        I = np.zeros(3)
+        self._check(self.lib.mdgpu_rigid_get_inertia(self.h, int(comp), ctypes.byref(m), _ptr(I)))
+        return m.value, I
+
+    def addParticles(self, ids, cid, r, v, q, D) -> None:
+        n = int(np.asarray(ids).shape[0])
+        self._check(self.lib.mdgpu_rigid_set_particles(
+            self.h, n, _ptr(_c64(ids, np.uint64)), _ptr(_c64(cid, np.int32)), _ptr(_c64(r, shape=(n, 3))),
+            _ptr(_c64(v, shape=(n, 3))), _ptr(_c64(q, shape=(n, 4))), _ptr(_c64(D, shape=(n, 3)))))
+        self.n = n
+
+    def getParticles(self) -> Dict[str, np.ndarray]:
+        n = self.n
+        ids = np.zeros(n, dtype=np.uint64)
+        cid = np.zeros(n, dtype=np.int32)
+        r, v, F, D, M = (np.zeros((n, 3)) for _ in range(5))
+        q = np.zeros((n, 4))
+        self._check(self.lib.mdgpu_rigid_get_particles(self.h, n, _ptr(ids), _ptr(cid), _ptr(r), _ptr(v), _ptr(F),
+                                                       _ptr(q), _ptr(D), _ptr(M)))
+        return dict(id=ids, cid=cid, r=r, v=v, F=F, q=q, D=D, M=M)
+
+    def update(self) -> None:
+        self._check(self.lib.mdgpu_rigid_update(self.h))
+
+    def traversePairs(self):
+        """(Upot, virial, molecule pairs within the cutoff); F and M of every molecule on the device."""
+        u, w, p = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.mdgpu_rigid_traverse_pairs(self.h, ctypes.byref(u), ctypes.byref(w), ctypes.byref(p)))
+        return u.value, w.value, p.value
+
+    def eventNewTimestep(self, dt: float, vcorr: float = 1.0, Dcorr: float = 1.0) -> None:
+        self._check(self.lib.mdgpu_rigid_leapfrog_pre(self.h, float(dt), float(vcorr), float(Dcorr)))
+
+    def eventForcesCalculated(self, dt: float):
+        """The closing half-kicks; returns (sum m v^2, sum I w^2)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.mdgpu_rigid_leapfrog_post(self.h, 0.5 * float(dt), ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def run(self, nsteps: int, dt: float, record: bool = True) -> Optional[np.ndarray]:
+        """nsteps NVE steps; returns (nsteps, 5) {Upot, virial, sum m v^2, sum I w^2, pairs}."""
+        out = np.zeros((nsteps, 5)) if record else None
+        self._check(self.lib.mdgpu_rigid_run(self.h, int(nsteps), float(dt), _ptr(out)))
+        return out
+
+    def launches(self) -> int:
+        k = ctypes.c_int64()
+        self._check(self.lib.mdgpu_rigid_profile(self.h, ctypes.byref(k)))
+        return k.value
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.lib.mdgpu_rigid_get_stream(self.h, ctypes.byref(s)))
+        return s.value or 0
 
 
 class LinkedCells:

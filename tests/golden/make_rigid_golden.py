@@ -10,7 +10,11 @@ rigid_<name>.npz (the start state is stored too, so the fixtures do not depend o
 * rigid_mix_256:   that molecule and a linear three-centre molecule with a different middle centre,
                    50/50, xi 0.9, eta 1.05, rho 0.15, T 2.0, rc 3.0;
 * rigid_bent_256:  a bent three-centre molecule with three non-zero moments, plain LJ, rho 0.25,
-                   T 1.5, rc 2.5.
+                   T 1.5, rc 2.5;
+* rigid_2clj_4000_energy: the per-step Upot, virial, sum m v^2 and sum I w^2 of 1000 steps
+                   (dt 0.001) of workloads.config_2clj(n_cells=10, temperature=1.5), 4,000
+                   molecules, with a checksum of the generated start (the energy drift of the
+                   reference's quaternion Leapfrog, which the device path must follow).
 
 Run from the repository root:
 
@@ -57,6 +61,23 @@ def main():
             upot=np.array([x["upot"] for x in sc]), virial=np.array([x["virial"] for x in sc]),
             summv2=np.array([x["summv2"] for x in sc]), sum_iw2=np.array([x["sum_iw2"] for x in sc]))
         print("wrote", f"{s.name}.npz")
+    s = energy_system()
+    out = O.run_reference(s, 1000)
+    sc = out["scalars"]
+    np.savez_compressed(os.path.join(OUT, "rigid_2clj_4000_energy.npz"), checksum=start_checksum(s),
+                        upot=np.array([x["upot"] for x in sc]), virial=np.array([x["virial"] for x in sc]),
+                        summv2=np.array([x["summv2"] for x in sc]), sum_iw2=np.array([x["sum_iw2"] for x in sc]))
+    print("wrote rigid_2clj_4000_energy.npz")
+
+
+def energy_system():
+    s = W.config_2clj(n_cells=10, temperature=1.5)
+    s.dt = 0.001
+    return s
+
+
+def start_checksum(s):
+    return np.array([s.r.sum(), s.v.sum(), s.q.sum(), s.D.sum(), float(s.n)])
 
 
 if __name__ == "__main__":

@@ -36,6 +36,17 @@ def golden_system(name):
     return s, d
 
 
+def energy_fixture():
+    """The 4,000-molecule two-centre start of tests/golden/make_rigid_golden.py (regenerated from its
+    seed, checked against the stored checksum) and the reference's 1000-step scalars."""
+    d = np.load(os.path.join(GOLDEN, "rigid_2clj_4000_energy.npz"))
+    s = W.config_2clj(n_cells=10, temperature=1.5)
+    s.dt = 0.001
+    got = np.array([s.r.sum(), s.v.sum(), s.q.sum(), s.D.sum(), float(s.n)])
+    np.testing.assert_allclose(got, d["checksum"], rtol=1e-13, atol=1e-9)
+    return s, d
+
+
 def rel(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
@@ -86,3 +97,8 @@ def test_rigid_phase_space_round_trip(tmp_path):
     w = R.rotate(s.q, s.D) * m.invI[s.cid]
     rot_dof = int(np.sum(m.I[s.cid] > 0))
     assert abs(float(np.sum(m.I[s.cid] * w * w)) - rot_dof * 1.0) < 1e-9
+
+
+def test_energy_fixture_start_is_reproducible():
+    s, d = energy_fixture()
+    assert s.n == 4000 and d["upot"].shape == (1001,)
