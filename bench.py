@@ -47,10 +47,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--skin", type=float, default=0.3,
                     help="Verlet skin of the step (0: cells and candidates rebuilt every step, as the reference)")
-    ap.add_argument("--workload", choices=["c2", "c3", "batched", "checkpoint"], default="c2",
+    ap.add_argument("--workload", choices=["c2", "c3", "batched", "checkpoint", "rigid"], default="c2",
                     help="c2: the 1M-molecule box (headline); c3: the 4M-molecule two-species slab; "
                          "batched: the 512-box ensemble; checkpoint: phase-space file write and read of the "
-                         "1M-molecule box through the C ABI")
+                         "1M-molecule box through the C ABI; rigid: a fluid of 1M two-centre LJ molecules")
     ap.add_argument("--boxes", type=int, default=512, help="boxes of the batched ensemble")
     ap.add_argument("--loop-steps", type=int, default=20,
                     help="steps of the loop-over-single-box comparison of the batched workload")
@@ -675,6 +675,149 @@ def run_checkpoint(args, dist: Dist):
     return out
 
 
+# ---------------------------------------------------------------------------- rigid molecules
+
+RIGID_METRIC = "LJ centre-pair interactions/s, 1M two-centre LJ molecules (2CLJ), 1 B200"
+RIGID_UNIT = "centre-pair interactions/s"
+# algorithmic flops per centre pair (FMA = 2): site distance 6, r^2 5, 1/r^2 1, s^2 1, s^6 2, s^12 1,
+# s^12-s^6 1, u 2, fac 3, f 3, virial drm.f 5, torque d x f 9, U 1
+FLOPS_PER_CENTRE_PAIR = 40
+
+
+def run_rigid(args, dist: Dist):
+    """Steps of a fluid of rigid two-centre LJ molecules (workloads.config_2clj: 4 fcc_cells^3
+    molecules, elongation 0.5, rho 0.3, T 2.0, rc 3.0 on the molecule centres, dt 0.002): Leapfrog with
+    quaternions, wrap and binning of the centres, site rotation, the centre-pair forces and torques,
+    closing kicks. Every step evaluates all centre pairs of every molecule pair within rc (4 here)."""
+    import torch
+
+    from madpac_b200 import mdgpu as M
+    from madpac_b200 import workloads as W
+
+    torch.cuda.set_device(dist.local)
+    system = W.config_2clj(seed=6 + dist.rank, n_cells=args.fcc_cells)
+    n = system.n
+    dt = system.dt
+    ncentre = 4   # centre pairs per molecule pair
+
+    def device_run(precision, steps, warmup):
+        lc = M.RigidLinkedCells.from_system(system, precision, device=dist.local)
+        lc.update()
+        lc.traversePairs()
+        lc.run(warmup, dt, record=False)
+        stream = torch.cuda.ExternalStream(lc.stream())
+        l0 = lc.launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        rec = lc.run(steps, dt)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) * 1e-3
+        launches = lc.launches() - l0
+        # kernel groups over a few more steps
+        lc.profileRead(reset=True)
+        lc.profileEnable(True)
+        kk = max(3, min(steps, 20))
+        krec = lc.run(kk, dt)
+        t, cnt = lc.profileRead(reset=True)
+        lc.profileEnable(False)
+        return lc, sec, rec, launches, t / kk, cnt, krec
+
+    clocks = ClockSampler(dist.local)
+    clocks.start()
+    lc, sec, rec, launches, groups_ms, cnt, krec = device_run(M.MIXED, args.steps, args.warmup)
+    clk = clocks.stop()
+    sec = dist.max(sec)
+    mol_pairs = float(rec[:, 4].sum())
+    value = dist.sum(mol_pairs * ncentre) / sec
+    fp32_peak, fp64_peak = M.device_peaks(dist.local)
+    pair_ms = float(groups_ms[1])
+    pairs_per_step = float(krec[:, 4].mean())
+    achieved = pairs_per_step * ncentre * FLOPS_PER_CENTRE_PAIR / (pair_ms * 1e-3) / 1e12
+
+    # e2e: host arrays in (id, cid, r, v, q, D), one run of `steps` steps, the final state out
+    st = lc.getParticles()
+    pin = lambda shape, dt_=np.float64: torch.empty(shape, dtype=getattr(torch, np.dtype(dt_).name),  # noqa: E731
+                                                    pin_memory=True).numpy()
+    hr, hv, hq, hD = pin((n, 3)), pin((n, 3)), pin((n, 4)), pin((n, 3))
+    hr[:], hv[:], hq[:], hD[:] = st["r"], st["v"], st["q"], st["D"]
+    e2e_steps = max(3, args.steps // 2)
+    stream = torch.cuda.ExternalStream(lc.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    lc.addParticles(st["id"], st["cid"], hr, hv, hq, hD)
+    lc.update()
+    lc.traversePairs()
+    erec = lc.run(e2e_steps, dt)
+    out_state = lc.getParticles()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_sec = e0.elapsed_time(e1) * 1e-3
+    e2e_value = float(erec[:, 4].sum()) * ncentre / e2e_sec
+    h2d = n * (8 + 4 + 8 * 14)
+    d2h = n * (8 + 4 + 8 * 22) + 40 * e2e_steps
+    del out_state
+    lc.close()
+
+    # the FP64 form of the same steps
+    fp64 = None
+    if not args.no_compare:
+        lc64, sec64, rec64, *_ = device_run(M.FP64, args.steps, args.warmup)
+        sec64 = dist.max(sec64)
+        fp64 = {"value": dist.sum(float(rec64[:, 4].sum()) * ncentre) / sec64, "ms_per_step": sec64 / args.steps * 1e3}
+        lc64.close()
+
+    out = {
+        "metric": RIGID_METRIC, "value": value, "unit": RIGID_UNIT, "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 centre-pair arithmetic, f64 accumulation",
+        "data": "synthetic (seeded FCC lattice of molecule centres, random orientations, Maxwell-Boltzmann "
+                "translational and rotational velocities)",
+        "config": {"workload": f"rigid_2clj_{n}", "n_molecules": n, "centres_per_molecule": 2, "elongation": 0.5,
+                   "density": 0.3, "temperature": 2.0, "cutoff": float(system.cutoff), "dt": dt, "ensemble": "NVE",
+                   "potential": "2CLJ, LJ 12-6 truncated-shifted per centre pair, cutoff on the molecule centres",
+                   "pair_search": "cells rebuilt and candidates searched every step",
+                   "l2": f"not flushed: each step reads the whole state ({n * 230 / 1e6:.0f} MB of molecule arrays, "
+                         "above the 126 MB L2)"},
+        "molecule_pairs_per_step": mol_pairs / args.steps,
+        "timing": "CUDA events on the library stream around one mdgpu_rigid_run of the timed steps",
+        "gpu_launches": int(launches),
+        "kernel_ms_per_step": {"binning": float(groups_ms[0]), "site_rotation_and_pairs": pair_ms,
+                               "integration": float(groups_ms[2])},
+        "roofline": {"bound": "fp32", "kernel": "site rotation + centre-pair forces", "achieved": achieved,
+                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                     "peak_source": "measured FMA microbenchmark (mdgpu_device_peaks)",
+                     "flops_per_centre_pair": FLOPS_PER_CENTRE_PAIR,
+                     "timed": "k_rigid_sites + k_rigid_pairs per step, CUDA events on the library stream"},
+        "fp64": fp64,
+        "speedup_vs_fp64": (value / fp64["value"]) if fp64 else None,
+        "e2e": {"value": e2e_value, "unit": RIGID_UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
+                "d2h_bytes_per_step": d2h / e2e_steps,
+                "note": f"one upload of id, cid, r, v, q, D and one download of the final state per run of "
+                        f"{e2e_steps} steps, plus the step records"},
+        "clocks": clk,
+    }
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline and os.path.exists(ref):
+        tmp = tempfile.mkdtemp(prefix="mdrig_")
+        W.write_inp(system, os.path.join(tmp, "sys.inp"))
+        W.write_cfg(system, os.path.join(tmp, "sys.cfg"), "sys.inp")
+        probe = subprocess.run([ref, "--time", "sys.cfg", "1"], cwd=tmp, capture_output=True, text=True, timeout=900)
+        t1 = json.loads(probe.stdout.strip().splitlines()[-1])["seconds_per_step"]
+        k = max(1, min(args.steps, int(args.cpu_seconds / max(t1, 1e-3))))
+        r = subprocess.run([ref, "--time", "sys.cfg", str(k)], cwd=tmp, capture_output=True, text=True, timeout=900)
+        secs = json.loads(r.stdout.strip().splitlines()[-1])["seconds_per_step"]
+        out["cpu_baseline"] = {"value": float(rec[0, 4]) * ncentre / secs, "unit": RIGID_UNIT, "cores": 1,
+                               "kind": "reference", "seconds_per_step": secs,
+                               "sample": f"{k} steps of the full {n}-molecule box (bounded to ~{args.cpu_seconds:g} s) "
+                                         "after prepare_start and one untimed probe step, single-threaded"}
+        shutil.rmtree(tmp, ignore_errors=True)
+    return out
+
+
 # ---------------------------------------------------------------------------- reference arm
 
 def run_reference(args, dist: Dist):
@@ -742,6 +885,8 @@ def main():
         out = run_batched(args, dist)
     elif args.workload == "checkpoint":
         out = run_checkpoint(args, dist)
+    elif args.workload == "rigid":
+        out = run_rigid(args, dist)
     else:
         out = run_ours(args, dist)
     if dist.rank == 0:

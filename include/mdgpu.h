@@ -298,8 +298,10 @@ int mdgpu_rigid_leapfrog_post(mdgpu_rigid* h, double dt_half, double* summv2, do
  * per_step (may be NULL): 5 doubles per step {Upot, virial, sum m v^2, sum I w^2, pairs}. */
 int mdgpu_rigid_run(mdgpu_rigid* h, int32_t nsteps, double dt, double* per_step);
 int mdgpu_rigid_get_stream(const mdgpu_rigid* h, void** stream);
-/* Kernel launches enqueued by the context so far. */
-int mdgpu_rigid_profile(mdgpu_rigid* h, int64_t* launches);
+/* Kernel timing of the context, as mdgpu_profile_enable / mdgpu_profile_read (groups: binning,
+ * site rotation + pairs, integration; counts[3] = all launches so far). */
+int mdgpu_rigid_profile_enable(mdgpu_rigid* h, int enable);
+int mdgpu_rigid_profile_read(mdgpu_rigid* h, double times_ms[3], int64_t counts[4], int reset);
 
 #ifdef __cplusplus
 }

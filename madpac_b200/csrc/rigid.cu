@@ -14,18 +14,19 @@
 // * k_rigid_pairs: the LJ block of PotForce (molecules/potforce.h:319-363) for every molecule pair
 //   whose centres are closer than rc (strict, particleContainer/BlockTraverse.cpp:155), every centre
 //   pair evaluated when dd < rcLJ^2: drs = (drm + d_i) - d_j (SiteSiteDistance, potforce.h:26-31),
-//   PotForceLJ (potforce.h:41-53), u += shift6, Upot6LJ += u, Virial += drm.f; the molecule's force
-//   is the sum of its centres' forces and its torque M = sum d x f (Molecule::calcFM,
-//   Molecule.cpp:386-411). One thread per molecule gathers over the 27 cells around it (each pair
-//   seen from both sides, halved at the end: no atomics, the same sums run to run), the site-pair
-//   parameters of Comp2Param::initialize (molecules/Comp2Param.cpp:28-115) in shared memory;
+//   PotForceLJ (potforce.h:41-53), u += shift6, Upot6LJ += u, Virial += drm.f; forces summed per
+//   centre, the molecule's force and torque formed from them as Molecule::calcFM does
+//   (Molecule.cpp:386-411). One thread per molecule gathers over the 27 cells around it (each pair
+//   seen from both sides, halved at the end: no atomics, the same sums run to run), first listing
+//   the accepted partners, then evaluating them; the site-pair parameters of Comp2Param::initialize
+//   (molecules/Comp2Param.cpp:28-115) in shared memory;
 // * k_rigid_pre / k_rigid_post: Molecule::upd_preF and upd_postF (Molecule.cpp:128-159, 193-216)
 //   with the quaternion algebra of Quaternion.cpp (rotate, differentiate, normalisation) and the
 //   sums m v^2 and I w^2 of Leapfrog::transition2to3 (integrators/Leapfrog.cpp:52-99).
 //
 // MDGPU_FP64 evaluates everything in double with the reference's operation order and no
-// contraction; MDGPU_MIXED evaluates each centre pair's LJ terms in float from the double site
-// distance and accumulates forces, torques, energy and virial in double.
+// contraction; MDGPU_MIXED evaluates the centre pairs of a molecule pair in float (from the double
+// centre distance) and adds their sums to double accumulators once per molecule pair.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -179,7 +180,32 @@ struct RigidOut {
 	int* status;
 };
 
-// One thread per sorted molecule i: force and torque from every molecule of the 27 cells around it.
+// Lanes per molecule of the pair kernel (consecutive lanes; a warp holds 16 consecutive molecules of
+// the cell order, about two cells, so its lanes walk mostly the same candidate cells), and the
+// accepted partners each lane lists per pass, in shared memory (one column per thread; the static
+// 48 KB bounds the depth). Measured on the 1M-molecule 2CLJ fluid: 2 lanes 2.21 ms per step, 4 lanes
+// 2.69, 8 lanes 3.46, 1 lane (40 entries, which the FCC start's 42 partners overflow) 11.9.
+#ifndef MDGPU_RIGID_LANES
+#define MDGPU_RIGID_LANES 2
+#endif
+#ifndef MDGPU_RIGID_LIST
+#define MDGPU_RIGID_LIST 32
+#endif
+constexpr int kRigidLanes = MDGPU_RIGID_LANES;
+constexpr int kRigidList = MDGPU_RIGID_LIST;
+static_assert(kRigidLanes == 1 || kRigidLanes == 2 || kRigidLanes == 4 || kRigidLanes == 8, "lanes per molecule");
+
+// kRigidLanes lanes per sorted molecule i: force and torque from every molecule of the 27 cells
+// around it (lane k of the molecule takes every kRigidLanes-th candidate of each cell), in two
+// phases so that the centre-pair arithmetic runs with the warp's lanes busy:
+//   scan:     every candidate j is tested against rc (the exact double test of the reference); the
+//             accepted ones within rcLJ go to the lane's list as j << 5 | image (the periodic image
+//             of j's cell, 27 codes);
+//   evaluate: the list's molecule pairs, every centre pair of each (a pass is evaluated early when
+//             the list fills).
+// Forces are summed per centre of i, the lanes' sums combined in a fixed order (butterfly), and the
+// torque formed at the end as calcFM does (M = sum_s d_s x F_s); the virial term of a molecule pair
+// is drm . (sum of its centre forces).
 template <bool kMixed, int NS>
 __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const double* __restrict__ rx,
                                                                const double* __restrict__ ry,
@@ -192,6 +218,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 	constexpr int TT = kMaxSiteTotal * kMaxSiteTotal;
 	__shared__ double s_e24[TT], s_sig2[TT], s_sh6[TT];
 	__shared__ int s_ns[kMaxSpecies], s_base[kMaxSpecies];
+	__shared__ uint32_t s_list[kRigidList * kRigidThreads];
 	for (int k = threadIdx.x; k < TT; k += blockDim.x) {
 		s_e24[k] = P->eps24[k];
 		s_sig2[k] = P->sig2[k];
@@ -203,19 +230,129 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 	}
 	__syncthreads();
 	const double rc2 = P->rc2, rclj2 = P->rclj2;
-	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
-	double F[3] = {0.0, 0.0, 0.0}, Mt[3] = {0.0, 0.0, 0.0};
+	const int64_t i = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) / kRigidLanes;
+	const int sub = (int) (threadIdx.x % kRigidLanes);
+	double Fs[NS][3];
+#pragma unroll
+	for (int s = 0; s < NS; s++) Fs[s][0] = Fs[s][1] = Fs[s][2] = 0.0;
 	double U = 0.0, W = 0.0, np = 0.0;
 	bool same = false;
+	double di[NS][3];
+	int nsi = 0;
 	if (i < n) {
 		const double xi = rx[i], yi = ry[i], zi = rz[i];
 		const int ci = cid[i];
-		const int nsi = s_ns[ci], bi = s_base[ci];
-		double di[NS][3];
+		nsi = s_ns[ci];
+		const int bi = s_base[ci];
 #pragma unroll
 		for (int s = 0; s < NS; s++)
 #pragma unroll
 			for (int k = 0; k < 3; k++) di[s][k] = s < nsi ? ds[(int64_t) (s * 3 + k) * n + i] : 0.0;
+		uint32_t* list = s_list + threadIdx.x;
+		int cnt = 0;
+
+		// the molecule pairs of the list: every centre pair of each
+		auto evaluate = [&]() {
+			for (int e = 0; e < cnt; e++) {
+				const uint32_t code = list[e * kRigidThreads];
+				const int j = (int) (code >> 5);
+				const int img = (int) (code & 31u);
+				const double sx = (double) (img % 3 - 1) * g.L[0];
+				const double sy = (double) ((img / 3) % 3 - 1) * g.L[1];
+				const double sz = (double) (img / 9 - 1) * g.L[2];
+				const double m0 = __dsub_rn(xi, __dadd_rn(rx[j], sx));
+				const double m1 = __dsub_rn(yi, __dadd_rn(ry[j], sy));
+				const double m2 = __dsub_rn(zi, __dadd_rn(rz[j], sz));
+				const int cj = cid[j];
+				const int nsj = s_ns[cj], bj = s_base[cj];
+				double fp0 = 0.0, fp1 = 0.0, fp2 = 0.0;   // force of this molecule pair
+				if (!kMixed) {
+#pragma unroll
+					for (int sj = 0; sj < NS; sj++) {
+						if (sj >= nsj) break;
+						const double dj0 = ds[(int64_t) (sj * 3 + 0) * n + j];
+						const double dj1 = ds[(int64_t) (sj * 3 + 1) * n + j];
+						const double dj2 = ds[(int64_t) (sj * 3 + 2) * n + j];
+#pragma unroll
+						for (int si = 0; si < NS; si++) {
+							if (si >= nsi) break;
+							const int pk = (bi + si) * kMaxSiteTotal + bj + sj;
+							// SiteSiteDistance: drs = drm + d_i - d_j
+							const double s0 = __dsub_rn(__dadd_rn(m0, di[si][0]), dj0);
+							const double s1 = __dsub_rn(__dadd_rn(m1, di[si][1]), dj1);
+							const double s2 = __dsub_rn(__dadd_rn(m2, di[si][2]), dj2);
+							const double dr2 =
+							    __dadd_rn(__dadd_rn(__dmul_rn(s0, s0), __dmul_rn(s1, s1)), __dmul_rn(s2, s2));
+							const double eps24 = s_e24[pk];
+							const double invdr2 = __ddiv_rn(1.0, dr2);
+							double lj6 = __dmul_rn(s_sig2[pk], invdr2);
+							lj6 = __dmul_rn(__dmul_rn(lj6, lj6), lj6);
+							const double lj12 = __dmul_rn(lj6, lj6);
+							const double lj12m6 = __dsub_rn(lj12, lj6);
+							U = __dadd_rn(U, __dadd_rn(__dmul_rn(eps24, lj12m6), s_sh6[pk]));
+							const double fac = __dmul_rn(__dmul_rn(eps24, __dadd_rn(lj12, lj12m6)), invdr2);
+							const double f0 = __dmul_rn(fac, s0), f1 = __dmul_rn(fac, s1), f2 = __dmul_rn(fac, s2);
+							Fs[si][0] = __dadd_rn(Fs[si][0], f0);
+							Fs[si][1] = __dadd_rn(Fs[si][1], f1);
+							Fs[si][2] = __dadd_rn(Fs[si][2], f2);
+							fp0 = __dadd_rn(fp0, f0);
+							fp1 = __dadd_rn(fp1, f1);
+							fp2 = __dadd_rn(fp2, f2);
+						}
+					}
+				} else {
+					const float e0 = (float) m0, e1 = (float) m1, e2 = (float) m2;
+					float fs[NS][3];
+#pragma unroll
+					for (int si = 0; si < NS; si++) fs[si][0] = fs[si][1] = fs[si][2] = 0.0f;
+					float uf = 0.0f;
+					double sh = 0.0;
+#pragma unroll
+					for (int sj = 0; sj < NS; sj++) {
+						if (sj >= nsj) break;
+						const float dj0 = (float) ds[(int64_t) (sj * 3 + 0) * n + j];
+						const float dj1 = (float) ds[(int64_t) (sj * 3 + 1) * n + j];
+						const float dj2 = (float) ds[(int64_t) (sj * 3 + 2) * n + j];
+#pragma unroll
+						for (int si = 0; si < NS; si++) {
+							if (si >= nsi) break;
+							const int pk = (bi + si) * kMaxSiteTotal + bj + sj;
+							const float s0 = e0 + (float) di[si][0] - dj0;
+							const float s1 = e1 + (float) di[si][1] - dj1;
+							const float s2 = e2 + (float) di[si][2] - dj2;
+							const float dr2 = s0 * s0 + s1 * s1 + s2 * s2;
+							const float eps24 = (float) s_e24[pk];
+							const float inv = __fdividef(1.0f, dr2);
+							const float q2 = (float) s_sig2[pk] * inv;
+							const float q6 = q2 * q2 * q2;
+							const float q12 = q6 * q6;
+							const float qm = q12 - q6;
+							const float fac = eps24 * (q12 + qm) * inv;
+							uf += eps24 * qm;
+							sh += s_sh6[pk];
+							fs[si][0] += fac * s0;
+							fs[si][1] += fac * s1;
+							fs[si][2] += fac * s2;
+						}
+					}
+					U += (double) uf + sh;
+#pragma unroll
+					for (int si = 0; si < NS; si++) {
+						if (si >= nsi) break;
+						Fs[si][0] += (double) fs[si][0];
+						Fs[si][1] += (double) fs[si][1];
+						Fs[si][2] += (double) fs[si][2];
+						fp0 += (double) fs[si][0];
+						fp1 += (double) fs[si][1];
+						fp2 += (double) fs[si][2];
+					}
+				}
+				// Virial += drm . f over the molecule pair's centre pairs
+				W = __dadd_rn(W, __dadd_rn(__dadd_rn(__dmul_rn(m0, fp0), __dmul_rn(m1, fp1)), __dmul_rn(m2, fp2)));
+			}
+			cnt = 0;
+		};
+
 		int cc[3];
 		const double r[3] = {xi, yi, zi};
 		for (int d = 0; d < 3; d++) {
@@ -223,114 +360,87 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 			cc[d] = c < 0 ? 0 : (c >= g.nc[d] ? g.nc[d] - 1 : c);
 		}
 		for (int dz = -1; dz <= 1; dz++) {
-			int z = cc[2] + dz;
-			double sz = 0.0;
+			int z = cc[2] + dz, iz = 1;
 			if (z < 0) {
 				z += g.nc[2];
-				sz = -g.L[2];
+				iz = 0;
 			} else if (z >= g.nc[2]) {
 				z -= g.nc[2];
-				sz = g.L[2];
+				iz = 2;
 			}
+			const double sz = (double) (iz - 1) * g.L[2];
 			for (int dy = -1; dy <= 1; dy++) {
-				int y = cc[1] + dy;
-				double sy = 0.0;
+				int y = cc[1] + dy, iy = 1;
 				if (y < 0) {
 					y += g.nc[1];
-					sy = -g.L[1];
+					iy = 0;
 				} else if (y >= g.nc[1]) {
 					y -= g.nc[1];
-					sy = g.L[1];
+					iy = 2;
 				}
+				const double sy = (double) (iy - 1) * g.L[1];
 				for (int dx = -1; dx <= 1; dx++) {
-					int x = cc[0] + dx;
-					double sx = 0.0;
+					int x = cc[0] + dx, ix = 1;
 					if (x < 0) {
 						x += g.nc[0];
-						sx = -g.L[0];
+						ix = 0;
 					} else if (x >= g.nc[0]) {
 						x -= g.nc[0];
-						sx = g.L[0];
+						ix = 2;
 					}
+					const double sx = (double) (ix - 1) * g.L[0];
+					const uint32_t img = (uint32_t) (ix + 3 * iy + 9 * iz);
+					const bool shifted = img != 13u;
 					const int nb = (z * g.nc[1] + y) * g.nc[0] + x;
-					const bool shifted = (sx != 0.0) || (sy != 0.0) || (sz != 0.0);
 					const int j0 = start[nb], j1 = start[nb + 1];
-					for (int j = j0; j < j1; j++) {
+					for (int j = j0 + sub; j < j1; j += kRigidLanes) {
 						if (j == i && !shifted) continue;
-						double xj = rx[j], yj = ry[j], zj = rz[j];
-						if (shifted) {   // the halo image of j (DomainDecompDummy.cpp:64-70, 93-99)
-							xj = __dadd_rn(xj, sx);
-							yj = __dadd_rn(yj, sy);
-							zj = __dadd_rn(zj, sz);
-						}
-						const double m0 = __dsub_rn(xi, xj), m1 = __dsub_rn(yi, yj), m2 = __dsub_rn(zi, zj);
+						// the halo image of j (DomainDecompDummy.cpp:64-70, 93-99); adding 0 is exact
+						const double m0 = __dsub_rn(xi, __dadd_rn(rx[j], sx));
+						const double m1 = __dsub_rn(yi, __dadd_rn(ry[j], sy));
+						const double m2 = __dsub_rn(zi, __dadd_rn(rz[j], sz));
 						const double dd =
 						    __dadd_rn(__dadd_rn(__dmul_rn(m0, m0), __dmul_rn(m1, m1)), __dmul_rn(m2, m2));
 						if (!(dd < rc2)) continue;
 						np += 1.0;
 						if (dd == 0.0) same = true;
 						if (!(dd < rclj2)) continue;
-						const int cj = cid[j];
-						const int nsj = s_ns[cj], bj = s_base[cj];
-#pragma unroll
-						for (int sj = 0; sj < NS; sj++) {
-							if (sj >= nsj) break;
-							const double dj0 = ds[(int64_t) (sj * 3 + 0) * n + j];
-							const double dj1 = ds[(int64_t) (sj * 3 + 1) * n + j];
-							const double dj2 = ds[(int64_t) (sj * 3 + 2) * n + j];
-#pragma unroll
-							for (int si = 0; si < NS; si++) {
-								if (si >= nsi) break;
-								const int pk = (bi + si) * kMaxSiteTotal + bj + sj;
-								// SiteSiteDistance: drs = drm + d_i - d_j
-								const double s0 = __dsub_rn(__dadd_rn(m0, di[si][0]), dj0);
-								const double s1 = __dsub_rn(__dadd_rn(m1, di[si][1]), dj1);
-								const double s2 = __dsub_rn(__dadd_rn(m2, di[si][2]), dj2);
-								double f0, f1, f2;
-								if (!kMixed) {
-									const double dr2 = __dadd_rn(__dadd_rn(__dmul_rn(s0, s0), __dmul_rn(s1, s1)),
-									                             __dmul_rn(s2, s2));
-									const double eps24 = s_e24[pk];
-									const double invdr2 = __ddiv_rn(1.0, dr2);
-									double lj6 = __dmul_rn(s_sig2[pk], invdr2);
-									lj6 = __dmul_rn(__dmul_rn(lj6, lj6), lj6);
-									const double lj12 = __dmul_rn(lj6, lj6);
-									const double lj12m6 = __dsub_rn(lj12, lj6);
-									U = __dadd_rn(U, __dadd_rn(__dmul_rn(eps24, lj12m6), s_sh6[pk]));
-									const double fac = __dmul_rn(__dmul_rn(eps24, __dadd_rn(lj12, lj12m6)), invdr2);
-									f0 = __dmul_rn(fac, s0);
-									f1 = __dmul_rn(fac, s1);
-									f2 = __dmul_rn(fac, s2);
-								} else {
-									const float e0 = (float) s0, e1 = (float) s1, e2 = (float) s2;
-									const float dr2 = e0 * e0 + e1 * e1 + e2 * e2;
-									const float eps24 = (float) s_e24[pk];
-									const float inv = __fdividef(1.0f, dr2);
-									const float q2 = (float) s_sig2[pk] * inv;
-									const float q6 = q2 * q2 * q2;
-									const float q12 = q6 * q6;
-									const float qm = q12 - q6;
-									const float fac = eps24 * (q12 + qm) * inv;
-									U += (double) (eps24 * qm) + s_sh6[pk];
-									f0 = (double) (fac * e0);
-									f1 = (double) (fac * e1);
-									f2 = (double) (fac * e2);
-								}
-								F[0] = __dadd_rn(F[0], f0);
-								F[1] = __dadd_rn(F[1], f1);
-								F[2] = __dadd_rn(F[2], f2);
-								// M += d_i x f (Molecule::calcFM)
-								Mt[0] = __dadd_rn(Mt[0], __dsub_rn(__dmul_rn(di[si][1], f2), __dmul_rn(di[si][2], f1)));
-								Mt[1] = __dadd_rn(Mt[1], __dsub_rn(__dmul_rn(di[si][2], f0), __dmul_rn(di[si][0], f2)));
-								Mt[2] = __dadd_rn(Mt[2], __dsub_rn(__dmul_rn(di[si][0], f1), __dmul_rn(di[si][1], f0)));
-								// Virial += drm . f
-								W = __dadd_rn(W, __dadd_rn(__dadd_rn(__dmul_rn(m0, f0), __dmul_rn(m1, f1)),
-								                           __dmul_rn(m2, f2)));
-							}
-						}
+						list[cnt * kRigidThreads] = ((uint32_t) j << 5) | img;
+						if (++cnt == kRigidList) evaluate();
 					}
 				}
 			}
+		}
+		evaluate();
+	} else {
+#pragma unroll
+		for (int s = 0; s < NS; s++) di[s][0] = di[s][1] = di[s][2] = 0.0;
+	}
+	// the molecule's lanes combine their sums (the same order in every lane)
+	__syncwarp();
+#pragma unroll
+	for (int o2 = 1; o2 < kRigidLanes; o2 <<= 1) {
+#pragma unroll
+		for (int s = 0; s < NS; s++)
+#pragma unroll
+			for (int k = 0; k < 3; k++) Fs[s][k] = __dadd_rn(Fs[s][k], __shfl_xor_sync(0xffffffffu, Fs[s][k], o2));
+		U = __dadd_rn(U, __shfl_xor_sync(0xffffffffu, U, o2));
+		W = __dadd_rn(W, __shfl_xor_sync(0xffffffffu, W, o2));
+		np += __shfl_xor_sync(0xffffffffu, np, o2);
+	}
+	if (sub != 0) U = W = np = 0.0;
+	if (i < n && sub == 0) {
+		double F[3] = {0.0, 0.0, 0.0}, Mt[3] = {0.0, 0.0, 0.0};
+		// Molecule::calcFM: F = sum F_s, M = sum d_s x F_s
+#pragma unroll
+		for (int s = 0; s < NS; s++) {
+			if (s >= nsi) break;
+			F[0] = __dadd_rn(F[0], Fs[s][0]);
+			F[1] = __dadd_rn(F[1], Fs[s][1]);
+			F[2] = __dadd_rn(F[2], Fs[s][2]);
+			Mt[0] = __dadd_rn(Mt[0], __dsub_rn(__dmul_rn(di[s][1], Fs[s][2]), __dmul_rn(di[s][2], Fs[s][1])));
+			Mt[1] = __dadd_rn(Mt[1], __dsub_rn(__dmul_rn(di[s][2], Fs[s][0]), __dmul_rn(di[s][0], Fs[s][2])));
+			Mt[2] = __dadd_rn(Mt[2], __dsub_rn(__dmul_rn(di[s][0], Fs[s][1]), __dmul_rn(di[s][1], Fs[s][0])));
 		}
 		o.fx[i] = F[0];
 		o.fy[i] = F[1];
@@ -473,6 +583,7 @@ struct mdgpu_rigid {
 	double* M = nullptr;        // 3 x cap
 	double* ds = nullptr;       // 3 x ns_max x cap, sorted order
 	double* stage = nullptr;    // 4 x cap host <-> device staging
+	double* partials = nullptr; // per-block reduction partials (4 doubles per block of the pair kernel)
 	double* scal = nullptr;     // [0..2] pair sums, [3..4] kinetic sums
 	double* steps = nullptr;    // 5 doubles per step of mdgpu_rigid_run
 	int64_t steps_cap = 0;
@@ -495,12 +606,14 @@ int launch_rigid_forces(mdgpu_rigid* h) {
 	Context* c = ctx_of(h);
 	const int64_t n = c->n;
 	const unsigned nb = (unsigned) nblocks(n);
+	const unsigned nbp = (unsigned) nblocks(n * kRigidLanes);
+	prof_begin(c, 1);
 	k_rigid_sites<<<nb, kRigidThreads, 0, c->stream>>>(n, c->p.uidx, c->p.cid, h->q, h->dp, h->ds);
-	RigidOut o{c->p.fx, c->p.fy, c->p.fz, h->M, c->partials, h->tickets, h->scal, c->status};
+	RigidOut o{c->p.fx, c->p.fy, c->p.fz, h->M, h->partials, h->tickets, h->scal, c->status};
 	const bool mixed = c->precision == MDGPU_MIXED;
 	const int ns = h->hp.ns_max;
 #define RG_PAIRS(MX, NSV)                                                                                   \
-	k_rigid_pairs<MX, NSV><<<nb, kRigidThreads, 0, c->stream>>>(n, c->p.rx, c->p.ry, c->p.rz, c->p.cid,     \
+	k_rigid_pairs<MX, NSV><<<nbp, kRigidThreads, 0, c->stream>>>(n, c->p.rx, c->p.ry, c->p.rz, c->p.cid,     \
 	                                                            c->p.uidx, c->cell_start, c->g, h->dp, h->ds, o)
 	if (ns <= 1)
 		mixed ? RG_PAIRS(true, 1) : RG_PAIRS(false, 1);
@@ -513,7 +626,7 @@ int launch_rigid_forces(mdgpu_rigid* h) {
 	else
 		mixed ? RG_PAIRS(true, kMaxSites) : RG_PAIRS(false, kMaxSites);
 #undef RG_PAIRS
-	count_launches(c, 2);
+	prof_end(c, 1, 2);
 	RG_CUDA(cudaGetLastError());
 	return MDGPU_OK;
 }
@@ -526,17 +639,19 @@ RigidState state_of(mdgpu_rigid* h) {
 
 int launch_rigid_pre(mdgpu_rigid* h, double dt, double vcorr, double Dcorr) {
 	Context* c = ctx_of(h);
+	prof_begin(c, 2);
 	k_rigid_pre<<<(unsigned) nblocks(c->n), kRigidThreads, 0, c->stream>>>(c->n, state_of(h), h->dp, dt, vcorr, Dcorr);
-	count_launches(c, 1);
+	prof_end(c, 2, 1);
 	RG_CUDA(cudaGetLastError());
 	return MDGPU_OK;
 }
 
 int launch_rigid_post(mdgpu_rigid* h, double dt_half, double* record) {
 	Context* c = ctx_of(h);
+	prof_begin(c, 2);
 	k_rigid_post<<<(unsigned) nblocks(c->n), kRigidThreads, 0, c->stream>>>(
-	    c->n, state_of(h), h->dp, dt_half, c->partials, h->tickets + 1, h->scal + 3, h->scal, record, c->status);
-	count_launches(c, 1);
+	    c->n, state_of(h), h->dp, dt_half, h->partials, h->tickets + 1, h->scal + 3, h->scal, record, c->status);
+	prof_end(c, 2, 1);
 	RG_CUDA(cudaGetLastError());
 	return MDGPU_OK;
 }
@@ -633,13 +748,15 @@ int ensure_capacity(mdgpu_rigid* h, int64_t n) {
 	cudaFree(h->M);
 	cudaFree(h->ds);
 	cudaFree(h->stage);
-	h->q = h->D = h->M = h->ds = h->stage = nullptr;
+	cudaFree(h->partials);
+	h->q = h->D = h->M = h->ds = h->stage = h->partials = nullptr;
 	h->cap = 0;
 	RG_CUDA(cudaMalloc(&h->q, sizeof(double) * 4 * n));
 	RG_CUDA(cudaMalloc(&h->D, sizeof(double) * 3 * n));
 	RG_CUDA(cudaMalloc(&h->M, sizeof(double) * 3 * n));
 	RG_CUDA(cudaMalloc(&h->ds, sizeof(double) * 3 * std::max(1, h->hp.ns_max) * n));
 	RG_CUDA(cudaMalloc(&h->stage, sizeof(double) * 4 * n));
+	RG_CUDA(cudaMalloc(&h->partials, sizeof(double) * 4 * nblocks(n * kRigidLanes)));
 	h->cap = n;
 	return MDGPU_OK;
 }
@@ -699,6 +816,7 @@ int mdgpu_rigid_destroy(mdgpu_rigid* h) {
 	cudaFree(h->M);
 	cudaFree(h->ds);
 	cudaFree(h->stage);
+	cudaFree(h->partials);
 	cudaFree(h->scal);
 	cudaFree(h->steps);
 	cudaFree(h->tickets);
@@ -730,6 +848,7 @@ int mdgpu_rigid_set_particles(mdgpu_rigid* h, int64_t n, const uint64_t* id, con
 	if (!h) return MDGPU_ERR_ARG;
 	Context* c = ctx_of(h);
 	if (!q || !D) return set_error(c, MDGPU_ERR_ARG, "q and D are required");
+	if (n > (int64_t(1) << 27)) return set_error(c, MDGPU_ERR_ARG, "at most 2^27 rigid molecules");
 	int st = mdgpu_set_particles(h->inner, n, id, cid, r, v, nullptr);
 	if (st) return st;
 	st = ensure_capacity(h, n);
@@ -850,10 +969,14 @@ int mdgpu_rigid_get_stream(const mdgpu_rigid* h, void** stream) {
 	return mdgpu_get_stream(h->inner, stream);
 }
 
-int mdgpu_rigid_profile(mdgpu_rigid* h, int64_t* launches) {
-	if (!h || !launches) return MDGPU_ERR_ARG;
-	*launches = h->inner->c.prof_count[3];
-	return MDGPU_OK;
+int mdgpu_rigid_profile_enable(mdgpu_rigid* h, int enable) {
+	if (!h) return MDGPU_ERR_ARG;
+	return mdgpu_profile_enable(h->inner, enable);
+}
+
+int mdgpu_rigid_profile_read(mdgpu_rigid* h, double times_ms[3], int64_t counts[4], int reset) {
+	if (!h) return MDGPU_ERR_ARG;
+	return mdgpu_profile_read(h->inner, times_ms, counts, reset);
 }
 
 }  // extern "C"

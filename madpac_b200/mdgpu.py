@@ -101,7 +101,8 @@ SIGNATURES = {
     "mdgpu_rigid_leapfrog_post": (_I, [_VP, _D, _VP, _VP]),
     "mdgpu_rigid_run": (_I, [_VP, _I32, _D, _VP]),
     "mdgpu_rigid_get_stream": (_I, [_VP, _VP]),
-    "mdgpu_rigid_profile": (_I, [_VP, _VP]),
+    "mdgpu_rigid_profile_enable": (_I, [_VP, _I]),
+    "mdgpu_rigid_profile_read": (_I, [_VP, _VP, _VP, _I]),
 }
 
 _lib = None
@@ -441,9 +442,17 @@ class RigidLinkedCells:
         return out
 
     def launches(self) -> int:
-        k = ctypes.c_int64()
-        self._check(self.lib.mdgpu_rigid_profile(self.h, ctypes.byref(k)))
-        return k.value
+        return int(self.profileRead()[1][3])
+
+    def profileEnable(self, enable: bool = True) -> None:
+        self._check(self.lib.mdgpu_rigid_profile_enable(self.h, 1 if enable else 0))
+
+    def profileRead(self, reset: bool = False):
+        """(ms per group [binning, site rotation + pairs, integration], launch counts [3 groups, all])."""
+        t = np.zeros(3)
+        cnt = np.zeros(4, dtype=np.int64)
+        self._check(self.lib.mdgpu_rigid_profile_read(self.h, _ptr(t), _ptr(cnt), 1 if reset else 0))
+        return t, cnt
 
     def stream(self) -> int:
         s = ctypes.c_void_p()
