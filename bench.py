@@ -52,6 +52,8 @@ def parse():
                          "batched: the 512-box ensemble; checkpoint: phase-space file write and read of the "
                          "1M-molecule box through the C ABI; rigid: a fluid of 1M two-centre LJ molecules")
     ap.add_argument("--boxes", type=int, default=512, help="boxes of the batched ensemble")
+    ap.add_argument("--charges", action="store_true",
+                    help="rigid workload: two-centre molecules with point charges +-0.5 (charge pairs besides LJ)")
     ap.add_argument("--loop-steps", type=int, default=20,
                     help="steps of the loop-over-single-box comparison of the batched workload")
     return ap.parse_args()
@@ -678,10 +680,13 @@ def run_checkpoint(args, dist: Dist):
 # ---------------------------------------------------------------------------- rigid molecules
 
 RIGID_METRIC = "LJ centre-pair interactions/s, 1M two-centre LJ molecules (2CLJ), 1 B200"
+RIGID_Q_METRIC = "site-pair interactions/s (LJ + charge pairs), 1M two-centre LJ molecules with point charges, 1 B200"
 RIGID_UNIT = "centre-pair interactions/s"
-# algorithmic flops per centre pair (FMA = 2): site distance 6, r^2 5, 1/r^2 1, s^2 1, s^6 2, s^12 1,
+# algorithmic flops per LJ centre pair (FMA = 2): site distance 6, r^2 5, 1/r^2 1, s^2 1, s^6 2, s^12 1,
 # s^12-s^6 1, u 2, fac 3, f 3, virial drm.f 5, torque d x f 9, U 1
 FLOPS_PER_CENTRE_PAIR = 40
+# per charge pair: site distance 6, r^2 5, 1/r^2 1, sqrt 1, u 2, fac 1, f 3, virial 5, torque 9, U 1
+FLOPS_PER_CHARGE_PAIR = 34
 
 
 def run_rigid(args, dist: Dist):
@@ -695,10 +700,10 @@ def run_rigid(args, dist: Dist):
     from madpac_b200 import workloads as W
 
     torch.cuda.set_device(dist.local)
-    system = W.config_2clj(seed=6 + dist.rank, n_cells=args.fcc_cells)
+    system = W.config_2clj(seed=6 + dist.rank, n_cells=args.fcc_cells, charged=args.charges)
     n = system.n
     dt = system.dt
-    ncentre = 4   # centre pairs per molecule pair
+    ncentre = 8 if args.charges else 4   # LJ centre pairs (+ charge pairs) per molecule pair
 
     def device_run(precision, steps, warmup):
         lc = M.RigidLinkedCells.from_system(system, precision, device=dist.local)
@@ -735,7 +740,8 @@ def run_rigid(args, dist: Dist):
     fp32_peak, fp64_peak = M.device_peaks(dist.local)
     pair_ms = float(groups_ms[1])
     pairs_per_step = float(krec[:, 4].mean())
-    achieved = pairs_per_step * ncentre * FLOPS_PER_CENTRE_PAIR / (pair_ms * 1e-3) / 1e12
+    flops_per_mol_pair = 4 * FLOPS_PER_CENTRE_PAIR + (4 * FLOPS_PER_CHARGE_PAIR if args.charges else 0)
+    achieved = pairs_per_step * flops_per_mol_pair / (pair_ms * 1e-3) / 1e12
 
     # e2e: host arrays in (id, cid, r, v, q, D), one run of `steps` steps, the final state out
     st = lc.getParticles()
@@ -771,14 +777,18 @@ def run_rigid(args, dist: Dist):
         lc64.close()
 
     out = {
-        "metric": RIGID_METRIC, "value": value, "unit": RIGID_UNIT, "n_gpus": dist.world, "steps": args.steps,
+        "metric": RIGID_Q_METRIC if args.charges else RIGID_METRIC, "value": value,
+        "unit": "site-pair interactions/s" if args.charges else RIGID_UNIT, "n_gpus": dist.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 centre-pair arithmetic, f64 accumulation",
         "data": "synthetic (seeded FCC lattice of molecule centres, random orientations, Maxwell-Boltzmann "
                 "translational and rotational velocities)",
-        "config": {"workload": f"rigid_2clj_{n}", "n_molecules": n, "centres_per_molecule": 2, "elongation": 0.5,
+        "config": {"workload": f"rigid_{system.name}", "n_molecules": n, "centres_per_molecule": 2,
+                   "charges_per_molecule": 2 if args.charges else 0, "elongation": 0.5,
                    "density": 0.3, "temperature": 2.0, "cutoff": float(system.cutoff), "dt": dt, "ensemble": "NVE",
-                   "potential": "2CLJ, LJ 12-6 truncated-shifted per centre pair, cutoff on the molecule centres",
+                   "potential": "2CLJ, LJ 12-6 truncated-shifted per centre pair" +
+                                (", point charges +-0.5 at z = +-0.35 (plain Coulomb)" if args.charges else "") +
+                                ", cutoff on the molecule centres",
                    "pair_search": "cells rebuilt and candidates searched every step",
                    "l2": f"not flushed: each step reads the whole state ({n * 230 / 1e6:.0f} MB of molecule arrays, "
                          "above the 126 MB L2)"},
@@ -790,7 +800,7 @@ def run_rigid(args, dist: Dist):
         "roofline": {"bound": "fp32", "kernel": "site rotation + centre-pair forces", "achieved": achieved,
                      "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
                      "peak_source": "measured FMA microbenchmark (mdgpu_device_peaks)",
-                     "flops_per_centre_pair": FLOPS_PER_CENTRE_PAIR,
+                     "flops_per_molecule_pair": flops_per_mol_pair,
                      "timed": "k_rigid_sites + k_rigid_pairs per step, CUDA events on the library stream"},
         "fp64": fp64,
         "speedup_vs_fp64": (value / fp64["value"]) if fp64 else None,

@@ -250,8 +250,8 @@ int mdgpu_batch_skin_builds(const mdgpu_batch* b, int64_t* builds);
  * (molecules/potforce.h:319-363), Molecule::upd_cache and calcFM (molecules/Molecule.cpp:161-190,
  * 386-411), and the rotational half of Molecule::upd_preF / upd_postF (Molecule.cpp:128-159,
  * 193-216). Arrays in the caller's order: r, v, F, D, M are (n, 3), q is (n, 4). */
-#define MDGPU_MAX_SITES 6         /* LJ centres per component */
-#define MDGPU_MAX_SITE_TOTAL 16   /* LJ centres over all components */
+#define MDGPU_MAX_SITES 6         /* LJ centres + charges per component */
+#define MDGPU_MAX_SITE_TOTAL 16   /* LJ centres + charges over all components */
 
 /* One LJ centre at r (principal-axes frame, the origin at the centre of mass), as read by
  * InputOldstyle (io/InputOldstyle.cpp:162-166) and added by Component::addLJcenter
@@ -264,15 +264,27 @@ typedef struct mdgpu_site {
 	int do_shift;
 } mdgpu_site;
 
+/* A point charge q at r with its mass (Component::addCharge, molecules/Component.cpp:115-133, read by
+ * InputOldstyle.cpp:167-171). Charge pairs of molecules within the cutoff interact by the plain
+ * Coulomb term of PotForce2Charge (molecules/potforce.h:244-253, 372-386), 4 pi eps0 = 1. */
+typedef struct mdgpu_charge {
+	double r[3];
+	double mass;
+	double q;
+} mdgpu_charge;
+
 typedef struct mdgpu_rigid mdgpu_rigid;
 
-/* nsites[c] centres for each component c, listed one component after another in `sites`;
- * inertia: 3 per component or NULL, values > 0 replace the principal moments computed from the
- * centres (the header's inertia line, InputOldstyle.cpp:188-195). Other arguments as mdgpu_create.
- * On failure *out may still be set (read mdgpu_rigid_last_error, then destroy it). */
+/* nsites[c] LJ centres (at least one) for each component c, listed one component after another in
+ * `sites`; ncharges[c] point charges in `charges` the same way (both may be NULL for none);
+ * MDGPU_MAX_SITES bounds centres + charges per component. inertia: 3 per component or NULL, values
+ * > 0 replace the principal moments computed from the centres and charges (the header's inertia
+ * line, InputOldstyle.cpp:188-195). Other arguments as mdgpu_create. On failure *out may still be
+ * set (read mdgpu_rigid_last_error, then destroy it). */
 int mdgpu_rigid_create(mdgpu_rigid** out, const double length[3], double cutoff, double lj_cutoff,
                        double cells_in_cutoff, int ncomp, const int32_t* nsites, const mdgpu_site* sites,
-                       const double* inertia, const double* mix, int precision, int device);
+                       const int32_t* ncharges, const mdgpu_charge* charges, const double* inertia,
+                       const double* mix, int precision, int device);
 int mdgpu_rigid_destroy(mdgpu_rigid* h);
 const char* mdgpu_rigid_last_error(const mdgpu_rigid* h);
 int mdgpu_rigid_set_precision(mdgpu_rigid* h, int precision);
@@ -286,9 +298,10 @@ int mdgpu_rigid_get_particles(mdgpu_rigid* h, int64_t n, uint64_t* id, int32_t* 
                               double* q, double* D, double* M);
 /* LinkedCells::update of the molecule centres (with the periodic wrap). */
 int mdgpu_rigid_update(mdgpu_rigid* h);
-/* Molecule::upd_cache for all molecules, LinkedCells::traversePairs with the LJ centre loop, and
- * Molecule::calcFM: F and M of every molecule, Upot = Upot6LJ/6, the virial sum drm.f and the
- * number of molecule pairs within the cutoff. */
+/* Molecule::upd_cache for all molecules, LinkedCells::traversePairs with the LJ centre loop and the
+ * charge pairs, and Molecule::calcFM: F and M of every molecule, Upot = Upot6LJ/6 + UpotXpoles
+ * (ParticlePairs2PotForceAdapter::finish), the virial sum drm.f and the number of molecule pairs
+ * within the cutoff. */
 int mdgpu_rigid_traverse_pairs(mdgpu_rigid* h, double* upot, double* virial, double* npairs);
 /* Molecule::upd_preF(dt, vcorr, Dcorr) for all molecules (Leapfrog::transition1to2). */
 int mdgpu_rigid_leapfrog_pre(mdgpu_rigid* h, double dt, double vcorr, double Dcorr);

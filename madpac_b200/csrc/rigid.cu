@@ -11,7 +11,8 @@
 // * k_rigid_sites: Molecule::upd_cache (molecules/Molecule.cpp:161-190): each centre's offset
 //   d = q.rotateinv(site) (Quaternion.cpp:50-66) once per force evaluation, stored per sorted
 //   molecule, centre-major (d[(s*3 + k)*n + i]);
-// * k_rigid_pairs: the LJ block of PotForce (molecules/potforce.h:319-363) for every molecule pair
+// * k_rigid_pairs: the LJ block and the charge-charge block of PotForce (molecules/potforce.h:319-386;
+//   PotForce2Charge, :244-253: u = q_i q_j sqrt(1/r^2), f = u/r^2 drs, UpotXpoles) for every molecule pair
 //   whose centres are closer than rc (strict, particleContainer/BlockTraverse.cpp:155), every centre
 //   pair evaluated when dd < rcLJ^2: drs = (drm + d_i) - d_j (SiteSiteDistance, potforce.h:26-31),
 //   PotForceLJ (potforce.h:41-53), u += shift6, Upot6LJ += u, Virial += drm.f; forces summed per
@@ -46,7 +47,9 @@ constexpr int kRigidThreads = kReduceBlock;
 // Site tables of a rigid context (device copy read by the kernels).
 struct RigidParams {
 	int nc, nsite_total, ns_max;
-	int nsites[kMaxSpecies];
+	int nsites[kMaxSpecies];               // LJ centres + charges of component c
+	int nlj[kMaxSpecies];                  // its LJ centres (sites 0..nlj-1; the charges follow)
+	double charge[kMaxSiteTotal];          // q of the charge sites (0 for LJ centres)
 	int base[kMaxSpecies];                 // first centre of component c in the site tables
 	double site[kMaxSiteTotal][3];         // body-frame centre positions
 	double mass[kMaxSpecies];
@@ -176,7 +179,7 @@ struct RigidOut {
 	double* M;          // caller order, M[k*n + u]
 	double* partials;
 	unsigned* ticket;
-	double* scalars;    // [0..2] = sum u (both sides), sum drm.f (both sides), pairs (both sides)
+	double* scalars;    // [0..3] = sum LJ u, sum drm.f, pairs, sum charge u (each pair from both sides)
 	int* status;
 };
 
@@ -206,7 +209,7 @@ static_assert(kRigidLanes == 1 || kRigidLanes == 2 || kRigidLanes == 4 || kRigid
 // Forces are summed per centre of i, the lanes' sums combined in a fixed order (butterfly), and the
 // torque formed at the end as calcFM does (M = sum_s d_s x F_s); the virial term of a molecule pair
 // is drm . (sum of its centre forces).
-template <bool kMixed, int NS>
+template <bool kMixed, int NS, bool kQ>
 __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const double* __restrict__ rx,
                                                                const double* __restrict__ ry,
                                                                const double* __restrict__ rz,
@@ -217,7 +220,8 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
                                                                const double* __restrict__ ds, RigidOut o) {
 	constexpr int TT = kMaxSiteTotal * kMaxSiteTotal;
 	__shared__ double s_e24[TT], s_sig2[TT], s_sh6[TT];
-	__shared__ int s_ns[kMaxSpecies], s_base[kMaxSpecies];
+	__shared__ int s_ns[kMaxSpecies], s_nlj[kMaxSpecies], s_base[kMaxSpecies];
+	__shared__ double s_q[kMaxSiteTotal];
 	__shared__ uint32_t s_list[kRigidList * kRigidThreads];
 	for (int k = threadIdx.x; k < TT; k += blockDim.x) {
 		s_e24[k] = P->eps24[k];
@@ -226,8 +230,10 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 	}
 	if (threadIdx.x < kMaxSpecies) {
 		s_ns[threadIdx.x] = P->nsites[threadIdx.x];
+		s_nlj[threadIdx.x] = P->nlj[threadIdx.x];
 		s_base[threadIdx.x] = P->base[threadIdx.x];
 	}
+	if (threadIdx.x < kMaxSiteTotal) s_q[threadIdx.x] = P->charge[threadIdx.x];
 	__syncthreads();
 	const double rc2 = P->rc2, rclj2 = P->rclj2;
 	const int64_t i = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) / kRigidLanes;
@@ -235,7 +241,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 	double Fs[NS][3];
 #pragma unroll
 	for (int s = 0; s < NS; s++) Fs[s][0] = Fs[s][1] = Fs[s][2] = 0.0;
-	double U = 0.0, W = 0.0, np = 0.0;
+	double U = 0.0, UX = 0.0, W = 0.0, np = 0.0;
 	bool same = false;
 	double di[NS][3];
 	int nsi = 0;
@@ -243,6 +249,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 		const double xi = rx[i], yi = ry[i], zi = rz[i];
 		const int ci = cid[i];
 		nsi = s_ns[ci];
+		const int nlji = s_nlj[ci];
 		const int bi = s_base[ci];
 #pragma unroll
 		for (int s = 0; s < NS; s++)
@@ -251,7 +258,8 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 		uint32_t* list = s_list + threadIdx.x;
 		int cnt = 0;
 
-		// the molecule pairs of the list: every centre pair of each
+		// the molecule pairs of the list: every LJ centre pair of each (within rcLJ) and every charge
+		// pair (PotForce2Charge, potforce.h:244-253)
 		auto evaluate = [&]() {
 			for (int e = 0; e < cnt; e++) {
 				const uint32_t code = list[e * kRigidThreads];
@@ -263,34 +271,47 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 				const double m0 = __dsub_rn(xi, __dadd_rn(rx[j], sx));
 				const double m1 = __dsub_rn(yi, __dadd_rn(ry[j], sy));
 				const double m2 = __dsub_rn(zi, __dadd_rn(rz[j], sz));
+				// without charges the list holds only partners within rcLJ
+				const bool lj =
+				    !kQ || __dadd_rn(__dadd_rn(__dmul_rn(m0, m0), __dmul_rn(m1, m1)), __dmul_rn(m2, m2)) < rclj2;
 				const int cj = cid[j];
-				const int nsj = s_ns[cj], bj = s_base[cj];
+				const int nsj = s_ns[cj], nljj = s_nlj[cj], bj = s_base[cj];
 				double fp0 = 0.0, fp1 = 0.0, fp2 = 0.0;   // force of this molecule pair
 				if (!kMixed) {
 #pragma unroll
 					for (int sj = 0; sj < NS; sj++) {
 						if (sj >= nsj) break;
+						const bool lj_j = !kQ || sj < nljj;
+						if (lj_j && !lj) continue;
 						const double dj0 = ds[(int64_t) (sj * 3 + 0) * n + j];
 						const double dj1 = ds[(int64_t) (sj * 3 + 1) * n + j];
 						const double dj2 = ds[(int64_t) (sj * 3 + 2) * n + j];
 #pragma unroll
 						for (int si = 0; si < NS; si++) {
 							if (si >= nsi) break;
-							const int pk = (bi + si) * kMaxSiteTotal + bj + sj;
+							if (kQ && (si < nlji) != lj_j) continue;   // LJ with LJ, charge with charge
 							// SiteSiteDistance: drs = drm + d_i - d_j
 							const double s0 = __dsub_rn(__dadd_rn(m0, di[si][0]), dj0);
 							const double s1 = __dsub_rn(__dadd_rn(m1, di[si][1]), dj1);
 							const double s2 = __dsub_rn(__dadd_rn(m2, di[si][2]), dj2);
 							const double dr2 =
 							    __dadd_rn(__dadd_rn(__dmul_rn(s0, s0), __dmul_rn(s1, s1)), __dmul_rn(s2, s2));
-							const double eps24 = s_e24[pk];
 							const double invdr2 = __ddiv_rn(1.0, dr2);
-							double lj6 = __dmul_rn(s_sig2[pk], invdr2);
-							lj6 = __dmul_rn(__dmul_rn(lj6, lj6), lj6);
-							const double lj12 = __dmul_rn(lj6, lj6);
-							const double lj12m6 = __dsub_rn(lj12, lj6);
-							U = __dadd_rn(U, __dadd_rn(__dmul_rn(eps24, lj12m6), s_sh6[pk]));
-							const double fac = __dmul_rn(__dmul_rn(eps24, __dadd_rn(lj12, lj12m6)), invdr2);
+							double fac;
+							if (lj_j) {
+								const int pk = (bi + si) * kMaxSiteTotal + bj + sj;
+								const double eps24 = s_e24[pk];
+								double lj6 = __dmul_rn(s_sig2[pk], invdr2);
+								lj6 = __dmul_rn(__dmul_rn(lj6, lj6), lj6);
+								const double lj12 = __dmul_rn(lj6, lj6);
+								const double lj12m6 = __dsub_rn(lj12, lj6);
+								U = __dadd_rn(U, __dadd_rn(__dmul_rn(eps24, lj12m6), s_sh6[pk]));
+								fac = __dmul_rn(__dmul_rn(eps24, __dadd_rn(lj12, lj12m6)), invdr2);
+							} else {
+								const double u = __dmul_rn(__dmul_rn(s_q[bi + si], s_q[bj + sj]), __dsqrt_rn(invdr2));
+								UX = __dadd_rn(UX, u);
+								fac = __dmul_rn(u, invdr2);
+							}
 							const double f0 = __dmul_rn(fac, s0), f1 = __dmul_rn(fac, s1), f2 = __dmul_rn(fac, s2);
 							Fs[si][0] = __dadd_rn(Fs[si][0], f0);
 							Fs[si][1] = __dadd_rn(Fs[si][1], f1);
@@ -305,37 +326,48 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 					float fs[NS][3];
 #pragma unroll
 					for (int si = 0; si < NS; si++) fs[si][0] = fs[si][1] = fs[si][2] = 0.0f;
-					float uf = 0.0f;
+					float uf = 0.0f, uq = 0.0f;
 					double sh = 0.0;
 #pragma unroll
 					for (int sj = 0; sj < NS; sj++) {
 						if (sj >= nsj) break;
+						const bool lj_j = !kQ || sj < nljj;
+						if (lj_j && !lj) continue;
 						const float dj0 = (float) ds[(int64_t) (sj * 3 + 0) * n + j];
 						const float dj1 = (float) ds[(int64_t) (sj * 3 + 1) * n + j];
 						const float dj2 = (float) ds[(int64_t) (sj * 3 + 2) * n + j];
 #pragma unroll
 						for (int si = 0; si < NS; si++) {
 							if (si >= nsi) break;
-							const int pk = (bi + si) * kMaxSiteTotal + bj + sj;
+							if (kQ && (si < nlji) != lj_j) continue;
 							const float s0 = e0 + (float) di[si][0] - dj0;
 							const float s1 = e1 + (float) di[si][1] - dj1;
 							const float s2 = e2 + (float) di[si][2] - dj2;
 							const float dr2 = s0 * s0 + s1 * s1 + s2 * s2;
-							const float eps24 = (float) s_e24[pk];
 							const float inv = __fdividef(1.0f, dr2);
-							const float q2 = (float) s_sig2[pk] * inv;
-							const float q6 = q2 * q2 * q2;
-							const float q12 = q6 * q6;
-							const float qm = q12 - q6;
-							const float fac = eps24 * (q12 + qm) * inv;
-							uf += eps24 * qm;
-							sh += s_sh6[pk];
+							float fac;
+							if (lj_j) {
+								const int pk = (bi + si) * kMaxSiteTotal + bj + sj;
+								const float eps24 = (float) s_e24[pk];
+								const float q2 = (float) s_sig2[pk] * inv;
+								const float q6 = q2 * q2 * q2;
+								const float q12 = q6 * q6;
+								const float qm = q12 - q6;
+								fac = eps24 * (q12 + qm) * inv;
+								uf += eps24 * qm;
+								sh += s_sh6[pk];
+							} else {
+								const float u = (float) (s_q[bi + si] * s_q[bj + sj]) * rsqrtf(dr2);
+								uq += u;
+								fac = u * inv;
+							}
 							fs[si][0] += fac * s0;
 							fs[si][1] += fac * s1;
 							fs[si][2] += fac * s2;
 						}
 					}
 					U += (double) uf + sh;
+					UX += (double) uq;
 #pragma unroll
 					for (int si = 0; si < NS; si++) {
 						if (si >= nsi) break;
@@ -347,7 +379,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 						fp2 += (double) fs[si][2];
 					}
 				}
-				// Virial += drm . f over the molecule pair's centre pairs
+				// Virial += drm . f over the molecule pair's site pairs
 				W = __dadd_rn(W, __dadd_rn(__dadd_rn(__dmul_rn(m0, fp0), __dmul_rn(m1, fp1)), __dmul_rn(m2, fp2)));
 			}
 			cnt = 0;
@@ -404,7 +436,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 						if (!(dd < rc2)) continue;
 						np += 1.0;
 						if (dd == 0.0) same = true;
-						if (!(dd < rclj2)) continue;
+						if (!kQ && !(dd < rclj2)) continue;
 						list[cnt * kRigidThreads] = ((uint32_t) j << 5) | img;
 						if (++cnt == kRigidList) evaluate();
 					}
@@ -425,10 +457,11 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 #pragma unroll
 			for (int k = 0; k < 3; k++) Fs[s][k] = __dadd_rn(Fs[s][k], __shfl_xor_sync(0xffffffffu, Fs[s][k], o2));
 		U = __dadd_rn(U, __shfl_xor_sync(0xffffffffu, U, o2));
+		UX = __dadd_rn(UX, __shfl_xor_sync(0xffffffffu, UX, o2));
 		W = __dadd_rn(W, __shfl_xor_sync(0xffffffffu, W, o2));
 		np += __shfl_xor_sync(0xffffffffu, np, o2);
 	}
-	if (sub != 0) U = W = np = 0.0;
+	if (sub != 0) U = UX = W = np = 0.0;
 	if (i < n && sub == 0) {
 		double F[3] = {0.0, 0.0, 0.0}, Mt[3] = {0.0, 0.0, 0.0};
 		// Molecule::calcFM: F = sum F_s, M = sum d_s x F_s
@@ -454,8 +487,8 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 		if (bad) atomicOr(o.status, kStatusNonFinite);
 	}
 	if (same) atomicOr(o.status, kStatusSamePosition);
-	block_sum3(U, W, np, o.partials);
-	last_block_sum(o.ticket, o.partials, gridDim.x, 3, o.scalars);
+	block_sum3_at(U, W, np, o.partials, blockIdx.x, UX);
+	last_block_sum(o.ticket, o.partials, gridDim.x, 4, o.scalars);
 }
 
 struct RigidState {
@@ -543,7 +576,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_post(int64_t n, RigidSt
 	}
 	block_sum3(mv2, iw2, 0.0, partials);
 	if (last_block_sum(ticket, partials, gridDim.x, 2, scalars) && threadIdx.x == 0 && record) {
-		record[0] = pair_scalars[0] * 0.5 / 6.;
+		record[0] = pair_scalars[0] * 0.5 / 6. + pair_scalars[3] * 0.5;
 		record[1] = pair_scalars[1] * 0.5;
 		record[2] = scalars[0];
 		record[3] = scalars[1];
@@ -612,9 +645,13 @@ int launch_rigid_forces(mdgpu_rigid* h) {
 	RigidOut o{c->p.fx, c->p.fy, c->p.fz, h->M, h->partials, h->tickets, h->scal, c->status};
 	const bool mixed = c->precision == MDGPU_MIXED;
 	const int ns = h->hp.ns_max;
-#define RG_PAIRS(MX, NSV)                                                                                   \
-	k_rigid_pairs<MX, NSV><<<nbp, kRigidThreads, 0, c->stream>>>(n, c->p.rx, c->p.ry, c->p.rz, c->p.cid,     \
-	                                                            c->p.uidx, c->cell_start, c->g, h->dp, h->ds, o)
+	bool charged = false;
+	for (int k = 0; k < h->hp.nc; k++) charged |= h->hp.nsites[k] > h->hp.nlj[k];
+#define RG_PAIRS(MX, NSV)                                                                                     \
+	(charged ? k_rigid_pairs<MX, NSV, true><<<nbp, kRigidThreads, 0, c->stream>>>(                            \
+	               n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->p.uidx, c->cell_start, c->g, h->dp, h->ds, o)  \
+	         : k_rigid_pairs<MX, NSV, false><<<nbp, kRigidThreads, 0, c->stream>>>(                           \
+	               n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->p.uidx, c->cell_start, c->g, h->dp, h->ds, o))
 	if (ns <= 1)
 		mixed ? RG_PAIRS(true, 1) : RG_PAIRS(false, 1);
 	else if (ns == 2)
@@ -650,49 +687,73 @@ int launch_rigid_post(mdgpu_rigid* h, double dt_half, double* record) {
 	Context* c = ctx_of(h);
 	prof_begin(c, 2);
 	k_rigid_post<<<(unsigned) nblocks(c->n), kRigidThreads, 0, c->stream>>>(
-	    c->n, state_of(h), h->dp, dt_half, h->partials, h->tickets + 1, h->scal + 3, h->scal, record, c->status);
+	    c->n, state_of(h), h->dp, dt_half, h->partials, h->tickets + 1, h->scal + 4, h->scal, record, c->status);
 	prof_end(c, 2, 1);
 	RG_CUDA(cudaGetLastError());
 	return MDGPU_OK;
 }
 
-// Site tables from the components (Comp2Param::initialize and Component::addLJcenter).
-int setup_rigid(Context* c, int ncomp, const int32_t* nsites, const mdgpu_site* sites, const double* inertia,
-                const double* mix, double rc, double rc_lj, RigidParams& P) {
+// Site tables from the components (Comp2Param::initialize, Component::addLJcenter/addCharge): per
+// component its LJ centres (nlj[k], listed one component after another in `sites`), then its charges
+// (ncharges[k] in `charges`, which may be NULL for none).
+int setup_rigid(Context* c, int ncomp, const int32_t* nlj, const mdgpu_site* sites, const int32_t* ncharges,
+                const mdgpu_charge* charges, const double* inertia, const double* mix, double rc, double rc_lj,
+                RigidParams& P) {
 	P = RigidParams{};
 	P.nc = ncomp;
 	P.rc2 = rc * rc;
 	P.rclj2 = rc_lj * rc_lj;
 	int total = 0;
+	std::vector<int> lj_off(ncomp), q_off(ncomp);
+	int lo = 0, qo = 0;
 	for (int k = 0; k < ncomp; k++) {
-		if (nsites[k] < 1 || nsites[k] > kMaxSites)
-			return set_error(c, MDGPU_ERR_ARG, "each component needs 1.." + std::to_string(kMaxSites) + " LJ centres");
-		P.nsites[k] = nsites[k];
+		const int nq = ncharges ? ncharges[k] : 0;
+		if (nlj[k] < 1 || nq < 0 || nlj[k] + nq > kMaxSites)
+			return set_error(c, MDGPU_ERR_ARG, "each component needs at least one LJ centre and at most " +
+			                                       std::to_string(kMaxSites) + " LJ centres and charges");
+		if (nq > 0 && !charges) return set_error(c, MDGPU_ERR_ARG, "charges missing");
+		P.nlj[k] = nlj[k];
+		P.nsites[k] = nlj[k] + nq;
 		P.base[k] = total;
-		total += nsites[k];
-		P.ns_max = std::max(P.ns_max, nsites[k]);
+		total += P.nsites[k];
+		P.ns_max = std::max(P.ns_max, P.nsites[k]);
+		lj_off[k] = lo;
+		q_off[k] = qo;
+		lo += nlj[k];
+		qo += nq;
 	}
 	if (total > kMaxSiteTotal)
-		return set_error(c, MDGPU_ERR_ARG, "at most " + std::to_string(kMaxSiteTotal) + " LJ centres in all components");
+		return set_error(c, MDGPU_ERR_ARG,
+		                 "at most " + std::to_string(kMaxSiteTotal) + " LJ centres and charges in all components");
 	P.nsite_total = total;
 	std::vector<double> shift(total, 0.0);
 	for (int k = 0; k < ncomp; k++) {
 		double m = 0.0, I[3] = {0.0, 0.0, 0.0};
-		for (int s = 0; s < nsites[k]; s++) {
-			const mdgpu_site& t = sites[P.base[k] + s];
+		auto add_mass = [&](const double r[3], double mass) {
+			const double x = r[0], y = r[1], z = r[2];
+			m += mass;
+			I[0] += mass * (y * y + z * z);
+			I[1] += mass * (x * x + z * z);
+			I[2] += mass * (x * x + y * y);
+		};
+		for (int s = 0; s < nlj[k]; s++) {
+			const mdgpu_site& t = sites[lj_off[k] + s];
 			if (!(t.mass > 0.0) || !(t.sigma > 0.0) || !(t.eps >= 0.0))
 				return set_error(c, MDGPU_ERR_ARG, "LJ centre with non-positive mass or sigma, or negative eps");
 			for (int d = 0; d < 3; d++) P.site[P.base[k] + s][d] = t.r[d];
-			m += t.mass;
-			const double x = t.r[0], y = t.r[1], z = t.r[2];
-			I[0] += t.mass * (y * y + z * z);
-			I[1] += t.mass * (x * x + z * z);
-			I[2] += t.mass * (x * x + y * y);
+			add_mass(t.r, t.mass);
 			if (t.do_shift) {   // Component::addLJcenter, with the centre's cutoff = LJCutoffRadius
 				const double sigperrc2 = t.sigma * t.sigma / (rc_lj * rc_lj);
 				const double sigperrc6 = sigperrc2 * sigperrc2 * sigperrc2;
 				shift[P.base[k] + s] = 24.0 * t.eps * (sigperrc6 - sigperrc6 * sigperrc6);
 			}
+		}
+		for (int s = nlj[k]; s < P.nsites[k]; s++) {
+			const mdgpu_charge& t = charges[q_off[k] + s - nlj[k]];
+			if (!(t.mass >= 0.0)) return set_error(c, MDGPU_ERR_ARG, "charge with negative mass");
+			for (int d = 0; d < 3; d++) P.site[P.base[k] + s][d] = t.r[d];
+			P.charge[P.base[k] + s] = t.q;
+			add_mass(t.r, t.mass);
 		}
 		P.mass[k] = m;
 		for (int d = 0; d < 3; d++) {
@@ -703,10 +764,10 @@ int setup_rigid(Context* c, int ncomp, const int32_t* nsites, const mdgpu_site* 
 	}
 	int mixpos = 0;
 	for (int ci = 0; ci < ncomp; ci++) {
-		for (int a = 0; a < nsites[ci]; a++) {
-			const mdgpu_site& A = sites[P.base[ci] + a];
-			for (int b = 0; b < nsites[ci]; b++) {
-				const mdgpu_site& B = sites[P.base[ci] + b];
+		for (int a = 0; a < nlj[ci]; a++) {
+			const mdgpu_site& A = sites[lj_off[ci] + a];
+			for (int b = 0; b < nlj[ci]; b++) {
+				const mdgpu_site& B = sites[lj_off[ci] + b];
 				const int k = (P.base[ci] + a) * kMaxSiteTotal + P.base[ci] + b;
 				double sigma2 = .5 * (A.sigma + B.sigma);
 				sigma2 *= sigma2;
@@ -718,10 +779,10 @@ int setup_rigid(Context* c, int ncomp, const int32_t* nsites, const mdgpu_site* 
 		for (int cj = ci + 1; cj < ncomp; cj++) {
 			const double xi = mix ? mix[2 * mixpos] : 1.0, eta = mix ? mix[2 * mixpos + 1] : 1.0;
 			mixpos++;
-			for (int a = 0; a < nsites[ci]; a++) {
-				const mdgpu_site& A = sites[P.base[ci] + a];
-				for (int b = 0; b < nsites[cj]; b++) {
-					const mdgpu_site& B = sites[P.base[cj] + b];
+			for (int a = 0; a < nlj[ci]; a++) {
+				const mdgpu_site& A = sites[lj_off[ci] + a];
+				for (int b = 0; b < nlj[cj]; b++) {
+					const mdgpu_site& B = sites[lj_off[cj] + b];
 					const double epsilon24 = 24. * xi * std::sqrt(A.eps * B.eps);
 					double sigma2 = eta * .5 * (A.sigma + B.sigma);
 					sigma2 *= sigma2;
@@ -767,21 +828,25 @@ extern "C" {
 
 int mdgpu_rigid_create(mdgpu_rigid** out, const double length[3], double cutoff, double lj_cutoff,
                        double cells_in_cutoff, int ncomp, const int32_t* nsites, const mdgpu_site* sites,
-                       const double* inertia, const double* mix, int precision, int device) {
+                       const int32_t* ncharges, const mdgpu_charge* charges, const double* inertia, const double* mix,
+                       int precision, int device) {
 	if (!out) return MDGPU_ERR_ARG;
 	*out = nullptr;
 	if (ncomp < 1 || ncomp > kMaxSpecies || !nsites || !sites) return MDGPU_ERR_ARG;
 	// the single-box context holds the molecule centres; its component table carries each component's
 	// total mass (the LJ table of the single-centre kernels is not used here)
 	std::vector<mdgpu_component> comps(ncomp);
-	int base = 0;
+	int base = 0, qbase = 0;
 	for (int k = 0; k < ncomp; k++) {
-		if (nsites[k] < 1 || nsites[k] > kMaxSites) return MDGPU_ERR_ARG;
+		const int nq = ncharges ? ncharges[k] : 0;
+		if (nsites[k] < 1 || nq < 0 || nsites[k] + nq > kMaxSites || (nq > 0 && !charges)) return MDGPU_ERR_ARG;
 		double m = 0.0;
 		for (int s = 0; s < nsites[k]; s++) m += sites[base + s].mass;
+		for (int s = 0; s < nq; s++) m += charges[qbase + s].mass;
 		comps[k] = mdgpu_component{sites[base].eps > 0 ? sites[base].eps : 1.0,
 		                           sites[base].sigma > 0 ? sites[base].sigma : 1.0, m > 0 ? m : 1.0, 0};
 		base += nsites[k];
+		qbase += nq;
 	}
 	mdgpu_ctx* inner = nullptr;
 	int st = mdgpu_create(&inner, length, cutoff, lj_cutoff, cells_in_cutoff, ncomp, comps.data(), mix, precision, device);
@@ -792,7 +857,7 @@ int mdgpu_rigid_create(mdgpu_rigid** out, const double length[3], double cutoff,
 	mdgpu_rigid* h = new mdgpu_rigid();
 	h->inner = inner;
 	Context* c = ctx_of(h);
-	st = setup_rigid(c, ncomp, nsites, sites, inertia, mix, c->rc, c->rc_lj, h->hp);
+	st = setup_rigid(c, ncomp, nsites, sites, ncharges, charges, inertia, mix, c->rc, c->rc_lj, h->hp);
 	if (st == MDGPU_OK) {
 		cudaError_t e = cudaMalloc(&h->dp, sizeof(RigidParams));
 		if (e == cudaSuccess) e = cudaMemcpy(h->dp, &h->hp, sizeof(RigidParams), cudaMemcpyHostToDevice);
@@ -899,11 +964,11 @@ int mdgpu_rigid_traverse_pairs(mdgpu_rigid* h, double* upot, double* virial, dou
 	RG_CUDA(cudaSetDevice(c->device));
 	int st = launch_rigid_forces(h);
 	if (st) return st;
-	RG_CUDA(cudaMemcpyAsync(h->h_scal, h->scal, sizeof(double) * 3, cudaMemcpyDeviceToHost, c->stream));
+	RG_CUDA(cudaMemcpyAsync(h->h_scal, h->scal, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->stream));
 	st = check_device_status(c);
 	if (st) return st;
-	// ParticlePairs2PotForceAdapter::finish: Upot = Upot6LJ/6 (each pair was seen twice)
-	if (upot) *upot = h->h_scal[0] * 0.5 / 6.;
+	// ParticlePairs2PotForceAdapter::finish: Upot = Upot6LJ/6 + UpotXpoles (each pair was seen twice)
+	if (upot) *upot = h->h_scal[0] * 0.5 / 6. + h->h_scal[3] * 0.5;
 	if (virial) *virial = h->h_scal[1] * 0.5;
 	if (npairs) *npairs = h->h_scal[2] * 0.5;
 	return MDGPU_OK;
@@ -926,11 +991,11 @@ int mdgpu_rigid_leapfrog_post(mdgpu_rigid* h, double dt_half, double* summv2, do
 	RG_CUDA(cudaSetDevice(c->device));
 	int st = launch_rigid_post(h, dt_half, nullptr);
 	if (st) return st;
-	RG_CUDA(cudaMemcpyAsync(h->h_scal + 3, h->scal + 3, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->stream));
+	RG_CUDA(cudaMemcpyAsync(h->h_scal + 4, h->scal + 4, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->stream));
 	st = check_device_status(c);
 	if (st) return st;
-	if (summv2) *summv2 = h->h_scal[3];
-	if (sum_iw2) *sum_iw2 = h->h_scal[4];
+	if (summv2) *summv2 = h->h_scal[4];
+	if (sum_iw2) *sum_iw2 = h->h_scal[5];
 	return MDGPU_OK;
 }
 

@@ -88,7 +88,7 @@ SIGNATURES = {
     "mdgpu_batch_set_barrier_timeout": (_I, [_VP, _I64]),
     "mdgpu_batch_set_skin": (_I, [_VP, _D]),
     "mdgpu_batch_skin_builds": (_I, [_VP, _VP]),
-    "mdgpu_rigid_create": (_I, [ctypes.POINTER(_VP), _VP, _D, _D, _D, _I, _VP, _VP, _VP, _VP, _I, _I]),
+    "mdgpu_rigid_create": (_I, [ctypes.POINTER(_VP), _VP, _D, _D, _D, _I, _VP, _VP, _VP, _VP, _VP, _VP, _I, _I]),
     "mdgpu_rigid_destroy": (_I, [_VP]),
     "mdgpu_rigid_last_error": (ctypes.c_char_p, [_VP]),
     "mdgpu_rigid_set_precision": (_I, [_VP, _I]),
@@ -122,6 +122,10 @@ class _MdComponent(ctypes.Structure):
 class _MdSite(ctypes.Structure):
     _fields_ = [("r", ctypes.c_double * 3), ("mass", ctypes.c_double), ("eps", ctypes.c_double),
                 ("sigma", ctypes.c_double), ("do_shift", ctypes.c_int)]
+
+
+class _MdCharge(ctypes.Structure):
+    _fields_ = [("r", ctypes.c_double * 3), ("mass", ctypes.c_double), ("q", ctypes.c_double)]
 
 
 def load_library(path: str = LIB_PATH):
@@ -320,7 +324,7 @@ class Batch:
 
 
 class RigidLinkedCells:
-    """The GPU container for rigid multi-centre LJ molecules (include/mdgpu.h, mdgpu_rigid_*): the
+    """The GPU container for rigid multi-centre LJ molecules with point charges (include/mdgpu.h, mdgpu_rigid_*): the
     molecule centres binned into cells of edge >= rc as in ``LinkedCells``, every molecule with an
     orientation q, angular momentum D and torque M. Mirrors the same reference sequence:
     ``update`` (LinkedCells::update), ``traversePairs`` (Molecule::upd_cache, traversePairs with
@@ -343,6 +347,15 @@ class RigidLinkedCells:
                 sites[k].mass, sites[k].eps, sites[k].sigma = float(t.mass), float(t.eps), float(t.sigma)
                 sites[k].do_shift = 1 if t.do_shift else 0
                 k += 1
+        qs = [c.point_charges() if hasattr(c, "point_charges") else [] for c in components]
+        ncharges = np.array([len(x) for x in qs], dtype=np.int32)
+        charges = (_MdCharge * max(1, int(ncharges.sum())))()
+        k = 0
+        for x in qs:
+            for t in x:
+                charges[k].r[0], charges[k].r[1], charges[k].r[2] = float(t.x), float(t.y), float(t.z)
+                charges[k].mass, charges[k].q = float(t.mass), float(t.q)
+                k += 1
         inertia = np.zeros((len(components), 3))
         for i, c in enumerate(components):
             if getattr(c, "inertia", None) is not None:
@@ -354,7 +367,8 @@ class RigidLinkedCells:
         h = ctypes.c_void_p()
         st = self.lib.mdgpu_rigid_create(ctypes.byref(h), _ptr(self._length), float(cutoffRadius),
                                          float(LJCutoffRadius), float(cellsInCutoffRadius), len(components),
-                                         _ptr(nsites), ctypes.cast(sites, ctypes.c_void_p), _ptr(inertia), _ptr(mix),
+                                         _ptr(nsites), ctypes.cast(sites, ctypes.c_void_p), _ptr(ncharges),
+                                         ctypes.cast(charges, ctypes.c_void_p), _ptr(inertia), _ptr(mix),
                                          int(precision), int(device))
         self.h = h.value
         if st != 0:

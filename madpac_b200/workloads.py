@@ -37,9 +37,22 @@ class Site:
 
 
 @dataclasses.dataclass
+class Charge:
+    """A point charge of a rigid molecule at (x, y, z) in the principal-axes frame, with its mass
+    (Component::addCharge, mardyn/molecules/Component.cpp:115-133)."""
+
+    x: float
+    y: float
+    z: float
+    mass: float
+    q: float
+
+
+@dataclasses.dataclass
 class Component:
     """One LJ component: a single LJ centre at the molecule origin (eps, sigma, mass, do_shift) or,
-    with ``sites``, a rigid molecule of several LJ centres (``rigid_component``)."""
+    with ``sites`` (and ``charges``), a rigid molecule of several LJ centres and point charges
+    (``rigid_component``)."""
 
     eps: float = 1.0
     sigma: float = 1.0
@@ -47,17 +60,22 @@ class Component:
     do_shift: bool = False
     sites: Optional[List[Site]] = None
     inertia: Optional[Sequence[float]] = None   # the header's inertia line; values > 0 replace the moments
+    charges: Optional[List[Charge]] = None
 
     def lj_centres(self) -> List[Site]:
         if self.sites is not None:
             return list(self.sites)
         return [Site(0.0, 0.0, 0.0, self.mass, self.eps, self.sigma, self.do_shift)]
 
+    def point_charges(self) -> List[Charge]:
+        return list(self.charges) if self.charges else []
+
     def moments(self) -> np.ndarray:
         """Principal moments I11, I22, I33: sum m (y^2+z^2), sum m (x^2+z^2), sum m (x^2+y^2) over the
-        centres, each replaced by the header's value where that is > 0 (InputOldstyle.cpp:188-195)."""
+        centres and charges, each replaced by the header's value where that is > 0
+        (InputOldstyle.cpp:188-195)."""
         I = np.zeros(3)
-        for c in self.lj_centres():
+        for c in list(self.lj_centres()) + self.point_charges():
             I[0] += c.mass * (c.y * c.y + c.z * c.z)
             I[1] += c.mass * (c.x * c.x + c.z * c.z)
             I[2] += c.mass * (c.x * c.x + c.y * c.y)
@@ -72,11 +90,22 @@ class Component:
         return self.sites is not None
 
 
-def rigid_component(sites: Sequence[Site], inertia: Optional[Sequence[float]] = None) -> Component:
-    """A rigid multi-centre component; its mass is the sum of the centres' masses."""
+def rigid_component(sites: Sequence[Site], inertia: Optional[Sequence[float]] = None,
+                    charges: Optional[Sequence[Charge]] = None) -> Component:
+    """A rigid multi-centre component; its mass is the sum of the centres' and charges' masses."""
     sites = list(sites)
-    return Component(sites[0].eps, sites[0].sigma, float(sum(c.mass for c in sites)), sites[0].do_shift,
-                     sites=sites, inertia=None if inertia is None else list(inertia))
+    charges = list(charges) if charges else None
+    mass = float(sum(c.mass for c in sites) + sum(c.mass for c in (charges or [])))
+    return Component(sites[0].eps, sites[0].sigma, mass, sites[0].do_shift,
+                     sites=sites, inertia=None if inertia is None else list(inertia), charges=charges)
+
+
+def charged_two_centre(q: float = 0.5, elongation: float = 0.5, charge_offset: float = 0.35) -> Component:
+    """A two-centre LJ molecule (as ``two_centre``) with two massless point charges +q and -q at
+    z = +-charge_offset: a neutral molecule with a dipole of 2 q charge_offset."""
+    base = two_centre(elongation)
+    return rigid_component(base.sites, charges=[Charge(0.0, 0.0, charge_offset, 0.0, q),
+                                                Charge(0.0, 0.0, -charge_offset, 0.0, -q)])
 
 
 def two_centre(elongation: float = 0.5, eps: float = 1.0, sigma: float = 1.0, mass: float = 1.0,
@@ -316,10 +345,13 @@ def rigid_fcc_box(n_cells: int, density: float, temperature: float, seed: int, c
 
 
 def config_2clj(seed: int = 6, n_cells: int = 40, density: float = 0.3, temperature: float = 2.0,
-                cutoff: float = 3.0) -> System:
+                cutoff: float = 3.0, charged: bool = False) -> System:
     """A two-centre LJ fluid (elongation 0.5, truncated-shifted, cutoff 3.0 on the molecule centres):
-    4 n_cells^3 molecules (256,000 at the default) at molecular density 0.3 and T = 2.0."""
-    return rigid_fcc_box(n_cells, density, temperature, seed, cutoff, [two_centre()], name=f"2clj_{4 * n_cells ** 3}")
+    4 n_cells^3 molecules (256,000 at the default) at molecular density 0.3 and T = 2.0; with
+    ``charged`` the molecules carry the point charges +-0.5 of ``charged_two_centre``."""
+    comp = charged_two_centre() if charged else two_centre()
+    tag = "2cljq" if charged else "2clj"
+    return rigid_fcc_box(n_cells, density, temperature, seed, cutoff, [comp], name=f"{tag}_{4 * n_cells ** 3}")
 
 
 def config_c5(seed: int = 5) -> System:
@@ -342,10 +374,13 @@ def write_inp(sys_: System, path: str, fmt: Optional[str] = None) -> None:
              f"NumberOfComponents {nc}"]
     for c in sys_.components:
         centres = c.lj_centres()
-        lines.append(f"{len(centres)} 0 0 0 0")
+        charges = c.point_charges()
+        lines.append(f"{len(centres)} {len(charges)} 0 0 0")
         for t in centres:
             lines.append(f"{float(t.x)!r} {float(t.y)!r} {float(t.z)!r} {float(t.mass)!r} {float(t.eps)!r} "
                          f"{float(t.sigma)!r} {float(sys_.lj_cutoff)!r} {1 if t.do_shift else 0}")
+        for t in charges:
+            lines.append(f"{float(t.x)!r} {float(t.y)!r} {float(t.z)!r} {float(t.mass)!r} {float(t.q)!r}")
         inertia = [0.0, 0.0, 0.0] if c.inertia is None else [float(x) for x in c.inertia]
         lines.append("{!r} {!r} {!r}".format(*inertia))
     k = 0
@@ -406,18 +441,22 @@ def read_inp(path: str) -> System:
             nc = int(nxt())
             for _ in range(nc):
                 nlj, nq, nd, nqq, nt = (int(nxt()) for _ in range(5))
-                if nlj < 1 or nq or nd or nqq or nt:
-                    raise ValueError("only LJ components are supported")
+                if nlj < 1 or nd or nqq or nt:
+                    raise ValueError("only LJ centres and point charges are supported")
                 centres = []
                 for _ in range(nlj):
                     x, y, z, m, eps, sig, tcut, shift = (float(nxt()) for _ in range(8))
                     centres.append(Site(x, y, z, m, eps, sig, shift != 0))
+                charges = []
+                for _ in range(nq):
+                    x, y, z, m, q = (float(nxt()) for _ in range(5))
+                    charges.append(Charge(x, y, z, m, q))
                 inertia = [float(nxt()) for _ in range(3)]
-                if nlj == 1 and not (centres[0].x or centres[0].y or centres[0].z) and not any(inertia):
+                if nlj == 1 and not nq and not (centres[0].x or centres[0].y or centres[0].z) and not any(inertia):
                     t = centres[0]
                     comps.append(Component(t.eps, t.sigma, t.mass, t.do_shift))
                 else:
-                    comps.append(rigid_component(centres, inertia if any(inertia) else None))
+                    comps.append(rigid_component(centres, inertia if any(inertia) else None, charges or None))
             for i in range(nc):
                 for j in range(i + 1, nc):
                     mix.append((float(nxt()), float(nxt())))

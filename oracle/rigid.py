@@ -15,9 +15,15 @@ What it restates, in the reference's own operation order where rounding matters:
   centres are closer than rc (strict, BlockTraverse.cpp:155), all centre pairs evaluated when
   dd < rcLJ^2: drs = drm + d_i - d_j (SiteSiteDistance, potforce.h:26-31), ``PotForceLJ``
   (potforce.h:41-53), u += shift6, site forces +f on i and -f on j, Upot6LJ += u,
-  Virial += drm . f; Upot = Upot6LJ / 6 (ParticlePairs2PotForceAdapter::finish);
-* ``Molecule::upd_cache`` (Molecule.cpp:161-190): site offsets d = q.rotateinv(site);
-* ``Molecule::calcFM`` (Molecule.cpp:386-411): F = sum of site forces, M = sum d x F_site;
+  Virial += drm . f;
+* its charge-charge block (potforce.h:372-386) for every such pair: ``PotForce2Charge``
+  (potforce.h:244-253: u = q_i q_j / r with 1/r = sqrt(1/r^2), f = u / r^2 drs; the product
+  q_i q_j of Comp2Param.cpp:126-135), UpotXpoles += u, Virial += drm . f;
+  Upot = Upot6LJ / 6 + UpotXpoles (ParticlePairs2PotForceAdapter::finish);
+* ``Molecule::upd_cache`` (Molecule.cpp:161-190): site offsets d = q.rotateinv(site) of the LJ
+  centres and the charges;
+* ``Molecule::calcFM`` (Molecule.cpp:386-411): F = sum of site forces, M = sum d x F_site over all
+  sites;
 * ``Molecule::upd_preF`` / ``upd_postF`` (Molecule.cpp:128-159, 193-216) with the quaternion
   algebra of Quaternion.cpp (rotate, rotateinv, differentiate);
 * the periodic wrap of DomainDecompDummy::exchangeMolecules (r + L below 0, r - L at or above L).
@@ -81,7 +87,11 @@ class Model:
         comps = system.components
         self.nc = len(comps)
         self.centres = [c.lj_centres() for c in comps]
-        self.site_r = [np.array([[t.x, t.y, t.z] for t in cs]) for cs in self.centres]
+        self.charges = [c.point_charges() for c in comps]
+        # site positions: the LJ centres, then the charges (the reference's site order)
+        self.site_r = [np.array([[t.x, t.y, t.z] for t in cs + qs]).reshape(-1, 3)
+                       for cs, qs in zip(self.centres, self.charges)]
+        self.nlj = [len(cs) for cs in self.centres]
         self.mass = np.array([c.mass for c in comps])
         self.I = np.stack([c.moments() for c in comps])
         self.invI = np.where(self.I != 0.0, 1.0 / np.where(self.I != 0.0, self.I, 1.0), 0.0)
@@ -121,23 +131,25 @@ class Model:
 def site_offsets(model: Model, cid: np.ndarray, q: np.ndarray) -> List[np.ndarray]:
     """upd_cache: per site index s, the (N, 3) space-frame offsets (zero where a molecule has fewer
     centres)."""
-    ns = max(len(c) for c in model.centres)
+    ns = max(len(r) for r in model.site_r)
     out = [np.zeros((cid.shape[0], 3)) for _ in range(ns)]
     for c in range(model.nc):
         sel = cid == c
-        for s in range(len(model.centres[c])):
+        for s in range(len(model.site_r[c])):
             out[s][sel] = rotate_inv(q[sel], np.repeat(model.site_r[c][s][None, :], int(sel.sum()), axis=0))
     return out
 
 
 def forces(model: Model, r: np.ndarray, cid: np.ndarray, q: np.ndarray) -> Dict:
-    """F, M per molecule, Upot (Upot6LJ/6), virial and the number of molecule pairs within rc."""
+    """F, M per molecule, Upot (Upot6LJ/6 + UpotXpoles), virial and the number of molecule pairs
+    within rc."""
     n = r.shape[0]
     L = model.L
     d = site_offsets(model, cid, q)
     F = np.zeros((n, 3))
     M = np.zeros((n, 3))
     U6 = 0.0
+    UX = 0.0
     W = 0.0
     npairs = 0
     rc2, rclj2 = model.rc * model.rc, model.rclj * model.rclj
@@ -149,9 +161,31 @@ def forces(model: Model, r: np.ndarray, cid: np.ndarray, q: np.ndarray) -> Dict:
         near = dd < rc2
         j, drm, dd = j[near], drm[near], dd[near]
         npairs += int(j.shape[0])
+        ci = int(cid[i])
+        # charge-charge: every pair within rc
+        for cj in range(model.nc):
+            sel = cid[j] == cj
+            if not sel.any() or not model.charges[ci] or not model.charges[cj]:
+                continue
+            jj, dm = j[sel], drm[sel]
+            for a, qa in enumerate(model.charges[ci]):
+                di = d[model.nlj[ci] + a][i]
+                for b, qb in enumerate(model.charges[cj]):
+                    dj = d[model.nlj[cj] + b][jj]
+                    drs = dm + di[None, :] - dj
+                    dr2 = np.einsum("ij,ij->i", drs, drs)
+                    invdr2 = 1.0 / dr2
+                    invdr = np.sqrt(invdr2)
+                    u = (qa.q * qb.q) * invdr
+                    f = (u * invdr2)[:, None] * drs
+                    F[i] += f.sum(axis=0)
+                    np.subtract.at(F, jj, f)
+                    M[i] += np.cross(di[None, :], f).sum(axis=0)
+                    np.subtract.at(M, jj, np.cross(dj, f))
+                    UX += float(u.sum())
+                    W += float(np.einsum("ij,ij->", dm, f))
         lj = dd < rclj2
         j, drm = j[lj], drm[lj]
-        ci = int(cid[i])
         for cj in range(model.nc):
             sel = cid[j] == cj
             if not sel.any():
@@ -178,7 +212,7 @@ def forces(model: Model, r: np.ndarray, cid: np.ndarray, q: np.ndarray) -> Dict:
                     np.subtract.at(M, jj, np.cross(dj, f))
                     U6 += float(u.sum())
                     W += float(np.einsum("ij,ij->", dm, f))
-    return dict(F=F, M=M, upot=U6 / 6.0, virial=W, npairs=npairs)
+    return dict(F=F, M=M, upot=U6 / 6.0 + UX, virial=W, npairs=npairs)
 
 
 # ----------------------------------------------------------------------------- integration

@@ -11,6 +11,10 @@ rigid_<name>.npz (the start state is stored too, so the fixtures do not depend o
                    50/50, xi 0.9, eta 1.05, rho 0.15, T 2.0, rc 3.0;
 * rigid_bent_256:  a bent three-centre molecule with three non-zero moments, plain LJ, rho 0.25,
                    T 1.5, rc 2.5;
+* rigid_charged_256: the two-centre molecule with point charges +-0.5 at z = +-0.35 (massless),
+                   rho 0.3, T 2.0, rc 3.0;
+* rigid_charged_mix_256: three components (the charged molecule with +-0.8, the plain two-centre
+                   molecule and the bent molecule), 40/30/30, rho 0.2, T 1.5, rc 3.0;
 * rigid_2clj_4000_energy: the per-step Upot, virial, sum m v^2 and sum I w^2 of 1000 steps
                    (dt 0.001) of workloads.config_2clj(n_cells=10, temperature=1.5), 4,000
                    molecules, with a checksum of the generated start (the energy drift of the
@@ -42,6 +46,10 @@ def systems():
         W.rigid_fcc_box(4, 0.15, 2.0, 12, 3.0, [W.two_centre(), W.three_centre_linear()], [0.5, 0.5],
                         np.array([[0.9, 1.05]]), name="rigid_mix_256"),
         W.rigid_fcc_box(4, 0.25, 1.5, 13, 2.5, [W.bent_three_centre()], name="rigid_bent_256"),
+        W.rigid_fcc_box(4, 0.3, 2.0, 14, 3.0, [W.charged_two_centre()], name="rigid_charged_256"),
+        W.rigid_fcc_box(4, 0.2, 1.5, 15, 3.0, [W.charged_two_centre(0.8), W.two_centre(), W.bent_three_centre()],
+                        [0.4, 0.3, 0.3], np.array([[0.9, 1.05], [1.0, 1.0], [0.95, 0.98]]),
+                        name="rigid_charged_mix_256"),
     ]
 
 

@@ -3,8 +3,10 @@
 * The reference's own numbers (tests/golden/rigid_*.npz, made by the compiled reference): forces,
   torques, Upot and virial of the start, and the state after 10 NVE steps (r, v, q, D, F, M, and the
   per-step Upot, virial, sum m v^2, sum I w^2) for a two-centre fluid, a two-component mix with a
-  three-centre molecule whose centres differ, and a bent molecule with three non-zero moments.
-  FP64 agrees to rounding (1e-12 at the start, 1e-10 after 10 steps).
+  three-centre molecule whose centres differ, a bent molecule with three non-zero moments, a
+  two-centre molecule with point charges, and a three-component mix with charged and uncharged
+  molecules. FP64 agrees to rounding (1e-12 at the start, 1e-10 after 10 steps).
+* Charged molecules on a larger box: FP64 against the oracle (1e-12), the mixed form within 1e-5.
 * The oracle (oracle/rigid.py) on a larger box (more cells, the same code path at other sizes).
 * Single-centre components through the rigid path give the single-centre container's forces.
 * The step-by-step sequence equals mdgpu_rigid_run bit for bit; the mixed form stays within 1e-5 of
@@ -124,6 +126,24 @@ def test_rigid_mixed_accuracy():
     a, ua, wa, _ = start(s, M.FP64)
     b, ub, wb, _ = start(s, M.MIXED)
     fa, fb = a.getParticles(), b.getParticles()
+    for key in ("F", "M"):
+        rms = np.sqrt(np.mean(np.sum(fa[key] ** 2, axis=1)))
+        err = np.sqrt(np.mean(np.sum((fb[key] - fa[key]) ** 2, axis=1))) / rms
+        assert err <= 1e-5, (key, err)
+    assert abs(ub - ua) <= 1e-5 * abs(ua) and abs(wb - wa) <= 1e-5 * abs(wa)
+    a.close()
+    b.close()
+
+
+def test_rigid_charged_mixed_accuracy():
+    s = W.rigid_fcc_box(8, 0.25, 1.5, 41, 3.0, [W.charged_two_centre(0.7), W.bent_three_centre()], [0.6, 0.4],
+                        np.array([[0.95, 1.0]]))
+    a, ua, wa, _ = start(s, M.FP64)
+    b, ub, wb, _ = start(s, M.MIXED)
+    f = R.forces(R.Model(s), s.r, s.cid.astype(np.int64), s.q)
+    fa, fb = a.getParticles(), b.getParticles()
+    assert rel(fa["F"], f["F"]) < 1e-12 and rel(fa["M"], f["M"]) < 1e-12
+    assert abs(ua - f["upot"]) <= 1e-12 * abs(f["upot"]) and abs(wa - f["virial"]) <= 1e-12 * abs(f["virial"])
     for key in ("F", "M"):
         rms = np.sqrt(np.mean(np.sum(fa[key] ** 2, axis=1)))
         err = np.sqrt(np.mean(np.sum((fb[key] - fa[key]) ** 2, axis=1))) / rms

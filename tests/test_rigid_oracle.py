@@ -1,10 +1,12 @@
 """The rigid multi-centre oracle (oracle/rigid.py) against the reference's own numbers.
 
-Fixtures (tests/golden/make_rigid_golden.py): the reference MarDyn run for 10 steps on three systems
-of rigid LJ molecules (two-centre; a two-component mix with a three-centre molecule whose centres
-differ; a bent molecule with three non-zero moments). The oracle restates PotForce's centre loop,
-calcFM's torques and the quaternion Leapfrog, and must reproduce the forces, torques, potential
-energy and virial of the start and the state after 10 steps to rounding.
+Fixtures (tests/golden/make_rigid_golden.py): the reference MarDyn run for 10 steps on five systems
+of rigid molecules (two-centre LJ; a two-component mix with a three-centre molecule whose centres
+differ; a bent molecule with three non-zero moments; a two-centre molecule with point charges; a
+three-component mix with charged and uncharged molecules). The oracle restates PotForce's LJ
+centre loop and charge-charge block, calcFM's torques and the quaternion Leapfrog, and must
+reproduce the forces, torques, potential energy and virial of the start and the state after 10
+steps to rounding.
 """
 import os
 import sys
@@ -24,6 +26,8 @@ COMPONENTS = {
     "rigid_2clj_256": lambda: [W.two_centre()],
     "rigid_mix_256": lambda: [W.two_centre(), W.three_centre_linear()],
     "rigid_bent_256": lambda: [W.bent_three_centre()],
+    "rigid_charged_256": lambda: [W.charged_two_centre()],
+    "rigid_charged_mix_256": lambda: [W.charged_two_centre(0.8), W.two_centre(), W.bent_three_centre()],
 }
 NAMES = sorted(COMPONENTS)
 
