@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_sites(int64_t n, const 
                                                                const int32_t* __restrict__ cid,
                                                                const double* __restrict__ q,
                                                                const RigidParams* __restrict__ P,
-                                                               double* __restrict__ ds) {
+                                                               double* __restrict__ ds, float* __restrict__ dsf) {
 	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	const Quat qi = load_q(q, n, uidx[i]);
@@ -168,7 +168,10 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_sites(int64_t n, const 
 			const double body[3] = {P->site[b + s][0], P->site[b + s][1], P->site[b + s][2]};
 			q_rotate_inv(qi, body, d);
 		}
-		for (int k = 0; k < 3; k++) ds[(int64_t) (s * 3 + k) * n + i] = d[k];
+		for (int k = 0; k < 3; k++) {
+			ds[(int64_t) (s * 3 + k) * n + i] = d[k];
+			if (dsf) dsf[(int64_t) (s * 3 + k) * n + i] = (float) d[k];
+		}
 	}
 }
 
@@ -217,17 +220,25 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
                                                                const int32_t* __restrict__ uidx,
                                                                const int32_t* __restrict__ start, Grid g,
                                                                const RigidParams* __restrict__ P,
-                                                               const double* __restrict__ ds, RigidOut o) {
+                                                               const double* __restrict__ ds,
+                                                               const float* __restrict__ dsf, RigidOut o) {
 	constexpr int TT = kMaxSiteTotal * kMaxSiteTotal;
 	__shared__ double s_e24[TT], s_sig2[TT], s_sh6[TT];
 	__shared__ int s_ns[kMaxSpecies], s_nlj[kMaxSpecies], s_base[kMaxSpecies];
 	__shared__ double s_q[kMaxSiteTotal];
+	__shared__ float s_e24f[kMixed ? TT : 1], s_sig2f[kMixed ? TT : 1], s_qf[kMixed ? kMaxSiteTotal : 1];
 	__shared__ uint32_t s_list[kRigidList * kRigidThreads];
 	for (int k = threadIdx.x; k < TT; k += blockDim.x) {
 		s_e24[k] = P->eps24[k];
 		s_sig2[k] = P->sig2[k];
 		s_sh6[k] = P->shift6[k];
+		if constexpr (kMixed) {
+			s_e24f[k] = (float) P->eps24[k];
+			s_sig2f[k] = (float) P->sig2[k];
+		}
 	}
+	if constexpr (kMixed)
+		if (threadIdx.x < kMaxSiteTotal) s_qf[threadIdx.x] = (float) P->charge[threadIdx.x];
 	if (threadIdx.x < kMaxSpecies) {
 		s_ns[threadIdx.x] = P->nsites[threadIdx.x];
 		s_nlj[threadIdx.x] = P->nlj[threadIdx.x];
@@ -243,7 +254,10 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 	for (int s = 0; s < NS; s++) Fs[s][0] = Fs[s][1] = Fs[s][2] = 0.0;
 	double U = 0.0, UX = 0.0, W = 0.0, np = 0.0;
 	bool same = false;
-	double di[NS][3];
+	// centre offsets of i: double for the FP64 form, float for the mixed one (the double values are
+	// read again for the torque at the end)
+	double di[kMixed ? 1 : NS][3];
+	float dif[kMixed ? NS : 1][3];
 	int nsi = 0;
 	if (i < n) {
 		const double xi = rx[i], yi = ry[i], zi = rz[i];
@@ -254,7 +268,13 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 #pragma unroll
 		for (int s = 0; s < NS; s++)
 #pragma unroll
-			for (int k = 0; k < 3; k++) di[s][k] = s < nsi ? ds[(int64_t) (s * 3 + k) * n + i] : 0.0;
+			for (int k = 0; k < 3; k++) {
+				const double v = s < nsi ? ds[(int64_t) (s * 3 + k) * n + i] : 0.0;
+				if constexpr (kMixed)
+					dif[s][k] = (float) v;
+				else
+					di[s][k] = v;
+			}
 		uint32_t* list = s_list + threadIdx.x;
 		int cnt = 0;
 
@@ -277,7 +297,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 				const int cj = cid[j];
 				const int nsj = s_ns[cj], nljj = s_nlj[cj], bj = s_base[cj];
 				double fp0 = 0.0, fp1 = 0.0, fp2 = 0.0;   // force of this molecule pair
-				if (!kMixed) {
+				if constexpr (!kMixed) {
 #pragma unroll
 					for (int sj = 0; sj < NS; sj++) {
 						if (sj >= nsj) break;
@@ -333,23 +353,23 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 						if (sj >= nsj) break;
 						const bool lj_j = !kQ || sj < nljj;
 						if (lj_j && !lj) continue;
-						const float dj0 = (float) ds[(int64_t) (sj * 3 + 0) * n + j];
-						const float dj1 = (float) ds[(int64_t) (sj * 3 + 1) * n + j];
-						const float dj2 = (float) ds[(int64_t) (sj * 3 + 2) * n + j];
+						const float dj0 = dsf[(int64_t) (sj * 3 + 0) * n + j];
+						const float dj1 = dsf[(int64_t) (sj * 3 + 1) * n + j];
+						const float dj2 = dsf[(int64_t) (sj * 3 + 2) * n + j];
 #pragma unroll
 						for (int si = 0; si < NS; si++) {
 							if (si >= nsi) break;
 							if (kQ && (si < nlji) != lj_j) continue;
-							const float s0 = e0 + (float) di[si][0] - dj0;
-							const float s1 = e1 + (float) di[si][1] - dj1;
-							const float s2 = e2 + (float) di[si][2] - dj2;
+							const float s0 = e0 + dif[si][0] - dj0;
+							const float s1 = e1 + dif[si][1] - dj1;
+							const float s2 = e2 + dif[si][2] - dj2;
 							const float dr2 = s0 * s0 + s1 * s1 + s2 * s2;
 							const float inv = __fdividef(1.0f, dr2);
 							float fac;
 							if (lj_j) {
 								const int pk = (bi + si) * kMaxSiteTotal + bj + sj;
-								const float eps24 = (float) s_e24[pk];
-								const float q2 = (float) s_sig2[pk] * inv;
+								const float eps24 = s_e24f[pk];
+								const float q2 = s_sig2f[pk] * inv;
 								const float q6 = q2 * q2 * q2;
 								const float q12 = q6 * q6;
 								const float qm = q12 - q6;
@@ -357,7 +377,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 								uf += eps24 * qm;
 								sh += s_sh6[pk];
 							} else {
-								const float u = (float) (s_q[bi + si] * s_q[bj + sj]) * rsqrtf(dr2);
+								const float u = s_qf[bi + si] * s_qf[bj + sj] * rsqrtf(dr2);
 								uq += u;
 								fac = u * inv;
 							}
@@ -446,7 +466,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 		evaluate();
 	} else {
 #pragma unroll
-		for (int s = 0; s < NS; s++) di[s][0] = di[s][1] = di[s][2] = 0.0;
+		for (int s = 0; s < (kMixed ? 1 : NS); s++) di[s][0] = di[s][1] = di[s][2] = 0.0;
 	}
 	// the molecule's lanes combine their sums (the same order in every lane)
 	__syncwarp();
@@ -471,9 +491,17 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 			F[0] = __dadd_rn(F[0], Fs[s][0]);
 			F[1] = __dadd_rn(F[1], Fs[s][1]);
 			F[2] = __dadd_rn(F[2], Fs[s][2]);
-			Mt[0] = __dadd_rn(Mt[0], __dsub_rn(__dmul_rn(di[s][1], Fs[s][2]), __dmul_rn(di[s][2], Fs[s][1])));
-			Mt[1] = __dadd_rn(Mt[1], __dsub_rn(__dmul_rn(di[s][2], Fs[s][0]), __dmul_rn(di[s][0], Fs[s][2])));
-			Mt[2] = __dadd_rn(Mt[2], __dsub_rn(__dmul_rn(di[s][0], Fs[s][1]), __dmul_rn(di[s][1], Fs[s][0])));
+			double d[3];
+			if constexpr (kMixed) {
+				for (int k = 0; k < 3; k++) d[k] = ds[(int64_t) (s * 3 + k) * n + i];
+			} else {
+				d[0] = di[s][0];
+				d[1] = di[s][1];
+				d[2] = di[s][2];
+			}
+			Mt[0] = __dadd_rn(Mt[0], __dsub_rn(__dmul_rn(d[1], Fs[s][2]), __dmul_rn(d[2], Fs[s][1])));
+			Mt[1] = __dadd_rn(Mt[1], __dsub_rn(__dmul_rn(d[2], Fs[s][0]), __dmul_rn(d[0], Fs[s][2])));
+			Mt[2] = __dadd_rn(Mt[2], __dsub_rn(__dmul_rn(d[0], Fs[s][1]), __dmul_rn(d[1], Fs[s][0])));
 		}
 		o.fx[i] = F[0];
 		o.fy[i] = F[1];
@@ -615,6 +643,7 @@ struct mdgpu_rigid {
 	double* D = nullptr;        // 3 x cap
 	double* M = nullptr;        // 3 x cap
 	double* ds = nullptr;       // 3 x ns_max x cap, sorted order
+	float* dsf = nullptr;       // the same in float (mixed form)
 	double* stage = nullptr;    // 4 x cap host <-> device staging
 	double* partials = nullptr; // per-block reduction partials (4 doubles per block of the pair kernel)
 	double* scal = nullptr;     // [0..2] pair sums, [3..4] kinetic sums
@@ -641,17 +670,18 @@ int launch_rigid_forces(mdgpu_rigid* h) {
 	const unsigned nb = (unsigned) nblocks(n);
 	const unsigned nbp = (unsigned) nblocks(n * kRigidLanes);
 	prof_begin(c, 1);
-	k_rigid_sites<<<nb, kRigidThreads, 0, c->stream>>>(n, c->p.uidx, c->p.cid, h->q, h->dp, h->ds);
-	RigidOut o{c->p.fx, c->p.fy, c->p.fz, h->M, h->partials, h->tickets, h->scal, c->status};
 	const bool mixed = c->precision == MDGPU_MIXED;
+	k_rigid_sites<<<nb, kRigidThreads, 0, c->stream>>>(n, c->p.uidx, c->p.cid, h->q, h->dp, h->ds,
+	                                                   mixed ? h->dsf : nullptr);
+	RigidOut o{c->p.fx, c->p.fy, c->p.fz, h->M, h->partials, h->tickets, h->scal, c->status};
 	const int ns = h->hp.ns_max;
 	bool charged = false;
 	for (int k = 0; k < h->hp.nc; k++) charged |= h->hp.nsites[k] > h->hp.nlj[k];
 #define RG_PAIRS(MX, NSV)                                                                                     \
 	(charged ? k_rigid_pairs<MX, NSV, true><<<nbp, kRigidThreads, 0, c->stream>>>(                            \
-	               n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->p.uidx, c->cell_start, c->g, h->dp, h->ds, o)  \
+	               n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->p.uidx, c->cell_start, c->g, h->dp, h->ds, h->dsf, o) \
 	         : k_rigid_pairs<MX, NSV, false><<<nbp, kRigidThreads, 0, c->stream>>>(                           \
-	               n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->p.uidx, c->cell_start, c->g, h->dp, h->ds, o))
+	               n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->p.uidx, c->cell_start, c->g, h->dp, h->ds, h->dsf, o))
 	if (ns <= 1)
 		mixed ? RG_PAIRS(true, 1) : RG_PAIRS(false, 1);
 	else if (ns == 2)
@@ -808,14 +838,17 @@ int ensure_capacity(mdgpu_rigid* h, int64_t n) {
 	cudaFree(h->D);
 	cudaFree(h->M);
 	cudaFree(h->ds);
+	cudaFree(h->dsf);
 	cudaFree(h->stage);
 	cudaFree(h->partials);
 	h->q = h->D = h->M = h->ds = h->stage = h->partials = nullptr;
+	h->dsf = nullptr;
 	h->cap = 0;
 	RG_CUDA(cudaMalloc(&h->q, sizeof(double) * 4 * n));
 	RG_CUDA(cudaMalloc(&h->D, sizeof(double) * 3 * n));
 	RG_CUDA(cudaMalloc(&h->M, sizeof(double) * 3 * n));
 	RG_CUDA(cudaMalloc(&h->ds, sizeof(double) * 3 * std::max(1, h->hp.ns_max) * n));
+	RG_CUDA(cudaMalloc(&h->dsf, sizeof(float) * 3 * std::max(1, h->hp.ns_max) * n));
 	RG_CUDA(cudaMalloc(&h->stage, sizeof(double) * 4 * n));
 	RG_CUDA(cudaMalloc(&h->partials, sizeof(double) * 4 * nblocks(n * kRigidLanes)));
 	h->cap = n;
@@ -880,6 +913,7 @@ int mdgpu_rigid_destroy(mdgpu_rigid* h) {
 	cudaFree(h->D);
 	cudaFree(h->M);
 	cudaFree(h->ds);
+	cudaFree(h->dsf);
 	cudaFree(h->stage);
 	cudaFree(h->partials);
 	cudaFree(h->scal);
