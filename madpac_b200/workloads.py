@@ -49,10 +49,38 @@ class Charge:
 
 
 @dataclasses.dataclass
+class Dipole:
+    """A massless point dipole at (x, y, z) with orientation e (body frame) and strength abs_my
+    (Component::addDipole, mardyn/molecules/Component.cpp:135-139; e is used as given)."""
+
+    x: float
+    y: float
+    z: float
+    ex: float
+    ey: float
+    ez: float
+    abs_my: float
+
+
+@dataclasses.dataclass
+class Quadrupole:
+    """A massless linear point quadrupole at (x, y, z) with axis e and strength abs_q
+    (Component::addQuadrupole, Component.cpp:141-145)."""
+
+    x: float
+    y: float
+    z: float
+    ex: float
+    ey: float
+    ez: float
+    abs_q: float
+
+
+@dataclasses.dataclass
 class Component:
     """One LJ component: a single LJ centre at the molecule origin (eps, sigma, mass, do_shift) or,
-    with ``sites`` (and ``charges``), a rigid molecule of several LJ centres and point charges
-    (``rigid_component``)."""
+    with ``sites`` (and ``charges``, ``dipoles``, ``quadrupoles``), a rigid molecule of several LJ
+    centres and point polarities (``rigid_component``)."""
 
     eps: float = 1.0
     sigma: float = 1.0
@@ -61,6 +89,8 @@ class Component:
     sites: Optional[List[Site]] = None
     inertia: Optional[Sequence[float]] = None   # the header's inertia line; values > 0 replace the moments
     charges: Optional[List[Charge]] = None
+    dipoles: Optional[List[Dipole]] = None
+    quadrupoles: Optional[List[Quadrupole]] = None
 
     def lj_centres(self) -> List[Site]:
         if self.sites is not None:
@@ -69,6 +99,12 @@ class Component:
 
     def point_charges(self) -> List[Charge]:
         return list(self.charges) if self.charges else []
+
+    def point_dipoles(self) -> List[Dipole]:
+        return list(self.dipoles) if self.dipoles else []
+
+    def point_quadrupoles(self) -> List[Quadrupole]:
+        return list(self.quadrupoles) if self.quadrupoles else []
 
     def moments(self) -> np.ndarray:
         """Principal moments I11, I22, I33: sum m (y^2+z^2), sum m (x^2+z^2), sum m (x^2+y^2) over the
@@ -91,13 +127,30 @@ class Component:
 
 
 def rigid_component(sites: Sequence[Site], inertia: Optional[Sequence[float]] = None,
-                    charges: Optional[Sequence[Charge]] = None) -> Component:
-    """A rigid multi-centre component; its mass is the sum of the centres' and charges' masses."""
+                    charges: Optional[Sequence[Charge]] = None, dipoles: Optional[Sequence[Dipole]] = None,
+                    quadrupoles: Optional[Sequence[Quadrupole]] = None) -> Component:
+    """A rigid multi-centre component; its mass is the sum of the centres' and charges' masses
+    (dipoles and quadrupoles are massless)."""
     sites = list(sites)
     charges = list(charges) if charges else None
     mass = float(sum(c.mass for c in sites) + sum(c.mass for c in (charges or [])))
     return Component(sites[0].eps, sites[0].sigma, mass, sites[0].do_shift,
-                     sites=sites, inertia=None if inertia is None else list(inertia), charges=charges)
+                     sites=sites, inertia=None if inertia is None else list(inertia), charges=charges,
+                     dipoles=list(dipoles) if dipoles else None, quadrupoles=list(quadrupoles) if quadrupoles else None)
+
+
+def dipolar_two_centre(my: float = 1.0, elongation: float = 0.5) -> Component:
+    """A two-centre LJ molecule with a point dipole of strength my at the centre of mass along the
+    molecule axis (2CLJD)."""
+    base = two_centre(elongation)
+    return rigid_component(base.sites, dipoles=[Dipole(0.0, 0.0, 0.0, 0.0, 0.0, 1.0, my)])
+
+
+def quadrupolar_two_centre(Q: float = 1.0, elongation: float = 0.5) -> Component:
+    """A two-centre LJ molecule with a linear point quadrupole of strength Q at the centre of mass
+    along the molecule axis (2CLJQ)."""
+    base = two_centre(elongation)
+    return rigid_component(base.sites, quadrupoles=[Quadrupole(0.0, 0.0, 0.0, 0.0, 0.0, 1.0, Q)])
 
 
 def charged_two_centre(q: float = 0.5, elongation: float = 0.5, charge_offset: float = 0.35) -> Component:
@@ -152,6 +205,7 @@ class System:
     name: str = "system"
     q: Optional[np.ndarray] = None     # (N, 4) orientation quaternions (w, x, y, z) of rigid molecules
     D: Optional[np.ndarray] = None     # (N, 3) angular momenta (space frame) of rigid molecules
+    epsilon_rf: float = 1.0e10         # reaction-field permittivity (the header's epsilon_RF)
 
     @property
     def n(self) -> int:
@@ -375,12 +429,19 @@ def write_inp(sys_: System, path: str, fmt: Optional[str] = None) -> None:
     for c in sys_.components:
         centres = c.lj_centres()
         charges = c.point_charges()
-        lines.append(f"{len(centres)} {len(charges)} 0 0 0")
+        dips, quads = c.point_dipoles(), c.point_quadrupoles()
+        lines.append(f"{len(centres)} {len(charges)} {len(dips)} {len(quads)} 0")
         for t in centres:
             lines.append(f"{float(t.x)!r} {float(t.y)!r} {float(t.z)!r} {float(t.mass)!r} {float(t.eps)!r} "
                          f"{float(t.sigma)!r} {float(sys_.lj_cutoff)!r} {1 if t.do_shift else 0}")
         for t in charges:
             lines.append(f"{float(t.x)!r} {float(t.y)!r} {float(t.z)!r} {float(t.mass)!r} {float(t.q)!r}")
+        for t in dips:
+            lines.append(f"{float(t.x)!r} {float(t.y)!r} {float(t.z)!r} {float(t.ex)!r} {float(t.ey)!r} "
+                         f"{float(t.ez)!r} {float(t.abs_my)!r}")
+        for t in quads:
+            lines.append(f"{float(t.x)!r} {float(t.y)!r} {float(t.z)!r} {float(t.ex)!r} {float(t.ey)!r} "
+                         f"{float(t.ez)!r} {float(t.abs_q)!r}")
         inertia = [0.0, 0.0, 0.0] if c.inertia is None else [float(x) for x in c.inertia]
         lines.append("{!r} {!r} {!r}".format(*inertia))
     k = 0
@@ -388,7 +449,7 @@ def write_inp(sys_: System, path: str, fmt: Optional[str] = None) -> None:
         for j in range(i + 1, nc):
             lines.append(f"{float(sys_.mix[k, 0])!r} {float(sys_.mix[k, 1])!r}")
             k += 1
-    lines.append("1.0e+10")
+    lines.append(repr(float(sys_.epsilon_rf)))
     lines.append(f"NumberOfMolecules {sys_.n}")
     lines.append(f"MoleculeFormat {fmt}")
     head = "\n".join(lines) + "\n"
@@ -428,7 +489,7 @@ def read_inp(path: str) -> System:
     if nxt() != "trunk":
         raise ValueError(f"{path}: wrong input file specifier")
     nxt()
-    temperature, length, comps, mix = 1.0, None, [], []
+    temperature, length, comps, mix, epsilon_rf = 1.0, None, [], [], 1.0e10
     while True:
         t = nxt()
         if t in ("currentTime", "t"):
@@ -441,8 +502,8 @@ def read_inp(path: str) -> System:
             nc = int(nxt())
             for _ in range(nc):
                 nlj, nq, nd, nqq, nt = (int(nxt()) for _ in range(5))
-                if nlj < 1 or nd or nqq or nt:
-                    raise ValueError("only LJ centres and point charges are supported")
+                if nlj < 1 or nt:
+                    raise ValueError("only LJ centres and point polarities are supported")
                 centres = []
                 for _ in range(nlj):
                     x, y, z, m, eps, sig, tcut, shift = (float(nxt()) for _ in range(8))
@@ -451,16 +512,20 @@ def read_inp(path: str) -> System:
                 for _ in range(nq):
                     x, y, z, m, q = (float(nxt()) for _ in range(5))
                     charges.append(Charge(x, y, z, m, q))
+                dips = [Dipole(*(float(nxt()) for _ in range(7))) for _ in range(nd)]
+                quads = [Quadrupole(*(float(nxt()) for _ in range(7))) for _ in range(nqq)]
                 inertia = [float(nxt()) for _ in range(3)]
-                if nlj == 1 and not nq and not (centres[0].x or centres[0].y or centres[0].z) and not any(inertia):
+                if (nlj == 1 and not (nq or nd or nqq) and not (centres[0].x or centres[0].y or centres[0].z)
+                        and not any(inertia)):
                     t = centres[0]
                     comps.append(Component(t.eps, t.sigma, t.mass, t.do_shift))
                 else:
-                    comps.append(rigid_component(centres, inertia if any(inertia) else None, charges or None))
+                    comps.append(rigid_component(centres, inertia if any(inertia) else None, charges or None,
+                                                 dips or None, quads or None))
             for i in range(nc):
                 for j in range(i + 1, nc):
                     mix.append((float(nxt()), float(nxt())))
-            nxt()  # epsilon_RF
+            epsilon_rf = float(nxt())
             break
         else:
             raise ValueError(f"unsupported header token {t}")
@@ -488,7 +553,8 @@ def read_inp(path: str) -> System:
     return System(length=length, components=comps,
                   mix=np.array(mix, dtype=np.float64).reshape(nc * (nc - 1) // 2, 2),
                   ids=ids.astype(np.uint64), cid=(cid.astype(np.int32) - 1), r=r.copy(), v=v.copy(),
-                  temperature=temperature, name=path, q=q if rigid else None, D=D if rigid else None)
+                  temperature=temperature, name=path, q=q if rigid else None, D=D if rigid else None,
+                  epsilon_rf=epsilon_rf)
 
 
 def write_cfg(sys_: System, cfg_path: str, inp_name: str) -> None:

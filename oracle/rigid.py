@@ -88,10 +88,20 @@ class Model:
         self.nc = len(comps)
         self.centres = [c.lj_centres() for c in comps]
         self.charges = [c.point_charges() for c in comps]
-        # site positions: the LJ centres, then the charges (the reference's site order)
-        self.site_r = [np.array([[t.x, t.y, t.z] for t in cs + qs]).reshape(-1, 3)
-                       for cs, qs in zip(self.centres, self.charges)]
+        self.dipoles = [c.point_dipoles() for c in comps]
+        self.quads = [c.point_quadrupoles() for c in comps]
+        # site positions: the LJ centres, the charges, the dipoles, the quadrupoles (the reference's
+        # site order); orientations of the dipoles and quadrupoles
+        self.site_r = [np.array([[t.x, t.y, t.z] for t in cs + qs + ds + qq]).reshape(-1, 3)
+                       for cs, qs, ds, qq in zip(self.centres, self.charges, self.dipoles, self.quads)]
+        self.site_e = [np.array([[0.0, 0.0, 0.0]] * (len(cs) + len(qs)) + [[t.ex, t.ey, t.ez] for t in ds + qq])
+                       .reshape(-1, 3) for cs, qs, ds, qq in zip(self.centres, self.charges, self.dipoles, self.quads)]
         self.nlj = [len(cs) for cs in self.centres]
+        self.first_dip = [len(cs) + len(qs) for cs, qs in zip(self.centres, self.charges)]
+        self.first_quad = [len(cs) + len(qs) + len(ds) for cs, qs, ds in zip(self.centres, self.charges, self.dipoles)]
+        eps_rf = float(getattr(system, "epsilon_rf", 1.0e10))
+        rc = float(system.cutoff)
+        self.eps_rf_inv_rc3 = 2. * (eps_rf - 1.) / ((rc * rc * rc) * (2. * eps_rf + 1.))
         self.mass = np.array([c.mass for c in comps])
         self.I = np.stack([c.moments() for c in comps])
         self.invI = np.where(self.I != 0.0, 1.0 / np.where(self.I != 0.0, self.I, 1.0), 0.0)
@@ -128,16 +138,129 @@ class Model:
 
 # ----------------------------------------------------------------------------- forces
 
-def site_offsets(model: Model, cid: np.ndarray, q: np.ndarray) -> List[np.ndarray]:
+def site_offsets(model: Model, cid: np.ndarray, q: np.ndarray, orient: bool = False):
     """upd_cache: per site index s, the (N, 3) space-frame offsets (zero where a molecule has fewer
-    centres)."""
+    sites); with orient also the rotated orientation vectors of the dipoles and quadrupoles."""
     ns = max(len(r) for r in model.site_r)
     out = [np.zeros((cid.shape[0], 3)) for _ in range(ns)]
+    oe = [np.zeros((cid.shape[0], 3)) for _ in range(ns)]
     for c in range(model.nc):
         sel = cid == c
+        k = int(sel.sum())
         for s in range(len(model.site_r[c])):
-            out[s][sel] = rotate_inv(q[sel], np.repeat(model.site_r[c][s][None, :], int(sel.sum()), axis=0))
-    return out
+            out[s][sel] = rotate_inv(q[sel], np.repeat(model.site_r[c][s][None, :], k, axis=0))
+            oe[s][sel] = rotate_inv(q[sel], np.repeat(model.site_e[c][s][None, :], k, axis=0))
+    return (out, oe) if orient else out
+
+
+# Point-polarity pair terms of potforce.h, vectorised over pairs (dr: (P, 3), dr2: (P,), e: (P, 3)).
+
+def _dot(a, b):
+    return a[:, 0] * b[:, 0] + a[:, 1] * b[:, 1] + a[:, 2] * b[:, 2]
+
+
+def _cross(a, b):
+    return np.stack([a[:, 1] * b[:, 2] - a[:, 2] * b[:, 1], a[:, 2] * b[:, 0] - a[:, 0] * b[:, 2],
+                     a[:, 0] * b[:, 1] - a[:, 1] * b[:, 0]], axis=1)
+
+
+def charge_quadrupole(dr, dr2, ejj, qQ025):
+    """PotForceChargeQuadrupole (potforce.h:256-281): f, m2 (torque on the quadrupole), u."""
+    invdr2 = 1.0 / dr2
+    invdr = np.sqrt(invdr2)
+    costj = ((ejj[:, 0] * dr[:, 0] + ejj[:, 1] * dr[:, 1]) + ejj[:, 2] * dr[:, 2]) * invdr
+    qQinv4dr3 = qQ025 * invdr * invdr2
+    u = qQinv4dr3 * (3.0 * costj * costj - 1)
+    pR = -3.0 * u * invdr2
+    pT = 6.0 * costj * qQinv4dr3 * invdr
+    fac = costj * pT * invdr - pR
+    f = fac[:, None] * dr - pT[:, None] * ejj
+    mx = np.stack([ejj[:, 2] * dr[:, 1] - ejj[:, 1] * dr[:, 2], ejj[:, 0] * dr[:, 2] - ejj[:, 2] * dr[:, 0],
+                   ejj[:, 1] * dr[:, 0] - ejj[:, 0] * dr[:, 1]], axis=1)
+    return f, pT[:, None] * mx, u
+
+
+def charge_dipole(dr, dr2, ejj, minusqmy):
+    """PotForceChargeDipole (potforce.h:284-311): f, m2 (torque on the dipole), u."""
+    invdr2 = 1.0 / dr2
+    invdr = np.sqrt(invdr2)
+    costj = ((ejj[:, 0] * dr[:, 0] + ejj[:, 1] * dr[:, 1]) + ejj[:, 2] * dr[:, 2]) * invdr
+    uInvcostj = minusqmy * invdr2
+    u = uInvcostj * costj
+    pT = uInvcostj * invdr
+    fac = 3.0 * u * invdr * invdr2
+    f = fac[:, None] * dr - pT[:, None] * ejj
+    mx = np.stack([ejj[:, 2] * dr[:, 1] - ejj[:, 1] * dr[:, 2], ejj[:, 0] * dr[:, 2] - ejj[:, 2] * dr[:, 0],
+                   ejj[:, 1] * dr[:, 0] - ejj[:, 0] * dr[:, 1]], axis=1)
+    return f, pT[:, None] * mx, u
+
+
+def _angles(dr, eii, ejj, invdr1):
+    costi = ((eii[:, 0] * dr[:, 0] + eii[:, 1] * dr[:, 1]) + eii[:, 2] * dr[:, 2]) * invdr1
+    costj = ((ejj[:, 0] * dr[:, 0] + ejj[:, 1] * dr[:, 1]) + ejj[:, 2] * dr[:, 2]) * invdr1
+    cosgij = (eii[:, 0] * ejj[:, 0] + eii[:, 1] * ejj[:, 1]) + eii[:, 2] * ejj[:, 2]
+    return costi, costj, cosgij
+
+
+def two_dipole(dr, dr2, eii, ejj, my2, rffac):
+    """PotForce2Dipole (potforce.h:66-113): f, m1, m2, u and the MyRF increment."""
+    invdr2 = 1. / dr2
+    invdr1 = np.sqrt(invdr2)
+    myfac = my2 * invdr2 * invdr1
+    costi, costj, cosgij = _angles(dr, eii, ejj, invdr1)
+    u = myfac * (cosgij - 3. * costi * costj)
+    rf = -rffac * cosgij
+    pR = -3. * u * invdr2
+    pTi = -myfac * 3. * costj * invdr1
+    pTj = -myfac * 3. * costi * invdr1
+    pG = myfac
+    fac = -pR + (costi * pTi + costj * pTj) * invdr1
+    f = fac[:, None] * dr - pTi[:, None] * eii - pTj[:, None] * ejj
+    eiXej = _cross(eii, ejj)
+    m1 = -pTi[:, None] * _cross(eii, dr) + (-pG + rffac)[:, None] * eiXej
+    m2 = -pTj[:, None] * _cross(ejj, dr) + (pG - rffac)[:, None] * eiXej
+    return f, m1, m2, u, rf
+
+
+def two_quadrupole(dr, dr2, eii, ejj, q2075):
+    """PotForce2Quadrupole (potforce.h:127-172): f, m1, m2, u."""
+    invdr2 = 1. / dr2
+    invdr1 = np.sqrt(invdr2)
+    qfac = q2075 * invdr2 * invdr2 * invdr1
+    costi, costj, cosgij = _angles(dr, eii, ejj, invdr1)
+    c2i, c2j = costi * costi, costj * costj
+    term = cosgij - 5. * costi * costj
+    u = qfac * (1. - 5. * (c2i + c2j) - 15. * c2i * c2j + 2. * term * term)
+    pR = -5. * u * invdr2
+    pTi = -qfac * 10. * (costi + 3. * costi * c2j + 2. * costj * term) * invdr1
+    pTj = -qfac * 10. * (costj + 3. * c2i * costj + 2. * costi * term) * invdr1
+    pG = qfac * 4. * term
+    fac = -pR + (costi * pTi + costj * pTj) * invdr1
+    f = fac[:, None] * dr - pTi[:, None] * eii - pTj[:, None] * ejj
+    eiXej = _cross(eii, ejj)
+    m1 = -pTi[:, None] * _cross(eii, dr) - pG[:, None] * eiXej
+    m2 = -pTj[:, None] * _cross(ejj, dr) + pG[:, None] * eiXej
+    return f, m1, m2, u
+
+
+def di_quadrupole(dr, dr2, eii, ejj, myq15):
+    """PotForceDiQuadrupole (potforce.h:186-229), dipole eii, quadrupole ejj: f, m1, m2, u."""
+    invdr2 = 1. / dr2
+    invdr1 = np.sqrt(invdr2)
+    myqfac = myq15 * invdr2 * invdr2
+    costi, costj, cosgij = _angles(dr, eii, ejj, invdr1)
+    c2j = costj * costj
+    u = myqfac * (-costi * (5. * c2j - 1.) + 2. * cosgij * costj)
+    pR = -4. * u * invdr2
+    pTi = myqfac * (-5. * c2j + 1.) * invdr1
+    pTj = myqfac * 2. * (-5. * costi * costj + cosgij) * invdr1
+    pG = myqfac * 2. * costj
+    fac = -pR + (costi * pTi + costj * pTj) * invdr1
+    f = fac[:, None] * dr - pTi[:, None] * eii - pTj[:, None] * ejj
+    eiXej = _cross(eii, ejj)
+    m1 = -pTi[:, None] * _cross(eii, dr) - pG[:, None] * eiXej
+    m2 = -pTj[:, None] * _cross(ejj, dr) + pG[:, None] * eiXej
+    return f, m1, m2, u
 
 
 def forces(model: Model, r: np.ndarray, cid: np.ndarray, q: np.ndarray) -> Dict:
@@ -145,11 +268,12 @@ def forces(model: Model, r: np.ndarray, cid: np.ndarray, q: np.ndarray) -> Dict:
     within rc."""
     n = r.shape[0]
     L = model.L
-    d = site_offsets(model, cid, q)
+    d, oe = site_offsets(model, cid, q, orient=True)
     F = np.zeros((n, 3))
     M = np.zeros((n, 3))
     U6 = 0.0
     UX = 0.0
+    RF = 0.0
     W = 0.0
     npairs = 0
     rc2, rclj2 = model.rc * model.rc, model.rclj * model.rclj
@@ -162,28 +286,13 @@ def forces(model: Model, r: np.ndarray, cid: np.ndarray, q: np.ndarray) -> Dict:
         j, drm, dd = j[near], drm[near], dd[near]
         npairs += int(j.shape[0])
         ci = int(cid[i])
-        # charge-charge: every pair within rc
+        # the point-polarity blocks of PotForce (potforce.h:365-542), mi = i, mj = j, every pair within rc
         for cj in range(model.nc):
             sel = cid[j] == cj
-            if not sel.any() or not model.charges[ci] or not model.charges[cj]:
+            if not sel.any():
                 continue
             jj, dm = j[sel], drm[sel]
-            for a, qa in enumerate(model.charges[ci]):
-                di = d[model.nlj[ci] + a][i]
-                for b, qb in enumerate(model.charges[cj]):
-                    dj = d[model.nlj[cj] + b][jj]
-                    drs = dm + di[None, :] - dj
-                    dr2 = np.einsum("ij,ij->i", drs, drs)
-                    invdr2 = 1.0 / dr2
-                    invdr = np.sqrt(invdr2)
-                    u = (qa.q * qb.q) * invdr
-                    f = (u * invdr2)[:, None] * drs
-                    F[i] += f.sum(axis=0)
-                    np.subtract.at(F, jj, f)
-                    M[i] += np.cross(di[None, :], f).sum(axis=0)
-                    np.subtract.at(M, jj, np.cross(dj, f))
-                    UX += float(u.sum())
-                    W += float(np.einsum("ij,ij->", dm, f))
+            UX, W, RF = _polar_blocks(model, ci, cj, i, jj, dm, d, oe, F, M, UX, W, RF)
         lj = dd < rclj2
         j, drm = j[lj], drm[lj]
         for cj in range(model.nc):
@@ -212,7 +321,104 @@ def forces(model: Model, r: np.ndarray, cid: np.ndarray, q: np.ndarray) -> Dict:
                     np.subtract.at(M, jj, np.cross(dj, f))
                     U6 += float(u.sum())
                     W += float(np.einsum("ij,ij->", dm, f))
-    return dict(F=F, M=M, upot=U6 / 6.0 + UX, virial=W, npairs=npairs)
+    # ParticlePairs2PotForceAdapter::finish: Upot6LJ/6 + UpotXpoles + MyRF, Virial + 3 MyRF
+    return dict(F=F, M=M, upot=U6 / 6.0 + UX + RF, virial=W + 3.0 * RF, npairs=npairs)
+
+
+def _polar_blocks(model, ci, cj, i, jj, dm, d, oe, F, M, UX, W, RF):
+    """Charge, dipole and quadrupole pairs of molecule i (mi) with the molecules jj (mj) of component
+    cj, drm = dm (from j to i), in PotForce's order (potforce.h:372-542): site forces (+f on the
+    SiteSiteDistance side), the direct torques (Madd), UpotXpoles, Virial and MyRF."""
+    nq_i, nq_j = len(model.charges[ci]), len(model.charges[cj])
+    nd_i, nd_j = len(model.dipoles[ci]), len(model.dipoles[cj])
+    nQ_i, nQ_j = len(model.quads[ci]), len(model.quads[cj])
+    ch_i = lambda a: model.nlj[ci] + a  # noqa: E731
+    ch_j = lambda b: model.nlj[cj] + b  # noqa: E731
+    dp_i = lambda a: model.first_dip[ci] + a  # noqa: E731
+    dp_j = lambda b: model.first_dip[cj] + b  # noqa: E731
+    qd_i = lambda a: model.first_quad[ci] + a  # noqa: E731
+    qd_j = lambda b: model.first_quad[cj] + b  # noqa: E731
+    Wacc = [W]
+
+    def apply(si, sj, f, sign, m_i=None, m_j=None):
+        # sign +1: mi gets +f, mj gets -f; sign -1 the other way round (minusSiteSiteDistance blocks)
+        di, dj = d[si][i], d[sj][jj]
+        fi = sign * f
+        F[i] += fi.sum(axis=0)
+        np.subtract.at(F, jj, fi)
+        M[i] += np.cross(di[None, :], fi).sum(axis=0)
+        np.subtract.at(M, jj, np.cross(dj, fi))
+        if m_i is not None:
+            M[i] += m_i.sum(axis=0)
+        if m_j is not None:
+            np.add.at(M, jj, m_j)
+        Wacc[0] += sign * float(np.einsum("ij,ij->", dm, f))
+
+    def plus(si, sj):
+        drs = dm + d[si][i][None, :] - d[sj][jj]
+        return drs, np.einsum("ij,ij->i", drs, drs)
+
+    def minus(si, sj):
+        drs = d[sj][jj] - dm - d[si][i][None, :]
+        return drs, np.einsum("ij,ij->i", drs, drs)
+
+    for a in range(nq_i):
+        qa = model.charges[ci][a].q
+        for b in range(nq_j):
+            drs, dr2 = plus(ch_i(a), ch_j(b))
+            invdr2 = 1.0 / dr2
+            u = (qa * model.charges[cj][b].q) * np.sqrt(invdr2)
+            apply(ch_i(a), ch_j(b), (u * invdr2)[:, None] * drs, 1.0)
+            UX += float(u.sum())
+        for b in range(nQ_j):
+            drs, dr2 = plus(ch_i(a), qd_j(b))
+            f, m2, u = charge_quadrupole(drs, dr2, oe[qd_j(b)][jj], 0.25 * qa * model.quads[cj][b].abs_q)
+            apply(ch_i(a), qd_j(b), f, 1.0, m_j=m2)
+            UX += float(u.sum())
+        for b in range(nd_j):
+            drs, dr2 = plus(ch_i(a), dp_j(b))
+            f, m2, u = charge_dipole(drs, dr2, oe[dp_j(b)][jj], -qa * model.dipoles[cj][b].abs_my)
+            apply(ch_i(a), dp_j(b), f, 1.0, m_j=m2)
+            UX += float(u.sum())
+    for a in range(nQ_i):
+        Qa = model.quads[ci][a].abs_q
+        ei = np.repeat(oe[qd_i(a)][i][None, :], jj.shape[0], axis=0)
+        for b in range(nq_j):
+            drs, dr2 = minus(qd_i(a), ch_j(b))
+            f, m1, u = charge_quadrupole(drs, dr2, ei, 0.25 * model.charges[cj][b].q * Qa)
+            apply(qd_i(a), ch_j(b), f, -1.0, m_i=m1)
+            UX += float(u.sum())
+        for b in range(nQ_j):
+            drs, dr2 = plus(qd_i(a), qd_j(b))
+            f, m1, m2, u = two_quadrupole(drs, dr2, ei, oe[qd_j(b)][jj], .75 * Qa * model.quads[cj][b].abs_q)
+            apply(qd_i(a), qd_j(b), f, 1.0, m_i=m1, m_j=m2)
+            UX += float(u.sum())
+        for b in range(nd_j):
+            drs, dr2 = minus(qd_i(a), dp_j(b))
+            f, m_dip, m_quad, u = di_quadrupole(drs, dr2, oe[dp_j(b)][jj], ei, 1.5 * Qa * model.dipoles[cj][b].abs_my)
+            apply(qd_i(a), dp_j(b), f, -1.0, m_i=m_quad, m_j=m_dip)
+            UX += float(u.sum())
+    for a in range(nd_i):
+        mya = model.dipoles[ci][a].abs_my
+        ei = np.repeat(oe[dp_i(a)][i][None, :], jj.shape[0], axis=0)
+        for b in range(nq_j):
+            drs, dr2 = minus(dp_i(a), ch_j(b))
+            f, m1, u = charge_dipole(drs, dr2, ei, -model.charges[cj][b].q * mya)
+            apply(dp_i(a), ch_j(b), f, -1.0, m_i=m1)
+            UX += float(u.sum())
+        for b in range(nQ_j):
+            drs, dr2 = plus(dp_i(a), qd_j(b))
+            f, m1, m2, u = di_quadrupole(drs, dr2, ei, oe[qd_j(b)][jj], 1.5 * mya * model.quads[cj][b].abs_q)
+            apply(dp_i(a), qd_j(b), f, 1.0, m_i=m1, m_j=m2)
+            UX += float(u.sum())
+        for b in range(nd_j):
+            drs, dr2 = plus(dp_i(a), dp_j(b))
+            my2 = mya * model.dipoles[cj][b].abs_my
+            f, m1, m2, u, rf = two_dipole(drs, dr2, ei, oe[dp_j(b)][jj], my2, my2 * model.eps_rf_inv_rc3)
+            apply(dp_i(a), dp_j(b), f, 1.0, m_i=m1, m_j=m2)
+            UX += float(u.sum())
+            RF += float(rf.sum())
+    return UX, Wacc[0], RF
 
 
 # ----------------------------------------------------------------------------- integration

@@ -15,6 +15,11 @@ rigid_<name>.npz (the start state is stored too, so the fixtures do not depend o
                    rho 0.3, T 2.0, rc 3.0;
 * rigid_charged_mix_256: three components (the charged molecule with +-0.8, the plain two-centre
                    molecule and the bent molecule), 40/30/30, rho 0.2, T 1.5, rc 3.0;
+* rigid_dipolar_256: the two-centre molecule with a point dipole 1.2 along its axis, rho 0.3,
+                   T 2.0, rc 3.0 (epsilon_RF 1e10);
+* rigid_polar_mix_256: quadrupolar (Q 1.0), dipolar (0.9) and charged (+-0.6) two-centre molecules,
+                   40/30/30, rho 0.25, T 1.8, rc 3.0, reaction field epsilon_RF 5 (every point-polarity
+                   block of PotForce and MyRF);
 * rigid_2clj_4000_energy: the per-step Upot, virial, sum m v^2 and sum I w^2 of 1000 steps
                    (dt 0.001) of workloads.config_2clj(n_cells=10, temperature=1.5), 4,000
                    molecules, with a checksum of the generated start (the energy drift of the
@@ -50,7 +55,17 @@ def systems():
         W.rigid_fcc_box(4, 0.2, 1.5, 15, 3.0, [W.charged_two_centre(0.8), W.two_centre(), W.bent_three_centre()],
                         [0.4, 0.3, 0.3], np.array([[0.9, 1.05], [1.0, 1.0], [0.95, 0.98]]),
                         name="rigid_charged_mix_256"),
+        W.rigid_fcc_box(4, 0.3, 2.0, 16, 3.0, [W.dipolar_two_centre(1.2)], name="rigid_dipolar_256"),
+        polar_mix(),
     ]
+
+
+def polar_mix():
+    s = W.rigid_fcc_box(4, 0.25, 1.8, 17, 3.0, [W.quadrupolar_two_centre(1.0), W.dipolar_two_centre(0.9),
+                                               W.charged_two_centre(0.6)], [0.4, 0.3, 0.3],
+                        np.array([[0.95, 1.0], [1.0, 1.02], [0.98, 1.0]]), name="rigid_polar_mix_256")
+    s.epsilon_rf = 5.0
+    return s
 
 
 def main():
@@ -62,7 +77,7 @@ def main():
         sc = out["scalars"]
         np.savez_compressed(
             os.path.join(OUT, f"{s.name}.npz"),
-            length=s.length, cutoff=s.cutoff, lj_cutoff=s.lj_cutoff, dt=s.dt, mix=s.mix,
+            length=s.length, cutoff=s.cutoff, lj_cutoff=s.lj_cutoff, dt=s.dt, mix=s.mix, epsilon_rf=s.epsilon_rf,
             ids=s.ids, cid=s.cid, r=s.r, v=s.v, q=s.q, D=s.D,
             F0=d0["F"], M0=d0["M"],
             r1=d1["r"], v1=d1["v"], q1=d1["q"], D1=d1["D"], F1=d1["F"], M1=d1["M"],

@@ -3,10 +3,11 @@
 Fixtures (tests/golden/make_rigid_golden.py): the reference MarDyn run for 10 steps on five systems
 of rigid molecules (two-centre LJ; a two-component mix with a three-centre molecule whose centres
 differ; a bent molecule with three non-zero moments; a two-centre molecule with point charges; a
-three-component mix with charged and uncharged molecules). The oracle restates PotForce's LJ
-centre loop and charge-charge block, calcFM's torques and the quaternion Leapfrog, and must
-reproduce the forces, torques, potential energy and virial of the start and the state after 10
-steps to rounding.
+three-component mix with charged and uncharged molecules; a dipolar two-centre fluid; a mix of
+quadrupolar, dipolar and charged molecules with a reaction field). The oracle restates PotForce's
+LJ centre loop and its point-polarity blocks (charge, dipole, quadrupole pairs, direct torques,
+MyRF), calcFM's torques and the quaternion Leapfrog, and must reproduce the forces, torques,
+potential energy and virial of the start and the state after 10 steps to rounding.
 """
 import os
 import sys
@@ -28,6 +29,8 @@ COMPONENTS = {
     "rigid_bent_256": lambda: [W.bent_three_centre()],
     "rigid_charged_256": lambda: [W.charged_two_centre()],
     "rigid_charged_mix_256": lambda: [W.charged_two_centre(0.8), W.two_centre(), W.bent_three_centre()],
+    "rigid_dipolar_256": lambda: [W.dipolar_two_centre(1.2)],
+    "rigid_polar_mix_256": lambda: [W.quadrupolar_two_centre(1.0), W.dipolar_two_centre(0.9), W.charged_two_centre(0.6)],
 }
 NAMES = sorted(COMPONENTS)
 
@@ -36,7 +39,7 @@ def golden_system(name):
     d = np.load(os.path.join(GOLDEN, f"{name}.npz"))
     s = W.System(length=d["length"], components=COMPONENTS[name](), mix=d["mix"], ids=d["ids"], cid=d["cid"],
                  r=d["r"], v=d["v"], cutoff=float(d["cutoff"]), lj_cutoff=float(d["lj_cutoff"]), dt=float(d["dt"]),
-                 q=d["q"], D=d["D"], name=name)
+                 q=d["q"], D=d["D"], name=name, epsilon_rf=float(d["epsilon_rf"]))
     return s, d
 
 
@@ -85,15 +88,19 @@ def test_quaternion_rotations_are_inverse():
 
 
 def test_rigid_phase_space_round_trip(tmp_path):
-    s = W.rigid_fcc_box(3, 0.2, 1.0, 5, 2.5, [W.two_centre(), W.bent_three_centre()], [0.5, 0.5],
-                        np.array([[0.95, 1.0]]))
+    s = W.rigid_fcc_box(3, 0.2, 1.0, 5, 2.5, [W.two_centre(), W.bent_three_centre(), W.dipolar_two_centre(),
+                                              W.quadrupolar_two_centre(), W.charged_two_centre()],
+                        [0.2] * 5, np.ones((10, 2)))
+    s.epsilon_rf = 7.5
     path = str(tmp_path / "rigid.inp")
     W.write_inp(s, path)
     t = W.read_inp(path)
-    assert [c.is_rigid for c in t.components] == [True, True]
+    assert [c.is_rigid for c in t.components] == [True] * 5 and t.epsilon_rf == 7.5
     for a, b in zip(s.components, t.components):
         np.testing.assert_array_equal(a.moments(), b.moments())
         assert a.mass == b.mass and len(a.lj_centres()) == len(b.lj_centres())
+        assert a.point_charges() == b.point_charges() and a.point_dipoles() == b.point_dipoles()
+        assert a.point_quadrupoles() == b.point_quadrupoles()
     for key in ("r", "v", "q", "D"):
         np.testing.assert_array_equal(getattr(t, key), getattr(s, key))
     # the rotational temperature of the start: sum I w^2 = rotDOF * T
