@@ -273,6 +273,15 @@ typedef struct mdgpu_charge {
 	double q;
 } mdgpu_charge;
 
+/* A massless point dipole (strength |my|) or linear quadrupole (|Q|) at r with orientation e in the
+ * body frame, used as given (Component::addDipole/addQuadrupole, molecules/Component.cpp:135-145,
+ * read by InputOldstyle.cpp:172-181). */
+typedef struct mdgpu_oriented {
+	double r[3];
+	double e[3];
+	double strength;
+} mdgpu_oriented;
+
 typedef struct mdgpu_rigid mdgpu_rigid;
 
 /* nsites[c] LJ centres (at least one) for each component c, listed one component after another in
@@ -288,6 +297,16 @@ int mdgpu_rigid_create(mdgpu_rigid** out, const double length[3], double cutoff,
 int mdgpu_rigid_destroy(mdgpu_rigid* h);
 const char* mdgpu_rigid_last_error(const mdgpu_rigid* h);
 int mdgpu_rigid_set_precision(mdgpu_rigid* h, int precision);
+/* Point dipoles and quadrupoles of the components (ndipoles[c] and nquadrupoles[c] per component,
+ * listed one component after another; either may be NULL) and the reaction field's permittivity
+ * epsilon_rf (the header's epsilonRF; 1e10 by default). Call before mdgpu_rigid_set_particles.
+ * Every point-polarity pair of molecules within the cutoff then interacts as in PotForce
+ * (molecules/potforce.h:65-311, 365-542): charge-quadrupole, charge-dipole, dipole-dipole with the
+ * reaction-field term MyRF, dipole-quadrupole and quadrupole-quadrupole, with their direct torques;
+ * Upot gains UpotXpoles + MyRF and the virial 3 MyRF (ParticlePairs2PotForceAdapter::finish). The
+ * pairs with a dipole or quadrupole are evaluated in double in both precision modes. */
+int mdgpu_rigid_set_polarities(mdgpu_rigid* h, const int32_t* ndipoles, const mdgpu_oriented* dipoles,
+                               const int32_t* nquadrupoles, const mdgpu_oriented* quadrupoles, double epsilon_rf);
 /* Total mass and principal moments of component comp (Component::m, I11/I22/I33). */
 int mdgpu_rigid_get_inertia(const mdgpu_rigid* h, int32_t comp, double* mass, double I[3]);
 /* Loads the molecules (q and D required); forces and torques start at zero. */

@@ -48,8 +48,13 @@ constexpr int kRigidThreads = kReduceBlock;
 struct RigidParams {
 	int nc, nsite_total, ns_max;
 	int nsites[kMaxSpecies];               // LJ centres + charges of component c
-	int nlj[kMaxSpecies];                  // its LJ centres (sites 0..nlj-1; the charges follow)
-	double charge[kMaxSiteTotal];          // q of the charge sites (0 for LJ centres)
+	int nlj[kMaxSpecies];                  // its LJ centres (sites 0..nlj-1; charges, dipoles, quadrupoles follow)
+	double charge[kMaxSiteTotal];          // q of the charge sites (0 for the others)
+	int type[kMaxSiteTotal];               // 0 LJ centre, 1 charge, 2 dipole, 3 quadrupole
+	double strength[kMaxSiteTotal];        // q, |my| or |Q|
+	double e_body[kMaxSiteTotal][3];       // orientation of a dipole or quadrupole (body frame, as given)
+	double eps_rf_inv_rc3;                 // 2 (epsRF - 1) / (rc^3 (2 epsRF + 1)) (Comp2Param.cpp:178)
+	int oriented;                          // any dipole or quadrupole
 	int base[kMaxSpecies];                 // first centre of component c in the site tables
 	double site[kMaxSiteTotal][3];         // body-frame centre positions
 	double mass[kMaxSpecies];
@@ -156,23 +161,145 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_sites(int64_t n, const 
                                                                const int32_t* __restrict__ cid,
                                                                const double* __restrict__ q,
                                                                const RigidParams* __restrict__ P,
-                                                               double* __restrict__ ds, float* __restrict__ dsf) {
+                                                               double* __restrict__ ds, float* __restrict__ dsf,
+                                                               double* __restrict__ es) {
 	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	const Quat qi = load_q(q, n, uidx[i]);
 	const int c = cid[i];
 	const int ns = P->nsites[c], b = P->base[c];
 	for (int s = 0; s < P->ns_max; s++) {
-		double d[3] = {0.0, 0.0, 0.0};
+		double d[3] = {0.0, 0.0, 0.0}, e[3] = {0.0, 0.0, 0.0};
 		if (s < ns) {
 			const double body[3] = {P->site[b + s][0], P->site[b + s][1], P->site[b + s][2]};
 			q_rotate_inv(qi, body, d);
+			if (es && P->type[b + s] >= 2) q_rotate_inv(qi, P->e_body[b + s], e);
 		}
 		for (int k = 0; k < 3; k++) {
 			ds[(int64_t) (s * 3 + k) * n + i] = d[k];
 			if (dsf) dsf[(int64_t) (s * 3 + k) * n + i] = (float) d[k];
+			if (es) es[(int64_t) (s * 3 + k) * n + i] = e[k];
 		}
 	}
+}
+
+// ---- point dipoles and quadrupoles (molecules/potforce.h), double without contraction -----------
+
+__device__ __forceinline__ double dm_(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double da_(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double ds_(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
+	return da_(da_(dm_(a[0], b[0]), dm_(a[1], b[1])), dm_(a[2], b[2]));
+}
+__device__ __forceinline__ void cross3(const double a[3], const double b[3], double o[3]) {
+	o[0] = ds_(dm_(a[1], b[2]), dm_(a[2], b[1]));
+	o[1] = ds_(dm_(a[2], b[0]), dm_(a[0], b[2]));
+	o[2] = ds_(dm_(a[0], b[1]), dm_(a[1], b[0]));
+}
+
+// PotForceChargeQuadrupole (potforce.h:256-281) / PotForceChargeDipole (:284-311): f, and m2 the
+// torque on the oriented site ejj.
+__device__ void charge_oriented(bool quad, const double dr[3], double dr2, const double ejj[3], double par,
+                                double f[3], double m2[3], double& u) {
+	const double invdr2 = __ddiv_rn(1.0, dr2);
+	const double invdr = __dsqrt_rn(invdr2);
+	const double costj = dm_(dot3(ejj, dr), invdr);
+	double pT, fac;
+	if (quad) {
+		const double qQinv4dr3 = dm_(dm_(par, invdr), invdr2);
+		u = dm_(qQinv4dr3, ds_(dm_(dm_(3.0, costj), costj), 1.0));
+		const double pR = dm_(dm_(-3.0, u), invdr2);
+		pT = dm_(dm_(dm_(6.0, costj), qQinv4dr3), invdr);
+		fac = ds_(dm_(dm_(costj, pT), invdr), pR);
+	} else {
+		const double uInvcostj = dm_(par, invdr2);
+		u = dm_(uInvcostj, costj);
+		pT = dm_(uInvcostj, invdr);
+		fac = dm_(dm_(dm_(3.0, u), invdr), invdr2);
+	}
+	for (int d = 0; d < 3; d++) f[d] = ds_(dm_(fac, dr[d]), dm_(pT, ejj[d]));
+	const double mx[3] = {ds_(dm_(ejj[2], dr[1]), dm_(ejj[1], dr[2])), ds_(dm_(ejj[0], dr[2]), dm_(ejj[2], dr[0])),
+	                      ds_(dm_(ejj[1], dr[0]), dm_(ejj[0], dr[1]))};
+	for (int d = 0; d < 3; d++) m2[d] = dm_(pT, mx[d]);
+}
+
+// PotForce2Dipole (kind 0, :66-113), PotForce2Quadrupole (1, :127-172), PotForceDiQuadrupole
+// (2, :186-229, dipole eii, quadrupole ejj): f, m1 (torque on eii), m2 (on ejj), u, MyRF increment.
+__device__ void two_oriented(int kind, const double dr[3], double dr2, const double eii[3], const double ejj[3],
+                             double par, double rffac, double f[3], double m1[3], double m2[3], double& u,
+                             double& rf) {
+	const double invdr2 = __ddiv_rn(1., dr2);
+	const double invdr1 = __dsqrt_rn(invdr2);
+	const double costi = dm_(dot3(eii, dr), invdr1);
+	const double costj = dm_(dot3(ejj, dr), invdr1);
+	const double cosgij = dot3(eii, ejj);
+	double pR, pTi, pTj, pG;
+	rf = 0.0;
+	if (kind == 0) {
+		const double myfac = dm_(dm_(par, invdr2), invdr1);
+		u = dm_(myfac, ds_(cosgij, dm_(dm_(3., costi), costj)));
+		rf = -dm_(rffac, cosgij);
+		pR = dm_(dm_(-3., u), invdr2);
+		pTi = dm_(dm_(dm_(-myfac, 3.), costj), invdr1);
+		pTj = dm_(dm_(dm_(-myfac, 3.), costi), invdr1);
+		pG = myfac;
+	} else if (kind == 1) {
+		const double qfac = dm_(dm_(dm_(par, invdr2), invdr2), invdr1);
+		const double c2i = dm_(costi, costi), c2j = dm_(costj, costj);
+		const double term = ds_(cosgij, dm_(dm_(5., costi), costj));
+		u = dm_(qfac, da_(ds_(ds_(1., dm_(5., da_(c2i, c2j))), dm_(dm_(15., c2i), c2j)), dm_(dm_(2., term), term)));
+		pR = dm_(dm_(-5., u), invdr2);
+		pTi = dm_(dm_(dm_(-qfac, 10.), da_(da_(costi, dm_(dm_(3., costi), c2j)), dm_(dm_(2., costj), term))), invdr1);
+		pTj = dm_(dm_(dm_(-qfac, 10.), da_(da_(costj, dm_(dm_(3., c2i), costj)), dm_(dm_(2., costi), term))), invdr1);
+		pG = dm_(dm_(qfac, 4.), term);
+	} else {
+		const double myqfac = dm_(dm_(par, invdr2), invdr2);
+		const double c2j = dm_(costj, costj);
+		u = dm_(myqfac, da_(dm_(-costi, ds_(dm_(5., c2j), 1.)), dm_(dm_(2., cosgij), costj)));
+		pR = dm_(dm_(-4., u), invdr2);
+		pTi = dm_(dm_(myqfac, da_(dm_(-5., c2j), 1.)), invdr1);
+		pTj = dm_(dm_(dm_(myqfac, 2.), da_(dm_(dm_(-5., costi), costj), cosgij)), invdr1);
+		pG = dm_(dm_(myqfac, 2.), costj);
+	}
+	const double fac = da_(-pR, dm_(da_(dm_(costi, pTi), dm_(costj, pTj)), invdr1));
+	for (int d = 0; d < 3; d++) f[d] = ds_(ds_(dm_(fac, dr[d]), dm_(pTi, eii[d])), dm_(pTj, ejj[d]));
+	double eiXej[3], eXr[3];
+	cross3(eii, ejj, eiXej);
+	cross3(eii, dr, eXr);
+	const double g1 = kind == 0 ? da_(-pG, rffac) : -pG;
+	for (int d = 0; d < 3; d++) m1[d] = da_(dm_(-pTi, eXr[d]), dm_(g1, eiXej[d]));
+	cross3(ejj, dr, eXr);
+	const double g2 = kind == 0 ? ds_(pG, rffac) : pG;
+	for (int d = 0; d < 3; d++) m2[d] = da_(dm_(-pTj, eXr[d]), dm_(g2, eiXej[d]));
+}
+
+// One point-polarity site pair of PotForce(mi = i, mj = j) (potforce.h:372-542; charge-charge is
+// evaluated by the caller): the force on i's site (fi), the direct torque on i (mi), u, the
+// molecule pair's virial term (w, with the block's sign) and the MyRF increment. drm from j to i.
+__device__ void polar_pair(int ti, int tj, const double drm[3], const double di[3], const double dj[3],
+                           const double ei[3], const double ej[3], double si, double sj, double rfc, double fi[3],
+                           double mi[3], double& u, double& w, double& rf) {
+	double dr[3], f[3], mo[3];
+	const bool minus = (ti == 3 && tj != 3) || (ti == 2 && tj == 1);   // minusSiteSiteDistance blocks
+	for (int d = 0; d < 3; d++)
+		dr[d] = minus ? ds_(ds_(dj[d], drm[d]), di[d]) : ds_(da_(drm[d], di[d]), dj[d]);
+	const double dr2 = dot3(dr, dr);
+	mi[0] = mi[1] = mi[2] = 0.0;
+	rf = 0.0;
+	if (ti == 1) {                                   // Charge-Quadrupole, Charge-Dipole
+		charge_oriented(tj == 3, dr, dr2, ej, tj == 3 ? dm_(dm_(0.25, si), sj) : dm_(-si, sj), f, mo, u);
+	} else if (tj == 1) {                            // Quadrupole-Charge, Dipole-Charge
+		charge_oriented(ti == 3, dr, dr2, ei, ti == 3 ? dm_(dm_(0.25, sj), si) : dm_(-sj, si), f, mi, u);
+	} else if (ti == 3 && tj == 2) {                 // Quadrupole-Dipole: the dipole is the first argument
+		two_oriented(2, dr, dr2, ej, ei, dm_(dm_(1.5, si), sj), 0.0, f, mo, mi, u, rf);
+	} else {                                         // Quadrupole-Quadrupole, Dipole-Quadrupole, Dipole-Dipole
+		const int kind = ti == 3 ? 1 : (tj == 3 ? 2 : 0);
+		const double par = kind == 1 ? dm_(dm_(.75, si), sj) : (kind == 2 ? dm_(dm_(1.5, si), sj) : dm_(si, sj));
+		two_oriented(kind, dr, dr2, ei, ej, par, kind == 0 ? dm_(par, rfc) : 0.0, f, mi, mo, u, rf);
+	}
+	const double sgn = minus ? -1.0 : 1.0;
+	for (int d = 0; d < 3; d++) fi[d] = sgn * f[d];
+	w = sgn * dot3(drm, f);
 }
 
 struct RigidOut {
@@ -212,7 +339,8 @@ static_assert(kRigidLanes == 1 || kRigidLanes == 2 || kRigidLanes == 4 || kRigid
 // Forces are summed per centre of i, the lanes' sums combined in a fixed order (butterfly), and the
 // torque formed at the end as calcFM does (M = sum_s d_s x F_s); the virial term of a molecule pair
 // is drm . (sum of its centre forces).
-template <bool kMixed, int NS, bool kQ>
+// kQ: 0 LJ centres only, 1 with charges, 2 with dipoles or quadrupoles as well
+template <bool kMixed, int NS, int kQ>
 __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const double* __restrict__ rx,
                                                                const double* __restrict__ ry,
                                                                const double* __restrict__ rz,
@@ -221,11 +349,13 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
                                                                const int32_t* __restrict__ start, Grid g,
                                                                const RigidParams* __restrict__ P,
                                                                const double* __restrict__ ds,
-                                                               const float* __restrict__ dsf, RigidOut o) {
+                                                               const float* __restrict__ dsf,
+                                                               const double* __restrict__ es, RigidOut o) {
 	constexpr int TT = kMaxSiteTotal * kMaxSiteTotal;
 	__shared__ double s_e24[TT], s_sig2[TT], s_sh6[TT];
 	__shared__ int s_ns[kMaxSpecies], s_nlj[kMaxSpecies], s_base[kMaxSpecies];
-	__shared__ double s_q[kMaxSiteTotal];
+	__shared__ double s_q[kMaxSiteTotal], s_str[kMaxSiteTotal];
+	__shared__ int s_type[kMaxSiteTotal];
 	__shared__ float s_e24f[kMixed ? TT : 1], s_sig2f[kMixed ? TT : 1], s_qf[kMixed ? kMaxSiteTotal : 1];
 	__shared__ uint32_t s_list[kRigidList * kRigidThreads];
 	for (int k = threadIdx.x; k < TT; k += blockDim.x) {
@@ -244,7 +374,13 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 		s_nlj[threadIdx.x] = P->nlj[threadIdx.x];
 		s_base[threadIdx.x] = P->base[threadIdx.x];
 	}
-	if (threadIdx.x < kMaxSiteTotal) s_q[threadIdx.x] = P->charge[threadIdx.x];
+	if (threadIdx.x < kMaxSiteTotal) {
+		s_q[threadIdx.x] = P->charge[threadIdx.x];
+		s_str[threadIdx.x] = P->strength[threadIdx.x];
+		s_type[threadIdx.x] = P->type[threadIdx.x];
+	}
+	constexpr bool oriented = kQ == 2;
+	const double rfc = P->eps_rf_inv_rc3;
 	__syncthreads();
 	const double rc2 = P->rc2, rclj2 = P->rclj2;
 	const int64_t i = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) / kRigidLanes;
@@ -253,6 +389,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 #pragma unroll
 	for (int s = 0; s < NS; s++) Fs[s][0] = Fs[s][1] = Fs[s][2] = 0.0;
 	double U = 0.0, UX = 0.0, W = 0.0, np = 0.0;
+	double Md[3] = {0.0, 0.0, 0.0};   // direct torques of the dipole and quadrupole pairs (Madd)
 	bool same = false;
 	// centre offsets of i: double for the FP64 form, float for the mixed one (the double values are
 	// read again for the torque at the end)
@@ -309,7 +446,8 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 #pragma unroll
 						for (int si = 0; si < NS; si++) {
 							if (si >= nsi) break;
-							if (kQ && (si < nlji) != lj_j) continue;   // LJ with LJ, charge with charge
+							// LJ with LJ, charge with charge (the other point-polarity pairs below)
+							if (kQ && (lj_j ? si >= nlji : (s_type[bi + si] != 1 || s_type[bj + sj] != 1))) continue;
 							// SiteSiteDistance: drs = drm + d_i - d_j
 							const double s0 = __dsub_rn(__dadd_rn(m0, di[si][0]), dj0);
 							const double s1 = __dsub_rn(__dadd_rn(m1, di[si][1]), dj1);
@@ -359,7 +497,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 #pragma unroll
 						for (int si = 0; si < NS; si++) {
 							if (si >= nsi) break;
-							if (kQ && (si < nlji) != lj_j) continue;
+							if (kQ && (lj_j ? si >= nlji : (s_type[bi + si] != 1 || s_type[bj + sj] != 1))) continue;
 							const float s0 = e0 + dif[si][0] - dj0;
 							const float s1 = e1 + dif[si][1] - dj1;
 							const float s2 = e2 + dif[si][2] - dj2;
@@ -397,6 +535,43 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 						fp0 += (double) fs[si][0];
 						fp1 += (double) fs[si][1];
 						fp2 += (double) fs[si][2];
+					}
+				}
+				if constexpr (oriented) {
+					// pairs with a dipole or quadrupole, in double in both forms (polar_pair)
+					const double drm[3] = {m0, m1, m2};
+					for (int sj = nljj; sj < nsj; sj++) {
+						const int tj = s_type[bj + sj];
+						double dj[3], ej[3];
+						for (int k = 0; k < 3; k++) {
+							dj[k] = ds[(int64_t) (sj * 3 + k) * n + j];
+							ej[k] = es[(int64_t) (sj * 3 + k) * n + j];
+						}
+#pragma unroll
+						for (int si = 0; si < NS; si++) {
+							if (si >= nsi) break;
+							const int ti = s_type[bi + si];
+							if (ti == 0 || (ti == 1 && tj == 1)) continue;
+							if (ti == 1 && tj == 0) continue;
+							double dii[3], eii[3], fi[3], mi[3], u, w, rf;
+							for (int k = 0; k < 3; k++) {
+								dii[k] = ds[(int64_t) (si * 3 + k) * n + i];
+								eii[k] = es[(int64_t) (si * 3 + k) * n + i];
+							}
+							polar_pair(ti, tj, drm, dii, dj, eii, ej, s_str[bi + si], s_str[bj + sj], rfc, fi, mi, u, w, rf);
+							Fs[si][0] = __dadd_rn(Fs[si][0], fi[0]);
+							Fs[si][1] = __dadd_rn(Fs[si][1], fi[1]);
+							Fs[si][2] = __dadd_rn(Fs[si][2], fi[2]);
+							fp0 = __dadd_rn(fp0, fi[0]);
+							fp1 = __dadd_rn(fp1, fi[1]);
+							fp2 = __dadd_rn(fp2, fi[2]);
+							Md[0] = __dadd_rn(Md[0], mi[0]);
+							Md[1] = __dadd_rn(Md[1], mi[1]);
+							Md[2] = __dadd_rn(Md[2], mi[2]);
+							// ParticlePairs2PotForceAdapter::finish adds MyRF to Upot and 3 MyRF to the virial
+							UX = __dadd_rn(UX, __dadd_rn(u, rf));
+							W = __dadd_rn(W, __dmul_rn(3.0, rf));
+						}
 					}
 				}
 				// Virial += drm . f over the molecule pair's site pairs
@@ -478,6 +653,8 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 			for (int k = 0; k < 3; k++) Fs[s][k] = __dadd_rn(Fs[s][k], __shfl_xor_sync(0xffffffffu, Fs[s][k], o2));
 		U = __dadd_rn(U, __shfl_xor_sync(0xffffffffu, U, o2));
 		UX = __dadd_rn(UX, __shfl_xor_sync(0xffffffffu, UX, o2));
+		if constexpr (kQ == 2)
+			for (int k = 0; k < 3; k++) Md[k] = __dadd_rn(Md[k], __shfl_xor_sync(0xffffffffu, Md[k], o2));
 		W = __dadd_rn(W, __shfl_xor_sync(0xffffffffu, W, o2));
 		np += __shfl_xor_sync(0xffffffffu, np, o2);
 	}
@@ -503,6 +680,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 			Mt[1] = __dadd_rn(Mt[1], __dsub_rn(__dmul_rn(d[2], Fs[s][0]), __dmul_rn(d[0], Fs[s][2])));
 			Mt[2] = __dadd_rn(Mt[2], __dsub_rn(__dmul_rn(d[0], Fs[s][1]), __dmul_rn(d[1], Fs[s][0])));
 		}
+		for (int k = 0; k < 3; k++) Mt[k] = __dadd_rn(Mt[k], Md[k]);
 		o.fx[i] = F[0];
 		o.fy[i] = F[1];
 		o.fz[i] = F[2];
@@ -644,6 +822,13 @@ struct mdgpu_rigid {
 	double* M = nullptr;        // 3 x cap
 	double* ds = nullptr;       // 3 x ns_max x cap, sorted order
 	float* dsf = nullptr;       // the same in float (mixed form)
+	double* es = nullptr;       // rotated orientations of dipoles and quadrupoles, as ds
+	// the components as given (mdgpu_rigid_set_polarities rebuilds the site tables from them)
+	int ncomp = 0;
+	std::vector<int32_t> nlj_in, nq_in;
+	std::vector<mdgpu_site> sites_in;
+	std::vector<mdgpu_charge> charges_in;
+	std::vector<double> inertia_in, mix_in;
 	double* stage = nullptr;    // 4 x cap host <-> device staging
 	double* partials = nullptr; // per-block reduction partials (4 doubles per block of the pair kernel)
 	double* scal = nullptr;     // [0..2] pair sums, [3..4] kinetic sums
@@ -672,16 +857,16 @@ int launch_rigid_forces(mdgpu_rigid* h) {
 	prof_begin(c, 1);
 	const bool mixed = c->precision == MDGPU_MIXED;
 	k_rigid_sites<<<nb, kRigidThreads, 0, c->stream>>>(n, c->p.uidx, c->p.cid, h->q, h->dp, h->ds,
-	                                                   mixed ? h->dsf : nullptr);
+	                                                   mixed ? h->dsf : nullptr, h->hp.oriented ? h->es : nullptr);
 	RigidOut o{c->p.fx, c->p.fy, c->p.fz, h->M, h->partials, h->tickets, h->scal, c->status};
 	const int ns = h->hp.ns_max;
-	bool charged = false;
+	bool charged = false;   // any point polarity: the kernel variant with the polarity blocks
 	for (int k = 0; k < h->hp.nc; k++) charged |= h->hp.nsites[k] > h->hp.nlj[k];
-#define RG_PAIRS(MX, NSV)                                                                                     \
-	(charged ? k_rigid_pairs<MX, NSV, true><<<nbp, kRigidThreads, 0, c->stream>>>(                            \
-	               n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->p.uidx, c->cell_start, c->g, h->dp, h->ds, h->dsf, o) \
-	         : k_rigid_pairs<MX, NSV, false><<<nbp, kRigidThreads, 0, c->stream>>>(                           \
-	               n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->p.uidx, c->cell_start, c->g, h->dp, h->ds, h->dsf, o))
+#define RG_PAIRS_Q(MX, NSV, QV)                                                                               \
+	k_rigid_pairs<MX, NSV, QV><<<nbp, kRigidThreads, 0, c->stream>>>(                                         \
+	    n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->p.uidx, c->cell_start, c->g, h->dp, h->ds, h->dsf, h->es, o)
+#define RG_PAIRS(MX, NSV) \
+	(h->hp.oriented ? RG_PAIRS_Q(MX, NSV, 2) : (charged ? RG_PAIRS_Q(MX, NSV, 1) : RG_PAIRS_Q(MX, NSV, 0)))
 	if (ns <= 1)
 		mixed ? RG_PAIRS(true, 1) : RG_PAIRS(false, 1);
 	else if (ns == 2)
@@ -693,6 +878,7 @@ int launch_rigid_forces(mdgpu_rigid* h) {
 	else
 		mixed ? RG_PAIRS(true, kMaxSites) : RG_PAIRS(false, kMaxSites);
 #undef RG_PAIRS
+#undef RG_PAIRS_Q
 	prof_end(c, 1, 2);
 	RG_CUDA(cudaGetLastError());
 	return MDGPU_OK;
@@ -723,38 +909,48 @@ int launch_rigid_post(mdgpu_rigid* h, double dt_half, double* record) {
 	return MDGPU_OK;
 }
 
-// Site tables from the components (Comp2Param::initialize, Component::addLJcenter/addCharge): per
-// component its LJ centres (nlj[k], listed one component after another in `sites`), then its charges
-// (ncharges[k] in `charges`, which may be NULL for none).
+// Site tables from the components (Comp2Param::initialize, Component::addLJcenter/addCharge/
+// addDipole/addQuadrupole): per component its LJ centres (nlj[k], listed one component after another
+// in `sites`), then its charges (ncharges[k] in `charges`), dipoles and quadrupoles (any of these
+// lists may be NULL for none). eps_rf: the reaction field's permittivity (epsilonRF).
 int setup_rigid(Context* c, int ncomp, const int32_t* nlj, const mdgpu_site* sites, const int32_t* ncharges,
-                const mdgpu_charge* charges, const double* inertia, const double* mix, double rc, double rc_lj,
-                RigidParams& P) {
+                const mdgpu_charge* charges, const int32_t* ndipoles, const mdgpu_oriented* dipoles,
+                const int32_t* nquadrupoles, const mdgpu_oriented* quadrupoles, double eps_rf, const double* inertia,
+                const double* mix, double rc, double rc_lj, RigidParams& P) {
 	P = RigidParams{};
 	P.nc = ncomp;
 	P.rc2 = rc * rc;
 	P.rclj2 = rc_lj * rc_lj;
+	P.eps_rf_inv_rc3 = 2. * (eps_rf - 1.) / ((rc * rc * rc) * (2. * eps_rf + 1.));   // Comp2Param.cpp:178
 	int total = 0;
-	std::vector<int> lj_off(ncomp), q_off(ncomp);
-	int lo = 0, qo = 0;
+	std::vector<int> lj_off(ncomp), q_off(ncomp), d_off(ncomp), qq_off(ncomp), nq(ncomp), nd(ncomp), nqq(ncomp);
+	int lo = 0, qo = 0, dof = 0, qqo = 0;
 	for (int k = 0; k < ncomp; k++) {
-		const int nq = ncharges ? ncharges[k] : 0;
-		if (nlj[k] < 1 || nq < 0 || nlj[k] + nq > kMaxSites)
+		nq[k] = ncharges ? ncharges[k] : 0;
+		nd[k] = ndipoles ? ndipoles[k] : 0;
+		nqq[k] = nquadrupoles ? nquadrupoles[k] : 0;
+		if (nlj[k] < 1 || nq[k] < 0 || nd[k] < 0 || nqq[k] < 0 || nlj[k] + nq[k] + nd[k] + nqq[k] > kMaxSites)
 			return set_error(c, MDGPU_ERR_ARG, "each component needs at least one LJ centre and at most " +
-			                                       std::to_string(kMaxSites) + " LJ centres and charges");
-		if (nq > 0 && !charges) return set_error(c, MDGPU_ERR_ARG, "charges missing");
+			                                       std::to_string(kMaxSites) + " sites");
+		if ((nq[k] > 0 && !charges) || (nd[k] > 0 && !dipoles) || (nqq[k] > 0 && !quadrupoles))
+			return set_error(c, MDGPU_ERR_ARG, "point polarities missing");
 		P.nlj[k] = nlj[k];
-		P.nsites[k] = nlj[k] + nq;
+		P.nsites[k] = nlj[k] + nq[k] + nd[k] + nqq[k];
 		P.base[k] = total;
 		total += P.nsites[k];
 		P.ns_max = std::max(P.ns_max, P.nsites[k]);
 		lj_off[k] = lo;
 		q_off[k] = qo;
+		d_off[k] = dof;
+		qq_off[k] = qqo;
 		lo += nlj[k];
-		qo += nq;
+		qo += nq[k];
+		dof += nd[k];
+		qqo += nqq[k];
+		if (nd[k] + nqq[k] > 0) P.oriented = 1;
 	}
 	if (total > kMaxSiteTotal)
-		return set_error(c, MDGPU_ERR_ARG,
-		                 "at most " + std::to_string(kMaxSiteTotal) + " LJ centres and charges in all components");
+		return set_error(c, MDGPU_ERR_ARG, "at most " + std::to_string(kMaxSiteTotal) + " sites in all components");
 	P.nsite_total = total;
 	std::vector<double> shift(total, 0.0);
 	for (int k = 0; k < ncomp; k++) {
@@ -766,24 +962,41 @@ int setup_rigid(Context* c, int ncomp, const int32_t* nlj, const mdgpu_site* sit
 			I[1] += mass * (x * x + z * z);
 			I[2] += mass * (x * x + y * y);
 		};
+		const int b = P.base[k];
 		for (int s = 0; s < nlj[k]; s++) {
 			const mdgpu_site& t = sites[lj_off[k] + s];
 			if (!(t.mass > 0.0) || !(t.sigma > 0.0) || !(t.eps >= 0.0))
 				return set_error(c, MDGPU_ERR_ARG, "LJ centre with non-positive mass or sigma, or negative eps");
-			for (int d = 0; d < 3; d++) P.site[P.base[k] + s][d] = t.r[d];
+			for (int d = 0; d < 3; d++) P.site[b + s][d] = t.r[d];
+			P.type[b + s] = 0;
 			add_mass(t.r, t.mass);
 			if (t.do_shift) {   // Component::addLJcenter, with the centre's cutoff = LJCutoffRadius
 				const double sigperrc2 = t.sigma * t.sigma / (rc_lj * rc_lj);
 				const double sigperrc6 = sigperrc2 * sigperrc2 * sigperrc2;
-				shift[P.base[k] + s] = 24.0 * t.eps * (sigperrc6 - sigperrc6 * sigperrc6);
+				shift[b + s] = 24.0 * t.eps * (sigperrc6 - sigperrc6 * sigperrc6);
 			}
 		}
-		for (int s = nlj[k]; s < P.nsites[k]; s++) {
-			const mdgpu_charge& t = charges[q_off[k] + s - nlj[k]];
-			if (!(t.mass >= 0.0)) return set_error(c, MDGPU_ERR_ARG, "charge with negative mass");
-			for (int d = 0; d < 3; d++) P.site[P.base[k] + s][d] = t.r[d];
-			P.charge[P.base[k] + s] = t.q;
-			add_mass(t.r, t.mass);
+		int s = nlj[k];
+		for (int t = 0; t < nq[k]; t++, s++) {
+			const mdgpu_charge& x = charges[q_off[k] + t];
+			if (!(x.mass >= 0.0)) return set_error(c, MDGPU_ERR_ARG, "charge with negative mass");
+			for (int d = 0; d < 3; d++) P.site[b + s][d] = x.r[d];
+			P.charge[b + s] = x.q;
+			P.strength[b + s] = x.q;
+			P.type[b + s] = 1;
+			add_mass(x.r, x.mass);
+		}
+		for (int kind = 2; kind <= 3; kind++) {   // dipoles, then quadrupoles (massless)
+			const int cnt = kind == 2 ? nd[k] : nqq[k];
+			const mdgpu_oriented* list = kind == 2 ? dipoles + (nd[k] ? d_off[k] : 0) : quadrupoles + (nqq[k] ? qq_off[k] : 0);
+			for (int t = 0; t < cnt; t++, s++) {
+				for (int d = 0; d < 3; d++) {
+					P.site[b + s][d] = list[t].r[d];
+					P.e_body[b + s][d] = list[t].e[d];
+				}
+				P.strength[b + s] = list[t].strength;
+				P.type[b + s] = kind;
+			}
 		}
 		P.mass[k] = m;
 		for (int d = 0; d < 3; d++) {
@@ -839,9 +1052,10 @@ int ensure_capacity(mdgpu_rigid* h, int64_t n) {
 	cudaFree(h->M);
 	cudaFree(h->ds);
 	cudaFree(h->dsf);
+	cudaFree(h->es);
 	cudaFree(h->stage);
 	cudaFree(h->partials);
-	h->q = h->D = h->M = h->ds = h->stage = h->partials = nullptr;
+	h->q = h->D = h->M = h->ds = h->stage = h->partials = h->es = nullptr;
 	h->dsf = nullptr;
 	h->cap = 0;
 	RG_CUDA(cudaMalloc(&h->q, sizeof(double) * 4 * n));
@@ -849,6 +1063,7 @@ int ensure_capacity(mdgpu_rigid* h, int64_t n) {
 	RG_CUDA(cudaMalloc(&h->M, sizeof(double) * 3 * n));
 	RG_CUDA(cudaMalloc(&h->ds, sizeof(double) * 3 * std::max(1, h->hp.ns_max) * n));
 	RG_CUDA(cudaMalloc(&h->dsf, sizeof(float) * 3 * std::max(1, h->hp.ns_max) * n));
+	RG_CUDA(cudaMalloc(&h->es, sizeof(double) * 3 * std::max(1, h->hp.ns_max) * n));
 	RG_CUDA(cudaMalloc(&h->stage, sizeof(double) * 4 * n));
 	RG_CUDA(cudaMalloc(&h->partials, sizeof(double) * 4 * nblocks(n * kRigidLanes)));
 	h->cap = n;
@@ -890,7 +1105,16 @@ int mdgpu_rigid_create(mdgpu_rigid** out, const double length[3], double cutoff,
 	mdgpu_rigid* h = new mdgpu_rigid();
 	h->inner = inner;
 	Context* c = ctx_of(h);
-	st = setup_rigid(c, ncomp, nsites, sites, ncharges, charges, inertia, mix, c->rc, c->rc_lj, h->hp);
+	h->ncomp = ncomp;
+	h->nlj_in.assign(nsites, nsites + ncomp);
+	h->nq_in.assign(ncomp, 0);
+	if (ncharges) h->nq_in.assign(ncharges, ncharges + ncomp);
+	h->sites_in.assign(sites, sites + base);
+	if (charges && qbase > 0) h->charges_in.assign(charges, charges + qbase);
+	if (inertia) h->inertia_in.assign(inertia, inertia + 3 * ncomp);
+	if (mix && ncomp > 1) h->mix_in.assign(mix, mix + ncomp * (ncomp - 1));
+	st = setup_rigid(c, ncomp, nsites, sites, ncharges, charges, nullptr, nullptr, nullptr, nullptr, 1.0e10, inertia,
+	                 mix, c->rc, c->rc_lj, h->hp);
 	if (st == MDGPU_OK) {
 		cudaError_t e = cudaMalloc(&h->dp, sizeof(RigidParams));
 		if (e == cudaSuccess) e = cudaMemcpy(h->dp, &h->hp, sizeof(RigidParams), cudaMemcpyHostToDevice);
@@ -905,6 +1129,25 @@ int mdgpu_rigid_create(mdgpu_rigid** out, const double length[3], double cutoff,
 	return st;
 }
 
+int mdgpu_rigid_set_polarities(mdgpu_rigid* h, const int32_t* ndipoles, const mdgpu_oriented* dipoles,
+                               const int32_t* nquadrupoles, const mdgpu_oriented* quadrupoles, double epsilon_rf) {
+	if (!h) return MDGPU_ERR_ARG;
+	Context* c = ctx_of(h);
+	if (h->cap > 0)
+		return set_error(c, MDGPU_ERR_STATE, "point polarities must be set before mdgpu_rigid_set_particles");
+	if (!(epsilon_rf > 0.0)) return set_error(c, MDGPU_ERR_ARG, "epsilon_rf must be positive");
+	RigidParams P{};
+	int st = setup_rigid(c, h->ncomp, h->nlj_in.data(), h->sites_in.data(), h->nq_in.data(),
+	                     h->charges_in.empty() ? nullptr : h->charges_in.data(), ndipoles, dipoles, nquadrupoles,
+	                     quadrupoles, epsilon_rf, h->inertia_in.empty() ? nullptr : h->inertia_in.data(),
+	                     h->mix_in.empty() ? nullptr : h->mix_in.data(), c->rc, c->rc_lj, P);
+	if (st) return st;
+	h->hp = P;
+	RG_CUDA(cudaSetDevice(c->device));
+	RG_CUDA(cudaMemcpy(h->dp, &h->hp, sizeof(RigidParams), cudaMemcpyHostToDevice));
+	return MDGPU_OK;
+}
+
 int mdgpu_rigid_destroy(mdgpu_rigid* h) {
 	if (!h) return MDGPU_ERR_ARG;
 	if (h->inner) cudaSetDevice(h->inner->c.device);
@@ -914,6 +1157,7 @@ int mdgpu_rigid_destroy(mdgpu_rigid* h) {
 	cudaFree(h->M);
 	cudaFree(h->ds);
 	cudaFree(h->dsf);
+	cudaFree(h->es);
 	cudaFree(h->stage);
 	cudaFree(h->partials);
 	cudaFree(h->scal);

@@ -90,6 +90,7 @@ SIGNATURES = {
     "mdgpu_batch_skin_builds": (_I, [_VP, _VP]),
     "mdgpu_rigid_create": (_I, [ctypes.POINTER(_VP), _VP, _D, _D, _D, _I, _VP, _VP, _VP, _VP, _VP, _VP, _I, _I]),
     "mdgpu_rigid_destroy": (_I, [_VP]),
+    "mdgpu_rigid_set_polarities": (_I, [_VP, _VP, _VP, _VP, _VP, _D]),
     "mdgpu_rigid_last_error": (ctypes.c_char_p, [_VP]),
     "mdgpu_rigid_set_precision": (_I, [_VP, _I]),
     "mdgpu_rigid_get_inertia": (_I, [_VP, _I32, _VP, _VP]),
@@ -126,6 +127,23 @@ class _MdSite(ctypes.Structure):
 
 class _MdCharge(ctypes.Structure):
     _fields_ = [("r", ctypes.c_double * 3), ("mass", ctypes.c_double), ("q", ctypes.c_double)]
+
+
+class _MdOriented(ctypes.Structure):
+    _fields_ = [("r", ctypes.c_double * 3), ("e", ctypes.c_double * 3), ("strength", ctypes.c_double)]
+
+
+def _oriented(lists, strength_attr):
+    counts = np.array([len(x) for x in lists], dtype=np.int32)
+    arr = (_MdOriented * max(1, int(counts.sum())))()
+    k = 0
+    for x in lists:
+        for t in x:
+            arr[k].r[0], arr[k].r[1], arr[k].r[2] = float(t.x), float(t.y), float(t.z)
+            arr[k].e[0], arr[k].e[1], arr[k].e[2] = float(t.ex), float(t.ey), float(t.ez)
+            arr[k].strength = float(getattr(t, strength_attr))
+            k += 1
+    return counts, arr
 
 
 def load_library(path: str = LIB_PATH):
@@ -335,7 +353,7 @@ class RigidLinkedCells:
 
     def __init__(self, length: Sequence[float], cutoffRadius: float, components, mixcoeff=None,
                  LJCutoffRadius: float = 0.0, cellsInCutoffRadius: float = 1.0, precision: int = FP64,
-                 device: int = 0):
+                 device: int = 0, epsilonRF: float = 1.0e10):
         self.lib = load_library()
         centres = [c.lj_centres() for c in components]
         nsites = np.array([len(cs) for cs in centres], dtype=np.int32)
@@ -379,10 +397,19 @@ class RigidLinkedCells:
             raise MdgpuError(st, msg)
         self.n = 0
         self.components = components
+        dips = [c.point_dipoles() if hasattr(c, "point_dipoles") else [] for c in components]
+        quads = [c.point_quadrupoles() if hasattr(c, "point_quadrupoles") else [] for c in components]
+        if any(dips) or any(quads) or epsilonRF != 1.0e10:
+            nd, da = _oriented(dips, "abs_my")
+            nqq, qa = _oriented(quads, "abs_q")
+            self._check(self.lib.mdgpu_rigid_set_polarities(self.h, _ptr(nd), ctypes.cast(da, ctypes.c_void_p),
+                                                            _ptr(nqq), ctypes.cast(qa, ctypes.c_void_p),
+                                                            float(epsilonRF)))
 
     @classmethod
     def from_system(cls, system, precision: int = FP64, device: int = 0) -> "RigidLinkedCells":
-        lc = cls(system.length, system.cutoff, system.components, system.mix, system.lj_cutoff, 1.0, precision, device)
+        lc = cls(system.length, system.cutoff, system.components, system.mix, system.lj_cutoff, 1.0, precision, device,
+                 getattr(system, "epsilon_rf", 1.0e10))
         n = system.n
         q = system.q if system.q is not None else np.tile([1.0, 0.0, 0.0, 0.0], (n, 1))
         D = system.D if system.D is not None else np.zeros((n, 3))

@@ -4,9 +4,11 @@
   torques, Upot and virial of the start, and the state after 10 NVE steps (r, v, q, D, F, M, and the
   per-step Upot, virial, sum m v^2, sum I w^2) for a two-centre fluid, a two-component mix with a
   three-centre molecule whose centres differ, a bent molecule with three non-zero moments, a
-  two-centre molecule with point charges, and a three-component mix with charged and uncharged
-  molecules. FP64 agrees to rounding (1e-12 at the start, 1e-10 after 10 steps).
-* Charged molecules on a larger box: FP64 against the oracle (1e-12), the mixed form within 1e-5.
+  two-centre molecule with point charges, a three-component mix with charged and uncharged
+  molecules, a dipolar fluid, and a mix of quadrupolar, dipolar and charged molecules with a
+  reaction field. FP64 agrees to rounding (1e-12 at the start, 1e-10 after 10 steps).
+* Charged molecules, and a mix with dipoles, quadrupoles and a reaction field, on a larger box:
+  FP64 against the oracle (1e-12), the mixed form within 1e-5.
 * The oracle (oracle/rigid.py) on a larger box (more cells, the same code path at other sizes).
 * Single-centre components through the rigid path give the single-centre container's forces.
 * The step-by-step sequence equals mdgpu_rigid_run bit for bit; the mixed form stays within 1e-5 of
@@ -135,9 +137,16 @@ def test_rigid_mixed_accuracy():
     b.close()
 
 
-def test_rigid_charged_mixed_accuracy():
-    s = W.rigid_fcc_box(8, 0.25, 1.5, 41, 3.0, [W.charged_two_centre(0.7), W.bent_three_centre()], [0.6, 0.4],
-                        np.array([[0.95, 1.0]]))
+@pytest.mark.parametrize("polar", [False, True])
+def test_rigid_charged_mixed_accuracy(polar):
+    if polar:
+        comps = [W.charged_two_centre(0.7), W.dipolar_two_centre(1.0), W.quadrupolar_two_centre(0.8),
+                 W.bent_three_centre()]
+        s = W.rigid_fcc_box(8, 0.25, 1.5, 42, 3.0, comps, [0.25] * 4, np.ones((6, 2)))
+        s.epsilon_rf = 3.0
+    else:
+        s = W.rigid_fcc_box(8, 0.25, 1.5, 41, 3.0, [W.charged_two_centre(0.7), W.bent_three_centre()], [0.6, 0.4],
+                            np.array([[0.95, 1.0]]))
     a, ua, wa, _ = start(s, M.FP64)
     b, ub, wb, _ = start(s, M.MIXED)
     f = R.forces(R.Model(s), s.r, s.cid.astype(np.int64), s.q)
