@@ -4,9 +4,13 @@
 accumulation on one B200 (one independent box per GPU when run on several).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision mixed|fp64]
+  python bench.py --workload c3|batched|checkpoint|rigid [--charges]
 
 One step = Leapfrog kick+drift, periodic wrap + linked-cell binning, the pair traversal (forces,
-Upot, virial) and the closing kick with sum m v^2, i.e. Simulation::simulateStep's hot path.
+Upot, virial) and the closing kick with sum m v^2, i.e. Simulation::simulateStep's hot path. The
+other workloads: the 4M-molecule two-species slab (c3), the 512-box ensemble (batched), phase-space
+file write and read of the 1M-molecule box (checkpoint), and 1M rigid two-centre molecules with
+quaternion integration, optionally with point charges (rigid).
 """
 from __future__ import annotations
 
