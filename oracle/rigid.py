@@ -263,9 +263,11 @@ def di_quadrupole(dr, dr2, eii, ejj, myq15):
     return f, m1, m2, u
 
 
-def forces(model: Model, r: np.ndarray, cid: np.ndarray, q: np.ndarray) -> Dict:
-    """F, M per molecule, Upot (Upot6LJ/6 + UpotXpoles), virial and the number of molecule pairs
-    within rc."""
+def forces(model: Model, r: np.ndarray, cid: np.ndarray, q: np.ndarray, both_sided: bool = False) -> Dict:
+    """F, M per molecule, Upot (Upot6LJ/6 + UpotXpoles + MyRF), virial and the number of molecule
+    pairs within rc. Each unordered pair once, as the reference; with both_sided every molecule i
+    takes PotForce(mi = i, mj = j) with every other j and keeps only its own share (the device
+    path's order of work), the scalars halved."""
     n = r.shape[0]
     L = model.L
     d, oe = site_offsets(model, cid, q, orient=True)
@@ -277,8 +279,9 @@ def forces(model: Model, r: np.ndarray, cid: np.ndarray, q: np.ndarray) -> Dict:
     W = 0.0
     npairs = 0
     rc2, rclj2 = model.rc * model.rc, model.rclj * model.rclj
-    for i in range(n - 1):
-        j = np.arange(i + 1, n)
+    Fs, Ms = (np.zeros((n, 3)), np.zeros((n, 3))) if both_sided else (F, M)   # partners' shares
+    for i in range(n if both_sided else n - 1):
+        j = np.delete(np.arange(n), i) if both_sided else np.arange(i + 1, n)
         drm = r[i][None, :] - r[j]
         drm -= L[None, :] * np.round(drm / L[None, :])
         dd = np.einsum("ij,ij->i", drm, drm)
@@ -292,7 +295,7 @@ def forces(model: Model, r: np.ndarray, cid: np.ndarray, q: np.ndarray) -> Dict:
             if not sel.any():
                 continue
             jj, dm = j[sel], drm[sel]
-            UX, W, RF = _polar_blocks(model, ci, cj, i, jj, dm, d, oe, F, M, UX, W, RF)
+            UX, W, RF = _polar_blocks(model, ci, cj, i, jj, dm, d, oe, F, M, UX, W, RF, Fs, Ms)
         lj = dd < rclj2
         j, drm = j[lj], drm[lj]
         for cj in range(model.nc):
@@ -316,16 +319,17 @@ def forces(model: Model, r: np.ndarray, cid: np.ndarray, q: np.ndarray) -> Dict:
                     fac = e24 * (lj12 + lj12m6) * inv
                     f = fac[:, None] * drs
                     F[i] += f.sum(axis=0)
-                    np.subtract.at(F, jj, f)
+                    np.subtract.at(Fs, jj, f)
                     M[i] += np.cross(di[None, :], f).sum(axis=0)
-                    np.subtract.at(M, jj, np.cross(dj, f))
+                    np.subtract.at(Ms, jj, np.cross(dj, f))
                     U6 += float(u.sum())
                     W += float(np.einsum("ij,ij->", dm, f))
+    h = 0.5 if both_sided else 1.0
     # ParticlePairs2PotForceAdapter::finish: Upot6LJ/6 + UpotXpoles + MyRF, Virial + 3 MyRF
-    return dict(F=F, M=M, upot=U6 / 6.0 + UX + RF, virial=W + 3.0 * RF, npairs=npairs)
+    return dict(F=F, M=M, upot=h * (U6 / 6.0 + UX + RF), virial=h * (W + 3.0 * RF), npairs=int(h * npairs))
 
 
-def _polar_blocks(model, ci, cj, i, jj, dm, d, oe, F, M, UX, W, RF):
+def _polar_blocks(model, ci, cj, i, jj, dm, d, oe, F, M, UX, W, RF, Fs=None, Ms=None):
     """Charge, dipole and quadrupole pairs of molecule i (mi) with the molecules jj (mj) of component
     cj, drm = dm (from j to i), in PotForce's order (potforce.h:372-542): site forces (+f on the
     SiteSiteDistance side), the direct torques (Madd), UpotXpoles, Virial and MyRF."""
@@ -339,19 +343,21 @@ def _polar_blocks(model, ci, cj, i, jj, dm, d, oe, F, M, UX, W, RF):
     qd_i = lambda a: model.first_quad[ci] + a  # noqa: E731
     qd_j = lambda b: model.first_quad[cj] + b  # noqa: E731
     Wacc = [W]
+    Fs = F if Fs is None else Fs
+    Ms = M if Ms is None else Ms
 
     def apply(si, sj, f, sign, m_i=None, m_j=None):
         # sign +1: mi gets +f, mj gets -f; sign -1 the other way round (minusSiteSiteDistance blocks)
         di, dj = d[si][i], d[sj][jj]
         fi = sign * f
         F[i] += fi.sum(axis=0)
-        np.subtract.at(F, jj, fi)
+        np.subtract.at(Fs, jj, fi)
         M[i] += np.cross(di[None, :], fi).sum(axis=0)
-        np.subtract.at(M, jj, np.cross(dj, fi))
+        np.subtract.at(Ms, jj, np.cross(dj, fi))
         if m_i is not None:
             M[i] += m_i.sum(axis=0)
         if m_j is not None:
-            np.add.at(M, jj, m_j)
+            np.add.at(Ms, jj, m_j)
         Wacc[0] += sign * float(np.einsum("ij,ij->", dm, f))
 
     def plus(si, sj):

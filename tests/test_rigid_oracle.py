@@ -113,3 +113,19 @@ def test_rigid_phase_space_round_trip(tmp_path):
 def test_energy_fixture_start_is_reproducible():
     s, d = energy_fixture()
     assert s.n == 4000 and d["upot"].shape == (1001,)
+
+
+@pytest.mark.parametrize("name", ["rigid_charged_mix_256", "rigid_polar_mix_256"])
+def test_both_sided_evaluation_equals_the_reference_order(name):
+    """The device path evaluates every pair from both sides, each molecule taking PotForce's blocks
+    with itself as mi (charge-dipole on one side, dipole-charge on the other, and so on) and keeping
+    its own share; that gives the reference's forces, torques, Upot and virial."""
+    s, d = golden_system(name)
+    m = R.Model(s)
+    one = R.forces(m, s.r, s.cid.astype(np.int64), s.q)
+    two = R.forces(m, s.r, s.cid.astype(np.int64), s.q, both_sided=True)
+    assert rel(two["F"], one["F"]) < 1e-12 and rel(two["M"], one["M"]) < 1e-12
+    assert abs(two["upot"] - one["upot"]) <= 1e-12 * abs(one["upot"])
+    assert abs(two["virial"] - one["virial"]) <= 1e-12 * abs(one["virial"])
+    assert two["npairs"] == one["npairs"]
+    assert rel(one["F"], d["F0"]) < 1e-12
