@@ -704,7 +704,8 @@ MIN_BETA = 0.9  # Domain.h:33
 
 
 class Domain:
-    """Upot, virial, temperature and the thermostat factor (Domain.cpp:102-263, one thermostat)."""
+    """Upot, virial, temperature and the thermostat factors (Domain.cpp:102-263, one thermostat),
+    with the rotational degrees of freedom of rigid molecules (sum I w^2, rotDOF, beta_rot)."""
 
     def __init__(self, target_temperature: float = 1.0, nve: bool = True):
         self.target_temperature = float(target_temperature)
@@ -718,6 +719,9 @@ class Domain:
         self.global_virial = 0.0
         self.temperature = target_temperature
         self.beta_trans = 1.0
+        self.beta_rot = 1.0
+        self.sum_iw2 = 0.0
+        self.rot_dof = 0
         self.n = 0
 
     def setLocalUpot(self, u: float) -> None:
@@ -729,19 +733,27 @@ class Domain:
     def getGlobalBetaTrans(self) -> float:
         return self.beta_trans
 
+    def getGlobalBetaRot(self) -> float:
+        return self.beta_rot
+
     def calculateGlobalValues(self, tfactor: float = 1.0) -> None:
         """Domain::calculateGlobalValues (Domain.cpp:158-263) for one process and one thermostat."""
         self.global_upot = self.local_upot + self.upot_corr
         self.global_virial = self.local_virial + self.virial_corr
         n = self.n
-        self.temperature = (self.summv2 + 0.0) / float(3 * n + 0) if n > 0 else self.target_temperature
+        rot_dof = self.rot_dof
+        sum_iw2 = self.sum_iw2 if rot_dof > 0 else 0.0
+        self.temperature = ((self.summv2 + sum_iw2) / float(3 * n + rot_dof) if n > 0
+                            else self.target_temperature)
         ti = tfactor * self.target_temperature
         if ti > 0.0 and not self.nve:
             self.beta_trans = math.pow(3.0 * n * ti / self.summv2, 0.4)
+            self.beta_rot = 1.0 if sum_iw2 == 0.0 else math.pow(rot_dof * ti / sum_iw2, 0.4)
         else:
             self.beta_trans = 1.0
-        if self.beta_trans < MIN_BETA:
-            raise MdgpuError(8, "explosion: beta_trans below MIN_BETA (the selective thermostat is not provided)")
+            self.beta_rot = 1.0
+        if self.beta_trans < MIN_BETA or self.beta_rot < MIN_BETA:
+            raise MdgpuError(8, "explosion: beta below MIN_BETA (the selective thermostat is not provided)")
 
 
 class Leapfrog:

@@ -129,3 +129,25 @@ def test_both_sided_evaluation_equals_the_reference_order(name):
     assert abs(two["virial"] - one["virial"]) <= 1e-12 * abs(one["virial"])
     assert two["npairs"] == one["npairs"]
     assert rel(one["F"], d["F0"]) < 1e-12
+
+
+def test_domain_temperature_and_betas_with_rotation():
+    """Domain::calculateGlobalValues with rotational degrees of freedom (Domain.cpp:223-262):
+    T = (sum m v^2 + sum I w^2) / (3N + rotDOF); beta_trans = (3N Ti / sum m v^2)^0.4,
+    beta_rot = (rotDOF Ti / sum I w^2)^0.4 when thermostatted, 1 under NVE."""
+    from madpac_b200 import mdgpu as M
+
+    d = M.Domain(1.5, nve=False)
+    d.n, d.rot_dof, d.summv2, d.sum_iw2 = 1000, 2000, 4200.0, 3100.0
+    d.calculateGlobalValues()
+    assert d.temperature == (4200.0 + 3100.0) / 5000.0
+    assert d.beta_trans == (3000 * 1.5 / 4200.0) ** 0.4 and d.beta_rot == (2000 * 1.5 / 3100.0) ** 0.4
+    nve = M.Domain(1.5, nve=True)
+    nve.n, nve.rot_dof, nve.summv2, nve.sum_iw2 = 1000, 2000, 4200.0, 3100.0
+    nve.calculateGlobalValues()
+    assert nve.beta_trans == 1.0 and nve.beta_rot == 1.0
+    # no rotational degrees of freedom: the single-centre formula
+    single = M.Domain(1.0, nve=False)
+    single.n, single.summv2 = 100, 310.0
+    single.calculateGlobalValues()
+    assert single.temperature == 310.0 / 300.0 and single.beta_rot == 1.0
