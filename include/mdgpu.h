@@ -307,6 +307,19 @@ int mdgpu_rigid_set_precision(mdgpu_rigid* h, int precision);
  * pairs with a dipole or quadrupole are evaluated in double in both precision modes. */
 int mdgpu_rigid_set_polarities(mdgpu_rigid* h, const int32_t* ndipoles, const mdgpu_oriented* dipoles,
                                const int32_t* nquadrupoles, const mdgpu_oriented* quadrupoles, double epsilon_rf);
+/* The far-field corrections of Domain::initFarFieldCorr (Domain.cpp:574-677) for rigid components:
+ * the LJ tail beyond LJCutoffRadius of every unshifted centre pair (TICC/TICS/TISS integrals of
+ * CutoffCorrections.cpp over the centres' distances from the centre of mass; MDGPU_ERR_ARG when two
+ * of them reach the cutoff together) and the reaction field's self term of each molecule's dipole
+ * (its charges' q r plus its dipoles). Host arithmetic only (no context, no device): components as
+ * for mdgpu_rigid_create (dipoles as for mdgpu_rigid_set_polarities; NULL for none), counts[c]
+ * molecules of component c in the box of edges `length`. upot_corr and virial_corr receive the
+ * reference's _UpotCorr and _VirialCorr. */
+int mdgpu_rigid_far_field_correction(int ncomp, const int32_t* nsites, const mdgpu_site* sites,
+                                     const int32_t* ncharges, const mdgpu_charge* charges,
+                                     const int32_t* ndipoles, const mdgpu_oriented* dipoles, const double* mix,
+                                     const int64_t* counts, const double length[3], double cutoff,
+                                     double lj_cutoff, double epsilon_rf, double* upot_corr, double* virial_corr);
 /* Total mass and principal moments of component comp (Component::m, I11/I22/I33). */
 int mdgpu_rigid_get_inertia(const mdgpu_rigid* h, int32_t comp, double* mass, double I[3]);
 /* Loads the molecules (q and D required); forces and torques start at zero. */

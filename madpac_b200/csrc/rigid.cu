@@ -1148,6 +1148,121 @@ int mdgpu_rigid_set_polarities(mdgpu_rigid* h, const int32_t* ndipoles, const md
 	return MDGPU_OK;
 }
 
+namespace {
+
+// CutoffCorrections.cpp: radial integrals of the LJ tail beyond rc for centre-centre (TICC),
+// centre-site (TICS) and site-site (TISS) pairs, tau the sites' distances from the centres of mass.
+double ticc_u(int n, double rc, double sigma2) { return -std::pow(rc, 2 * n + 3) / (std::pow(sigma2, n) * (2 * n + 3)); }
+double tics_u(int n, double rc, double sigma2, double tau) {
+	return -(std::pow(rc + tau, 2 * n + 3) - std::pow(rc - tau, 2 * n + 3)) * rc /
+	           (4 * std::pow(sigma2, n) * tau * (n + 1) * (2 * n + 3)) +
+	       (std::pow(rc + tau, 2 * n + 4) - std::pow(rc - tau, 2 * n + 4)) /
+	           (4 * std::pow(sigma2, n) * tau * (n + 1) * (2 * n + 3) * (2 * n + 4));
+}
+double tiss_u(int n, double rc, double sigma2, double tau1, double tau2) {
+	const double tp = tau1 + tau2, tm = tau1 - tau2;
+	return -(std::pow(rc + tp, 2 * n + 4) - std::pow(rc + tm, 2 * n + 4) - std::pow(rc - tm, 2 * n + 4) +
+	         std::pow(rc - tp, 2 * n + 4)) *
+	           rc / (8 * std::pow(sigma2, n) * tau1 * tau2 * (n + 1) * (2 * n + 3) * (2 * n + 4)) +
+	       (std::pow(rc + tp, 2 * n + 5) - std::pow(rc + tm, 2 * n + 5) - std::pow(rc - tm, 2 * n + 5) +
+	        std::pow(rc - tp, 2 * n + 5)) /
+	           (8 * std::pow(sigma2, n) * tau1 * tau2 * (n + 1) * (2 * n + 3) * (2 * n + 4) * (2 * n + 5));
+}
+double ticc_v(int n, double rc, double sigma2) { return 2 * n * ticc_u(n, rc, sigma2); }
+double tics_v(int n, double rc, double sigma2, double tau) {
+	return -(std::pow(rc + tau, 2 * n + 2) - std::pow(rc - tau, 2 * n + 2)) * rc * rc /
+	           (4 * std::pow(sigma2, n) * tau * (n + 1)) -
+	       3 * tics_u(n, rc, sigma2, tau);
+}
+double tiss_v(int n, double rc, double sigma2, double tau1, double tau2) {
+	const double tp = tau1 + tau2, tm = tau1 - tau2;
+	return -(std::pow(rc + tp, 2 * n + 3) - std::pow(rc + tm, 2 * n + 3) - std::pow(rc - tm, 2 * n + 3) +
+	         std::pow(rc - tp, 2 * n + 3)) *
+	           rc * rc / (8 * std::pow(sigma2, n) * tau1 * tau2 * (n + 1) * (2 * n + 3)) -
+	       3 * tiss_u(n, rc, sigma2, tau1, tau2);
+}
+
+}  // namespace
+
+int mdgpu_rigid_far_field_correction(int ncomp, const int32_t* nsites, const mdgpu_site* sites, const int32_t* ncharges,
+                                     const mdgpu_charge* charges, const int32_t* ndipoles,
+                                     const mdgpu_oriented* dipoles, const double* mix, const int64_t* counts,
+                                     const double length[3], double cutoff, double lj_cutoff, double epsilon_rf,
+                                     double* upot_corr, double* virial_corr) {
+	if (ncomp < 1 || ncomp > kMaxSpecies || !nsites || !sites || !counts || !length) return MDGPU_ERR_ARG;
+	if (!(cutoff > 0.0)) return MDGPU_ERR_ARG;
+	const double rc_lj = lj_cutoff > 0.0 ? lj_cutoff : cutoff;
+	Context c;   // host-only: receives the error text of the table set-up
+	RigidParams P;
+	int st = setup_rigid(&c, ncomp, nsites, sites, ncharges, charges, nullptr, nullptr, nullptr, nullptr, epsilon_rf,
+	                     nullptr, mix, cutoff, rc_lj, P);
+	if (st) return st;
+	double upot_lj = 0., virial_lj = 0., self_term = 0.;
+	int64_t nmol = 0;
+	int lo = 0, qo = 0, dof = 0;
+	std::vector<int> lj_off(ncomp);
+	for (int i = 0; i < ncomp; ++i) {
+		lj_off[i] = lo;
+		lo += nsites[i];
+	}
+	for (int i = 0; i < ncomp; ++i) {
+		nmol += counts[i];
+		// the molecule's dipole from its charges and dipoles (Domain.cpp:586-609)
+		double balance[3] = {0., 0., 0.};
+		const int nq = ncharges ? ncharges[i] : 0, nd = ndipoles ? ndipoles[i] : 0;
+		for (int s = 0; s < nq; s++)
+			for (int d = 0; d < 3; d++) balance[d] += charges[qo + s].q * charges[qo + s].r[d];
+		for (int s = 0; s < nd; s++) {
+			const mdgpu_oriented& t = dipoles[dof + s];
+			double evect = 0;
+			for (int d = 0; d < 3; d++) evect += t.e[d] * t.e[d];
+			const double norm = 1.0 / std::sqrt(evect);
+			for (int d = 0; d < 3; d++) balance[d] += t.strength * t.e[d] * norm;
+		}
+		qo += nq;
+		dof += nd;
+		double my2 = 0.0;
+		for (int d = 0; d < 3; d++) my2 += balance[d] * balance[d];
+		self_term += my2 * (double) counts[i];
+		for (int j = 0; j < ncomp; ++j) {
+			for (int si = 0; si < nsites[i]; ++si) {
+				const double* ri = sites[lj_off[i] + si].r;
+				const double tau1 = std::sqrt(ri[0] * ri[0] + ri[1] * ri[1] + ri[2] * ri[2]);
+				for (int sj = 0; sj < nsites[j]; ++sj) {
+					const double* rj = sites[lj_off[j] + sj].r;
+					double tau2 = std::sqrt(rj[0] * rj[0] + rj[1] * rj[1] + rj[2] * rj[2]);
+					if (tau1 + tau2 >= rc_lj) return MDGPU_ERR_ARG;   // "rc too small" (Domain.cpp:622-625)
+					const int k = (P.base[i] + si) * kMaxSiteTotal + P.base[j] + sj;
+					if (P.shift6[k] != 0.0) continue;   // truncated-shifted pairs have no tail correction
+					const double eps24 = P.eps24[k], sig2 = P.sig2[k];
+					const double fac = double(counts[i]) * double(counts[j]) * eps24;
+					if (tau1 == 0. && tau2 == 0.) {
+						upot_lj += fac * (ticc_u(-6, rc_lj, sig2) - ticc_u(-3, rc_lj, sig2));
+						virial_lj += fac * (ticc_v(-6, rc_lj, sig2) - ticc_v(-3, rc_lj, sig2));
+					} else if (tau1 != 0. && tau2 != 0.) {
+						upot_lj += fac * (tiss_u(-6, rc_lj, sig2, tau1, tau2) - tiss_u(-3, rc_lj, sig2, tau1, tau2));
+						virial_lj += fac * (tiss_v(-6, rc_lj, sig2, tau1, tau2) - tiss_v(-3, rc_lj, sig2, tau1, tau2));
+					} else {
+						if (tau2 == 0.) tau2 = tau1;
+						upot_lj += fac * (tics_u(-6, rc_lj, sig2, tau2) - tics_u(-3, rc_lj, sig2, tau2));
+						virial_lj += fac * (tics_v(-6, rc_lj, sig2, tau2) - tics_v(-3, rc_lj, sig2, tau2));
+					}
+				}
+			}
+		}
+	}
+	if (nmol <= 0) return MDGPU_ERR_ARG;
+	const double rho = double(nmol) / (length[0] * length[1] * length[2]);
+	const double fac = M_PI * rho / (3. * double(nmol));
+	upot_lj *= fac;
+	virial_lj *= -fac;
+	const double eps_rf_inv_rc3 = 2. * (epsilon_rf - 1.) / ((cutoff * cutoff * cutoff) * (2. * epsilon_rf + 1.));
+	self_term *= -0.5 * eps_rf_inv_rc3;
+	if (upot_corr) *upot_corr = upot_lj + self_term;
+	if (virial_corr) *virial_corr = virial_lj + 3. * self_term;
+	return MDGPU_OK;
+}
+
 int mdgpu_rigid_destroy(mdgpu_rigid* h) {
 	if (!h) return MDGPU_ERR_ARG;
 	if (h->inner) cudaSetDevice(h->inner->c.device);

@@ -91,6 +91,7 @@ SIGNATURES = {
     "mdgpu_rigid_create": (_I, [ctypes.POINTER(_VP), _VP, _D, _D, _D, _I, _VP, _VP, _VP, _VP, _VP, _VP, _I, _I]),
     "mdgpu_rigid_destroy": (_I, [_VP]),
     "mdgpu_rigid_set_polarities": (_I, [_VP, _VP, _VP, _VP, _VP, _D]),
+    "mdgpu_rigid_far_field_correction": (_I, [_I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _D, _D, _D, _VP, _VP]),
     "mdgpu_rigid_last_error": (ctypes.c_char_p, [_VP]),
     "mdgpu_rigid_set_precision": (_I, [_VP, _I]),
     "mdgpu_rigid_get_inertia": (_I, [_VP, _I32, _VP, _VP]),
@@ -131,6 +132,52 @@ class _MdCharge(ctypes.Structure):
 
 class _MdOriented(ctypes.Structure):
     _fields_ = [("r", ctypes.c_double * 3), ("e", ctypes.c_double * 3), ("strength", ctypes.c_double)]
+
+
+def _site_tables(components):
+    """ctypes arrays of the components' LJ centres and charges: (nsites, sites, ncharges, charges)."""
+    centres = [c.lj_centres() for c in components]
+    nsites = np.array([len(cs) for cs in centres], dtype=np.int32)
+    sites = (_MdSite * int(nsites.sum()))()
+    k = 0
+    for cs in centres:
+        for t in cs:
+            sites[k].r[0], sites[k].r[1], sites[k].r[2] = float(t.x), float(t.y), float(t.z)
+            sites[k].mass, sites[k].eps, sites[k].sigma = float(t.mass), float(t.eps), float(t.sigma)
+            sites[k].do_shift = 1 if t.do_shift else 0
+            k += 1
+    qs = [c.point_charges() if hasattr(c, "point_charges") else [] for c in components]
+    ncharges = np.array([len(x) for x in qs], dtype=np.int32)
+    charges = (_MdCharge * max(1, int(ncharges.sum())))()
+    k = 0
+    for x in qs:
+        for t in x:
+            charges[k].r[0], charges[k].r[1], charges[k].r[2] = float(t.x), float(t.y), float(t.z)
+            charges[k].mass, charges[k].q = float(t.mass), float(t.q)
+            k += 1
+    return nsites, sites, ncharges, charges
+
+
+def rigid_far_field_correction(system):
+    """Domain::initFarFieldCorr (Domain.cpp:574-677) for the system's rigid components and molecule
+    counts: (UpotCorr, VirialCorr). Host arithmetic in libmdgpu.so; no device needed."""
+    lib = load_library()
+    comps = system.components
+    nsites, sites, ncharges, charges = _site_tables(comps)
+    nd, da = _oriented([c.point_dipoles() if hasattr(c, "point_dipoles") else [] for c in comps], "abs_my")
+    counts = np.bincount(np.asarray(system.cid, dtype=np.int64), minlength=len(comps)).astype(np.int64)
+    length = _c64(system.length)
+    mix = _c64(system.mix).reshape(-1)
+    u, w = ctypes.c_double(), ctypes.c_double()
+    st = lib.mdgpu_rigid_far_field_correction(len(comps), _ptr(nsites), ctypes.cast(sites, ctypes.c_void_p),
+                                              _ptr(ncharges), ctypes.cast(charges, ctypes.c_void_p), _ptr(nd),
+                                              ctypes.cast(da, ctypes.c_void_p), _ptr(mix) if mix.size else None,
+                                              _ptr(counts), _ptr(length), float(system.cutoff),
+                                              float(system.lj_cutoff), float(getattr(system, "epsilon_rf", 1.0e10)),
+                                              ctypes.byref(u), ctypes.byref(w))
+    if st != 0:
+        raise MdgpuError(st, "far-field correction: cutoff too small for the molecules or bad components")
+    return u.value, w.value
 
 
 def _oriented(lists, strength_attr):

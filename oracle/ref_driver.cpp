@@ -19,6 +19,7 @@
 //        ref_driver --checkpoint <cfg> <nsteps> <file> <outdir>   (the reference's checkpoint after
 //                   nsteps steps, and the exact state of that step)
 //        ref_driver --time-checkpoint <cfg> <file>   (seconds to write the initial state's checkpoint)
+//        ref_driver --farfield <cfg>   (Domain::initFarFieldCorr's _UpotCorr and _VirialCorr as JSON)
 #include <sys/time.h>
 
 #include <algorithm>
@@ -30,12 +31,13 @@
 #include <string>
 #include <vector>
 
-// getCellIndexOfMolecule is private in LinkedCells; the harness reads it directly.
+// getCellIndexOfMolecule is private in LinkedCells and the far-field terms are private in Domain;
+// the harness reads them directly.
 #define private public
 #include "particleContainer/LinkedCells.h"
+#include "Domain.h"
 #undef private
 
-#include "Domain.h"
 #include "Simulation.h"
 #include "molecules/Molecule.h"
 #include "particleContainer/ParticleContainer.h"
@@ -63,6 +65,8 @@ struct Rec {
 
 class RefDriver : public Simulation {
 public:
+	Domain* domain() { return _domain; }
+
 	double summv2() {
 		double s = 0.0;
 		for (Molecule* m = _moleculeContainer->begin(); m != _moleculeContainer->end(); m = _moleculeContainer->next()) {
@@ -204,6 +208,13 @@ int main(int argc, char** argv) {
 		RefDriver sim;
 		sim.readConfigFile(argv[2]);
 		sim.checkpoint(strtoul(argv[3], nullptr, 10), argv[4], argv[5]);
+		return 0;
+	}
+	if (argc >= 3 && std::string(argv[1]) == "--farfield") {
+		RefDriver sim;
+		sim.readConfigFile(argv[2]);
+		printf("{\"upot_corr\": %.17g, \"virial_corr\": %.17g}\n", sim.domain()->_UpotCorr,
+		       sim.domain()->_VirialCorr);
 		return 0;
 	}
 	if (argc >= 4 && std::string(argv[1]) == "--time-checkpoint") {

@@ -20,6 +20,9 @@ rigid_<name>.npz (the start state is stored too, so the fixtures do not depend o
 * rigid_polar_mix_256: quadrupolar (Q 1.0), dipolar (0.9) and charged (+-0.6) two-centre molecules,
                    40/30/30, rho 0.25, T 1.8, rc 3.0, reaction field epsilon_RF 5 (every point-polarity
                    block of PotForce and MyRF);
+* rigid_far_field.json: Domain::initFarFieldCorr's UpotCorr and VirialCorr (the LJ tails of
+                   unshifted centre pairs at and off the centre of mass, the reaction field's self
+                   term of charged and dipolar molecules) of two systems;
 * rigid_2clj_4000_energy: the per-step Upot, virial, sum m v^2 and sum I w^2 of 1000 steps
                    (dt 0.001) of workloads.config_2clj(n_cells=10, temperature=1.5), 4,000
                    molecules, with a checksum of the generated start (the energy drift of the
@@ -30,6 +33,7 @@ Run from the repository root:
     make -C oracle ref && python tests/golden/make_rigid_golden.py
 """
 import os
+import shutil
 import sys
 
 import numpy as np
@@ -84,6 +88,21 @@ def main():
             upot=np.array([x["upot"] for x in sc]), virial=np.array([x["virial"] for x in sc]),
             summv2=np.array([x["summv2"] for x in sc]), sum_iw2=np.array([x["sum_iw2"] for x in sc]))
         print("wrote", f"{s.name}.npz")
+    import json
+    import subprocess
+    import tempfile
+
+    ff = {}
+    for s in far_field_systems():
+        tmp = tempfile.mkdtemp(prefix="mdff_")
+        W.write_inp(s, os.path.join(tmp, "sys.inp"))
+        W.write_cfg(s, os.path.join(tmp, "sys.cfg"), "sys.inp")
+        r = subprocess.run([O.REF_DRIVER, "--farfield", "sys.cfg"], cwd=tmp, check=True, capture_output=True, text=True)
+        ff[s.name] = json.loads(r.stdout.strip().splitlines()[-1])
+        shutil.rmtree(tmp)
+    with open(os.path.join(OUT, "rigid_far_field.json"), "w") as f:
+        json.dump(ff, f, indent=1)
+    print("wrote rigid_far_field.json")
     s = energy_system()
     out = O.run_reference(s, 1000)
     sc = out["scalars"]
@@ -91,6 +110,25 @@ def main():
                         upot=np.array([x["upot"] for x in sc]), virial=np.array([x["virial"] for x in sc]),
                         summv2=np.array([x["summv2"] for x in sc]), sum_iw2=np.array([x["sum_iw2"] for x in sc]))
     print("wrote rigid_2clj_4000_energy.npz")
+
+
+def far_field_systems():
+    """Unshifted and shifted centres, charges and dipoles, off-centre sites (TICS and TISS terms)."""
+    a = W.rigid_fcc_box(4, 0.25, 1.8, 18, 3.0, [W.quadrupolar_two_centre(1.0), W.dipolar_two_centre(0.9),
+                                               W.charged_two_centre(0.6), W.bent_three_centre()],
+                        [0.25] * 4, np.ones((6, 2)) * np.array([0.97, 1.01]), name="ff_polar_mix")
+    a.epsilon_rf = 5.0
+    for comp in a.components[:2]:
+        for t in comp.sites:
+            t.do_shift = False
+    b = W.rigid_fcc_box(4, 0.3, 2.0, 19, 3.5, [W.three_centre_linear(), W.rigid_component(
+        [W.Site(0.0, 0.0, 0.0, 1.0, 1.0, 1.0, False)], charges=[W.Charge(0.0, 0.0, 0.3, 0.0, 0.4),
+                                                             W.Charge(0.0, 0.0, -0.3, 0.0, -0.4)])],
+                        [0.5, 0.5], np.array([[0.9, 1.1]]), name="ff_centre_site")
+    for t in b.components[0].sites:
+        t.do_shift = False
+    b.lj_cutoff = 3.0
+    return [a, b]
 
 
 def energy_system():

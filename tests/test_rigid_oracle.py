@@ -151,3 +151,26 @@ def test_domain_temperature_and_betas_with_rotation():
     single.n, single.summv2 = 100, 310.0
     single.calculateGlobalValues()
     assert single.temperature == 310.0 / 300.0 and single.beta_rot == 1.0
+
+
+def test_far_field_correction_matches_reference():
+    """mdgpu_rigid_far_field_correction (host arithmetic of libmdgpu.so) gives the reference's
+    Domain::initFarFieldCorr terms: the LJ tails of unshifted centre pairs at and off the centre of
+    mass (TICC, TICS, TISS) and the reaction field's self term of charged and dipolar molecules."""
+    import json
+
+    from madpac_b200 import mdgpu as M
+
+    sys.path.insert(0, GOLDEN)
+    from make_rigid_golden import far_field_systems
+
+    want = json.load(open(os.path.join(GOLDEN, "rigid_far_field.json")))
+    for s in far_field_systems():
+        u, w = M.rigid_far_field_correction(s)
+        assert abs(u - want[s.name]["upot_corr"]) <= 1e-12 * abs(want[s.name]["upot_corr"]), s.name
+        assert abs(w - want[s.name]["virial_corr"]) <= 1e-12 * abs(want[s.name]["virial_corr"]), s.name
+    # two sites whose distances from the centre of mass add up to the cutoff: refused
+    s = far_field_systems()[1]
+    s.lj_cutoff = 1.0
+    with pytest.raises(M.MdgpuError):
+        M.rigid_far_field_correction(s)
