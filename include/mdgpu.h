@@ -169,8 +169,8 @@ int mdgpu_device_peaks(int device, double* fp32_tflops, double* fp64_tflops);
 
 /* Forces, local potential energy and virial of one periodic box without any device allocation.
  * No counterpart in the reference: this is for callers that cannot call cudaMalloc while they
- * run (hosts that own all device memory through their own pool, code inside a stream capture,
- * latency-bound loops that must not block on the driver's allocator). Inputs and outputs are the
+ * run (hosts that own all device memory through their own pool, latency-bound loops that must not
+ * block on the driver's allocator). Inputs and outputs are the
  * caller's device buffers: d_r (n, 3) positions and d_cid (n) 0-based component ids in, d_F
  * (n, 3) forces out; upot and virial (host, may be NULL) receive what mdgpu_traverse_pairs
  * returns. All intermediate buffers live in one static device array of about 7.5 MB that every
@@ -178,8 +178,11 @@ int mdgpu_device_peaks(int device, double* fp32_tflops, double* fp64_tflops);
  * (larger inputs return MDGPU_ERR_CAPACITY). Calls share that array and keep its last contents
  * (each call clears what must start at zero); calls that overlap on the GPU race and must be
  * serialised. The first call on a device looks up the array's address with that device current;
- * make it before any stream capture. stream may be NULL (default stream); the call waits for it.
- * errbuf (may be NULL) receives a message of at most errlen bytes. */
+ * make it before any stream capture, and do not use the library across a cudaDeviceReset. stream
+ * may be NULL (default stream); the call is synchronous: it uploads its parameter table from host
+ * memory, waits for the stream and returns upot, virial and the status on the host. The caller's
+ * current device is unchanged on return. lj_cutoff 0 means the cutoff; negative values are
+ * rejected. errbuf (may be NULL) receives a message of at most errlen bytes. */
 int mdgpu_forces_noalloc(int device, void* stream, int64_t n, const double* d_r, const int32_t* d_cid,
                          const double length[3], double cutoff, double lj_cutoff, int ncomp,
                          const mdgpu_component* comps, const double* mix, int precision, double* d_F,
@@ -313,13 +316,16 @@ int mdgpu_rigid_set_polarities(mdgpu_rigid* h, const int32_t* ndipoles, const md
  * of them reach the cutoff together) and the reaction field's self term of each molecule's dipole
  * (its charges' q r plus its dipoles). Host arithmetic only (no context, no device): components as
  * for mdgpu_rigid_create (dipoles as for mdgpu_rigid_set_polarities; NULL for none), counts[c]
- * molecules of component c in the box of edges `length`. upot_corr and virial_corr receive the
- * reference's _UpotCorr and _VirialCorr. */
+ * molecules of component c in the box of edges `length`; lj_cutoff 0 means the cutoff. upot_corr and
+ * virial_corr receive the reference's _UpotCorr and _VirialCorr. Negative counts, a dipole direction
+ * of zero length, an empty box and a too small LJ cutoff return MDGPU_ERR_ARG; errbuf (may be NULL)
+ * receives a message of at most errlen bytes. */
 int mdgpu_rigid_far_field_correction(int ncomp, const int32_t* nsites, const mdgpu_site* sites,
                                      const int32_t* ncharges, const mdgpu_charge* charges,
                                      const int32_t* ndipoles, const mdgpu_oriented* dipoles, const double* mix,
                                      const int64_t* counts, const double length[3], double cutoff,
-                                     double lj_cutoff, double epsilon_rf, double* upot_corr, double* virial_corr);
+                                     double lj_cutoff, double epsilon_rf, double* upot_corr, double* virial_corr,
+                                     char* errbuf, int errlen);
 /* Total mass and principal moments of component comp (Component::m, I11/I22/I33). */
 int mdgpu_rigid_get_inertia(const mdgpu_rigid* h, int32_t comp, double* mass, double I[3]);
 /* Loads the molecules (q and D required); forces and torques start at zero. */

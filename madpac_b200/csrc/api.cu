@@ -2,6 +2,8 @@
 // the step sequence and device-side timing.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include <utility>
 
 #include <cmath>
@@ -368,6 +370,22 @@ PairParams pair_params(const Species& sp, double rc, double rc_lj) {
 	return hp;
 }
 
+int device_max_optin(int device) {
+	static std::mutex mu;
+	static int known[kMaxDevices] = {};
+	const bool cached = device >= 0 && device < kMaxDevices;
+	{
+		std::lock_guard<std::mutex> lock(mu);
+		if (cached && known[device] > 0) return known[device];
+	}
+	int v = 0;
+	if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess || v <= 0)
+		v = 48 * 1024;
+	std::lock_guard<std::mutex> lock(mu);
+	if (cached) known[device] = v;
+	return v;
+}
+
 }  // namespace mdgpu
 
 using namespace mdgpu;
@@ -384,6 +402,7 @@ int mdgpu_create(mdgpu_ctx** out, const double length[3], double cutoff, double 
 	*out = &full->pub;
 	if (ncomp < 1 || ncomp > kMaxSpecies) return fail(c, MDGPU_ERR_ARG, "ncomp must be in 1..8");
 	if (!(cutoff > 0)) return fail(c, MDGPU_ERR_ARG, "cutoff must be positive");
+	if (!(lj_cutoff >= 0)) return fail(c, MDGPU_ERR_ARG, "lj_cutoff must be 0 (= cutoff) or positive");
 	if (cells_in_cutoff != 1.0) return fail(c, MDGPU_ERR_ARG, "only cellsInCutoffRadius = 1 is supported");
 	if (precision != MDGPU_FP64 && precision != MDGPU_MIXED) return fail(c, MDGPU_ERR_ARG, "unknown precision mode");
 	if (ncomp > 1 && !mix) return fail(c, MDGPU_ERR_ARG, "mixing coefficients are required for ncomp > 1");

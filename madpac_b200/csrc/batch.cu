@@ -879,6 +879,7 @@ int mdgpu_batch_create(mdgpu_batch** out, int32_t nboxes, const double* lengths,
 	if (nboxes < 1) return bfail(b, MDGPU_ERR_ARG, "nboxes must be >= 1");
 	if (ncomp < 1 || ncomp > kMaxSpecies) return bfail(b, MDGPU_ERR_ARG, "ncomp must be in 1..8");
 	if (!(cutoff > 0)) return bfail(b, MDGPU_ERR_ARG, "cutoff must be positive");
+	if (!(lj_cutoff >= 0)) return bfail(b, MDGPU_ERR_ARG, "lj_cutoff must be 0 (= cutoff) or positive");
 	if (cells_in_cutoff != 1.0) return bfail(b, MDGPU_ERR_ARG, "only cellsInCutoffRadius = 1 is supported");
 	if (precision != MDGPU_FP64 && precision != MDGPU_MIXED) return bfail(b, MDGPU_ERR_ARG, "unknown precision mode");
 	if (ncomp > 1 && !mix) return bfail(b, MDGPU_ERR_ARG, "mixing coefficients are required for ncomp > 1");

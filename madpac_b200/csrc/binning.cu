@@ -17,6 +17,8 @@
 // asked for a build in this step.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include <algorithm>
 
 #include "grid_sync.cuh"
@@ -367,14 +369,23 @@ cudaError_t launch_bin(Context* c, bool permute_forces) {
 }
 
 cudaError_t launch_rebuild(Context* c, const Grid& g) {
-	static int max_ctas = -1;
-	if (max_ctas < 0) {
-		int per_sm = 0, sms = 0;
+	// co-resident CTAs per SM of k_rebuild, per device (the occupancy query is a host call of
+	// several microseconds, paid once per device)
+	static std::mutex mu;
+	static int per_sm_of[kMaxDevices] = {};
+	int per_sm = 0;
+	{
+		std::lock_guard<std::mutex> lock(mu);
+		if (c->device >= 0 && c->device < kMaxDevices) per_sm = per_sm_of[c->device];
+	}
+	if (per_sm == 0) {
 		cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rebuild, kRebuildThreads, 0);
 		if (e != cudaSuccess) return e;
-		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-		max_ctas = per_sm * sms;
+		if (per_sm < 1) per_sm = 1;
+		std::lock_guard<std::mutex> lock(mu);
+		if (c->device >= 0 && c->device < kMaxDevices) per_sm_of[c->device] = per_sm;
 	}
+	const int max_ctas = per_sm * c->num_sms;
 	prof_begin(c, 0);
 	RebuildArgs a{};
 	a.n = c->n;

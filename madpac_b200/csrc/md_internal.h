@@ -11,6 +11,7 @@
 namespace mdgpu {
 
 constexpr int kMaxSpecies = 8;
+constexpr int kMaxDevices = 64;   // device ordinals whose attributes the library caches
 constexpr int kReduceBlock = 256;   // block size of every kernel that writes reduction partials
 
 // Device status bits (OR-ed by kernels, mapped to MDGPU_ERR_* by the host).
@@ -176,6 +177,9 @@ PairParams pair_params(const Species& sp, double rc, double rc_lj);
 int check_device_status(Context* c);
 int set_error(Context* c, int code, const std::string& msg);
 int set_cuda_error(Context* c, cudaError_t e, const char* where);
+
+// cudaDevAttrMaxSharedMemoryPerBlockOptin of a device, queried once per device (api.cu).
+int device_max_optin(int device);
 
 // Timing brackets around a group of launches (0 = binning, 1 = pairs, 2 = integration).
 void prof_begin(Context* c, int group);

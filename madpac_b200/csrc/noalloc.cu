@@ -2,13 +2,15 @@
 //
 // Who needs it: callers that cannot call cudaMalloc while they run this code. Examples are hosts
 // that own all device memory through their own pool allocator (a foreign cudaMalloc would bypass
-// their accounting or fail once the pool has reserved the device), code running inside a CUDA
-// stream capture where an allocation would break the capture or synchronise the device, and
-// real-time or latency-bound loops that must not block on the driver's allocator. They pass
-// device buffers they already own for the inputs and outputs; every intermediate buffer of the
-// binning and the pair traversal (sorted copies of the molecules, cell counts and offsets,
-// reduction partials, status word, parameter table) comes from one file-scope device array,
-// g_scratch, sized for at most kNoAllocMaxMolecules molecules and kNoAllocMaxCells cells.
+// their accounting or fail once the pool has reserved the device), and latency-bound loops that
+// must not block on the driver's allocator. They pass device buffers they already own for the
+// inputs and outputs; every intermediate buffer of the binning and the pair traversal (sorted
+// copies of the molecules, cell counts and offsets, reduction partials, status word, parameter
+// table) comes from one file-scope device array, g_scratch, sized for at most
+// kNoAllocMaxMolecules molecules and kNoAllocMaxCells cells.
+//
+// The call is synchronous: it uploads its parameter table from host memory, waits for its stream
+// and returns Upot, the virial and the status on the host.
 //
 // Consequences of a static scratch array:
 //  * every GPU that loads the library holds g_scratch (about 7.5 MB) until the process exits;
@@ -17,7 +19,9 @@
 //  * calls that overlap on the GPU (other host threads, or several streams in flight) race on
 //    g_scratch and corrupt each other's results -- serialise them;
 //  * the first call on a device looks up g_scratch's device address (cudaGetSymbolAddress, with
-//    that device current); make that first call before any stream capture begins.
+//    that device current) and keeps it for the rest of the process; make that first call before
+//    any stream capture begins, and do not use the library across a cudaDeviceReset of that
+//    device (the module, and with it g_scratch, is loaded again at another address).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -32,7 +36,6 @@ namespace {
 
 constexpr int64_t kNoAllocMaxMolecules = 32768;
 constexpr int64_t kNoAllocMaxCells = 32768;
-constexpr int kMaxDevices = 64;
 
 constexpr size_t na_align(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -133,6 +136,15 @@ __global__ void k_na_store(int64_t n, Particles p, double* __restrict__ F) {
 	F[3 * u + 2] = p.fz[s];
 }
 
+// Restores the calling thread's current device when the entry point returns.
+struct DeviceGuard {
+	int dev;
+	explicit DeviceGuard(int d) : dev(d) {}
+	~DeviceGuard() {
+		if (dev >= 0) cudaSetDevice(dev);
+	}
+};
+
 int na_fail(char* errbuf, int errlen, int code, const char* msg) {
 	if (errbuf && errlen > 0) snprintf(errbuf, (size_t) errlen, "%s", msg);
 	return code;
@@ -155,6 +167,8 @@ extern "C" int mdgpu_forces_noalloc(int device, void* stream, int64_t n, const d
 	if (ncomp < 1 || ncomp > kMaxSpecies) return na_fail(errbuf, errlen, MDGPU_ERR_ARG, "ncomp must be in 1..8");
 	if (ncomp > 1 && !mix) return na_fail(errbuf, errlen, MDGPU_ERR_ARG, "mixing coefficients required");
 	if (!(cutoff > 0)) return na_fail(errbuf, errlen, MDGPU_ERR_ARG, "cutoff must be positive");
+	if (!(lj_cutoff >= 0))
+		return na_fail(errbuf, errlen, MDGPU_ERR_ARG, "lj_cutoff must be 0 (= cutoff) or positive");
 	if (precision != MDGPU_FP64 && precision != MDGPU_MIXED)
 		return na_fail(errbuf, errlen, MDGPU_ERR_ARG, "unknown precision mode");
 	if (device < 0 || device >= kMaxDevices) return na_fail(errbuf, errlen, MDGPU_ERR_ARG, "device out of range");
@@ -226,7 +240,12 @@ extern "C" int mdgpu_forces_noalloc(int device, void* stream, int64_t n, const d
 		c.sp.shift6[k] = hp.shift6[k];
 	}
 
-	cudaError_t e = cudaSetDevice(device);
+	// the caller's current device is put back on every return below
+	int prev_device = -1;
+	cudaError_t e = cudaGetDevice(&prev_device);
+	if (e != cudaSuccess) return na_fail(errbuf, errlen, MDGPU_ERR_CUDA, cudaGetErrorString(e));
+	DeviceGuard guard(prev_device);
+	e = cudaSetDevice(device);
 	if (e != cudaSuccess) return na_fail(errbuf, errlen, MDGPU_ERR_CUDA, cudaGetErrorString(e));
 	unsigned char* base = nullptr;
 	{

@@ -179,8 +179,7 @@ Plan plan(Context* c, const Grid& g, double filter_radius, int kind) {
 	const bool fp64 = c->precision == MDGPU_FP64;
 	Plan P;
 	brick::init_box(P.bx, g, filter_radius, 0, kind == 0 ? 0.0 : 0.5 * c->skin);
-	static int max_optin = -1;
-	if (max_optin < 0) cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+	const int max_optin = device_max_optin(c->device);
 	size_t budget = 110 * 1024;
 	if (kind == 2 && !fp64) budget = std::min(budget, (size_t) (224 / kListMinBlocks - 2) * 1024);
 	if (budget > (size_t) max_optin) budget = (size_t) max_optin;

@@ -1188,15 +1188,42 @@ int mdgpu_rigid_far_field_correction(int ncomp, const int32_t* nsites, const mdg
                                      const mdgpu_charge* charges, const int32_t* ndipoles,
                                      const mdgpu_oriented* dipoles, const double* mix, const int64_t* counts,
                                      const double length[3], double cutoff, double lj_cutoff, double epsilon_rf,
-                                     double* upot_corr, double* virial_corr) {
-	if (ncomp < 1 || ncomp > kMaxSpecies || !nsites || !sites || !counts || !length) return MDGPU_ERR_ARG;
-	if (!(cutoff > 0.0)) return MDGPU_ERR_ARG;
+                                     double* upot_corr, double* virial_corr, char* errbuf, int errlen) {
+	if (errbuf && errlen > 0) errbuf[0] = '\0';
+	auto fail = [&](int code, const std::string& msg) {
+		if (errbuf && errlen > 0) snprintf(errbuf, (size_t) errlen, "%s", msg.c_str());
+		return code;
+	};
+	if (ncomp < 1 || ncomp > kMaxSpecies) return fail(MDGPU_ERR_ARG, "ncomp must be in 1..8");
+	if (!nsites || !sites || !counts || !length) return fail(MDGPU_ERR_ARG, "null argument");
+	if (!(cutoff > 0.0)) return fail(MDGPU_ERR_ARG, "cutoff must be positive");
+	if (!(lj_cutoff >= 0.0)) return fail(MDGPU_ERR_ARG, "lj_cutoff must be 0 (= cutoff) or positive");
+	for (int d = 0; d < 3; d++)
+		if (!(length[d] > 0.0)) return fail(MDGPU_ERR_ARG, "box lengths must be positive");
+	for (int i = 0; i < ncomp; i++) {
+		if (counts[i] < 0) return fail(MDGPU_ERR_ARG, "molecule counts must not be negative");
+		if (ndipoles && ndipoles[i] < 0) return fail(MDGPU_ERR_ARG, "dipole counts must not be negative");
+	}
+	if (ndipoles && !dipoles) {
+		for (int i = 0; i < ncomp; i++)
+			if (ndipoles[i] > 0) return fail(MDGPU_ERR_ARG, "dipoles are counted but not given");
+	}
+	if (ndipoles && dipoles) {
+		int off = 0;
+		for (int i = 0; i < ncomp; i++)
+			for (int s = 0; s < ndipoles[i]; s++, off++) {
+				const double* e = dipoles[off].e;
+				// the reference divides by |e| (Domain.cpp:596-603): a zero direction has no dipole
+				if (!(e[0] * e[0] + e[1] * e[1] + e[2] * e[2] > 0.0))
+					return fail(MDGPU_ERR_ARG, "a dipole direction has zero length");
+			}
+	}
 	const double rc_lj = lj_cutoff > 0.0 ? lj_cutoff : cutoff;
 	Context c;   // host-only: receives the error text of the table set-up
 	RigidParams P;
 	int st = setup_rigid(&c, ncomp, nsites, sites, ncharges, charges, nullptr, nullptr, nullptr, nullptr, epsilon_rf,
 	                     nullptr, mix, cutoff, rc_lj, P);
-	if (st) return st;
+	if (st) return fail(st, c.err);
 	double upot_lj = 0., virial_lj = 0., self_term = 0.;
 	int64_t nmol = 0;
 	int lo = 0, qo = 0, dof = 0;
@@ -1231,7 +1258,9 @@ int mdgpu_rigid_far_field_correction(int ncomp, const int32_t* nsites, const mdg
 				for (int sj = 0; sj < nsites[j]; ++sj) {
 					const double* rj = sites[lj_off[j] + sj].r;
 					double tau2 = std::sqrt(rj[0] * rj[0] + rj[1] * rj[1] + rj[2] * rj[2]);
-					if (tau1 + tau2 >= rc_lj) return MDGPU_ERR_ARG;   // "rc too small" (Domain.cpp:622-625)
+					if (tau1 + tau2 >= rc_lj)   // "rc too small" (Domain.cpp:622-625)
+						return fail(MDGPU_ERR_ARG, "LJ cutoff too small: two LJ centres' distances from their centres of "
+						                           "mass add up to the cutoff or more");
 					const int k = (P.base[i] + si) * kMaxSiteTotal + P.base[j] + sj;
 					if (P.shift6[k] != 0.0) continue;   // truncated-shifted pairs have no tail correction
 					const double eps24 = P.eps24[k], sig2 = P.sig2[k];
@@ -1251,7 +1280,7 @@ int mdgpu_rigid_far_field_correction(int ncomp, const int32_t* nsites, const mdg
 			}
 		}
 	}
-	if (nmol <= 0) return MDGPU_ERR_ARG;
+	if (nmol <= 0) return fail(MDGPU_ERR_ARG, "the box holds no molecules");
 	const double rho = double(nmol) / (length[0] * length[1] * length[2]);
 	const double fac = M_PI * rho / (3. * double(nmol));
 	upot_lj *= fac;

@@ -91,7 +91,8 @@ SIGNATURES = {
     "mdgpu_rigid_create": (_I, [ctypes.POINTER(_VP), _VP, _D, _D, _D, _I, _VP, _VP, _VP, _VP, _VP, _VP, _I, _I]),
     "mdgpu_rigid_destroy": (_I, [_VP]),
     "mdgpu_rigid_set_polarities": (_I, [_VP, _VP, _VP, _VP, _VP, _D]),
-    "mdgpu_rigid_far_field_correction": (_I, [_I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _D, _D, _D, _VP, _VP]),
+    "mdgpu_rigid_far_field_correction": (_I, [_I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _D, _D, _D, _VP, _VP,
+                                              ctypes.c_char_p, _I]),
     "mdgpu_rigid_last_error": (ctypes.c_char_p, [_VP]),
     "mdgpu_rigid_set_precision": (_I, [_VP, _I]),
     "mdgpu_rigid_get_inertia": (_I, [_VP, _I32, _VP, _VP]),
@@ -169,14 +170,15 @@ def rigid_far_field_correction(system):
     length = _c64(system.length)
     mix = _c64(system.mix).reshape(-1)
     u, w = ctypes.c_double(), ctypes.c_double()
+    err = ctypes.create_string_buffer(256)
     st = lib.mdgpu_rigid_far_field_correction(len(comps), _ptr(nsites), ctypes.cast(sites, ctypes.c_void_p),
                                               _ptr(ncharges), ctypes.cast(charges, ctypes.c_void_p), _ptr(nd),
                                               ctypes.cast(da, ctypes.c_void_p), _ptr(mix) if mix.size else None,
                                               _ptr(counts), _ptr(length), float(system.cutoff),
                                               float(system.lj_cutoff), float(getattr(system, "epsilon_rf", 1.0e10)),
-                                              ctypes.byref(u), ctypes.byref(w))
+                                              ctypes.byref(u), ctypes.byref(w), err, 256)
     if st != 0:
-        raise MdgpuError(st, "far-field correction: cutoff too small for the molecules or bad components")
+        raise MdgpuError(st, "far-field correction: " + err.value.decode())
     return u.value, w.value
 
 
@@ -234,10 +236,10 @@ def forces_noalloc(d_r: int, d_cid: int, d_F: int, n: int, length, cutoff: float
     """Forces, local Upot and virial of one box with no device allocation inside the call.
 
     For callers that cannot allocate device memory while they run (a host owning all memory
-    through its own pool, a stream being captured, a latency-bound loop): d_r, d_cid and d_F are
-    device addresses of buffers the caller owns ((n, 3) float64, (n,) int32, (n, 3) float64).
-    At most 32768 molecules and 32768 cells (the size of the library's static scratch array).
-    Returns (upot, virial).
+    through its own pool, a latency-bound loop): d_r, d_cid and d_F are device addresses of
+    buffers the caller owns ((n, 3) float64, (n,) int32, (n, 3) float64). At most 32768 molecules
+    and 32768 cells (the size of the library's static scratch array). The call is synchronous (it
+    waits for `stream`) and leaves the current device as it found it. Returns (upot, virial).
     """
     lib = load_library()
     comps = (_MdComponent * len(components))()

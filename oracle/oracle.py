@@ -14,6 +14,10 @@ from typing import Dict, Optional
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# Where the reference's MarDyn sources lie (the one place this location is set; the environment
+# variable MADPAC_REFERENCE_MARDYN overrides it). Only the recipe that compiles the reference into
+# oracle/_ref reads it; without the sources, the prebuilt oracle/_ref is used as it is.
+REFERENCE_MARDYN = os.environ.get("MADPAC_REFERENCE_MARDYN", "/root/reference/madpac/mardyn")
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_DRIVER = os.path.join(HERE, "_ref", "ref_driver")
 
@@ -25,7 +29,7 @@ def build() -> None:
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
 
 
-def build_reference(ref_dir: str = "/root/reference/madpac/mardyn") -> bool:
+def build_reference(ref_dir: str = REFERENCE_MARDYN) -> bool:
     """Compile the reference sources into oracle/_ref when the reference tree is present."""
     if not os.path.isdir(ref_dir):
         return False

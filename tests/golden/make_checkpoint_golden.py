@@ -6,7 +6,7 @@ oracle/_ref/ref_driver (the reference sources compiled unmodified, see oracle/Ma
 checkpoint text (ck_<name>.txt) and the state and system parameters (ck_<name>.npz), from which
 tests/test_phase_space.py checks the device-path writer and reader. Run from the repository root:
 
-    make -C oracle ref && python tests/golden/make_checkpoint_golden.py
+    make -C oracle ref REF=<the reference mardyn/ directory> && python tests/golden/make_checkpoint_golden.py
 """
 import os
 import shutil
@@ -37,7 +37,7 @@ def systems():
 
 def main():
     if not os.path.exists(O.REF_DRIVER):
-        raise SystemExit("build the reference harness first: make -C oracle ref")
+        raise SystemExit("build the reference harness first: make -C oracle ref REF=<the reference mardyn/ directory>")
     for s in systems():
         tmp = tempfile.mkdtemp(prefix="mdck_")
         W.write_inp(s, os.path.join(tmp, "sys.inp"))

@@ -5,7 +5,7 @@ target `ref`), which runs Simulation::prepare_start + simulateStep on a seeded .
 dumps every molecule's r, v, F and LinkedCells cell index. The systems are the seeded synthetic
 ones of madpac_b200.workloads. Run from the repository root:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref REF=<the reference mardyn/ directory> && python tests/golden/make_golden.py
 """
 import json
 import os
@@ -49,7 +49,7 @@ def systems():
 
 def main():
     if not os.path.exists(O.REF_DRIVER):
-        raise SystemExit("build the reference harness first: make -C oracle ref")
+        raise SystemExit("build the reference harness first: make -C oracle ref REF=<the reference mardyn/ directory>")
     meta = {}
     for name, (s, nsteps, dumps) in systems().items():
         ref = O.run_reference(s, nsteps, dumps)

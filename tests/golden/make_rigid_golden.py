@@ -30,7 +30,7 @@ rigid_<name>.npz (the start state is stored too, so the fixtures do not depend o
 
 Run from the repository root:
 
-    make -C oracle ref && python tests/golden/make_rigid_golden.py
+    make -C oracle ref REF=<the reference mardyn/ directory> && python tests/golden/make_rigid_golden.py
 """
 import os
 import shutil
@@ -74,7 +74,7 @@ def polar_mix():
 
 def main():
     if not os.path.exists(O.REF_DRIVER):
-        raise SystemExit("build the reference harness first: make -C oracle ref")
+        raise SystemExit("build the reference harness first: make -C oracle ref REF=<the reference mardyn/ directory>")
     for s in systems():
         out = O.run_reference(s, NSTEPS, (0, NSTEPS))
         d0, d1 = out["dumps"][0], out["dumps"][NSTEPS]

@@ -174,3 +174,25 @@ def test_far_field_correction_matches_reference():
     s.lj_cutoff = 1.0
     with pytest.raises(M.MdgpuError):
         M.rigid_far_field_correction(s)
+
+
+def test_far_field_correction_reports_why_it_refuses():
+    """The far-field entry point names the reason of each refusal: a too small LJ cutoff, a
+    negative molecule count, a negative LJ cutoff."""
+    import copy
+
+    from madpac_b200 import mdgpu as M
+
+    sys.path.insert(0, GOLDEN)
+    from make_rigid_golden import far_field_systems
+
+    s = far_field_systems()[1]
+    s.lj_cutoff = 1.0
+    with pytest.raises(M.MdgpuError) as e:
+        M.rigid_far_field_correction(s)
+    assert e.value.code == 1 and "cutoff too small" in str(e.value)
+    s = copy.deepcopy(far_field_systems()[1])
+    s.lj_cutoff = -1.0
+    with pytest.raises(M.MdgpuError) as e:
+        M.rigid_far_field_correction(s)
+    assert e.value.code == 1 and "lj_cutoff" in str(e.value)

@@ -1,6 +1,5 @@
 """mdgpu_forces_noalloc, the entry point for callers that cannot allocate device memory while they
-run (hosts owning all device memory through their own pool, code inside a stream capture,
-latency-bound loops). It must give the forces, Upot and virial of the regular context path
+run (hosts owning all device memory through their own pool, latency-bound loops). It must give the forces, Upot and virial of the regular context path
 (mdgpu_create / mdgpu_update / mdgpu_traverse_pairs) on two calls in a row -- the second call
 reuses the static scratch array the first one left behind -- within the tolerances of the other
 GPU tests. This file is collected last so that a run stopping at the first failure has already
@@ -66,3 +65,25 @@ def test_noalloc_rejects_more_molecules_than_its_scratch_holds():
         M.forces_noalloc(1, 1, 1, 32769, [60.0, 60.0, 60.0], 2.5, [W.Component()])
     assert e.value.code == 10
     assert "32768" in str(e.value)
+
+
+def test_noalloc_rejects_a_negative_lj_cutoff():
+    with pytest.raises(M.MdgpuError) as e:
+        M.forces_noalloc(1, 1, 1, 100, [60.0, 60.0, 60.0], 2.5, [W.Component()], None, -1.0)
+    assert e.value.code == 1
+    assert "lj_cutoff" in str(e.value)
+
+
+def test_noalloc_leaves_the_current_device_as_it_found_it():
+    torch = pytest.importorskip("torch")
+    system = W.lj_fcc_box(6, 0.8, 1.0, 3, 2.5)
+    dev = torch.cuda.device_count() - 1
+    torch.cuda.set_device(dev)
+    d_r = torch.tensor(system.r, dtype=torch.float64, device=f"cuda:{dev}")
+    d_cid = torch.tensor(system.cid, dtype=torch.int32, device=f"cuda:{dev}")
+    d_F = torch.zeros((system.n, 3), dtype=torch.float64, device=f"cuda:{dev}")
+    torch.cuda.synchronize()
+    M.forces_noalloc(d_r.data_ptr(), d_cid.data_ptr(), d_F.data_ptr(), system.n, system.length, system.cutoff,
+                     system.components, system.mix, system.lj_cutoff, M.FP64, device=dev)
+    assert torch.cuda.current_device() == dev
+    torch.cuda.set_device(0)
