@@ -287,9 +287,26 @@ int orc_status(const orc_sys* s) { return s->status; }
 
 /* ---------------------------------------------------------------- container */
 
-/* LinkedCells::addParticle, LinkedCells.cpp:182-204 */
+/* Whether floor((r - haloMin) / cellLength) names a cell of the halo-inclusive grid. A position
+ * inside the halo box can fail this: an image placed by exchangeMolecules within an ulp of the
+ * halo box's upper face (a molecule exactly on a cell face, r + L rounding up to haloMax) gives
+ * an index one past the last cell. */
+static int cell_in_range(const orc_sys* s, const double r[3]) {
+	for (int d = 0; d < 3; d++) {
+		const int ci = (int) floor((r[d] - s->haloMin[d]) / s->cellLength[d]);
+		if (ci < 0 || ci >= s->cpd[d]) return 0;
+	}
+	return 1;
+}
+
+/* LinkedCells::addParticle, LinkedCells.cpp:182-204.
+ * One departure from the reference: where its cell index runs one past the cell array (see
+ * cell_in_range) the reference writes beyond the array (undefined behaviour: the compiled reference
+ * crashes); here that image is not added. It lies a cell length (>= cutoff) beyond every molecule of
+ * the box, so it has no partner within the cutoff and the forces, Upot and virial are unchanged. */
 static void add_particle(orc_sys* s, const orc_mol* m) {
 	if (!in_halo_box(s, m->r)) return;
+	if (!cell_in_range(s, m->r)) return;
 	long idx = pool_new(s);
 	s->pool[idx] = *m;
 	list_push_front(s, idx);

@@ -252,3 +252,30 @@ def run_reference(system, nsteps: int, dump_steps=(), workdir: Optional[str] = N
             rec["sum_iw2"] = float(line.split()[1])
     dumps = {s: read_ref_dump(os.path.join(tmp, f"step{s:06d}.bin")) for s in dump_steps}
     return dict(scalars=scal, dumps=dumps, workdir=tmp)
+
+
+def _run_oracle_job(args):
+    system, nsteps, dump_steps = args
+    return run_oracle(system, nsteps, dump_steps)
+
+
+def run_oracle_many(systems, nsteps: int, dump_steps=(), processes: Optional[int] = None):
+    """run_oracle on many independent boxes, spread over the host cores by a pool of freshly
+    spawned processes (spawn, not fork: the caller may hold a CUDA context). Results in the order
+    of `systems`."""
+    import multiprocessing as mp
+
+    if processes is None:
+        processes = max(1, min(len(systems), os.cpu_count() or 1, 32))
+    jobs = [(s, nsteps, tuple(dump_steps)) for s in systems]
+    if processes == 1:
+        return [_run_oracle_job(j) for j in jobs]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(processes) as pool:
+        # largest boxes first, so that the pool ends together
+        order = sorted(range(len(jobs)), key=lambda k: -systems[k].n)
+        out = pool.map(_run_oracle_job, [jobs[k] for k in order], chunksize=1)
+    res = [None] * len(jobs)
+    for k, r in zip(order, out):
+        res[k] = r
+    return res

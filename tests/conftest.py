@@ -13,6 +13,23 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
     config.addinivalue_line("markers", "slow: long-running check")
+    config.addinivalue_line("markers", "fullsize: parity at a workload's stated size (1M, 4.2M molecules, 512 boxes)")
+
+
+_FULLSIZE = []
+
+
+def pytest_runtest_logreport(report):
+    if report.when == "call" and "fullsize" in report.keywords:
+        _FULLSIZE.append((report.nodeid.split("::")[-1], report.outcome, report.duration))
+
+
+def pytest_terminal_summary(terminalreporter, exitstatus, config):
+    """Names the full-size parity tests and their outcome at the end of a quiet run."""
+    if _FULLSIZE:
+        terminalreporter.write_line("full-size parity against the oracle:")
+        for name, outcome, dur in _FULLSIZE:
+            terminalreporter.write_line(f"  {outcome:7s} {name} ({dur:.0f} s)")
 
 
 def _build_oracle():

@@ -131,3 +131,39 @@ def test_geometry_and_params():
 def test_golden_metadata_consistent():
     meta = json.load(open(os.path.join(GOLDEN, "ref_systems.json")))
     assert set(meta) == set(GOLDEN_NAMES)
+
+
+def test_image_on_the_halo_face_is_dropped_without_changing_the_forces():
+    """Box 285 of the 512-box ensemble (1,117 molecules, L = 11.30, 4 cells per dimension) has FCC
+    sites exactly on a cell face; exchangeMolecules then places an image within an ulp of the halo
+    box's upper face, whose cell index runs past the reference's cell array (the compiled reference
+    crashes there). The oracle leaves that image out; it has no partner within the cutoff, so the
+    forces, Upot and virial equal a direct minimum-image sum over all pairs."""
+    s = W.config_c4()[285]
+    o = O.Oracle(s)
+    o.init()
+    o.prepare_start()
+    st, sc = o.state(), o.scalars()
+    L, rc2 = s.length, s.cutoff ** 2
+    r = s.r[np.argsort(s.ids)]
+    n = len(r)
+    eps24, sig2, shift6 = o.params(0, 0)
+    F = np.zeros((n, 3))
+    U6 = W6 = 0.0
+    for i in range(n):
+        d = r[i] - r[i + 1:]
+        d -= L * np.round(d / L)
+        dd = np.sum(d * d, axis=1)
+        m = dd < rc2
+        inv = 1.0 / dd[m]
+        s6 = (sig2 * inv) ** 3
+        fac = eps24 * (s6 * s6 + (s6 * s6 - s6)) * inv
+        f = fac[:, None] * d[m]
+        F[i] += f.sum(axis=0)
+        F[i + 1:][m] -= f
+        U6 += np.sum(eps24 * (s6 * s6 - s6) + shift6)
+        W6 += np.sum(fac * dd[m])
+    rms = np.sqrt(np.mean(np.sum(F * F, axis=1)))
+    assert np.max(np.linalg.norm(st["F"] - F, axis=1)) / rms <= 1e-12
+    assert abs(sc["upot_exact"] - U6 / 6.0) <= 1e-12 * abs(U6 / 6.0)
+    assert abs(sc["virial_exact"] - W6) <= 1e-12 * abs(W6)
