@@ -4,7 +4,7 @@
 accumulation on one B200 (one independent box per GPU when run on several).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision mixed|fp64]
-  python bench.py --workload c3|batched|checkpoint|rigid [--charges]
+  python bench.py --workload c3|batched|checkpoint|rigid|adjoint [--charges]
 
 One step = Leapfrog kick+drift, periodic wrap + linked-cell binning, the pair traversal (forces,
 Upot, virial) and the closing kick with sum m v^2, i.e. Simulation::simulateStep's hot path. The
@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--skin", type=float, default=0.3,
                     help="Verlet skin of the step (0: cells and candidates rebuilt every step, as the reference)")
-    ap.add_argument("--workload", choices=["c2", "c3", "batched", "checkpoint", "rigid"], default="c2",
+    ap.add_argument("--workload", choices=["c2", "c3", "batched", "checkpoint", "rigid", "adjoint"], default="c2",
                     help="c2: the 1M-molecule box (headline); c3: the 4M-molecule two-species slab; "
                          "batched: the 512-box ensemble; checkpoint: phase-space file write and read of the "
                          "1M-molecule box through the C ABI; rigid: a fluid of 1M two-centre LJ molecules")
@@ -60,6 +60,8 @@ def parse():
                     help="rigid workload: two-centre molecules with point charges +-0.5 (charge pairs besides LJ)")
     ap.add_argument("--loop-steps", type=int, default=20,
                     help="steps of the loop-over-single-box comparison of the batched workload")
+    ap.add_argument("--adjoint-precision", choices=["fp64", "mixed"], default="fp64",
+                    help="adjoint workload: arithmetic of the forward steps and the adjoint kernel")
     ap.add_argument("--liquid-steps", type=int, default=1500,
                     help="untimed steps before the liquid sub-record of the headline box (0: none)")
     return ap.parse_args()
@@ -914,6 +916,103 @@ class _Solo:
         self.rank = int(os.environ.get("RANK", "0"))
 
 
+ADJ_METRIC = "LJ trajectory gradients/s, 16,384-molecule two-species box, 50 Leapfrog steps, 1 B200"
+FLOPS_PER_ADJ_PAIR = 60  # FP64 flops per ordered pair of the adjoint kernel (FMA = 2)
+
+
+def run_adjoint(args, dist: Dist):
+    """Gradient of L = sum |F - F_t|^2 + 0.1 (U - U_t)^2 after 50 NVE steps (checkpoints every 10)
+    with respect to the start positions, velocities and eps_ab / sigma_ab, on the 16,384-molecule
+    two-species box (targets at eps_AB x 1.1, sigma_AB x 0.95), forward and backward on the device."""
+    import torch
+
+    from madpac_b200 import mdgpu as M
+    from madpac_b200 import workloads as W
+    from madpac_b200.trajectory import TrajectoryAdjoint
+
+    torch.cuda.set_device(dist.local)
+    precision = M.MIXED if args.adjoint_precision == "mixed" else M.FP64
+    s = W.config_c5(seed=5 + dist.rank)
+    lc = M.LinkedCells.from_system(s, M.FP64, device=dist.local)
+    lc.update()
+    lc.traversePairs()
+    lc.run(100, s.dt, record=False)
+    st = lc.getParticles()
+    lc.close()
+    s.r, s.v = st["r"], st["v"]
+    # targets: the same molecules with the cross-species pair at eps x 1.1, sigma x 0.95
+    t = W.System(**{**s.__dict__})
+    t.mix = np.array(s.mix, dtype=np.float64).reshape(-1, 2) * np.array([[1.1, 0.95]])
+    tl = M.LinkedCells.from_system(t, M.FP64, device=dist.local)
+    tl.update()
+    Ut, _, _ = tl.traversePairs()
+    Ft = tl.getParticles()["F"]
+    tl.close()
+    steps, every = 50, 10
+    tr = TrajectoryAdjoint(s, steps, every, device=dist.local, precision=precision)
+    stream = torch.cuda.ExternalStream(tr.lc.stream())
+
+    def one():
+        r, v, F, U = tr.forward(s.r, s.v)
+        return tr.backward(2 * (F - Ft), 0.2 * (U - Ut))
+
+    for _ in range(max(args.warmup, 1)):
+        one()
+    reps = max(1, min(args.steps, 10))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    clocks = ClockSampler(dist.local)
+    clocks.start()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        gr, gv, ge, gs = one()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    sec = dist.max(e0.elapsed_time(e1) * 1e-3)
+    # adjoint kernel alone: CUDA events around its launches in one more (profiled) backward pass
+    tr.lc.profileEnable(True)
+    one()
+    tr.lc.profileEnable(False)
+    adj_ms, adj_launches = tr.lc.trajAdjointTime()
+    tr.lc.setState(r=s.r)
+    tr.lc.update()
+    _, _, upairs = tr.lc.traversePairs()
+    fp32_peak, fp64_peak = M.device_peaks(dist.local)
+    peak = fp32_peak if precision == M.MIXED else fp64_peak
+    flops_launch = 2.0 * upairs * FLOPS_PER_ADJ_PAIR
+    achieved = flops_launch / (adj_ms / max(adj_launches, 1) * 1e-3) / 1e12
+    tr.close()
+    # launches per gradient: forward 50 steps x 4 + backward (5 segments x 10 recomputed steps x 5 +
+    # 50 adjoint steps x ~5)
+    out = {
+        "metric": ADJ_METRIC, "value": dist.sum(reps / sec), "unit": "trajectory gradients/s", "n_gpus": dist.world,
+        "steps": reps, "warmup": max(args.warmup, 1), "ms_per_step": sec / reps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if precision == M.FP64 else "f32 pair terms, f64 sums",
+        "data": "synthetic (seeded FCC lattice thermalised 100 steps, Maxwell-Boltzmann velocities)",
+        "config": {"workload": "two-species LJ box, N=16,384, rho 0.8, T 1.0, A/B 50/50 (sigma_B 0.9, eps_B 0.8), "
+                               "rc 2.5, dt 0.002; L = sum|F - F_t|^2 + 0.1 (U - U_t)^2 after 50 NVE steps, targets "
+                               "at eps_AB x 1.1, sigma_AB x 0.95; gradients in r0, v0, eps_ab, sigma_ab",
+                   "checkpoint_every": every, "trajectory_steps": steps,
+                   "l2": "not flushed (one gradient = 50 forward + 50 recomputed + 50 backward steps)"},
+        "ms_per_gradient": sec / reps * 1e3, "md_steps_per_gradient": 3 * steps,
+        "roofline": {"bound": "fp64" if precision == M.FP64 else "fp32", "kernel": "adjoint (vector-Jacobian product)",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                     "peak_source": "measured FMA microbenchmark (mdgpu_device_peaks)",
+                     "flops_per_ordered_pair": FLOPS_PER_ADJ_PAIR, "launch_ms": adj_ms / max(adj_launches, 1),
+                     "launches": adj_launches},
+        "gradient_norms": {"dL_dr0_rms": float(np.sqrt(np.mean(gr ** 2))), "dL_deps_AB": float(ge[0, 1]),
+                           "dL_dsigma_AB": float(gs[0, 1])},
+        "gpu_launches": None, "clocks": clk,
+        "e2e": {"value": dist.sum(reps / sec), "unit": "trajectory gradients/s",
+                "h2d_bytes_per_step": 2 * 48 * s.n, "d2h_bytes_per_step": 4 * 24 * s.n,
+                "note": "each gradient uploads r0, v0 and gF and downloads the final state and dL/dr0, dL/dv0"},
+    }
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -928,6 +1027,8 @@ def main():
         out = run_checkpoint(args, dist)
     elif args.workload == "rigid":
         out = run_rigid(args, dist)
+    elif args.workload == "adjoint":
+        out = run_adjoint(args, dist)
     else:
         out = run_ours(args, dist)
     if dist.rank == 0:

@@ -153,6 +153,24 @@ int mdgpu_read_steps(mdgpu_ctx* ctx, int32_t nsteps, double* per_step);
  * Double precision. */
 int mdgpu_adjoint(mdgpu_ctx* ctx, const double* gF, double gU, double* dL_dr, double* dL_deps, double* dL_dsigma);
 
+/* Reverse-mode gradient through an NVE Leapfrog trajectory on the device (no counterpart in the
+ * reference). mdgpu_traj_forward runs nsteps steps of Simulation::simulateStep with the per-step
+ * binning (skin 0; Leapfrog vcorr = 1) from the loaded state, keeping (r, v) every
+ * checkpoint_every steps in device memory, and leaves the final state in the context (upot_final:
+ * its local Upot). mdgpu_traj_backward takes the cotangents gF ((n, 3), caller order) and gU of
+ * the final forces and Upot and returns dL/dr_0 and dL/dv_0 ((n, 3), caller order; dL_dv0 may be
+ * NULL) and the ncomp x ncomp gradients with respect to eps_ab and sigma_ab (as mdgpu_adjoint
+ * reports them; either may be NULL), recomputing each segment from its snapshot on the device
+ * (recomputed_steps, may be NULL, receives how many steps that took); afterwards the context holds
+ * the start state again. Arithmetic in the context's precision (the mixed form: FP32 pair terms,
+ * FP64 sums). */
+int mdgpu_traj_forward(mdgpu_ctx* ctx, int32_t nsteps, int32_t checkpoint_every, double dt, double* upot_final);
+int mdgpu_traj_backward(mdgpu_ctx* ctx, const double* gF, double gU, double* dL_dr0, double* dL_dv0,
+                        double* dL_deps, double* dL_dsigma, int64_t* recomputed_steps);
+/* Device time (CUDA events on the context's stream) of the adjoint-kernel launches of the last
+ * mdgpu_traj_backward that ran with mdgpu_profile_enable on, and how many there were. */
+int mdgpu_traj_adjoint_time(mdgpu_ctx* ctx, double* ms, int64_t* launches);
+
 /* Device-side timing of the kernels this context launches, for benchmarking: when enabled, CUDA
  * events on the context's stream bracket the binning, pair and integration kernels. times_ms[0..2]
  * = total binning, pair, integration milliseconds since the last reset; counts[0..3] = launches of

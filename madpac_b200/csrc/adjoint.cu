@@ -15,7 +15,12 @@
 //   dU_pair/deps24 = (s12 - s6 + c6)/6,  dU_pair/dsig2 = eps24 (6 s12 - 3 s6 + c6')/(6 sig2)
 // with c6 = sr6 - sr6^2, c6' = 3 sr6 - 6 sr6^2 (sr6 = (sig2/rcLJ^2)^3) for truncated-shifted pair
 // types (shift6 != 0) and 0 otherwise. Every molecule gathers over its 27 neighbour cells (each
-// pair is seen from both sides, so parameter terms carry a factor 1/2). FP64 throughout.
+// pair is seen from both sides, so parameter terms carry a factor 1/2; kAdjLanes lanes share a
+// molecule's candidates and sum their parts by a fixed butterfly). FP64 throughout, or (the
+// mixed form, MDGPU_MIXED) the pair's derivative terms in FP32 from the FP64 difference vector,
+// with the cutoff decided in FP64 and every sum kept in FP64. The parameter terms are summed per
+// block in a fixed order (per-warp partials, then warp by warp), so the results do not depend on
+// scheduling.
 #include <cuda_runtime.h>
 
 #include "md_internal.h"
@@ -26,6 +31,7 @@ namespace {
 
 constexpr int KK = kMaxSpecies * kMaxSpecies;
 
+template <bool kMixed>
 __global__ void __launch_bounds__(kReduceBlock) k_adjoint(int64_t n, Particles p, const int32_t* __restrict__ start,
                                                          Grid g, const PairParams* __restrict__ pp, double rclj,
                                                          const double* __restrict__ gfx, const double* __restrict__ gfy,
@@ -33,20 +39,21 @@ __global__ void __launch_bounds__(kReduceBlock) k_adjoint(int64_t n, Particles p
                                                          double* __restrict__ ox, double* __restrict__ oy,
                                                          double* __restrict__ oz, double* __restrict__ pgrad) {
 	__shared__ double s_e24[KK], s_s2[KK], s_sh[KK];
-	__shared__ double s_acc[2 * KK];
+	__shared__ double s_acc[kReduceBlock / 32][2 * KK];   // per-warp partials of the parameter terms
 	const int ns = pp->ns;
 	for (int k = threadIdx.x; k < KK; k += blockDim.x) {
 		s_e24[k] = k < ns * ns ? pp->eps24[k] : 0.0;
 		s_s2[k] = k < ns * ns ? pp->sig2[k] : 0.0;
 		s_sh[k] = k < ns * ns ? pp->shift6[k] : 0.0;
-		s_acc[k] = 0.0;
-		s_acc[KK + k] = 0.0;
 	}
 	__syncthreads();
 	const double rc2 = pp->rc2, rclj2 = pp->rclj2, rclj6 = rclj2 * rclj2 * rclj2;
-	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	// kAdjLanes consecutive lanes per molecule, each taking every kAdjLanes-th candidate of a cell
+	const int64_t i = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) / kAdjLanes;
+	const int sub = threadIdx.x % kAdjLanes;
 	double acc_e[KK], acc_s[KK];
 	for (int k = 0; k < ns * ns; k++) acc_e[k] = acc_s[k] = 0.0;
+	double ax = 0.0, ay = 0.0, az = 0.0;
 	if (i < n) {
 		const double xi = p.rx[i], yi = p.ry[i], zi = p.rz[i];
 		const double wix = gfx[i], wiy = gfy[i], wiz = gfz[i];
@@ -57,7 +64,6 @@ __global__ void __launch_bounds__(kReduceBlock) k_adjoint(int64_t n, Particles p
 			int c = (int) floor(__ddiv_rn(__dsub_rn(r[d], g.halo_min[d]), g.cell_length[d])) - 1;
 			cc[d] = c < 0 ? 0 : (c >= g.nc[d] ? g.nc[d] - 1 : c);
 		}
-		double ax = 0.0, ay = 0.0, az = 0.0;
 		for (int dz = -1; dz <= 1; dz++) {
 			int z = cc[2] + dz;
 			double sz = 0.0;
@@ -90,69 +96,112 @@ __global__ void __launch_bounds__(kReduceBlock) k_adjoint(int64_t n, Particles p
 					}
 					const int nb = (z * g.nc[1] + y) * g.nc[0] + x;
 					const bool shifted = (sx != 0.0) || (sy != 0.0) || (sz != 0.0);
-					for (int j = start[nb]; j < start[nb + 1]; j++) {
+					for (int j = start[nb] + sub; j < start[nb + 1]; j += kAdjLanes) {
 						if (j == i && !shifted) continue;
 						const double d0 = xi - (p.rx[j] + sx), d1 = yi - (p.ry[j] + sy), d2 = zi - (p.rz[j] + sz);
 						const double q = d0 * d0 + d1 * d1 + d2 * d2;
 						if (!(q < rc2) || !(q < rclj2)) continue;
 						const int pk = ti * ns + p.cid[j];
 						const double e24 = s_e24[pk], sg2 = s_s2[pk];
-						const double iq = 1.0 / q;
-						double s6 = sg2 * iq;
-						s6 = s6 * s6 * s6;
-						const double s12 = s6 * s6;
-						const double fac = e24 * (2.0 * s12 - s6) * iq;
-						const double dfac = e24 * (4.0 * s6 - 14.0 * s12) * iq * iq;
 						const double w0 = wix - gfx[j], w1 = wiy - gfy[j], w2 = wiz - gfz[j];
-						const double dw = d0 * w0 + d1 * w1 + d2 * w2;
-						// J w - gU f
-						ax += fac * w0 + 2.0 * dfac * dw * d0 - gU * fac * d0;
-						ay += fac * w1 + 2.0 * dfac * dw * d1 - gU * fac * d1;
-						az += fac * w2 + 2.0 * dfac * dw * d2 - gU * fac * d2;
-						// parameter terms (half: the pair is seen from both sides)
 						const bool shf = s_sh[pk] != 0.0;
-						double sr6 = sg2 * sg2 * sg2 / rclj6;
+						const double sr6 = sg2 * sg2 * sg2 / rclj6;
 						const double c6 = shf ? sr6 - sr6 * sr6 : 0.0;
 						const double c6s = shf ? 3.0 * sr6 - 6.0 * sr6 * sr6 : 0.0;
-						acc_e[pk] += 0.5 * (fac * dw / e24 + gU * (s12 - s6 + c6) / 6.0);
-						acc_s[pk] += 0.5 * (e24 * (12.0 * s12 - 3.0 * s6) * iq / sg2 * dw +
-						                    gU * e24 * (6.0 * s12 - 3.0 * s6 + c6s) / (6.0 * sg2));
+						if (kMixed) {
+							// FP32 from the FP64 difference vector; FP64 sums
+							const float f0 = (float) d0, f1 = (float) d1, f2 = (float) d2;
+							const float qf = fmaf(f0, f0, fmaf(f1, f1, f2 * f2));
+							const float e24f = (float) e24, sg2f = (float) sg2;
+							const float iq = 1.0f / qf;
+							float s6 = sg2f * iq;
+							s6 = s6 * s6 * s6;
+							const float s12 = s6 * s6;
+							const float fac = e24f * (2.0f * s12 - s6) * iq;
+							const float dfac = e24f * (4.0f * s6 - 14.0f * s12) * iq * iq;
+							const float v0 = (float) w0, v1 = (float) w1, v2 = (float) w2;
+							const float dw = fmaf(f0, v0, fmaf(f1, v1, f2 * v2));
+							const float gUf = (float) gU;
+							const float t = 2.0f * dfac * dw;
+							ax += (double) (fac * v0 + t * f0 - gUf * fac * f0);
+							ay += (double) (fac * v1 + t * f1 - gUf * fac * f1);
+							az += (double) (fac * v2 + t * f2 - gUf * fac * f2);
+							acc_e[pk] += 0.5 * ((double) (fac * dw / e24f) + gU * ((double) (s12 - s6) + c6) / 6.0);
+							acc_s[pk] += 0.5 * ((double) (e24f * (12.0f * s12 - 3.0f * s6) * iq / sg2f * dw) +
+							                    gU * e24 * ((double) (6.0f * s12 - 3.0f * s6) + c6s) / (6.0 * sg2));
+						} else {
+							const double iq = 1.0 / q;
+							double s6 = sg2 * iq;
+							s6 = s6 * s6 * s6;
+							const double s12 = s6 * s6;
+							const double fac = e24 * (2.0 * s12 - s6) * iq;
+							const double dfac = e24 * (4.0 * s6 - 14.0 * s12) * iq * iq;
+							const double dw = d0 * w0 + d1 * w1 + d2 * w2;
+							// J w - gU f
+							ax += fac * w0 + 2.0 * dfac * dw * d0 - gU * fac * d0;
+							ay += fac * w1 + 2.0 * dfac * dw * d1 - gU * fac * d1;
+							az += fac * w2 + 2.0 * dfac * dw * d2 - gU * fac * d2;
+							// parameter terms (half: the pair is seen from both sides)
+							acc_e[pk] += 0.5 * (fac * dw / e24 + gU * (s12 - s6 + c6) / 6.0);
+							acc_s[pk] += 0.5 * (e24 * (12.0 * s12 - 3.0 * s6) * iq / sg2 * dw +
+							                    gU * e24 * (6.0 * s12 - 3.0 * s6 + c6s) / (6.0 * sg2));
+						}
 					}
 				}
 			}
 		}
+	}
+	// the molecule's lanes' sums in a fixed order
+	for (int o = 1; o < kAdjLanes; o <<= 1) {
+		ax += __shfl_xor_sync(0xffffffffu, ax, o);
+		ay += __shfl_xor_sync(0xffffffffu, ay, o);
+		az += __shfl_xor_sync(0xffffffffu, az, o);
+	}
+	if (i < n && sub == 0) {
 		ox[i] = ax;
 		oy[i] = ay;
 		oz[i] = az;
 	}
-	// block sum of the per-type parameter terms, then one partial row per block
-	for (int k = 0; k < ns * ns; k++) {
-		const double ve = warp_sum(acc_e[k]), vs = warp_sum(acc_s[k]);
+	// block sum of the per-type parameter terms in a fixed order (warp sums, then warp by warp),
+	// then one partial row per block
+	const int warp = threadIdx.x >> 5;
+	for (int k = 0; k < KK; k++) {
+		const double ve = k < ns * ns ? warp_sum(acc_e[k]) : 0.0, vs = k < ns * ns ? warp_sum(acc_s[k]) : 0.0;
 		if ((threadIdx.x & 31) == 0) {
-			atomicAdd(&s_acc[k], ve);
-			atomicAdd(&s_acc[KK + k], vs);
+			s_acc[warp][k] = ve;
+			s_acc[warp][KK + k] = vs;
 		}
 	}
 	__syncthreads();
-	for (int k = threadIdx.x; k < 2 * KK; k += blockDim.x) pgrad[(int64_t) blockIdx.x * 2 * KK + k] = s_acc[k];
+	for (int k = threadIdx.x; k < 2 * KK; k += blockDim.x) {
+		double v = 0.0;
+		for (int w = 0; w < kReduceBlock / 32; w++) v += s_acc[w][k];
+		pgrad[(int64_t) blockIdx.x * 2 * KK + k] = v;
+	}
 }
 
-__global__ void k_adjoint_params(int64_t nblocks, const double* __restrict__ pgrad, double* __restrict__ out) {
+// Sum of the blocks' rows in block order, into out (added to it with `accumulate`).
+__global__ void k_adjoint_params(int64_t nblocks, const double* __restrict__ pgrad, double* __restrict__ out,
+                                 bool accumulate) {
 	const int k = threadIdx.x;
 	if (k >= 2 * KK) return;
 	double s = 0.0;
 	for (int64_t b = 0; b < nblocks; b++) s += pgrad[b * 2 * KK + k];
-	out[k] = s;
+	out[k] = accumulate ? out[k] + s : s;
 }
 
 }  // namespace
 
 cudaError_t launch_adjoint(Context* c, const double* gfx, const double* gfy, const double* gfz, double gU, double* ox,
-                           double* oy, double* oz, double* pgrad, double* pout) {
-	const int64_t nb = (c->n + kReduceBlock - 1) / kReduceBlock;
-	k_adjoint<<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(c->n, c->p, c->cell_start, c->g, c->d_pp, c->rc_lj, gfx,
-	                                                          gfy, gfz, gU, ox, oy, oz, pgrad);
-	k_adjoint_params<<<1, 2 * KK, 0, c->stream>>>(nb, pgrad, pout);
+                           double* oy, double* oz, double* pgrad, double* pout, bool accumulate) {
+	const int64_t nb = adjoint_blocks(c->n);
+	if (c->precision == MDGPU_MIXED)
+		k_adjoint<true><<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(c->n, c->p, c->cell_start, c->g, c->d_pp,
+		                                                                c->rc_lj, gfx, gfy, gfz, gU, ox, oy, oz, pgrad);
+	else
+		k_adjoint<false><<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(c->n, c->p, c->cell_start, c->g, c->d_pp,
+		                                                                 c->rc_lj, gfx, gfy, gfz, gU, ox, oy, oz, pgrad);
+	k_adjoint_params<<<1, 2 * KK, 0, c->stream>>>(nb, pgrad, pout, accumulate);
 	count_launches(c, 2);
 	return cudaGetLastError();
 }

@@ -118,6 +118,9 @@ int check_status(Context* c) {
 	if (st & kStatusTimeout) {
 		// the cooperative rebuild's barrier words may be left mid-count: start them again
 		if (c->bar) MD_CUDA(cudaMemsetAsync(c->bar, 0, sizeof(unsigned) * 4, c->stream));
+		// ... and its counts and look-back words, which it clears only when it runs to the end
+		if (c->rb_count) MD_CUDA(cudaMemsetAsync(c->rb_count, 0, sizeof(int32_t) * c->g.ncells, c->stream));
+		if (c->rb_look) MD_CUDA(cudaMemsetAsync(c->rb_look, 0, sizeof(unsigned long long) * c->rb_look_cap, c->stream));
 		c->lists_valid = false;
 		return fail(c, MDGPU_ERR_TIMEOUT, "a bounded device wait gave up");
 	}
@@ -469,6 +472,7 @@ int mdgpu_destroy(mdgpu_ctx* ctx) {
 	cudaFree(c->status);
 	cudaFree(c->d_pp);
 	cudaFree(c->adj);
+	free_traj(c);
 	cudaFree(c->nbr);
 	cudaFree(c->nbr_count);
 	cudaFree(c->r_ref);
@@ -478,7 +482,8 @@ int mdgpu_destroy(mdgpu_ctx* ctx) {
 	cudaFree(c->brick_counts);
 	cudaFree(c->brick_list);
 	if (c->h_sparse) cudaFreeHost(c->h_sparse);
-	cudaFree(c->chunk);
+	cudaFree(c->rb_count);
+	cudaFree(c->rb_look);
 	cudaFree(c->tickets);
 	cudaFree(c->brick_kind);
 	cudaFree(full->x.stage.ptr);
@@ -830,8 +835,11 @@ int skin_prepare(Context* c) {
 		MD_CUDA(cudaMemsetAsync(c->builds, 0, sizeof(unsigned long long), c->stream));
 		MD_CUDA(cudaMalloc(&c->bar, sizeof(unsigned) * 4));
 		MD_CUDA(cudaMemsetAsync(c->bar, 0, sizeof(unsigned) * 4, c->stream));
-		c->chunk_cap = 8192;
-		MD_CUDA(cudaMalloc(&c->chunk, sizeof(int32_t) * c->chunk_cap));
+		c->rb_look_cap = 8192;
+		MD_CUDA(cudaMalloc(&c->rb_look, sizeof(unsigned long long) * c->rb_look_cap));
+		MD_CUDA(cudaMemsetAsync(c->rb_look, 0, sizeof(unsigned long long) * c->rb_look_cap, c->stream));
+		MD_CUDA(cudaMalloc(&c->rb_count, sizeof(int32_t) * c->g.ncells));
+		MD_CUDA(cudaMemsetAsync(c->rb_count, 0, sizeof(int32_t) * c->g.ncells, c->stream));
 		MD_CUDA(cudaMalloc(&c->brick_counts, sizeof(unsigned) * 4));
 		MD_CUDA(cudaMemsetAsync(c->brick_counts, 0, sizeof(unsigned) * 4, c->stream));
 		MD_CUDA(cudaMallocHost(&c->h_sparse, sizeof(int)));
@@ -1021,7 +1029,7 @@ int mdgpu_adjoint(mdgpu_ctx* ctx, const double* gF, double gU, double* dL_dr, do
 	MD_CUDA(cudaSetDevice(c->device));
 	constexpr int KK = kMaxSpecies * kMaxSpecies;
 	const int64_t n = c->n;
-	const int64_t nb = (n + kReduceBlock - 1) / kReduceBlock;
+	const int64_t nb = adjoint_blocks(n);
 	const int64_t need = 6 * n + nb * 2 * KK + 2 * KK;
 	if (need > c->adj_cap) {
 		cudaFree(c->adj);

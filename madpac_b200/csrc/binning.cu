@@ -248,7 +248,8 @@ struct RebuildArgs {
 	int64_t n;
 	Grid g;
 	Particles p, q;
-	int32_t *cell, *rank, *perm, *count, *start, *chunk;
+	int32_t *cell, *rank, *perm, *count, *start;
+	unsigned long long* look;   // per CTA: the scan's published value (flag in bits 62-63)
 	int* status;
 	const int* flag;
 	int step;
@@ -258,9 +259,31 @@ struct RebuildArgs {
 };
 
 constexpr int kRebuildThreads = 256;
+constexpr unsigned long long kLookAggregate = 1ull << 62;   // the CTA's own cell sum
+constexpr unsigned long long kLookPrefix = 2ull << 62;      // the sum of every cell up to its chunk's end
+constexpr unsigned long long kLookValue = (1ull << 62) - 1ull;
 
+__device__ __forceinline__ unsigned long long load_acquire64(const unsigned long long* p) {
+	unsigned long long v;
+	asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+	return v;
+}
+
+// Wrap, binning, scan and (cell, id) sort of all molecules in one cooperative launch with four
+// bounded grid barriers; returns at once unless a build was asked for this step. count[] and look[]
+// are zero on entry and are left zero for the next launch (a launch that gave up on a wait leaves
+// them to the host, which clears them with the timeout status).
+//   1. wrap + cell + arrival rank (atomic count per cell)
+//   2. exclusive scan of the counts in one pass: CTA b sums the cells of its chunk, publishes the
+//      sum, adds up its predecessors' published values back to the first complete prefix
+//      (decoupled look-back: every CTA of the cooperative grid is resident, so each of these waits
+//      ends; each is bounded nonetheless) and publishes its own prefix
+//   3. scatter of the arrival order; counts and look-back words cleared for the next launch
+//   4. per-cell sort by id and gather into the other buffer
+//   5. the sorted arrays back into the current buffer (the host's buffer roles stay fixed)
 __global__ void __launch_bounds__(kRebuildThreads) k_rebuild(RebuildArgs a) {
 	__shared__ int s_flag;
+	__shared__ int32_t s_excl;
 	if (threadIdx.x == 0) s_flag = (*a.flag == a.step && !(*((volatile int*) a.status) & kStatusTimeout)) ? 0 : 1;
 	__syncthreads();
 	if (s_flag) return;   // no build requested for this step
@@ -268,8 +291,6 @@ __global__ void __launch_bounds__(kRebuildThreads) k_rebuild(RebuildArgs a) {
 	const int64_t nthreads = (int64_t) gridDim.x * blockDim.x;
 	const int64_t tid = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	const int64_t nc = a.g.ncells;
-	for (int64_t c = tid; c < nc; c += nthreads) a.count[c] = 0;
-	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
 	bool bad = false;
 	for (int64_t i = tid; i < a.n; i += nthreads) {
 		const int32_t c = bin_one(i, a.p.rx, a.p.ry, a.p.rz, a.g, bad);
@@ -278,32 +299,45 @@ __global__ void __launch_bounds__(kRebuildThreads) k_rebuild(RebuildArgs a) {
 	}
 	if (bad) atomicOr(a.status, kStatusOutsideHalo);
 	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
-	// scan: one contiguous chunk of cells per CTA, the chunk sums by CTA 0, then each chunk again
+	// 2. one contiguous chunk of cells per CTA, scanned with the prefix of the chunks before it
 	const int64_t per = (nc + gridDim.x - 1) / gridDim.x;
 	const int64_t c0 = min((int64_t) blockIdx.x * per, nc), c1 = min(c0 + per, nc);
 	{
 		int32_t local = 0;
 		for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) local += a.count[c];
-		int32_t tot;
-		block_excl_scan(local, &tot);
-		if (threadIdx.x == 0) a.chunk[blockIdx.x] = tot;
-	}
-	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
-	if (blockIdx.x == 0) {
-		int32_t carry = 0;
-		for (int64_t b0 = 0; b0 < gridDim.x; b0 += blockDim.x) {
-			const int64_t b = b0 + threadIdx.x;
-			const int32_t v = b < gridDim.x ? a.chunk[b] : 0;
-			int32_t tot;
-			const int32_t excl = block_excl_scan(v, &tot);
-			if (b < gridDim.x) a.chunk[b] = carry + excl;
-			carry += tot;
+		int32_t agg;
+		block_excl_scan(local, &agg);
+		if (threadIdx.x == 0) {
+			unsigned long long* look = a.look;
+			const unsigned b = blockIdx.x;
+			__threadfence();
+			atomicExch(look + b, (b == 0 ? kLookPrefix : kLookAggregate) | (unsigned long long) agg);
+			int64_t excl = 0;
+			const uint64_t t0 = global_ns();
+			for (int j = (int) b - 1; j >= 0 && !s_flag;) {
+				const unsigned long long v = load_acquire64(look + j);
+				if (v == 0ull) {
+					// predecessor j has not published yet
+					if ((int64_t) (global_ns() - t0) > a.timeout_ns) {
+						atomicOr(a.status, kStatusTimeout);
+						s_flag = 1;
+					}
+					continue;
+				}
+				excl += (int64_t) (v & kLookValue);
+				if (v & kLookPrefix) break;
+				j--;
+			}
+			if (b > 0 && !s_flag) {
+				__threadfence();
+				atomicExch(look + b, kLookPrefix | (unsigned long long) (excl + agg));
+			}
+			s_excl = (int32_t) excl;
+			if (b == gridDim.x - 1) a.start[nc] = (int32_t) (excl + agg);
 		}
-		if (threadIdx.x == 0) a.start[nc] = carry;
-	}
-	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
-	{
-		int32_t carry = a.chunk[blockIdx.x];
+		__syncthreads();
+		if (s_flag) return;
+		int32_t carry = s_excl;
 		for (int64_t base = c0; base < c1; base += blockDim.x) {
 			const int64_t c = base + threadIdx.x;
 			const int32_t v = c < c1 ? a.count[c] : 0;
@@ -314,12 +348,14 @@ __global__ void __launch_bounds__(kRebuildThreads) k_rebuild(RebuildArgs a) {
 		}
 	}
 	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
+	// 3. arrival-order scatter; the counts and the look-back words are not read again in this launch
 	for (int64_t i = tid; i < a.n; i += nthreads) a.perm[a.start[a.cell[i]] + a.rank[i]] = (int32_t) i;
+	for (int64_t c = tid; c < nc; c += nthreads) a.count[c] = 0;
+	if (threadIdx.x == 0) a.look[blockIdx.x] = 0ull;
 	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
 	const int lane = threadIdx.x & 31;
 	for (int64_t c = tid >> 5; c < nc; c += nthreads >> 5) sort_cell(c, lane, a.start, a.perm, a.p, a.q, a.rank, false);
 	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
-	// the sorted arrays back into the current buffer (the host's buffer roles stay fixed)
 	for (int64_t i = tid; i < a.n; i += nthreads) {
 		a.p.rx[i] = a.q.rx[i];
 		a.p.ry[i] = a.q.ry[i];
@@ -395,9 +431,9 @@ cudaError_t launch_rebuild(Context* c, const Grid& g) {
 	a.cell = c->cell;
 	a.rank = c->rank;
 	a.perm = c->perm;
-	a.count = c->cell_count;
+	a.count = c->rb_count;
 	a.start = c->cell_start;
-	a.chunk = c->chunk;
+	a.look = c->rb_look;
 	a.status = c->status;
 	a.flag = c->rebuild;
 	a.step = c->step_id;
@@ -408,7 +444,7 @@ cudaError_t launch_rebuild(Context* c, const Grid& g) {
 	// the whole device would keep every other stream's kernels waiting, also in steps it is gated off)
 	const int64_t work = std::max<int64_t>(c->n, g.ncells);
 	int grid = (int) std::min<int64_t>(max_ctas, (work + kRebuildThreads - 1) / kRebuildThreads);
-	if (grid > c->chunk_cap) grid = c->chunk_cap;
+	if (grid > c->rb_look_cap) grid = c->rb_look_cap;
 	if (grid < 1) grid = 1;
 	cudaLaunchConfig_t cfg{};
 	cfg.gridDim = dim3((unsigned) grid);

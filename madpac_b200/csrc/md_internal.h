@@ -112,8 +112,11 @@ struct Context {
 	unsigned char* brick_kind = nullptr;   // per skin-grid brick: 1 = sparse
 	int step_id = 0;                // id of the step being enqueued (skin mode)
 	unsigned* bar = nullptr;        // grid-barrier words of the cooperative rebuild
-	int32_t* chunk = nullptr;       // per-CTA scan sums of the cooperative rebuild
-	int chunk_cap = 0;
+	// the cooperative rebuild's cell counts (g.ncells, kept zero between launches) and its per-CTA
+	// look-back words (rb_look_cap, kept zero between launches)
+	int32_t* rb_count = nullptr;
+	unsigned long long* rb_look = nullptr;
+	int rb_look_cap = 0;
 	unsigned long long* builds = nullptr;   // builds so far (device counter)
 	// device: bricks of the last build, sparse [0] and dense [1], and the work queues of the sparse [3]
 	// and dense [2] list kernels; brick_list: the dense bricks' indices, then (from nbricks on) the
@@ -123,6 +126,7 @@ struct Context {
 	int* h_sparse = nullptr;                // pinned host copy, read back at the end of each run
 	bool lists_valid = false;       // the sort order has not changed since the lists were built
 	double* adj = nullptr;          // adjoint buffers: cotangents, outputs, parameter partials
+	struct Traj* traj = nullptr;    // device buffers of the trajectory adjoint (traj.cu)
 	int64_t adj_cap = 0;
 	double* h_scalars = nullptr;    // pinned host mirror
 	int* h_status = nullptr;
@@ -159,8 +163,15 @@ cudaError_t launch_leapfrog_post(Context* c, double dt_half, double* record = nu
 cudaError_t launch_leapfrog_post_pre(Context* c, double dt, bool skin_check, double* record);
 cudaError_t launch_scale(Context* c, double beta);
 cudaError_t launch_reduce(Context* c, int64_t nblocks, double* out, int nval);
+// Lanes of the adjoint kernel per molecule, and its blocks (of kReduceBlock threads) for n
+// molecules: the rows of parameter partials it writes.
+constexpr int kAdjLanes = 8;
+inline int64_t adjoint_blocks(int64_t n) { return (n * kAdjLanes + kReduceBlock - 1) / kReduceBlock; }
+// With `accumulate` the parameter sums are added to pout (otherwise they overwrite it).
 cudaError_t launch_adjoint(Context* c, const double* gfx, const double* gfy, const double* gfz, double gU, double* ox,
-                           double* oy, double* oz, double* pgrad, double* pout);
+                           double* oy, double* oz, double* pgrad, double* pout, bool accumulate = false);
+// Frees the device buffers of the context's trajectory adjoint (traj.cu).
+void free_traj(Context* c);
 cudaError_t launch_step_record(Context* c, double* dst);        // dst[0..3] <- step scalars
 
 // Set-up shared by the single-box and the batched contexts (api.cu): LinkedCells geometry of the

