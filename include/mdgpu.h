@@ -171,6 +171,53 @@ int mdgpu_traj_backward(mdgpu_ctx* ctx, const double* gF, double gU, double* dL_
  * mdgpu_traj_backward that ran with mdgpu_profile_enable on, and how many there were. */
 int mdgpu_traj_adjoint_time(mdgpu_ctx* ctx, double* ms, int64_t* launches);
 
+/* ---- molecule-side operations of MaDPaC's coupled step --------------------------------------
+ * MarDynSimulation::simulateStep (coupling/MarDynSimulation.cpp:61-160) interleaves the MD step with
+ * the lattice-Boltzmann connector's operations on molecules; these are the molecule-side ones on the
+ * device container (per-step binning, skin 0), the connector's parameters given as arguments.
+ *
+ * mdgpu_reflect_boundary replaces ReflectingBoundary::applyBoundary (coupling/boundary/
+ * ReflectingBoundary.cpp:47-130); call it after mdgpu_leapfrog_pre and before mdgpu_update. Each
+ * molecule outside the box in a dimension i < dim (2 or 3) has v_i negated and is moved back inside
+ * with the reference's arithmetic (r + (-r - 2r) at the lower face, r - 2 (r - L) at the upper one),
+ * except beyond the upper face of stream_out_dir when the stream-out is on (always without a moving
+ * wall, as the reference sets it): those are counted in *streamed_out (may be NULL) and left as they
+ * are (the connector deletes them; the device container's next mdgpu_update would wrap them). */
+int mdgpu_reflect_boundary(mdgpu_ctx* ctx, int32_t dim, int32_t stream_out_dir, int32_t moving_wall, int32_t stream_out,
+                           int64_t* streamed_out);
+/* The wall force of ForceBoundary::applyBoundary (coupling/boundary/ForceBoundary.cpp:52-226) added to
+ * the forces of the molecules within `border` of a face (X, Y, and Z when dim is 3; [0, border) and
+ * [L - border, L), the box in the other dimensions): ForceBoundary::calcFm's piecewise fit
+ * (ForceBoundary.h:56-82) of the distance to the face, outward at the upper faces and scaled by
+ * stream_damping at the upper face of stream_out_dir. Call it after mdgpu_traverse_pairs. (In the
+ * reference the region lists are filled in copies -- FBoundary::getLower/getUpper take them by
+ * value -- so its applyBoundary changes no force; this is the force its code computes.) */
+int mdgpu_force_boundary(mdgpu_ctx* ctx, int32_t dim, double border, int32_t stream_out_dir, double stream_damping);
+
+/* The coupling-cell grid of the connector's DataContainer (madpac/core/DataContainer.cpp:209-261):
+ * molecules at lower <= r <= upper (first dim dimensions) belong to cell
+ * ((ix * size[1] + iy) * size[2] + iz), ix = (int) ((x - lower[0]) / cell_size); size[2] = 1 in 2D. */
+typedef struct mdgpu_coupling_cells {
+	double lower[3];
+	double upper[3];
+	double cell_size;
+	int32_t size[3];
+	int32_t dim;
+} mdgpu_coupling_cells;
+
+typedef struct mdgpu_thermostat mdgpu_thermostat;
+/* CellWiseThermostat (coupling/thermostat/CellWiseThermostat.cpp:46-156) on the device container:
+ * mdgpu_thermostat_apply(th, iteration) after mdgpu_leapfrog_post does applyThermostat(iteration):
+ * each call adds every molecule's velocity to its coupling cell's sums; when iteration is a multiple
+ * of `interval` it forms the cells' mean velocities in the directed dimensions, their peculiar
+ * kinetic energies E and rescales v = (v - vc)(1 + gamma (beta - 1)) + vc with
+ * beta = sqrt(1.5 samples / interval * T / E), then clears the sums. The global-energy diagnostics
+ * of updateGlobalE do not act on molecules and are not computed. Sums are 64-bit fixed point. */
+int mdgpu_thermostat_create(mdgpu_thermostat** out, mdgpu_ctx* ctx, const mdgpu_coupling_cells* cells,
+                            double target_temperature, double gamma, int32_t interval, const int32_t directed[3]);
+int mdgpu_thermostat_apply(mdgpu_thermostat* th, int64_t iteration);
+int mdgpu_thermostat_destroy(mdgpu_thermostat* th);
+
 /* Device-side timing of the kernels this context launches, for benchmarking: when enabled, CUDA
  * events on the context's stream bracket the binning, pair and integration kernels. times_ms[0..2]
  * = total binning, pair, integration milliseconds since the last reset; counts[0..3] = launches of

@@ -10,7 +10,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmdgpu.so")
 SOURCES = ["api.cu", "binning.cu", "pairs.cu", "pairs_brick.cu", "integrate.cu", "peaks.cu", "noalloc.cu", "adjoint.cu",
-           "traj.cu",
+           "traj.cu", "coupling.cu",
            "batch.cu", "phase_space.cu", "rigid.cu"]
 HEADERS = ["md_internal.h", "reduce.cuh", "pair_common.cuh", "brick.cuh"]
 

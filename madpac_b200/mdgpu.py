@@ -67,6 +67,11 @@ SIGNATURES = {
     "mdgpu_traj_forward": (_I, [_VP, _I32, _I32, _D, _VP]),
     "mdgpu_traj_backward": (_I, [_VP, _VP, _D, _VP, _VP, _VP, _VP, _VP]),
     "mdgpu_traj_adjoint_time": (_I, [_VP, _VP, _VP]),
+    "mdgpu_reflect_boundary": (_I, [_VP, _I32, _I32, _I32, _I32, _VP]),
+    "mdgpu_force_boundary": (_I, [_VP, _I32, _D, _I32, _D]),
+    "mdgpu_thermostat_create": (_I, [ctypes.POINTER(_VP), _VP, _VP, _D, _D, _I32, _VP]),
+    "mdgpu_thermostat_apply": (_I, [_VP, _I64]),
+    "mdgpu_thermostat_destroy": (_I, [_VP]),
     "mdgpu_profile_enable": (_I, [_VP, _I]),
     "mdgpu_profile_read": (_I, [_VP, _VP, _VP, _I]),
     "mdgpu_get_stream": (_I, [_VP, _VP]),
@@ -735,6 +740,20 @@ class LinkedCells:
                                                  _ptr(gv), _ptr(ge), _ptr(gs), ctypes.byref(rec)))
         return gr, gv, ge, gs, rec.value
 
+    # -- molecule-side operations of MaDPaC's coupled step ---------------------------------------
+    def reflectBoundary(self, dim: int, streamOutDir: int, movingWall: bool = False, streamOut: bool = False) -> int:
+        """ReflectingBoundary::applyBoundary on the device (after leapfrogPre, before update);
+        returns the molecules left beyond the stream-out face."""
+        out = ctypes.c_int64()
+        self._check(self.lib.mdgpu_reflect_boundary(self.h, int(dim), int(streamOutDir), 1 if movingWall else 0,
+                                                    1 if streamOut else 0, ctypes.byref(out)))
+        return out.value
+
+    def forceBoundary(self, dim: int, border: float, streamOutDir: int, streamDamping: float = 1.0) -> None:
+        """The wall force ForceBoundary computes for the boundary regions (after traversePairs)."""
+        self._check(self.lib.mdgpu_force_boundary(self.h, int(dim), float(border), int(streamOutDir),
+                                                  float(streamDamping)))
+
     def trajAdjointTime(self):
         """(ms, launches) of the adjoint kernel in the last trajBackward run with profiling on."""
         ms, k = ctypes.c_double(), ctypes.c_int64()
@@ -775,6 +794,48 @@ class LinkedCells:
 
     def synchronize(self) -> None:
         self._check(self.lib.mdgpu_synchronize(self.h))
+
+
+class _MdCouplingCells(ctypes.Structure):
+    _fields_ = [("lower", ctypes.c_double * 3), ("upper", ctypes.c_double * 3), ("cell_size", ctypes.c_double),
+                ("size", ctypes.c_int32 * 3), ("dim", ctypes.c_int32)]
+
+
+class CellWiseThermostat:
+    """CellWiseThermostat (coupling/thermostat/CellWiseThermostat.cpp:46-156) on the molecules of a
+    LinkedCells, over the coupling-cell grid lower..upper of cells of edge cellSize (size cells per
+    dimension; size[2] = 1 when dim is 2). applyThermostat(iteration) samples the velocities every
+    call and rescales them towards targetTemperature every `interval` iterations. Destroy it (close)
+    before its container."""
+
+    def __init__(self, container: LinkedCells, lower, upper, cellSize: float, size, dim: int,
+                 targetTemperature: float, gamma: float, interval: int, directed=(0, 0, 0)):
+        self.lib = container.lib
+        self.container = container
+        g = _MdCouplingCells()
+        for d in range(3):
+            g.lower[d], g.upper[d], g.size[d] = float(lower[d]), float(upper[d]), int(size[d])
+        g.cell_size, g.dim = float(cellSize), int(dim)
+        dirs = (ctypes.c_int32 * 3)(*[int(x) for x in directed])
+        h = ctypes.c_void_p()
+        container._check(self.lib.mdgpu_thermostat_create(ctypes.byref(h), container.h, ctypes.byref(g),
+                                                          float(targetTemperature), float(gamma), int(interval),
+                                                          ctypes.cast(dirs, ctypes.c_void_p)))
+        self.h = h.value
+
+    def applyThermostat(self, iteration: int) -> None:
+        self.container._check(self.lib.mdgpu_thermostat_apply(self.h, int(iteration)))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.mdgpu_thermostat_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 MIN_BETA = 0.9  # Domain.h:33

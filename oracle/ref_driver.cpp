@@ -39,7 +39,10 @@
 #undef private
 
 #include "Simulation.h"
+#include "coupling/boundary/ForceBoundary.h"
+#include "coupling/boundary/ReflectingBoundary.h"
 #include "molecules/Molecule.h"
+#include "parallel/DomainDecompBase.h"
 #include "particleContainer/ParticleContainer.h"
 #include "utils/Logger.h"
 
@@ -184,6 +187,46 @@ public:
 		return now_s() - t0;
 	}
 
+	// The molecule-side boundaries of MaDPaC's coupled step (coupling/MarDynSimulation.cpp:61-160)
+	// on the configuration as read (molecules placed outside the box stand for those that left it
+	// in the drift): the container is binned, ReflectingBoundary::applyBoundary runs (step 1 dump:
+	// r, v after it), the pair forces follow with the decomposition's halo copies (step 2 dump), then
+	// ForceBoundary::applyBoundary (step 3 dump); calcfm.txt samples ForceBoundary::calcFm.
+	void boundary(int dim, int stream_out_dir, int stream_out, const std::string& outdir, const std::string& moves) {
+		using madpac::mardyncoupling::boundary::ForceBoundary;
+		using madpac::mardyncoupling::boundary::ReflectingBoundary;
+		// new positions "id x y z" (outside the box) for some molecules: the reader itself drops
+		// molecules outside the box, so they are moved after reading
+		FILE* mf = fopen(moves.c_str(), "r");
+		unsigned long mid;
+		double mx, my, mz;
+		while (mf && fscanf(mf, "%lu %lf %lf %lf", &mid, &mx, &my, &mz) == 4)
+			for (Molecule* m = _moleculeContainer->begin(); m != _moleculeContainer->end(); m = _moleculeContainer->next())
+				if (m->id() == mid) {
+					m->setr(0, mx);
+					m->setr(1, my);
+					m->setr(2, mz);
+				}
+		if (mf) fclose(mf);
+		_moleculeContainer->update();
+		ReflectingBoundary rb(_moleculeContainer, _domain, stream_out_dir, false, dim, stream_out != 0);
+		rb.applyBoundary();
+		writeArrays(outdir, 1);
+		_domainDecomposition->balanceAndExchange(true, _moleculeContainer, _domain->getComponents(), _domain);
+		_moleculeContainer->traversePairs();
+		_moleculeContainer->deleteOuterParticles();
+		writeArrays(outdir, 2);
+		ForceBoundary fb(_moleculeContainer, _domain, _moleculeContainer->getCutoff(), stream_out_dir, dim);
+		fb.applyBoundary();
+		writeArrays(outdir, 3);
+		FILE* f = fopen((outdir + "/calcfm.txt").c_str(), "w");
+		for (int k = 0; k <= 400; k++) {
+			const double r = 0.0075 * k;
+			fprintf(f, "%.17g %.17g\n", r, ForceBoundary::calcFm(r));
+		}
+		fclose(f);
+	}
+
 	double timeSteps(unsigned long nsteps) {
 		prepare_start();
 		simulateStart();
@@ -215,6 +258,12 @@ int main(int argc, char** argv) {
 		sim.readConfigFile(argv[2]);
 		printf("{\"upot_corr\": %.17g, \"virial_corr\": %.17g}\n", sim.domain()->_UpotCorr,
 		       sim.domain()->_VirialCorr);
+		return 0;
+	}
+	if (argc >= 8 && std::string(argv[1]) == "--boundary") {
+		RefDriver sim;
+		sim.readConfigFile(argv[2]);
+		sim.boundary(atoi(argv[3]), atoi(argv[4]), atoi(argv[5]), argv[6], argv[7]);
 		return 0;
 	}
 	if (argc >= 4 && std::string(argv[1]) == "--time-checkpoint") {
