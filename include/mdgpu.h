@@ -212,7 +212,9 @@ typedef struct mdgpu_thermostat mdgpu_thermostat;
  * of `interval` it forms the cells' mean velocities in the directed dimensions, their peculiar
  * kinetic energies E and rescales v = (v - vc)(1 + gamma (beta - 1)) + vc with
  * beta = sqrt(1.5 samples / interval * T / E), then clears the sums. The global-energy diagnostics
- * of updateGlobalE do not act on molecules and are not computed. Sums are 64-bit fixed point. */
+ * of updateGlobalE do not act on molecules and are not computed. The per-cell sums are 64-bit fixed
+ * point in steps of 2^-40 (independent of the order of the additions); a cell whose velocity or
+ * kinetic-energy sum reaches 2^23 makes the call fail with MDGPU_ERR_CAPACITY. */
 int mdgpu_thermostat_create(mdgpu_thermostat** out, mdgpu_ctx* ctx, const mdgpu_coupling_cells* cells,
                             double target_temperature, double gamma, int32_t interval, const int32_t directed[3]);
 int mdgpu_thermostat_apply(mdgpu_thermostat* th, int64_t iteration);

@@ -125,6 +125,8 @@ int check_status(Context* c) {
 		return fail(c, MDGPU_ERR_TIMEOUT, "a bounded device wait gave up");
 	}
 	if (st & kStatusCapacity) return fail(c, MDGPU_ERR_CAPACITY, "a device buffer is too small for the workload");
+	if (st & kStatusRange)
+		return fail(c, MDGPU_ERR_CAPACITY, "a per-cell fixed-point sum left its range (|sum| >= 2^23)");
 	return fail(c, MDGPU_ERR_CUDA, "unknown device status");
 }
 
@@ -484,6 +486,8 @@ int mdgpu_destroy(mdgpu_ctx* ctx) {
 	if (c->h_sparse) cudaFreeHost(c->h_sparse);
 	cudaFree(c->rb_count);
 	cudaFree(c->rb_look);
+	cudaFree(c->rb_key);
+	cudaFree(c->rb_scell);
 	cudaFree(c->tickets);
 	cudaFree(c->brick_kind);
 	cudaFree(full->x.stage.ptr);
@@ -810,6 +814,16 @@ int skin_prepare(Context* c) {
 		c->list_n = n;
 		c->list_cap = cap;
 		c->lists_valid = false;
+	}
+	if (c->rb_cap < n) {
+		cudaFree(c->rb_key);
+		cudaFree(c->rb_scell);
+		c->rb_key = nullptr;
+		c->rb_scell = nullptr;
+		c->rb_cap = 0;
+		MD_CUDA(cudaMalloc(&c->rb_key, sizeof(uint64_t) * n));
+		MD_CUDA(cudaMalloc(&c->rb_scell, sizeof(int32_t) * n));
+		c->rb_cap = n;
 	}
 	const int64_t parts = skin_partials_needed(c);
 	if (c->brick_kind == nullptr || c->list_n != n || c->lists_valid == false) {

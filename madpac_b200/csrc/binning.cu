@@ -249,6 +249,8 @@ struct RebuildArgs {
 	Grid g;
 	Particles p, q;
 	int32_t *cell, *rank, *perm, *count, *start;
+	uint64_t* key;              // ids in scatter order
+	int32_t* scell;             // cells in scatter order
 	unsigned long long* look;   // per CTA: the scan's published value (flag in bits 62-63)
 	int* status;
 	const int* flag;
@@ -273,13 +275,16 @@ __device__ __forceinline__ unsigned long long load_acquire64(const unsigned long
 // bounded grid barriers; returns at once unless a build was asked for this step. count[] and look[]
 // are zero on entry and are left zero for the next launch (a launch that gave up on a wait leaves
 // them to the host, which clears them with the timeout status).
-//   1. wrap + cell + arrival rank (atomic count per cell)
+//   1. wrap + cell + arrival rank: one atomic per cell and warp (the warp's molecules of a cell,
+//      found by __match_any_sync, take consecutive ranks)
 //   2. exclusive scan of the counts in one pass: CTA b sums the cells of its chunk, publishes the
-//      sum, adds up its predecessors' published values back to the first complete prefix
-//      (decoupled look-back: every CTA of the cooperative grid is resident, so each of these waits
-//      ends; each is bounded nonetheless) and publishes its own prefix
-//   3. scatter of the arrival order; counts and look-back words cleared for the next launch
-//   4. per-cell sort by id and gather into the other buffer
+//      sum, adds up its predecessors' published values back to the first complete prefix, 32 at a
+//      time by one warp (decoupled look-back: every CTA of the cooperative grid is resident, so each
+//      of these waits ends; each is bounded nonetheless) and publishes its own prefix
+//   3. scatter of the arrival order with each slot's id and cell; counts and look-back words
+//      cleared for the next launch
+//   4. one thread per slot: its rank by (id, previous slot) among its cell's slots, read from the
+//      contiguous ids of the cell, and the gather into the other buffer
 //   5. the sorted arrays back into the current buffer (the host's buffer roles stay fixed)
 __global__ void __launch_bounds__(kRebuildThreads) k_rebuild(RebuildArgs a) {
 	__shared__ int s_flag;
@@ -291,11 +296,22 @@ __global__ void __launch_bounds__(kRebuildThreads) k_rebuild(RebuildArgs a) {
 	const int64_t nthreads = (int64_t) gridDim.x * blockDim.x;
 	const int64_t tid = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	const int64_t nc = a.g.ncells;
+	const int lane = threadIdx.x & 31;
 	bool bad = false;
-	for (int64_t i = tid; i < a.n; i += nthreads) {
-		const int32_t c = bin_one(i, a.p.rx, a.p.ry, a.p.rz, a.g, bad);
-		a.cell[i] = c;
-		a.rank[i] = atomicAdd(&a.count[c], 1);
+	// warp-uniform trip count (nthreads is a multiple of 32): every lane takes part in the match
+	for (int64_t i0 = tid - lane; i0 < a.n; i0 += nthreads) {
+		const int64_t i = i0 + lane;
+		const bool valid = i < a.n;
+		const int32_t c = valid ? bin_one(i, a.p.rx, a.p.ry, a.p.rz, a.g, bad) : -1;
+		const unsigned peers = __match_any_sync(0xffffffffu, c);
+		const int leader = __ffs(peers) - 1;
+		int32_t base = 0;
+		if (valid && lane == leader) base = atomicAdd(&a.count[c], __popc(peers));
+		base = __shfl_sync(0xffffffffu, base, leader);
+		if (valid) {
+			a.cell[i] = c;
+			a.rank[i] = base + __popc(peers & ((1u << lane) - 1u));
+		}
 	}
 	if (bad) atomicOr(a.status, kStatusOutsideHalo);
 	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
@@ -307,33 +323,45 @@ __global__ void __launch_bounds__(kRebuildThreads) k_rebuild(RebuildArgs a) {
 		for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) local += a.count[c];
 		int32_t agg;
 		block_excl_scan(local, &agg);
-		if (threadIdx.x == 0) {
+		if (threadIdx.x < 32) {
 			unsigned long long* look = a.look;
-			const unsigned b = blockIdx.x;
-			__threadfence();
-			atomicExch(look + b, (b == 0 ? kLookPrefix : kLookAggregate) | (unsigned long long) agg);
+			const int b = (int) blockIdx.x;
+			if (lane == 0) {
+				__threadfence();
+				atomicExch(look + b, (b == 0 ? kLookPrefix : kLookAggregate) | (unsigned long long) agg);
+			}
+			// predecessors b-1-lane, 32 per round; those before CTA 0 count as a zero prefix
 			int64_t excl = 0;
-			const uint64_t t0 = global_ns();
-			for (int j = (int) b - 1; j >= 0 && !s_flag;) {
-				const unsigned long long v = load_acquire64(look + j);
-				if (v == 0ull) {
-					// predecessor j has not published yet
-					if ((int64_t) (global_ns() - t0) > a.timeout_ns) {
-						atomicOr(a.status, kStatusTimeout);
-						s_flag = 1;
-					}
+			bool late = false;
+			const uint64_t t0 = __shfl_sync(0xffffffffu, global_ns(), 0);
+			for (int j = b - 1; j >= 0;) {
+				const int idx = j - lane;
+				const unsigned long long v = idx >= 0 ? load_acquire64(look + idx) : kLookPrefix;
+				if (__any_sync(0xffffffffu, v == 0ull)) {
+					// a predecessor of the window has not published yet
+					late = __shfl_sync(0xffffffffu, (int64_t) (global_ns() - t0) > a.timeout_ns, 0);
+					if (late) break;
 					continue;
 				}
-				excl += (int64_t) (v & kLookValue);
-				if (v & kLookPrefix) break;
-				j--;
+				const unsigned pm = __ballot_sync(0xffffffffu, (v & kLookPrefix) != 0ull);
+				const int first = pm ? __ffs(pm) - 1 : 32;   // the nearest complete prefix
+				unsigned long long val = (lane <= first && idx >= 0) ? (v & kLookValue) : 0ull;
+				for (int o = 16; o; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+				excl += (int64_t) val;
+				if (pm) break;
+				j -= 32;
 			}
-			if (b > 0 && !s_flag) {
-				__threadfence();
-				atomicExch(look + b, kLookPrefix | (unsigned long long) (excl + agg));
+			if (lane == 0) {
+				if (late) {
+					atomicOr(a.status, kStatusTimeout);
+					s_flag = 1;
+				} else if (b > 0) {
+					__threadfence();
+					atomicExch(look + b, kLookPrefix | (unsigned long long) (excl + agg));
+				}
+				s_excl = (int32_t) excl;
+				if (b == (int) gridDim.x - 1) a.start[nc] = (int32_t) (excl + agg);
 			}
-			s_excl = (int32_t) excl;
-			if (b == gridDim.x - 1) a.start[nc] = (int32_t) (excl + agg);
 		}
 		__syncthreads();
 		if (s_flag) return;
@@ -349,12 +377,29 @@ __global__ void __launch_bounds__(kRebuildThreads) k_rebuild(RebuildArgs a) {
 	}
 	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
 	// 3. arrival-order scatter; the counts and the look-back words are not read again in this launch
-	for (int64_t i = tid; i < a.n; i += nthreads) a.perm[a.start[a.cell[i]] + a.rank[i]] = (int32_t) i;
+	for (int64_t i = tid; i < a.n; i += nthreads) {
+		const int32_t c = a.cell[i];
+		const int32_t slot = a.start[c] + a.rank[i];
+		a.perm[slot] = (int32_t) i;
+		a.key[slot] = a.p.id[i];
+		a.scell[slot] = c;
+	}
 	for (int64_t c = tid; c < nc; c += nthreads) a.count[c] = 0;
 	if (threadIdx.x == 0) a.look[blockIdx.x] = 0ull;
 	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
-	const int lane = threadIdx.x & 31;
-	for (int64_t c = tid >> 5; c < nc; c += nthreads >> 5) sort_cell(c, lane, a.start, a.perm, a.p, a.q, a.rank, false);
+	// 4. slot t's place in its cell: the cell's slots with a smaller (id, previous slot)
+	for (int64_t t = tid; t < a.n; t += nthreads) {
+		const int32_t c = a.scell[t];
+		const int32_t s = a.start[c], e = a.start[c + 1];
+		const int32_t from = a.perm[t];
+		const uint64_t key = a.key[t];
+		int32_t pos = 0;
+		for (int32_t k = s; k < e; k++) {
+			const uint64_t ok = a.key[k];
+			if (ok < key || (ok == key && a.perm[k] < from)) pos++;
+		}
+		move_one(from, s + pos, key, c, a.p, a.q, a.rank, false);
+	}
 	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
 	for (int64_t i = tid; i < a.n; i += nthreads) {
 		a.p.rx[i] = a.q.rx[i];
@@ -431,6 +476,8 @@ cudaError_t launch_rebuild(Context* c, const Grid& g) {
 	a.cell = c->cell;
 	a.rank = c->rank;
 	a.perm = c->perm;
+	a.key = c->rb_key;
+	a.scell = c->rb_scell;
 	a.count = c->rb_count;
 	a.start = c->cell_start;
 	a.look = c->rb_look;

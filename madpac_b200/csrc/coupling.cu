@@ -21,8 +21,9 @@
 //    dimensions), their peculiar kinetic energies and the rescaling v = (v - vc)(1 + gamma (beta - 1))
 //    + vc with beta = sqrt(1.5 N_samples / interval T / E_cell); after the closing kick.
 //
-// Sums over molecules use 64-bit fixed point (velocities in steps of 2^-40, energies of 2^-32), so
-// the results do not depend on the order in which atomics land.
+// Sums over molecules use 64-bit fixed point (velocities and energies in steps of 2^-40), so the
+// results do not depend on the order in which atomics land; a per-cell sum of 2^23 or more would
+// wrap, which a double sum kept beside it detects (status kStatusRange, an error of the call).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -38,7 +39,13 @@ constexpr int kT = 256;
 inline unsigned nblk(int64_t n) { return (unsigned) ((n + kT - 1) / kT); }
 
 constexpr double kVScale = 1099511627776.0;   // 2^40
-constexpr double kEScale = 4294967296.0;      // 2^32
+constexpr double kEScale = 1099511627776.0;   // 2^40
+
+// A fixed-point sum that disagrees with its double shadow by 1 or more has wrapped (a wrap moves it
+// by 2^24; the shadow's own rounding is many orders below 1 for sums in range).
+__device__ __forceinline__ void check_range(unsigned long long fixed, double scale, double shadow, int* status) {
+	if (!(fabs((double) (long long) fixed / scale - shadow) < 1.0)) atomicOr(status, kStatusRange);
+}
 
 __global__ void k_reflect(int64_t n, Particles p, Grid g, int dim, int sod, bool so, unsigned long long* nout) {
 	const int64_t s = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
@@ -144,29 +151,36 @@ __device__ int coupling_cell(const CellGrid& c, const double pos[3]) {
 	return (ip[0] * c.size[1] + ip[1]) * c.size[2] + ip[2];
 }
 
-__global__ void k_th_save(int64_t n, Particles p, CellGrid cg, unsigned long long* vsum) {
+__global__ void k_th_save(int64_t n, Particles p, CellGrid cg, unsigned long long* vsum, double* shadow) {
 	const int64_t s = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (s >= n) return;
 	const double pos[3] = {p.rx[s], p.ry[s], p.rz[s]};
 	const int k = coupling_cell(cg, pos);
 	if (k < 0) return;
 	const double v[3] = {p.vx[s], p.vy[s], p.vz[s]};
-	for (int i = 0; i < 3; i++) atomicAdd(vsum + 4 * k + i, (unsigned long long) __double2ll_rn(v[i] * kVScale));
+	for (int i = 0; i < 3; i++) {
+		atomicAdd(vsum + 4 * k + i, (unsigned long long) __double2ll_rn(v[i] * kVScale));
+		atomicAdd(shadow + 4 * k + i, v[i]);
+	}
 	atomicAdd(vsum + 4 * k + 3, 1ull);
 }
 
 __global__ void k_th_cells(int ncells, const unsigned long long* vsum, int dx, int dy, int dz, double* vc,
-                           unsigned long long* esum) {
+                           unsigned long long* esum, double* shadow, int* status) {
 	const int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= ncells) return;
 	const double cnt = (double) (long long) vsum[4 * k + 3];
 	const int dir[3] = {dx, dy, dz};
-	for (int i = 0; i < 3; i++)
+	for (int i = 0; i < 3; i++) {
+		check_range(vsum[4 * k + i], kVScale, shadow[4 * k + i], status);
 		vc[3 * k + i] = dir[i] != 0 ? ((double) (long long) vsum[4 * k + i] / kVScale) / cnt : 0.0;
+	}
 	esum[k] = 0ull;
+	shadow[4 * k + 3] = 0.0;
 }
 
-__global__ void k_th_energy(int64_t n, Particles p, CellGrid cg, Species sp, const double* vc, unsigned long long* esum) {
+__global__ void k_th_energy(int64_t n, Particles p, CellGrid cg, Species sp, const double* vc, unsigned long long* esum,
+                            double* shadow) {
 	const int64_t s = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (s >= n) return;
 	const double pos[3] = {p.rx[s], p.ry[s], p.rz[s]};
@@ -180,15 +194,18 @@ __global__ void k_th_energy(int64_t n, Particles p, CellGrid cg, Species sp, con
 	}
 	e = __dmul_rn(e, __dmul_rn(0.5, sp.mass[p.cid[s]]));
 	atomicAdd(esum + k, (unsigned long long) __double2ll_rn(e * kEScale));
+	atomicAdd(shadow + 4 * k + 3, e);
 }
 
 __global__ void k_th_adjust(int64_t n, Particles p, CellGrid cg, const unsigned long long* vsum, const double* vc,
-                            const unsigned long long* esum, double interval, double T, double gamma) {
+                            const unsigned long long* esum, const double* shadow, int* status, double interval,
+                            double T, double gamma) {
 	const int64_t s = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (s >= n) return;
 	const double pos[3] = {p.rx[s], p.ry[s], p.rz[s]};
 	const int k = coupling_cell(cg, pos);
 	if (k < 0) return;
+	check_range(esum[k], kEScale, shadow[4 * k + 3], status);
 	const double target = __dmul_rn(__ddiv_rn(__dmul_rn(1.5, (double) (long long) vsum[4 * k + 3]), interval), T);
 	const double beta = __dsqrt_rn(__ddiv_rn(target, (double) (long long) esum[k] / kEScale));
 	const double f = __dadd_rn(1.0, __dmul_rn(gamma, __dsub_rn(beta, 1.0)));
@@ -212,6 +229,7 @@ struct mdgpu_thermostat {
 	unsigned long long* vsum;   // 4 per cell: fixed-point v sums and the sample count
 	unsigned long long* esum;   // per cell, fixed point
 	double* vc;                 // 3 per cell
+	double* shadow;             // 4 per cell: the sums in double, to detect a wrap
 };
 
 extern "C" {
@@ -292,14 +310,19 @@ int mdgpu_thermostat_create(mdgpu_thermostat** out, mdgpu_ctx* ctx, const mdgpu_
 	th->gamma = gamma;
 	th->interval = interval;
 	cudaError_t e = cudaSetDevice(c->device);
-	if (e == cudaSuccess) e = cudaMalloc(&th->vsum, sizeof(unsigned long long) * 5 * ncells + sizeof(double) * 3 * ncells);
-	if (e == cudaSuccess) e = cudaMemsetAsync(th->vsum, 0, sizeof(unsigned long long) * 5 * ncells, c->stream);
+	// vsum (4), esum (1), shadow (4), vc (3) per cell; everything but vc starts at zero
+	const size_t bytes = sizeof(unsigned long long) * 5 * ncells + sizeof(double) * 7 * ncells;
+	th->vsum = nullptr;
+	if (e == cudaSuccess) e = cudaMalloc(&th->vsum, bytes);
+	if (e == cudaSuccess) e = cudaMemsetAsync(th->vsum, 0, bytes, c->stream);
 	if (e != cudaSuccess) {
+		cudaFree(th->vsum);
 		delete th;
 		return set_cuda_error(c, e, "mdgpu_thermostat_create");
 	}
 	th->esum = th->vsum + 4 * ncells;
-	th->vc = reinterpret_cast<double*>(th->esum + ncells);
+	th->shadow = reinterpret_cast<double*>(th->esum + ncells);
+	th->vc = th->shadow + 4 * ncells;
 	*out = th;
 	return MDGPU_OK;
 }
@@ -311,19 +334,21 @@ int mdgpu_thermostat_apply(mdgpu_thermostat* th, int64_t iteration) {
 	cudaError_t e = cudaSetDevice(c->device);
 	const int64_t n = c->n;
 	if (e == cudaSuccess) {
-		k_th_save<<<nblk(n), kT, 0, c->stream>>>(n, c->p, th->cg, th->vsum);
+		k_th_save<<<nblk(n), kT, 0, c->stream>>>(n, c->p, th->cg, th->vsum, th->shadow);
 		count_launches(c, 1);
 		e = cudaGetLastError();
 	}
 	if (e == cudaSuccess && th->interval != 0 && iteration % th->interval == 0) {
 		k_th_cells<<<nblk(th->ncells), kT, 0, c->stream>>>(th->ncells, th->vsum, th->directed[0], th->directed[1],
-		                                                     th->directed[2], th->vc, th->esum);
-		k_th_energy<<<nblk(n), kT, 0, c->stream>>>(n, c->p, th->cg, c->sp, th->vc, th->esum);
-		k_th_adjust<<<nblk(n), kT, 0, c->stream>>>(n, c->p, th->cg, th->vsum, th->vc, th->esum, (double) th->interval,
-		                                           th->T, th->gamma);
+		                                                     th->directed[2], th->vc, th->esum, th->shadow, c->status);
+		k_th_energy<<<nblk(n), kT, 0, c->stream>>>(n, c->p, th->cg, c->sp, th->vc, th->esum, th->shadow);
+		k_th_adjust<<<nblk(n), kT, 0, c->stream>>>(n, c->p, th->cg, th->vsum, th->vc, th->esum, th->shadow, c->status,
+		                                           (double) th->interval, th->T, th->gamma);
 		count_launches(c, 3);
 		e = cudaGetLastError();
+		// the next interval's sums start from zero (the energies are cleared by k_th_cells)
 		if (e == cudaSuccess) e = cudaMemsetAsync(th->vsum, 0, sizeof(unsigned long long) * 4 * th->ncells, c->stream);
+		if (e == cudaSuccess) e = cudaMemsetAsync(th->shadow, 0, sizeof(double) * 4 * th->ncells, c->stream);
 	}
 	if (e != cudaSuccess) return set_cuda_error(c, e, "mdgpu_thermostat_apply");
 	return check_device_status(c);

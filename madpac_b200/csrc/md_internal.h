@@ -21,6 +21,7 @@ enum : int {
 	kStatusNonFinite = 4,
 	kStatusTimeout = 8,
 	kStatusCapacity = 16,
+	kStatusRange = 32,   // a 64-bit fixed-point sum left its range
 };
 
 // Comp2Param stream entries per ordered component pair, as doubles and floats.
@@ -117,6 +118,10 @@ struct Context {
 	int32_t* rb_count = nullptr;
 	unsigned long long* rb_look = nullptr;
 	int rb_look_cap = 0;
+	// its ids and cells in scatter order (rb_cap molecules)
+	uint64_t* rb_key = nullptr;
+	int32_t* rb_scell = nullptr;
+	int64_t rb_cap = 0;
 	unsigned long long* builds = nullptr;   // builds so far (device counter)
 	// device: bricks of the last build, sparse [0] and dense [1], and the work queues of the sparse [3]
 	// and dense [2] list kernels; brick_list: the dense bricks' indices, then (from nbricks on) the

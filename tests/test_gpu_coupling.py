@@ -133,3 +133,22 @@ def test_thermostat_matches_the_oracle(dim, directed, gamma):
         lc.setState(v=vr)
     th.close()
     lc.close()
+
+
+def test_thermostat_reports_a_sum_out_of_range():
+    """A cell whose velocity sum reaches the fixed-point range (2^23) fails the call instead of
+    rescaling with a wrapped sum; the container stays usable."""
+    s = W.lj_fcc_box(4, 0.8, 1.0, 9, 2.5, LJ, name="thermostat_range")
+    lc = M.LinkedCells.from_system(s)
+    v = s.v.copy()
+    v[:, 0] = 1.0e6
+    lc.setState(v=v)
+    L = s.length
+    th = M.CellWiseThermostat(lc, [0, 0, 0], L, L[0], [1, 1, 1], 3, 1.0, 1.0, 1, (1, 0, 0))
+    with pytest.raises(M.MdgpuError, match="fixed-point"):
+        th.applyThermostat(1)
+    lc.setState(v=s.v)
+    lc.update()
+    lc.traversePairs()
+    th.close()
+    lc.close()
