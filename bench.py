@@ -738,11 +738,14 @@ def run_rigid(args, dist: Dist):
     dt = system.dt
     ncentre = 8 if args.charges else 4   # LJ centre pairs (+ charge pairs) per molecule pair
 
-    def device_run(precision, steps, warmup):
+    def device_run(precision, steps, warmup, skin=args.skin):
         lc = M.RigidLinkedCells.from_system(system, precision, device=dist.local)
         lc.update()
         lc.traversePairs()
+        if skin > 0.0:
+            lc.setSkin(skin)
         lc.run(warmup, dt, record=False)
+        b0 = lc.skinBuilds() if skin > 0.0 else 0
         stream = torch.cuda.ExternalStream(lc.stream())
         l0 = lc.launches()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -754,6 +757,7 @@ def run_rigid(args, dist: Dist):
         torch.cuda.synchronize()
         sec = e0.elapsed_time(e1) * 1e-3
         launches = lc.launches() - l0
+        device_run.builds = (lc.skinBuilds() - b0) if skin > 0.0 else None
         # kernel groups over a few more steps
         lc.profileRead(reset=True)
         lc.profileEnable(True)
@@ -766,6 +770,7 @@ def run_rigid(args, dist: Dist):
     clocks = ClockSampler(dist.local)
     clocks.start()
     lc, sec, rec, launches, groups_ms, cnt, krec = device_run(M.MIXED, args.steps, args.warmup)
+    builds = device_run.builds
     clk = clocks.stop()
     sec = dist.max(sec)
     mol_pairs = float(rec[:, 4].sum())
@@ -803,11 +808,19 @@ def run_rigid(args, dist: Dist):
 
     # the FP64 form of the same steps
     fp64 = None
+    rebinned = None
     if not args.no_compare:
         lc64, sec64, rec64, *_ = device_run(M.FP64, args.steps, args.warmup)
         sec64 = dist.max(sec64)
         fp64 = {"value": dist.sum(float(rec64[:, 4].sum()) * ncentre) / sec64, "ms_per_step": sec64 / args.steps * 1e3}
         lc64.close()
+        if args.skin > 0.0:
+            # the reference's sequence: binning and candidate search every step
+            lcb, secb, recb, *_ = device_run(M.MIXED, args.steps, args.warmup, skin=0.0)
+            secb = dist.max(secb)
+            rebinned = {"value": dist.sum(float(recb[:, 4].sum()) * ncentre) / secb,
+                        "ms_per_step": secb / args.steps * 1e3}
+            lcb.close()
 
     out = {
         "metric": RIGID_Q_METRIC if args.charges else RIGID_METRIC, "value": value,
@@ -822,7 +835,9 @@ def run_rigid(args, dist: Dist):
                    "potential": "2CLJ, LJ 12-6 truncated-shifted per centre pair" +
                                 (", point charges +-0.5 at z = +-0.35 (plain Coulomb)" if args.charges else "") +
                                 ", cutoff on the molecule centres",
-                   "pair_search": "cells rebuilt and candidates searched every step",
+                   "pair_search": (f"lists of the molecule pairs within rc + {args.skin:g}, rebuilt (with the "
+                                   f"binning) when a centre moved more than {args.skin / 2:g}; exact rc test on every "
+                                   "list entry") if args.skin > 0.0 else "cells rebuilt and candidates searched every step",
                    "l2": f"not flushed: each step reads the whole state ({n * 230 / 1e6:.0f} MB of molecule arrays, "
                          "above the 126 MB L2)"},
         "molecule_pairs_per_step": mol_pairs / args.steps,
@@ -837,6 +852,8 @@ def run_rigid(args, dist: Dist):
                      "timed": "k_rigid_sites + k_rigid_pairs per step, CUDA events on the library stream"},
         "fp64": fp64,
         "speedup_vs_fp64": (value / fp64["value"]) if fp64 else None,
+        "rebuilds_per_step": (builds / args.steps) if builds is not None else None,
+        "rebinned_every_step": rebinned,
         "e2e": {"value": e2e_value, "unit": RIGID_UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
                 "d2h_bytes_per_step": d2h / e2e_steps,
                 "note": f"one upload of id, cid, r, v, q, D and one download of the final state per run of "

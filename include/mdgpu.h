@@ -415,6 +415,16 @@ int mdgpu_rigid_leapfrog_post(mdgpu_rigid* h, double dt_half, double* summv2, do
 /* nsteps NVE steps of Simulation::simulateStep (after the forces of the start are in place);
  * per_step (may be NULL): 5 doubles per step {Upot, virial, sum m v^2, sum I w^2, pairs}. */
 int mdgpu_rigid_run(mdgpu_rigid* h, int32_t nsteps, double dt, double* per_step);
+/* Verlet-skin mode of mdgpu_rigid_run (no reference counterpart; skin 0 turns it off): each step
+ * tests every molecule pair of a list of radius rc + skin with the exact cutoff, and the rebinning
+ * (on cells of edge >= rc + skin) and the list build run only when a molecule has moved more than
+ * skin/2 since the last build; 0 < skin <= rc/2. list_cap: list entries per molecule (0: from the
+ * densest cell of the loaded positions); a molecule with more candidates scans its cells instead.
+ * After skin steps the cells are not the reference's: mdgpu_rigid_traverse_pairs needs
+ * mdgpu_rigid_update first. */
+int mdgpu_rigid_set_skin(mdgpu_rigid* h, double skin, int32_t list_cap);
+/* List builds of the rigid context's skin mode so far (synchronises its stream). */
+int mdgpu_rigid_skin_builds(mdgpu_rigid* h, int64_t* builds);
 int mdgpu_rigid_get_stream(const mdgpu_rigid* h, void** stream);
 /* Kernel timing of the context, as mdgpu_profile_enable / mdgpu_profile_read (groups: binning,
  * site rotation + pairs, integration; counts[3] = all launches so far). */

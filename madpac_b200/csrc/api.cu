@@ -391,6 +391,38 @@ int device_max_optin(int device) {
 	return v;
 }
 
+int rebuild_prepare(Context* c) {
+	const int64_t n = c->n;
+	if (c->rb_cap < n) {
+		cudaFree(c->rb_slot);
+		c->rb_slot = nullptr;
+		c->rb_cap = 0;
+		MD_CUDA(cudaMalloc(&c->rb_slot, sizeof(int4) * n));
+		c->rb_cap = n;
+	}
+	if (!c->rebuild) {
+		MD_CUDA(cudaMalloc(&c->rebuild, sizeof(int)));
+		MD_CUDA(cudaMemsetAsync(c->rebuild, 0xff, sizeof(int), c->stream));
+		MD_CUDA(cudaMalloc(&c->builds, sizeof(unsigned long long)));
+		MD_CUDA(cudaMemsetAsync(c->builds, 0, sizeof(unsigned long long), c->stream));
+		MD_CUDA(cudaMalloc(&c->bar, sizeof(unsigned) * 4));
+		MD_CUDA(cudaMemsetAsync(c->bar, 0, sizeof(unsigned) * 4, c->stream));
+		c->rb_look_cap = 8192;
+		MD_CUDA(cudaMalloc(&c->rb_look, sizeof(unsigned long long) * c->rb_look_cap));
+		MD_CUDA(cudaMemsetAsync(c->rb_look, 0, sizeof(unsigned long long) * c->rb_look_cap, c->stream));
+		MD_CUDA(cudaMalloc(&c->rb_count, sizeof(int32_t) * c->g.ncells));
+		MD_CUDA(cudaMemsetAsync(c->rb_count, 0, sizeof(int32_t) * c->g.ncells, c->stream));
+	}
+	return MDGPU_OK;
+}
+
+int request_build(Context* c) {
+	k_set_int<<<1, 1, 0, c->stream>>>(c->rebuild, c->step_id);
+	count_launches(c, 1);
+	MD_CUDA(cudaGetLastError());
+	return MDGPU_OK;
+}
+
 }  // namespace mdgpu
 
 using namespace mdgpu;
@@ -486,8 +518,7 @@ int mdgpu_destroy(mdgpu_ctx* ctx) {
 	if (c->h_sparse) cudaFreeHost(c->h_sparse);
 	cudaFree(c->rb_count);
 	cudaFree(c->rb_look);
-	cudaFree(c->rb_key);
-	cudaFree(c->rb_scell);
+	cudaFree(c->rb_slot);
 	cudaFree(c->tickets);
 	cudaFree(c->brick_kind);
 	cudaFree(full->x.stage.ptr);
@@ -815,15 +846,9 @@ int skin_prepare(Context* c) {
 		c->list_cap = cap;
 		c->lists_valid = false;
 	}
-	if (c->rb_cap < n) {
-		cudaFree(c->rb_key);
-		cudaFree(c->rb_scell);
-		c->rb_key = nullptr;
-		c->rb_scell = nullptr;
-		c->rb_cap = 0;
-		MD_CUDA(cudaMalloc(&c->rb_key, sizeof(uint64_t) * n));
-		MD_CUDA(cudaMalloc(&c->rb_scell, sizeof(int32_t) * n));
-		c->rb_cap = n;
+	{
+		const int st = rebuild_prepare(c);
+		if (st) return st;
 	}
 	const int64_t parts = skin_partials_needed(c);
 	if (c->brick_kind == nullptr || c->list_n != n || c->lists_valid == false) {
@@ -842,18 +867,7 @@ int skin_prepare(Context* c) {
 		MD_CUDA(cudaMalloc(&c->partials, sizeof(double) * 4 * (parts + 1024)));
 		c->partial_cap = parts + 1024;
 	}
-	if (!c->rebuild) {
-		MD_CUDA(cudaMalloc(&c->rebuild, sizeof(int)));
-		MD_CUDA(cudaMemsetAsync(c->rebuild, 0xff, sizeof(int), c->stream));
-		MD_CUDA(cudaMalloc(&c->builds, sizeof(unsigned long long)));
-		MD_CUDA(cudaMemsetAsync(c->builds, 0, sizeof(unsigned long long), c->stream));
-		MD_CUDA(cudaMalloc(&c->bar, sizeof(unsigned) * 4));
-		MD_CUDA(cudaMemsetAsync(c->bar, 0, sizeof(unsigned) * 4, c->stream));
-		c->rb_look_cap = 8192;
-		MD_CUDA(cudaMalloc(&c->rb_look, sizeof(unsigned long long) * c->rb_look_cap));
-		MD_CUDA(cudaMemsetAsync(c->rb_look, 0, sizeof(unsigned long long) * c->rb_look_cap, c->stream));
-		MD_CUDA(cudaMalloc(&c->rb_count, sizeof(int32_t) * c->g.ncells));
-		MD_CUDA(cudaMemsetAsync(c->rb_count, 0, sizeof(int32_t) * c->g.ncells, c->stream));
+	if (!c->brick_counts) {
 		MD_CUDA(cudaMalloc(&c->brick_counts, sizeof(unsigned) * 4));
 		MD_CUDA(cudaMemsetAsync(c->brick_counts, 0, sizeof(unsigned) * 4, c->stream));
 		MD_CUDA(cudaMallocHost(&c->h_sparse, sizeof(int)));

@@ -29,9 +29,8 @@ namespace {
 
 constexpr int kScanBlock = 1024;   // elements per scan block (256 threads x 4)
 
-// Wrap molecule i, return its inner cell and flag positions outside the halo box.
-__device__ __forceinline__ int32_t bin_one(int64_t i, double* rx, double* ry, double* rz, const Grid& g, bool& bad) {
-	double r[3] = {rx[i], ry[i], rz[i]};
+// Wrap the position r in place and return its inner cell; flags positions outside the halo box.
+__device__ __forceinline__ int32_t wrap_cell(double r[3], const Grid& g, bool& bad) {
 	int ci[3];
 	for (int d = 0; d < 3; d++) {
 		double x = r[d];
@@ -50,33 +49,52 @@ __device__ __forceinline__ int32_t bin_one(int64_t i, double* rx, double* ry, do
 		ci[d] = c - 1;
 		if (!(x == x)) bad = true;
 	}
-	if (r[0] != rx[i]) rx[i] = r[0];
-	if (r[1] != ry[i]) ry[i] = r[1];
-	if (r[2] != rz[i]) rz[i] = r[2];
 	return (int32_t) (((int64_t) ci[2] * g.nc[1] + ci[1]) * g.nc[0] + ci[0]);
+}
+
+// Wrap molecule i, return its inner cell and flag positions outside the halo box.
+__device__ __forceinline__ int32_t bin_one(int64_t i, double* rx, double* ry, double* rz, const Grid& g, bool& bad) {
+	const double r0[3] = {rx[i], ry[i], rz[i]};
+	double r[3] = {r0[0], r0[1], r0[2]};
+	const int32_t c = wrap_cell(r, g, bad);
+	if (r[0] != r0[0]) rx[i] = r[0];
+	if (r[1] != r0[1]) ry[i] = r[1];
+	if (r[2] != r0[2]) rz[i] = r[2];
+	return c;
 }
 
 __device__ __forceinline__ bool key_less(uint64_t ka, int32_t sa, uint64_t kb, int32_t sb) {
 	return ka < kb || (ka == kb && sa < sb);
 }
 
-// Molecule `from` to slot `to` of the other buffer.
+// Molecule `from` to slot `to` of the other buffer. Every field is loaded before the first store:
+// the compiler cannot tell the two buffers apart, and a load after a store to a possibly aliasing
+// address would wait for it, serialising the loads' latencies.
 __device__ __forceinline__ void move_one(int32_t from, int32_t to, uint64_t key, int64_t c, const Particles& src,
                                          const Particles& dst, int32_t* cell_out, bool with_forces) {
-	dst.rx[to] = src.rx[from];
-	dst.ry[to] = src.ry[from];
-	dst.rz[to] = src.rz[from];
-	dst.vx[to] = src.vx[from];
-	dst.vy[to] = src.vy[from];
-	dst.vz[to] = src.vz[from];
+	const double x = src.rx[from], y = src.ry[from], z = src.rz[from];
+	const double vx = src.vx[from], vy = src.vy[from], vz = src.vz[from];
+	double fx = 0.0, fy = 0.0, fz = 0.0;
 	if (with_forces) {
-		dst.fx[to] = src.fx[from];
-		dst.fy[to] = src.fy[from];
-		dst.fz[to] = src.fz[from];
+		fx = src.fx[from];
+		fy = src.fy[from];
+		fz = src.fz[from];
+	}
+	const int32_t ci = src.cid[from], ui = src.uidx[from];
+	dst.rx[to] = x;
+	dst.ry[to] = y;
+	dst.rz[to] = z;
+	dst.vx[to] = vx;
+	dst.vy[to] = vy;
+	dst.vz[to] = vz;
+	if (with_forces) {
+		dst.fx[to] = fx;
+		dst.fy[to] = fy;
+		dst.fz[to] = fz;
 	}
 	dst.id[to] = key;
-	dst.cid[to] = src.cid[from];
-	dst.uidx[to] = src.uidx[from];
+	dst.cid[to] = ci;
+	dst.uidx[to] = ui;
 	cell_out[to] = (int32_t) c;
 }
 
@@ -249,8 +267,7 @@ struct RebuildArgs {
 	Grid g;
 	Particles p, q;
 	int32_t *cell, *rank, *perm, *count, *start;
-	uint64_t* key;              // ids in scatter order
-	int32_t* scell;             // cells in scatter order
+	int4* slot;                 // per arrival slot: cell, cell start, cell end, previous slot
 	unsigned long long* look;   // per CTA: the scan's published value (flag in bits 62-63)
 	int* status;
 	const int* flag;
@@ -271,7 +288,7 @@ __device__ __forceinline__ unsigned long long load_acquire64(const unsigned long
 	return v;
 }
 
-// Wrap, binning, scan and (cell, id) sort of all molecules in one cooperative launch with four
+// Wrap, binning, scan and (cell, id) sort of all molecules in one cooperative launch with three
 // bounded grid barriers; returns at once unless a build was asked for this step. count[] and look[]
 // are zero on entry and are left zero for the next launch (a launch that gave up on a wait leaves
 // them to the host, which clears them with the timeout status).
@@ -281,12 +298,12 @@ __device__ __forceinline__ unsigned long long load_acquire64(const unsigned long
 //      sum, adds up its predecessors' published values back to the first complete prefix, 32 at a
 //      time by one warp (decoupled look-back: every CTA of the cooperative grid is resident, so each
 //      of these waits ends; each is bounded nonetheless) and publishes its own prefix
-//   3. scatter of the arrival order with each slot's id and cell; counts and look-back words
-//      cleared for the next launch
+//   3. every molecule to its arrival slot in the other buffer, with its cell and previous slot;
+//      counts and look-back words cleared for the next launch
 //   4. one thread per slot: its rank by (id, previous slot) among its cell's slots, read from the
-//      contiguous ids of the cell, and the gather into the other buffer
-//   5. the sorted arrays back into the current buffer (the host's buffer roles stay fixed)
-__global__ void __launch_bounds__(kRebuildThreads) k_rebuild(RebuildArgs a) {
+//      contiguous ids of the cell, and the molecule back into the current buffer at that rank (the
+//      host's buffer roles stay fixed)
+__global__ void __launch_bounds__(kRebuildThreads, 4) k_rebuild(RebuildArgs a) {
 	__shared__ int s_flag;
 	__shared__ int32_t s_excl;
 	if (threadIdx.x == 0) s_flag = (*a.flag == a.step && !(*((volatile int*) a.status) & kStatusTimeout)) ? 0 : 1;
@@ -322,7 +339,8 @@ __global__ void __launch_bounds__(kRebuildThreads) k_rebuild(RebuildArgs a) {
 		int32_t local = 0;
 		for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) local += a.count[c];
 		int32_t agg;
-		block_excl_scan(local, &agg);
+		// with at most one cell per thread this is already the chunk's own exclusive scan
+		const int32_t lexcl = block_excl_scan(local, &agg);
 		if (threadIdx.x < 32) {
 			unsigned long long* look = a.look;
 			const int b = (int) blockIdx.x;
@@ -365,53 +383,72 @@ __global__ void __launch_bounds__(kRebuildThreads) k_rebuild(RebuildArgs a) {
 		}
 		__syncthreads();
 		if (s_flag) return;
-		int32_t carry = s_excl;
-		for (int64_t base = c0; base < c1; base += blockDim.x) {
-			const int64_t c = base + threadIdx.x;
-			const int32_t v = c < c1 ? a.count[c] : 0;
-			int32_t tot;
-			const int32_t excl = block_excl_scan(v, &tot);
-			if (c < c1) a.start[c] = carry + excl;
-			carry += tot;
+		if (per <= (int64_t) blockDim.x) {
+			if (c0 + threadIdx.x < c1) a.start[c0 + threadIdx.x] = s_excl + lexcl;
+		} else {
+			int32_t carry = s_excl;
+			for (int64_t base = c0; base < c1; base += blockDim.x) {
+				const int64_t c = base + threadIdx.x;
+				const int32_t v = c < c1 ? a.count[c] : 0;
+				int32_t tot;
+				const int32_t excl = block_excl_scan(v, &tot);
+				if (c < c1) a.start[c] = carry + excl;
+				carry += tot;
+			}
 		}
 	}
 	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
-	// 3. arrival-order scatter; the counts and the look-back words are not read again in this launch
+	// 3. every molecule, all fields, to its arrival slot in the other buffer, with its cell and
+	// previous slot; the counts and the look-back words are not read again in this launch. All loads
+	// come before the stores (the compiler cannot tell the buffers apart).
 	for (int64_t i = tid; i < a.n; i += nthreads) {
-		const int32_t c = a.cell[i];
-		const int32_t slot = a.start[c] + a.rank[i];
-		a.perm[slot] = (int32_t) i;
-		a.key[slot] = a.p.id[i];
-		a.scell[slot] = c;
+		const int32_t c = a.cell[i], rk = a.rank[i];
+		const double x = a.p.rx[i], y = a.p.ry[i], z = a.p.rz[i];
+		const double vx = a.p.vx[i], vy = a.p.vy[i], vz = a.p.vz[i];
+		const uint64_t id = a.p.id[i];
+		const int32_t ci = a.p.cid[i], ui = a.p.uidx[i];
+		const int32_t s = a.start[c], e = a.start[c + 1];
+		const int32_t slot = s + rk;
+		a.q.rx[slot] = x;
+		a.q.ry[slot] = y;
+		a.q.rz[slot] = z;
+		a.q.vx[slot] = vx;
+		a.q.vy[slot] = vy;
+		a.q.vz[slot] = vz;
+		a.q.id[slot] = id;
+		a.q.cid[slot] = ci;
+		a.q.uidx[slot] = ui;
+		a.slot[slot] = make_int4(c, s, e, (int32_t) i);
 	}
 	for (int64_t c = tid; c < nc; c += nthreads) a.count[c] = 0;
 	if (threadIdx.x == 0) a.look[blockIdx.x] = 0ull;
 	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
-	// 4. slot t's place in its cell: the cell's slots with a smaller (id, previous slot)
+	// 4. slot t's place in its cell, the cell's slots with a smaller (id, previous slot), read from
+	// the cell's contiguous ids; the molecule back into the current buffer there
 	for (int64_t t = tid; t < a.n; t += nthreads) {
-		const int32_t c = a.scell[t];
-		const int32_t s = a.start[c], e = a.start[c + 1];
-		const int32_t from = a.perm[t];
-		const uint64_t key = a.key[t];
+		const int4 sl = a.slot[t];
+		const double x = a.q.rx[t], y = a.q.ry[t], z = a.q.rz[t];
+		const double vx = a.q.vx[t], vy = a.q.vy[t], vz = a.q.vz[t];
+		const uint64_t key = a.q.id[t];
+		const int32_t ci = a.q.cid[t], ui = a.q.uidx[t];
 		int32_t pos = 0;
-		for (int32_t k = s; k < e; k++) {
-			const uint64_t ok = a.key[k];
-			if (ok < key || (ok == key && a.perm[k] < from)) pos++;
+#pragma unroll 4
+		for (int32_t k = sl.y; k < sl.z; k++) {
+			const uint64_t ok = a.q.id[k];
+			// equal ids (not in valid input) keep the order of their previous slots
+			pos += ok < key ? 1 : ((ok == key && a.slot[k].w < sl.w) ? 1 : 0);
 		}
-		move_one(from, s + pos, key, c, a.p, a.q, a.rank, false);
-	}
-	if (!grid_barrier(a.bar, a.status, a.timeout_ns, &s_flag)) return;
-	for (int64_t i = tid; i < a.n; i += nthreads) {
-		a.p.rx[i] = a.q.rx[i];
-		a.p.ry[i] = a.q.ry[i];
-		a.p.rz[i] = a.q.rz[i];
-		a.p.vx[i] = a.q.vx[i];
-		a.p.vy[i] = a.q.vy[i];
-		a.p.vz[i] = a.q.vz[i];
-		a.p.id[i] = a.q.id[i];
-		a.p.cid[i] = a.q.cid[i];
-		a.p.uidx[i] = a.q.uidx[i];
-		a.cell[i] = a.rank[i];
+		const int32_t to = sl.y + pos;
+		a.p.rx[to] = x;
+		a.p.ry[to] = y;
+		a.p.rz[to] = z;
+		a.p.vx[to] = vx;
+		a.p.vy[to] = vy;
+		a.p.vz[to] = vz;
+		a.p.id[to] = key;
+		a.p.cid[to] = ci;
+		a.p.uidx[to] = ui;
+		a.cell[to] = sl.x;
 	}
 }
 
@@ -476,8 +513,7 @@ cudaError_t launch_rebuild(Context* c, const Grid& g) {
 	a.cell = c->cell;
 	a.rank = c->rank;
 	a.perm = c->perm;
-	a.key = c->rb_key;
-	a.scell = c->rb_scell;
+	a.slot = c->rb_slot;
 	a.count = c->rb_count;
 	a.start = c->cell_start;
 	a.look = c->rb_look;

@@ -118,9 +118,9 @@ struct Context {
 	int32_t* rb_count = nullptr;
 	unsigned long long* rb_look = nullptr;
 	int rb_look_cap = 0;
-	// its ids and cells in scatter order (rb_cap molecules)
-	uint64_t* rb_key = nullptr;
-	int32_t* rb_scell = nullptr;
+	// per arrival slot (rb_cap of them): the molecule's cell, the cell's first and end slots, and the
+	// molecule's previous slot
+	int4* rb_slot = nullptr;
 	int64_t rb_cap = 0;
 	unsigned long long* builds = nullptr;   // builds so far (device counter)
 	// device: bricks of the last build, sparse [0] and dense [1], and the work queues of the sparse [3]
@@ -184,6 +184,14 @@ cudaError_t launch_step_record(Context* c, double* dst);        // dst[0..3] <- 
 int setup_grid(const double length[3], double cutoff, double cells_in_cutoff, Grid& g, std::string& err);
 // The Verlet-skin grid: an odd cell count of 5 or more in a dimension is lowered by one (cells grow).
 void even_grid(Grid& g);
+// The grid on which the Verlet-skin lists of radius rc + skin are built (cells of edge >= rc + skin,
+// larger in a dilute liquid), from the context's box and loaded positions.
+int skin_grid(const Context* c, double skin, Grid& gs, std::string& err);
+// Buffers of the cooperative rebuild (launch_rebuild) for the loaded molecules: the build flag, the
+// build counter, the barrier and look-back words, the cell counts and the arrival-slot records.
+int rebuild_prepare(Context* c);
+// Asks for a build in the step c->step_id (sets *c->rebuild on the context's stream).
+int request_build(Context* c);
 int setup_species(int ncomp, const mdgpu_component* comps, const double* mix, double rc_lj, Species& sp,
                   std::string& err);
 PairParams pair_params(const Species& sp, double rc, double rc_lj);

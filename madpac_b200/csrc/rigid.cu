@@ -340,6 +340,17 @@ static_assert(kRigidLanes == 1 || kRigidLanes == 2 || kRigidLanes == 4 || kRigid
 // torque formed at the end as calcFM does (M = sum_s d_s x F_s); the virial term of a molecule pair
 // is drm . (sum of its centre forces).
 // kQ: 0 LJ centres only, 1 with charges, 2 with dipoles or quadrupoles as well
+//
+// Verlet-skin mode (vl.list non-null): the candidates are molecule i's entries of the list that
+// k_rigid_build made (codes j << 5 | image, within rc + skin at the build), tested with the same
+// exact double cutoff; a molecule whose list overflowed at the build (count -1) scans its 27 cells
+// of the skin grid instead, which finds the same partners: since the build no molecule has moved
+// more than skin/2, and the cells are at least rc + skin wide.
+struct RigidLists {
+	const uint32_t* list;    // cap x n, entry k of molecule i at k * n + i
+	const int32_t* count;    // per molecule; -1: overflowed at the build
+};
+
 template <bool kMixed, int NS, int kQ>
 __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const double* __restrict__ rx,
                                                                const double* __restrict__ ry,
@@ -350,7 +361,8 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
                                                                const RigidParams* __restrict__ P,
                                                                const double* __restrict__ ds,
                                                                const float* __restrict__ dsf,
-                                                               const double* __restrict__ es, RigidOut o) {
+                                                               const double* __restrict__ es, RigidOut o,
+                                                               RigidLists vl) {
 	constexpr int TT = kMaxSiteTotal * kMaxSiteTotal;
 	__shared__ double s_e24[TT], s_sig2[TT], s_sh6[TT];
 	__shared__ int s_ns[kMaxSpecies], s_nlj[kMaxSpecies], s_base[kMaxSpecies];
@@ -580,60 +592,74 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 			cnt = 0;
 		};
 
-		int cc[3];
-		const double r[3] = {xi, yi, zi};
-		for (int d = 0; d < 3; d++) {
-			int c = (int) floor(__ddiv_rn(__dsub_rn(r[d], g.halo_min[d]), g.cell_length[d])) - 1;
-			cc[d] = c < 0 ? 0 : (c >= g.nc[d] ? g.nc[d] - 1 : c);
-		}
-		for (int dz = -1; dz <= 1; dz++) {
-			int z = cc[2] + dz, iz = 1;
-			if (z < 0) {
-				z += g.nc[2];
-				iz = 0;
-			} else if (z >= g.nc[2]) {
-				z -= g.nc[2];
-				iz = 2;
+		// candidate j in image img (shift sx, sy, sz): the exact cutoff test of the reference; the
+		// accepted ones go to the lane's list
+		auto consider = [&](int j, uint32_t img, double sx, double sy, double sz) {
+			// the halo image of j (DomainDecompDummy.cpp:64-70, 93-99); adding 0 is exact
+			const double m0 = __dsub_rn(xi, __dadd_rn(rx[j], sx));
+			const double m1 = __dsub_rn(yi, __dadd_rn(ry[j], sy));
+			const double m2 = __dsub_rn(zi, __dadd_rn(rz[j], sz));
+			const double dd = __dadd_rn(__dadd_rn(__dmul_rn(m0, m0), __dmul_rn(m1, m1)), __dmul_rn(m2, m2));
+			if (!(dd < rc2)) return;
+			np += 1.0;
+			if (dd == 0.0) same = true;
+			if (!kQ && !(dd < rclj2)) return;
+			list[cnt * kRigidThreads] = ((uint32_t) j << 5) | img;
+			if (++cnt == kRigidList) evaluate();
+		};
+		const int32_t nlist = vl.list ? vl.count[i] : -1;
+		if (nlist >= 0) {
+			for (int e = sub; e < nlist; e += kRigidLanes) {
+				const uint32_t code = vl.list[(int64_t) e * n + i];
+				const uint32_t img = code & 31u;
+				consider((int) (code >> 5), img, (double) ((int) (img % 3u) - 1) * g.L[0],
+				         (double) ((int) ((img / 3u) % 3u) - 1) * g.L[1], (double) ((int) (img / 9u) - 1) * g.L[2]);
 			}
-			const double sz = (double) (iz - 1) * g.L[2];
-			for (int dy = -1; dy <= 1; dy++) {
-				int y = cc[1] + dy, iy = 1;
-				if (y < 0) {
-					y += g.nc[1];
-					iy = 0;
-				} else if (y >= g.nc[1]) {
-					y -= g.nc[1];
-					iy = 2;
+		} else {
+			int cc[3];
+			const double r[3] = {xi, yi, zi};
+			for (int d = 0; d < 3; d++) {
+				int c = (int) floor(__ddiv_rn(__dsub_rn(r[d], g.halo_min[d]), g.cell_length[d])) - 1;
+				cc[d] = c < 0 ? 0 : (c >= g.nc[d] ? g.nc[d] - 1 : c);
+			}
+			for (int dz = -1; dz <= 1; dz++) {
+				int z = cc[2] + dz, iz = 1;
+				if (z < 0) {
+					z += g.nc[2];
+					iz = 0;
+				} else if (z >= g.nc[2]) {
+					z -= g.nc[2];
+					iz = 2;
 				}
-				const double sy = (double) (iy - 1) * g.L[1];
-				for (int dx = -1; dx <= 1; dx++) {
-					int x = cc[0] + dx, ix = 1;
-					if (x < 0) {
-						x += g.nc[0];
-						ix = 0;
-					} else if (x >= g.nc[0]) {
-						x -= g.nc[0];
-						ix = 2;
+				const double sz = (double) (iz - 1) * g.L[2];
+				for (int dy = -1; dy <= 1; dy++) {
+					int y = cc[1] + dy, iy = 1;
+					if (y < 0) {
+						y += g.nc[1];
+						iy = 0;
+					} else if (y >= g.nc[1]) {
+						y -= g.nc[1];
+						iy = 2;
 					}
-					const double sx = (double) (ix - 1) * g.L[0];
-					const uint32_t img = (uint32_t) (ix + 3 * iy + 9 * iz);
-					const bool shifted = img != 13u;
-					const int nb = (z * g.nc[1] + y) * g.nc[0] + x;
-					const int j0 = start[nb], j1 = start[nb + 1];
-					for (int j = j0 + sub; j < j1; j += kRigidLanes) {
-						if (j == i && !shifted) continue;
-						// the halo image of j (DomainDecompDummy.cpp:64-70, 93-99); adding 0 is exact
-						const double m0 = __dsub_rn(xi, __dadd_rn(rx[j], sx));
-						const double m1 = __dsub_rn(yi, __dadd_rn(ry[j], sy));
-						const double m2 = __dsub_rn(zi, __dadd_rn(rz[j], sz));
-						const double dd =
-						    __dadd_rn(__dadd_rn(__dmul_rn(m0, m0), __dmul_rn(m1, m1)), __dmul_rn(m2, m2));
-						if (!(dd < rc2)) continue;
-						np += 1.0;
-						if (dd == 0.0) same = true;
-						if (!kQ && !(dd < rclj2)) continue;
-						list[cnt * kRigidThreads] = ((uint32_t) j << 5) | img;
-						if (++cnt == kRigidList) evaluate();
+					const double sy = (double) (iy - 1) * g.L[1];
+					for (int dx = -1; dx <= 1; dx++) {
+						int x = cc[0] + dx, ix = 1;
+						if (x < 0) {
+							x += g.nc[0];
+							ix = 0;
+						} else if (x >= g.nc[0]) {
+							x -= g.nc[0];
+							ix = 2;
+						}
+						const double sx = (double) (ix - 1) * g.L[0];
+						const uint32_t img = (uint32_t) (ix + 3 * iy + 9 * iz);
+						const bool shifted = img != 13u;
+						const int nb = (z * g.nc[1] + y) * g.nc[0] + x;
+						const int j0 = start[nb], j1 = start[nb + 1];
+						for (int j = j0 + sub; j < j1; j += kRigidLanes) {
+							if (j == i && !shifted) continue;
+							consider(j, img, sx, sy, sz);
+						}
 					}
 				}
 			}
@@ -697,6 +723,84 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 	last_block_sum(o.ticket, o.partials, gridDim.x, 4, o.scalars);
 }
 
+// Verlet-skin build (only in the steps for which *flag == step, right after the rebinning on the
+// skin grid g): every molecule's candidates within rc + skin (rl2, the exact double test of the
+// pair kernel with the larger radius) as codes j << 5 | image in the scan order of the pair
+// kernel, column k of molecule i at k * n + i; count -1 when more than cap were found (the pair
+// kernel then scans the cells); the positions of the build for the displacement check.
+__global__ void __launch_bounds__(kRigidThreads) k_rigid_build(int64_t n, const double* __restrict__ rx,
+                                                               const double* __restrict__ ry,
+                                                               const double* __restrict__ rz,
+                                                               const int32_t* __restrict__ start, Grid g, double rl2,
+                                                               const int* flag, int step, int cap,
+                                                               uint32_t* __restrict__ list, int32_t* __restrict__ count,
+                                                               double* __restrict__ rref,
+                                                               unsigned long long* builds) {
+	if (*flag != step) return;
+	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (i == 0) atomicAdd(builds, 1ull);
+	if (i >= n) return;
+	const double xi = rx[i], yi = ry[i], zi = rz[i];
+	rref[i] = xi;
+	rref[n + i] = yi;
+	rref[2 * n + i] = zi;
+	const double r[3] = {xi, yi, zi};
+	int cc[3];
+	for (int d = 0; d < 3; d++) {
+		int c = (int) floor(__ddiv_rn(__dsub_rn(r[d], g.halo_min[d]), g.cell_length[d])) - 1;
+		cc[d] = c < 0 ? 0 : (c >= g.nc[d] ? g.nc[d] - 1 : c);
+	}
+	int cnt = 0;
+	for (int dz = -1; dz <= 1; dz++) {
+		int z = cc[2] + dz, iz = 1;
+		if (z < 0) {
+			z += g.nc[2];
+			iz = 0;
+		} else if (z >= g.nc[2]) {
+			z -= g.nc[2];
+			iz = 2;
+		}
+		const double sz = (double) (iz - 1) * g.L[2];
+		for (int dy = -1; dy <= 1; dy++) {
+			int y = cc[1] + dy, iy = 1;
+			if (y < 0) {
+				y += g.nc[1];
+				iy = 0;
+			} else if (y >= g.nc[1]) {
+				y -= g.nc[1];
+				iy = 2;
+			}
+			const double sy = (double) (iy - 1) * g.L[1];
+			for (int dx = -1; dx <= 1; dx++) {
+				int x = cc[0] + dx, ix = 1;
+				if (x < 0) {
+					x += g.nc[0];
+					ix = 0;
+				} else if (x >= g.nc[0]) {
+					x -= g.nc[0];
+					ix = 2;
+				}
+				const double sx = (double) (ix - 1) * g.L[0];
+				const uint32_t img = (uint32_t) (ix + 3 * iy + 9 * iz);
+				const bool shifted = img != 13u;
+				const int nb = (z * g.nc[1] + y) * g.nc[0] + x;
+				const int j0 = start[nb], j1 = start[nb + 1];
+				for (int j = j0; j < j1; j++) {
+					if (j == i && !shifted) continue;
+					const double m0 = __dsub_rn(xi, __dadd_rn(rx[j], sx));
+					const double m1 = __dsub_rn(yi, __dadd_rn(ry[j], sy));
+					const double m2 = __dsub_rn(zi, __dadd_rn(rz[j], sz));
+					const double dd = __dadd_rn(__dadd_rn(__dmul_rn(m0, m0), __dmul_rn(m1, m1)), __dmul_rn(m2, m2));
+					if (!(dd < rl2)) continue;
+					if (cnt < cap) list[(int64_t) cnt * n + i] = ((uint32_t) j << 5) | img;
+					cnt++;
+				}
+			}
+		}
+	}
+	count[i] = cnt <= cap ? cnt : -1;
+}
+
 struct RigidState {
 	double *rx, *ry, *rz, *vx, *vy, *vz;
 	const double *fx, *fy, *fz;
@@ -707,9 +811,18 @@ struct RigidState {
 	const double* M;
 };
 
+// Displacement check of the Verlet-skin mode: with rref, a molecule farther than skin/2 from its
+// position at the last build (half_skin2 = (skin/2)^2) asks for a build in this step.
+struct SkinCheck {
+	const double* rref;   // 3 x n, sorted order
+	double half_skin2;
+	int* flag;
+	int step;
+};
+
 // Molecule::upd_preF for every molecule
 __global__ void __launch_bounds__(kRigidThreads) k_rigid_pre(int64_t n, RigidState s, const RigidParams* __restrict__ P,
-                                                             double dt, double vcorr, double Dcorr) {
+                                                             double dt, double vcorr, double Dcorr, SkinCheck sk) {
 	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	const int c = s.cid[i];
@@ -722,9 +835,16 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pre(int64_t n, RigidSta
 	s.vx[i] = v0;
 	s.vy[i] = v1;
 	s.vz[i] = v2;
-	s.rx[i] = __dadd_rn(s.rx[i], __dmul_rn(dt, v0));
-	s.ry[i] = __dadd_rn(s.ry[i], __dmul_rn(dt, v1));
-	s.rz[i] = __dadd_rn(s.rz[i], __dmul_rn(dt, v2));
+	const double x = __dadd_rn(s.rx[i], __dmul_rn(dt, v0));
+	const double y = __dadd_rn(s.ry[i], __dmul_rn(dt, v1));
+	const double z = __dadd_rn(s.rz[i], __dmul_rn(dt, v2));
+	s.rx[i] = x;
+	s.ry[i] = y;
+	s.rz[i] = z;
+	if (sk.rref) {
+		const double dx = x - sk.rref[i], dy = y - sk.rref[n + i], dz = z - sk.rref[2 * n + i];
+		if (dx * dx + dy * dy + dz * dz > sk.half_skin2) *sk.flag = sk.step;
+	}
 
 	const Quat q = load_q(s.q, n, u);
 	double D[3] = {s.D[u], s.D[n + u], s.D[2 * n + u]};
@@ -837,6 +957,17 @@ struct mdgpu_rigid {
 	unsigned* tickets = nullptr;
 	double* h_scal = nullptr;
 	int64_t cap = 0;
+	// Verlet-skin mode of mdgpu_rigid_run (skin > 0)
+	double skin = 0.0;
+	int list_cap_req = 0;        // entries per molecule asked for (0: from the densest cell)
+	Grid gs{};                   // the skin grid of the loaded positions
+	bool gs_valid = false;
+	uint32_t* list = nullptr;    // list_cap x list_n codes
+	int32_t* list_count = nullptr;
+	double* rref = nullptr;      // 3 x list_n positions of the last build
+	int list_cap = 0;
+	int64_t list_n = 0;
+	bool lists_valid = false;    // the sort order has not changed since the lists were built
 };
 
 namespace {
@@ -849,9 +980,13 @@ Context* ctx_of(mdgpu_rigid* h) { return &h->inner->c; }
 		if (e_ != cudaSuccess) return set_cuda_error(c, e_, #call);        \
 	} while (0)
 
-int launch_rigid_forces(mdgpu_rigid* h) {
+// Forces of the current positions: on the container's cells, or in the skin mode (skin) from the
+// lists on the skin grid.
+int launch_rigid_forces(mdgpu_rigid* h, bool skin = false) {
 	Context* c = ctx_of(h);
 	const int64_t n = c->n;
+	const Grid& grid = skin ? h->gs : c->g;
+	const RigidLists vl{skin ? h->list : nullptr, skin ? h->list_count : nullptr};
 	const unsigned nb = (unsigned) nblocks(n);
 	const unsigned nbp = (unsigned) nblocks(n * kRigidLanes);
 	prof_begin(c, 1);
@@ -864,7 +999,7 @@ int launch_rigid_forces(mdgpu_rigid* h) {
 	for (int k = 0; k < h->hp.nc; k++) charged |= h->hp.nsites[k] > h->hp.nlj[k];
 #define RG_PAIRS_Q(MX, NSV, QV)                                                                               \
 	k_rigid_pairs<MX, NSV, QV><<<nbp, kRigidThreads, 0, c->stream>>>(                                         \
-	    n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->p.uidx, c->cell_start, c->g, h->dp, h->ds, h->dsf, h->es, o)
+	    n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->p.uidx, c->cell_start, grid, h->dp, h->ds, h->dsf, h->es, o, vl)
 #define RG_PAIRS(MX, NSV) \
 	(h->hp.oriented ? RG_PAIRS_Q(MX, NSV, 2) : (charged ? RG_PAIRS_Q(MX, NSV, 1) : RG_PAIRS_Q(MX, NSV, 0)))
 	if (ns <= 1)
@@ -890,11 +1025,69 @@ RigidState state_of(mdgpu_rigid* h) {
 	                  c->p.cid, c->p.uidx, h->q, h->D, h->M};
 }
 
-int launch_rigid_pre(mdgpu_rigid* h, double dt, double vcorr, double Dcorr) {
+int launch_rigid_pre(mdgpu_rigid* h, double dt, double vcorr, double Dcorr, bool skin_check = false) {
 	Context* c = ctx_of(h);
 	prof_begin(c, 2);
-	k_rigid_pre<<<(unsigned) nblocks(c->n), kRigidThreads, 0, c->stream>>>(c->n, state_of(h), h->dp, dt, vcorr, Dcorr);
+	const double hs = 0.5 * h->skin;
+	const SkinCheck sk{skin_check ? h->rref : nullptr, hs * hs, c->rebuild, c->step_id};
+	k_rigid_pre<<<(unsigned) nblocks(c->n), kRigidThreads, 0, c->stream>>>(c->n, state_of(h), h->dp, dt, vcorr, Dcorr,
+	                                                                       sk);
 	prof_end(c, 2, 1);
+	RG_CUDA(cudaGetLastError());
+	return MDGPU_OK;
+}
+
+// Buffers and grid of the skin mode for the loaded molecules.
+int rigid_skin_prepare(mdgpu_rigid* h) {
+	Context* c = ctx_of(h);
+	const int64_t n = c->n;
+	if (!h->gs_valid) {
+		std::string err;
+		Grid gs{};
+		const int st = skin_grid(c, h->skin, gs, err);
+		if (st) return set_error(c, st, "cutoff + skin: " + err);
+		if (gs.ncells > c->g.ncells) return set_error(c, MDGPU_ERR_ARG, "the skin grid has more cells than the box");
+		h->gs = gs;
+		h->gs_valid = true;
+		h->lists_valid = false;
+	}
+	int cap = h->list_cap_req;
+	if (cap <= 0) {
+		// 1.25 x the partners within rc + skin at the densest cell's density, and a margin
+		const double rl = c->rc + h->skin;
+		const double vol = c->g.cell_length[0] * c->g.cell_length[1] * c->g.cell_length[2];
+		const double rho = (c->max_occ > 0 ? c->max_occ : 1) / vol;
+		cap = (int) std::ceil(1.25 * 4.18879020478639 * rl * rl * rl * rho) + 16;
+	}
+	if (h->list_n != n || h->list_cap != cap) {
+		cudaFree(h->list);
+		cudaFree(h->list_count);
+		cudaFree(h->rref);
+		h->list = nullptr;
+		h->list_count = nullptr;
+		h->rref = nullptr;
+		h->list_n = 0;
+		RG_CUDA(cudaMalloc(&h->list, sizeof(uint32_t) * (size_t) cap * n));
+		RG_CUDA(cudaMalloc(&h->list_count, sizeof(int32_t) * n));
+		RG_CUDA(cudaMalloc(&h->rref, sizeof(double) * 3 * n));
+		h->list_n = n;
+		h->list_cap = cap;
+		h->lists_valid = false;
+	}
+	return rebuild_prepare(c);
+}
+
+// The build step's rebinning on the skin grid and list build; both return at once unless the
+// displacement check (or an invalid list) asked for a build in this step.
+int launch_rigid_build(mdgpu_rigid* h) {
+	Context* c = ctx_of(h);
+	RG_CUDA(launch_rebuild(c, h->gs));
+	prof_begin(c, 0);
+	const double rl = c->rc + h->skin;
+	k_rigid_build<<<(unsigned) nblocks(c->n), kRigidThreads, 0, c->stream>>>(
+	    c->n, c->p.rx, c->p.ry, c->p.rz, c->cell_start, h->gs, rl * rl, c->rebuild, c->step_id, h->list_cap, h->list,
+	    h->list_count, h->rref, c->builds);
+	prof_end(c, 0, 1);
 	RG_CUDA(cudaGetLastError());
 	return MDGPU_OK;
 }
@@ -1307,6 +1500,9 @@ int mdgpu_rigid_destroy(mdgpu_rigid* h) {
 	cudaFree(h->scal);
 	cudaFree(h->steps);
 	cudaFree(h->tickets);
+	cudaFree(h->list);
+	cudaFree(h->list_count);
+	cudaFree(h->rref);
 	if (h->h_scal) cudaFreeHost(h->h_scal);
 	int st = h->inner ? mdgpu_destroy(h->inner) : MDGPU_OK;
 	delete h;
@@ -1349,6 +1545,8 @@ int mdgpu_rigid_set_particles(mdgpu_rigid* h, int64_t n, const uint64_t* id, con
 	RG_CUDA(cudaMemsetAsync(h->M, 0, sizeof(double) * 3 * n, c->stream));
 	RG_CUDA(cudaGetLastError());
 	RG_CUDA(cudaStreamSynchronize(c->stream));
+	h->gs_valid = false;   // the skin grid follows the density of the new positions
+	h->lists_valid = false;
 	return MDGPU_OK;
 }
 
@@ -1375,6 +1573,7 @@ int mdgpu_rigid_get_particles(mdgpu_rigid* h, int64_t n, uint64_t* id, int32_t* 
 
 int mdgpu_rigid_update(mdgpu_rigid* h) {
 	if (!h) return MDGPU_ERR_ARG;
+	h->lists_valid = false;   // the sort order changes
 	return mdgpu_update(h->inner);
 }
 
@@ -1403,6 +1602,7 @@ int mdgpu_rigid_leapfrog_pre(mdgpu_rigid* h, double dt, double vcorr, double Dco
 	RG_CUDA(cudaSetDevice(c->device));
 	int st = launch_rigid_pre(h, dt, vcorr, Dcorr);
 	c->cells_valid = false;
+	h->lists_valid = false;   // moved without the displacement check
 	return st;
 }
 
@@ -1434,21 +1634,73 @@ int mdgpu_rigid_run(mdgpu_rigid* h, int32_t nsteps, double dt, double* per_step)
 		RG_CUDA(cudaMalloc(&h->steps, sizeof(double) * 5 * nsteps));
 		h->steps_cap = nsteps;
 	}
+	if (h->skin > 0.0) {
+		int st = rigid_skin_prepare(h);
+		if (st) return st;
+	}
 	for (int32_t k = 0; k < nsteps; k++) {
 		// Simulation::simulateStep: upd_preF, update (wrap, bin), upd_cache + traversePairs, upd_postF
-		int st = launch_rigid_pre(h, dt, 1.0, 1.0);
-		if (st) return st;
-		RG_CUDA(launch_bin(c, true));
-		st = launch_rigid_forces(h);
+		int st;
+		if (h->skin > 0.0) {
+			// the Verlet-skin step: the rebinning and the list build run only when a molecule moved
+			// more than skin/2 since the last build (or the lists do not fit the sort order)
+			c->step_id++;
+			if (!h->lists_valid) {
+				st = request_build(c);
+				if (st) return st;
+				h->lists_valid = true;
+			}
+			st = launch_rigid_pre(h, dt, 1.0, 1.0, true);
+			if (st) return st;
+			st = launch_rigid_build(h);
+			if (st) return st;
+			st = launch_rigid_forces(h, true);
+		} else {
+			st = launch_rigid_pre(h, dt, 1.0, 1.0);
+			if (st) return st;
+			RG_CUDA(launch_bin(c, true));
+			st = launch_rigid_forces(h);
+		}
 		if (st) return st;
 		st = launch_rigid_post(h, 0.5 * dt, h->steps + 5 * (int64_t) k);
 		if (st) return st;
 	}
-	c->cells_valid = true;
+	if (h->skin <= 0.0)
+		c->cells_valid = true;
+	else if (nsteps > 0)
+		c->cells_valid = false;   // the cells are the skin grid's, the positions not wrapped
 	c->lists_valid = false;
 	if (per_step && nsteps > 0)
 		RG_CUDA(cudaMemcpyAsync(per_step, h->steps, sizeof(double) * 5 * nsteps, cudaMemcpyDeviceToHost, c->stream));
 	return check_device_status(c);
+}
+
+int mdgpu_rigid_set_skin(mdgpu_rigid* h, double skin, int32_t list_cap) {
+	if (!h) return MDGPU_ERR_ARG;
+	Context* c = ctx_of(h);
+	if (!(skin >= 0.0)) return set_error(c, MDGPU_ERR_ARG, "skin must not be negative");
+	if (skin > 0.5 * c->rc) return set_error(c, MDGPU_ERR_ARG, "skin must not exceed half the cutoff");
+	if (list_cap < 0 || list_cap > (1 << 16)) return set_error(c, MDGPU_ERR_ARG, "list capacity must be in 0..65536");
+	if (skin != h->skin) {
+		h->gs_valid = false;
+		h->lists_valid = false;
+	}
+	h->skin = skin;
+	h->list_cap_req = list_cap;
+	return MDGPU_OK;
+}
+
+int mdgpu_rigid_skin_builds(mdgpu_rigid* h, int64_t* builds) {
+	if (!h || !builds) return MDGPU_ERR_ARG;
+	Context* c = ctx_of(h);
+	unsigned long long b = 0;
+	if (c->builds) {
+		RG_CUDA(cudaSetDevice(c->device));
+		RG_CUDA(cudaMemcpyAsync(&b, c->builds, sizeof(b), cudaMemcpyDeviceToHost, c->stream));
+		RG_CUDA(cudaStreamSynchronize(c->stream));
+	}
+	*builds = (int64_t) b;
+	return MDGPU_OK;
 }
 
 int mdgpu_rigid_get_stream(const mdgpu_rigid* h, void** stream) {

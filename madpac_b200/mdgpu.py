@@ -111,6 +111,8 @@ SIGNATURES = {
     "mdgpu_rigid_leapfrog_pre": (_I, [_VP, _D, _D, _D]),
     "mdgpu_rigid_leapfrog_post": (_I, [_VP, _D, _VP, _VP]),
     "mdgpu_rigid_run": (_I, [_VP, _I32, _D, _VP]),
+    "mdgpu_rigid_set_skin": (_I, [_VP, _D, _I32]),
+    "mdgpu_rigid_skin_builds": (_I, [_VP, _VP]),
     "mdgpu_rigid_get_stream": (_I, [_VP, _VP]),
     "mdgpu_rigid_profile_enable": (_I, [_VP, _I]),
     "mdgpu_rigid_profile_read": (_I, [_VP, _VP, _VP, _I]),
@@ -538,6 +540,16 @@ class RigidLinkedCells:
         out = np.zeros((nsteps, 5)) if record else None
         self._check(self.lib.mdgpu_rigid_run(self.h, int(nsteps), float(dt), _ptr(out)))
         return out
+
+    def setSkin(self, skin: float, listCap: int = 0) -> None:
+        """Verlet-skin mode of ``run`` (0 turns it off): candidate lists of radius rc + skin, rebuilt
+        when a molecule moved more than skin/2; listCap entries per molecule (0: automatic)."""
+        self._check(self.lib.mdgpu_rigid_set_skin(self.h, float(skin), int(listCap)))
+
+    def skinBuilds(self) -> int:
+        b = ctypes.c_int64()
+        self._check(self.lib.mdgpu_rigid_skin_builds(self.h, ctypes.byref(b)))
+        return b.value
 
     def launches(self) -> int:
         return int(self.profileRead()[1][3])
