@@ -31,7 +31,9 @@ namespace {
 
 constexpr int KK = kMaxSpecies * kMaxSpecies;
 
-template <bool kMixed>
+// NP: the number of species pairs held in registers (ns * ns, 1 or 4), or 0 for any ns up to
+// kMaxSpecies with the per-pair sums in a KK-entry array (local memory).
+template <bool kMixed, int NP>
 __global__ void __launch_bounds__(kReduceBlock) k_adjoint(int64_t n, Particles p, const int32_t* __restrict__ start,
                                                          Grid g, const PairParams* __restrict__ pp, double rclj,
                                                          const double* __restrict__ gfx, const double* __restrict__ gfy,
@@ -51,8 +53,24 @@ __global__ void __launch_bounds__(kReduceBlock) k_adjoint(int64_t n, Particles p
 	// kAdjLanes consecutive lanes per molecule, each taking every kAdjLanes-th candidate of a cell
 	const int64_t i = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) / kAdjLanes;
 	const int sub = threadIdx.x % kAdjLanes;
-	double acc_e[KK], acc_s[KK];
-	for (int k = 0; k < ns * ns; k++) acc_e[k] = acc_s[k] = 0.0;
+	constexpr int NA = NP > 0 ? NP : KK;
+	double acc_e[NA], acc_s[NA];
+#pragma unroll
+	for (int k = 0; k < NA; k++) acc_e[k] = acc_s[k] = 0.0;
+	// adds to the sums of species pair pk (with NP > 0 by selection, so the sums stay in registers)
+	auto add_param = [&](int pk, double ve, double vs) {
+		if constexpr (NP > 0) {
+#pragma unroll
+			for (int k = 0; k < NP; k++)
+				if (k == pk) {
+					acc_e[k] += ve;
+					acc_s[k] += vs;
+				}
+		} else {
+			acc_e[pk] += ve;
+			acc_s[pk] += vs;
+		}
+	};
 	double ax = 0.0, ay = 0.0, az = 0.0;
 	if (i < n) {
 		const double xi = p.rx[i], yi = p.ry[i], zi = p.rz[i];
@@ -126,9 +144,9 @@ __global__ void __launch_bounds__(kReduceBlock) k_adjoint(int64_t n, Particles p
 							ax += (double) (fac * v0 + t * f0 - gUf * fac * f0);
 							ay += (double) (fac * v1 + t * f1 - gUf * fac * f1);
 							az += (double) (fac * v2 + t * f2 - gUf * fac * f2);
-							acc_e[pk] += 0.5 * ((double) (fac * dw / e24f) + gU * ((double) (s12 - s6) + c6) / 6.0);
-							acc_s[pk] += 0.5 * ((double) (e24f * (12.0f * s12 - 3.0f * s6) * iq / sg2f * dw) +
-							                    gU * e24 * ((double) (6.0f * s12 - 3.0f * s6) + c6s) / (6.0 * sg2));
+							add_param(pk, 0.5 * ((double) (fac * dw / e24f) + gU * ((double) (s12 - s6) + c6) / 6.0),
+							          0.5 * ((double) (e24f * (12.0f * s12 - 3.0f * s6) * iq / sg2f * dw) +
+							                 gU * e24 * ((double) (6.0f * s12 - 3.0f * s6) + c6s) / (6.0 * sg2)));
 						} else {
 							const double iq = 1.0 / q;
 							double s6 = sg2 * iq;
@@ -142,9 +160,9 @@ __global__ void __launch_bounds__(kReduceBlock) k_adjoint(int64_t n, Particles p
 							ay += fac * w1 + 2.0 * dfac * dw * d1 - gU * fac * d1;
 							az += fac * w2 + 2.0 * dfac * dw * d2 - gU * fac * d2;
 							// parameter terms (half: the pair is seen from both sides)
-							acc_e[pk] += 0.5 * (fac * dw / e24 + gU * (s12 - s6 + c6) / 6.0);
-							acc_s[pk] += 0.5 * (e24 * (12.0 * s12 - 3.0 * s6) * iq / sg2 * dw +
-							                    gU * e24 * (6.0 * s12 - 3.0 * s6 + c6s) / (6.0 * sg2));
+							add_param(pk, 0.5 * (fac * dw / e24 + gU * (s12 - s6 + c6) / 6.0),
+							          0.5 * (e24 * (12.0 * s12 - 3.0 * s6) * iq / sg2 * dw +
+							                 gU * e24 * (6.0 * s12 - 3.0 * s6 + c6s) / (6.0 * sg2)));
 						}
 					}
 				}
@@ -165,13 +183,17 @@ __global__ void __launch_bounds__(kReduceBlock) k_adjoint(int64_t n, Particles p
 	// block sum of the per-type parameter terms in a fixed order (warp sums, then warp by warp),
 	// then one partial row per block
 	const int warp = threadIdx.x >> 5;
-	for (int k = 0; k < KK; k++) {
-		const double ve = k < ns * ns ? warp_sum(acc_e[k]) : 0.0, vs = k < ns * ns ? warp_sum(acc_s[k]) : 0.0;
+#pragma unroll
+	for (int k = 0; k < NA; k++) {
+		if (NP == 0 && k >= ns * ns) break;   // warp-uniform
+		const double ve = warp_sum(acc_e[k]), vs = warp_sum(acc_s[k]);
 		if ((threadIdx.x & 31) == 0) {
 			s_acc[warp][k] = ve;
 			s_acc[warp][KK + k] = vs;
 		}
 	}
+	if ((threadIdx.x & 31) == 0)
+		for (int k = ns * ns; k < KK; k++) s_acc[warp][k] = s_acc[warp][KK + k] = 0.0;
 	__syncthreads();
 	for (int k = threadIdx.x; k < 2 * KK; k += blockDim.x) {
 		double v = 0.0;
@@ -180,14 +202,24 @@ __global__ void __launch_bounds__(kReduceBlock) k_adjoint(int64_t n, Particles p
 	}
 }
 
-// Sum of the blocks' rows in block order, into out (added to it with `accumulate`).
-__global__ void k_adjoint_params(int64_t nblocks, const double* __restrict__ pgrad, double* __restrict__ out,
-                                 bool accumulate) {
-	const int k = threadIdx.x;
-	if (k >= 2 * KK) return;
+// Sum of the blocks' rows into out (added to it with `accumulate`), in a fixed order: one block of
+// kParamGroups x 2 KK threads; group q sums rows q, q + kParamGroups, ... (each load of a group is
+// one contiguous row), then the groups' sums are added in group order.
+constexpr int kParamGroups = 8;
+__global__ void __launch_bounds__(kParamGroups * 2 * KK) k_adjoint_params(int64_t nblocks,
+                                                                          const double* __restrict__ pgrad,
+                                                                          double* __restrict__ out, bool accumulate) {
+	__shared__ double s_part[kParamGroups][2 * KK];
+	const int k = threadIdx.x % (2 * KK), q = threadIdx.x / (2 * KK);
 	double s = 0.0;
-	for (int64_t b = 0; b < nblocks; b++) s += pgrad[b * 2 * KK + k];
-	out[k] = accumulate ? out[k] + s : s;
+	for (int64_t b = q; b < nblocks; b += kParamGroups) s += pgrad[b * 2 * KK + k];
+	s_part[q][k] = s;
+	__syncthreads();
+	if (q == 0) {
+		double t = s_part[0][k];
+		for (int g = 1; g < kParamGroups; g++) t += s_part[g][k];
+		out[k] = accumulate ? out[k] + t : t;
+	}
 }
 
 }  // namespace
@@ -195,13 +227,19 @@ __global__ void k_adjoint_params(int64_t nblocks, const double* __restrict__ pgr
 cudaError_t launch_adjoint(Context* c, const double* gfx, const double* gfy, const double* gfz, double gU, double* ox,
                            double* oy, double* oz, double* pgrad, double* pout, bool accumulate) {
 	const int64_t nb = adjoint_blocks(c->n);
-	if (c->precision == MDGPU_MIXED)
-		k_adjoint<true><<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(c->n, c->p, c->cell_start, c->g, c->d_pp,
-		                                                                c->rc_lj, gfx, gfy, gfz, gU, ox, oy, oz, pgrad);
+	const int np = c->sp.n * c->sp.n;
+#define MD_ADJ(MX, NPV)                                                                                           \
+	k_adjoint<MX, NPV><<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(c->n, c->p, c->cell_start, c->g, c->d_pp,   \
+	                                                                   c->rc_lj, gfx, gfy, gfz, gU, ox, oy, oz, pgrad)
+	const bool mixed = c->precision == MDGPU_MIXED;
+	if (np == 1)
+		mixed ? MD_ADJ(true, 1) : MD_ADJ(false, 1);
+	else if (np == 4)
+		mixed ? MD_ADJ(true, 4) : MD_ADJ(false, 4);
 	else
-		k_adjoint<false><<<(unsigned) nb, kReduceBlock, 0, c->stream>>>(c->n, c->p, c->cell_start, c->g, c->d_pp,
-		                                                                 c->rc_lj, gfx, gfy, gfz, gU, ox, oy, oz, pgrad);
-	k_adjoint_params<<<1, 2 * KK, 0, c->stream>>>(nb, pgrad, pout, accumulate);
+		mixed ? MD_ADJ(true, 0) : MD_ADJ(false, 0);
+#undef MD_ADJ
+	k_adjoint_params<<<1, kParamGroups * 2 * KK, 0, c->stream>>>(nb, pgrad, pout, accumulate);
 	count_launches(c, 2);
 	return cudaGetLastError();
 }
