@@ -449,6 +449,7 @@ __global__ void __launch_bounds__(kRebuildThreads, 4) k_rebuild(RebuildArgs a) {
 		a.p.cid[to] = ci;
 		a.p.uidx[to] = ui;
 		a.cell[to] = sl.x;
+		a.perm[to] = sl.w;   // the slot's molecule before the rebuild, for state kept beside p
 	}
 }
 

@@ -148,7 +148,8 @@ struct Context {
 // Each returns cudaSuccess or the launch error; kernels report data errors in ctx->status.
 cudaError_t launch_bin(Context* c, bool permute_forces);
 // Verlet-skin mode: wrap, binning on grid g and sort in one cooperative launch that returns at
-// once unless *c->rebuild == c->step_id; the sorted arrays end in c->p (buffer roles unchanged).
+// once unless *c->rebuild == c->step_id; the sorted arrays end in c->p (buffer roles unchanged)
+// and c->perm[i] holds the index before the sort of the molecule now at i.
 cudaError_t launch_rebuild(Context* c, const Grid& g);
 cudaError_t launch_pairs(Context* c);                 // partials -> scalars[0..2] (U6sum, W, npairs)
 // The same in the Verlet-skin mode; with kick_mode 1 or 2 the kernels also apply the closing kick

@@ -157,17 +157,32 @@ __device__ __forceinline__ void store_q(double* q, int64_t n, int64_t u, const Q
 // ---- kernels ------------------------------------------------------------------------------------
 
 // Molecule::upd_cache: the centres' space-frame offsets of every (sorted) molecule
+// The mixed form of molecules with at most two LJ centres and no point polarities reads each
+// partner from one 64-byte record (4 float4: x, y, z as doubles, the two centre offsets as floats,
+// the component id), so a partner costs two or four 16-byte loads from one or two sectors instead
+// of loads from ten separate arrays.
+constexpr int kRecFloat4 = 4;
+__device__ __forceinline__ float lo_f(double x) { return __int_as_float(__double2loint(x)); }
+__device__ __forceinline__ float hi_f(double x) { return __int_as_float(__double2hiint(x)); }
+__device__ __forceinline__ double dbl_of(float lo, float hi) {
+	return __hiloint2double(__float_as_int(hi), __float_as_int(lo));
+}
+
 __global__ void __launch_bounds__(kRigidThreads) k_rigid_sites(int64_t n, const int32_t* __restrict__ uidx,
                                                                const int32_t* __restrict__ cid,
                                                                const double* __restrict__ q,
                                                                const RigidParams* __restrict__ P,
                                                                double* __restrict__ ds, float* __restrict__ dsf,
-                                                               double* __restrict__ es) {
+                                                               double* __restrict__ es, const double* __restrict__ rx,
+                                                               const double* __restrict__ ry,
+                                                               const double* __restrict__ rz,
+                                                               float4* __restrict__ rec) {
 	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
-	const Quat qi = load_q(q, n, uidx[i]);
+	const Quat qi = load_q(q, n, uidx ? uidx[i] : i);   // caller order, or sorted with no map
 	const int c = cid[i];
 	const int ns = P->nsites[c], b = P->base[c];
+	float df[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 	for (int s = 0; s < P->ns_max; s++) {
 		double d[3] = {0.0, 0.0, 0.0}, e[3] = {0.0, 0.0, 0.0};
 		if (s < ns) {
@@ -179,7 +194,16 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_sites(int64_t n, const 
 			ds[(int64_t) (s * 3 + k) * n + i] = d[k];
 			if (dsf) dsf[(int64_t) (s * 3 + k) * n + i] = (float) d[k];
 			if (es) es[(int64_t) (s * 3 + k) * n + i] = e[k];
+			if (s < 2) df[3 * s + k] = (float) d[k];
 		}
+	}
+	if (rec) {
+		const double x = rx[i], y = ry[i], z = rz[i];
+		float4* r = rec + (int64_t) kRecFloat4 * i;
+		r[0] = make_float4(lo_f(x), hi_f(x), lo_f(y), hi_f(y));
+		r[1] = make_float4(lo_f(z), hi_f(z), df[0], df[1]);
+		r[2] = make_float4(df[2], df[3], df[4], df[5]);
+		r[3] = make_float4(__int_as_float(c), 0.f, 0.f, 0.f);
 	}
 }
 
@@ -324,6 +348,11 @@ struct RigidOut {
 #ifndef MDGPU_RIGID_LIST
 #define MDGPU_RIGID_LIST 32
 #endif
+#ifndef MDGPU_RIGID_DIRECT
+#define MDGPU_RIGID_DIRECT 0
+#endif
+// list entries evaluated as they are accepted instead of through the lane's shared-memory list
+constexpr bool kDirect = MDGPU_RIGID_DIRECT != 0;
 constexpr int kRigidLanes = MDGPU_RIGID_LANES;
 constexpr int kRigidList = MDGPU_RIGID_LIST;
 static_assert(kRigidLanes == 1 || kRigidLanes == 2 || kRigidLanes == 4 || kRigidLanes == 8, "lanes per molecule");
@@ -351,8 +380,11 @@ struct RigidLists {
 	const int32_t* count;    // per molecule; -1: overflowed at the build
 };
 
+// The mixed two-centre LJ variant (the records') is held to three CTAs per SM (85 registers, a few
+// spilled): 1.19 against 1.45 ms per step at two CTAs on the 1 M two-centre fluid.
 template <bool kMixed, int NS, int kQ>
-__global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const double* __restrict__ rx,
+__global__ void __launch_bounds__(kRigidThreads, (kMixed && NS <= 2 && kQ == 0) ? 3 : 1)
+    k_rigid_pairs(int64_t n, const double* __restrict__ rx,
                                                                const double* __restrict__ ry,
                                                                const double* __restrict__ rz,
                                                                const int32_t* __restrict__ cid,
@@ -362,7 +394,9 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
                                                                const double* __restrict__ ds,
                                                                const float* __restrict__ dsf,
                                                                const double* __restrict__ es, RigidOut o,
-                                                               RigidLists vl) {
+                                                               RigidLists vl, const float4* __restrict__ rec) {
+	// partners from the 64-byte records (filled by k_rigid_sites for these variants)
+	constexpr bool kRec = kMixed && NS <= 2 && kQ == 0;
 	constexpr int TT = kMaxSiteTotal * kMaxSiteTotal;
 	__shared__ double s_e24[TT], s_sig2[TT], s_sh6[TT];
 	__shared__ int s_ns[kMaxSpecies], s_nlj[kMaxSpecies], s_base[kMaxSpecies];
@@ -429,21 +463,42 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 
 		// the molecule pairs of the list: every LJ centre pair of each (within rcLJ) and every charge
 		// pair (PotForce2Charge, potforce.h:244-253)
-		auto evaluate = [&]() {
-			for (int e = 0; e < cnt; e++) {
-				const uint32_t code = list[e * kRigidThreads];
+		// one accepted molecule pair (code j << 5 | image)
+		auto eval_pair = [&](uint32_t code) {
+			{
 				const int j = (int) (code >> 5);
 				const int img = (int) (code & 31u);
 				const double sx = (double) (img % 3 - 1) * g.L[0];
 				const double sy = (double) ((img / 3) % 3 - 1) * g.L[1];
 				const double sz = (double) (img / 9 - 1) * g.L[2];
-				const double m0 = __dsub_rn(xi, __dadd_rn(rx[j], sx));
-				const double m1 = __dsub_rn(yi, __dadd_rn(ry[j], sy));
-				const double m2 = __dsub_rn(zi, __dadd_rn(rz[j], sz));
+				double xj, yj, zj;
+				int cj;
+				float djr[2][3];
+				if constexpr (kRec) {
+					const float4* r4 = rec + (int64_t) kRecFloat4 * j;
+					const float4 A = r4[0], B = r4[1], C = r4[2], D = r4[3];
+					xj = dbl_of(A.x, A.y);
+					yj = dbl_of(A.z, A.w);
+					zj = dbl_of(B.x, B.y);
+					djr[0][0] = B.z;
+					djr[0][1] = B.w;
+					djr[0][2] = C.x;
+					djr[1][0] = C.y;
+					djr[1][1] = C.z;
+					djr[1][2] = C.w;
+					cj = __float_as_int(D.x);
+				} else {
+					xj = rx[j];
+					yj = ry[j];
+					zj = rz[j];
+					cj = cid[j];
+				}
+				const double m0 = __dsub_rn(xi, __dadd_rn(xj, sx));
+				const double m1 = __dsub_rn(yi, __dadd_rn(yj, sy));
+				const double m2 = __dsub_rn(zi, __dadd_rn(zj, sz));
 				// without charges the list holds only partners within rcLJ
 				const bool lj =
 				    !kQ || __dadd_rn(__dadd_rn(__dmul_rn(m0, m0), __dmul_rn(m1, m1)), __dmul_rn(m2, m2)) < rclj2;
-				const int cj = cid[j];
 				const int nsj = s_ns[cj], nljj = s_nlj[cj], bj = s_base[cj];
 				double fp0 = 0.0, fp1 = 0.0, fp2 = 0.0;   // force of this molecule pair
 				if constexpr (!kMixed) {
@@ -503,9 +558,16 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 						if (sj >= nsj) break;
 						const bool lj_j = !kQ || sj < nljj;
 						if (lj_j && !lj) continue;
-						const float dj0 = dsf[(int64_t) (sj * 3 + 0) * n + j];
-						const float dj1 = dsf[(int64_t) (sj * 3 + 1) * n + j];
-						const float dj2 = dsf[(int64_t) (sj * 3 + 2) * n + j];
+						float dj0, dj1, dj2;
+						if constexpr (kRec) {
+							dj0 = djr[sj][0];
+							dj1 = djr[sj][1];
+							dj2 = djr[sj][2];
+						} else {
+							dj0 = dsf[(int64_t) (sj * 3 + 0) * n + j];
+							dj1 = dsf[(int64_t) (sj * 3 + 1) * n + j];
+							dj2 = dsf[(int64_t) (sj * 3 + 2) * n + j];
+						}
 #pragma unroll
 						for (int si = 0; si < NS; si++) {
 							if (si >= nsi) break;
@@ -589,22 +651,42 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 				// Virial += drm . f over the molecule pair's site pairs
 				W = __dadd_rn(W, __dadd_rn(__dadd_rn(__dmul_rn(m0, fp0), __dmul_rn(m1, fp1)), __dmul_rn(m2, fp2)));
 			}
+		};
+		auto evaluate = [&]() {
+			for (int e = 0; e < cnt; e++) eval_pair(list[e * kRigidThreads]);
 			cnt = 0;
 		};
 
 		// candidate j in image img (shift sx, sy, sz): the exact cutoff test of the reference; the
 		// accepted ones go to the lane's list
 		auto consider = [&](int j, uint32_t img, double sx, double sy, double sz) {
+			double xj, yj, zj;
+			if constexpr (kRec) {
+				const float4* r4 = rec + (int64_t) kRecFloat4 * j;
+				const float4 A = r4[0], B = r4[1];
+				xj = dbl_of(A.x, A.y);
+				yj = dbl_of(A.z, A.w);
+				zj = dbl_of(B.x, B.y);
+			} else {
+				xj = rx[j];
+				yj = ry[j];
+				zj = rz[j];
+			}
 			// the halo image of j (DomainDecompDummy.cpp:64-70, 93-99); adding 0 is exact
-			const double m0 = __dsub_rn(xi, __dadd_rn(rx[j], sx));
-			const double m1 = __dsub_rn(yi, __dadd_rn(ry[j], sy));
-			const double m2 = __dsub_rn(zi, __dadd_rn(rz[j], sz));
+			const double m0 = __dsub_rn(xi, __dadd_rn(xj, sx));
+			const double m1 = __dsub_rn(yi, __dadd_rn(yj, sy));
+			const double m2 = __dsub_rn(zi, __dadd_rn(zj, sz));
 			const double dd = __dadd_rn(__dadd_rn(__dmul_rn(m0, m0), __dmul_rn(m1, m1)), __dmul_rn(m2, m2));
 			if (!(dd < rc2)) return;
 			np += 1.0;
 			if (dd == 0.0) same = true;
 			if (!kQ && !(dd < rclj2)) return;
-			list[cnt * kRigidThreads] = ((uint32_t) j << 5) | img;
+			const uint32_t code = ((uint32_t) j << 5) | img;
+			if (kDirect && vl.list) {
+				eval_pair(code);   // from a list: evaluated at once
+				return;
+			}
+			list[cnt * kRigidThreads] = code;
 			if (++cnt == kRigidList) evaluate();
 		};
 		const int32_t nlist = vl.list ? vl.count[i] : -1;
@@ -710,7 +792,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 		o.fx[i] = F[0];
 		o.fy[i] = F[1];
 		o.fz[i] = F[2];
-		const int64_t u = uidx[i];
+		const int64_t u = uidx ? uidx[i] : i;
 		o.M[u] = Mt[0];
 		o.M[n + u] = Mt[1];
 		o.M[2 * n + u] = Mt[2];
@@ -728,18 +810,11 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pairs(int64_t n, const 
 // pair kernel with the larger radius) as codes j << 5 | image in the scan order of the pair
 // kernel, column k of molecule i at k * n + i; count -1 when more than cap were found (the pair
 // kernel then scans the cells); the positions of the build for the displacement check.
-__global__ void __launch_bounds__(kRigidThreads) k_rigid_build(int64_t n, const double* __restrict__ rx,
-                                                               const double* __restrict__ ry,
-                                                               const double* __restrict__ rz,
-                                                               const int32_t* __restrict__ start, Grid g, double rl2,
-                                                               const int* flag, int step, int cap,
-                                                               uint32_t* __restrict__ list, int32_t* __restrict__ count,
-                                                               double* __restrict__ rref,
-                                                               unsigned long long* builds) {
-	if (*flag != step) return;
-	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
-	if (i == 0) atomicAdd(builds, 1ull);
-	if (i >= n) return;
+__device__ __forceinline__ void rigid_build_one(int64_t i, int64_t n, const double* __restrict__ rx,
+                                                const double* __restrict__ ry, const double* __restrict__ rz,
+                                                const int32_t* __restrict__ start, const Grid& g, double rl2, int cap,
+                                                uint32_t* __restrict__ list, int32_t* __restrict__ count,
+                                                double* __restrict__ rref) {
 	const double xi = rx[i], yi = ry[i], zi = rz[i];
 	rref[i] = xi;
 	rref[n + i] = yi;
@@ -801,6 +876,21 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_build(int64_t n, const 
 	count[i] = cnt <= cap ? cnt : -1;
 }
 
+// (one thread per molecule; the loop covers any grid)
+__global__ void __launch_bounds__(kRigidThreads) k_rigid_build(int64_t n, const double* __restrict__ rx,
+                                                               const double* __restrict__ ry,
+                                                               const double* __restrict__ rz,
+                                                               const int32_t* __restrict__ start, Grid g, double rl2,
+                                                               const int* flag, int step, int cap,
+                                                               uint32_t* __restrict__ list, int32_t* __restrict__ count,
+                                                               double* __restrict__ rref,
+                                                               unsigned long long* builds) {
+	if (*flag != step) return;
+	if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(builds, 1ull);
+	for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+		rigid_build_one(i, n, rx, ry, rz, start, g, rl2, cap, list, count, rref);
+}
+
 struct RigidState {
 	double *rx, *ry, *rz, *vx, *vy, *vz;
 	const double *fx, *fy, *fz;
@@ -826,7 +916,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_pre(int64_t n, RigidSta
 	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	const int c = s.cid[i];
-	const int64_t u = s.uidx[i];
+	const int64_t u = s.uidx ? s.uidx[i] : i;
 	const double dt_halve = __dmul_rn(.5, dt);
 	const double dtInv2m = __ddiv_rn(dt_halve, P->mass[c]);
 	double v0 = __dadd_rn(__dmul_rn(vcorr, s.vx[i]), __dmul_rn(dtInv2m, s.fx[i]));
@@ -876,7 +966,7 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_post(int64_t n, RigidSt
 	double mv2 = 0.0, iw2 = 0.0;
 	if (i < n) {
 		const int c = s.cid[i];
-		const int64_t u = s.uidx[i];
+		const int64_t u = s.uidx ? s.uidx[i] : i;
 		const double m = P->mass[c];
 		const double dtInv2m = __ddiv_rn(dt_half, m);
 		const double v0 = __dadd_rn(s.vx[i], __dmul_rn(dtInv2m, s.fx[i]));
@@ -928,6 +1018,45 @@ __global__ void k_scatter_soa(int64_t n, int k, const T* __restrict__ src, T* __
 	dst[d * n + i] = src[t];
 }
 
+// The skin mode keeps q, D and M in the sorted order of the particle arrays (kRigidPlanes planes of
+// n doubles: q 4, D 3, M 3), so that the per-step kernels read them coalesced; the caller's order
+// (index uidx of the sorted arrays) is restored when a run ends.
+constexpr int kRigidPlanes = 10;
+
+// caller order -> sorted order (to_sorted) or back, plane by plane, for the k planes at src / dst
+__global__ void k_state_map(int64_t n, int k, const int32_t* __restrict__ uidx, const double* __restrict__ src,
+                            double* __restrict__ dst, bool to_sorted) {
+	const int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= n * k) return;
+	const int64_t d = t / n, i = t % n, u = uidx[i];
+	if (to_sorted)
+		dst[d * n + i] = src[d * n + u];
+	else
+		dst[d * n + u] = src[d * n + i];
+}
+
+// The rebuild's new order for the sorted state: into tmp by perm, then back (both only in a step
+// whose build ran).
+// (grid-stride over a small grid: in the steps without a build they return at once, and a launch
+// of a few blocks costs little then)
+__global__ void k_state_permute(int64_t n, const int* flag, int step, const int32_t* __restrict__ perm,
+                                const double* __restrict__ s, double* __restrict__ tmp) {
+	if (*flag != step) return;
+	for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < n * kRigidPlanes;
+	     t += (int64_t) gridDim.x * blockDim.x) {
+		const int64_t d = t / n, i = t % n;
+		tmp[d * n + i] = s[d * n + perm[i]];
+	}
+}
+
+__global__ void k_state_copy(int64_t n, const int* flag, int step, const double* __restrict__ tmp,
+                             double* __restrict__ s) {
+	if (*flag != step) return;
+	for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < n * kRigidPlanes;
+	     t += (int64_t) gridDim.x * blockDim.x)
+		s[t] = tmp[t];
+}
+
 }  // namespace
 }  // namespace mdgpu
 
@@ -943,6 +1072,8 @@ struct mdgpu_rigid {
 	double* ds = nullptr;       // 3 x ns_max x cap, sorted order
 	float* dsf = nullptr;       // the same in float (mixed form)
 	double* es = nullptr;       // rotated orientations of dipoles and quadrupoles, as ds
+	float4* rec = nullptr;      // 64-byte partner records of the mixed two-centre variants, sorted order
+	double* ss = nullptr;       // the skin mode's q, D, M in sorted order (kRigidPlanes x cap), then as much scratch
 	// the components as given (mdgpu_rigid_set_polarities rebuilds the site tables from them)
 	int ncomp = 0;
 	std::vector<int32_t> nlj_in, nq_in;
@@ -991,15 +1122,20 @@ int launch_rigid_forces(mdgpu_rigid* h, bool skin = false) {
 	const unsigned nbp = (unsigned) nblocks(n * kRigidLanes);
 	prof_begin(c, 1);
 	const bool mixed = c->precision == MDGPU_MIXED;
-	k_rigid_sites<<<nb, kRigidThreads, 0, c->stream>>>(n, c->p.uidx, c->p.cid, h->q, h->dp, h->ds,
-	                                                   mixed ? h->dsf : nullptr, h->hp.oriented ? h->es : nullptr);
-	RigidOut o{c->p.fx, c->p.fy, c->p.fz, h->M, h->partials, h->tickets, h->scal, c->status};
 	const int ns = h->hp.ns_max;
 	bool charged = false;   // any point polarity: the kernel variant with the polarity blocks
 	for (int k = 0; k < h->hp.nc; k++) charged |= h->hp.nsites[k] > h->hp.nlj[k];
+	const bool records = mixed && ns <= 2 && !charged && !h->hp.oriented;
+	const int32_t* qmap = skin ? nullptr : c->p.uidx;   // the skin mode's q and M are in sorted order
+	double* const qsrc = skin ? h->ss : h->q;
+	double* const Mdst = skin ? h->ss + 7 * n : h->M;
+	k_rigid_sites<<<nb, kRigidThreads, 0, c->stream>>>(n, qmap, c->p.cid, qsrc, h->dp, h->ds,
+	                                                   mixed ? h->dsf : nullptr, h->hp.oriented ? h->es : nullptr,
+	                                                   c->p.rx, c->p.ry, c->p.rz, records ? h->rec : nullptr);
+	RigidOut o{c->p.fx, c->p.fy, c->p.fz, Mdst, h->partials, h->tickets, h->scal, c->status};
 #define RG_PAIRS_Q(MX, NSV, QV)                                                                               \
 	k_rigid_pairs<MX, NSV, QV><<<nbp, kRigidThreads, 0, c->stream>>>(                                         \
-	    n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, c->p.uidx, c->cell_start, grid, h->dp, h->ds, h->dsf, h->es, o, vl)
+	    n, c->p.rx, c->p.ry, c->p.rz, c->p.cid, qmap, c->cell_start, grid, h->dp, h->ds, h->dsf, h->es, o, vl, h->rec)
 #define RG_PAIRS(MX, NSV) \
 	(h->hp.oriented ? RG_PAIRS_Q(MX, NSV, 2) : (charged ? RG_PAIRS_Q(MX, NSV, 1) : RG_PAIRS_Q(MX, NSV, 0)))
 	if (ns <= 1)
@@ -1019,10 +1155,35 @@ int launch_rigid_forces(mdgpu_rigid* h, bool skin = false) {
 	return MDGPU_OK;
 }
 
-RigidState state_of(mdgpu_rigid* h) {
+// The kernels' view of the state: q, D, M in the caller's order (index uidx), or in the skin mode
+// the sorted copies (no index map).
+RigidState state_of(mdgpu_rigid* h, bool skin = false) {
 	Context* c = ctx_of(h);
+	const int64_t n = c->n;
+	if (skin)
+		return RigidState{c->p.rx, c->p.ry, c->p.rz, c->p.vx, c->p.vy, c->p.vz, c->p.fx, c->p.fy, c->p.fz,
+		                  c->p.cid, nullptr, h->ss, h->ss + 4 * n, h->ss + 7 * n};
 	return RigidState{c->p.rx, c->p.ry, c->p.rz, c->p.vx, c->p.vy, c->p.vz, c->p.fx, c->p.fy, c->p.fz,
 	                  c->p.cid, c->p.uidx, h->q, h->D, h->M};
+}
+
+// Copies q, D, M between the caller's order and the sorted copies of the skin mode.
+int rigid_state_map(mdgpu_rigid* h, bool to_sorted) {
+	Context* c = ctx_of(h);
+	const int64_t n = c->n;
+	struct {
+		double* caller;
+		int64_t off;
+		int k;
+	} sets[3] = {{h->q, 0, 4}, {h->D, 4 * n, 3}, {h->M, 7 * n, 3}};
+	for (auto& st : sets) {
+		double* sorted = h->ss + st.off;
+		k_state_map<<<(unsigned) nblocks(n * st.k), kRigidThreads, 0, c->stream>>>(
+		    n, st.k, c->p.uidx, to_sorted ? st.caller : sorted, to_sorted ? sorted : st.caller, to_sorted);
+	}
+	count_launches(c, 3);
+	RG_CUDA(cudaGetLastError());
+	return MDGPU_OK;
 }
 
 int launch_rigid_pre(mdgpu_rigid* h, double dt, double vcorr, double Dcorr, bool skin_check = false) {
@@ -1030,8 +1191,8 @@ int launch_rigid_pre(mdgpu_rigid* h, double dt, double vcorr, double Dcorr, bool
 	prof_begin(c, 2);
 	const double hs = 0.5 * h->skin;
 	const SkinCheck sk{skin_check ? h->rref : nullptr, hs * hs, c->rebuild, c->step_id};
-	k_rigid_pre<<<(unsigned) nblocks(c->n), kRigidThreads, 0, c->stream>>>(c->n, state_of(h), h->dp, dt, vcorr, Dcorr,
-	                                                                       sk);
+	k_rigid_pre<<<(unsigned) nblocks(c->n), kRigidThreads, 0, c->stream>>>(c->n, state_of(h, skin_check), h->dp, dt,
+	                                                                       vcorr, Dcorr, sk);
 	prof_end(c, 2, 1);
 	RG_CUDA(cudaGetLastError());
 	return MDGPU_OK;
@@ -1042,9 +1203,12 @@ int rigid_skin_prepare(mdgpu_rigid* h) {
 	Context* c = ctx_of(h);
 	const int64_t n = c->n;
 	if (!h->gs_valid) {
+		// cells of edge rc + skin: the build scans the 27 cells around each molecule, so unlike the
+		// single-centre bricks it gains nothing from larger cells
 		std::string err;
 		Grid gs{};
-		const int st = skin_grid(c, h->skin, gs, err);
+		const double length[3] = {c->g.L[0], c->g.L[1], c->g.L[2]};
+		const int st = setup_grid(length, c->rc + h->skin, 1.0, gs, err);
 		if (st) return set_error(c, st, "cutoff + skin: " + err);
 		if (gs.ncells > c->g.ncells) return set_error(c, MDGPU_ERR_ARG, "the skin grid has more cells than the box");
 		h->gs = gs;
@@ -1081,22 +1245,28 @@ int rigid_skin_prepare(mdgpu_rigid* h) {
 // displacement check (or an invalid list) asked for a build in this step.
 int launch_rigid_build(mdgpu_rigid* h) {
 	Context* c = ctx_of(h);
+	const int64_t n = c->n;
 	RG_CUDA(launch_rebuild(c, h->gs));
 	prof_begin(c, 0);
+	// the sorted q, D, M follow the rebuild's new order
+	const unsigned nbs = (unsigned) std::min<int64_t>(nblocks(n * kRigidPlanes), 8 * (int64_t) c->num_sms);
+	k_state_permute<<<nbs, kRigidThreads, 0, c->stream>>>(n, c->rebuild, c->step_id, c->perm, h->ss,
+	                                                      h->ss + kRigidPlanes * n);
+	k_state_copy<<<nbs, kRigidThreads, 0, c->stream>>>(n, c->rebuild, c->step_id, h->ss + kRigidPlanes * n, h->ss);
 	const double rl = c->rc + h->skin;
-	k_rigid_build<<<(unsigned) nblocks(c->n), kRigidThreads, 0, c->stream>>>(
+	k_rigid_build<<<(unsigned) nblocks(n), kRigidThreads, 0, c->stream>>>(
 	    c->n, c->p.rx, c->p.ry, c->p.rz, c->cell_start, h->gs, rl * rl, c->rebuild, c->step_id, h->list_cap, h->list,
 	    h->list_count, h->rref, c->builds);
-	prof_end(c, 0, 1);
+	prof_end(c, 0, 3);
 	RG_CUDA(cudaGetLastError());
 	return MDGPU_OK;
 }
 
-int launch_rigid_post(mdgpu_rigid* h, double dt_half, double* record) {
+int launch_rigid_post(mdgpu_rigid* h, double dt_half, double* record, bool skin = false) {
 	Context* c = ctx_of(h);
 	prof_begin(c, 2);
 	k_rigid_post<<<(unsigned) nblocks(c->n), kRigidThreads, 0, c->stream>>>(
-	    c->n, state_of(h), h->dp, dt_half, h->partials, h->tickets + 1, h->scal + 4, h->scal, record, c->status);
+	    c->n, state_of(h, skin), h->dp, dt_half, h->partials, h->tickets + 1, h->scal + 4, h->scal, record, c->status);
 	prof_end(c, 2, 1);
 	RG_CUDA(cudaGetLastError());
 	return MDGPU_OK;
@@ -1246,9 +1416,12 @@ int ensure_capacity(mdgpu_rigid* h, int64_t n) {
 	cudaFree(h->ds);
 	cudaFree(h->dsf);
 	cudaFree(h->es);
+	cudaFree(h->rec);
+	cudaFree(h->ss);
 	cudaFree(h->stage);
 	cudaFree(h->partials);
-	h->q = h->D = h->M = h->ds = h->stage = h->partials = h->es = nullptr;
+	h->q = h->D = h->M = h->ds = h->stage = h->partials = h->es = h->ss = nullptr;
+	h->rec = nullptr;
 	h->dsf = nullptr;
 	h->cap = 0;
 	RG_CUDA(cudaMalloc(&h->q, sizeof(double) * 4 * n));
@@ -1257,6 +1430,8 @@ int ensure_capacity(mdgpu_rigid* h, int64_t n) {
 	RG_CUDA(cudaMalloc(&h->ds, sizeof(double) * 3 * std::max(1, h->hp.ns_max) * n));
 	RG_CUDA(cudaMalloc(&h->dsf, sizeof(float) * 3 * std::max(1, h->hp.ns_max) * n));
 	RG_CUDA(cudaMalloc(&h->es, sizeof(double) * 3 * std::max(1, h->hp.ns_max) * n));
+	RG_CUDA(cudaMalloc(&h->rec, sizeof(float4) * kRecFloat4 * n));
+	RG_CUDA(cudaMalloc(&h->ss, sizeof(double) * 2 * kRigidPlanes * n));
 	RG_CUDA(cudaMalloc(&h->stage, sizeof(double) * 4 * n));
 	RG_CUDA(cudaMalloc(&h->partials, sizeof(double) * 4 * nblocks(n * kRigidLanes)));
 	h->cap = n;
@@ -1495,6 +1670,8 @@ int mdgpu_rigid_destroy(mdgpu_rigid* h) {
 	cudaFree(h->ds);
 	cudaFree(h->dsf);
 	cudaFree(h->es);
+	cudaFree(h->rec);
+	cudaFree(h->ss);
 	cudaFree(h->stage);
 	cudaFree(h->partials);
 	cudaFree(h->scal);
@@ -1634,41 +1811,45 @@ int mdgpu_rigid_run(mdgpu_rigid* h, int32_t nsteps, double dt, double* per_step)
 		RG_CUDA(cudaMalloc(&h->steps, sizeof(double) * 5 * nsteps));
 		h->steps_cap = nsteps;
 	}
-	if (h->skin > 0.0) {
+	if (h->skin > 0.0 && nsteps > 0) {
 		int st = rigid_skin_prepare(h);
+		if (!st) st = rigid_state_map(h, true);
 		if (st) return st;
 	}
-	for (int32_t k = 0; k < nsteps; k++) {
+	int st = MDGPU_OK;
+	for (int32_t k = 0; k < nsteps && !st; k++) {
 		// Simulation::simulateStep: upd_preF, update (wrap, bin), upd_cache + traversePairs, upd_postF
-		int st;
+		double* record = h->steps + 5 * (int64_t) k;
 		if (h->skin > 0.0) {
 			// the Verlet-skin step: the rebinning and the list build run only when a molecule moved
 			// more than skin/2 since the last build (or the lists do not fit the sort order)
 			c->step_id++;
 			if (!h->lists_valid) {
 				st = request_build(c);
-				if (st) return st;
 				h->lists_valid = true;
 			}
-			st = launch_rigid_pre(h, dt, 1.0, 1.0, true);
-			if (st) return st;
-			st = launch_rigid_build(h);
-			if (st) return st;
-			st = launch_rigid_forces(h, true);
+			if (!st) st = launch_rigid_pre(h, dt, 1.0, 1.0, true);
+			if (!st) st = launch_rigid_build(h);
+			if (!st) st = launch_rigid_forces(h, true);
+			if (!st) st = launch_rigid_post(h, 0.5 * dt, record, true);
 		} else {
 			st = launch_rigid_pre(h, dt, 1.0, 1.0);
-			if (st) return st;
-			RG_CUDA(launch_bin(c, true));
-			st = launch_rigid_forces(h);
+			if (!st) {
+				const cudaError_t e = launch_bin(c, true);
+				if (e != cudaSuccess) st = set_cuda_error(c, e, "launch_bin");
+			}
+			if (!st) st = launch_rigid_forces(h);
+			if (!st) st = launch_rigid_post(h, 0.5 * dt, record);
 		}
-		if (st) return st;
-		st = launch_rigid_post(h, 0.5 * dt, h->steps + 5 * (int64_t) k);
-		if (st) return st;
 	}
-	if (h->skin <= 0.0)
+	if (h->skin <= 0.0) {
 		c->cells_valid = true;
-	else if (nsteps > 0)
+	} else if (nsteps > 0) {
 		c->cells_valid = false;   // the cells are the skin grid's, the positions not wrapped
+		const int back = rigid_state_map(h, false);   // q, D, M back in the caller's order
+		if (!st) st = back;
+	}
+	if (st) return st;
 	c->lists_valid = false;
 	if (per_step && nsteps > 0)
 		RG_CUDA(cudaMemcpyAsync(per_step, h->steps, sizeof(double) * 5 * nsteps, cudaMemcpyDeviceToHost, c->stream));
