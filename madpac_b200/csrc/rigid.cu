@@ -415,6 +415,19 @@ __global__ void __launch_bounds__(kRigidThreads, (kMixed && NS <= 2 && kQ == 0) 
 	}
 	if constexpr (kMixed)
 		if (threadIdx.x < kMaxSiteTotal) s_qf[threadIdx.x] = (float) P->charge[threadIdx.x];
+	// the records' variant: the shift6 terms of all centre pairs of a component pair, summed once
+	// (every centre pair of a listed molecule pair is evaluated there: no charges, all within rcLJ)
+	__shared__ double s_shpair[kRec ? kMaxSpecies * kMaxSpecies : 1];
+	if constexpr (kRec)
+		if (threadIdx.x < kMaxSpecies * kMaxSpecies) {
+			const int ca = threadIdx.x / kMaxSpecies, cb = threadIdx.x % kMaxSpecies;
+			double t = 0.0;
+			if (ca < P->nc && cb < P->nc)
+				for (int sa = 0; sa < P->nsites[ca]; sa++)
+					for (int sb = 0; sb < P->nsites[cb]; sb++)
+						t += P->shift6[(P->base[ca] + sa) * kMaxSiteTotal + P->base[cb] + sb];
+			s_shpair[threadIdx.x] = t;
+		}
 	if (threadIdx.x < kMaxSpecies) {
 		s_ns[threadIdx.x] = P->nsites[threadIdx.x];
 		s_nlj[threadIdx.x] = P->nlj[threadIdx.x];
@@ -587,7 +600,7 @@ __global__ void __launch_bounds__(kRigidThreads, (kMixed && NS <= 2 && kQ == 0) 
 								const float qm = q12 - q6;
 								fac = eps24 * (q12 + qm) * inv;
 								uf += eps24 * qm;
-								sh += s_sh6[pk];
+								if constexpr (!kRec) sh += s_sh6[pk];
 							} else {
 								const float u = s_qf[bi + si] * s_qf[bj + sj] * rsqrtf(dr2);
 								uq += u;
@@ -598,17 +611,34 @@ __global__ void __launch_bounds__(kRigidThreads, (kMixed && NS <= 2 && kQ == 0) 
 							fs[si][2] += fac * s2;
 						}
 					}
-					U += (double) uf + sh;
-					UX += (double) uq;
+					if constexpr (kRec) {
+						// the molecule pair's force and its virial term drm . f in float
+						float q0 = 0.f, q1 = 0.f, q2 = 0.f;
 #pragma unroll
-					for (int si = 0; si < NS; si++) {
-						if (si >= nsi) break;
-						Fs[si][0] += (double) fs[si][0];
-						Fs[si][1] += (double) fs[si][1];
-						Fs[si][2] += (double) fs[si][2];
-						fp0 += (double) fs[si][0];
-						fp1 += (double) fs[si][1];
-						fp2 += (double) fs[si][2];
+						for (int si = 0; si < NS; si++) {
+							if (si >= nsi) break;
+							Fs[si][0] += (double) fs[si][0];
+							Fs[si][1] += (double) fs[si][1];
+							Fs[si][2] += (double) fs[si][2];
+							q0 += fs[si][0];
+							q1 += fs[si][1];
+							q2 += fs[si][2];
+						}
+						U += (double) uf + s_shpair[ci * kMaxSpecies + cj];
+						W += (double) (e0 * q0 + e1 * q1 + e2 * q2);
+					} else {
+						U += (double) uf + sh;
+						UX += (double) uq;
+#pragma unroll
+						for (int si = 0; si < NS; si++) {
+							if (si >= nsi) break;
+							Fs[si][0] += (double) fs[si][0];
+							Fs[si][1] += (double) fs[si][1];
+							Fs[si][2] += (double) fs[si][2];
+							fp0 += (double) fs[si][0];
+							fp1 += (double) fs[si][1];
+							fp2 += (double) fs[si][2];
+						}
 					}
 				}
 				if constexpr (oriented) {
@@ -649,7 +679,8 @@ __global__ void __launch_bounds__(kRigidThreads, (kMixed && NS <= 2 && kQ == 0) 
 					}
 				}
 				// Virial += drm . f over the molecule pair's site pairs
-				W = __dadd_rn(W, __dadd_rn(__dadd_rn(__dmul_rn(m0, fp0), __dmul_rn(m1, fp1)), __dmul_rn(m2, fp2)));
+				if constexpr (!kRec)
+					W = __dadd_rn(W, __dadd_rn(__dadd_rn(__dmul_rn(m0, fp0), __dmul_rn(m1, fp1)), __dmul_rn(m2, fp2)));
 			}
 		};
 		auto evaluate = [&]() {
