@@ -275,6 +275,9 @@ struct RebuildArgs {
 	unsigned* bar;
 	int64_t timeout_ns;
 	unsigned* brick_counts;   // sparse/dense brick counts, zeroed for the list build that follows
+	double* xs;               // nx more planes of n doubles sorted with the molecules (may be none)
+	double* xt;               // nx planes of scratch for them
+	int nx;
 };
 
 constexpr int kRebuildThreads = 256;
@@ -419,6 +422,7 @@ __global__ void __launch_bounds__(kRebuildThreads, 4) k_rebuild(RebuildArgs a) {
 		a.q.cid[slot] = ci;
 		a.q.uidx[slot] = ui;
 		a.slot[slot] = make_int4(c, s, e, (int32_t) i);
+		for (int k = 0; k < a.nx; k++) a.xt[(int64_t) k * a.n + slot] = a.xs[(int64_t) k * a.n + i];
 	}
 	for (int64_t c = tid; c < nc; c += nthreads) a.count[c] = 0;
 	if (threadIdx.x == 0) a.look[blockIdx.x] = 0ull;
@@ -450,6 +454,7 @@ __global__ void __launch_bounds__(kRebuildThreads, 4) k_rebuild(RebuildArgs a) {
 		a.p.uidx[to] = ui;
 		a.cell[to] = sl.x;
 		a.perm[to] = sl.w;   // the slot's molecule before the rebuild, for state kept beside p
+		for (int k = 0; k < a.nx; k++) a.xs[(int64_t) k * a.n + to] = a.xt[(int64_t) k * a.n + t];
 	}
 }
 
@@ -487,7 +492,7 @@ cudaError_t launch_bin(Context* c, bool permute_forces) {
 	return e;
 }
 
-cudaError_t launch_rebuild(Context* c, const Grid& g) {
+cudaError_t launch_rebuild(Context* c, const Grid& g, double* extra, double* scratch, int nextra) {
 	// co-resident CTAs per SM of k_rebuild, per device (the occupancy query is a host call of
 	// several microseconds, paid once per device)
 	static std::mutex mu;
@@ -524,6 +529,9 @@ cudaError_t launch_rebuild(Context* c, const Grid& g) {
 	a.bar = c->bar;
 	a.timeout_ns = 2000000000LL;
 	a.brick_counts = c->brick_counts;
+	a.xs = extra;
+	a.xt = scratch;
+	a.nx = extra ? nextra : 0;
 	// one chunk sum per CTA; no more CTAs than the molecules and cells need (a co-resident grid of
 	// the whole device would keep every other stream's kernels waiting, also in steps it is gated off)
 	const int64_t work = std::max<int64_t>(c->n, g.ncells);

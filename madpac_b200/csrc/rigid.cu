@@ -191,8 +191,10 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_sites(int64_t n, const 
 			if (es && P->type[b + s] >= 2) q_rotate_inv(qi, P->e_body[b + s], e);
 		}
 		for (int k = 0; k < 3; k++) {
-			ds[(int64_t) (s * 3 + k) * n + i] = d[k];
-			if (dsf) dsf[(int64_t) (s * 3 + k) * n + i] = (float) d[k];
+			if (!rec) {   // the records' variant reads only the records
+				ds[(int64_t) (s * 3 + k) * n + i] = d[k];
+				if (dsf) dsf[(int64_t) (s * 3 + k) * n + i] = (float) d[k];
+			}
 			if (es) es[(int64_t) (s * 3 + k) * n + i] = e[k];
 			if (s < 2) df[3 * s + k] = (float) d[k];
 		}
@@ -461,16 +463,27 @@ __global__ void __launch_bounds__(kRigidThreads, (kMixed && NS <= 2 && kQ == 0) 
 		nsi = s_ns[ci];
 		const int nlji = s_nlj[ci];
 		const int bi = s_base[ci];
+		if constexpr (kRec) {
+			// the molecule's own centre offsets from its record (the variant writes no ds)
+			const float4* r4 = rec + (int64_t) kRecFloat4 * i;
+			const float4 B = r4[1], C = r4[2];
+			const float o[6] = {B.z, B.w, C.x, C.y, C.z, C.w};
 #pragma unroll
-		for (int s = 0; s < NS; s++)
+			for (int s = 0; s < NS; s++)
 #pragma unroll
-			for (int k = 0; k < 3; k++) {
-				const double v = s < nsi ? ds[(int64_t) (s * 3 + k) * n + i] : 0.0;
-				if constexpr (kMixed)
-					dif[s][k] = (float) v;
-				else
-					di[s][k] = v;
-			}
+				for (int k = 0; k < 3; k++) dif[s][k] = s < nsi ? o[3 * s + k] : 0.f;
+		} else {
+#pragma unroll
+			for (int s = 0; s < NS; s++)
+#pragma unroll
+				for (int k = 0; k < 3; k++) {
+					const double v = s < nsi ? ds[(int64_t) (s * 3 + k) * n + i] : 0.0;
+					if constexpr (kMixed)
+						dif[s][k] = (float) v;
+					else
+						di[s][k] = v;
+				}
+		}
 		uint32_t* list = s_list + threadIdx.x;
 		int cnt = 0;
 
@@ -808,7 +821,9 @@ __global__ void __launch_bounds__(kRigidThreads, (kMixed && NS <= 2 && kQ == 0) 
 			F[1] = __dadd_rn(F[1], Fs[s][1]);
 			F[2] = __dadd_rn(F[2], Fs[s][2]);
 			double d[3];
-			if constexpr (kMixed) {
+			if constexpr (kRec) {
+				for (int k = 0; k < 3; k++) d[k] = (double) dif[s][k];   // the float offsets of the record
+			} else if constexpr (kMixed) {
 				for (int k = 0; k < 3; k++) d[k] = ds[(int64_t) (s * 3 + k) * n + i];
 			} else {
 				d[0] = di[s][0];
@@ -1031,6 +1046,79 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_post(int64_t n, RigidSt
 	}
 }
 
+// The closing kicks of a step (k_rigid_post, its sums and record) and the opening kicks, drift and
+// rotation of the next (k_rigid_pre with vcorr = Dcorr = 1) in one pass over the molecules: the same
+// operations in the same order as the two kernels, the intermediate v, D and w kept in registers.
+__global__ void __launch_bounds__(kRigidThreads) k_rigid_post_pre(int64_t n, RigidState s,
+                                                                  const RigidParams* __restrict__ P, double dt,
+                                                                  double* partials, unsigned* ticket, double* scalars,
+                                                                  const double* pair_scalars, double* record,
+                                                                  int* status, SkinCheck sk) {
+	const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	double mv2 = 0.0, iw2 = 0.0;
+	if (i < n) {
+		const int c = s.cid[i];
+		const int64_t u = s.uidx ? s.uidx[i] : i;
+		const double m = P->mass[c];
+		const double dt_half = __dmul_rn(.5, dt);
+		const double dtInv2m = __ddiv_rn(dt_half, m);
+		const double f0 = s.fx[i], f1 = s.fy[i], f2 = s.fz[i];
+		// Molecule::upd_postF
+		double v0 = __dadd_rn(s.vx[i], __dmul_rn(dtInv2m, f0));
+		double v1 = __dadd_rn(s.vy[i], __dmul_rn(dtInv2m, f1));
+		double v2 = __dadd_rn(s.vz[i], __dmul_rn(dtInv2m, f2));
+		const double vv = __dadd_rn(__dadd_rn(__dmul_rn(v0, v0), __dmul_rn(v1, v1)), __dmul_rn(v2, v2));
+		mv2 = __dmul_rn(m, vv);
+		const double M[3] = {s.M[u], s.M[n + u], s.M[2 * n + u]};
+		double D[3];
+		for (int d = 0; d < 3; d++) D[d] = __dadd_rn(s.D[d * n + u], __dmul_rn(dt_half, M[d]));
+		const Quat q = load_q(s.q, n, u);
+		double w[3];
+		q_rotate(q, D, w);
+		for (int d = 0; d < 3; d++) {
+			w[d] = __dmul_rn(w[d], P->invI[c][d]);
+			iw2 = __dadd_rn(iw2, __dmul_rn(__dmul_rn(P->I[c][d], w[d]), w[d]));
+		}
+		if (!(isfinite(mv2) && isfinite(iw2))) atomicOr(status, kStatusNonFinite);
+		// Molecule::upd_preF of the next step
+		v0 = __dadd_rn(__dmul_rn(1.0, v0), __dmul_rn(dtInv2m, f0));
+		v1 = __dadd_rn(__dmul_rn(1.0, v1), __dmul_rn(dtInv2m, f1));
+		v2 = __dadd_rn(__dmul_rn(1.0, v2), __dmul_rn(dtInv2m, f2));
+		s.vx[i] = v0;
+		s.vy[i] = v1;
+		s.vz[i] = v2;
+		const double x = __dadd_rn(s.rx[i], __dmul_rn(dt, v0));
+		const double y = __dadd_rn(s.ry[i], __dmul_rn(dt, v1));
+		const double z = __dadd_rn(s.rz[i], __dmul_rn(dt, v2));
+		s.rx[i] = x;
+		s.ry[i] = y;
+		s.rz[i] = z;
+		if (sk.rref) {
+			const double dx = x - sk.rref[i], dy = y - sk.rref[n + i], dz = z - sk.rref[2 * n + i];
+			if (dx * dx + dy * dy + dz * dz > sk.half_skin2) *sk.flag = sk.step;
+		}
+		Quat qh = q_add(q_scale(q_differentiate(q, w), dt_half), q);
+		qh = q_scale(qh, __ddiv_rn(1., __dsqrt_rn(q_magnitude2(qh))));
+		for (int d = 0; d < 3; d++) D[d] = __dadd_rn(__dmul_rn(1.0, D[d]), __dmul_rn(dt_half, M[d]));
+		q_rotate(qh, D, w);
+		for (int d = 0; d < 3; d++) w[d] = __dmul_rn(w[d], P->invI[c][d]);
+		Quat qn = q_add(q, q_scale(q_differentiate(qh, w), dt));
+		qn = q_scale(qn, __ddiv_rn(1., __dsqrt_rn(q_magnitude2(qn))));
+		store_q(s.q, n, u, qn);
+		s.D[u] = D[0];
+		s.D[n + u] = D[1];
+		s.D[2 * n + u] = D[2];
+	}
+	block_sum3(mv2, iw2, 0.0, partials);
+	if (last_block_sum(ticket, partials, gridDim.x, 2, scalars) && threadIdx.x == 0 && record) {
+		record[0] = pair_scalars[0] * 0.5 / 6. + pair_scalars[3] * 0.5;
+		record[1] = pair_scalars[1] * 0.5;
+		record[2] = scalars[0];
+		record[3] = scalars[1];
+		record[4] = pair_scalars[2] * 0.5;
+	}
+}
+
 template <typename T>
 __global__ void k_gather_soa(int64_t n, int k, const T* __restrict__ src, T* __restrict__ dst) {
 	// (k, n) component-major -> (n, k) row-major
@@ -1064,28 +1152,6 @@ __global__ void k_state_map(int64_t n, int k, const int32_t* __restrict__ uidx, 
 		dst[d * n + i] = src[d * n + u];
 	else
 		dst[d * n + u] = src[d * n + i];
-}
-
-// The rebuild's new order for the sorted state: into tmp by perm, then back (both only in a step
-// whose build ran).
-// (grid-stride over a small grid: in the steps without a build they return at once, and a launch
-// of a few blocks costs little then)
-__global__ void k_state_permute(int64_t n, const int* flag, int step, const int32_t* __restrict__ perm,
-                                const double* __restrict__ s, double* __restrict__ tmp) {
-	if (*flag != step) return;
-	for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < n * kRigidPlanes;
-	     t += (int64_t) gridDim.x * blockDim.x) {
-		const int64_t d = t / n, i = t % n;
-		tmp[d * n + i] = s[d * n + perm[i]];
-	}
-}
-
-__global__ void k_state_copy(int64_t n, const int* flag, int step, const double* __restrict__ tmp,
-                             double* __restrict__ s) {
-	if (*flag != step) return;
-	for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < n * kRigidPlanes;
-	     t += (int64_t) gridDim.x * blockDim.x)
-		s[t] = tmp[t];
 }
 
 }  // namespace
@@ -1229,6 +1295,19 @@ int launch_rigid_pre(mdgpu_rigid* h, double dt, double vcorr, double Dcorr, bool
 	return MDGPU_OK;
 }
 
+// The closing kicks of the step (record) and the opening kicks and drift of the next, one launch.
+int launch_rigid_post_pre(mdgpu_rigid* h, double dt, double* record, bool skin) {
+	Context* c = ctx_of(h);
+	prof_begin(c, 2);
+	const double hs = 0.5 * h->skin;
+	const SkinCheck sk{skin ? h->rref : nullptr, hs * hs, c->rebuild, c->step_id};
+	k_rigid_post_pre<<<(unsigned) nblocks(c->n), kRigidThreads, 0, c->stream>>>(
+	    c->n, state_of(h, skin), h->dp, dt, h->partials, h->tickets + 1, h->scal + 4, h->scal, record, c->status, sk);
+	prof_end(c, 2, 1);
+	RG_CUDA(cudaGetLastError());
+	return MDGPU_OK;
+}
+
 // Buffers and grid of the skin mode for the loaded molecules.
 int rigid_skin_prepare(mdgpu_rigid* h) {
 	Context* c = ctx_of(h);
@@ -1277,18 +1356,14 @@ int rigid_skin_prepare(mdgpu_rigid* h) {
 int launch_rigid_build(mdgpu_rigid* h) {
 	Context* c = ctx_of(h);
 	const int64_t n = c->n;
-	RG_CUDA(launch_rebuild(c, h->gs));
+	// the sorted q, D, M move with the molecules
+	RG_CUDA(launch_rebuild(c, h->gs, h->ss, h->ss + kRigidPlanes * n, kRigidPlanes));
 	prof_begin(c, 0);
-	// the sorted q, D, M follow the rebuild's new order
-	const unsigned nbs = (unsigned) std::min<int64_t>(nblocks(n * kRigidPlanes), 8 * (int64_t) c->num_sms);
-	k_state_permute<<<nbs, kRigidThreads, 0, c->stream>>>(n, c->rebuild, c->step_id, c->perm, h->ss,
-	                                                      h->ss + kRigidPlanes * n);
-	k_state_copy<<<nbs, kRigidThreads, 0, c->stream>>>(n, c->rebuild, c->step_id, h->ss + kRigidPlanes * n, h->ss);
 	const double rl = c->rc + h->skin;
 	k_rigid_build<<<(unsigned) nblocks(n), kRigidThreads, 0, c->stream>>>(
 	    c->n, c->p.rx, c->p.ry, c->p.rz, c->cell_start, h->gs, rl * rl, c->rebuild, c->step_id, h->list_cap, h->list,
 	    h->list_count, h->rref, c->builds);
-	prof_end(c, 0, 3);
+	prof_end(c, 0, 1);
 	RG_CUDA(cudaGetLastError());
 	return MDGPU_OK;
 }
@@ -1853,16 +1928,24 @@ int mdgpu_rigid_run(mdgpu_rigid* h, int32_t nsteps, double dt, double* per_step)
 		double* record = h->steps + 5 * (int64_t) k;
 		if (h->skin > 0.0) {
 			// the Verlet-skin step: the rebinning and the list build run only when a molecule moved
-			// more than skin/2 since the last build (or the lists do not fit the sort order)
-			c->step_id++;
-			if (!h->lists_valid) {
-				st = request_build(c);
-				h->lists_valid = true;
+			// more than skin/2 since the last build (or the lists do not fit the sort order); the
+			// closing kicks of a step and the opening kicks of the next run as one pass
+			if (k == 0) {
+				c->step_id++;
+				if (!h->lists_valid) {
+					st = request_build(c);
+					h->lists_valid = true;
+				}
+				if (!st) st = launch_rigid_pre(h, dt, 1.0, 1.0, true);
 			}
-			if (!st) st = launch_rigid_pre(h, dt, 1.0, 1.0, true);
 			if (!st) st = launch_rigid_build(h);
 			if (!st) st = launch_rigid_forces(h, true);
-			if (!st) st = launch_rigid_post(h, 0.5 * dt, record, true);
+			if (!st && k + 1 < nsteps) {
+				c->step_id++;   // the next step's displacement check asks for its build
+				st = launch_rigid_post_pre(h, dt, record, true);
+			} else if (!st) {
+				st = launch_rigid_post(h, 0.5 * dt, record, true);
+			}
 		} else {
 			st = launch_rigid_pre(h, dt, 1.0, 1.0);
 			if (!st) {
