@@ -382,10 +382,12 @@ struct RigidLists {
 	const int32_t* count;    // per molecule; -1: overflowed at the build
 };
 
-// The mixed two-centre LJ variant (the records') is held to three CTAs per SM (85 registers, a few
-// spilled): 1.19 against 1.45 ms per step at two CTAs on the 1 M two-centre fluid.
+// CTAs per SM: the mixed two-centre LJ variant (the records') three (85 registers, a few spilled:
+// 1.19 against 1.45 ms per step at two CTAs on the 1 M two-centre fluid), the others with up to four
+// sites and no dipoles or quadrupoles two (128 registers), the rest one.
 template <bool kMixed, int NS, int kQ>
-__global__ void __launch_bounds__(kRigidThreads, (kMixed && NS <= 2 && kQ == 0) ? 3 : 1)
+__global__ void __launch_bounds__(kRigidThreads,
+                                  (kMixed && NS <= 2 && kQ == 0) ? 3 : ((kQ == 2 || NS > 4) ? 1 : 2))
     k_rigid_pairs(int64_t n, const double* __restrict__ rx,
                                                                const double* __restrict__ ry,
                                                                const double* __restrict__ rz,
