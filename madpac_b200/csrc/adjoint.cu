@@ -30,6 +30,7 @@ namespace mdgpu {
 namespace {
 
 constexpr int KK = kMaxSpecies * kMaxSpecies;
+constexpr int kAdjList = 16;   // accepted partners a lane lists before evaluating them
 
 // NP: the number of species pairs held in registers (ns * ns, 1 or 4), or 0 for any ns up to
 // kMaxSpecies with the per-pair sums in a KK-entry array (local memory).
@@ -42,6 +43,8 @@ __global__ void __launch_bounds__(kReduceBlock) k_adjoint(int64_t n, Particles p
                                                          double* __restrict__ oz, double* __restrict__ pgrad) {
 	__shared__ double s_e24[KK], s_s2[KK], s_sh[KK];
 	__shared__ double s_acc[kReduceBlock / 32][2 * KK];   // per-warp partials of the parameter terms
+	__shared__ int32_t s_aj[kAdjList * kReduceBlock];      // each lane's accepted partners (column per lane)
+	__shared__ uint8_t s_ai[kAdjList * kReduceBlock];      // and their periodic images (27 codes)
 	const int ns = pp->ns;
 	for (int k = threadIdx.x; k < KK; k += blockDim.x) {
 		s_e24[k] = k < ns * ns ? pp->eps24[k] : 0.0;
@@ -82,6 +85,69 @@ __global__ void __launch_bounds__(kReduceBlock) k_adjoint(int64_t n, Particles p
 			int c = (int) floor(__ddiv_rn(__dsub_rn(r[d], g.halo_min[d]), g.cell_length[d])) - 1;
 			cc[d] = c < 0 ? 0 : (c >= g.nc[d] ? g.nc[d] - 1 : c);
 		}
+		// accepted partners are listed per lane and evaluated together, so that the lanes of a warp run
+		// the pair VJP side by side (each lane in the order it accepted them, as it would inline)
+		uint32_t acnt = 0;
+		int32_t* aj = s_aj + threadIdx.x;
+		uint8_t* ai = s_ai + threadIdx.x;
+		auto eval_pair = [&](int j, double sx, double sy, double sz) {
+			const double d0 = xi - (p.rx[j] + sx), d1 = yi - (p.ry[j] + sy), d2 = zi - (p.rz[j] + sz);
+			const double q = d0 * d0 + d1 * d1 + d2 * d2;
+			const int pk = ti * ns + p.cid[j];
+			const double e24 = s_e24[pk], sg2 = s_s2[pk];
+			const double w0 = wix - gfx[j], w1 = wiy - gfy[j], w2 = wiz - gfz[j];
+			const bool shf = s_sh[pk] != 0.0;
+			const double sr6 = sg2 * sg2 * sg2 / rclj6;
+			const double c6 = shf ? sr6 - sr6 * sr6 : 0.0;
+			const double c6s = shf ? 3.0 * sr6 - 6.0 * sr6 * sr6 : 0.0;
+			if (kMixed) {
+				// FP32 from the FP64 difference vector; FP64 sums
+				const float f0 = (float) d0, f1 = (float) d1, f2 = (float) d2;
+				const float qf = fmaf(f0, f0, fmaf(f1, f1, f2 * f2));
+				const float e24f = (float) e24, sg2f = (float) sg2;
+				const float iq = 1.0f / qf;
+				float s6 = sg2f * iq;
+				s6 = s6 * s6 * s6;
+				const float s12 = s6 * s6;
+				const float fac = e24f * (2.0f * s12 - s6) * iq;
+				const float dfac = e24f * (4.0f * s6 - 14.0f * s12) * iq * iq;
+				const float v0 = (float) w0, v1 = (float) w1, v2 = (float) w2;
+				const float dw = fmaf(f0, v0, fmaf(f1, v1, f2 * v2));
+				const float gUf = (float) gU;
+				const float t = 2.0f * dfac * dw;
+				ax += (double) (fac * v0 + t * f0 - gUf * fac * f0);
+				ay += (double) (fac * v1 + t * f1 - gUf * fac * f1);
+				az += (double) (fac * v2 + t * f2 - gUf * fac * f2);
+				add_param(pk, 0.5 * ((double) (fac * dw / e24f) + gU * ((double) (s12 - s6) + c6) / 6.0),
+				          0.5 * ((double) (e24f * (12.0f * s12 - 3.0f * s6) * iq / sg2f * dw) +
+				                 gU * e24 * ((double) (6.0f * s12 - 3.0f * s6) + c6s) / (6.0 * sg2)));
+			} else {
+				const double iq = 1.0 / q;
+				double s6 = sg2 * iq;
+				s6 = s6 * s6 * s6;
+				const double s12 = s6 * s6;
+				const double fac = e24 * (2.0 * s12 - s6) * iq;
+				const double dfac = e24 * (4.0 * s6 - 14.0 * s12) * iq * iq;
+				const double dw = d0 * w0 + d1 * w1 + d2 * w2;
+				// J w - gU f
+				ax += fac * w0 + 2.0 * dfac * dw * d0 - gU * fac * d0;
+				ay += fac * w1 + 2.0 * dfac * dw * d1 - gU * fac * d1;
+				az += fac * w2 + 2.0 * dfac * dw * d2 - gU * fac * d2;
+				// parameter terms (half: the pair is seen from both sides)
+				add_param(pk, 0.5 * (fac * dw / e24 + gU * (s12 - s6 + c6) / 6.0),
+				          0.5 * (e24 * (12.0 * s12 - 3.0 * s6) * iq / sg2 * dw +
+				                 gU * e24 * (6.0 * s12 - 3.0 * s6 + c6s) / (6.0 * sg2)));
+			}
+		};
+		auto flush = [&]() {
+			for (uint32_t e = 0; e < acnt; e++) {
+				const int j = aj[e * kReduceBlock];
+				const int img = ai[e * kReduceBlock];
+				eval_pair(j, (double) (img % 3 - 1) * g.L[0], (double) ((img / 3) % 3 - 1) * g.L[1],
+				          (double) (img / 9 - 1) * g.L[2]);
+			}
+			acnt = 0;
+		};
 		for (int dz = -1; dz <= 1; dz++) {
 			int z = cc[2] + dz;
 			double sz = 0.0;
@@ -114,60 +180,21 @@ __global__ void __launch_bounds__(kReduceBlock) k_adjoint(int64_t n, Particles p
 					}
 					const int nb = (z * g.nc[1] + y) * g.nc[0] + x;
 					const bool shifted = (sx != 0.0) || (sy != 0.0) || (sz != 0.0);
+					const uint8_t img = (uint8_t) ((sx < 0.0 ? 0 : sx > 0.0 ? 2 : 1) + 3 * (sy < 0.0 ? 0 : sy > 0.0 ? 2 : 1) +
+					                               9 * (sz < 0.0 ? 0 : sz > 0.0 ? 2 : 1));
 					for (int j = start[nb] + sub; j < start[nb + 1]; j += kAdjLanes) {
 						if (j == i && !shifted) continue;
 						const double d0 = xi - (p.rx[j] + sx), d1 = yi - (p.ry[j] + sy), d2 = zi - (p.rz[j] + sz);
 						const double q = d0 * d0 + d1 * d1 + d2 * d2;
 						if (!(q < rc2) || !(q < rclj2)) continue;
-						const int pk = ti * ns + p.cid[j];
-						const double e24 = s_e24[pk], sg2 = s_s2[pk];
-						const double w0 = wix - gfx[j], w1 = wiy - gfy[j], w2 = wiz - gfz[j];
-						const bool shf = s_sh[pk] != 0.0;
-						const double sr6 = sg2 * sg2 * sg2 / rclj6;
-						const double c6 = shf ? sr6 - sr6 * sr6 : 0.0;
-						const double c6s = shf ? 3.0 * sr6 - 6.0 * sr6 * sr6 : 0.0;
-						if (kMixed) {
-							// FP32 from the FP64 difference vector; FP64 sums
-							const float f0 = (float) d0, f1 = (float) d1, f2 = (float) d2;
-							const float qf = fmaf(f0, f0, fmaf(f1, f1, f2 * f2));
-							const float e24f = (float) e24, sg2f = (float) sg2;
-							const float iq = 1.0f / qf;
-							float s6 = sg2f * iq;
-							s6 = s6 * s6 * s6;
-							const float s12 = s6 * s6;
-							const float fac = e24f * (2.0f * s12 - s6) * iq;
-							const float dfac = e24f * (4.0f * s6 - 14.0f * s12) * iq * iq;
-							const float v0 = (float) w0, v1 = (float) w1, v2 = (float) w2;
-							const float dw = fmaf(f0, v0, fmaf(f1, v1, f2 * v2));
-							const float gUf = (float) gU;
-							const float t = 2.0f * dfac * dw;
-							ax += (double) (fac * v0 + t * f0 - gUf * fac * f0);
-							ay += (double) (fac * v1 + t * f1 - gUf * fac * f1);
-							az += (double) (fac * v2 + t * f2 - gUf * fac * f2);
-							add_param(pk, 0.5 * ((double) (fac * dw / e24f) + gU * ((double) (s12 - s6) + c6) / 6.0),
-							          0.5 * ((double) (e24f * (12.0f * s12 - 3.0f * s6) * iq / sg2f * dw) +
-							                 gU * e24 * ((double) (6.0f * s12 - 3.0f * s6) + c6s) / (6.0 * sg2)));
-						} else {
-							const double iq = 1.0 / q;
-							double s6 = sg2 * iq;
-							s6 = s6 * s6 * s6;
-							const double s12 = s6 * s6;
-							const double fac = e24 * (2.0 * s12 - s6) * iq;
-							const double dfac = e24 * (4.0 * s6 - 14.0 * s12) * iq * iq;
-							const double dw = d0 * w0 + d1 * w1 + d2 * w2;
-							// J w - gU f
-							ax += fac * w0 + 2.0 * dfac * dw * d0 - gU * fac * d0;
-							ay += fac * w1 + 2.0 * dfac * dw * d1 - gU * fac * d1;
-							az += fac * w2 + 2.0 * dfac * dw * d2 - gU * fac * d2;
-							// parameter terms (half: the pair is seen from both sides)
-							add_param(pk, 0.5 * (fac * dw / e24 + gU * (s12 - s6 + c6) / 6.0),
-							          0.5 * (e24 * (12.0 * s12 - 3.0 * s6) * iq / sg2 * dw +
-							                 gU * e24 * (6.0 * s12 - 3.0 * s6 + c6s) / (6.0 * sg2)));
-						}
+						aj[acnt * kReduceBlock] = j;
+						ai[acnt * kReduceBlock] = img;
+						if (++acnt == kAdjList) flush();
 					}
 				}
 			}
 		}
+		flush();
 	}
 	// the molecule's lanes' sums in a fixed order
 	for (int o = 1; o < kAdjLanes; o <<= 1) {
