@@ -309,7 +309,9 @@ __device__ __forceinline__ unsigned long long load_acquire64(const unsigned long
 __global__ void __launch_bounds__(kRebuildThreads, 4) k_rebuild(RebuildArgs a) {
 	__shared__ int s_flag;
 	__shared__ int32_t s_excl;
-	if (threadIdx.x == 0) s_flag = (*a.flag == a.step && !(*((volatile int*) a.status) & kStatusTimeout)) ? 0 : 1;
+	// (no flag: a build in every launch)
+	if (threadIdx.x == 0)
+		s_flag = ((!a.flag || *a.flag == a.step) && !(*((volatile int*) a.status) & kStatusTimeout)) ? 0 : 1;
 	__syncthreads();
 	if (s_flag) return;   // no build requested for this step
 	if (blockIdx.x == 0 && threadIdx.x < 2 && a.brick_counts) a.brick_counts[threadIdx.x] = 0u;
@@ -492,7 +494,7 @@ cudaError_t launch_bin(Context* c, bool permute_forces) {
 	return e;
 }
 
-cudaError_t launch_rebuild(Context* c, const Grid& g, double* extra, double* scratch, int nextra) {
+cudaError_t launch_rebuild(Context* c, const Grid& g, double* extra, double* scratch, int nextra, bool always) {
 	// co-resident CTAs per SM of k_rebuild, per device (the occupancy query is a host call of
 	// several microseconds, paid once per device)
 	static std::mutex mu;
@@ -524,7 +526,7 @@ cudaError_t launch_rebuild(Context* c, const Grid& g, double* extra, double* scr
 	a.start = c->cell_start;
 	a.look = c->rb_look;
 	a.status = c->status;
-	a.flag = c->rebuild;
+	a.flag = always ? nullptr : c->rebuild;
 	a.step = c->step_id;
 	a.bar = c->bar;
 	a.timeout_ns = 2000000000LL;

@@ -150,9 +150,10 @@ cudaError_t launch_bin(Context* c, bool permute_forces);
 // Verlet-skin mode: wrap, binning on grid g and sort in one cooperative launch that returns at
 // once unless *c->rebuild == c->step_id; the sorted arrays end in c->p (buffer roles unchanged)
 // and c->perm[i] holds the index before the sort of the molecule now at i. `extra` (nextra planes of
-// n doubles, `scratch` as large) are sorted with the molecules.
+// n doubles, `scratch` as large) are sorted with the molecules. With `always` it builds in every
+// launch (the per-step binning of the trajectory adjoint: one launch instead of launch_bin's six).
 cudaError_t launch_rebuild(Context* c, const Grid& g, double* extra = nullptr, double* scratch = nullptr,
-                           int nextra = 0);
+                           int nextra = 0, bool always = false);
 cudaError_t launch_pairs(Context* c);                 // partials -> scalars[0..2] (U6sum, W, npairs)
 // The same in the Verlet-skin mode; with kick_mode 1 or 2 the kernels also apply the closing kick
 // of the step (mode 2, the last step of a run: forces and velocities stored) or the closing kick,

@@ -157,10 +157,14 @@ void free_traj(Context* c) {
 
 namespace {
 
+// The binning of every step: the cooperative rebuild in its always-build form, one launch (the
+// same (cell, id) order as launch_bin's six kernels).
+cudaError_t traj_bin(Context* c) { return launch_rebuild(c, c->g, nullptr, nullptr, 0, true); }
+
 // One reference step (NVE) on the context: pre-kick and drift, binning, forces, closing kick.
 cudaError_t traj_step(Context* c, double dt) {
 	cudaError_t e = launch_leapfrog_pre(c, dt, 1.0);
-	if (e == cudaSuccess) e = launch_bin(c, false);
+	if (e == cudaSuccess) e = traj_bin(c);
 	if (e == cudaSuccess) e = launch_pairs(c);
 	if (e == cudaSuccess) e = launch_leapfrog_post(c, 0.5 * dt);
 	return e;
@@ -221,6 +225,10 @@ int mdgpu_traj_forward(mdgpu_ctx* ctx, int32_t nsteps, int32_t checkpoint_every,
 	if (!(dt > 0.0)) return set_error(c, MDGPU_ERR_ARG, "dt must be positive");
 	cudaError_t e = cudaSetDevice(c->device);
 	if (e != cudaSuccess) return set_cuda_error(c, e, "cudaSetDevice");
+	{
+		const int st = rebuild_prepare(c);   // the buffers of the per-step binning (traj_bin)
+		if (st) return st;
+	}
 	if (!c->traj) c->traj = new Traj();
 	Traj* t = c->traj;
 	const int64_t n = c->n;
@@ -265,7 +273,7 @@ int mdgpu_traj_forward(mdgpu_ctx* ctx, int32_t nsteps, int32_t checkpoint_every,
 	t->pgrad = t->os + 3 * n;
 	t->par = t->pgrad + nb * 2 * KK;
 	// forces of the start, then the steps; every `every` steps a snapshot (r, v)
-	e = launch_bin(c, false);
+	e = traj_bin(c);
 	if (e == cudaSuccess) e = launch_pairs(c);
 	if (e == cudaSuccess) e = traj_snap(c, t->snaps, true);
 	size_t si = 1;
@@ -317,7 +325,7 @@ int mdgpu_traj_backward(mdgpu_ctx* ctx, const double* gF, double gU, double* dL_
 		const int k1 = si + 1 < (int) t->starts.size() ? t->starts[si + 1] : t->nsteps;
 		// the segment from its snapshot: forces of r_k0, then steps k0+1 .. k1, positions kept
 		e = traj_restore(c, t->snaps + 6 * n * si, true);
-		if (e == cudaSuccess) e = launch_bin(c, false);
+		if (e == cudaSuccess) e = traj_bin(c);
 		if (e == cudaSuccess) e = launch_pairs(c);
 		for (int k = k0 + 1; k <= k1 && e == cudaSuccess; k++) {
 			e = traj_step(c, dt);
@@ -327,14 +335,14 @@ int mdgpu_traj_backward(mdgpu_ctx* ctx, const double* gF, double gU, double* dL_
 		// backwards through the segment: F_k = F(r_k) for k = k1 .. k0 + 1
 		for (int k = k1; k > k0 && e == cudaSuccess; k--) {
 			e = traj_restore(c, t->seg + 3 * n * (k - k0), false);
-			if (e == cudaSuccess) e = launch_bin(c, false);
+			if (e == cudaSuccess) e = traj_bin(c);
 			if (e == cudaSuccess) e = traj_vjp(c, t, gUk, true, true);
 			gUk = 0.0;
 		}
 	}
 	// the start: rbar += J(r_0)^T Fbar
 	if (e == cudaSuccess) e = traj_restore(c, t->snaps, true);
-	if (e == cudaSuccess) e = launch_bin(c, false);
+	if (e == cudaSuccess) e = traj_bin(c);
 	if (e == cudaSuccess) e = traj_vjp(c, t, gUk, false, false);
 	double par[2 * KK];
 	if (e == cudaSuccess) {
