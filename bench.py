@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--skin", type=float, default=0.3,
                     help="Verlet skin of the step (0: cells and candidates rebuilt every step, as the reference)")
+    ap.add_argument("--prune", type=float, default=0.0,
+                    help="inner skin of the pruned lists (0: the steps evaluate the build lists)")
     ap.add_argument("--workload", choices=["c2", "c3", "batched", "checkpoint", "rigid", "adjoint"], default="c2",
                     help="c2: the 1M-molecule box (headline); c3: the 4M-molecule two-species slab; "
                          "batched: the 512-box ensemble; checkpoint: phase-space file write and read of the "
@@ -67,7 +69,7 @@ def parse():
     return ap.parse_args()
 
 
-def workload_config(system, precision, skin=0.0):
+def workload_config(system, precision, skin=0.0, prune=0.0):
     if system.name.startswith("c3"):
         head = {"workload": f"lj_slab_two_species_{system.n}", "n_molecules": int(system.n),
                 "box": [float(x) for x in system.length], "density": "liquid 0.70 (middle third), vapour 0.02",
@@ -83,6 +85,9 @@ def workload_config(system, precision, skin=0.0):
             "pair_search": (f"candidate lists of radius rc + {skin} rebuilt (with the binning) when a molecule moved "
                             f"more than {skin / 2:g} since the last build; exact r^2 < rc^2 test on every pair")
             if skin > 0 else "cells rebuilt and candidates searched every step",
+            "list_prune": (f"the steps evaluate the list entries within rc + {prune:g} at the last prune, re-pruned "
+                           f"after each build and when the summed largest drifts reach {prune / 2:g}")
+            if 0 < prune < skin else None,
             "l2": "not flushed: each step reads the whole state (molecule arrays and candidate lists, "
                   "several times the 126 MB L2); the timed steps run as one mdgpu_run_async"}
 
@@ -389,6 +394,7 @@ def run_ours(args, dist: Dist):
     lc.update()
     lc.traversePairs()
     lc.setSkin(args.skin)
+    lc.setListPrune(args.prune)
     stream = torch.cuda.ExternalStream(lc.stream())
 
     dist.barrier()
@@ -403,8 +409,10 @@ def run_ours(args, dist: Dist):
 
     # kernel-level timing for the roofline (separate, profiled pass)
     builds0 = lc.skinBuilds() if args.skin > 0 else 0
+    prunes0 = lc.listPrunes() if args.skin > 0 else 0
     tk, cnt, rec2 = time_kernels(lc, system, args.steps)
     rebuilds = (lc.skinBuilds() - builds0) if args.skin > 0 else args.steps
+    prunes = (lc.listPrunes() - prunes0) if args.skin > 0 else 0
     pair_ms = tk[1] / args.steps   # all pair launches of a step (the build is gated off in most steps)
     pairs_per_launch = float(rec2[:, 3].mean())
     fp32_peak, fp64_peak = M.device_peaks(dist.local)
@@ -447,7 +455,7 @@ def run_ours(args, dist: Dist):
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 pair arithmetic, f64 accumulation" if precision == M.MIXED else "f64",
         "data": "synthetic (seeded FCC lattice, Maxwell-Boltzmann velocities)",
-        "config": workload_config(system, args.precision, args.skin),
+        "config": workload_config(system, args.precision, args.skin, args.prune),
         "steps_per_s": args.steps / t_max,
         "pairs_per_step": pairs / args.steps,
         "roofline": {"bound": "fp32" if precision == M.MIXED else "fp64", "kernel": "pair traversal",
@@ -460,6 +468,7 @@ def run_ours(args, dist: Dist):
         "kernels_ms_per_step": {"binning": tk[0] / args.steps, "pairs": tk[1] / args.steps,
                                 "integration": tk[2] / args.steps},
         "rebuilds_per_step": rebuilds / args.steps,
+        "prunes_per_step": prunes / args.steps,
         "hbm_kernels": {"binning_gbs": bin_bytes * max(rebuilds, 1) / (tk[0] * 1e-3) / 1e9,
                         "binning_note": "per binning pass (wrap, bin, sort), counted over the passes that ran",
                         "integration_gbs": (int_bytes / (tk[2] / args.steps * 1e-3) / 1e9) if args.skin == 0 else None,
@@ -491,6 +500,7 @@ def run_ours(args, dist: Dist):
         y.update()
         y.traversePairs()
         y.setSkin(args.skin)
+        y.setListPrune(args.prune)
         so, po, _, _ = time_device_resident(M, y, system, args.steps, 3, torch.cuda.ExternalStream(y.stream()))
         y.close()
         ratio = (pl / sl) / (po / so)
@@ -511,6 +521,7 @@ def run_ours(args, dist: Dist):
             x.update()
             x.traversePairs()
             x.setSkin(skin)
+            x.setListPrune(args.prune if skin > 0 else 0.0)
             s2, p2, _, _ = time_device_resident(M, x, system, csteps, args.warmup,
                                                 torch.cuda.ExternalStream(x.stream()))
             x.close()
@@ -1025,10 +1036,12 @@ def run_adjoint(args, dist: Dist):
     clocks = ClockSampler(dist.local)
     clocks.start()
     torch.cuda.synchronize()
+    launches0 = tr.lc.profileRead()[1][3]
     e0.record(stream)
     for _ in range(reps):
         gr, gv, ge, gs = one()
     e1.record(stream)
+    launches = int(tr.lc.profileRead()[1][3] - launches0)
     torch.cuda.synchronize()
     clk = clocks.stop()
     sec = dist.max(e0.elapsed_time(e1) * 1e-3)
@@ -1045,8 +1058,6 @@ def run_adjoint(args, dist: Dist):
     flops_launch = 2.0 * upairs * FLOPS_PER_ADJ_PAIR
     achieved = flops_launch / (adj_ms / max(adj_launches, 1) * 1e-3) / 1e12
     tr.close()
-    # launches per gradient: forward 50 steps x 4 + backward (5 segments x 10 recomputed steps x 5 +
-    # 50 adjoint steps x ~5)
     out = {
         "metric": ADJ_METRIC, "value": dist.sum(reps / sec), "unit": "trajectory gradients/s", "n_gpus": dist.world,
         "steps": reps, "warmup": max(args.warmup, 1), "ms_per_step": sec / reps * 1e3, "higher_is_better": True,
@@ -1066,7 +1077,7 @@ def run_adjoint(args, dist: Dist):
                      "launches": adj_launches},
         "gradient_norms": {"dL_dr0_rms": float(np.sqrt(np.mean(gr ** 2))), "dL_deps_AB": float(ge[0, 1]),
                            "dL_dsigma_AB": float(gs[0, 1])},
-        "gpu_launches": None, "clocks": clk,
+        "gpu_launches": launches, "launches_per_gradient": launches / reps, "clocks": clk,
         "e2e": {"value": dist.sum(reps / sec), "unit": "trajectory gradients/s",
                 "h2d_bytes_per_step": 2 * 48 * s.n, "d2h_bytes_per_step": 4 * 24 * s.n,
                 "note": "each gradient uploads r0, v0 and gF and downloads the final state and dL/dr0, dL/dv0"},

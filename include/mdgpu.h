@@ -267,6 +267,16 @@ int mdgpu_forces_noalloc(int device, void* stream, int64_t n, const double* d_r,
 int mdgpu_set_skin(mdgpu_ctx* ctx, double skin);
 /* Number of list builds of the Verlet-skin mode so far (synchronises the context's stream). */
 int mdgpu_skin_builds(mdgpu_ctx* ctx, int64_t* builds);
+/* Pruned lists of the Verlet-skin mode (0 < prune < skin; 0 = off, the default). No reference
+ * counterpart. The steps evaluate inner lists: the entries of each build list that were within
+ * cutoff + prune at the last prune. A prune re-filters the build lists at the current positions.
+ * It runs after every build, and whenever the per-step largest drifts summed since the last prune
+ * reach prune/2, decided on the device. A pair left out of an inner list is therefore beyond the
+ * cutoff until the next prune: the same pairs are evaluated as without pruning, fewer entries are
+ * read. prune must be in [0, cutoff); it is in effect while it is also below the skin.
+ * mdgpu_list_prunes: prunes so far (synchronises the context's stream). */
+int mdgpu_set_list_prune(mdgpu_ctx* ctx, double prune);
+int mdgpu_list_prunes(mdgpu_ctx* ctx, int64_t* prunes);
 
 /* ---- batched ensemble of independent boxes ------------------------------------------------
  * No reference counterpart: in MarDyn every box is its own Simulation with its own LinkedCells

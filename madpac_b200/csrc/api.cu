@@ -509,6 +509,9 @@ int mdgpu_destroy(mdgpu_ctx* ctx) {
 	free_traj(c);
 	cudaFree(c->nbr);
 	cudaFree(c->nbr_count);
+	cudaFree(c->nbr_in);
+	cudaFree(c->nbr_in_count);
+	cudaFree(c->prune_st);
 	cudaFree(c->r_ref);
 	cudaFree(c->rebuild);
 	cudaFree(c->builds);
@@ -768,6 +771,7 @@ int mdgpu_leapfrog_pre(mdgpu_ctx* ctx, double dt, double vcorr) {
 	MD_CUDA(cudaSetDevice(c->device));
 	MD_CUDA(launch_leapfrog_pre(c, dt, vcorr));
 	c->cells_valid = false;
+	if (pruning(c)) c->lists_valid = false;   // a drift the pruned lists did not see
 	return MDGPU_OK;
 }
 
@@ -831,20 +835,33 @@ int skin_prepare(Context* c) {
 	int cap = (int) std::ceil(1.25 * 4.18879020478639 * rl * rl * rl * rho_max) + 32;
 	cap = (cap + 31) & ~31;
 	cap = std::min(cap, 65504);
-	if (c->list_n != n || c->list_cap < cap) {
+	if (c->list_n != n || c->list_cap < cap || (pruning(c) && !c->nbr_in)) {
 		cudaFree(c->nbr);
 		cudaFree(c->nbr_count);
+		cudaFree(c->nbr_in);
+		cudaFree(c->nbr_in_count);
 		cudaFree(c->r_ref);
 		c->nbr = nullptr;
 		c->nbr_count = nullptr;
+		c->nbr_in = nullptr;
+		c->nbr_in_count = nullptr;
 		c->r_ref = nullptr;
+		if (c->list_n == n) cap = std::max(cap, c->list_cap);
 		c->list_n = 0;
 		MD_CUDA(cudaMalloc(&c->nbr, sizeof(unsigned short) * (size_t) cap * n));
 		MD_CUDA(cudaMalloc(&c->nbr_count, sizeof(unsigned short) * n));
+		if (pruning(c)) {
+			MD_CUDA(cudaMalloc(&c->nbr_in, sizeof(unsigned short) * (size_t) cap * n));
+			MD_CUDA(cudaMalloc(&c->nbr_in_count, sizeof(unsigned short) * n));
+		}
 		MD_CUDA(cudaMalloc(&c->r_ref, sizeof(double) * 3 * n));
 		c->list_n = n;
 		c->list_cap = cap;
 		c->lists_valid = false;
+	}
+	if (pruning(c) && !c->prune_st) {
+		MD_CUDA(cudaMalloc(&c->prune_st, sizeof(PruneState)));
+		MD_CUDA(cudaMemsetAsync(c->prune_st, 0, sizeof(PruneState), c->stream));
 	}
 	{
 		const int st = rebuild_prepare(c);
@@ -924,6 +941,28 @@ int mdgpu_set_skin(mdgpu_ctx* ctx, double skin) {
 	}
 	c->skin = skin;
 	c->lists_valid = false;
+	return MDGPU_OK;
+}
+
+int mdgpu_set_list_prune(mdgpu_ctx* ctx, double prune) {
+	if (!ctx) return MDGPU_ERR_ARG;
+	Context* c = &ctx->c;
+	if (!(prune >= 0.0) || !(prune < c->rc)) return fail(c, MDGPU_ERR_ARG, "prune must be in [0, cutoff)");
+	c->prune = prune;
+	c->lists_valid = false;
+	return MDGPU_OK;
+}
+
+int mdgpu_list_prunes(mdgpu_ctx* ctx, int64_t* prunes) {
+	if (!ctx || !prunes) return MDGPU_ERR_ARG;
+	Context* c = &ctx->c;
+	*prunes = 0;
+	if (!c->prune_st) return MDGPU_OK;
+	PruneState st{};
+	MD_CUDA(cudaSetDevice(c->device));
+	MD_CUDA(cudaMemcpyAsync(&st, c->prune_st, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
+	MD_CUDA(cudaStreamSynchronize(c->stream));
+	*prunes = (int64_t) st.count;
 	return MDGPU_OK;
 }
 

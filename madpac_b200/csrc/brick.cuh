@@ -435,6 +435,8 @@ struct Lists {
 	unsigned* counts;                  // sparse [0] and dense [1] bricks of the build (or null)
 	int32_t* blist;                    // dense bricks at [0, nbricks), sparse ones from nbricks on
 	int nbricks;
+	PruneState* pst;                   // pruned lists: their state (the evaluation's last CTA updates it)
+	int step;                          // id of the step being evaluated
 };
 // A brick is sparse when its whole staged region holds at most kSparseCap molecules and its own
 // cells at most 32: one warp stages and evaluates it, without CTA-wide barriers.
@@ -796,6 +798,13 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 // r' = r + dt v (Molecule::upd_preF with vcorr = 1, Molecule.cpp:128-135), writes r' to the other
 // position buffer (other bricks still stage r) and flags a rebuild with `id` when r' is farther than
 // skin/2 from the position of the last build. Same operations and roundings as the Leapfrog kernels.
+// The CTA's largest squared drift of a list kernel with pruned lists (float bits; set to 0 before the
+// first finish, flushed by drift_flush).
+__device__ __forceinline__ unsigned& drift_slot() {
+	__shared__ unsigned s_drift;
+	return s_drift;
+}
+
 struct Kick {
 	int mode;
 	int id;
@@ -807,6 +816,7 @@ struct Kick {
 	double *vx, *vy, *vz;
 	double *ox, *oy, *oz;         // positions after the drift (mode 1)
 	int* flag;
+	unsigned* dmax;               // mode 1 with pruned lists: the largest squared drift, as float bits
 };
 
 __device__ __forceinline__ double finish(const Kick& k, int64_t gi, double Fx, double Fy, double Fz, const double* rx,
@@ -837,9 +847,15 @@ __device__ __forceinline__ double finish(const Kick& k, int64_t gi, double Fx, d
 	const double wx = __dadd_rn(__dmul_rn(1.0, vx), __dmul_rn(b, Fx));
 	const double wy = __dadd_rn(__dmul_rn(1.0, vy), __dmul_rn(b, Fy));
 	const double wz = __dadd_rn(__dmul_rn(1.0, vz), __dmul_rn(b, Fz));
-	const double x = __dadd_rn(rx[gi], __dmul_rn(k.dt, wx));
-	const double y = __dadd_rn(ry[gi], __dmul_rn(k.dt, wy));
-	const double z = __dadd_rn(rz[gi], __dmul_rn(k.dt, wz));
+	const double x0 = rx[gi], y0 = ry[gi], z0 = rz[gi];
+	const double x = __dadd_rn(x0, __dmul_rn(k.dt, wx));
+	const double y = __dadd_rn(y0, __dmul_rn(k.dt, wy));
+	const double z = __dadd_rn(z0, __dmul_rn(k.dt, wz));
+	if (k.dmax) {
+		// this drift's length squared, rounded up (the bits of a non-negative float order as it does)
+		const double sx = x - x0, sy = y - y0, sz = z - z0;
+		atomicMax(&drift_slot(), __float_as_uint(__double2float_ru(sx * sx + sy * sy + sz * sz)));
+	}
 	k.vx[gi] = wx;
 	k.vy[gi] = wy;
 	k.vz[gi] = wz;
@@ -849,6 +865,12 @@ __device__ __forceinline__ double finish(const Kick& k, int64_t gi, double Fx, d
 	const double dx = x - lists.rx_ref[gi], dy = y - lists.ry_ref[gi], dz = z - lists.rz_ref[gi];
 	if (!(dx * dx + dy * dy + dz * dz <= k.half2)) *k.flag = k.id;
 	return mv2;
+}
+
+// The CTA's largest squared drift into *dmax (thread 0, after a CTA barrier that follows every
+// finish; the atomic is skipped when the value there is already as large).
+__device__ __forceinline__ void drift_flush(unsigned* dmax) {
+	if (dmax && threadIdx.x == 0 && drift_slot() > __ldcg(dmax)) atomicMax(dmax, drift_slot());
 }
 
 // Lanes per molecule for g molecules on one warp: the largest power of two with lpm * g <= 32.
@@ -1162,6 +1184,100 @@ __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int br
 	}
 	if (same) atomicOr(status, kStatusSamePosition);
 	block_sum3_at(U, W, NP, partials, slot, MV);
+}
+
+// Entries of each thread's ring in prune_lists: up to 7 unwritten entries plus the 8 of one block.
+constexpr int kPruneRing = 16;
+
+// Shared-memory bytes of prune_lists for a staged capacity s_cap.
+__host__ __device__ inline size_t prune_bytes(int s_cap) {
+	return layout(s_cap, false, 0, false).total + sizeof(unsigned short) * kPruneRing * kThreads;
+}
+
+// Pruning of the lists of brick `brick`: with the positions staged as list_pairs stages them, each own
+// molecule (one thread each) keeps the entries of its build list (`outer`) whose squared distance
+// in the staged frame is below rp2f, in list order, and writes them to `inner` in the same layout,
+// the last block padded with the sentinel slot. rp2f is (rc + prune)^2 plus a margin that covers
+// the rounding of that distance. A brick whose region exceeds the staged capacity is skipped: the
+// evaluation gathers it from global memory without reading its lists.
+__device__ __forceinline__ void prune_lists(const Const& p, const Box& bx, int brick, unsigned char* smem,
+                                            const double* rx, const double* ry, const double* rz,
+                                            const int32_t* cid, const int32_t* cstart, const Lists& outer,
+                                            const Lists& inner, float rp2f) {
+	const SmemLayout L = layout(p.s_cap, false, 0, false);
+	const Smem S = views(smem, L);
+	// ring entry k of thread t at k * kThreads + t: a warp's writes of one entry each fall in 16 banks
+	unsigned short* ring = reinterpret_cast<unsigned short*>(smem + L.total);
+	const int tid = threadIdx.x;
+	const bool staged = stage<false, false>(p, bx, brick, S, rx, ry, rz, cid, cstart);
+	__shared__ int s_own[9], s_ocell[8];
+	if (tid == 0) {
+		int acc = 0;
+		for (int w = 0; w < 8; w++) {
+			int ic;
+			const bool ok = own_cell(bx, brick, w, ic);
+			s_own[w] = acc;
+			s_ocell[w] = ic;
+			acc += ok ? S.cnt[ic] : 0;
+		}
+		s_own[8] = acc;
+	}
+	__syncthreads();
+	if (!staged) return;
+	const int n_own = s_own[8];
+	const unsigned sent = (unsigned) outer.sentinel;
+	for (int t = tid; t < n_own; t += kThreads) {
+		int w = 0;
+		while (w < 7 && s_own[w + 1] <= t) w++;
+		const int slot_i = S.cs[s_ocell[w]] + (t - s_own[w]);
+		const int gi = S.gst[s_ocell[w]] + (t - s_own[w]);
+		const int cnt = outer.count[gi];
+		if (cnt == kListOverflow) {
+			inner.count[gi] = kListOverflow;
+			continue;
+		}
+		const float4 hi_i = S.hi[slot_i];
+		const unsigned wi = __float_as_uint(hi_i.w);
+		const float mix = __uint_as_float(0x4B000000u | (wi & 511u));
+		const float miy = __uint_as_float(0x4B000000u | ((wi >> 9) & 511u));
+		const float miz = __uint_as_float(0x4B000000u | ((wi >> 18) & 511u));
+		const uint4* src = reinterpret_cast<const uint4*>(outer.nbr) + gi;
+		uint4* dst = reinterpret_cast<uint4*>(inner.nbr) + gi;
+		const int nblk = (cnt + 7) >> 3;
+		int kept = 0, done = 0;
+		auto flush = [&]() {
+			unsigned v[4];
+#pragma unroll
+			for (int k = 0; k < 4; k++)
+				v[k] = (unsigned) ring[((done + 2 * k) & (kPruneRing - 1)) * kThreads + tid] |
+				       ((unsigned) ring[((done + 2 * k + 1) & (kPruneRing - 1)) * kThreads + tid] << 16);
+			dst[(int64_t) (done >> 3) * outer.n] = make_uint4(v[0], v[1], v[2], v[3]);
+			done += 8;
+		};
+		for (int b = 0; b < nblk; b++) {
+			const uint4 cur = src[(int64_t) b * outer.n];
+#pragma unroll
+			for (int u = 0; u < 8; u++) {
+				const int j = min((int) ((list_word(cur, u >> 1) >> (16 * (u & 1))) & 0xffffu), p.s_cap);
+				const float4 hj = S.hi[j];
+				const unsigned wj = __float_as_uint(hj.w);
+				const float e0 = fmaf(mix - __uint_as_float(0x4B000000u | (wj & 511u)), bx.lo_step[0], hi_i.x - hj.x);
+				const float e1 = fmaf(miy - __uint_as_float(0x4B000000u | ((wj >> 9) & 511u)), bx.lo_step[1], hi_i.y - hj.y);
+				const float e2 = fmaf(miz - __uint_as_float(0x4B000000u | ((wj >> 18) & 511u)), bx.lo_step[2], hi_i.z - hj.z);
+				const float d2f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2));
+				if (8 * b + u < cnt && d2f < rp2f) {
+					ring[(kept & (kPruneRing - 1)) * kThreads + tid] = (unsigned short) j;
+					kept++;
+				}
+			}
+			if (kept - done >= 8) flush();
+		}
+		if (kept > done) {
+			for (int k = kept; k < done + 8; k++) ring[(k & (kPruneRing - 1)) * kThreads + tid] = (unsigned short) sent;
+			flush();
+		}
+		inner.count[gi] = (unsigned short) kept;
+	}
 }
 
 // A sparse brick (see kSparseCap) by one warp, in its own shared-memory area laid out as

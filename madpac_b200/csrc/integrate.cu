@@ -24,37 +24,51 @@ struct SpeciesScale {
 
 // Verlet-skin check of the pre-kick: the positions at the last build, the squared half skin, and
 // the step id written to *flag when a molecule moved farther.
+// With pruned lists, dmax receives the largest squared drift (float bits, rounded up).
 struct SkinCheck {
 	const double *rx, *ry, *rz;
 	double half2;
 	int* flag;
 	int id;
+	unsigned* dmax;
 };
 
 __global__ void __launch_bounds__(kReduceBlock) k_leapfrog_pre(int64_t n, Particles p, SpeciesScale s, double dt,
                                                               double vcorr, SkinCheck sk) {
 	int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n) return;
-	// every load first: the arrays may alias as far as the compiler knows
-	const double a = s.dtInv2m[p.cid[i]];
-	const double vx0 = p.vx[i], vy0 = p.vy[i], vz0 = p.vz[i];
-	const double fx = p.fx[i], fy = p.fy[i], fz = p.fz[i];
-	const double x0 = p.rx[i], y0 = p.ry[i], z0 = p.rz[i];
-	const double vx = __dadd_rn(__dmul_rn(vcorr, vx0), __dmul_rn(a, fx));
-	const double vy = __dadd_rn(__dmul_rn(vcorr, vy0), __dmul_rn(a, fy));
-	const double vz = __dadd_rn(__dmul_rn(vcorr, vz0), __dmul_rn(a, fz));
-	const double x = __dadd_rn(x0, __dmul_rn(dt, vx));
-	const double y = __dadd_rn(y0, __dmul_rn(dt, vy));
-	const double z = __dadd_rn(z0, __dmul_rn(dt, vz));
-	p.vx[i] = vx;
-	p.vy[i] = vy;
-	p.vz[i] = vz;
-	p.rx[i] = x;
-	p.ry[i] = y;
-	p.rz[i] = z;
-	if (sk.flag) {
-		const double dx = x - sk.rx[i], dy = y - sk.ry[i], dz = z - sk.rz[i];
-		if (!(dx * dx + dy * dy + dz * dz <= sk.half2)) *sk.flag = sk.id;
+	const bool in = i < n;
+	unsigned dm = 0u;
+	if (in) {
+		// every load first: the arrays may alias as far as the compiler knows
+		const double a = s.dtInv2m[p.cid[i]];
+		const double vx0 = p.vx[i], vy0 = p.vy[i], vz0 = p.vz[i];
+		const double fx = p.fx[i], fy = p.fy[i], fz = p.fz[i];
+		const double x0 = p.rx[i], y0 = p.ry[i], z0 = p.rz[i];
+		const double vx = __dadd_rn(__dmul_rn(vcorr, vx0), __dmul_rn(a, fx));
+		const double vy = __dadd_rn(__dmul_rn(vcorr, vy0), __dmul_rn(a, fy));
+		const double vz = __dadd_rn(__dmul_rn(vcorr, vz0), __dmul_rn(a, fz));
+		const double x = __dadd_rn(x0, __dmul_rn(dt, vx));
+		const double y = __dadd_rn(y0, __dmul_rn(dt, vy));
+		const double z = __dadd_rn(z0, __dmul_rn(dt, vz));
+		p.vx[i] = vx;
+		p.vy[i] = vy;
+		p.vz[i] = vz;
+		p.rx[i] = x;
+		p.ry[i] = y;
+		p.rz[i] = z;
+		if (sk.flag) {
+			const double dx = x - sk.rx[i], dy = y - sk.ry[i], dz = z - sk.rz[i];
+			if (!(dx * dx + dy * dy + dz * dz <= sk.half2)) *sk.flag = sk.id;
+		}
+		if (sk.dmax) {
+			// this drift's length squared, rounded up (the bits of a non-negative float order as it does)
+			const double sx = x - x0, sy = y - y0, sz = z - z0;
+			dm = __float_as_uint(__double2float_ru(sx * sx + sy * sy + sz * sz));
+		}
+	}
+	if (sk.dmax) {
+		dm = __reduce_max_sync(0xffffffffu, dm);
+		if ((threadIdx.x & 31) == 0 && dm > __ldcg(sk.dmax)) atomicMax(sk.dmax, dm);
 	}
 }
 
@@ -193,6 +207,7 @@ SkinCheck skin_check_of(const Context* c, bool on) {
 		sk.half2 = 0.25 * c->skin * c->skin;
 		sk.flag = c->rebuild;
 		sk.id = c->step_id;
+		if (pruning(c)) sk.dmax = &c->prune_st->dmax[c->step_id & 1];
 	}
 	return sk;
 }

@@ -42,6 +42,19 @@ struct PairParams {
 	double shift6[kMaxSpecies * kMaxSpecies];
 };
 
+// Device state of the pruned Verlet-skin lists (mdgpu_set_list_prune). A molecule's inner list
+// holds the entries of its build list that were closer than rc + prune at the positions of the
+// last prune. Between prunes, acc bounds how far any molecule has moved since then. It is the sum,
+// over the drifts, of the largest distance any molecule moved in that drift. A pair left out is
+// therefore still beyond rc while 2 acc < prune.
+struct PruneState {
+	unsigned dmax[2];           // float bits of the largest squared drift of the last step of each parity
+	int pruned;                 // id of the step whose inner lists were last made
+	int pad;
+	double acc;                 // summed largest drifts since the positions of the last prune
+	unsigned long long count;   // prunes so far
+};
+
 // LinkedCells geometry. The device keeps only the box's own cells (nc per dimension, no halo
 // layer); the reference's halo-inclusive numbering is recovered as inner index + 1 per dimension.
 struct Grid {
@@ -109,6 +122,11 @@ struct Context {
 	unsigned short* nbr = nullptr;  // list_cap x n staged-slot indices
 	unsigned short* nbr_count = nullptr;
 	double* r_ref = nullptr;        // 3 x n positions at the last build
+	// pruned lists (0 < prune < skin): the entries within rc + prune, which the evaluation reads
+	double prune = 0.0;
+	unsigned short* nbr_in = nullptr;       // list_cap x n, the layout of nbr
+	unsigned short* nbr_in_count = nullptr;
+	PruneState* prune_st = nullptr;         // device
 	int* rebuild = nullptr;         // device: the step id for which a build was asked
 	unsigned char* brick_kind = nullptr;   // per skin-grid brick: 1 = sparse
 	int step_id = 0;                // id of the step being enqueued (skin mode)
@@ -143,6 +161,9 @@ struct Context {
 	double prof_ms[3] = {0, 0, 0};
 	int64_t prof_count[4] = {0, 0, 0, 0};
 };
+
+// Whether the Verlet-skin steps evaluate pruned lists (an inner radius between rc and rc + skin).
+inline bool pruning(const Context* c) { return c->skin > 0.0 && c->prune > 0.0 && c->prune < c->skin; }
 
 // ---- launch helpers implemented in the .cu files -------------------------------------------
 // Each returns cudaSuccess or the launch error; kernels report data errors in ctx->status.

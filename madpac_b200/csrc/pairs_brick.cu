@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -51,6 +52,28 @@ __global__ void __launch_bounds__(brick::kThreads, 3)
 	}
 }
 
+// Pruning step of the pruned lists: runs when this step builds the lists or when the summed largest
+// drifts since the last prune have reached half the inner skin; then every brick's inner lists
+// from its build lists at the current positions (a resident grid walks the bricks).
+__global__ void __launch_bounds__(brick::kThreads, 2)
+    k_prune_lists(brick::Const p, brick::Box bx, int nbricks, const double* __restrict__ rx,
+                  const double* __restrict__ ry, const double* __restrict__ rz, const int32_t* __restrict__ cid,
+                  const int32_t* __restrict__ cstart, const int* __restrict__ gate, int step, brick::Lists outer,
+                  brick::Lists inner, float rp2f, double half_prune) {
+	const PruneState* st = inner.pst;
+	const double moved = st->acc + sqrt((double) __uint_as_float(st->dmax[step & 1]));
+	if (*gate != step && moved < half_prune) return;
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
+		inner.pst->pruned = step;
+		inner.pst->count++;
+	}
+	extern __shared__ __align__(16) unsigned char smem[];
+	for (int b = blockIdx.x; b < nbricks; b += gridDim.x) {
+		brick::prune_lists(p, bx, b, smem, rx, ry, rz, cid, cstart, outer, inner, rp2f);
+		__syncthreads();
+	}
+}
+
 #ifndef MDGPU_LIST_MINB
 #define MDGPU_LIST_MINB 3
 #endif
@@ -68,6 +91,7 @@ __global__ void __launch_bounds__(brick::kThreads, kFP64 ? 2 : kListMinBlocks)
 	extern __shared__ __align__(16) unsigned char smem[];
 	__shared__ int s_item;
 	brick::load_params(smem, brick::layout(p.s_cap, kFP64, 0, false), pp, p.ns);
+	if (threadIdx.x == 0) brick::drift_slot() = 0u;   // read after the barriers below
 	if (lists.kind == nullptr) {
 		// every brick, one CTA each
 		__syncthreads();
@@ -88,12 +112,21 @@ __global__ void __launch_bounds__(brick::kThreads, kFP64 ? 2 : kListMinBlocks)
 			                                           partials, status, lists, kick);
 		}
 	}
+	__syncthreads();
+	brick::drift_flush(kick.dmax);
 	// U6 sum, virial sum, pair count (and sum m v^2 of the closing kick) of the step over every
 	// brick's partials, summed by the last CTA to finish, which also writes the step record
 	// {Upot, virial, sum m v^2, pairs} and resets both work queues
 	if (last_block_sum(tickets, partials, lists.nbricks, kick.mode ? 4 : 3, scalars) && threadIdx.x == 0) {
 		lists.counts[2] = 0u;
 		lists.counts[3] = 0u;
+		if (lists.pst) {
+			// the drift into this step's positions joins the sum, which a prune at this step restarts
+			PruneState* st = lists.pst;
+			const int par = lists.step & 1;
+			st->acc = st->pruned == lists.step ? 0.0 : st->acc + sqrt((double) __uint_as_float(st->dmax[par]));
+			st->dmax[par] = 0u;
+		}
 		if (record) {
 			record[0] = scalars[0] * 0.5 / 6.;
 			record[1] = scalars[1] * 0.5;
@@ -130,6 +163,8 @@ __global__ void __launch_bounds__(brick::kThreads, 2)
 	if (lane == 0)
 		reinterpret_cast<float4*>(ws + L.hi)[brick::kSparseCap] =
 		    make_float4(1e15f, 1e15f, 1e15f, __uint_as_float((256u << 18) | (256u << 9) | 256u));
+	if (threadIdx.x == 0) brick::drift_slot() = 0u;
+	__syncthreads();
 	const int nwork = (int) *(volatile unsigned*) lists.counts;
 	for (;;) {
 		__syncwarp();
@@ -141,6 +176,8 @@ __global__ void __launch_bounds__(brick::kThreads, 2)
 		brick::list_pairs_warp<kFP64, kSingle, kLjIsRc>(p, bx, b, ws, rx, ry, rz, cid, cstart, fx, fy, fz, partials,
 		                                                status, lists, kick);
 	}
+	__syncthreads();
+	brick::drift_flush(kick.dmax);
 }
 
 // Resident grid of a kernel: the CTAs that fit on the device at once (at most `cap`). The
@@ -278,6 +315,7 @@ cudaError_t launch_pairs_skin(Context* c, int kick_mode, double dt, double* reco
 		kick.oy = c->q.ry;
 		kick.oz = c->q.rz;
 		kick.flag = c->rebuild;
+		if (pruning(c) && kick_mode == 1) kick.dmax = &c->prune_st->dmax[(c->step_id + 1) & 1];
 	}
 	const Plan P = plan(c, c->gs, c->rc, 2);
 	l.sentinel = P.p.s_cap;   // the evaluation kernel's sentinel slot terminates every list
@@ -294,6 +332,31 @@ cudaError_t launch_pairs_skin(Context* c, int kick_mode, double dt, double* reco
 	if (e == cudaSuccess)
 		k_build_lists<<<grid, brick::kThreads, bbytes, c->stream>>>(bb, nbricks, s_cap, c->p.rx, c->p.ry, c->p.rz,
 		                                                           c->cell_start, c->rebuild, c->step_id, l);
+	int launches = 2;
+	if (pruning(c)) {
+		// pruning (gated), then the evaluation reads the inner lists
+		brick::Lists in = l;
+		in.nbr = c->nbr_in;
+		in.count = c->nbr_in_count;
+		in.pst = c->prune_st;
+		in.step = c->step_id;
+		// (rc + prune)^2 rounded up, with a margin above the rounding of the staged-frame distance
+		// (below 1e-6 of it)
+		const double rp = c->rc + c->prune;
+		const double rp2 = rp * rp * (1.0 + 4e-6);
+		float rp2f = (float) rp2;
+		if ((double) rp2f < rp2) rp2f = std::nextafter(rp2f, 2.0f * rp2f);
+		const size_t pbytes = brick::prune_bytes(P.p.s_cap);
+		if (e == cudaSuccess)
+			e = cudaFuncSetAttribute(k_prune_lists, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) pbytes);
+		const int pgrid = resident_grid(c, k_prune_lists, pbytes, P.nbricks);
+		if (e == cudaSuccess)
+			k_prune_lists<<<pgrid, brick::kThreads, pbytes, c->stream>>>(P.p, P.bx, P.nbricks, c->p.rx, c->p.ry, c->p.rz,
+			                                                             c->p.cid, c->cell_start, c->rebuild, c->step_id,
+			                                                             l, in, rp2f, 0.5 * c->prune);
+		l = in;
+		launches++;
+	}
 	// evaluation, every step: sparse bricks one warp each, then the others (whose last CTA sums the
 	// partials of all bricks). When the last build of an earlier run found no sparse brick the
 	// dense kernel takes every brick (kind not consulted) and the sparse kernel is not launched.
@@ -318,7 +381,7 @@ cudaError_t launch_pairs_skin(Context* c, int kick_mode, double dt, double* reco
 	}
 	if (e == cudaSuccess) e = dispatch<2>(c, P, nullptr, ld, kick, record);
 	if (e == cudaSuccess) e = cudaGetLastError();
-	prof_end(c, 1, sparse ? 3 : 2);
+	prof_end(c, 1, sparse ? launches + 1 : launches);
 	return e;
 }
 

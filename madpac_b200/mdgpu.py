@@ -82,6 +82,8 @@ SIGNATURES = {
     "mdgpu_write_checkpoint": (_I, [_VP, ctypes.c_char_p, _D, _D, _D, _I]),
     "mdgpu_read_phase_space": (_I, [_VP, ctypes.c_char_p, _VP, _VP]),
     "mdgpu_skin_builds": (_I, [_VP, _VP]),
+    "mdgpu_set_list_prune": (_I, [_VP, _D]),
+    "mdgpu_list_prunes": (_I, [_VP, _VP]),
     "mdgpu_batch_create": (_I, [ctypes.POINTER(_VP), _I32, _VP, _VP, _D, _D, _D, _I, _VP, _VP, _I, _I]),
     "mdgpu_batch_destroy": (_I, [_VP]),
     "mdgpu_batch_last_error": (ctypes.c_char_p, [_VP]),
@@ -687,6 +689,18 @@ class LinkedCells:
         """List builds of the Verlet-skin mode so far."""
         b = ctypes.c_int64()
         self._check(self.lib.mdgpu_skin_builds(self.h, ctypes.byref(b)))
+        return b.value
+
+    def setListPrune(self, prune: float) -> None:
+        """Pruned lists of the Verlet-skin mode (0 = off; in effect while 0 < prune < skin): the steps
+        evaluate the entries within rc + prune at the last prune, re-pruned on the device after each
+        build and when the summed largest drifts since the last prune reach prune/2."""
+        self._check(self.lib.mdgpu_set_list_prune(self.h, float(prune)))
+
+    def listPrunes(self) -> int:
+        """Prunes of the pruned lists so far."""
+        b = ctypes.c_int64()
+        self._check(self.lib.mdgpu_list_prunes(self.h, ctypes.byref(b)))
         return b.value
 
     # -- phase-space files ---------------------------------------------------------------------------
