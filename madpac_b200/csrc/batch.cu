@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_step(StepArgs a) {
 		__syncthreads();
 		for_bricks(2, [&](int item) {
 			const BatchBox& B = a.boxes[box_of(item)];
-			brick::pairs<kFP64, kSingle, kLjIsRc, kCap>(a.pc, B.bx, item - B.brick0, item, smem, a.dst.rx, a.dst.ry,
+			brick::pairs<kFP64, kSingle, kLjIsRc, kCap, false>(a.pc, B.bx, item - B.brick0, item, smem, a.dst.rx, a.dst.ry,
 			                                            a.dst.rz, a.dst.cid, a.cstart, a.dst.fx, a.dst.fy, a.dst.fz,
 			                                            a.partials, a.status);
 			__syncthreads();
@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_step(StepArgs a) {
 		__syncthreads();
 		for_bricks(3, [&](int item) {
 			const BatchBox& B = a.boxes[box_of(item)];
-			brick::list_pairs<kFP64, kSingle, kLjIsRc>(a.lc, B.bx, item - B.brick0, item, smem, a.src.rx, a.src.ry,
+			brick::list_pairs<kFP64, kSingle, kLjIsRc, false>(a.lc, B.bx, item - B.brick0, item, smem, a.src.rx, a.src.ry,
 			                                           a.src.rz, a.src.cid, a.cstart, a.src.fx, a.src.fy, a.src.fz,
 			                                           a.partials, a.status, a.lists, brick::Kick{});
 			__syncthreads();

@@ -246,10 +246,36 @@ __device__ __forceinline__ float3 unpack_lo(unsigned w, const Box& bx) {
 
 __device__ __forceinline__ int unpack_cid(unsigned w) { return (int) ((w >> 27) & 7u); }
 
+// Stages molecule e of staged cell c at double position (x, y, z), component q: the hi/lo frame
+// position, and the half-precision copy or the double image as the staging mode asks.
+template <bool kFP64, bool kHalf>
+__device__ __forceinline__ void stage_one(const Const& p, const Box& bx, const Smem& S, int c, int e, double x,
+                                          double y, double z, int q) {
+	const double Xd = __dadd_rn(x, S.ck[3 * c]), Yd = __dadd_rn(y, S.ck[3 * c + 1]);
+	const double Zd = __dadd_rn(z, S.ck[3 * c + 2]);
+	const float X = __double2float_rn(Xd), Y = __double2float_rn(Yd), Z = __double2float_rn(Zd);
+	const int slot_s = S.cs[c] + e;
+	const unsigned w = pack_lo(__double2float_rn(Xd - (double) X), __double2float_rn(Yd - (double) Y),
+	                           __double2float_rn(Zd - (double) Z), q, bx);
+	S.hi[slot_s] = make_float4(X, Y, Z, __uint_as_float(w));
+	if (kHalf) {
+		// half-precision copy relative to the brick centre (slot pairs share one HalfPair)
+		__half* hp = S.h + 8 * (slot_s >> 1) + (slot_s & 1);
+		hp[0] = __float2half_rn(X - bx.frame_c[0]);
+		hp[2] = __float2half_rn(Y - bx.frame_c[1]);
+		hp[4] = __float2half_rn(Z - bx.frame_c[2]);
+	}
+	if (kFP64) {
+		S.img[slot_s] = __dadd_rn(x, S.csh[3 * c]);
+		S.img[p.s_cap + slot_s] = __dadd_rn(y, S.csh[3 * c + 1]);
+		S.img[2 * p.s_cap + slot_s] = __dadd_rn(z, S.csh[3 * c + 2]);
+	}
+}
+
 // Stages the 4x4x4 cells around brick `brick` (positions in the local frame; double images in the
 // FP64 mode). Returns false when the region exceeds the staged capacity (nothing staged then; the
 // cell ranges s_gst/s_cnt are set either way). Ends with a CTA barrier.
-template <bool kFP64, bool kHalf = true>
+template <bool kFP64, bool kHalf = true, bool kWide = true>
 __device__ __forceinline__ bool stage(const Const& p, const Box& bx, int brick, const Smem& S, const double* rx,
                                       const double* ry, const double* rz, const int32_t* cid, const int32_t* cstart) {
 	const Grid& g = bx.g;
@@ -296,32 +322,39 @@ __device__ __forceinline__ bool stage(const Const& p, const Box& bx, int brick, 
 	}
 	__syncthreads();
 	const bool staged = S.cs[64] <= p.s_cap;
-	// cell-major, each staged cell's molecules in their (id) order
-	if (staged) {
-		for (int c = warp; c < 64; c += kWarps) {
-			const int st = S.gst[c], cnt = S.cnt[c], base = S.cs[c];
-			const double kx = S.ck[3 * c], ky = S.ck[3 * c + 1], kz = S.ck[3 * c + 2];
-			const double shx = S.csh[3 * c], shy = S.csh[3 * c + 1], shz = S.csh[3 * c + 2];
-			for (int e = lane; e < cnt; e += 32) {
-				const int gi = st + e;
-				const double x = rx[gi], y = ry[gi], z = rz[gi];
-				const double Xd = __dadd_rn(x, kx), Yd = __dadd_rn(y, ky), Zd = __dadd_rn(z, kz);
-				const float X = __double2float_rn(Xd), Y = __double2float_rn(Yd), Z = __double2float_rn(Zd);
-				const int slot_s = base + e;
-				const unsigned w = pack_lo(__double2float_rn(Xd - (double) X), __double2float_rn(Yd - (double) Y),
-				                           __double2float_rn(Zd - (double) Z), cid[gi], bx);
-				S.hi[slot_s] = make_float4(X, Y, Z, __uint_as_float(w));
-				if (kHalf) {
-					// half-precision copy relative to the brick centre (slot pairs share one HalfPair)
-					__half* hp = S.h + 8 * (slot_s >> 1) + (slot_s & 1);
-					hp[0] = __float2half_rn(X - bx.frame_c[0]);
-					hp[2] = __float2half_rn(Y - bx.frame_c[1]);
-					hp[4] = __float2half_rn(Z - bx.frame_c[2]);
-				}
-				if (kFP64) {
-					S.img[slot_s] = __dadd_rn(x, shx);
-					S.img[p.s_cap + slot_s] = __dadd_rn(y, shy);
-					S.img[2 * p.s_cap + slot_s] = __dadd_rn(z, shz);
+	// cell-major, each staged cell's molecules in their (id) order. A warp stages cells warp,
+	// warp + 8, ...; kWide: four cells per round, every load of the round issued before the first
+	// store (the stores to shared memory would otherwise hold back the next cell's loads). The
+	// persistent ensemble kernel, at its register limit, stages one cell at a time.
+	if (staged && !kWide) {
+		for (int c = warp; c < 64; c += kWarps)
+			for (int e = lane; e < S.cnt[c]; e += 32) {
+				const int gi = S.gst[c] + e;
+				stage_one<kFP64, kHalf>(p, bx, S, c, e, rx[gi], ry[gi], rz[gi], cid[gi]);
+			}
+	}
+	if (staged && kWide) {
+		for (int c0 = warp; c0 < 64; c0 += 4 * kWarps) {
+			double x[4], y[4], z[4];
+			int q[4];
+#pragma unroll
+			for (int u = 0; u < 4; u++) {
+				const int c = c0 + u * kWarps;
+				const int gi = S.gst[c] + lane;
+				const bool a = lane < S.cnt[c];
+				x[u] = a ? rx[gi] : 0.0;
+				y[u] = a ? ry[gi] : 0.0;
+				z[u] = a ? rz[gi] : 0.0;
+				q[u] = a ? cid[gi] : 0;
+			}
+#pragma unroll
+			for (int u = 0; u < 4; u++) {
+				const int c = c0 + u * kWarps;
+				const int cnt = S.cnt[c];
+				if (lane < cnt) stage_one<kFP64, kHalf>(p, bx, S, c, lane, x[u], y[u], z[u], q[u]);
+				for (int e = lane + 32; e < cnt; e += 32) {
+					const int gi = S.gst[c] + e;
+					stage_one<kFP64, kHalf>(p, bx, S, c, e, rx[gi], ry[gi], rz[gi], cid[gi]);
 				}
 			}
 		}
@@ -446,7 +479,7 @@ constexpr unsigned short kListOverflow = 0xffff;
 // Forces on the molecules of brick `brick` (index within its box) of box `bx`; U, W and the pair
 // count go to partials[slot]. The pair table must already be in shared memory (load_params).
 // Ends with a CTA-wide barrier after which no thread reads the staged data.
-template <bool kFP64, bool kSingle, bool kLjIsRc, int kCap>
+template <bool kFP64, bool kSingle, bool kLjIsRc, int kCap, bool kWide = true>
 __device__ __forceinline__ void pairs(const Const& p, const Box& bx, int brick, int64_t slot, unsigned char* smem,
                                       const double* rx, const double* ry, const double* rz, const int32_t* cid,
                                       const int32_t* cstart, double* fx, double* fy, double* fz, double* partials,
@@ -465,7 +498,7 @@ __device__ __forceinline__ void pairs(const Const& p, const Box& bx, int brick, 
 	const Grid& g = bx.g;
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 	const int ns = p.ns;
-	const bool staged = stage<kFP64>(p, bx, brick, S, rx, ry, rz, cid, cstart);
+	const bool staged = stage<kFP64, true, kWide>(p, bx, brick, S, rx, ry, rz, cid, cstart);
 
 	// ---- pairs: warp w owns brick cell (1 + (w&1), 1 + ((w>>1)&1), 1 + (w>>2)) -----------------
 	double U = 0.0, W = 0.0, NP = 0.0;
@@ -899,18 +932,34 @@ __device__ __forceinline__ double acc_sum(const float* a) {
 	return (double) a[0];
 }
 
+// Where the evaluation of a prune step writes the inner lists: the entries of each molecule's build
+// list whose squared staged distance is below rp2f, in list order, in the layout of Lists::nbr.
+struct PruneOut {
+	unsigned short* nbr;
+	unsigned short* count;
+	float rp2f;
+};
+
+// Entries of each thread's ring in shared memory in a prune step: up to 7 unwritten entries plus the
+// 8 of one block; entry k of thread t at k * kThreads + t (a warp's stores of one entry each fall in
+// 16 banks). The prune variant's shared memory is the layout's plus kPruneRingBytes.
+constexpr int kPruneRing = 16;
+constexpr size_t kPruneRingBytes = sizeof(unsigned short) * kPruneRing * kThreads;
+
 // A warp evaluates the lists of the brick's own molecules t0 .. t1-1 (in the order of the own cells
 // own[0..8] / ocell[0..7]), lpm lanes per molecule (a power of two, (t1 - t0) * lpm <= 32): lane
 // sub = lane % lpm takes the blocks sub, sub + lpm, ... of its molecule's list, the lanes' forces
 // are summed by a fixed butterfly and the molecule is finished by its first lane; U, W, the pair
-// count and the same-position flag are accumulated into the caller's sums.
-template <bool kFP64, bool kSingle, bool kLjIsRc, bool kClampJ = false>
+// count and the same-position flag are accumulated into the caller's sums. kPrune (a prune step, one
+// lane per molecule): the entries also pass the prune test into the molecule's inner list (po).
+template <bool kFP64, bool kSingle, bool kLjIsRc, bool kClampJ = false, bool kPrune = false>
 __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const Smem& S, const int* s_own,
                                            const int* s_ocell, int t0, int t1, int lpm, const double* rx,
                                            const double* ry,
                                            const double* rz, const int32_t* cid, const int32_t* cstart, double* fx,
                                            double* fy, double* fz, int* status, const Lists& lists, const Kick& kick,
-                                           double& U, double& W, double& NP, double& MV, bool& same) {
+                                           double& U, double& W, double& NP, double& MV, bool& same,
+                                           const PruneOut& po = PruneOut{}, unsigned short* ring = nullptr) {
 	const int lane = threadIdx.x & 31;
 	const int ns = p.ns;
 	const float eps24_1 = S.pf[0], sig2_1 = S.pf[KK], shift6_1 = S.pf[2 * KK];
@@ -951,6 +1000,22 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 	const int nk = (nb8 + lpm - 1) / lpm;
 	double Fx = 0.0, Fy = 0.0, Fz = 0.0;
 	int anp = 0;
+	// a prune step: kept entries go through this thread's ring and leave it in blocks of 8
+	int kept = 0, done = 0;
+	uint4* const pdst = kPrune ? reinterpret_cast<uint4*>(po.nbr) + gi : nullptr;
+	auto keep = [&](unsigned e) {
+		ring[(kept & (kPruneRing - 1)) * kThreads] = (unsigned short) e;
+		kept++;
+	};
+	auto flush = [&]() {
+		unsigned v[4];
+#pragma unroll
+		for (int q = 0; q < 4; q++)
+			v[q] = (unsigned) ring[((done + 2 * q) & (kPruneRing - 1)) * kThreads] |
+			       ((unsigned) ring[((done + 2 * q + 1) & (kPruneRing - 1)) * kThreads] << 16);
+		pdst[(int64_t) (done >> 3) * lists.n] = make_uint4(v[0], v[1], v[2], v[3]);
+		done += 8;
+	};
 	uint4 nxt = sub < nb8 ? my8[(int64_t) sub * lists.n] : make_uint4(0u, 0u, 0u, 0u);
 	if (kFP64) {
 		double ax[2] = {0, 0}, ay[2] = {0, 0}, az[2] = {0, 0}, au[2] = {0, 0}, aw[2] = {0, 0};
@@ -965,7 +1030,14 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 				const int j = min((int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu), p.s_cap - 1);
 				if (kk < cnt) lj64<kSingle>(p, xi, yi, zi, ti, ns, j, S, ax[u & 1], ay[u & 1], az[u & 1], au[u & 1],
 				                            aw[u & 1], anp, same);
+				if (kPrune && kk < cnt) {
+					// the prune test on the staged hi parts (rp2f covers the lo parts)
+					const float4 hj = S.hi[j];
+					const float d0 = hi_i.x - hj.x, d1 = hi_i.y - hj.y, d2 = hi_i.z - hj.z;
+					if (fmaf(d0, d0, fmaf(d1, d1, d2 * d2)) < po.rp2f) keep((unsigned) j);
+				}
 			}
+			if (kPrune && kept - done >= 8) flush();
 		}
 		Fx += ax[0] + ax[1];
 		Fy += ay[0] + ay[1];
@@ -1036,6 +1108,7 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 				const float e2 = fmaf(g2, bx.lo_step[2], h2);
 				const float d2f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2));
 				const bool in = d2f < p.rc2f;
+				if (kPrune && d2f < po.rp2f) keep((unsigned) j);   // padding is far: never kept
 				// within a few ulp of rc: decided after the block as the FP64 computation does
 				amb |= fabsf(d2f - p.rc2f) <= p.band;
 				anp += in ? 1 : 0;
@@ -1067,6 +1140,7 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 					aw[a] += r;
 				}
 			}
+			if (kPrune && kept - done >= 8) flush();
 			if (__any_sync(kFull, amb)) {
 				// rare: pairs within a few ulp of rc whose FP64 decision differs from the FP32 one
 #pragma unroll 1
@@ -1112,6 +1186,14 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 		}
 	}
 	NP += (double) anp;
+	if (kPrune) {
+		// the last block padded with the sentinel slot; the inner count (lpm is 1 here)
+		if (kept > done) {
+			for (int k = kept; k < done + 8; k++) ring[(k & (kPruneRing - 1)) * kThreads] = (unsigned short) lists.sentinel;
+			flush();
+		}
+		if (act) po.count[gi] = ovf ? kListOverflow : (unsigned short) kept;
+	}
 	// the molecule's force: its lanes' partial sums in a fixed order
 	for (int o = 1; o < lpm; o <<= 1) {
 		Fx += __shfl_xor_sync(kFull, Fx, o);
@@ -1126,17 +1208,18 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 // own cells, 32 per warp regardless of their cell, each evaluate their list with the exact cutoff.
 // Chunks of 64 entries are summed in FP32 and added to FP64 accumulators.
 // Shared memory: layout(s_cap, kFP64, 0, false) (no filter lists, no half-precision copy).
-template <bool kFP64, bool kSingle, bool kLjIsRc>
+// kPrune: a prune step (the build lists in, the inner lists out through po), one lane per molecule.
+template <bool kFP64, bool kSingle, bool kLjIsRc, bool kWide = true, bool kPrune = false>
 __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int brick, int64_t slot,
                                            unsigned char* smem, const double* rx, const double* ry, const double* rz,
                                            const int32_t* cid, const int32_t* cstart, double* fx, double* fy,
                                            double* fz, double* partials, int* status, const Lists lists,
-                                           const Kick& kick) {
+                                           const Kick& kick, const PruneOut& po = PruneOut{}) {
 	const SmemLayout L = layout(p.s_cap, kFP64, 0, false);
 	const Smem S = views(smem, L);
 	const int tid = threadIdx.x, warp = tid >> 5;
 	const int ns = p.ns;
-	const bool staged = stage<kFP64, false>(p, bx, brick, S, rx, ry, rz, cid, cstart);
+	const bool staged = stage<kFP64, false, kWide>(p, bx, brick, S, rx, ry, rz, cid, cstart);
 	__shared__ int s_own[9], s_ocell[8];
 	if (tid == 0) {
 		// sentinel slot: far from every molecule (entries past a list's end point to it)
@@ -1175,109 +1258,17 @@ __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int br
 		for (int base = 0; base < n_own; base += kThreads) {
 			const int m = min(kThreads, n_own - base);
 			const int g = base == 0 ? 32 : (m + kWarps - 1) / kWarps;
-			const int lpm = lanes_per_molecule(g);
+			const int lpm = kPrune ? 1 : lanes_per_molecule(g);
 			const int w0 = base + warp * g, w1 = min(w0 + g, base + m);
 			if (w0 < w1)
-				list_chunk<kFP64, kSingle, kLjIsRc>(p, bx, S, s_own, s_ocell, w0, w1, lpm, rx, ry, rz, cid, cstart, fx,
-				                                    fy, fz, status, lists, kick, U, W, NP, MV, same);
+				list_chunk<kFP64, kSingle, kLjIsRc, false, kPrune>(p, bx, S, s_own, s_ocell, w0, w1, lpm, rx, ry, rz, cid,
+				                                                   cstart, fx, fy, fz, status, lists, kick, U, W, NP,
+				                                                   MV, same, po,
+				                                                   reinterpret_cast<unsigned short*>(smem + L.total) + tid);
 		}
 	}
 	if (same) atomicOr(status, kStatusSamePosition);
 	block_sum3_at(U, W, NP, partials, slot, MV);
-}
-
-// Entries of each thread's ring in prune_lists: up to 7 unwritten entries plus the 8 of one block.
-constexpr int kPruneRing = 16;
-
-// Shared-memory bytes of prune_lists for a staged capacity s_cap.
-__host__ __device__ inline size_t prune_bytes(int s_cap) {
-	return layout(s_cap, false, 0, false).total + sizeof(unsigned short) * kPruneRing * kThreads;
-}
-
-// Pruning of the lists of brick `brick`: with the positions staged as list_pairs stages them, each own
-// molecule (one thread each) keeps the entries of its build list (`outer`) whose squared distance
-// in the staged frame is below rp2f, in list order, and writes them to `inner` in the same layout,
-// the last block padded with the sentinel slot. rp2f is (rc + prune)^2 plus a margin that covers
-// the rounding of that distance. A brick whose region exceeds the staged capacity is skipped: the
-// evaluation gathers it from global memory without reading its lists.
-__device__ __forceinline__ void prune_lists(const Const& p, const Box& bx, int brick, unsigned char* smem,
-                                            const double* rx, const double* ry, const double* rz,
-                                            const int32_t* cid, const int32_t* cstart, const Lists& outer,
-                                            const Lists& inner, float rp2f) {
-	const SmemLayout L = layout(p.s_cap, false, 0, false);
-	const Smem S = views(smem, L);
-	// ring entry k of thread t at k * kThreads + t: a warp's writes of one entry each fall in 16 banks
-	unsigned short* ring = reinterpret_cast<unsigned short*>(smem + L.total);
-	const int tid = threadIdx.x;
-	const bool staged = stage<false, false>(p, bx, brick, S, rx, ry, rz, cid, cstart);
-	__shared__ int s_own[9], s_ocell[8];
-	if (tid == 0) {
-		int acc = 0;
-		for (int w = 0; w < 8; w++) {
-			int ic;
-			const bool ok = own_cell(bx, brick, w, ic);
-			s_own[w] = acc;
-			s_ocell[w] = ic;
-			acc += ok ? S.cnt[ic] : 0;
-		}
-		s_own[8] = acc;
-	}
-	__syncthreads();
-	if (!staged) return;
-	const int n_own = s_own[8];
-	const unsigned sent = (unsigned) outer.sentinel;
-	for (int t = tid; t < n_own; t += kThreads) {
-		int w = 0;
-		while (w < 7 && s_own[w + 1] <= t) w++;
-		const int slot_i = S.cs[s_ocell[w]] + (t - s_own[w]);
-		const int gi = S.gst[s_ocell[w]] + (t - s_own[w]);
-		const int cnt = outer.count[gi];
-		if (cnt == kListOverflow) {
-			inner.count[gi] = kListOverflow;
-			continue;
-		}
-		const float4 hi_i = S.hi[slot_i];
-		const unsigned wi = __float_as_uint(hi_i.w);
-		const float mix = __uint_as_float(0x4B000000u | (wi & 511u));
-		const float miy = __uint_as_float(0x4B000000u | ((wi >> 9) & 511u));
-		const float miz = __uint_as_float(0x4B000000u | ((wi >> 18) & 511u));
-		const uint4* src = reinterpret_cast<const uint4*>(outer.nbr) + gi;
-		uint4* dst = reinterpret_cast<uint4*>(inner.nbr) + gi;
-		const int nblk = (cnt + 7) >> 3;
-		int kept = 0, done = 0;
-		auto flush = [&]() {
-			unsigned v[4];
-#pragma unroll
-			for (int k = 0; k < 4; k++)
-				v[k] = (unsigned) ring[((done + 2 * k) & (kPruneRing - 1)) * kThreads + tid] |
-				       ((unsigned) ring[((done + 2 * k + 1) & (kPruneRing - 1)) * kThreads + tid] << 16);
-			dst[(int64_t) (done >> 3) * outer.n] = make_uint4(v[0], v[1], v[2], v[3]);
-			done += 8;
-		};
-		for (int b = 0; b < nblk; b++) {
-			const uint4 cur = src[(int64_t) b * outer.n];
-#pragma unroll
-			for (int u = 0; u < 8; u++) {
-				const int j = min((int) ((list_word(cur, u >> 1) >> (16 * (u & 1))) & 0xffffu), p.s_cap);
-				const float4 hj = S.hi[j];
-				const unsigned wj = __float_as_uint(hj.w);
-				const float e0 = fmaf(mix - __uint_as_float(0x4B000000u | (wj & 511u)), bx.lo_step[0], hi_i.x - hj.x);
-				const float e1 = fmaf(miy - __uint_as_float(0x4B000000u | ((wj >> 9) & 511u)), bx.lo_step[1], hi_i.y - hj.y);
-				const float e2 = fmaf(miz - __uint_as_float(0x4B000000u | ((wj >> 18) & 511u)), bx.lo_step[2], hi_i.z - hj.z);
-				const float d2f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2));
-				if (8 * b + u < cnt && d2f < rp2f) {
-					ring[(kept & (kPruneRing - 1)) * kThreads + tid] = (unsigned short) j;
-					kept++;
-				}
-			}
-			if (kept - done >= 8) flush();
-		}
-		if (kept > done) {
-			for (int k = kept; k < done + 8; k++) ring[(k & (kPruneRing - 1)) * kThreads + tid] = (unsigned short) sent;
-			flush();
-		}
-		inner.count[gi] = (unsigned short) kept;
-	}
 }
 
 // A sparse brick (see kSparseCap) by one warp, in its own shared-memory area laid out as

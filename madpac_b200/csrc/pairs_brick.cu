@@ -52,42 +52,39 @@ __global__ void __launch_bounds__(brick::kThreads, 3)
 	}
 }
 
-// Pruning step of the pruned lists: runs when this step builds the lists or when the summed largest
-// drifts since the last prune have reached half the inner skin; then every brick's inner lists
-// from its build lists at the current positions (a resident grid walks the bricks).
-__global__ void __launch_bounds__(brick::kThreads, 2)
-    k_prune_lists(brick::Const p, brick::Box bx, int nbricks, const double* __restrict__ rx,
-                  const double* __restrict__ ry, const double* __restrict__ rz, const int32_t* __restrict__ cid,
-                  const int32_t* __restrict__ cstart, const int* __restrict__ gate, int step, brick::Lists outer,
-                  brick::Lists inner, float rp2f, double half_prune) {
-	const PruneState* st = inner.pst;
-	const double moved = st->acc + sqrt((double) __uint_as_float(st->dmax[step & 1]));
-	if (*gate != step && moved < half_prune) return;
-	if (blockIdx.x == 0 && threadIdx.x == 0) {
-		inner.pst->pruned = step;
-		inner.pst->count++;
-	}
-	extern __shared__ __align__(16) unsigned char smem[];
-	for (int b = blockIdx.x; b < nbricks; b += gridDim.x) {
-		brick::prune_lists(p, bx, b, smem, rx, ry, rz, cid, cstart, outer, inner, rp2f);
-		__syncthreads();
-	}
-}
-
 #ifndef MDGPU_LIST_MINB
 #define MDGPU_LIST_MINB 3
 #endif
 // Resident CTAs per SM of the FP32 list kernel (registers and shared memory are sized for it).
 constexpr int kListMinBlocks = MDGPU_LIST_MINB;
 
-template <bool kFP64, bool kSingle, bool kLjIsRc>
+// The list evaluation of a step. With pruned lists (lists.pst set) it comes in two variants, launched
+// one after the other in every step: kPrune runs in the steps that prune (the lists were built in
+// this step, or the summed largest drifts since the last prune reached half_prune), reads the build
+// lists and writes the inner lists (po) besides the forces; the plain variant runs in the other
+// steps and reads the inner lists.
+template <bool kFP64, bool kSingle, bool kLjIsRc, bool kPrune = false>
 __global__ void __launch_bounds__(brick::kThreads, kFP64 ? 2 : kListMinBlocks)
     k_pairs_list(brick::Const p, brick::Box bx, const double* __restrict__ rx, const double* __restrict__ ry,
                  const double* __restrict__ rz, const int32_t* __restrict__ cid,
                  const int32_t* __restrict__ cstart, const PairParams* __restrict__ pp,
                  double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
                  double* __restrict__ partials, int* __restrict__ status, const int* __restrict__ gate,
-                 brick::Lists lists, unsigned* tickets, double* scalars, brick::Kick kick, double* record) {
+                 brick::Lists lists, unsigned* tickets, double* scalars, brick::Kick kick, double* record,
+                 brick::PruneOut po, double half_prune) {
+	if (lists.pst) {
+		const PruneState* st = lists.pst;
+		if (kPrune) {
+			const double moved = st->acc + sqrt((double) __uint_as_float(st->dmax[lists.step & 1]));
+			if (*gate != lists.step && moved < half_prune) return;
+			if (blockIdx.x == 0 && threadIdx.x == 0) {
+				lists.pst->pruned = lists.step;
+				lists.pst->count++;
+			}
+		} else if (st->pruned == lists.step) {
+			return;   // the prune variant evaluated this step
+		}
+	}
 	extern __shared__ __align__(16) unsigned char smem[];
 	__shared__ int s_item;
 	brick::load_params(smem, brick::layout(p.s_cap, kFP64, 0, false), pp, p.ns);
@@ -95,8 +92,8 @@ __global__ void __launch_bounds__(brick::kThreads, kFP64 ? 2 : kListMinBlocks)
 	if (lists.kind == nullptr) {
 		// every brick, one CTA each
 		__syncthreads();
-		brick::list_pairs<kFP64, kSingle, kLjIsRc>(p, bx, blockIdx.x, blockIdx.x, smem, rx, ry, rz, cid, cstart, fx,
-		                                           fy, fz, partials, status, lists, kick);
+		brick::list_pairs<kFP64, kSingle, kLjIsRc, true, kPrune>(p, bx, blockIdx.x, blockIdx.x, smem, rx, ry, rz, cid,
+		                                                         cstart, fx, fy, fz, partials, status, lists, kick, po);
 	} else {
 		// the dense bricks of the last build (the sparse ones go to k_pairs_list_sparse): a resident
 		// grid takes them from a queue
@@ -108,8 +105,8 @@ __global__ void __launch_bounds__(brick::kThreads, kFP64 ? 2 : kListMinBlocks)
 			const int item = s_item;
 			if (item >= nwork) break;
 			const int b = lists.blist[item];
-			brick::list_pairs<kFP64, kSingle, kLjIsRc>(p, bx, b, b, smem, rx, ry, rz, cid, cstart, fx, fy, fz,
-			                                           partials, status, lists, kick);
+			brick::list_pairs<kFP64, kSingle, kLjIsRc, true, kPrune>(p, bx, b, b, smem, rx, ry, rz, cid, cstart, fx, fy,
+			                                                         fz, partials, status, lists, kick, po);
 		}
 	}
 	__syncthreads();
@@ -124,7 +121,7 @@ __global__ void __launch_bounds__(brick::kThreads, kFP64 ? 2 : kListMinBlocks)
 			// the drift into this step's positions joins the sum, which a prune at this step restarts
 			PruneState* st = lists.pst;
 			const int par = lists.step & 1;
-			st->acc = st->pruned == lists.step ? 0.0 : st->acc + sqrt((double) __uint_as_float(st->dmax[par]));
+			st->acc = kPrune ? 0.0 : st->acc + sqrt((double) __uint_as_float(st->dmax[par]));
 			st->dmax[par] = 0u;
 		}
 		if (record) {
@@ -219,6 +216,7 @@ Plan plan(Context* c, const Grid& g, double filter_radius, int kind) {
 	const int max_optin = device_max_optin(c->device);
 	size_t budget = 110 * 1024;
 	if (kind == 2 && !fp64) budget = std::min(budget, (size_t) (224 / kListMinBlocks - 2) * 1024);
+	if (kind == 2 && pruning(c)) budget -= brick::kPruneRingBytes;   // the prune variant's ring
 	if (budget > (size_t) max_optin) budget = (size_t) max_optin;
 	const int lcap = kind == 2 ? 0 : kListCap;
 	const bool half = kind != 2;
@@ -242,21 +240,27 @@ cudaError_t go(Context* c, const Plan& P, K kern, const int* gate, const brick::
 	return r;
 }
 
-// kind 0: plain traversal, 2: list evaluation of the skin mode
-template <int kKind>
+// kind 0: plain traversal, 2: list evaluation of the skin mode (kPr: its prune variant)
+template <int kKind, bool kPr = false>
 cudaError_t dispatch(Context* c, const Plan& P, const int* gate, const brick::Lists& lists,
-                     const brick::Kick& kick = brick::Kick{}, double* record = nullptr) {
+                     const brick::Kick& kick = brick::Kick{}, double* record = nullptr,
+                     const brick::PruneOut& po = brick::PruneOut{}, double half_prune = 0.0) {
 	const bool fp64 = c->precision == MDGPU_FP64;
 	const bool single = c->sp.n == 1, ljrc = c->rc_lj == c->rc;
 	if (kKind == 2) {
 		unsigned* t = c->tickets;
 		double* out = c->scalars;
-		if (fp64) return single ? go(c, P, k_pairs_list<true, true, false>, gate, lists, t, out, kick, record)
-		                        : go(c, P, k_pairs_list<true, false, false>, gate, lists, t, out, kick, record);
-		if (ljrc) return single ? go(c, P, k_pairs_list<false, true, true>, gate, lists, t, out, kick, record)
-		                        : go(c, P, k_pairs_list<false, false, true>, gate, lists, t, out, kick, record);
-		return single ? go(c, P, k_pairs_list<false, true, false>, gate, lists, t, out, kick, record)
-		              : go(c, P, k_pairs_list<false, false, false>, gate, lists, t, out, kick, record);
+		if (fp64)
+			return single ? go(c, P, k_pairs_list<true, true, false, kPr>, gate, lists, t, out, kick, record, po, half_prune)
+			              : go(c, P, k_pairs_list<true, false, false, kPr>, gate, lists, t, out, kick, record, po,
+			                   half_prune);
+		if (ljrc)
+			return single ? go(c, P, k_pairs_list<false, true, true, kPr>, gate, lists, t, out, kick, record, po, half_prune)
+			              : go(c, P, k_pairs_list<false, false, true, kPr>, gate, lists, t, out, kick, record, po,
+			                   half_prune);
+		return single ? go(c, P, k_pairs_list<false, true, false, kPr>, gate, lists, t, out, kick, record, po, half_prune)
+		              : go(c, P, k_pairs_list<false, false, false, kPr>, gate, lists, t, out, kick, record, po,
+		                   half_prune);
 	}
 	if (fp64) return single ? go(c, P, k_pairs_brick<true, true, false>, gate, lists)
 	                        : go(c, P, k_pairs_brick<true, false, false>, gate, lists);
@@ -333,36 +337,40 @@ cudaError_t launch_pairs_skin(Context* c, int kick_mode, double dt, double* reco
 		k_build_lists<<<grid, brick::kThreads, bbytes, c->stream>>>(bb, nbricks, s_cap, c->p.rx, c->p.ry, c->p.rz,
 		                                                           c->cell_start, c->rebuild, c->step_id, l);
 	int launches = 2;
-	if (pruning(c)) {
-		// pruning (gated), then the evaluation reads the inner lists
-		brick::Lists in = l;
-		in.nbr = c->nbr_in;
-		in.count = c->nbr_in_count;
-		in.pst = c->prune_st;
-		in.step = c->step_id;
-		// (rc + prune)^2 rounded up, with a margin above the rounding of the staged-frame distance
-		// (below 1e-6 of it)
-		const double rp = c->rc + c->prune;
-		const double rp2 = rp * rp * (1.0 + 4e-6);
-		float rp2f = (float) rp2;
-		if ((double) rp2f < rp2) rp2f = std::nextafter(rp2f, 2.0f * rp2f);
-		const size_t pbytes = brick::prune_bytes(P.p.s_cap);
-		if (e == cudaSuccess)
-			e = cudaFuncSetAttribute(k_prune_lists, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) pbytes);
-		const int pgrid = resident_grid(c, k_prune_lists, pbytes, P.nbricks);
-		if (e == cudaSuccess)
-			k_prune_lists<<<pgrid, brick::kThreads, pbytes, c->stream>>>(P.p, P.bx, P.nbricks, c->p.rx, c->p.ry, c->p.rz,
-			                                                             c->p.cid, c->cell_start, c->rebuild, c->step_id,
-			                                                             l, in, rp2f, 0.5 * c->prune);
-		l = in;
+	// pruned lists: the prune variant of the evaluation reads the build lists (and writes the inner
+	// ones) in the steps that prune, the plain variant reads the inner lists in the others; the
+	// sparse bricks always evaluate their build lists
+	brick::Lists inner = l;
+	brick::PruneOut po{};
+	double half_prune = 0.0;
+	const bool prune = pruning(c);
+	if (prune) {
+		l.pst = c->prune_st;
+		l.step = c->step_id;
+		inner = l;
+		inner.nbr = c->nbr_in;
+		inner.count = c->nbr_in_count;
+		po.nbr = c->nbr_in;
+		po.count = c->nbr_in_count;
+		// the FP64 form tests the staged hi parts only: the lo parts (at most 256 steps each way
+		// per coordinate, plus half a step of quantisation) move the distance by at most
+		// sqrt(3) * 513 steps; the float arithmetic by a few 1e-7 of it
+		const double lo = 520.0 * std::max(P.bx.lo_step[0], std::max(P.bx.lo_step[1], P.bx.lo_step[2]));
+		const double rp = c->rc + c->prune + 1.7320508075688772 * lo;
+		const double rp2 = rp * rp * (1.0 + 2e-6);
+		po.rp2f = (float) rp2;
+		if ((double) po.rp2f < rp2) po.rp2f = std::nextafter(po.rp2f, 2.0f * po.rp2f);
+		// prune when the drifts reach half the inner skin, less a margin that keeps every pair left
+		// out farther than rc (1 + 1e-5) from the other molecule until then
+		half_prune = 0.5 * c->prune - 1e-5 * (c->rc + c->prune);
 		launches++;
 	}
 	// evaluation, every step: sparse bricks one warp each, then the others (whose last CTA sums the
 	// partials of all bricks). When the last build of an earlier run found no sparse brick the
 	// dense kernel takes every brick (kind not consulted) and the sparse kernel is not launched.
 	const bool sparse = !c->h_sparse || *(volatile int*) c->h_sparse != 0;
-	brick::Lists ld = l;
-	if (!sparse) ld.kind = nullptr;
+	brick::Lists ld = l, ldi = inner;
+	if (!sparse) ld.kind = ldi.kind = nullptr;
 	if (e == cudaSuccess && sparse) {
 		const bool fp64 = c->precision == MDGPU_FP64;
 		const bool single = c->sp.n == 1, ljrc = c->rc_lj == c->rc;
@@ -379,7 +387,12 @@ cudaError_t launch_pairs_skin(Context* c, int kick_mode, double dt, double* reco
 			                                                   c->cell_start, c->d_pp, c->p.fx, c->p.fy, c->p.fz,
 			                                                   c->partials, c->status, l, kick);
 	}
-	if (e == cudaSuccess) e = dispatch<2>(c, P, nullptr, ld, kick, record);
+	if (e == cudaSuccess && prune) {
+		Plan Pp = P;
+		Pp.bytes += brick::kPruneRingBytes;
+		e = dispatch<2, true>(c, Pp, c->rebuild, ld, kick, record, po, half_prune);
+	}
+	if (e == cudaSuccess) e = dispatch<2>(c, P, nullptr, prune ? ldi : ld, kick, record);
 	if (e == cudaSuccess) e = cudaGetLastError();
 	prof_end(c, 1, sparse ? launches + 1 : launches);
 	return e;
