@@ -950,8 +950,8 @@ constexpr size_t kPruneRingBytes = sizeof(unsigned short) * kPruneRing * kThread
 // own[0..8] / ocell[0..7]), lpm lanes per molecule (a power of two, (t1 - t0) * lpm <= 32): lane
 // sub = lane % lpm takes the blocks sub, sub + lpm, ... of its molecule's list, the lanes' forces
 // are summed by a fixed butterfly and the molecule is finished by its first lane; U, W, the pair
-// count and the same-position flag are accumulated into the caller's sums. kPrune (a prune step, one
-// lane per molecule): the entries also pass the prune test into the molecule's inner list (po).
+// count and the same-position flag are accumulated into the caller's sums. kPrune (a prune step): the
+// entries also pass the prune test into the molecule's inner list (po).
 template <bool kFP64, bool kSingle, bool kLjIsRc, bool kClampJ = false, bool kPrune = false>
 __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const Smem& S, const int* s_own,
                                            const int* s_ocell, int t0, int t1, int lpm, const double* rx,
@@ -1000,12 +1000,15 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 	const int nk = (nb8 + lpm - 1) / lpm;
 	double Fx = 0.0, Fy = 0.0, Fz = 0.0;
 	int anp = 0;
-	// a prune step: kept entries go through this thread's ring and leave it in blocks of 8
+	// a prune step: kept entries go through this thread's ring and leave it in blocks of 8, the
+	// lane's k-th block at inner block sub + k lpm (the blocks it would read at this split)
 	int kept = 0, done = 0;
 	uint4* const pdst = kPrune ? reinterpret_cast<uint4*>(po.nbr) + gi : nullptr;
-	auto keep = [&](unsigned e) {
+	// branch-free: every entry is stored at the next free place, which only a kept entry takes
+	// (at most 15 entries are unwritten, so the next free place is never one of them)
+	auto keep = [&](unsigned e, bool k) {
 		ring[(kept & (kPruneRing - 1)) * kThreads] = (unsigned short) e;
-		kept++;
+		kept += k ? 1 : 0;
 	};
 	auto flush = [&]() {
 		unsigned v[4];
@@ -1013,7 +1016,7 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 		for (int q = 0; q < 4; q++)
 			v[q] = (unsigned) ring[((done + 2 * q) & (kPruneRing - 1)) * kThreads] |
 			       ((unsigned) ring[((done + 2 * q + 1) & (kPruneRing - 1)) * kThreads] << 16);
-		pdst[(int64_t) (done >> 3) * lists.n] = make_uint4(v[0], v[1], v[2], v[3]);
+		pdst[(int64_t) (sub + (done >> 3) * lpm) * lists.n] = make_uint4(v[0], v[1], v[2], v[3]);
 		done += 8;
 	};
 	uint4 nxt = sub < nb8 ? my8[(int64_t) sub * lists.n] : make_uint4(0u, 0u, 0u, 0u);
@@ -1027,14 +1030,16 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 #pragma unroll
 			for (int u = 0; u < 8; u++) {
 				const int kk = 8 * b + u;
-				const int j = min((int) ((e[u >> 1] >> (16 * (u & 1))) & 0xffffu), p.s_cap - 1);
-				if (kk < cnt) lj64<kSingle>(p, xi, yi, zi, ti, ns, j, S, ax[u & 1], ay[u & 1], az[u & 1], au[u & 1],
+				const unsigned raw = (e[u >> 1] >> (16 * (u & 1))) & 0xffffu;
+				const int j = min((int) raw, p.s_cap - 1);
+				// (a pruned list may hold sentinel slots before its end)
+				if (kk < cnt && raw < (unsigned) p.s_cap) lj64<kSingle>(p, xi, yi, zi, ti, ns, j, S, ax[u & 1], ay[u & 1], az[u & 1], au[u & 1],
 				                            aw[u & 1], anp, same);
-				if (kPrune && kk < cnt) {
+				if (kPrune) {
 					// the prune test on the staged hi parts (rp2f covers the lo parts)
 					const float4 hj = S.hi[j];
 					const float d0 = hi_i.x - hj.x, d1 = hi_i.y - hj.y, d2 = hi_i.z - hj.z;
-					if (fmaf(d0, d0, fmaf(d1, d1, d2 * d2)) < po.rp2f) keep((unsigned) j);
+					keep((unsigned) j, kk < cnt && fmaf(d0, d0, fmaf(d1, d1, d2 * d2)) < po.rp2f);
 				}
 			}
 			if (kPrune && kept - done >= 8) flush();
@@ -1108,7 +1113,7 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 				const float e2 = fmaf(g2, bx.lo_step[2], h2);
 				const float d2f = fmaf(e0, e0, fmaf(e1, e1, e2 * e2));
 				const bool in = d2f < p.rc2f;
-				if (kPrune && d2f < po.rp2f) keep((unsigned) j);   // padding is far: never kept
+				if (kPrune) keep((unsigned) j, d2f < po.rp2f);   // padding is far: never kept
 				// within a few ulp of rc: decided after the block as the FP64 computation does
 				amb |= fabsf(d2f - p.rc2f) <= p.band;
 				anp += in ? 1 : 0;
@@ -1187,12 +1192,18 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 	}
 	NP += (double) anp;
 	if (kPrune) {
-		// the last block padded with the sentinel slot; the inner count (lpm is 1 here)
+		// each lane's last block padded with the sentinel slot; the list ends after the molecule's
+		// last written block, and a lane's blocks below that end which it did not fill hold
+		// sentinels only (the evaluation reads them as far away)
 		if (kept > done) {
 			for (int k = kept; k < done + 8; k++) ring[(k & (kPruneRing - 1)) * kThreads] = (unsigned short) lists.sentinel;
 			flush();
 		}
-		if (act) po.count[gi] = ovf ? kListOverflow : (unsigned short) kept;
+		int end = done > 0 ? sub + ((done >> 3) - 1) * lpm + 1 : 0;
+		for (int o = 1; o < lpm; o <<= 1) end = max(end, __shfl_xor_sync(kFull, end, o));
+		const unsigned s2 = (unsigned) lists.sentinel | ((unsigned) lists.sentinel << 16);
+		for (int b = sub + (done >> 3) * lpm; b < end; b += lpm) pdst[(int64_t) b * lists.n] = make_uint4(s2, s2, s2, s2);
+		if (act && sub == 0) po.count[gi] = ovf ? kListOverflow : (unsigned short) (8 * end);
 	}
 	// the molecule's force: its lanes' partial sums in a fixed order
 	for (int o = 1; o < lpm; o <<= 1) {
@@ -1208,7 +1219,7 @@ __device__ __forceinline__ void list_chunk(const Const& p, const Box& bx, const 
 // own cells, 32 per warp regardless of their cell, each evaluate their list with the exact cutoff.
 // Chunks of 64 entries are summed in FP32 and added to FP64 accumulators.
 // Shared memory: layout(s_cap, kFP64, 0, false) (no filter lists, no half-precision copy).
-// kPrune: a prune step (the build lists in, the inner lists out through po), one lane per molecule.
+// kPrune: a prune step (the build lists in, the inner lists out through po).
 template <bool kFP64, bool kSingle, bool kLjIsRc, bool kWide = true, bool kPrune = false>
 __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int brick, int64_t slot,
                                            unsigned char* smem, const double* rx, const double* ry, const double* rz,
@@ -1258,7 +1269,7 @@ __device__ __forceinline__ void list_pairs(const Const& p, const Box& bx, int br
 		for (int base = 0; base < n_own; base += kThreads) {
 			const int m = min(kThreads, n_own - base);
 			const int g = base == 0 ? 32 : (m + kWarps - 1) / kWarps;
-			const int lpm = kPrune ? 1 : lanes_per_molecule(g);
+			const int lpm = lanes_per_molecule(g);
 			const int w0 = base + warp * g, w1 = min(w0 + g, base + m);
 			if (w0 < w1)
 				list_chunk<kFP64, kSingle, kLjIsRc, false, kPrune>(p, bx, S, s_own, s_ocell, w0, w1, lpm, rx, ry, rz, cid,
