@@ -49,8 +49,8 @@ struct PairParams {
 // therefore still beyond rc while 2 acc < prune.
 struct PruneState {
 	unsigned dmax[2];           // float bits of the largest squared drift of the last step of each parity
+	int built;                  // id of the step whose lists were last built (set by the build)
 	int pruned;                 // id of the step whose inner lists were last made
-	int pad;
 	double acc;                 // summed largest drifts since the positions of the last prune
 	unsigned long long count;   // prunes so far
 };

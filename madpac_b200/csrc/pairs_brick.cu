@@ -44,6 +44,7 @@ __global__ void __launch_bounds__(brick::kThreads, 3)
                   const double* __restrict__ ry, const double* __restrict__ rz, const int32_t* __restrict__ cstart,
                   const int* __restrict__ gate, int step, brick::Lists lists) {
 	if (*gate != step) return;
+	if (lists.pst && blockIdx.x == 0 && threadIdx.x == 0) lists.pst->built = step;   // pruned lists: prune now
 	extern __shared__ __align__(16) unsigned char smem[];
 	// a resident grid walks the bricks: a step without a build costs one launch of that grid only
 	for (int b = blockIdx.x; b < nbricks; b += gridDim.x) {
@@ -62,7 +63,8 @@ constexpr int kListMinBlocks = MDGPU_LIST_MINB;
 // one after the other in every step: kPrune runs in the steps that prune (the lists were built in
 // this step, or the summed largest drifts since the last prune reached half_prune), reads the build
 // lists and writes the inner lists (po) besides the forces; the plain variant runs in the other
-// steps and reads the inner lists.
+// steps and reads the inner lists. Both decide from values that no CTA of their launch changes (not
+// from the rebuild flag, which the fused kick of this step may set for the next one).
 template <bool kFP64, bool kSingle, bool kLjIsRc, bool kPrune = false>
 __global__ void __launch_bounds__(brick::kThreads, kFP64 ? 2 : kListMinBlocks)
     k_pairs_list(brick::Const p, brick::Box bx, const double* __restrict__ rx, const double* __restrict__ ry,
@@ -76,7 +78,7 @@ __global__ void __launch_bounds__(brick::kThreads, kFP64 ? 2 : kListMinBlocks)
 		const PruneState* st = lists.pst;
 		if (kPrune) {
 			const double moved = st->acc + sqrt((double) __uint_as_float(st->dmax[lists.step & 1]));
-			if (*gate != lists.step && moved < half_prune) return;
+			if (st->built != lists.step && moved < half_prune) return;
 			if (blockIdx.x == 0 && threadIdx.x == 0) {
 				lists.pst->pruned = lists.step;
 				lists.pst->count++;
@@ -323,23 +325,10 @@ cudaError_t launch_pairs_skin(Context* c, int kick_mode, double dt, double* reco
 	}
 	const Plan P = plan(c, c->gs, c->rc, 2);
 	l.sentinel = P.p.s_cap;   // the evaluation kernel's sentinel slot terminates every list
-	prof_begin(c, 1);
-	// build (gated): half-precision staging only, three CTAs per SM
-	brick::Box bb{};
-	brick::init_box(bb, c->gs, c->rc + c->skin, 0, 0.5 * c->skin);
-	int s_cap = 256;
-	while (brick::build_bytes(s_cap + 64) <= 72 * 1024) s_cap += 64;
-	const size_t bbytes = brick::build_bytes(s_cap);
-	const int nbricks = bb.nb[0] * bb.nb[1] * bb.nb[2];
-	cudaError_t e = cudaFuncSetAttribute(k_build_lists, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bbytes);
-	const int grid = std::min(nbricks, 3 * c->num_sms);   // three CTAs per SM (launch bounds, 72 KB each)
-	if (e == cudaSuccess)
-		k_build_lists<<<grid, brick::kThreads, bbytes, c->stream>>>(bb, nbricks, s_cap, c->p.rx, c->p.ry, c->p.rz,
-		                                                           c->cell_start, c->rebuild, c->step_id, l);
 	int launches = 2;
 	// pruned lists: the prune variant of the evaluation reads the build lists (and writes the inner
 	// ones) in the steps that prune, the plain variant reads the inner lists in the others; the
-	// sparse bricks always evaluate their build lists
+	// sparse bricks always evaluate their build lists; the build records its step in the prune state
 	brick::Lists inner = l;
 	brick::PruneOut po{};
 	double half_prune = 0.0;
@@ -365,6 +354,19 @@ cudaError_t launch_pairs_skin(Context* c, int kick_mode, double dt, double* reco
 		half_prune = 0.5 * c->prune - 1e-5 * (c->rc + c->prune);
 		launches++;
 	}
+	prof_begin(c, 1);
+	// build (gated): half-precision staging only, three CTAs per SM
+	brick::Box bb{};
+	brick::init_box(bb, c->gs, c->rc + c->skin, 0, 0.5 * c->skin);
+	int s_cap = 256;
+	while (brick::build_bytes(s_cap + 64) <= 72 * 1024) s_cap += 64;
+	const size_t bbytes = brick::build_bytes(s_cap);
+	const int nbricks = bb.nb[0] * bb.nb[1] * bb.nb[2];
+	cudaError_t e = cudaFuncSetAttribute(k_build_lists, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bbytes);
+	const int grid = std::min(nbricks, 3 * c->num_sms);   // three CTAs per SM (launch bounds, 72 KB each)
+	if (e == cudaSuccess)
+		k_build_lists<<<grid, brick::kThreads, bbytes, c->stream>>>(bb, nbricks, s_cap, c->p.rx, c->p.ry, c->p.rz,
+		                                                           c->cell_start, c->rebuild, c->step_id, l);
 	// evaluation, every step: sparse bricks one warp each, then the others (whose last CTA sums the
 	// partials of all bricks). When the last build of an earlier run found no sparse brick the
 	// dense kernel takes every brick (kind not consulted) and the sparse kernel is not launched.
@@ -390,7 +392,7 @@ cudaError_t launch_pairs_skin(Context* c, int kick_mode, double dt, double* reco
 	if (e == cudaSuccess && prune) {
 		Plan Pp = P;
 		Pp.bytes += brick::kPruneRingBytes;
-		e = dispatch<2, true>(c, Pp, c->rebuild, ld, kick, record, po, half_prune);
+		e = dispatch<2, true>(c, Pp, nullptr, ld, kick, record, po, half_prune);
 	}
 	if (e == cudaSuccess) e = dispatch<2>(c, P, nullptr, prune ? ldi : ld, kick, record);
 	if (e == cudaSuccess) e = cudaGetLastError();
