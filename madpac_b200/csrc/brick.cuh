@@ -748,7 +748,8 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 			// each lane's entries go through its ring in shared memory and leave it in blocks of
 			// 8 (one 16-byte store each); the rotation by lane spreads the ring writes over banks
 			const int rot = 8 * (lane & 7);
-			for (int b0 = 0; b0 < ncell; b0 += 32) {
+			// the cell's first 32 molecules, a lane each
+			for (int b0 = 0; b0 < min(ncell, 32); b0 += 32) {
 				const bool act = b0 + lane < ncell;
 				const int slot_i = i0 + (act ? b0 + lane : 0);
 				const int gi = st + (slot_i - i0);
@@ -800,6 +801,47 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 							dst[(int64_t) (done >> 3) * lists.n] =
 							    *reinterpret_cast<const uint4*>(ring + ((done + rot) & (kBuildRing - 1)));
 					}
+					lists.count[gi] = cnt <= lists.cap ? (unsigned short) cnt : kListOverflow;
+					lists.rx_ref[gi] = rx[gi];
+					lists.ry_ref[gi] = ry[gi];
+					lists.rz_ref[gi] = rz[gi];
+				}
+			}
+			// the rest of a fuller cell (a liquid's cells hold a few more than 32 now and then): a warp
+			// per molecule and a lane per candidate, with the same half-precision test and the same
+			// candidate order (the even slots of each 32-slot block, then the odd ones), so that each
+			// list is the one a lane of another pass would make, at a fraction of a pass's time
+			const __half rc2_1 = __low2half(rc2h);
+			for (int m = 32; m < ncell; m++) {
+				const int slot_i = i0 + m;
+				const int gi = st + m;
+				const __half* hp = s_h + 8 * (slot_i >> 1) + (slot_i & 1);
+				const __half xi = hp[0], yi = hp[2], zi = hp[4];
+				int cnt = 0;
+				for (int r = 0; r < 9; r++) {
+					const int ky = il[1] + (r % 3) - 1, kz = il[2] + (r / 3) - 1;
+					const int k0 = (il[0] - 1) + 4 * ky + 16 * kz;
+					const int a = s_cs[k0], b = s_cs[k0 + 3];
+					for (int base = a & ~1; base < b; base += 32) {
+						const int j = base + 2 * (lane & 15) + (lane >> 4);
+						bool hit = false;
+						if (j >= a && j < b && j != slot_i) {
+							const __half* hq = s_h + 8 * (j >> 1) + (j & 1);
+							const __half dx = __hsub(xi, hq[0]), dy = __hsub(yi, hq[2]), dz = __hsub(zi, hq[4]);
+							hit = __hlt(__hfma(dx, dx, __hfma(dy, dy, __hmul(dz, dz))), rc2_1);
+						}
+						const unsigned hits = __ballot_sync(kFull, hit);
+						const int k = cnt + __popc(hits & ((1u << lane) - 1u));
+						if (hit && k < lists.cap)
+							lists.nbr[(((int64_t) (k >> 3) * lists.n + gi) << 3) + (k & 7)] = (unsigned short) j;
+						cnt += __popc(hits);
+					}
+				}
+				// the last block of 8, padded with the list kernel's sentinel slot
+				const int k = cnt + lane;
+				if (cnt <= lists.cap && k < ((cnt + 7) & ~7))
+					lists.nbr[(((int64_t) (k >> 3) * lists.n + gi) << 3) + (k & 7)] = (unsigned short) lists.sentinel;
+				if (lane == 0) {
 					lists.count[gi] = cnt <= lists.cap ? (unsigned short) cnt : kListOverflow;
 					lists.rx_ref[gi] = rx[gi];
 					lists.ry_ref[gi] = ry[gi];
