@@ -248,13 +248,14 @@ __device__ __forceinline__ int unpack_cid(unsigned w) { return (int) ((w >> 27) 
 
 // Stages molecule e of staged cell c at double position (x, y, z), component q: the hi/lo frame
 // position, and the half-precision copy or the double image as the staging mode asks.
+// The same with the cell's frame offset (kx, ky, kz) and image shift (shx, shy, shz) given, at slot
+// slot_s.
 template <bool kFP64, bool kHalf>
-__device__ __forceinline__ void stage_one(const Const& p, const Box& bx, const Smem& S, int c, int e, double x,
-                                          double y, double z, int q) {
-	const double Xd = __dadd_rn(x, S.ck[3 * c]), Yd = __dadd_rn(y, S.ck[3 * c + 1]);
-	const double Zd = __dadd_rn(z, S.ck[3 * c + 2]);
+__device__ __forceinline__ void stage_at(const Const& p, const Box& bx, const Smem& S, int slot_s, double x, double y,
+                                         double z, int q, double kx, double ky, double kz, double shx, double shy,
+                                         double shz) {
+	const double Xd = __dadd_rn(x, kx), Yd = __dadd_rn(y, ky), Zd = __dadd_rn(z, kz);
 	const float X = __double2float_rn(Xd), Y = __double2float_rn(Yd), Z = __double2float_rn(Zd);
-	const int slot_s = S.cs[c] + e;
 	const unsigned w = pack_lo(__double2float_rn(Xd - (double) X), __double2float_rn(Yd - (double) Y),
 	                           __double2float_rn(Zd - (double) Z), q, bx);
 	S.hi[slot_s] = make_float4(X, Y, Z, __uint_as_float(w));
@@ -266,10 +267,17 @@ __device__ __forceinline__ void stage_one(const Const& p, const Box& bx, const S
 		hp[4] = __float2half_rn(Z - bx.frame_c[2]);
 	}
 	if (kFP64) {
-		S.img[slot_s] = __dadd_rn(x, S.csh[3 * c]);
-		S.img[p.s_cap + slot_s] = __dadd_rn(y, S.csh[3 * c + 1]);
-		S.img[2 * p.s_cap + slot_s] = __dadd_rn(z, S.csh[3 * c + 2]);
+		S.img[slot_s] = __dadd_rn(x, shx);
+		S.img[p.s_cap + slot_s] = __dadd_rn(y, shy);
+		S.img[2 * p.s_cap + slot_s] = __dadd_rn(z, shz);
 	}
+}
+
+template <bool kFP64, bool kHalf>
+__device__ __forceinline__ void stage_one(const Const& p, const Box& bx, const Smem& S, int c, int e, double x,
+                                          double y, double z, int q) {
+	stage_at<kFP64, kHalf>(p, bx, S, S.cs[c] + e, x, y, z, q, S.ck[3 * c], S.ck[3 * c + 1], S.ck[3 * c + 2],
+	                       S.csh[3 * c], S.csh[3 * c + 1], S.csh[3 * c + 2]);
 }
 
 // Stages the 4x4x4 cells around brick `brick` (positions in the local frame; double images in the
@@ -327,11 +335,15 @@ __device__ __forceinline__ bool stage(const Const& p, const Box& bx, int brick, 
 	// store (the stores to shared memory would otherwise hold back the next cell's loads). The
 	// persistent ensemble kernel, at its register limit, stages one cell at a time.
 	if (staged && !kWide) {
-		for (int c = warp; c < 64; c += kWarps)
-			for (int e = lane; e < S.cnt[c]; e += 32) {
-				const int gi = S.gst[c] + e;
-				stage_one<kFP64, kHalf>(p, bx, S, c, e, rx[gi], ry[gi], rz[gi], cid[gi]);
+		for (int c = warp; c < 64; c += kWarps) {
+			const int st = S.gst[c], cnt = S.cnt[c], base = S.cs[c];
+			const double kx = S.ck[3 * c], ky = S.ck[3 * c + 1], kz = S.ck[3 * c + 2];
+			const double shx = S.csh[3 * c], shy = S.csh[3 * c + 1], shz = S.csh[3 * c + 2];
+			for (int e = lane; e < cnt; e += 32) {
+				const int gi = st + e;
+				stage_at<kFP64, kHalf>(p, bx, S, base + e, rx[gi], ry[gi], rz[gi], cid[gi], kx, ky, kz, shx, shy, shz);
 			}
+		}
 	}
 	if (staged && kWide) {
 		for (int c0 = warp; c0 < 64; c0 += 4 * kWarps) {
@@ -748,8 +760,7 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 			// each lane's entries go through its ring in shared memory and leave it in blocks of
 			// 8 (one 16-byte store each); the rotation by lane spreads the ring writes over banks
 			const int rot = 8 * (lane & 7);
-			// the cell's first 32 molecules, a lane each
-			for (int b0 = 0; b0 < min(ncell, 32); b0 += 32) {
+			for (int b0 = 0; b0 < ncell; b0 += 32) {
 				const bool act = b0 + lane < ncell;
 				const int slot_i = i0 + (act ? b0 + lane : 0);
 				const int gi = st + (slot_i - i0);
@@ -801,47 +812,6 @@ __device__ __forceinline__ void build_lists(const Box& bx, int brick, int s_cap,
 							dst[(int64_t) (done >> 3) * lists.n] =
 							    *reinterpret_cast<const uint4*>(ring + ((done + rot) & (kBuildRing - 1)));
 					}
-					lists.count[gi] = cnt <= lists.cap ? (unsigned short) cnt : kListOverflow;
-					lists.rx_ref[gi] = rx[gi];
-					lists.ry_ref[gi] = ry[gi];
-					lists.rz_ref[gi] = rz[gi];
-				}
-			}
-			// the rest of a fuller cell (a liquid's cells hold a few more than 32 now and then): a warp
-			// per molecule and a lane per candidate, with the same half-precision test and the same
-			// candidate order (the even slots of each 32-slot block, then the odd ones), so that each
-			// list is the one a lane of another pass would make, at a fraction of a pass's time
-			const __half rc2_1 = __low2half(rc2h);
-			for (int m = 32; m < ncell; m++) {
-				const int slot_i = i0 + m;
-				const int gi = st + m;
-				const __half* hp = s_h + 8 * (slot_i >> 1) + (slot_i & 1);
-				const __half xi = hp[0], yi = hp[2], zi = hp[4];
-				int cnt = 0;
-				for (int r = 0; r < 9; r++) {
-					const int ky = il[1] + (r % 3) - 1, kz = il[2] + (r / 3) - 1;
-					const int k0 = (il[0] - 1) + 4 * ky + 16 * kz;
-					const int a = s_cs[k0], b = s_cs[k0 + 3];
-					for (int base = a & ~1; base < b; base += 32) {
-						const int j = base + 2 * (lane & 15) + (lane >> 4);
-						bool hit = false;
-						if (j >= a && j < b && j != slot_i) {
-							const __half* hq = s_h + 8 * (j >> 1) + (j & 1);
-							const __half dx = __hsub(xi, hq[0]), dy = __hsub(yi, hq[2]), dz = __hsub(zi, hq[4]);
-							hit = __hlt(__hfma(dx, dx, __hfma(dy, dy, __hmul(dz, dz))), rc2_1);
-						}
-						const unsigned hits = __ballot_sync(kFull, hit);
-						const int k = cnt + __popc(hits & ((1u << lane) - 1u));
-						if (hit && k < lists.cap)
-							lists.nbr[(((int64_t) (k >> 3) * lists.n + gi) << 3) + (k & 7)] = (unsigned short) j;
-						cnt += __popc(hits);
-					}
-				}
-				// the last block of 8, padded with the list kernel's sentinel slot
-				const int k = cnt + lane;
-				if (cnt <= lists.cap && k < ((cnt + 7) & ~7))
-					lists.nbr[(((int64_t) (k >> 3) * lists.n + gi) << 3) + (k & 7)] = (unsigned short) lists.sentinel;
-				if (lane == 0) {
 					lists.count[gi] = cnt <= lists.cap ? (unsigned short) cnt : kListOverflow;
 					lists.rx_ref[gi] = rx[gi];
 					lists.ry_ref[gi] = ry[gi];
