@@ -310,7 +310,9 @@ int mdgpu_batch_run(mdgpu_batch* b, int32_t nsteps, double dt, double* per_step)
 int mdgpu_batch_set_tiles(mdgpu_batch* b, int32_t list_cap, int32_t ctas_per_sm, int32_t dynamic);
 int mdgpu_batch_get_tiles(const mdgpu_batch* b, int32_t tiles[3]);
 /* Times every tile shape for trial_steps steps from the current state (restored afterwards), keeps
- * the fastest; best: its 3 values, ms: device ms per step of each of the 8 candidates (may be NULL). */
+ * the fastest; best: its 3 values, ms: device ms per step of each of the 8 candidates (may be NULL),
+ * -1 for a candidate not timed: a shape whose staging does not fit, and in the Verlet-skin mode the
+ * list depth other than the current one (the depth does not act on skin-mode lists). */
 int mdgpu_batch_autotune(mdgpu_batch* b, double dt, int32_t trial_steps, int32_t best[3], double* ms);
 /* Device time of the last mdgpu_batch_run (CUDA events around the graph launch). */
 int mdgpu_batch_last_run_ms(const mdgpu_batch* b, double* ms);

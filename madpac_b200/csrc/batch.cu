@@ -1106,11 +1106,15 @@ int mdgpu_batch_autotune(mdgpu_batch* h, double dt, int32_t trial_steps, int32_t
 	Tiles bestt = keep;
 	double bestms = 1e300;
 	int k = 0;
+	// In the Verlet-skin mode the lists live in global memory and the shared-memory layout does not
+	// depend on the list depth (both depths compile to the same register count), so only the current
+	// depth is timed there and the other depth's candidates report -1.
+	const bool skin_mode = b->skin > 0.0;
 	for (int cap : {32, 64})
 		for (int ctas : {1, 2})
 			for (int dyn : {0, 1}) {
 				double t = -1.0;
-				if (!(ctas == 2 && b->max_bin_bytes > 110 * 1024)) {
+				if (!(ctas == 2 && b->max_bin_bytes > 110 * 1024) && !(skin_mode && cap != keep.cap)) {
 					b->tiles = Tiles{cap, ctas, dyn};
 					// warm-up (graph capture), then the timed replay, each from the saved state
 					int st = MDGPU_OK;

@@ -378,7 +378,9 @@ class Batch:
 
     def autotune(self, dt: float, trial_steps: int = 5):
         """Times every tile shape from the current state (restored afterwards) and keeps the fastest.
-        Returns (best (list_cap, ctas_per_sm, dynamic), {candidate: ms per step})."""
+        Returns (best (list_cap, ctas_per_sm, dynamic), {candidate: ms per step}); a candidate not
+        timed reads -1 (staging that does not fit; in the Verlet-skin mode every list depth other
+        than the current one, since the depth does not act on skin-mode lists)."""
         best = np.zeros(3, dtype=np.int32)
         ms = np.zeros(len(self.TILE_CANDIDATES))
         self._check(self.lib.mdgpu_batch_autotune(self.h, float(dt), int(trial_steps), _ptr(best), _ptr(ms)))

@@ -200,6 +200,23 @@ def test_batch_autotune_restores_state():
     c.close()
 
 
+def test_batch_autotune_skin_mode_times_one_list_depth():
+    systems = ensemble(seed=53, sizes=(400, 1600, 3000))
+    b = M.Batch.from_systems(systems, M.MIXED)
+    b.setSkin(0.3)
+    b.prepare()
+    depth = b.tiles()[0]
+    before = b.getParticles()
+    best, ms = b.autotune(DT, trial_steps=3)
+    after = b.getParticles()
+    for key in ("id", "r", "v", "F"):
+        np.testing.assert_array_equal(after[key], before[key])
+    assert best[0] == depth and b.tiles() == best
+    for (cap, _, _), t in ms.items():
+        assert (t > 0) if cap == depth else (t == -1)
+    b.close()
+
+
 def test_batch_barrier_timeout_reports_and_recovers():
     systems = ensemble(seed=61, sizes=(256, 3000, 6000))
     b = M.Batch.from_systems(systems, M.FP64)
